@@ -1,0 +1,205 @@
+/*
+ * jpgpu.h -- C ABI of the B200 engine for md_run's per-step force/integrate path.
+ *
+ * The reference (j_presto md_run, Fortran 90 + OpenMP) has no plugin or FFI layer: its
+ * routines share state through modules.  Each entry point below replaces one reference call
+ * site, named in its comment as file:line inside src_md_run/.  A Fortran driver binds these
+ * through iso_c_binding; the bundled Python/ctypes host does the same.
+ *
+ * Conventions
+ *   - Units follow md_run: Angstrom, fs, amu, kcal/mol, e.  Velocities in Angstrom/fs.
+ *   - real(8) cord(3,N) column-major == C double[N][3]; grad likewise (dE/dx, i.e. -force).
+ *   - Atom indices in jp_system are 0-based unless jp_system.index_base == 1 (Fortran arrays
+ *     can then be passed unchanged).
+ *   - The caller owns every host array; the library copies in and out and keeps no host
+ *     pointer after a call returns.  The library owns all device memory inside jp_ctx.
+ *   - Return codes mirror md_run's `ier`: 0 ok, >0 warning, <0 fatal (JP_E_* below).
+ *   - One host thread per jp_ctx; calls on one context are not re-entrant.
+ */
+#ifndef JPGPU_H
+#define JPGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JP_MAXENE 15      /* energy slots, md_run COMPAR.f90:37 maxene */
+#define JP_MAXNFRG 3      /* cluster-pair classes (ALSD), md_run inpcls.f90 n_matrix */
+
+/* energy slot indices (0-based) of eneval/enevcc, md_run dnergy.f90:17-35 */
+enum {
+  JP_E_TOTAL = 0, JP_E_BOND = 1, JP_E_ANGLE = 2, JP_E_TORS = 3, JP_E_IMPR = 4,
+  JP_E_VDW14 = 5, JP_E_ELE14 = 6, JP_E_VDW15 = 7, JP_E_ELE15 = 8, JP_E_HBOND = 9
+};
+
+/* precision of the force path */
+enum { JP_PREC_FP64 = 0, JP_PREC_MIXED = 1 };
+
+/* METHOD= keyword (md_run inpmd.f90:65, stored as idfvsl) */
+enum { JP_METHOD_CONS = 1, JP_METHOD_MICR = 2, JP_METHOD_CANO = 3, JP_METHOD_GE = 4 };
+
+/* SHAKEM= keyword (inpmd.f90:71, iyfshk): 0 = no SHAKE */
+enum { JP_SHAKE_NONE = 0, JP_SHAKE_HBON = 1, JP_SHAKE_ALLB = 2 };
+
+/* return codes.  Positive values are warnings (md_run ier > 0). */
+enum {
+  JP_OK = 0,
+  JP_W_SHAKE_NOT_CONVERGED = 1,   /* shake.f90:304 ier=1 */
+  JP_E_SHAKE_SINGULAR = -2,       /* shake.f90:288 ier=-2 */
+  JP_E_SHAKE_ABORT = -9999,       /* verlethe.f90:567 dt halving exhausted */
+  JP_E_INVALID = -100,            /* bad argument / inconsistent topology */
+  JP_E_CELL_OVERFLOW = -128,      /* celpar.f90 ier=28 analogue: too many tiles */
+  JP_E_LIST_OVERFLOW = -151,      /* cutoff.f90 ier=51 analogue */
+  JP_E_NONFINITE = -200,          /* non-finite force or coordinate */
+  JP_E_FIXED_OVERFLOW = -201,     /* a force contribution left the 64-bit fixed-point range */
+  JP_E_CUDA = -300,               /* CUDA runtime error */
+  JP_E_NO_DEVICE = -301,
+  JP_E_TIMEOUT = -302             /* a bounded device wait ran out */
+};
+
+/* Generalized-ensemble weight (.nf file, md_run inmcmd.f90:22-40; verlethe.f90:196-321). */
+typedef struct jp_ge {
+  int32_t nwindow, ndeg;
+  const double *coef;        /* [nwindow][ndeg+1]  c(0:ndeg, iwin) */
+  const double *low, *high;  /* [nwindow] window bounds in reduced coordinate */
+  double alphalw, alphaup;   /* d lnP/dE outside [celw, ceup] */
+  double celw, ceup;         /* energy (or lambda) range */
+  double tempce;             /* temperature T0 of the weight */
+  double lower, upper;       /* ALSD linear wall slopes (LMD only) */
+} jp_ge;
+
+/* One replica's system: topology, parameters and coordinates.
+ * Mirrors md_run's COMBAS/COMERG/COMMIS module arrays. */
+typedef struct jp_system {
+  int32_t natom;
+  int32_t index_base;          /* 0 (C) or 1 (Fortran) for every atom index below */
+  double box[3];               /* PBC cell lengths fxcell(1:3) (BOUNDA= PBC) */
+  const double *cord;          /* [natom][3] initial coordinates */
+  const double *vel;           /* [natom][3] initial velocities, v(t-dt/2); NULL = zero */
+  const double *mass;          /* [natom] fxmass */
+  const double *charge;        /* [natom] fxchrg (e) */
+  const int32_t *atype;        /* [natom] LJ type ixatyp */
+  const int32_t *molecule;     /* [natom] molecule-entry id ixamol (sub-system for TEMPCO);
+                                  NULL = one sub-system */
+  int32_t ntype;
+  const double *c6;            /* [ntype][ntype] fynbpp(1,:,:)  E = C12/r^12 - C6/r^6 */
+  const double *c12;           /* [ntype][ntype] fynbpp(2,:,:) */
+  const double *s14_vdw;       /* [ntype] fy14sv, 1-4 vdW scale */
+  const double *s14_ele;       /* [ntype] fy14se, 1-4 electrostatic scale */
+  const int32_t *excl_ptr;     /* [natom+1] CSR of 1-2/1-3/1-4 partners (ix14lt, symmetric) */
+  const int32_t *excl_idx;
+  int32_t nbond;
+  const int32_t *bond;         /* [nbond][2] iypbnd */
+  const double *bond_k, *bond_r0;          /* fyfbnd, fyqbnd */
+  int32_t nangle;
+  const int32_t *angle;        /* [nangle][3] iypang */
+  const double *angle_k, *angle_theta0;    /* fyfang, fyqang (radian) */
+  int32_t ntors;
+  const int32_t *tors;         /* [ntors][4] iyptor */
+  const double *tors_k, *tors_nrot, *tors_phase;   /* fyftor, fytrot, fytphs (radian) */
+  const int32_t *tors_div, *tors_nbf;              /* iytdiv, iytnbf (1 = 1-4 pair counted) */
+  int32_t nimpr;
+  const int32_t *impr;         /* [nimpr][4] iypimp */
+  const double *impr_k, *impr_nrot, *impr_phase;
+  const int32_t *impr_div;
+  int32_t nshake;
+  const int32_t *shake_n;      /* [nshake] atoms in group (2..4) = iuhshk+1 */
+  const int32_t *shake_atoms;  /* [nshake][4] iuashk */
+  const double *shake_dist;    /* [nshake][6] target distances d0 in md_run pair order
+                                  (1,2),(2,3),(3,1),(4,1),(3,4),(2,4) -- setshk.f90 redshk */
+  const jp_ge *ge;             /* McMD weight for METHOD= GE; NULL otherwise */
+} jp_system;
+
+/* Run parameters shared by all replicas of a context (md.inp EXE> MD keywords). */
+typedef struct jp_params {
+  int32_t precision;     /* JP_PREC_FP64 or JP_PREC_MIXED */
+  int32_t method;        /* METHOD= (JP_METHOD_MICR / CANO / GE) */
+  double dt;             /* TIMEST (fs) */
+  double cutoff;         /* CUTLEN (Angstrom), ZD cut-off */
+  double dielectric;     /* DIEVAL */
+  int32_t update;        /* UPDATE: pair-list rebuild interval (steps) */
+  double temp;           /* SETTEM (K) */
+  double temp_start;     /* STARTT (K) */
+  int32_t heat_loop;     /* HEATLO (steps); 0 = no heating ramp */
+  int32_t tempco;        /* TEMPCO: 1 = one temperature, 2 = per sub-system (itmeth) */
+  int32_t shake_method;  /* SHAKEM (JP_SHAKE_*) */
+  double shake_tol;      /* COVSHK */
+  int32_t shake_maxit;   /* LIMSHK */
+  int32_t icslop;        /* SHAKE <-> thermostat iterations (md_run default 3) */
+  double fcstol;         /* their tolerance (md_run default 1e-3) */
+  double psetmp;         /* PSETMP pseudo temperature; 0 = off */
+  int32_t device;        /* CUDA device ordinal */
+} jp_params;
+
+typedef struct jp_ctx jp_ctx;
+
+/* Fill *prm with md_run's defaults (inpmd.f90:120-160, main.f90:134-174). */
+void jp_default_params(jp_params *prm);
+
+/* Set-up after incel (md.f90:82): copies topology, derives the ZD excess list, dself and
+ * 1-4 pairs (incel.f90:627-689, :755-787, :1084-1087), drops SHAKE-constrained bonds and
+ * angles (setshk.f90 reabnd/reaang), builds the first pair list (celprp).
+ * `sys` points at nrep replica systems; all replicas share `prm`. */
+int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx **out);
+
+/* celprp(iprint,ilflag,ier) (md.f90:657, :888, :1059, :1138): rebuild cells and the pair
+ * list from the current device coordinates.  replica = -1 rebuilds all. */
+int jp_rebuild_cells(jp_ctx *ctx, int32_t replica);
+
+/* dnergy(eneval, enevcc) (verlet.f90:63, verlethe.f90:103, staver.f90:41).
+ * If cord != NULL it replaces the replica's coordinates first (the pair list is NOT
+ * rebuilt; call jp_rebuild_cells for a list at these coordinates).  Outputs are nullable:
+ * eneval[JP_MAXENE], grad[natom][3] (dE/dx, kcal/mol/Angstrom). */
+int jp_energy_grad(jp_ctx *ctx, int32_t replica, const double *cord, double *eneval,
+                   double *grad);
+
+/* nsteps iterations of runmd's loop body (md.f90:519-694): one verlet (MICR) or verlethe
+ * (CANO/GE) step including SHAKE, then the pair-list rebuild every UPDATE steps.
+ * ene_out (nullable) receives [nsteps][nrep][JP_MAXENE] potential energies at time t of
+ * each step (the NAMETO .ene values, md.f90:578-601); temp_out (nullable) [nsteps][nrep]
+ * the instantaneous temperature of v(t+dt/2). */
+int jp_step(jp_ctx *ctx, int32_t nsteps, double *ene_out, double *temp_out);
+
+/* shake_PB(r1, r2, iprint, ier) (verlet.f90:196): constrain r1 against reference r2,
+ * both [natom][3] host arrays of one replica.  Test hook. */
+int jp_shake(jp_ctx *ctx, int32_t replica, double *r1, const double *r2);
+
+/* Coordinates/velocities of one replica for restart and monitor output
+ * (outrst.f90:56-61, monmd.f90).  Any pointer may be NULL. */
+int jp_get_state(jp_ctx *ctx, int32_t replica, double *cord, double *vel);
+int jp_set_state(jp_ctx *ctx, int32_t replica, const double *cord, const double *vel);
+
+/* Number of pair interactions within the cut-off evaluated at the last force call
+ * (counts r <= rc among listed pairs, one per unordered pair), per replica. */
+int jp_pair_count(jp_ctx *ctx, int32_t replica, int64_t *count);
+
+/* Timing.  jp_set_timing(ctx, 1) makes jp_step launch its kernels directly (no CUDA graph)
+ * with CUDA events around each phase; 0 (default) replays one captured graph per step.
+ * jp_last_timing returns the device time of the last jp_step call (events on the
+ * context's stream around all of its kernels) and, in timing mode, the summed time of each
+ * phase: [0] pair kernel, [1] bonded, [2] integrate+SHAKE, [3] list rebuild, plus
+ * launches[0..3] = number of launches timed per phase (nullable arrays). */
+int jp_set_timing(jp_ctx *ctx, int enable);
+int jp_last_timing(jp_ctx *ctx, double *total_ms, double *phase_ms4, int32_t *launches4);
+
+/* Kernel launches per jp_step step (excluding list rebuilds) and per list rebuild. */
+int jp_launch_counts(jp_ctx *ctx, int32_t *per_step, int32_t *per_rebuild);
+
+/* Pair-list statistics of the current list, all replicas: tiles (32x32 atom blocks), pair
+ * slots set in their masks (pairs within rc+1.5 at the last rebuild, exclusions removed),
+ * and the number of atoms padded into blocks. */
+int jp_list_stats(jp_ctx *ctx, int64_t *ntiles, int64_t *npairs_listed, int64_t *nslots);
+
+/* FP32 FMA throughput of `device` in TFLOP/s (best of 5 timed FMA-chain launches): the
+ * peak the pair kernel's FP32 arithmetic is measured against. */
+int jp_calibrate_fp32(int32_t device, double *tflops);
+
+const char *jp_strerror(int code);
+void jp_destroy(jp_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JPGPU_H */

@@ -1,0 +1,159 @@
+"""ctypes mirror of include/jpgpu.h (the C ABI that replaces md_run's call sites).
+
+`make_system` turns a topology dict (numpy arrays, see `systems.py`) into a `JpSystem`
+struct whose pointers stay valid as long as the returned keep-alive list lives.
+"""
+import ctypes as C
+
+import numpy as np
+
+JP_MAXENE = 15
+JP_PREC_FP64, JP_PREC_MIXED = 0, 1
+JP_METHOD_CONS, JP_METHOD_MICR, JP_METHOD_CANO, JP_METHOD_GE = 1, 2, 3, 4
+JP_SHAKE_NONE, JP_SHAKE_HBON, JP_SHAKE_ALLB = 0, 1, 2
+# return codes (md_run ier convention: >0 warning, <0 fatal)
+JP_OK = 0
+JP_W_SHAKE_NOT_CONVERGED = 1
+JP_E_SHAKE_SINGULAR = -2
+JP_E_SHAKE_ABORT = -9999
+JP_E_INVALID = -100
+JP_E_LIST_OVERFLOW = -151
+JP_E_NONFINITE = -200
+JP_E_CUDA = -300
+JP_E_NO_DEVICE = -301
+
+# energy slot names (md_run main.f90:157-159 cyenam order)
+ENERGY_NAMES = ["TOTAL", "BOND", "ANGLE", "TORSION", "IMPROPER", "VDW14", "ELEC14",
+                "VDW15", "ELEC15", "HBOND", "VDW15_NC", "ELEC15_NC", "HBOND_NC",
+                "POSRES", "DISRES"]
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+class JpGe(C.Structure):
+    _fields_ = [("nwindow", C.c_int32), ("ndeg", C.c_int32),
+                ("coef", _dp), ("low", _dp), ("high", _dp),
+                ("alphalw", C.c_double), ("alphaup", C.c_double),
+                ("celw", C.c_double), ("ceup", C.c_double),
+                ("tempce", C.c_double), ("lower", C.c_double), ("upper", C.c_double)]
+
+
+class JpSystem(C.Structure):
+    _fields_ = [
+        ("natom", C.c_int32), ("index_base", C.c_int32), ("box", C.c_double * 3),
+        ("cord", _dp), ("vel", _dp), ("mass", _dp), ("charge", _dp),
+        ("atype", _ip), ("molecule", _ip),
+        ("ntype", C.c_int32), ("c6", _dp), ("c12", _dp), ("s14_vdw", _dp), ("s14_ele", _dp),
+        ("excl_ptr", _ip), ("excl_idx", _ip),
+        ("nbond", C.c_int32), ("bond", _ip), ("bond_k", _dp), ("bond_r0", _dp),
+        ("nangle", C.c_int32), ("angle", _ip), ("angle_k", _dp), ("angle_theta0", _dp),
+        ("ntors", C.c_int32), ("tors", _ip), ("tors_k", _dp), ("tors_nrot", _dp),
+        ("tors_phase", _dp), ("tors_div", _ip), ("tors_nbf", _ip),
+        ("nimpr", C.c_int32), ("impr", _ip), ("impr_k", _dp), ("impr_nrot", _dp),
+        ("impr_phase", _dp), ("impr_div", _ip),
+        ("nshake", C.c_int32), ("shake_n", _ip), ("shake_atoms", _ip), ("shake_dist", _dp),
+        ("ge", C.POINTER(JpGe)),
+    ]
+
+
+class JpParams(C.Structure):
+    _fields_ = [
+        ("precision", C.c_int32), ("method", C.c_int32), ("dt", C.c_double),
+        ("cutoff", C.c_double), ("dielectric", C.c_double), ("update", C.c_int32),
+        ("temp", C.c_double), ("temp_start", C.c_double), ("heat_loop", C.c_int32),
+        ("tempco", C.c_int32), ("shake_method", C.c_int32), ("shake_tol", C.c_double),
+        ("shake_maxit", C.c_int32), ("icslop", C.c_int32), ("fcstol", C.c_double),
+        ("psetmp", C.c_double), ("device", C.c_int32),
+    ]
+
+
+def default_params(**kw):
+    """md_run defaults (inpmd.f90:120-160, main.f90:134-174) plus keyword overrides."""
+    p = JpParams(precision=JP_PREC_MIXED, method=JP_METHOD_CANO, dt=2.0, cutoff=12.0,
+                 dielectric=1.0, update=10, temp=300.0, temp_start=300.0, heat_loop=0,
+                 tempco=2, shake_method=JP_SHAKE_HBON, shake_tol=1e-6, shake_maxit=1000,
+                 icslop=3, fcstol=1e-3, psetmp=0.0, device=0)
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a, ctype, keep):
+    if a is None:
+        return None
+    dt = np.float64 if ctype is C.c_double else np.int32
+    a = np.ascontiguousarray(a, dtype=dt)
+    keep.append(a)
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def make_system(top, keep, cord=None, vel=None):
+    """Build a JpSystem from a topology dict; arrays are appended to `keep`."""
+    s = JpSystem()
+    s.natom = int(top["natom"])
+    s.index_base = 0
+    for k in range(3):
+        s.box[k] = float(top["box"][k])
+    s.cord = _ptr(top["cord"] if cord is None else cord, C.c_double, keep)
+    v = top.get("vel") if vel is None else vel
+    s.vel = _ptr(v, C.c_double, keep)
+    s.mass = _ptr(top["mass"], C.c_double, keep)
+    s.charge = _ptr(top["charge"], C.c_double, keep)
+    s.atype = _ptr(top["atype"], C.c_int32, keep)
+    s.molecule = _ptr(top.get("molecule"), C.c_int32, keep)
+    s.ntype = int(top["ntype"])
+    s.c6 = _ptr(top["c6"], C.c_double, keep)
+    s.c12 = _ptr(top["c12"], C.c_double, keep)
+    s.s14_vdw = _ptr(top["s14_vdw"], C.c_double, keep)
+    s.s14_ele = _ptr(top["s14_ele"], C.c_double, keep)
+    s.excl_ptr = _ptr(top["excl_ptr"], C.c_int32, keep)
+    s.excl_idx = _ptr(top["excl_idx"] if len(top["excl_idx"]) else np.zeros(1, np.int32),
+                      C.c_int32, keep)
+
+    def seg(name, cols, fields):
+        arr = top[name]
+        n = len(arr) // cols if np.ndim(arr) == 1 else len(arr)
+        setattr(s, "n" + name, n)
+        setattr(s, name, _ptr(np.asarray(arr).reshape(-1) if n else np.zeros(cols, np.int32),
+                              C.c_int32, keep))
+        for f, ct in fields:
+            val = top[f] if n else np.zeros(1)
+            setattr(s, f, _ptr(val, ct, keep))
+
+    seg("bond", 2, [("bond_k", C.c_double), ("bond_r0", C.c_double)])
+    seg("angle", 3, [("angle_k", C.c_double), ("angle_theta0", C.c_double)])
+    seg("tors", 4, [("tors_k", C.c_double), ("tors_nrot", C.c_double),
+                    ("tors_phase", C.c_double), ("tors_div", C.c_int32),
+                    ("tors_nbf", C.c_int32)])
+    seg("impr", 4, [("impr_k", C.c_double), ("impr_nrot", C.c_double),
+                    ("impr_phase", C.c_double), ("impr_div", C.c_int32)])
+    sh_n = np.asarray(top["shake_n"], np.int32)
+    s.nshake = len(sh_n)
+    s.shake_n = _ptr(sh_n if len(sh_n) else np.zeros(1, np.int32), C.c_int32, keep)
+    s.shake_atoms = _ptr(np.asarray(top["shake_atoms"]).reshape(-1) if len(sh_n)
+                         else np.zeros(4, np.int32), C.c_int32, keep)
+    s.shake_dist = _ptr(np.asarray(top["shake_dist"]).reshape(-1) if len(sh_n)
+                        else np.zeros(6), C.c_double, keep)
+    ge = top.get("ge")
+    if ge is not None:
+        g = JpGe(nwindow=int(ge["nwindow"]), ndeg=int(ge["ndeg"]),
+                 alphalw=float(ge["alphalw"]), alphaup=float(ge["alphaup"]),
+                 celw=float(ge["celw"]), ceup=float(ge["ceup"]), tempce=float(ge["tempce"]),
+                 lower=float(ge.get("lower", 0.0)), upper=float(ge.get("upper", 0.0)))
+        g.coef = _ptr(np.asarray(ge["coef"]).reshape(-1), C.c_double, keep)
+        g.low = _ptr(ge["low"], C.c_double, keep)
+        g.high = _ptr(ge["high"], C.c_double, keep)
+        keep.append(g)
+        s.ge = C.pointer(g)
+    return s
+
+
+def make_systems(tops, keep):
+    """Array of JpSystem for several replicas."""
+    arr = (JpSystem * len(tops))()
+    for i, t in enumerate(tops):
+        arr[i] = make_system(t, keep)
+    return arr

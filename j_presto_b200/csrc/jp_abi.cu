@@ -1,0 +1,905 @@
+// jp_abi.cu -- host side of the engine: the C ABI of include/jpgpu.h.
+//
+// jp_create derives, in C++ on the host, what md_run's set-up derives in Fortran:
+//   * chgmod = q*sqrt(332.06378/eps)                      inpcls.f90:215-227
+//   * SHAKE groups ordered 2/3/4 atoms, squared lengths     setshk.f90 redshk/modshk
+//   * bonds/angles whose pair is a SHAKE constraint dropped setshk.f90 reabnd/reaang
+//   * 1-4 pairs of torsions with nbf=1, scales min(s_i,s_j) incel.f90:972-987,
+//                                                           inptpl.f90:453-462, incel.f90:1084
+//   * ZD constants, dself, excess list                       incel.f90:29-39, :627-689
+//   * degrees of freedom (whole / per sub-system)            md.f90:116-183
+// and lays out device memory (see jp_common.cuh).  jp_step replays one CUDA graph per
+// MD step (forces + integration) and one per list rebuild.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <new>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "jp_kernels.h"
+
+using namespace jp;
+
+namespace {
+
+struct Timing {
+  bool enabled = false;
+  double total_ms = 0.0;
+  double phase_ms[4] = {0, 0, 0, 0};
+  int launches[4] = {0, 0, 0, 0};
+};
+
+}  // namespace
+
+struct jp_ctx {
+  int nrep = 0;
+  jp_params prm{};
+  int device = 0;
+  int natom = 0, nblk = 0, nslot = 0, nunit = 0, nterm = 0, nsub = 0, nkeys = 0, nkin = 8;
+  int tile_cap_total = 0, nchunk = 0;
+  std::vector<Rep> reps;
+  std::vector<int> rep_natom;
+  DevPtrs P{};
+  ZdConst zc{};
+  IntConst ic{};
+  double qscale = 1.0;
+  bool fp64 = false;
+  bool minimg = true;
+  int pair_warps = 0;
+  int hist_cap = 1024;
+  long long idloop = 0;
+  cudaStream_t st = nullptr;
+  cudaGraphExec_t g_step = nullptr, g_rebuild = nullptr;
+  int *scan_scratch = nullptr;
+  std::vector<void *> allocs;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+  std::vector<cudaEvent_t> tev;
+  Timing tm;
+  int launches_step = 0, launches_rebuild = 0;
+};
+
+namespace {
+
+const char *g_last_err = "";
+
+#define CK(call)                                                      \
+  do {                                                                \
+    cudaError_t e_ = (call);                                          \
+    if (e_ != cudaSuccess) {                                          \
+      g_last_err = cudaGetErrorString(e_);                            \
+      std::fprintf(stderr, "jpgpu: %s at %s:%d\n", g_last_err, __FILE__, __LINE__); \
+      return JP_E_CUDA;                                               \
+    }                                                                 \
+  } while (0)
+
+template <class T>
+int dalloc(jp_ctx *c, T **p, size_t n) {
+  if (n == 0) n = 1;
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+  if (e != cudaSuccess) {
+    g_last_err = cudaGetErrorString(e);
+    return JP_E_CUDA;
+  }
+  cudaMemset(q, 0, n * sizeof(T));
+  c->allocs.push_back(q);
+  *p = static_cast<T *>(q);
+  return 0;
+}
+
+template <class T>
+int dput(jp_ctx *c, T **p, const std::vector<T> &h) {
+  int r = dalloc(c, p, h.size());
+  if (r) return r;
+  if (!h.empty()) {
+    cudaError_t e = cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { g_last_err = cudaGetErrorString(e); return JP_E_CUDA; }
+  }
+  return 0;
+}
+
+constexpr double kEekcal = 332.06378;
+
+int ceil_log2(int v) {
+  int b = 0;
+  while ((1 << b) < v) ++b;
+  return b;
+}
+
+// ---- rebuild: cells + tiles -------------------------------------------------------------
+void enqueue_rebuild(jp_ctx *c) {
+  DevPtrs &P = c->P;
+  cudaStream_t st = c->st;
+  const int nt = 256;
+  cudaMemsetAsync(P.hist, 0, sizeof(int) * c->nkeys, st);
+  cudaMemsetAsync(P.cursor, 0, sizeof(int) * c->nkeys, st);
+  k_cell_key<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
+  scan_exclusive(P.hist, P.hist_scan, c->nkeys, c->scan_scratch, nullptr, st);
+  k_scatter<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
+  k_sort_bins<<<(c->nkeys + nt - 1) / nt, nt, 0, st>>>(P, c->nkeys);
+  k_clear_slots<<<(c->nslot + nt - 1) / nt, nt, 0, st>>>(P, c->nslot, c->zc.nt1 - 1);
+  k_fill_slots<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
+  k_block_setup<<<(c->nblk * 32 + nt - 1) / nt, nt, 0, st>>>(P, c->nblk, c->qscale);
+  if (c->fp64) k_fill_pos_d<<<(c->nslot + nt - 1) / nt, nt, 0, st>>>(P, c->nslot, c->qscale);
+  const double rlim = c->prm.cutoff + 1.5;
+  const int nwb = (c->nchunk * 32 + 127) / 128;
+  k_tile_scan_chunks<<<nwb, 128, 0, st>>>(P, c->nchunk, rlim * rlim, (float)rlim);
+  scan_exclusive(P.chunk_cnt, P.chunk_off, c->nchunk + 1, c->scan_scratch, P.ntiles, st);
+  k_tile_emit<<<nwb, 128, 0, st>>>(P, c->nchunk);
+  c->launches_rebuild = 14 + (c->fp64 ? 1 : 0);
+}
+
+// ---- one MD step ------------------------------------------------------------------------
+void enqueue_zero(jp_ctx *c, bool count) {
+  DevPtrs &P = c->P;
+  cudaStream_t st = c->st;
+  if (c->fp64) cudaMemsetAsync(P.grd, 0, sizeof(double) * 3 * c->natom, st);
+  else cudaMemsetAsync(P.frc, 0, sizeof(long long) * 3 * c->natom, st);
+  cudaMemsetAsync(P.ene_fix, 0, sizeof(long long) * 16 * c->nrep, st);
+  if (count) cudaMemsetAsync(P.pair_cnt, 0, sizeof(long long) * c->nrep, st);
+}
+
+void enqueue_pair(jp_ctx *c, bool count) {
+  if (c->fp64) launch_pair_fp64(c->P, c->zc, c->pair_warps, count, c->st);
+  else launch_pair_mixed(c->P, c->zc, c->pair_warps, c->minimg, count, c->st);
+}
+
+void enqueue_forces(jp_ctx *c, bool count) {
+  enqueue_zero(c, count);
+  enqueue_pair(c, count);
+}
+
+void enqueue_bonded(jp_ctx *c) {
+  launch_bonded(c->P, c->nterm, c->fp64, c->zc.bcoeff, c->zc.fcoeff, c->st);
+}
+
+void enqueue_integrate(jp_ctx *c) {
+  DevPtrs &P = c->P;
+  cudaMemsetAsync(P.kin_fix, 0, sizeof(long long) * c->nkin * c->nsub, c->st);
+  launch_prepare(P, c->ic, c->nrep, c->st);
+  if (c->prm.method == JP_METHOD_MICR) launch_micr(P, c->ic, c->nunit, c->fp64, c->st);
+  else launch_cano(P, c->ic, c->nunit, c->fp64, c->st);
+  launch_finish(P, c->ic, c->nrep, c->st);
+}
+
+int launches_per_step(const jp_ctx *c) {
+  int n = 1;                       // pair
+  n += c->nterm > 0 ? 1 : 0;      // bonded
+  n += 2;                          // prepare + finish
+  if (c->prm.method == JP_METHOD_MICR) n += 1;
+  else {
+    const bool shk = c->prm.shake_method != JP_SHAKE_NONE;
+    n += 1 + (shk ? 1 + c->prm.icslop + 2 * (c->prm.icslop - 1) : 0);
+  }
+  return n;
+}
+
+int capture(jp_ctx *c, cudaGraphExec_t *out, bool rebuild) {
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+  if (rebuild) {
+    enqueue_rebuild(c);
+  } else {
+    enqueue_forces(c, false);
+    enqueue_bonded(c);
+    enqueue_integrate(c);
+  }
+  CK(cudaStreamEndCapture(c->st, &g));
+  CK(cudaGraphInstantiate(out, g, 0));
+  CK(cudaGraphDestroy(g));
+  return 0;
+}
+
+int check_status(jp_ctx *c) {
+  unsigned s = 0;
+  CK(cudaMemcpy(&s, c->P.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (s == 0) return JP_OK;
+  CK(cudaMemset(c->P.status, 0, sizeof(unsigned)));
+  if (s & ERR_LIST_OVERFLOW) return JP_E_LIST_OVERFLOW;
+  if (s & ERR_NONFINITE) return JP_E_NONFINITE;
+  if (s & ERR_FIX_OVERFLOW) return JP_E_FIXED_OVERFLOW;
+  if (s & ERR_SHAKE_SINGULAR) return JP_E_SHAKE_SINGULAR;
+  if (s & ERR_SHAKE_NOCONV) return JP_W_SHAKE_NOT_CONVERGED;
+  return JP_E_INVALID;
+}
+
+int validate(const jp_system *sys, int nrep, const jp_params *prm) {
+  if (!sys || nrep <= 0 || !prm) return JP_E_INVALID;
+  if (prm->cutoff <= 0.0 || prm->dt <= 0.0 || prm->dielectric <= 0.0) return JP_E_INVALID;
+  if (prm->method != JP_METHOD_MICR && prm->method != JP_METHOD_CANO && prm->method != JP_METHOD_GE)
+    return JP_E_INVALID;
+  if (prm->precision != JP_PREC_FP64 && prm->precision != JP_PREC_MIXED) return JP_E_INVALID;
+  const double rlim = prm->cutoff + 1.5;
+  for (int r = 0; r < nrep; ++r) {
+    const jp_system &s = sys[r];
+    if (s.natom <= 0 || !s.cord || !s.mass || !s.charge || !s.atype || !s.c6 || !s.c12 || !s.excl_ptr)
+      return JP_E_INVALID;
+    for (int k = 0; k < 3; ++k)
+      if (!(s.box[k] > 2.0 * rlim)) return JP_E_INVALID;   // unique minimum image
+    if (s.ntype != sys[0].ntype) return JP_E_INVALID;
+    const size_t nt2 = (size_t)s.ntype * s.ntype;
+    for (size_t q = 0; q < nt2; ++q)
+      if (s.c6[q] != sys[0].c6[q] || s.c12[q] != sys[0].c12[q]) return JP_E_INVALID;
+    for (int i = 0; i < s.ntors; ++i) {
+      int n = (int)std::lround(s.tors_nrot[i]);
+      if (n < 1 || n > 6 || s.tors_div[i] == 0) return JP_E_INVALID;
+    }
+    for (int i = 0; i < s.nimpr; ++i) {
+      int n = (int)std::lround(s.impr_nrot[i]);
+      if (n < 1 || n > 6 || s.impr_div[i] == 0) return JP_E_INVALID;
+    }
+    for (int g = 0; g < s.nshake; ++g)
+      if (s.shake_n[g] < 2 || s.shake_n[g] > 4) return JP_E_INVALID;
+    if (prm->method == JP_METHOD_GE && !s.ge) return JP_E_INVALID;
+    // every index that reaches a kernel must be in range
+    const int b = s.index_base, n = s.natom;
+    auto okatom = [&](int a) { return a - b >= 0 && a - b < n; };
+    for (int i = 0; i < n; ++i) {
+      if (s.atype[i] - b < 0 || s.atype[i] - b >= s.ntype) return JP_E_INVALID;
+      if (s.molecule && s.molecule[i] - b < 0) return JP_E_INVALID;
+      if (!(s.mass[i] > 0.0)) return JP_E_INVALID;
+      if (s.excl_ptr[i + 1] < s.excl_ptr[i]) return JP_E_INVALID;
+    }
+    if (s.excl_ptr[0] != 0) return JP_E_INVALID;
+    for (int p = 0; p < s.excl_ptr[n]; ++p)
+      if (!okatom(s.excl_idx[p])) return JP_E_INVALID;
+    for (int i = 0; i < 2 * s.nbond; ++i) if (!okatom(s.bond[i])) return JP_E_INVALID;
+    for (int i = 0; i < 3 * s.nangle; ++i) if (!okatom(s.angle[i])) return JP_E_INVALID;
+    for (int i = 0; i < 4 * s.ntors; ++i) if (!okatom(s.tors[i])) return JP_E_INVALID;
+    for (int i = 0; i < 4 * s.nimpr; ++i) if (!okatom(s.impr[i])) return JP_E_INVALID;
+    for (int g = 0; g < s.nshake; ++g)
+      for (int k = 0; k < s.shake_n[g]; ++k)
+        if (!okatom(s.shake_atoms[4 * g + k])) return JP_E_INVALID;
+    if (s.ge && (s.ge->nwindow < 1 || s.ge->ndeg < 0 || !s.ge->coef || !s.ge->low || !s.ge->high))
+      return JP_E_INVALID;
+  }
+  return 0;
+}
+
+}  // namespace
+
+// =======================================================================================
+extern "C" {
+
+void jp_default_params(jp_params *p) {
+  std::memset(p, 0, sizeof(*p));
+  p->precision = JP_PREC_MIXED;
+  p->method = JP_METHOD_CANO;      // inpmd.f90:126 intele(9)=3
+  p->dt = 2.0;                     // inpmd.f90:127
+  p->cutoff = 12.0;                // main.f90:155 fycutl
+  p->dielectric = 1.0;             // main.f90:155 fydiel
+  p->update = 10;                  // inpmd.f90:126 intele(4)
+  p->temp = 300.0;
+  p->temp_start = 300.0;
+  p->heat_loop = 0;
+  p->tempco = 2;                   // inpmd.f90:148 intele(63)=2
+  p->shake_method = JP_SHAKE_HBON;
+  p->shake_tol = 1.0e-6;           // main.f90:167 fustol
+  p->shake_maxit = 1000;           // main.f90:166 iuslop
+  p->icslop = 3;                   // main.f90:166
+  p->fcstol = 1.0e-3;              // main.f90:167
+  p->psetmp = 0.0;
+  p->device = 0;
+}
+
+const char *jp_strerror(int code) {
+  switch (code) {
+    case JP_OK: return "ok";
+    case JP_W_SHAKE_NOT_CONVERGED: return "SHAKE not converged (warning)";
+    case JP_E_SHAKE_SINGULAR: return "SHAKE gradient matrix singular";
+    case JP_E_SHAKE_ABORT: return "SHAKE failed after time-step halving";
+    case JP_E_INVALID: return "invalid argument or topology";
+    case JP_E_CELL_OVERFLOW: return "cell table overflow";
+    case JP_E_LIST_OVERFLOW: return "pair-tile list overflow";
+    case JP_E_NONFINITE: return "non-finite coordinate or force";
+    case JP_E_FIXED_OVERFLOW: return "fixed-point force overflow";
+    case JP_E_CUDA: return g_last_err;
+    case JP_E_NO_DEVICE: return "no CUDA device";
+    case JP_E_TIMEOUT: return "device wait timed out";
+    default: return "unknown error";
+  }
+}
+
+int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx **out) {
+  if (!out) return JP_E_INVALID;
+  *out = nullptr;
+  int v = validate(sys, nrep, prm);
+  if (v) return v;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return JP_E_NO_DEVICE;
+  if (prm->device < 0 || prm->device >= ndev) return JP_E_INVALID;
+  CK(cudaSetDevice(prm->device));
+
+  jp_ctx *c = new (std::nothrow) jp_ctx();
+  if (!c) return JP_E_INVALID;
+  c->nrep = nrep;
+  c->prm = *prm;
+  c->device = prm->device;
+  c->fp64 = prm->precision == JP_PREC_FP64;
+  const double ccoef = kEekcal / prm->dielectric;
+  c->qscale = std::sqrt(ccoef);
+  const double rc = prm->cutoff;
+  const double rlim = rc + 1.5;
+
+  // ---- host-side topology derivation -----------------------------------------------
+  std::vector<double> hx, hv, hmass, himass, hchg;
+  std::vector<int> htyp, hrep, hexp{0}, hexi;
+  std::vector<Unit> units;
+  std::vector<Term> terms_by_kind[6];
+  std::vector<double> hnfr, hge;
+  std::vector<Rep> reps(nrep);
+  const int ntype = sys[0].ntype;
+  const int nt1 = ntype + 1;
+  std::vector<float2> ljf(nt1 * nt1, make_float2(0.f, 0.f));
+  std::vector<double2> ljd(nt1 * nt1, make_double2(0.0, 0.0));
+  for (int i = 0; i < ntype; ++i)
+    for (int j = 0; j < ntype; ++j) {
+      ljd[i * nt1 + j] = make_double2(sys[0].c6[i * ntype + j], sys[0].c12[i * ntype + j]);
+      ljf[i * nt1 + j] = make_float2((float)sys[0].c6[i * ntype + j], (float)sys[0].c12[i * ntype + j]);
+    }
+  int atom0 = 0, blk0 = 0, key0 = 0, sub0 = 0;
+  for (int r = 0; r < nrep; ++r) {
+    const jp_system &s = sys[r];
+    const int b = s.index_base;
+    const int n = s.natom;
+    Rep &R = reps[r];
+    std::memset(&R, 0, sizeof(Rep));
+    R.atom0 = atom0;
+    R.natom = n;
+    R.blk0 = blk0;
+    R.nblk = (n + kTile - 1) / kTile;
+    for (int k = 0; k < 3; ++k) {
+      R.box[k] = s.box[k];
+      R.invbox[k] = 1.0 / s.box[k];
+      R.grid[k] = std::max(1, std::min(1024, (int)std::floor(s.box[k] / 2.4)));
+      R.cell[k] = s.box[k] / R.grid[k];
+    }
+    R.keybits = ceil_log2(std::max(R.grid[0], std::max(R.grid[1], R.grid[2])));
+    R.key0 = key0;
+    key0 += 1 << (3 * R.keybits);
+    for (int i = 0; i < n; ++i) {
+      for (int k = 0; k < 3; ++k) {
+        hx.push_back(s.cord[3 * i + k]);
+        hv.push_back(s.vel ? s.vel[3 * i + k] : 0.0);
+      }
+      hmass.push_back(s.mass[i]);
+      himass.push_back(1.0 / s.mass[i]);
+      hchg.push_back(s.charge[i]);
+      htyp.push_back(s.atype[i] - b);
+      hrep.push_back(r);
+    }
+    // exclusions
+    for (int i = 0; i < n; ++i) {
+      std::vector<int> L;
+      for (int p = s.excl_ptr[i]; p < s.excl_ptr[i + 1]; ++p) L.push_back(atom0 + s.excl_idx[p] - b);
+      std::sort(L.begin(), L.end());
+      for (int q : L) hexi.push_back(q);
+      hexp.push_back((int)hexi.size());
+    }
+    // sub-systems
+    // sub-systems: molecule-entry ids renumbered densely, empty ids removed (md.f90:133-151)
+    std::vector<int> mol(n, 0);
+    int nmol = 1;
+    if (s.molecule && prm->tempco == 2) {
+      std::vector<int> u;
+      for (int i = 0; i < n; ++i) u.push_back(s.molecule[i] - b);
+      std::sort(u.begin(), u.end());
+      u.erase(std::unique(u.begin(), u.end()), u.end());
+      for (int i = 0; i < n; ++i)
+        mol[i] = (int)(std::lower_bound(u.begin(), u.end(), s.molecule[i] - b) - u.begin());
+      nmol = (int)u.size();
+    }
+    R.sub0 = sub0;
+    R.nsub = nmol;
+    std::vector<double> nfr(nmol, 0.0);
+    for (int i = 0; i < n; ++i) nfr[mol[i]] += 3.0;
+    // SHAKE groups -> units
+    const bool shk = prm->shake_method != JP_SHAKE_NONE && s.nshake > 0;
+    std::set<std::pair<int, int>> cpairs;
+    std::vector<char> in_group(n, 0);
+    std::vector<Unit> ru;
+    static const int pl[6][2] = {{0, 1}, {1, 2}, {2, 0}, {3, 0}, {2, 3}, {1, 3}};
+    if (shk) {
+      for (int ng = 2; ng <= 4; ++ng)   // md_run order: 2-, 3-, then 4-atom groups
+        for (int g = 0; g < s.nshake; ++g) {
+          if (s.shake_n[g] != ng) continue;
+          Unit u;
+          std::memset(&u, 0, sizeof(u));
+          u.n = ng;
+          u.rep = r;
+          for (int k = 0; k < 4; ++k) u.a[k] = k < ng ? atom0 + s.shake_atoms[4 * g + k] - b : -1;
+          const int nc = ng * (ng - 1) / 2;
+          for (int q = 0; q < 6; ++q) {
+            const double d = q < nc ? s.shake_dist[6 * g + q] : 0.0;
+            u.d2[q] = d * d;
+          }
+          for (int q = 0; q < nc; ++q) {
+            int a1 = u.a[pl[q][0]] - atom0, a2 = u.a[pl[q][1]] - atom0;
+            cpairs.insert({std::min(a1, a2), std::max(a1, a2)});
+          }
+          for (int k = 0; k < ng; ++k) {
+            if (in_group[u.a[k] - atom0]) { delete c; return JP_E_INVALID; }
+            in_group[u.a[k] - atom0] = 1;
+          }
+          u.sub = sub0 + mol[u.a[0] - atom0];
+          nfr[mol[u.a[0] - atom0]] -= (double)nc;
+          ru.push_back(u);
+        }
+    }
+    for (int i = 0; i < n; ++i)
+      if (!in_group[i]) {
+        Unit u;
+        std::memset(&u, 0, sizeof(u));
+        u.n = 1;
+        u.rep = r;
+        u.a[0] = atom0 + i;
+        u.a[1] = u.a[2] = u.a[3] = -1;
+        u.sub = sub0 + mol[i];
+        ru.push_back(u);
+      }
+    std::stable_sort(ru.begin(), ru.end(), [](const Unit &x, const Unit &y) { return x.sub < y.sub; });
+    R.unit0 = (int)units.size();
+    R.nunit = (int)ru.size();
+    units.insert(units.end(), ru.begin(), ru.end());
+    for (double f : nfr) hnfr.push_back(f);
+    sub0 += nmol;
+    auto constrained = [&](int a1, int a2) {
+      return shk && cpairs.count({std::min(a1, a2), std::max(a1, a2)}) > 0;
+    };
+    // bonded terms
+    std::vector<double> dwork(s.charge, s.charge + n);
+    auto mkterm = [&](int kind) {
+      Term t;
+      std::memset(&t, 0, sizeof(t));
+      t.kind = kind;
+      t.rep = r;
+      t.idiv = 1;
+      return t;
+    };
+    auto excess = [&](int a1, int a2) {   // incel.f90:635-654, :665-688
+      dwork[a1] += s.charge[a2];
+      dwork[a2] += s.charge[a1];
+      Term t = mkterm(T_EXCESS);
+      t.a[0] = atom0 + a1;
+      t.a[1] = atom0 + a2;
+      t.p0 = ccoef * s.charge[a1] * s.charge[a2];
+      terms_by_kind[T_EXCESS].push_back(t);
+    };
+    for (int i = 0; i < s.nbond; ++i) {
+      int a1 = s.bond[2 * i] - b, a2 = s.bond[2 * i + 1] - b;
+      excess(a1, a2);
+      if (constrained(a1, a2)) continue;
+      Term t = mkterm(T_BOND);
+      t.a[0] = atom0 + a1;
+      t.a[1] = atom0 + a2;
+      t.p0 = s.bond_k[i];
+      t.p1 = s.bond_r0[i];
+      terms_by_kind[T_BOND].push_back(t);
+    }
+    for (int i = 0; i < s.nangle; ++i) {
+      int a1 = s.angle[3 * i] - b, a2 = s.angle[3 * i + 1] - b, a3 = s.angle[3 * i + 2] - b;
+      excess(a1, a3);
+      if (constrained(a1, a3)) continue;
+      Term t = mkterm(T_ANGLE);
+      t.a[0] = atom0 + a1;
+      t.a[1] = atom0 + a2;
+      t.a[2] = atom0 + a3;
+      t.p0 = s.angle_k[i];
+      t.p1 = s.angle_theta0[i];
+      terms_by_kind[T_ANGLE].push_back(t);
+    }
+    for (int i = 0; i < s.ntors; ++i) {
+      Term t = mkterm(T_TORS);
+      for (int k = 0; k < 4; ++k) t.a[k] = atom0 + s.tors[4 * i + k] - b;
+      t.p0 = s.tors_k[i];
+      t.p1 = s.tors_nrot[i];
+      t.p2 = s.tors_phase[i];
+      t.idiv = s.tors_div[i];
+      terms_by_kind[T_TORS].push_back(t);
+      if (s.tors_nbf && s.tors_nbf[i] == 1) {
+        const int a1 = s.tors[4 * i] - b, a4 = s.tors[4 * i + 3] - b;
+        excess(a1, a4);
+        const int t1 = s.atype[a1] - b, t4 = s.atype[a4] - b;
+        Term p = mkterm(T_P14);
+        p.a[0] = atom0 + a1;
+        p.a[1] = atom0 + a4;
+        p.a[2] = t1 * nt1 + t4;   // LJ table index
+        p.p0 = std::min(s.s14_vdw[t1], s.s14_vdw[t4]);
+        p.p1 = std::min(s.s14_ele[t1], s.s14_ele[t4]) * ccoef * s.charge[a1] * s.charge[a4];
+        terms_by_kind[T_P14].push_back(p);
+      }
+    }
+    for (int i = 0; i < s.nimpr; ++i) {
+      Term t = mkterm(T_IMPR);
+      for (int k = 0; k < 4; ++k) t.a[k] = atom0 + s.impr[4 * i + k] - b;
+      t.p0 = s.impr_k[i];
+      t.p1 = s.impr_nrot[i];
+      t.p2 = s.impr_phase[i];
+      t.idiv = s.impr_div[i];
+      terms_by_kind[T_IMPR].push_back(t);
+    }
+    double ds = 0.0;
+    for (int i = 0; i < n; ++i) ds += s.charge[i] * dwork[i];
+    R.dself = -(1.5 / rc) * ds * 0.5 * ccoef;
+    // GE weight: per window [low, high, c0..cndeg]
+    if (s.ge) {
+      R.ge_off = (int)hge.size();
+      R.ge_nwin = s.ge->nwindow;
+      R.ge_ndeg = s.ge->ndeg;
+      R.ge_alphalw = s.ge->alphalw;
+      R.ge_alphaup = s.ge->alphaup;
+      R.ge_celw = s.ge->celw;
+      R.ge_ceup = s.ge->ceup;
+      R.ge_tempce = s.ge->tempce;
+      for (int w = 0; w < s.ge->nwindow; ++w) {
+        hge.push_back(s.ge->low[w]);
+        hge.push_back(s.ge->high[w]);
+        for (int k = 0; k <= s.ge->ndeg; ++k) hge.push_back(s.ge->coef[w * (s.ge->ndeg + 1) + k]);
+      }
+    }
+    atom0 += n;
+    blk0 += R.nblk;
+  }
+  c->reps = reps;
+  c->natom = atom0;
+  c->nblk = blk0;
+  c->nslot = blk0 * kTile;
+  c->nunit = (int)units.size();
+  c->nsub = sub0;
+  c->nkeys = key0;
+  c->nkin = std::max(8, 2 * prm->icslop + 2);
+  std::vector<Term> terms;
+  for (auto &v2 : terms_by_kind) terms.insert(terms.end(), v2.begin(), v2.end());
+  c->nterm = (int)terms.size();
+  std::vector<int> hblk_rep(c->nblk);
+  for (int r = 0; r < nrep; ++r)
+    for (int bb = 0; bb < reps[r].nblk; ++bb) hblk_rep[reps[r].blk0 + bb] = r;
+  // tile-list chunks: (i-block, j0) for j0 = i, i+32, ... inside the replica
+  std::vector<int> chunk_i, chunk_j0;
+  for (int bb = 0; bb < c->nblk; ++bb) {
+    const Rep &R = reps[hblk_rep[bb]];
+    for (int j0 = bb; j0 < R.blk0 + R.nblk; j0 += 32) {
+      chunk_i.push_back(bb);
+      chunk_j0.push_back(j0);
+    }
+  }
+  c->nchunk = (int)chunk_i.size();
+  c->tile_cap_total = c->nchunk * 32;   // every candidate could be a tile: no overflow
+
+  // ---- device allocation ---------------------------------------------------------------
+  DevPtrs &P = c->P;
+  int e = 0;
+  const int N = c->natom;
+  e |= dput(c, &P.x, hx);
+  e |= dput(c, &P.v, hv);
+  e |= dalloc(c, &P.x0, 3 * (size_t)N);
+  e |= dalloc(c, &P.vback, 3 * (size_t)N);
+  e |= dalloc(c, &P.xback, 3 * (size_t)N);
+  e |= dalloc(c, &P.forcec, 3 * (size_t)N);
+  e |= dput(c, &P.mass, hmass);
+  e |= dput(c, &P.imass, himass);
+  e |= dput(c, &P.chg, hchg);
+  e |= dput(c, &P.typ, htyp);
+  e |= dput(c, &P.rep_of, hrep);
+  e |= dalloc(c, &P.slot_of, (size_t)N);
+  e |= dalloc(c, &P.frc, 3 * (size_t)N);
+  e |= dalloc(c, &P.grd, 3 * (size_t)N);
+  e |= dput(c, &P.excl_ptr, hexp);
+  e |= dput(c, &P.excl_idx, hexi);
+  e |= dalloc(c, &P.pos_f, (size_t)c->nslot);
+  e |= dalloc(c, &P.pos_d, (size_t)c->nslot);
+  e |= dalloc(c, &P.off, 3 * (size_t)c->nslot);
+  e |= dalloc(c, &P.styp, (size_t)c->nslot);
+  e |= dalloc(c, &P.satom, (size_t)c->nslot);
+  e |= dput(c, &P.blk_rep, hblk_rep);
+  e |= dalloc(c, &P.blk_ctr, (size_t)c->nblk);
+  e |= dalloc(c, &P.blk_half, (size_t)c->nblk);
+  e |= dalloc(c, &P.blk_ref, 3 * (size_t)c->nblk);
+  e |= dput(c, &P.chunk_i, chunk_i);
+  e |= dput(c, &P.chunk_j0, chunk_j0);
+  e |= dalloc(c, &P.chunk_nz, (size_t)c->nchunk);
+  e |= dalloc(c, &P.chunk_cnt, (size_t)c->nchunk + 1);
+  e |= dalloc(c, &P.chunk_off, (size_t)c->nchunk + 1);
+  e |= dalloc(c, &P.tmp_masks, (size_t)c->tile_cap_total * 32);
+  e |= dalloc(c, &P.tiles, (size_t)c->tile_cap_total);
+  e |= dalloc(c, &P.tile_shift, (size_t)c->tile_cap_total);
+  e |= dalloc(c, &P.masks, (size_t)c->tile_cap_total * 32);
+  e |= dalloc(c, &P.ntiles, 1);
+  e |= dalloc(c, &P.key, (size_t)N);
+  e |= dalloc(c, &P.hist, (size_t)c->nkeys);
+  e |= dalloc(c, &P.hist_scan, (size_t)c->nkeys);
+  e |= dalloc(c, &P.cursor, (size_t)c->nkeys);
+  e |= dalloc(c, &P.sorted, (size_t)N);
+  e |= dput(c, &P.units, units);
+  e |= dput(c, &P.terms, terms);
+  e |= dput(c, &P.reps, reps);
+  e |= dput(c, &P.ge_coef, hge);
+  e |= dalloc(c, &P.ene_fix, 16 * (size_t)nrep);
+  e |= dalloc(c, &P.kin_fix, (size_t)c->nkin * c->nsub);
+  e |= dput(c, &P.nfr, hnfr);
+  e |= dalloc(c, &P.scale, (size_t)nrep);
+  e |= dalloc(c, &P.done, (size_t)nrep);
+  e |= dalloc(c, &P.status, 1);
+  e |= dalloc(c, &P.pair_cnt, (size_t)nrep);
+  e |= dalloc(c, &P.ene_hist, (size_t)c->hist_cap * nrep * JP_MAXENE);
+  e |= dalloc(c, &P.temp_hist, (size_t)c->hist_cap * nrep);
+  e |= dalloc(c, &P.step_ctr, 2);
+  e |= dput(c, &P.lj_f, ljf);
+  e |= dput(c, &P.lj_d, ljd);
+  e |= dalloc(c, &c->scan_scratch, (size_t)std::max(c->nkeys, c->nchunk + 1) / 1024 + 2);
+  if (e) { jp_destroy(c); return JP_E_CUDA; }
+  // the tile-row prefix must cover the sentinel entry; row_cnt[nblk] stays 0
+  // ---- constants ---------------------------------------------------------------------------
+  c->zc.rc2 = rc * rc;
+  c->zc.zcore = 1.5 / rc;
+  c->zc.fcoeff = 1.0 / (rc * rc * rc);
+  c->zc.bcoeff = 0.5 * c->zc.fcoeff;
+  c->zc.nt1 = nt1;
+  IntConst &ic = c->ic;
+  ic.dt = prm->dt;
+  ic.temp = prm->temp;
+  ic.temp_start = prm->temp_start;
+  ic.heat_loop = prm->heat_loop;
+  ic.tempco = prm->tempco;
+  ic.shake_method = prm->shake_method;
+  ic.shake_tol = prm->shake_tol;
+  ic.shake_maxit = prm->shake_maxit;
+  ic.icslop = prm->icslop;
+  ic.fcstol = prm->fcstol;
+  ic.psetmp = prm->psetmp;
+  ic.method = prm->method;
+  ic.nrep = nrep;
+  ic.nsub_total = c->nsub;
+  ic.natom = N;
+  ic.nkin = c->nkin;
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  c->pair_warps = std::max(1, nsm) * 8 * 6;   // 6 blocks of 8 warps per SM
+  CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&c->ev_a));
+  CK(cudaEventCreate(&c->ev_b));
+  enqueue_rebuild(c);
+  CK(cudaStreamSynchronize(c->st));
+  int rs = check_status(c);
+  if (rs < 0) { jp_destroy(c); return rs; }
+  *out = c;
+  return JP_OK;
+}
+
+void jp_destroy(jp_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  if (c->g_step) cudaGraphExecDestroy(c->g_step);
+  if (c->g_rebuild) cudaGraphExecDestroy(c->g_rebuild);
+  for (void *p : c->allocs) cudaFree(p);
+  for (auto ev : c->tev) cudaEventDestroy(ev);
+  if (c->ev_a) cudaEventDestroy(c->ev_a);
+  if (c->ev_b) cudaEventDestroy(c->ev_b);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+int jp_rebuild_cells(jp_ctx *c, int32_t replica) {
+  if (!c || replica < -1 || replica >= c->nrep) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  enqueue_rebuild(c);   // all replicas share one pass
+  CK(cudaStreamSynchronize(c->st));
+  return check_status(c);
+}
+
+int jp_set_state(jp_ctx *c, int32_t r, const double *cord, const double *vel) {
+  if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  const Rep &R = c->reps[r];
+  if (cord) CK(cudaMemcpyAsync(c->P.x + 3 * (size_t)R.atom0, cord, sizeof(double) * 3 * R.natom,
+                               cudaMemcpyHostToDevice, c->st));
+  if (vel) CK(cudaMemcpyAsync(c->P.v + 3 * (size_t)R.atom0, vel, sizeof(double) * 3 * R.natom,
+                              cudaMemcpyHostToDevice, c->st));
+  if (cord) launch_update_pos(c->P, c->nslot, c->fp64, c->qscale, c->st);
+  CK(cudaStreamSynchronize(c->st));
+  return JP_OK;
+}
+
+int jp_get_state(jp_ctx *c, int32_t r, double *cord, double *vel) {
+  if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  const Rep &R = c->reps[r];
+  if (cord) CK(cudaMemcpyAsync(cord, c->P.x + 3 * (size_t)R.atom0, sizeof(double) * 3 * R.natom,
+                               cudaMemcpyDeviceToHost, c->st));
+  if (vel) CK(cudaMemcpyAsync(vel, c->P.v + 3 * (size_t)R.atom0, sizeof(double) * 3 * R.natom,
+                              cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return JP_OK;
+}
+
+int jp_energy_grad(jp_ctx *c, int32_t r, const double *cord, double *eneval, double *grad) {
+  if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  const Rep &R = c->reps[r];
+  if (cord) {
+    CK(cudaMemcpyAsync(c->P.x + 3 * (size_t)R.atom0, cord, sizeof(double) * 3 * R.natom,
+                       cudaMemcpyHostToDevice, c->st));
+    launch_update_pos(c->P, c->nslot, c->fp64, c->qscale, c->st);
+  }
+  enqueue_forces(c, true);
+  enqueue_bonded(c);
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaGetLastError());
+  if (eneval) {
+    long long ef[16];
+    CK(cudaMemcpy(ef, c->P.ene_fix + 16 * (size_t)r, sizeof(ef), cudaMemcpyDeviceToHost));
+    double tot = 0.0;
+    for (int k = 1; k < JP_MAXENE; ++k) {
+      eneval[k] = (double)ef[k] * kEneInv;
+      if (k == JP_E_ELE15) eneval[k] += R.dself;
+      tot += eneval[k];
+    }
+    eneval[0] = tot;
+  }
+  if (grad) {
+    if (c->fp64) {
+      CK(cudaMemcpy(grad, c->P.grd + 3 * (size_t)R.atom0, sizeof(double) * 3 * R.natom,
+                    cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<long long> g(3 * (size_t)R.natom);
+      CK(cudaMemcpy(g.data(), c->P.frc + 3 * (size_t)R.atom0, sizeof(long long) * g.size(),
+                    cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < g.size(); ++i) grad[i] = (double)g[i] * kFrcInv;
+    }
+  }
+  return check_status(c);
+}
+
+int jp_pair_count(jp_ctx *c, int32_t r, int64_t *count) {
+  if (!c || r < 0 || r >= c->nrep || !count) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  long long v = 0;
+  CK(cudaMemcpy(&v, c->P.pair_cnt + r, sizeof(long long), cudaMemcpyDeviceToHost));
+  *count = v;
+  return JP_OK;
+}
+
+int jp_set_timing(jp_ctx *c, int enable) {
+  if (!c) return JP_E_INVALID;
+  c->tm.enabled = enable != 0;
+  return JP_OK;
+}
+
+int jp_last_timing(jp_ctx *c, double *total_ms, double *phase_ms4, int32_t *launches4) {
+  if (!c) return JP_E_INVALID;
+  if (total_ms) *total_ms = c->tm.total_ms;
+  for (int k = 0; k < 4; ++k) {
+    if (phase_ms4) phase_ms4[k] = c->tm.phase_ms[k];
+    if (launches4) launches4[k] = c->tm.launches[k];
+  }
+  return JP_OK;
+}
+
+int jp_list_stats(jp_ctx *c, int64_t *ntiles, int64_t *npairs_listed, int64_t *nslots) {
+  if (!c) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  int nt = 0;
+  CK(cudaMemcpy(&nt, c->P.ntiles, sizeof(int), cudaMemcpyDeviceToHost));
+  if (ntiles) *ntiles = nt;
+  if (nslots) *nslots = c->nslot;
+  if (npairs_listed) {
+    std::vector<unsigned> m((size_t)nt * 32);
+    if (nt) CK(cudaMemcpy(m.data(), c->P.masks, sizeof(unsigned) * m.size(), cudaMemcpyDeviceToHost));
+    int64_t s = 0;
+    for (unsigned v : m) s += __builtin_popcount(v);
+    *npairs_listed = s;
+  }
+  return JP_OK;
+}
+
+int jp_launch_counts(jp_ctx *c, int32_t *per_step, int32_t *per_rebuild) {
+  if (!c) return JP_E_INVALID;
+  if (per_step) *per_step = launches_per_step(c);
+  if (per_rebuild) *per_rebuild = c->launches_rebuild;
+  return JP_OK;
+}
+
+int jp_step(jp_ctx *c, int32_t nsteps, double *ene_out, double *temp_out) {
+  if (!c || nsteps < 0) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  if (nsteps == 0) return JP_OK;
+  if (!c->tm.enabled && !c->g_step) {
+    if (capture(c, &c->g_step, false)) return JP_E_CUDA;
+    if (capture(c, &c->g_rebuild, true)) return JP_E_CUDA;
+  }
+  for (int k = 0; k < 4; ++k) { c->tm.phase_ms[k] = 0.0; c->tm.launches[k] = 0; }
+  c->tm.total_ms = 0.0;
+  int done = 0;
+  while (done < nsteps) {
+    const int chunk = std::min(nsteps - done, c->hist_cap);
+    CK(cudaMemsetAsync(c->P.step_ctr + 1, 0, sizeof(int), c->st));
+    CK(cudaEventRecord(c->ev_a, c->st));
+    if (c->tm.enabled) {
+      const size_t need = (size_t)chunk * 8;
+      while (c->tev.size() < need) {
+        cudaEvent_t ev;
+        CK(cudaEventCreate(&ev));
+        c->tev.push_back(ev);
+      }
+      std::vector<int> rebuilt(chunk, 0);
+      for (int s = 0; s < chunk; ++s) {
+        cudaEvent_t *E = &c->tev[(size_t)s * 8];
+        enqueue_zero(c, false);
+        CK(cudaEventRecord(E[0], c->st));
+        enqueue_pair(c, false);
+        CK(cudaEventRecord(E[1], c->st));
+        enqueue_bonded(c);
+        CK(cudaEventRecord(E[2], c->st));
+        enqueue_integrate(c);
+        CK(cudaEventRecord(E[3], c->st));
+        c->idloop += 1;
+        if (c->prm.update > 0 && c->idloop % c->prm.update == 0) {
+          enqueue_rebuild(c);
+          rebuilt[s] = 1;
+        }
+        CK(cudaEventRecord(E[4], c->st));
+      }
+      CK(cudaEventRecord(c->ev_b, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      CK(cudaGetLastError());
+      for (int s = 0; s < chunk; ++s) {
+        cudaEvent_t *E = &c->tev[(size_t)s * 8];
+        float ms;
+        for (int k = 0; k < 3; ++k) {
+          CK(cudaEventElapsedTime(&ms, E[k], E[k + 1]));
+          c->tm.phase_ms[k] += ms;
+          c->tm.launches[k] += 1;
+        }
+        if (rebuilt[s]) {
+          CK(cudaEventElapsedTime(&ms, E[3], E[4]));
+          c->tm.phase_ms[3] += ms;
+          c->tm.launches[3] += 1;
+        }
+      }
+    } else {
+      for (int s = 0; s < chunk; ++s) {
+        CK(cudaGraphLaunch(c->g_step, c->st));
+        c->idloop += 1;
+        if (c->prm.update > 0 && c->idloop % c->prm.update == 0) CK(cudaGraphLaunch(c->g_rebuild, c->st));
+      }
+      CK(cudaEventRecord(c->ev_b, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      CK(cudaGetLastError());
+    }
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev_a, c->ev_b));
+    c->tm.total_ms += ms;
+    if (ene_out)
+      CK(cudaMemcpy(ene_out + (size_t)done * c->nrep * JP_MAXENE, c->P.ene_hist,
+                    sizeof(double) * (size_t)chunk * c->nrep * JP_MAXENE, cudaMemcpyDeviceToHost));
+    if (temp_out)
+      CK(cudaMemcpy(temp_out + (size_t)done * c->nrep, c->P.temp_hist,
+                    sizeof(double) * (size_t)chunk * c->nrep, cudaMemcpyDeviceToHost));
+    int rs = check_status(c);
+    if (rs != JP_OK) return rs;
+    done += chunk;
+  }
+  return JP_OK;
+}
+
+int jp_shake(jp_ctx *c, int32_t r, double *r1, const double *r2) {
+  if (!c || r < 0 || r >= c->nrep || !r1 || !r2) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  const Rep &R = c->reps[r];
+  const size_t n3 = 3 * (size_t)R.natom;
+  CK(cudaMemcpyAsync(c->P.xback + 3 * (size_t)R.atom0, r1, sizeof(double) * n3, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->P.x0 + 3 * (size_t)R.atom0, r2, sizeof(double) * n3, cudaMemcpyHostToDevice, c->st));
+  launch_shake_only(c->P, c->ic, R.unit0, R.nunit, c->st);
+  CK(cudaMemcpyAsync(r1, c->P.xback + 3 * (size_t)R.atom0, sizeof(double) * n3, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return check_status(c);
+}
+
+}  // extern "C"

@@ -1,0 +1,320 @@
+// jp_cells.cu -- device cell-list build and pair-tile list (replaces md_run celprp/celpar/
+// cutoff: src_md_run/celprp.f90:2-175, celpar.f90:2-244, cutoff.f90:2-505).
+//
+// Pipeline (every UPDATE steps, all replicas in one pass):
+//   1. k_cell_key      radix binning: wrapped position -> fine cell -> Morton key per replica
+//   2. scan            counting-sort offsets (deterministic exclusive scan)
+//   3. k_scatter       bin atoms; k_sort_bins makes the order within a bin deterministic
+//   4. k_fill_slots    compact order -> 32-atom blocks padded per replica
+//   5. k_block_setup   per-block bounding box, frame origin, block-local coordinates
+//   6. k_tile_scan_chunks  one warp per (i-block, 32 candidate j-blocks): bounding-box test
+//                      of the 32 candidates at once, warp-ballot compaction of the
+//                      survivors, then the exact 32x32 interaction mask in FP64:
+//                      r^2 <= (rc+1.5)^2 at build time (cutatm `dd .le. rlim2`), minus
+//                      1-2/1-3/1-4 partners (cutoff.f90:50-96).
+//   7. scan of the per-chunk tile counts, k_tile_emit writes one dense list in row-major,
+//      ascending-j order (deterministic).
+#include "jp_common.cuh"
+#include "jp_kernels.h"
+
+namespace jp {
+
+__device__ __forceinline__ unsigned spread3(unsigned v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__global__ void k_cell_key(DevPtrs P, int natom) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natom) return;
+  const Rep R = P.reps[P.rep_of[a]];
+  unsigned c[3];
+  for (int k = 0; k < 3; ++k) {
+    double x = P.x[3 * a + k];
+    double w = x - R.box[k] * floor(x * R.invbox[k]);
+    int q = (int)(w / R.cell[k]);
+    q = q < 0 ? 0 : (q >= R.grid[k] ? R.grid[k] - 1 : q);
+    c[k] = (unsigned)q;
+  }
+  unsigned key = (unsigned)R.key0 + (spread3(c[0]) | (spread3(c[1]) << 1) | (spread3(c[2]) << 2));
+  P.key[a] = key;
+  atomicAdd(&P.hist[key], 1);
+}
+
+__global__ void k_scatter(DevPtrs P, int natom) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natom) return;
+  unsigned key = P.key[a];
+  int pos = P.hist_scan[key] + atomicAdd(&P.cursor[key], 1);
+  P.sorted[pos] = a;
+}
+
+// deterministic order inside each bin: ascending atom index (bins hold a few atoms)
+__global__ void k_sort_bins(DevPtrs P, int nkeys) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nkeys) return;
+  int n = P.hist[k];
+  if (n < 2) return;
+  int* s = P.sorted + P.hist_scan[k];
+  for (int i = 1; i < n; ++i) {
+    int v = s[i];
+    int j = i - 1;
+    while (j >= 0 && s[j] > v) { s[j + 1] = s[j]; --j; }
+    s[j + 1] = v;
+  }
+}
+
+__global__ void k_clear_slots(DevPtrs P, int nslot, int dummy_type) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslot) return;
+  P.satom[s] = -1;
+  P.styp[s] = dummy_type;
+}
+
+__global__ void k_fill_slots(DevPtrs P, int natom) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= natom) return;
+  int a = P.sorted[c];
+  const Rep& R = P.reps[P.rep_of[a]];
+  int slot = c - R.atom0 + kTile * R.blk0;
+  P.slot_of[a] = slot;
+  P.satom[slot] = a;
+  P.styp[slot] = P.typ[a];
+}
+
+// one warp per block
+__global__ void k_block_setup(DevPtrs P, int nblk, double qscale) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= nblk) return;
+  const int slot = warp * kTile + lane;
+  const int a = P.satom[slot];
+  const Rep R = P.reps[P.blk_rep[warp]];
+  double w[3] = {0, 0, 0}, img[3] = {0, 0, 0};
+  double lo[3], hi[3];
+  for (int k = 0; k < 3; ++k) {
+    if (a >= 0) {
+      double x = P.x[3 * a + k];
+      img[k] = floor(x * R.invbox[k]);
+      w[k] = x - R.box[k] * img[k];
+      lo[k] = w[k];
+      hi[k] = w[k];
+    } else {
+      lo[k] = 1e300;
+      hi[k] = -1e300;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+  }
+  double ref[3];
+  for (int k = 0; k < 3; ++k) ref[k] = 0.5 * (lo[k] + hi[k]);
+  if (lane == 0) {
+    P.blk_ref[3 * warp + 0] = ref[0];
+    P.blk_ref[3 * warp + 1] = ref[1];
+    P.blk_ref[3 * warp + 2] = ref[2];
+    P.blk_ctr[warp] = make_float4((float)ref[0], (float)ref[1], (float)ref[2], 0.f);
+    P.blk_half[warp] = make_float4((float)(0.5 * (hi[0] - lo[0])) + 1e-4f,
+                                   (float)(0.5 * (hi[1] - lo[1])) + 1e-4f,
+                                   (float)(0.5 * (hi[2] - lo[2])) + 1e-4f, 0.f);
+  }
+  double o[3];
+  for (int k = 0; k < 3; ++k) o[k] = ref[k] + R.box[k] * img[k];
+  P.off[3 * slot + 0] = o[0];
+  P.off[3 * slot + 1] = o[1];
+  P.off[3 * slot + 2] = o[2];
+  if (a >= 0) {
+    float q = (float)((double)qscale * P.chg[a]);
+    P.pos_f[slot] = make_float4((float)(P.x[3 * a] - o[0]), (float)(P.x[3 * a + 1] - o[1]),
+                                (float)(P.x[3 * a + 2] - o[2]), q);
+  } else {
+    P.pos_f[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+// FP64 slot positions (absolute master coordinates) + charges; used every step by the FP64
+// path and after a rebuild by both paths.
+__global__ void k_fill_pos_d(DevPtrs P, int nslot, double qscale) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslot) return;
+  int a = P.satom[s];
+  if (a >= 0) P.pos_d[s] = make_double4(P.x[3 * a], P.x[3 * a + 1], P.x[3 * a + 2], qscale * P.chg[a]);
+  else P.pos_d[s] = make_double4(0.0, 0.0, 0.0, 0.0);
+}
+
+__device__ __forceinline__ bool excluded(const DevPtrs& P, int ai, int aj) {
+  int b = P.excl_ptr[ai], e = P.excl_ptr[ai + 1];
+  for (int p = b; p < e; ++p)
+    if (P.excl_idx[p] == aj) return true;
+  return false;
+}
+
+// Tile list, pass A: one warp per chunk = (i-block, 32 consecutive candidate j-blocks
+// starting at j0 >= i, same replica).  Bounding-box test of the 32 candidates at once, then
+// for each survivor the exact mask; non-empty masks go to the chunk's scratch slots.
+__device__ __forceinline__ unsigned tile_mask(const DevPtrs& P, const Rep& R, int bi, int bj, int lane,
+                                              int ai, double xi, double yi, double zi, bool iexcl,
+                                              double rlim2) {
+  const int aj = P.satom[bj * kTile + lane];
+  double xj = 0, yj = 0, zj = 0;
+  if (aj >= 0) { xj = P.x[3 * aj]; yj = P.x[3 * aj + 1]; zj = P.x[3 * aj + 2]; }
+  unsigned mask = 0;
+  for (int k = 0; k < 32; ++k) {
+    const int src = (lane + k) & 31;
+    const double xk = __shfl_sync(0xffffffffu, xj, src);
+    const double yk = __shfl_sync(0xffffffffu, yj, src);
+    const double zk = __shfl_sync(0xffffffffu, zj, src);
+    const int ak = __shfl_sync(0xffffffffu, aj, src);
+    if (ai < 0 || ak < 0) continue;
+    if (bj == bi && (k == 0 || k > 16 || (k == 16 && lane >= 16))) continue;
+    double dx = xi - xk, dy = yi - yk, dz = zi - zk;
+    dx -= R.box[0] * anint(dx * R.invbox[0]);
+    dy -= R.box[1] * anint(dy * R.invbox[1]);
+    dz -= R.box[2] * anint(dz * R.invbox[2]);
+    if (dx * dx + dy * dy + dz * dz <= rlim2) {
+      if (iexcl && excluded(P, ai, ak)) continue;
+      mask |= 1u << k;
+    }
+  }
+  return mask;
+}
+
+__global__ void k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rlimf) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= nchunk) return;
+  const int bi = P.chunk_i[w], j0 = P.chunk_j0[w];
+  const Rep R = P.reps[P.blk_rep[bi]];
+  const int bend = R.blk0 + R.nblk;
+  const float4 ci = P.blk_ctr[bi], hi = P.blk_half[bi];
+  const int bj = j0 + lane;
+  bool cand = false;
+  if (bj < bend) {
+    const float4 cj = P.blk_ctr[bj], hj = P.blk_half[bj];
+    float dx = ci.x - cj.x, dy = ci.y - cj.y, dz = ci.z - cj.z;
+    dx -= (float)R.box[0] * rintf(dx * (float)R.invbox[0]);
+    dy -= (float)R.box[1] * rintf(dy * (float)R.invbox[1]);
+    dz -= (float)R.box[2] * rintf(dz * (float)R.invbox[2]);
+    const float gx = fmaxf(fabsf(dx) - hi.x - hj.x, 0.f);
+    const float gy = fmaxf(fabsf(dy) - hi.y - hj.y, 0.f);
+    const float gz = fmaxf(fabsf(dz) - hi.z - hj.z, 0.f);
+    cand = gx * gx + gy * gy + gz * gz <= rlimf * rlimf * 1.0001f + 1e-3f;
+  }
+  unsigned ball = __ballot_sync(0xffffffffu, cand);
+  unsigned nz = 0;
+  if (ball) {
+    const int ai = P.satom[bi * kTile + lane];
+    double xi = 0, yi = 0, zi = 0;
+    if (ai >= 0) { xi = P.x[3 * ai]; yi = P.x[3 * ai + 1]; zi = P.x[3 * ai + 2]; }
+    const bool iexcl = ai >= 0 && P.excl_ptr[ai + 1] > P.excl_ptr[ai];
+    while (ball) {
+      const int b = __ffs(ball) - 1;
+      ball &= ball - 1;
+      const unsigned m = tile_mask(P, R, bi, j0 + b, lane, ai, xi, yi, zi, iexcl, rlim2);
+      if (__any_sync(0xffffffffu, m != 0)) {
+        P.tmp_masks[((size_t)w * 32 + b) * 32 + lane] = m;
+        nz |= 1u << b;
+      }
+    }
+  }
+  if (lane == 0) {
+    P.chunk_nz[w] = nz;
+    P.chunk_cnt[w] = __popc(nz);
+  }
+}
+
+// pass C: copy non-empty tiles to the dense list at the scanned offsets (row-major, j order)
+__global__ void k_tile_emit(DevPtrs P, int nchunk) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= nchunk) return;
+  unsigned nz = P.chunk_nz[w];
+  if (!nz) return;
+  const int bi = P.chunk_i[w], j0 = P.chunk_j0[w];
+  const Rep& R = P.reps[P.blk_rep[bi]];
+  int t = P.chunk_off[w];
+  while (nz) {
+    const int b = __ffs(nz) - 1;
+    nz &= nz - 1;
+    P.masks[(size_t)t * 32 + lane] = P.tmp_masks[((size_t)w * 32 + b) * 32 + lane];
+    if (lane == 0) {
+      const int bj = j0 + b;
+      P.tiles[t] = make_int2(bi, bj);
+      double s[3];
+      for (int k = 0; k < 3; ++k) {
+        const double d = P.blk_ref[3 * bi + k] - P.blk_ref[3 * bj + k];
+        s[k] = d - R.box[k] * anint(d * R.invbox[k]);
+      }
+      P.tile_shift[t] = make_float4((float)s[0], (float)s[1], (float)s[2], 0.f);
+    }
+    ++t;
+  }
+}
+
+// ---- deterministic exclusive scan (3 passes) --------------------------------------------
+__global__ void k_scan_block_sums(const int* in, int n, int* bsum) {
+  __shared__ int sh[1024];
+  int i = blockIdx.x * 1024 + threadIdx.x;
+  int v = i < n ? in[i] : 0;
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 512; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) bsum[blockIdx.x] = sh[0];
+}
+
+// single block: exclusive scan of nb block sums (any nb)
+__global__ void k_scan_small(int* bsum, int nb) {
+  __shared__ int sh[1024];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < nb; b0 += 1024) {
+    int i = b0 + threadIdx.x;
+    int v = i < nb ? bsum[i] : 0;
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+      int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+      __syncthreads();
+      sh[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < nb) bsum[i] = carry + sh[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += sh[1023];
+    __syncthreads();
+  }
+}
+
+__global__ void k_scan_final(const int* in, int n, const int* bsum, int* out, int* total) {
+  __shared__ int sh[1024];
+  int i = blockIdx.x * 1024 + threadIdx.x;
+  int v = i < n ? in[i] : 0;
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+    __syncthreads();
+    sh[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < n) out[i] = bsum[blockIdx.x] + sh[threadIdx.x] - v;
+  if (i == n - 1 && total) *total = bsum[blockIdx.x] + sh[threadIdx.x];
+}
+
+void scan_exclusive(const int* in, int* out, int n, int* scratch, int* total, cudaStream_t st) {
+  int nb = (n + 1023) / 1024;
+  k_scan_block_sums<<<nb, 1024, 0, st>>>(in, n, scratch);
+  k_scan_small<<<1, 1024, 0, st>>>(scratch, nb);
+  k_scan_final<<<nb, 1024, 0, st>>>(in, n, scratch, out, total);
+}
+
+}  // namespace jp

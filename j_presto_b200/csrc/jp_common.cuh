@@ -1,0 +1,140 @@
+// jp_common.cuh -- device-side data layout shared by the engine's kernels.
+//
+// Layout in HBM (all replicas concatenated; "atom" = original md_run order, "slot" =
+// cell-sorted order padded to 32-atom blocks):
+//   atoms : x, v      double[N][3]   master FP64 state (cord, vel of md_run)
+//           frc       long long[N][3] 64-bit fixed-point gradient (mixed path)
+//           grd       double[N][3]   FP64 gradient (FP64 path)
+//   slots : pos_f     float4[S]      (x-off, y-off, z-off, q*sqrt(332/eps)) block-local
+//           pos_d     double4[S]     (x, y, z, q*sqrt(332/eps)) absolute (FP64 path)
+//           off       double[S][3]   block frame origin of the slot (ref + L*image)
+//           styp      int[S]         LJ type (padding -> dummy zero type)
+//           satom     int[S]         atom of the slot, -1 for padding
+//   blocks: 32 slots each; tiles = (i-block, j-block) pairs with a 32x32 interaction mask.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "jpgpu.h"
+
+namespace jp {
+
+constexpr int kTile = 32;
+// fixed-point scales: forces 2^32 per kcal/mol/A, energies 2^32 per kcal/mol,
+// kinetic sums (m v^2, amu A^2/fs^2) 2^40.
+constexpr double kFrcScale = 4294967296.0;
+constexpr double kFrcInv = 1.0 / 4294967296.0;
+constexpr double kEneScale = 4294967296.0;
+constexpr double kEneInv = 1.0 / 4294967296.0;
+constexpr double kKinScale = 1099511627776.0;
+constexpr double kKinInv = 1.0 / 1099511627776.0;
+constexpr double kFixMax = 9.0e18;   // |value*scale| must stay below this
+
+constexpr double kConvcv = 4.184e-4;       // md.f90:56
+constexpr double kGas = 8.31451;           // PHYCNS gascst
+constexpr double kJouCal = 4.184;
+
+// error bits of the device status word
+enum : unsigned {
+  ERR_SHAKE_NOCONV = 1u, ERR_SHAKE_SINGULAR = 2u, ERR_NONFINITE = 4u,
+  ERR_FIX_OVERFLOW = 8u, ERR_LIST_OVERFLOW = 16u, ERR_SORT = 32u
+};
+
+// per-replica constants
+struct Rep {
+  int atom0, natom;        // atom range
+  int blk0, nblk;          // block range (slots [32*blk0, 32*(blk0+nblk)))
+  int unit0, nunit;        // integration units
+  int sub0, nsub;          // temperature sub-systems (global ids)
+  int key0, keybits;       // cell-key range start, Morton bits per dimension
+  int grid[3];
+  double box[3], invbox[3];
+  double cell[3];          // cell edge per dimension
+  double dself;
+  int ge_off, ge_nwin, ge_ndeg;   // offset into the GE coefficient array
+  double ge_alphalw, ge_alphaup, ge_celw, ge_ceup, ge_tempce;
+};
+
+// integration unit: a SHAKE group (2-4 atoms) or a lone atom (n = 1)
+struct Unit {
+  int n;
+  int a[4];
+  int sub;                 // sub-system of its atoms
+  int rep;
+  double d2[6];            // squared constraint lengths, md_run pair order
+};
+
+// bonded term of any kind, flattened
+enum : int { T_BOND = 0, T_ANGLE = 1, T_TORS = 2, T_IMPR = 3, T_P14 = 4, T_EXCESS = 5 };
+struct Term {
+  int kind;
+  int rep;
+  int a[4];
+  double p0, p1, p2;       // bond: k, r0 | angle: k, t0 | tors: k, nrot, phase | 14: svdw, sele
+  int idiv;
+  int pad;
+};
+
+struct DevPtrs {
+  // atoms
+  double *x, *v, *x0, *vback, *xback, *forcec;
+  double *mass, *imass, *chg;
+  int *typ, *rep_of, *slot_of;
+  long long *frc;
+  double *grd;
+  // exclusions (global atom ids)
+  int *excl_ptr, *excl_idx;
+  // slots / blocks
+  float4 *pos_f;
+  double4 *pos_d;
+  double *off;
+  int *styp, *satom;
+  int *blk_rep;
+  float4 *blk_ctr, *blk_half;     // bbox (wrapped frame) centre / half extent
+  double *blk_ref;                // [B][3]
+  // tile-list build: chunk = (i-block, 32 candidate j-blocks from j0)
+  int *chunk_i, *chunk_j0;        // static per context
+  unsigned *chunk_nz;             // non-empty candidates of the chunk (bit b = j0+b)
+  int *chunk_cnt, *chunk_off;     // their count and its exclusive scan [nchunk+1]
+  unsigned *tmp_masks;            // [nchunk*32][32] masks of the chunk candidates
+  // tiles
+  int2 *tiles;                    // dense (i-block, j-block)
+  float4 *tile_shift;             // dense min-image shift of block refs (mixed path)
+  unsigned *masks;                // dense masks [T][32]
+  int *ntiles;                    // device scalar
+  // cell sort
+  unsigned *key;                  // per atom
+  int *hist, *hist_scan, *cursor; // per key
+  int *sorted;                    // compact order -> atom
+  // units / terms
+  Unit *units;
+  Term *terms;
+  // replicas
+  Rep *reps;
+  double *ge_coef;
+  // accumulators
+  long long *ene_fix;             // [nrep][16]
+  long long *kin_fix;             // [nslots_kin][nsub_total]
+  double *nfr;                    // DOF per sub-system
+  double *scale;                  // per replica force scale (GE / pseudo-T)
+  int *done;                      // per replica SHAKE-thermostat loop finished
+  unsigned *status;               // error bits
+  long long *pair_cnt;            // [nrep]
+  double *ene_hist;               // [max_steps][nrep][15]
+  double *temp_hist;              // [max_steps][nrep]
+  int *step_ctr;                  // device step counter (idloop)
+  // LJ table
+  float2 *lj_f;                   // (C6, C12) [(nt+1)^2]
+  double2 *lj_d;
+};
+
+__device__ __forceinline__ long long to_fix(double v, double scale) {
+  return __double2ll_rn(v * scale);
+}
+
+__device__ __forceinline__ void atomic_add_ll(long long *p, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long *>(p), static_cast<unsigned long long>(v));
+}
+
+__host__ __device__ __forceinline__ double anint(double x) { return round(x); }
+
+}  // namespace jp

@@ -1,0 +1,639 @@
+// jp_integrate.cu -- leap-frog integration fused with SHAKE, temperature control and the
+// generalized-ensemble force scaling.
+//
+// Replaces verlet (src_md_run/verlet.f90:2-226, METHOD= MICR), verlethe (verlethe.f90:2-758,
+// METHOD= CANO and GE/McMD), shake_PB (shake.f90:2-755) and caltmp/caltmp2 (caltmp.f90).
+// One thread owns one integration unit: a SHAKE group (2-4 atoms, all pair distances
+// constrained) or a lone atom, so SHAKE needs no inter-thread communication.  Everything
+// is FP64.  Kinetic-energy sums for the thermostat are 64-bit fixed point (order
+// independent); all replicas are processed by the same launches and each replica keeps
+// its own temperatures, SHAKE<->thermostat iteration count and force scale.
+#include "jp_kernels.h"
+
+namespace jp {
+
+// Loop over the 1-4 atoms of an integration unit.  The trip count is fixed at 4 and fully
+// unrolled with a guard: the per-unit arrays then live in registers.  (A runtime trip count
+// over these small local arrays produced wrong values on sm_100a with nvcc 12.9.)
+#define JP_UNIT_LOOP(q) _Pragma("unroll") for (int q = 0; q < 4; ++q) if (q < u.n)
+
+__host__ __device__ __forceinline__ void mimg(const Rep& R, double* d) {
+  for (int k = 0; k < 3; ++k) d[k] -= R.box[k] * anint(d[k] * R.invbox[k]);
+}
+
+template <bool FP64>
+__device__ __forceinline__ void load_grad(const DevPtrs& P, int a, double s, double* g) {
+  if (FP64) {
+    for (int k = 0; k < 3; ++k) g[k] = P.grd[3 * a + k] * s;
+  } else {
+    for (int k = 0; k < 3; ++k) g[k] = (double)P.frc[3 * a + k] * kFrcInv * s;
+  }
+}
+
+// ---- SHAKE on one group (r1 constrained against reference r2) --------------------------
+// returns 0 converged, 1 not converged, -2 singular
+__host__ __device__ int shake_group(const Rep& R, const Unit& u, const double* im, double r1[4][3],
+                           const double r2[4][3], int method, double tol, int maxit) {
+  const int n = u.n;
+  if (n == 2) {
+    double d1[3], d2[3];
+    if (method == JP_SHAKE_HBON) {   // shak2e (shake.f90:687-755): exact quadratic
+      for (int k = 0; k < 3; ++k) { d1[k] = r1[1][k] - r1[0][k]; d2[k] = r2[1][k] - r2[0][k]; }
+      mimg(R, d1);
+      mimg(R, d2);
+      const double i3 = im[0] + im[1], i4 = i3 * i3;
+      const double d1d1 = d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2];
+      const double d1d2 = d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2];
+      const double d2d2 = d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2];
+      const double A = i4 * d2d2, B = i3 * d1d2, C = d1d1 - u.d2[0];
+      const double G = (B - sqrt(B * B - C * A)) / A;
+      for (int k = 0; k < 3; ++k) {
+        r1[0][k] += im[0] * G * d2[k];
+        r1[1][k] -= im[1] * G * d2[k];
+      }
+      return 0;
+    }
+    // shak2i (shake.f90:568-681): iterate this constraint to its own tolerance
+    for (int k = 0; k < 3; ++k) d2[k] = r2[0][k] - r2[1][k];
+    mimg(R, d2);
+    const double i3 = 0.5 / (im[0] + im[1]);
+    for (int it = 0; it < maxit; ++it) {
+      for (int k = 0; k < 3; ++k) d1[k] = r1[0][k] - r1[1][k];
+      mimg(R, d1);
+      double dif = u.d2[0] - (d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
+      const double inpro = d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2];
+      const double G = dif * i3 / inpro;
+      for (int k = 0; k < 3; ++k) {
+        r1[0][k] += im[0] * G * d2[k];
+        r1[1][k] -= im[1] * G * d2[k];
+      }
+      for (int k = 0; k < 3; ++k) d1[k] = r1[0][k] - r1[1][k];
+      mimg(R, d1);
+      dif = u.d2[0] - (d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
+      if (fabs(dif / u.d2[0]) < tol) return 0;
+    }
+    return 1;
+  }
+  if (n == 3) {   // shake3 (shake.f90:113-327): Newton, closed-form 3x3 inverse
+    const double cg[3][3] = {{im[0] + im[1], -im[1], -im[0]},
+                             {-im[1], im[1] + im[2], -im[2]},
+                             {-im[0], -im[2], im[2] + im[0]}};
+    const int pa[3][2] = {{0, 1}, {1, 2}, {2, 0}};
+    double d1[3][3], d2[3][3];
+    for (int q = 0; q < 3; ++q) {
+      for (int k = 0; k < 3; ++k) {
+        d1[q][k] = r1[pa[q][0]][k] - r1[pa[q][1]][k];
+        d2[q][k] = r2[pa[q][0]][k] - r2[pa[q][1]][k];
+      }
+      mimg(R, d1[q]);
+      mimg(R, d2[q]);
+    }
+    double G[6] = {0, 0, 0, 0, 0, 0};
+    bool singular = false;
+    for (int it = 0; it < maxit; ++it) {
+      double B[3];
+      for (int q = 0; q < 3; ++q) B[q] = u.d2[q] - (d1[q][0] * d1[q][0] + d1[q][1] * d1[q][1] + d1[q][2] * d1[q][2]);
+      if (fabs(B[0]) < tol * u.d2[0] && fabs(B[1]) < tol * u.d2[1] && fabs(B[2]) < tol * u.d2[2]) {
+        for (int k = 0; k < 3; ++k) {
+          r1[0][k] += im[0] * (G[3] * d2[0][k] - G[5] * d2[2][k]);
+          r1[1][k] += im[1] * (-G[3] * d2[0][k] + G[4] * d2[1][k]);
+          r1[2][k] += im[2] * (-G[4] * d2[1][k] + G[5] * d2[2][k]);
+        }
+        return singular ? -2 : 0;
+      }
+      double gf[3][3];
+      for (int ig = 0; ig < 3; ++ig)
+        for (int q = 0; q < 3; ++q)
+          gf[q][ig] = 2.0 * cg[q][ig] * (d1[q][0] * d2[ig][0] + d1[q][1] * d2[ig][1] + d1[q][2] * d2[ig][2]);
+      double deta = gf[0][0] * gf[1][1] * gf[2][2] + gf[0][1] * gf[1][2] * gf[2][0] +
+                    gf[0][2] * gf[1][0] * gf[2][1] - gf[0][0] * gf[1][2] * gf[2][1] -
+                    gf[0][1] * gf[1][0] * gf[2][2] - gf[0][2] * gf[1][1] * gf[2][0];
+      if (deta == 0.0) singular = true;
+      else deta = 1.0 / deta;
+      double db[3][3];
+      db[0][0] = gf[1][1] * gf[2][2] - gf[1][2] * gf[2][1];
+      db[0][1] = gf[2][1] * gf[0][2] - gf[2][2] * gf[0][1];
+      db[0][2] = gf[0][1] * gf[1][2] - gf[0][2] * gf[1][1];
+      db[1][0] = gf[1][2] * gf[2][0] - gf[1][0] * gf[2][2];
+      db[1][1] = gf[2][2] * gf[0][0] - gf[2][0] * gf[0][2];
+      db[1][2] = gf[0][2] * gf[1][0] - gf[0][0] * gf[1][2];
+      db[2][0] = gf[1][0] * gf[2][1] - gf[1][1] * gf[2][0];
+      db[2][1] = gf[2][0] * gf[0][1] - gf[2][1] * gf[0][0];
+      db[2][2] = gf[0][0] * gf[1][1] - gf[0][1] * gf[1][0];
+      for (int q = 0; q < 3; ++q) G[q] = deta * (db[q][0] * B[0] + db[q][1] * B[1] + db[q][2] * B[2]);
+      for (int q = 0; q < 3; ++q) G[3 + q] += G[q];
+      for (int q = 0; q < 3; ++q)
+        for (int k = 0; k < 3; ++k)
+          d1[q][k] += cg[q][0] * d2[0][k] * G[0] + cg[q][1] * d2[1][k] * G[1] + cg[q][2] * d2[2][k] * G[2];
+    }
+    return singular ? -2 : 1;
+  }
+  // n == 4: shake4 (shake.f90:333-562): Newton with LU (simulu.f90)
+  const double cg[6][6] = {
+      {im[0] + im[1], -im[1], -im[0], -im[0], 0.0, -im[1]},
+      {-im[1], im[1] + im[2], -im[2], 0.0, -im[2], im[1]},
+      {-im[0], -im[2], im[2] + im[0], im[0], im[2], 0.0},
+      {-im[0], 0.0, im[0], im[3] + im[0], -im[3], -im[3]},
+      {0.0, -im[2], im[2], -im[3], im[2] + im[3], im[3]},
+      {-im[1], im[1], 0.0, -im[3], im[3], im[1] + im[3]}};
+  const int pa[6][2] = {{0, 1}, {1, 2}, {2, 0}, {3, 0}, {2, 3}, {1, 3}};
+  double d1[6][3], d2[6][3], wk[6][3], G[6] = {0, 0, 0, 0, 0, 0};
+  for (int q = 0; q < 6; ++q) {
+    for (int k = 0; k < 3; ++k) {
+      d1[q][k] = r1[pa[q][0]][k] - r1[pa[q][1]][k];
+      d2[q][k] = r2[pa[q][0]][k] - r2[pa[q][1]][k];
+    }
+    mimg(R, d1[q]);
+    mimg(R, d2[q]);
+    for (int k = 0; k < 3; ++k) wk[q][k] = d1[q][k];
+  }
+  bool singular = false;
+  for (int it = 0; it < maxit; ++it) {
+    double B[6];
+    bool ok = true;
+    for (int q = 0; q < 6; ++q) {
+      B[q] = u.d2[q] - (wk[q][0] * wk[q][0] + wk[q][1] * wk[q][1] + wk[q][2] * wk[q][2]);
+      if (fabs(B[q]) >= tol * u.d2[q]) ok = false;
+    }
+    if (ok) {
+      for (int k = 0; k < 3; ++k) {
+        r1[0][k] += im[0] * (G[0] * d2[0][k] - G[2] * d2[2][k] - G[3] * d2[3][k]);
+        r1[1][k] += im[1] * (-G[0] * d2[0][k] + G[1] * d2[1][k] + G[5] * d2[5][k]);
+        r1[2][k] += im[2] * (-G[1] * d2[1][k] + G[2] * d2[2][k] + G[4] * d2[4][k]);
+        r1[3][k] += im[3] * (G[3] * d2[3][k] - G[4] * d2[4][k] - G[5] * d2[5][k]);
+      }
+      return singular ? -2 : 0;
+    }
+    double A[6][6];
+    for (int ig = 0; ig < 6; ++ig)
+      for (int q = 0; q < 6; ++q)
+        A[q][ig] = 2.0 * cg[q][ig] * (wk[q][0] * d2[ig][0] + wk[q][1] * d2[ig][1] + wk[q][2] * d2[ig][2]);
+    for (int ig = 0; ig < 6; ++ig)
+      for (int q = 0; q < 6; ++q) B[q] += A[q][ig] * G[ig];
+    // LU with partial pivoting through a row permutation (simulu.f90 ludeco + solve)
+    int ip[6] = {0, 1, 2, 3, 4, 5};
+    bool lu_ok = true;
+    for (int k = 0; k < 6 && lu_ok; ++k) {
+      int l = k;
+      double al = fabs(A[ip[l]][k]);
+      for (int i = k + 1; i < 6; ++i)
+        if (fabs(A[ip[i]][k]) > al) { l = i; al = fabs(A[ip[l]][k]); }
+      if (l != k) { int t = ip[k]; ip[k] = ip[l]; ip[l] = t; }
+      if (fabs(A[ip[k]][k]) < 1.0e-30) { lu_ok = false; break; }
+      A[ip[k]][k] = 1.0 / A[ip[k]][k];
+      for (int i = k + 1; i < 6; ++i) {
+        A[ip[i]][k] *= A[ip[k]][k];
+        for (int j = k + 1; j < 6; ++j) A[ip[i]][j] -= A[ip[i]][k] * A[ip[k]][j];
+      }
+    }
+    if (!lu_ok) {
+      singular = true;
+    } else {
+      for (int i = 0; i < 6; ++i) {
+        double t = B[ip[i]];
+        for (int j = 0; j < i; ++j) t -= A[ip[i]][j] * G[j];
+        G[i] = t;
+      }
+      for (int i = 5; i >= 0; --i) {
+        double t = G[i];
+        for (int j = i + 1; j < 6; ++j) t -= A[ip[i]][j] * G[j];
+        G[i] = t * A[ip[i]][i];
+      }
+    }
+    for (int q = 0; q < 6; ++q)
+      for (int k = 0; k < 3; ++k) wk[q][k] = d1[q][k];
+    for (int ig = 0; ig < 6; ++ig)
+      for (int q = 0; q < 6; ++q)
+        for (int k = 0; k < 3; ++k) wk[q][k] += cg[q][ig] * d2[ig][k] * G[ig];
+  }
+  return singular ? -2 : 1;
+}
+
+__device__ __forceinline__ void shake_status(const DevPtrs& P, int ier) {
+  if (ier == 1) atomicOr(P.status, ERR_SHAKE_NOCONV);
+  else if (ier == -2) atomicOr(P.status, ERR_SHAKE_SINGULAR);
+}
+
+// warp-aggregated fixed-point add of m v^2 into kin_fix[slot][sub]
+__device__ __forceinline__ void add_kin(const DevPtrs& P, int nsub_total, int kslot, int sub, double e) {
+  const unsigned full = 0xffffffffu;
+  const int s0 = __shfl_sync(full, sub, 0);
+  long long* dst = P.kin_fix + (size_t)kslot * nsub_total;
+  if (__all_sync(full, sub == s0)) {
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(full, e, o);
+    if ((threadIdx.x & 31) == 0 && s0 >= 0) atomic_add_ll(&dst[s0], to_fix(e, kKinScale));
+  } else if (sub >= 0 && e != 0.0) {
+    atomic_add_ll(&dst[sub], to_fix(e, kKinScale));
+  }
+}
+
+__device__ __forceinline__ void write_slot(const DevPtrs& P, int a, const double* x, bool fp64) {
+  const int s = P.slot_of[a];
+  if (fp64) {
+    double4 p = P.pos_d[s];
+    p.x = x[0]; p.y = x[1]; p.z = x[2];
+    P.pos_d[s] = p;
+  } else {
+    float4 p = P.pos_f[s];
+    p.x = (float)(x[0] - P.off[3 * s]);
+    p.y = (float)(x[1] - P.off[3 * s + 1]);
+    p.z = (float)(x[2] - P.off[3 * s + 2]);
+    P.pos_f[s] = p;
+  }
+}
+
+// target temperature with the heating ramp (verlethe.f90:412-416)
+__device__ __forceinline__ double target_temp(const IntConst& c, long long idloop) {
+  if (c.heat_loop <= 0 || idloop > c.heat_loop) return c.temp;
+  return c.temp_start + ((c.temp - c.temp_start) / (double)c.heat_loop) * (double)idloop;
+}
+
+__device__ __forceinline__ double sub_temp(const DevPtrs& P, const IntConst& c, int kslot, int sub) {
+  const double ek = (double)P.kin_fix[(size_t)kslot * c.nsub_total + sub] * kKinInv;
+  return ek * 1.0e7 / (kGas * P.nfr[sub]);
+}
+
+// converged after iteration `it` (kinetic slot 2*it-1)?  verlethe.f90:614-623
+__device__ bool cano_conv(const DevPtrs& P, const IntConst& c, const Rep& R, int it, double tt) {
+  const int ks = 2 * it - 1;
+  double mn = 1e300, mx = -1e300;
+  for (int s = R.sub0; s < R.sub0 + R.nsub; ++s) {
+    if (P.nfr[s] <= 0.0) continue;
+    const double t = sub_temp(P, c, ks, s);
+    mn = fmin(mn, t);
+    mx = fmax(mx, t);
+  }
+  return fmax(fabs(mn - tt), fabs(mx - tt)) < c.fcstol * tt;
+}
+
+// iteration `it` of the SHAKE <-> thermostat loop still running for this replica?
+__device__ bool cano_active(const DevPtrs& P, const IntConst& c, const Rep& R, int it, bool after_check,
+                            double tt) {
+  const int last = after_check ? it : it - 1;
+  for (int q = 1; q <= last; ++q) {
+    if (q == c.icslop) return false;
+    if (cano_conv(P, c, R, q, tt)) return false;
+  }
+  return true;
+}
+
+// ---- per-replica preparation: energies of this step, force scale ----------------------
+__global__ void k_prepare(DevPtrs P, IntConst c, int nrep) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nrep) return;
+  const Rep& R = P.reps[r];
+  double e[JP_MAXENE];
+  double tot = 0.0;
+  for (int k = 1; k < JP_MAXENE; ++k) {
+    e[k] = (double)P.ene_fix[r * 16 + k] * kEneInv;
+    if (k == JP_E_ELE15) e[k] += R.dself;
+    tot += e[k];
+  }
+  e[0] = tot;
+  const int h = P.step_ctr[1];
+  double* out = P.ene_hist + ((size_t)h * nrep + r) * JP_MAXENE;
+  for (int k = 0; k < JP_MAXENE; ++k) out[k] = e[k];
+  double s = 1.0;
+  if (c.method == JP_METHOD_GE && R.ge_nwin > 0) {
+    // McMD weight (verlethe.f90:196-238)
+    double dprobl;
+    if (tot <= R.ge_celw) dprobl = R.ge_alphalw;
+    else if (tot >= R.ge_ceup) dprobl = R.ge_alphaup;
+    else {
+      double rt = (tot - R.ge_celw) / (R.ge_ceup - R.ge_celw);
+      const double* cf = P.ge_coef + R.ge_off;   // per window: low, high, c0..cndeg
+      const int stride = R.ge_ndeg + 3;
+      int i = 0;
+      for (i = 0; i < R.ge_nwin; ++i)
+        if (rt < cf[i * stride + 1]) break;
+      if (i >= R.ge_nwin) i = R.ge_nwin - 1;
+      rt -= cf[i * stride + 0];
+      const double* cc = cf + i * stride + 2;
+      dprobl = cc[0];
+      for (int j = 1; j <= R.ge_ndeg; ++j) dprobl += cc[j] * pow(rt, (double)j);
+    }
+    s = (kGas / kJouCal) * 1.0e-3 * R.ge_tempce * dprobl;
+  } else if (c.psetmp > 1.0e-10) {
+    s = c.temp / c.psetmp;
+  }
+  P.scale[r] = s;
+}
+
+// ---- METHOD= MICR: verlet.f90 fused with SHAKE, one thread per unit ---------------------
+template <bool FP64>
+__global__ void __launch_bounds__(128) k_micr(DevPtrs P, IntConst c, int nunit) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double ke = 0.0;
+  int sub = -1;
+  if (t < nunit) {
+    const Unit u = P.units[t];
+    const Rep& R = P.reps[u.rep];
+    sub = u.sub;
+    const double s = P.scale[u.rep];
+    const double rt = -c.dt * kConvcv;
+    double x0[4][3], x1[4][3], vb[4][3], im[4];
+    JP_UNIT_LOOP(q) {
+      const int a = u.a[q];
+      double g[3];
+      load_grad<FP64>(P, a, s, g);
+      im[q] = P.imass[a];
+      for (int k = 0; k < 3; ++k) {
+        x0[q][k] = P.x[3 * a + k];
+        vb[q][k] = P.v[3 * a + k];
+        const double v = vb[q][k] + rt * g[k] * im[q];
+        x1[q][k] = x0[q][k] + c.dt * v;
+        P.v[3 * a + k] = v;
+      }
+    }
+    if (u.n >= 2 && c.shake_method != JP_SHAKE_NONE) {
+      const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
+      if (ier) shake_status(P, ier);
+      const double ri = 1.0 / c.dt;
+      JP_UNIT_LOOP(q)
+        for (int k = 0; k < 3; ++k) P.v[3 * u.a[q] + k] = (x1[q][k] - x0[q][k]) * ri;
+    }
+    bool bad = false;
+    JP_UNIT_LOOP(q) {
+      const int a = u.a[q];
+      double vv = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        P.x[3 * a + k] = x1[q][k];
+        const double vm = 0.5 * (vb[q][k] + P.v[3 * a + k]);
+        vv += vm * vm;
+        bad |= !isfinite(x1[q][k]);
+      }
+      ke += P.mass[a] * vv;
+      write_slot(P, a, x1[q], FP64);
+    }
+    if (bad) atomicOr(P.status, ERR_NONFINITE);
+  }
+  if (__any_sync(0xffffffffu, t < nunit)) add_kin(P, c.nsub_total, c.nkin - 1, sub, ke);
+}
+
+// ---- METHOD= CANO / GE: verlethe.f90 ----------------------------------------------------
+// phase 1 (verlethe.f90:380-398): back up x, v; velt = v - dt/2 c g/m; KE(velt) -> slot 0
+template <bool FP64>
+__global__ void __launch_bounds__(128) k_cano1(DevPtrs P, IntConst c, int nunit) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double ke = 0.0;
+  int sub = -1;
+  if (t < nunit) {
+    const Unit u = P.units[t];
+    sub = u.sub;
+    const double s = P.scale[u.rep];
+    const double rt = 0.5 * c.dt * kConvcv;
+    JP_UNIT_LOOP(q) {
+      const int a = u.a[q];
+      double g[3];
+      load_grad<FP64>(P, a, s, g);
+      const double im = P.imass[a];
+      double vv = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        const double v = P.v[3 * a + k];
+        P.x0[3 * a + k] = P.x[3 * a + k];
+        P.vback[3 * a + k] = v;
+        const double vt = v - rt * g[k] * im;
+        vv += vt * vt;
+      }
+      ke += P.mass[a] * vv;
+    }
+  }
+  if (__any_sync(0xffffffffu, t < nunit)) add_kin(P, c.nsub_total, 0, sub, ke);
+}
+
+// phase 2 (verlethe.f90:400-516): chi from slot 0; v = (2chi-1)v - chi dt c g/m; x += dt v
+template <bool FP64>
+__global__ void __launch_bounds__(128) k_cano2(DevPtrs P, IntConst c, int nunit) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nunit) return;
+  const Unit u = P.units[t];
+  const double s = P.scale[u.rep];
+  const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
+  double tempc = c.temp;
+  if (c.shake_method != JP_SHAKE_NONE) tempc = sub_temp(P, c, 0, u.sub);
+  const double chi = sqrt(tt / tempc);
+  const double a1 = chi * c.dt * kConvcv, b1 = 2.0 * chi - 1.0;
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    double g[3];
+    load_grad<FP64>(P, a, s, g);
+    const double im = P.imass[a];
+    for (int k = 0; k < 3; ++k) {
+      const double v = b1 * P.v[3 * a + k] - a1 * g[k] * im;
+      P.v[3 * a + k] = v;
+      P.x[3 * a + k] += c.dt * v;
+      P.forcec[3 * a + k] = 0.0;
+    }
+    if (c.shake_method == JP_SHAKE_NONE) write_slot(P, a, P.x + 3 * a, FP64);
+  }
+}
+
+// phase 3 of iteration `it` (verlethe.f90:524-612): SHAKE, v = (x-x0)/dt,
+// velt = (vback+v)/2, KE(velt) -> slot 2*it-1
+template <bool FP64>
+__global__ void __launch_bounds__(128) k_cano3(DevPtrs P, IntConst c, int nunit, int it) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double ke = 0.0;
+  int sub = -1;
+  if (t < nunit) {
+    const Unit u = P.units[t];
+    const Rep& R = P.reps[u.rep];
+    const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
+    if (cano_active(P, c, R, it, false, tt)) {
+      sub = u.sub;
+      double x1[4][3], x0[4][3], im[4];
+      JP_UNIT_LOOP(q) {
+        const int a = u.a[q];
+        im[q] = P.imass[a];
+        for (int k = 0; k < 3; ++k) {
+          x1[q][k] = P.x[3 * a + k];
+          x0[q][k] = P.x0[3 * a + k];
+          P.xback[3 * a + k] = x1[q][k];
+        }
+      }
+      if (u.n >= 2) {
+        const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
+        if (ier) shake_status(P, ier);
+      }
+      const double ri = 1.0 / c.dt;
+      bool bad = false;
+      JP_UNIT_LOOP(q) {
+        const int a = u.a[q];
+        double vv = 0.0;
+        for (int k = 0; k < 3; ++k) {
+          const double v = (x1[q][k] - x0[q][k]) * ri;
+          P.v[3 * a + k] = v;
+          P.x[3 * a + k] = x1[q][k];
+          const double vt = 0.5 * (P.vback[3 * a + k] + v);
+          vv += vt * vt;
+          bad |= !isfinite(x1[q][k]);
+        }
+        ke += P.mass[a] * vv;
+        write_slot(P, a, x1[q], FP64);
+      }
+      if (bad) atomicOr(P.status, ERR_NONFINITE);
+    }
+  }
+  if (__any_sync(0xffffffffu, t < nunit)) add_kin(P, c.nsub_total, 2 * it - 1, sub, ke);
+}
+
+// phase 4 (verlethe.f90:625-640): forcec += (x - xback)/dt^2; velt; KE -> slot 2*it
+template <bool FP64>
+__global__ void __launch_bounds__(128) k_cano4(DevPtrs P, IntConst c, int nunit, int it) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double ke = 0.0;
+  int sub = -1;
+  if (t < nunit) {
+    const Unit u = P.units[t];
+    const Rep& R = P.reps[u.rep];
+    const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
+    if (cano_active(P, c, R, it, true, tt)) {
+      sub = u.sub;
+      const double s = P.scale[u.rep];
+      const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
+      JP_UNIT_LOOP(q) {
+        const int a = u.a[q];
+        double g[3];
+        load_grad<FP64>(P, a, s, g);
+        const double im = P.imass[a];
+        double vv = 0.0;
+        for (int k = 0; k < 3; ++k) {
+          const int i = 3 * a + k;
+          const double fc = P.forcec[i] + r2 * (P.x[i] - P.xback[i]);
+          P.forcec[i] = fc;
+          const double vt = h * (-kConvcv * g[k] * im + fc) + P.vback[i];
+          vv += vt * vt;
+        }
+        ke += P.mass[a] * vv;
+      }
+    }
+  }
+  if (__any_sync(0xffffffffu, t < nunit)) add_kin(P, c.nsub_total, 2 * it, sub, ke);
+}
+
+// phase 5 (verlethe.f90:641-718): chi from slot 2*it; v = chi dt (-c g/m + forcec) +
+// (2chi-1) vback; x = x0 + dt v
+template <bool FP64>
+__global__ void __launch_bounds__(128) k_cano5(DevPtrs P, IntConst c, int nunit, int it) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nunit) return;
+  const Unit u = P.units[t];
+  const Rep& R = P.reps[u.rep];
+  const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
+  if (!cano_active(P, c, R, it, true, tt)) return;
+  const double s = P.scale[u.rep];
+  const double chi = sqrt(tt / sub_temp(P, c, 2 * it, u.sub));
+  const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    double g[3];
+    load_grad<FP64>(P, a, s, g);
+    const double im = P.imass[a];
+    for (int k = 0; k < 3; ++k) {
+      const int i = 3 * a + k;
+      const double v = (-kConvcv * g[k] * im + P.forcec[i]) * a1 + P.vback[i] * b1;
+      P.v[i] = v;
+      P.x[i] = P.x0[i] + c.dt * v;
+    }
+  }
+}
+
+// ---- end of step: temperatures, counters --------------------------------------------------
+__global__ void k_finish(DevPtrs P, IntConst c, int nrep) {
+  const int h = P.step_ctr[1];
+  for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
+    const Rep& R = P.reps[r];
+    int ks = c.nkin - 1;   // MICR: KE of (v(t-dt/2)+v(t+dt/2))/2
+    if (c.method != JP_METHOD_MICR && c.shake_method != JP_SHAKE_NONE) {
+      const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
+      int q = 1;
+      for (; q < c.icslop; ++q)
+        if (cano_conv(P, c, R, q, tt)) break;
+      ks = 2 * q - 1;
+    }
+    double ek = 0.0, nf = 0.0;
+    for (int s = R.sub0; s < R.sub0 + R.nsub; ++s) {
+      ek += (double)P.kin_fix[(size_t)ks * c.nsub_total + s] * kKinInv;
+      nf += P.nfr[s];
+    }
+    P.temp_hist[(size_t)h * nrep + r] = (c.method == JP_METHOD_MICR || c.shake_method != JP_SHAKE_NONE)
+                                            ? ek * 1.0e7 / (kGas * nf) : -1.0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    P.step_ctr[0] += 1;
+    P.step_ctr[1] += 1;
+  }
+}
+
+// ---- standalone SHAKE (test hook): r1 constrained against r2, positions in x / x0 -------
+__global__ void k_shake_only(DevPtrs P, IntConst c, int unit0, int nunit) {
+  const int tt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tt >= nunit) return;
+  const int t = unit0 + tt;
+  const Unit u = P.units[t];
+  if (u.n < 2) return;
+  const Rep& R = P.reps[u.rep];
+  double x1[4][3], x0[4][3], im[4];
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    im[q] = P.imass[a];
+    for (int k = 0; k < 3; ++k) {
+      x1[q][k] = P.xback[3 * a + k];
+      x0[q][k] = P.x0[3 * a + k];
+    }
+  }
+  const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
+  if (ier) shake_status(P, ier);
+  JP_UNIT_LOOP(q)
+    for (int k = 0; k < 3; ++k) P.xback[3 * u.a[q] + k] = x1[q][k];
+}
+
+void launch_prepare(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t st) {
+  k_prepare<<<(nrep + 127) / 128, 128, 0, st>>>(P, c, nrep);
+}
+
+void launch_micr(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, cudaStream_t st) {
+  const int nb = (nunit + 127) / 128;
+  if (fp64) k_micr<true><<<nb, 128, 0, st>>>(P, c, nunit);
+  else k_micr<false><<<nb, 128, 0, st>>>(P, c, nunit);
+}
+
+void launch_cano(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, cudaStream_t st) {
+  const int nb = (nunit + 127) / 128;
+  const bool shk = c.shake_method != JP_SHAKE_NONE;
+  if (fp64) {
+    if (shk) k_cano1<true><<<nb, 128, 0, st>>>(P, c, nunit);
+    k_cano2<true><<<nb, 128, 0, st>>>(P, c, nunit);
+    if (shk)
+      for (int it = 1; it <= c.icslop; ++it) {
+        k_cano3<true><<<nb, 128, 0, st>>>(P, c, nunit, it);
+        if (it < c.icslop) {
+          k_cano4<true><<<nb, 128, 0, st>>>(P, c, nunit, it);
+          k_cano5<true><<<nb, 128, 0, st>>>(P, c, nunit, it);
+        }
+      }
+  } else {
+    if (shk) k_cano1<false><<<nb, 128, 0, st>>>(P, c, nunit);
+    k_cano2<false><<<nb, 128, 0, st>>>(P, c, nunit);
+    if (shk)
+      for (int it = 1; it <= c.icslop; ++it) {
+        k_cano3<false><<<nb, 128, 0, st>>>(P, c, nunit, it);
+        if (it < c.icslop) {
+          k_cano4<false><<<nb, 128, 0, st>>>(P, c, nunit, it);
+          k_cano5<false><<<nb, 128, 0, st>>>(P, c, nunit, it);
+        }
+      }
+  }
+}
+
+void launch_finish(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t st) {
+  k_finish<<<1, 1024, 0, st>>>(P, c, nrep);
+}
+
+void launch_shake_only(const DevPtrs& P, const IntConst& c, int unit0, int nunit, cudaStream_t st) {
+  if (nunit <= 0) return;
+  k_shake_only<<<(nunit + 127) / 128, 128, 0, st>>>(P, c, unit0, nunit);
+}
+
+}  // namespace jp

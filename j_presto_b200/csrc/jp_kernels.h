@@ -1,0 +1,58 @@
+// jp_kernels.h -- kernel entry points shared between the engine's translation units.
+#pragma once
+#include "jp_common.cuh"
+
+namespace jp {
+
+// cells / tiles (jp_cells.cu)
+__global__ void k_cell_key(DevPtrs P, int natom);
+__global__ void k_scatter(DevPtrs P, int natom);
+__global__ void k_sort_bins(DevPtrs P, int nkeys);
+__global__ void k_clear_slots(DevPtrs P, int nslot, int dummy_type);
+__global__ void k_fill_slots(DevPtrs P, int natom);
+__global__ void k_block_setup(DevPtrs P, int nblk, double qscale);
+__global__ void k_fill_pos_d(DevPtrs P, int nslot, double qscale);
+__global__ void k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rlimf);
+__global__ void k_tile_emit(DevPtrs P, int nchunk);
+void scan_exclusive(const int* in, int* out, int n, int* scratch, int* total, cudaStream_t st);
+
+// ZD pair constants
+struct ZdConst {
+  double rc2, zcore, bcoeff, fcoeff;
+  int nt1;                 // LJ table stride (ntype + 1 incl. the dummy type)
+};
+
+// pair kernels (jp_pair.cu)
+void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool minimg, bool count,
+                       cudaStream_t st);
+void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, cudaStream_t st);
+void launch_update_pos(const DevPtrs& P, int nslot, bool fp64, double qscale, cudaStream_t st);
+
+// bonded (jp_bonded.cu)
+void launch_bonded(const DevPtrs& P, int nterm, bool fp64, double zb, double zf, cudaStream_t st);
+
+// integration (jp_integrate.cu)
+struct IntConst {
+  double dt;
+  double temp, temp_start;
+  int heat_loop;
+  int tempco;              // 1 whole-system, 2 per sub-system
+  int shake_method;        // 0 none, 1 exact 2-atom, 2 iterative 2-atom
+  double shake_tol;
+  int shake_maxit;
+  int icslop;
+  double fcstol;
+  double psetmp;
+  int method;
+  int nrep;
+  int nsub_total;
+  int natom;
+  int nkin;                // kinetic-sum slots; the last one is MICR's
+};
+void launch_prepare(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t st);
+void launch_micr(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, cudaStream_t st);
+void launch_cano(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, cudaStream_t st);
+void launch_finish(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t st);
+void launch_shake_only(const DevPtrs& P, const IntConst& c, int unit0, int nunit, cudaStream_t st);
+
+}  // namespace jp

@@ -1,0 +1,306 @@
+// jp_pair.cu -- zero-dipole (ZD) cut-off Coulomb + Lennard-Jones pair kernels.
+//
+// Replaces enear_ZD_{redu,high,doub}_PB (src_md_run/enear.f90:2-593, lines tagged #ZD #PB):
+//   co   = [r <= rc]                                  (enear.f90:134, sign(0.5,dd2i-irlim2)+.5)
+//   E_el += qi qj co (1/r + b r^2 - z)                 (enear.f90:138-141)
+//   E_lj += co (C12/r^12 - C6/r^6)                      (enear.f90:199-210)
+//   dE/dxi = -d [qi qj co (1/r^3 - f) + co (12 C12/r^12 - 6 C6/r^6)/r^2],  d = xi - xj
+// with q = charge * sqrt(332.06378/eps) (chgmod, inpcls.f90:215-227), b = 1/(2 rc^3),
+// f = 1/rc^3, z = 1.5/rc (incel.f90:655-658).
+//
+// Work unit: a tile = (i-block, j-block) of 32 x 32 cell-sorted atoms with an interaction
+// mask fixed at list-build time.  One warp per tile: lane l holds i-atom l; the j-atoms and
+// their force accumulators rotate one lane per step through warp shuffles, so after 32
+// steps every lane has seen every j and each j-force is back in the lane that loaded it.
+// Newton's third law: each unordered pair is evaluated once.
+//
+// Mixed path: FP32 pair arithmetic on block-local coordinates (|x| < ~10 A), forces summed
+// per tile in FP32 then added as 64-bit fixed point (2^-32 kcal/mol/A) with integer
+// atomics -- order independent, so results are bit-identical run to run.
+// FP64 path: the same tiles in FP64 with absolute coordinates and FP64 atomics.
+#include "jp_kernels.h"
+
+namespace jp {
+
+constexpr int kPairThreads = 256;
+
+__device__ __forceinline__ void flush_energy(const DevPtrs& P, int rep, double eel, double elj,
+                                             long long npair, bool count) {
+  for (int o = 16; o > 0; o >>= 1) {
+    eel += __shfl_xor_sync(0xffffffffu, eel, o);
+    elj += __shfl_xor_sync(0xffffffffu, elj, o);
+    if (count) npair += __shfl_xor_sync(0xffffffffu, npair, o);
+  }
+  if ((threadIdx.x & 31) == 0 && rep >= 0) {
+    atomic_add_ll(&P.ene_fix[rep * 16 + JP_E_ELE15], to_fix(eel, kEneScale));
+    atomic_add_ll(&P.ene_fix[rep * 16 + JP_E_VDW15], to_fix(elj, kEneScale));
+    if (count) atomicAdd(reinterpret_cast<unsigned long long*>(&P.pair_cnt[rep]),
+                         static_cast<unsigned long long>(npair));
+  }
+}
+
+template <bool MINIMG, bool COUNT>
+__global__ void __launch_bounds__(kPairThreads)
+k_pair_mixed(DevPtrs P, ZdConst z) {
+  extern __shared__ float2 s_lj[];
+  const int nlj = z.nt1 * z.nt1;
+  for (int i = threadIdx.x; i < nlj; i += blockDim.x) s_lj[i] = P.lj_f[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int T = *P.ntiles;
+  const int chunk = (T + nw - 1) / nw;
+  const int t0 = gw * chunk;
+  const int t1 = min(T, t0 + chunk);
+  if (t0 >= t1) return;
+  const float rc2 = (float)z.rc2, zb = (float)z.bcoeff, zf = (float)z.fcoeff, zc = (float)z.zcore;
+  int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
+  float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+  long long gix = 0, giy = 0, giz = 0;
+  double eel = 0.0, elj = 0.0;
+  long long npair = 0;
+  float bx = 0.f, by = 0.f, bz = 0.f, ibx = 0.f, iby = 0.f, ibz = 0.f;
+  for (int t = t0; t < t1; ++t) {
+    const int2 ij = P.tiles[t];
+    if (ij.x != cur_bi) {
+      if (ai >= 0 && (gix | giy | giz)) {
+        atomic_add_ll(&P.frc[3 * ai + 0], gix);
+        atomic_add_ll(&P.frc[3 * ai + 1], giy);
+        atomic_add_ll(&P.frc[3 * ai + 2], giz);
+      }
+      gix = giy = giz = 0;
+      cur_bi = ij.x;
+      const int s = cur_bi * kTile + lane;
+      pi = P.pos_f[s];
+      ti = P.styp[s];
+      ai = P.satom[s];
+      const int rep = P.blk_rep[cur_bi];
+      if (rep != cur_rep) {
+        if (cur_rep >= 0) flush_energy(P, cur_rep, eel, elj, npair, COUNT);
+        eel = elj = 0.0;
+        npair = 0;
+        cur_rep = rep;
+        const Rep& R = P.reps[rep];
+        bx = (float)R.box[0]; by = (float)R.box[1]; bz = (float)R.box[2];
+        ibx = (float)R.invbox[0]; iby = (float)R.invbox[1]; ibz = (float)R.invbox[2];
+      }
+    }
+    const float4 sh = P.tile_shift[t];
+    unsigned m = P.masks[(size_t)t * 32 + lane];
+    const int sj = ij.y * kTile + lane;
+    float4 pj = P.pos_f[sj];
+    int tj = P.styp[sj];
+    const float xi = pi.x + sh.x, yi = pi.y + sh.y, zi = pi.z + sh.z;
+    const int row = ti * z.nt1;
+    float gjx = 0.f, gjy = 0.f, gjz = 0.f;
+    float fix = 0.f, fiy = 0.f, fiz = 0.f;
+    float te = 0.f, tl = 0.f;
+    int tn = 0;
+#pragma unroll 4
+    for (int k = 0; k < 32; ++k) {
+      if (m & 1u) {
+        float dx = xi - pj.x, dy = yi - pj.y, dz = zi - pj.z;
+        if (MINIMG) {
+          dx -= bx * rintf(dx * ibx);
+          dy -= by * rintf(dy * iby);
+          dz -= bz * rintf(dz * ibz);
+        }
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        if (r2 <= rc2) {
+          const float rinv = rsqrtf(r2);
+          const float r2inv = rinv * rinv;
+          const float r6inv = r2inv * r2inv * r2inv;
+          const float2 lj = s_lj[row + tj];
+          const float qq = pi.w * pj.w;
+          const float v1 = lj.x * r6inv;
+          const float v2 = lj.y * r6inv * r6inv;
+          te = fmaf(qq, rinv + fmaf(zb, r2, -zc), te);
+          tl += v2 - v1;
+          const float fs = fmaf(qq, fmaf(rinv, r2inv, -zf), (12.f * v2 - 6.f * v1) * r2inv);
+          const float fx = dx * fs, fy = dy * fs, fz = dz * fs;
+          fix -= fx; fiy -= fy; fiz -= fz;
+          gjx += fx; gjy += fy; gjz += fz;
+          if (COUNT) ++tn;
+        }
+      }
+      m >>= 1;
+      const int src = (lane + 1) & 31;
+      pj.x = __shfl_sync(0xffffffffu, pj.x, src);
+      pj.y = __shfl_sync(0xffffffffu, pj.y, src);
+      pj.z = __shfl_sync(0xffffffffu, pj.z, src);
+      pj.w = __shfl_sync(0xffffffffu, pj.w, src);
+      tj = __shfl_sync(0xffffffffu, tj, src);
+      gjx = __shfl_sync(0xffffffffu, gjx, src);
+      gjy = __shfl_sync(0xffffffffu, gjy, src);
+      gjz = __shfl_sync(0xffffffffu, gjz, src);
+    }
+    const int aj = P.satom[sj];
+    if (aj >= 0 && (gjx != 0.f || gjy != 0.f || gjz != 0.f)) {
+      atomic_add_ll(&P.frc[3 * aj + 0], to_fix((double)gjx, kFrcScale));
+      atomic_add_ll(&P.frc[3 * aj + 1], to_fix((double)gjy, kFrcScale));
+      atomic_add_ll(&P.frc[3 * aj + 2], to_fix((double)gjz, kFrcScale));
+    }
+    gix += to_fix((double)fix, kFrcScale);
+    giy += to_fix((double)fiy, kFrcScale);
+    giz += to_fix((double)fiz, kFrcScale);
+    eel += (double)te;
+    elj += (double)tl;
+    if (COUNT) npair += tn;
+  }
+  if (ai >= 0 && (gix | giy | giz)) {
+    atomic_add_ll(&P.frc[3 * ai + 0], gix);
+    atomic_add_ll(&P.frc[3 * ai + 1], giy);
+    atomic_add_ll(&P.frc[3 * ai + 2], giz);
+  }
+  flush_energy(P, cur_rep, eel, elj, npair, COUNT);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kPairThreads)
+k_pair_fp64(DevPtrs P, ZdConst z) {
+  extern __shared__ double2 s_ljd[];
+  const int nlj = z.nt1 * z.nt1;
+  for (int i = threadIdx.x; i < nlj; i += blockDim.x) s_ljd[i] = P.lj_d[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int T = *P.ntiles;
+  const int chunk = (T + nw - 1) / nw;
+  const int t0 = gw * chunk;
+  const int t1 = min(T, t0 + chunk);
+  if (t0 >= t1) return;
+  const double irlim2 = 1.0 / z.rc2;
+  int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
+  double4 pi = make_double4(0, 0, 0, 0);
+  double gix = 0, giy = 0, giz = 0;
+  double eel = 0.0, elj = 0.0;
+  long long npair = 0;
+  double bx = 0, by = 0, bz = 0, ibx = 0, iby = 0, ibz = 0;
+  for (int t = t0; t < t1; ++t) {
+    const int2 ij = P.tiles[t];
+    if (ij.x != cur_bi) {
+      if (ai >= 0) {
+        atomicAdd(&P.grd[3 * ai + 0], gix);
+        atomicAdd(&P.grd[3 * ai + 1], giy);
+        atomicAdd(&P.grd[3 * ai + 2], giz);
+      }
+      gix = giy = giz = 0;
+      cur_bi = ij.x;
+      const int s = cur_bi * kTile + lane;
+      pi = P.pos_d[s];
+      ti = P.styp[s];
+      ai = P.satom[s];
+      const int rep = P.blk_rep[cur_bi];
+      if (rep != cur_rep) {
+        if (cur_rep >= 0) flush_energy(P, cur_rep, eel, elj, npair, COUNT);
+        eel = elj = 0.0;
+        npair = 0;
+        cur_rep = rep;
+        const Rep& R = P.reps[rep];
+        bx = R.box[0]; by = R.box[1]; bz = R.box[2];
+        ibx = R.invbox[0]; iby = R.invbox[1]; ibz = R.invbox[2];
+      }
+    }
+    unsigned m = P.masks[(size_t)t * 32 + lane];
+    const int sj = ij.y * kTile + lane;
+    double4 pj = P.pos_d[sj];
+    int tj = P.styp[sj];
+    const int row = ti * z.nt1;
+    double gjx = 0, gjy = 0, gjz = 0;
+    int tn = 0;
+#pragma unroll 2
+    for (int k = 0; k < 32; ++k) {
+      if (m & 1u) {
+        double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        dx -= bx * anint(dx * ibx);
+        dy -= by * anint(dy * iby);
+        dz -= bz * anint(dz * ibz);
+        const double dd2 = dx * dx + dy * dy + dz * dz;
+        const double dd2i = 1.0 / dd2;
+        if (dd2i - irlim2 >= 0.0) {
+          const double ddi = sqrt(dd2i);
+          const double dd6i = dd2i * dd2i * dd2i;
+          const double ee = pi.w * pj.w;
+          eel += ee * (ddi + z.bcoeff * dd2 - z.zcore);
+          const double2 lj = s_ljd[row + tj];
+          const double v1 = lj.x * dd6i;
+          const double v2 = lj.y * dd6i * dd6i;
+          elj += -v1 + v2;
+          const double cc = ee * (dd2i * ddi - z.fcoeff) + (-6.0 * v1 + 12.0 * v2) * dd2i;
+          const double fx = dx * cc, fy = dy * cc, fz = dz * cc;
+          gix -= fx; giy -= fy; giz -= fz;
+          gjx += fx; gjy += fy; gjz += fz;
+          if (COUNT) ++tn;
+        }
+      }
+      m >>= 1;
+      const int src = (lane + 1) & 31;
+      pj.x = __shfl_sync(0xffffffffu, pj.x, src);
+      pj.y = __shfl_sync(0xffffffffu, pj.y, src);
+      pj.z = __shfl_sync(0xffffffffu, pj.z, src);
+      pj.w = __shfl_sync(0xffffffffu, pj.w, src);
+      tj = __shfl_sync(0xffffffffu, tj, src);
+      gjx = __shfl_sync(0xffffffffu, gjx, src);
+      gjy = __shfl_sync(0xffffffffu, gjy, src);
+      gjz = __shfl_sync(0xffffffffu, gjz, src);
+    }
+    const int aj = P.satom[sj];
+    if (aj >= 0 && (gjx != 0.0 || gjy != 0.0 || gjz != 0.0)) {
+      atomicAdd(&P.grd[3 * aj + 0], gjx);
+      atomicAdd(&P.grd[3 * aj + 1], gjy);
+      atomicAdd(&P.grd[3 * aj + 2], gjz);
+    }
+    if (COUNT) npair += tn;
+  }
+  if (ai >= 0) {
+    atomicAdd(&P.grd[3 * ai + 0], gix);
+    atomicAdd(&P.grd[3 * ai + 1], giy);
+    atomicAdd(&P.grd[3 * ai + 2], giz);
+  }
+  flush_energy(P, cur_rep, eel, elj, npair, COUNT);
+}
+
+void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool minimg, bool count,
+                       cudaStream_t st) {
+  const int wpb = kPairThreads / 32;
+  const int nb = (nwarps + wpb - 1) / wpb;
+  const size_t sh = sizeof(float2) * z.nt1 * z.nt1;
+  if (minimg) {
+    if (count) k_pair_mixed<true, true><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_mixed<true, false><<<nb, kPairThreads, sh, st>>>(P, z);
+  } else {
+    if (count) k_pair_mixed<false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_mixed<false, false><<<nb, kPairThreads, sh, st>>>(P, z);
+  }
+}
+
+void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, cudaStream_t st) {
+  const int wpb = kPairThreads / 32;
+  const int nb = (nwarps + wpb - 1) / wpb;
+  const size_t sh = sizeof(double2) * z.nt1 * z.nt1;
+  if (count) k_pair_fp64<true><<<nb, kPairThreads, sh, st>>>(P, z);
+  else k_pair_fp64<false><<<nb, kPairThreads, sh, st>>>(P, z);
+}
+
+// slot positions from the master coordinates (after an external coordinate change)
+__global__ void k_update_pos(DevPtrs P, int nslot, int fp64, double qscale) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslot) return;
+  int a = P.satom[s];
+  if (a < 0) return;
+  const double x = P.x[3 * a], y = P.x[3 * a + 1], zz = P.x[3 * a + 2];
+  if (fp64) {
+    P.pos_d[s] = make_double4(x, y, zz, qscale * P.chg[a]);
+  } else {
+    P.pos_f[s] = make_float4((float)(x - P.off[3 * s]), (float)(y - P.off[3 * s + 1]),
+                             (float)(zz - P.off[3 * s + 2]), (float)(qscale * P.chg[a]));
+  }
+}
+
+void launch_update_pos(const DevPtrs& P, int nslot, bool fp64, double qscale, cudaStream_t st) {
+  k_update_pos<<<(nslot + 255) / 256, 256, 0, st>>>(P, nslot, fp64 ? 1 : 0, qscale);
+}
+
+}  // namespace jp

@@ -1,0 +1,175 @@
+"""Python host binding of libjpgpu.so (the C ABI in include/jpgpu.h).
+
+`Engine` mirrors the md_run call sites the ABI replaces: celprp -> rebuild(), dnergy ->
+energy_grad(), verlet/verlethe loop -> step(), shake_PB -> shake(), restart/monitor state
+-> get_state()/set_state().  Errors raise `JpError` carrying md_run's ier convention.
+There is no CPU fallback: without the CUDA library or a GPU the constructor raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libjpgpu.so")
+_lib = None
+
+# every symbol the header declares
+EXPORTS = ["jp_default_params", "jp_create", "jp_rebuild_cells", "jp_energy_grad", "jp_step",
+           "jp_shake", "jp_get_state", "jp_set_state", "jp_pair_count", "jp_set_timing",
+           "jp_last_timing", "jp_launch_counts", "jp_list_stats", "jp_calibrate_fp32",
+           "jp_strerror", "jp_destroy"]
+
+
+class JpError(RuntimeError):
+    def __init__(self, code, where):
+        self.code = code
+        msg = lib().jp_strerror(code).decode() if _lib is not None else str(code)
+        super().__init__(f"{where}: {msg} (code {code})")
+
+
+def lib():
+    """Load libjpgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} missing: run `python -m j_presto_b200.build` first")
+        L = C.CDLL(LIB_PATH)
+        vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.c_int32
+        L.jp_default_params.argtypes = [C.POINTER(abi.JpParams)]
+        L.jp_default_params.restype = None
+        L.jp_create.argtypes = [C.POINTER(abi.JpSystem), ip, C.POINTER(abi.JpParams), C.POINTER(vp)]
+        L.jp_rebuild_cells.argtypes = [vp, ip]
+        L.jp_energy_grad.argtypes = [vp, ip, dp, dp, dp]
+        L.jp_step.argtypes = [vp, ip, dp, dp]
+        L.jp_shake.argtypes = [vp, ip, dp, dp]
+        L.jp_get_state.argtypes = [vp, ip, dp, dp]
+        L.jp_set_state.argtypes = [vp, ip, dp, dp]
+        L.jp_pair_count.argtypes = [vp, ip, C.POINTER(C.c_int64)]
+        L.jp_set_timing.argtypes = [vp, C.c_int]
+        L.jp_last_timing.argtypes = [vp, dp, dp, C.POINTER(C.c_int32)]
+        L.jp_launch_counts.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.jp_list_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_int64)]
+        L.jp_calibrate_fp32.argtypes = [C.c_int32, C.POINTER(C.c_double)]
+        L.jp_strerror.argtypes = [C.c_int]
+        L.jp_strerror.restype = C.c_char_p
+        L.jp_destroy.argtypes = [vp]
+        L.jp_destroy.restype = None
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _chk(code, where, warn_ok=False):
+    if code < 0 or (code > 0 and not warn_ok):
+        raise JpError(code, where)
+    return code
+
+
+def calibrate_fp32(device=0):
+    """Measured FP32 FMA throughput (TFLOP/s) of the device."""
+    v = C.c_double()
+    _chk(lib().jp_calibrate_fp32(int(device), C.byref(v)), "jp_calibrate_fp32")
+    return v.value
+
+
+class Engine:
+    """A device context over one or more replicas sharing run parameters."""
+
+    def __init__(self, tops, params=None, **kw):
+        if isinstance(tops, dict):
+            tops = [tops]
+        self.tops = tops
+        self.nrep = len(tops)
+        self.natoms = [int(t["natom"]) for t in tops]
+        self.params = params if params is not None else abi.default_params(**kw)
+        self._keep = []
+        self._sys = abi.make_systems(tops, self._keep)
+        h = C.c_void_p()
+        _chk(lib().jp_create(self._sys, self.nrep, C.byref(self.params), C.byref(h)), "jp_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().jp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- state ----
+    def get_state(self, rep=0, cord=None, vel=None):
+        n = self.natoms[rep]
+        cord = np.empty((n, 3)) if cord is None else cord
+        vel = np.empty((n, 3)) if vel is None else vel
+        _chk(lib().jp_get_state(self._h, rep, _dp(cord), _dp(vel)), "jp_get_state")
+        return cord, vel
+
+    def set_state(self, rep=0, cord=None, vel=None):
+        c = None if cord is None else np.ascontiguousarray(cord, np.float64)
+        v = None if vel is None else np.ascontiguousarray(vel, np.float64)
+        _chk(lib().jp_set_state(self._h, rep, _dp(c), _dp(v)), "jp_set_state")
+
+    def rebuild(self, rep=-1):
+        _chk(lib().jp_rebuild_cells(self._h, rep), "jp_rebuild_cells")
+
+    # ---- dnergy ----
+    def energy_grad(self, rep=0, cord=None):
+        n = self.natoms[rep]
+        c = None if cord is None else np.ascontiguousarray(cord, np.float64)
+        e = np.zeros(abi.JP_MAXENE)
+        g = np.zeros((n, 3))
+        _chk(lib().jp_energy_grad(self._h, rep, _dp(c), _dp(e), _dp(g)), "jp_energy_grad")
+        return e, g
+
+    def pair_count(self, rep=0):
+        v = C.c_int64()
+        _chk(lib().jp_pair_count(self._h, rep, C.byref(v)), "jp_pair_count")
+        return v.value
+
+    # ---- runmd ----
+    def step(self, nsteps=1, energies=True, temps=True, warn_ok=False):
+        e = np.zeros((nsteps, self.nrep, abi.JP_MAXENE)) if energies else None
+        t = np.zeros((nsteps, self.nrep)) if temps else None
+        code = _chk(lib().jp_step(self._h, int(nsteps), _dp(e), _dp(t)), "jp_step", warn_ok)
+        self.last_code = code
+        return e, t
+
+    def shake(self, r1, r2, rep=0):
+        r1 = np.ascontiguousarray(r1, np.float64).copy()
+        r2 = np.ascontiguousarray(r2, np.float64)
+        code = lib().jp_shake(self._h, rep, _dp(r1), _dp(r2))
+        return code, r1
+
+    # ---- timing ----
+    def set_timing(self, on):
+        _chk(lib().jp_set_timing(self._h, 1 if on else 0), "jp_set_timing")
+
+    def last_timing(self):
+        tot = C.c_double()
+        ph = (C.c_double * 4)()
+        ln = (C.c_int32 * 4)()
+        _chk(lib().jp_last_timing(self._h, C.byref(tot), ph, ln), "jp_last_timing")
+        return tot.value, list(ph), list(ln)
+
+    def list_stats(self):
+        t, p, s = C.c_int64(), C.c_int64(), C.c_int64()
+        _chk(lib().jp_list_stats(self._h, C.byref(t), C.byref(p), C.byref(s)), "jp_list_stats")
+        return t.value, p.value, s.value
+
+    def launch_counts(self):
+        a, b = C.c_int32(), C.c_int32()
+        _chk(lib().jp_launch_counts(self._h, C.byref(a), C.byref(b)), "jp_launch_counts")
+        return a.value, b.value

@@ -1,0 +1,130 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes wrapper of the CPU FP64 oracle (oracle.cpp).
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker.
+The product path (j_presto_b200) never imports this package.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from j_presto_b200 import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(
+                os.path.join(_HERE, "oracle.cpp")):
+            build()
+        L = C.CDLL(_LIB)
+        vp, dp = C.c_void_p, C.POINTER(C.c_double)
+        L.or_create.restype = vp
+        L.or_create.argtypes = [C.POINTER(abi.JpSystem), C.POINTER(abi.JpParams), C.c_int]
+        L.or_destroy.argtypes = [vp]
+        L.or_set_state.argtypes = [vp, dp, dp]
+        L.or_get_state.argtypes = [vp, dp, dp]
+        L.or_rebuild.argtypes = [vp]
+        L.or_npairs_listed.argtypes = [vp]
+        L.or_npairs_listed.restype = C.c_longlong
+        L.or_npairs_cut.argtypes = [vp]
+        L.or_npairs_cut.restype = C.c_longlong
+        L.or_dself.argtypes = [vp]
+        L.or_dself.restype = C.c_double
+        L.or_dof.argtypes = [vp]
+        L.or_dof.restype = C.c_int
+        L.or_energy_grad.argtypes = [vp, dp, dp, dp]
+        L.or_shake.argtypes = [vp, dp, dp]
+        L.or_temperature.argtypes = [vp, dp]
+        L.or_temperature.restype = C.c_double
+        L.or_run.argtypes = [vp, C.c_int, dp, dp]
+        L.or_mcmd_scale.argtypes = [vp, C.c_double]
+        L.or_mcmd_scale.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Oracle:
+    """One replica of the reference algorithm on the host cores."""
+
+    def __init__(self, top, params=None, nthreads=0, **kw):
+        self._keep = []
+        self.top = top
+        self.n = int(top["natom"])
+        self.params = params if params is not None else abi.default_params(**kw)
+        self._sys = abi.make_system(top, self._keep)
+        self._h = lib().or_create(C.byref(self._sys), C.byref(self.params), int(nthreads))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().or_destroy(self._h)
+            self._h = None
+
+    def set_state(self, cord=None, vel=None):
+        c = None if cord is None else np.ascontiguousarray(cord, np.float64)
+        v = None if vel is None else np.ascontiguousarray(vel, np.float64)
+        lib().or_set_state(self._h, _dp(c), _dp(v))
+
+    def get_state(self):
+        c = np.empty((self.n, 3))
+        v = np.empty((self.n, 3))
+        lib().or_get_state(self._h, _dp(c), _dp(v))
+        return c, v
+
+    def rebuild(self):
+        lib().or_rebuild(self._h)
+
+    def energy_grad(self, cord=None):
+        c = None if cord is None else np.ascontiguousarray(cord, np.float64)
+        e = np.zeros(abi.JP_MAXENE)
+        g = np.zeros((self.n, 3))
+        lib().or_energy_grad(self._h, _dp(c), _dp(e), _dp(g))
+        return e, g
+
+    def shake(self, r1, r2):
+        r1 = np.ascontiguousarray(r1, np.float64).copy()
+        r2 = np.ascontiguousarray(r2, np.float64)
+        ier = lib().or_shake(self._h, _dp(r1), _dp(r2))
+        return ier, r1
+
+    def temperature(self, vel=None):
+        v = None if vel is None else np.ascontiguousarray(vel, np.float64)
+        return lib().or_temperature(self._h, _dp(v))
+
+    def run(self, nsteps):
+        e = np.zeros((nsteps, abi.JP_MAXENE))
+        t = np.zeros(nsteps)
+        ier = lib().or_run(self._h, int(nsteps), _dp(e), _dp(t))
+        return ier, e, t
+
+    @property
+    def npairs_listed(self):
+        return lib().or_npairs_listed(self._h)
+
+    @property
+    def npairs_cut(self):
+        return lib().or_npairs_cut(self._h)
+
+    @property
+    def dself(self):
+        return lib().or_dself(self._h)
+
+    @property
+    def dof(self):
+        return lib().or_dof(self._h)
+
+    def mcmd_scale(self, e):
+        return lib().or_mcmd_scale(self._h, float(e))

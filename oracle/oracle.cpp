@@ -1,0 +1,976 @@
+// oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU/OpenMP FP64 restatement of j_presto md_run's per-step force/integrate path, used as
+// the correctness oracle for the CUDA engine (tests, smoke check, bench CPU baseline).
+// It is never linked into or called by the product library.
+//
+// Every routine cites the md_run source (src_md_run/<file>:<line>) it follows.  The
+// reference itself cannot be compiled in this environment (no Fortran compiler), and the
+// reference ships no tests or golden vectors, so the oracle is pinned by hand-derived
+// known-answer tests under tests/golden/ and by analytic identities (finite-difference
+// gradients, energy conservation); see DESIGN.md "parity pinning".
+//
+// Build: oracle/Makefile -> oracle/liboracle.so (C ABI, see or_* below).
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include <array>
+#include <algorithm>
+#include <omp.h>
+
+#include "../include/jpgpu.h"
+
+namespace {
+
+// PHYCNS.f90 constants
+constexpr double kPi = 3.141592653589793;
+constexpr double kGas = 8.31451;         // gascst J/mol/K
+constexpr double kJouCal = 4.184;        // joucal
+constexpr double kEekcal = 332.06378;    // eekcal
+constexpr double kEps = 1.0e-10;         // eps
+constexpr double kConvcv = 4.184e-4;     // md.f90:56 fdcvcv
+
+inline double anint(double x) { return std::round(x); }  // Fortran anint: half away from 0
+
+struct Shake {
+  int n;            // atoms 2..4
+  int a[4];
+  double d2[6];     // squared target distances, pair order (1,2),(2,3),(3,1),(4,1),(3,4),(2,4)
+};
+
+struct Ctx {
+  // ---- topology (0-based) ----
+  int n = 0;
+  double box[3], invbox[3];
+  std::vector<double> mass, imass, chg, chgmod;
+  std::vector<int> typ, mol;
+  int ntype = 0;
+  std::vector<double> c6, c12;
+  std::vector<std::vector<int>> excl;  // sorted partner list per atom
+  struct Bond { int i, j; double k, r0; };
+  struct Angle { int i, j, k; double kf, t0; };
+  struct Tors { int a[4]; double k, nrot, phase; int div; };
+  struct P14 { int i, j; double svdw, sele; };
+  std::vector<Bond> bonds;       // active bonds (SHAKE-constrained removed)
+  std::vector<Angle> angles;     // active angles
+  std::vector<Tors> tors, imprs;
+  std::vector<P14> p14;
+  std::vector<std::array<int, 2>> excess;
+  std::vector<Shake> sk2, sk3, sk4;
+  int nconstr = 0;
+  // ---- ZD constants (incel.f90:29-39, :655-662) ----
+  double rc, rlim, rlim2, irlim2, zcore, fcoeff, bcoeff, ccoef, dself;
+  // ---- run parameters ----
+  jp_params prm;
+  jp_ge ge{};
+  std::vector<double> ge_coef, ge_low, ge_high;
+  bool has_ge = false;
+  // ---- DOF (md.f90:116-228) ----
+  int idnfre = 0;
+  int nsub = 1;
+  std::vector<double> nfrmol;   // per sub-system DOF
+  // ---- pair list: half list (j listed under i) of pairs within rlim at build ----
+  std::vector<std::vector<int>> nb;
+  // ---- state ----
+  std::vector<double> cord, vel, grad;
+  long long idloop = 0;
+  long long npair_last = 0;
+  int nthreads = 1;
+};
+
+inline void minimg(const Ctx& c, double* d) {
+  for (int k = 0; k < 3; ++k) d[k] -= c.box[k] * anint(d[k] * c.invbox[k]);
+}
+
+// ---------------------------------------------------------------------------------------
+// Pair list: every pair with r^2 <= rlim^2 (minimum image) that is not a 1-2/1-3/1-4
+// partner.  Semantics of cutatm_PB (cutoff.f90:166-505: `dd .le. rlim2`) followed by
+// the itab14 removal (cutoff.f90:50-96).  A plain cell grid replaces the reference's
+// cell hierarchy; the resulting pair SET is the same.
+// ---------------------------------------------------------------------------------------
+void build_list(Ctx& c) {
+  const int n = c.n;
+  c.nb.assign(n, {});
+  const double* x = c.cord.data();
+  int g[3];
+  for (int k = 0; k < 3; ++k) g[k] = std::max(1, (int)std::floor(c.box[k] / c.rlim));
+  const bool brute = (g[0] < 3 || g[1] < 3 || g[2] < 3);
+  std::vector<int> cellof(n), head, next(n, -1);
+  if (!brute) {
+    head.assign(g[0] * g[1] * g[2], -1);
+    for (int i = n - 1; i >= 0; --i) {
+      int ci[3];
+      for (int k = 0; k < 3; ++k) {
+        double w = x[3 * i + k] - c.box[k] * std::floor(x[3 * i + k] * c.invbox[k]);
+        int q = (int)(w / c.box[k] * g[k]);
+        if (q >= g[k]) q = g[k] - 1;
+        if (q < 0) q = 0;
+        ci[k] = q;
+      }
+      int id = (ci[2] * g[1] + ci[1]) * g[0] + ci[0];
+      cellof[i] = id;
+      next[i] = head[id];
+      head[id] = i;
+    }
+  }
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < n; ++i) {
+    std::vector<int>& L = c.nb[i];
+    auto consider = [&](int j) {
+      if (j <= i) return;
+      double d[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
+      minimg(c, d);
+      double dd = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      if (dd <= c.rlim2) {
+        if (std::binary_search(c.excl[i].begin(), c.excl[i].end(), j)) return;
+        L.push_back(j);
+      }
+    };
+    if (brute) {
+      for (int j = i + 1; j < n; ++j) consider(j);
+    } else {
+      int id = cellof[i];
+      int cx = id % g[0], cy = (id / g[0]) % g[1], cz = id / (g[0] * g[1]);
+      for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            int jx = (cx + dx + g[0]) % g[0], jy = (cy + dy + g[1]) % g[1], jz = (cz + dz + g[2]) % g[2];
+            for (int j = head[(jz * g[1] + jy) * g[0] + jx]; j >= 0; j = next[j]) consider(j);
+          }
+      std::sort(L.begin(), L.end());
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// dnergy (dnergy.f90:2-84) -> dnergv_PB (dnergv.f90:2-59): bonds, angles, torsions,
+// impropers, 1-4, then cmmdo -> enear_ZD_redu_PB (enear.f90, #ZD #REDU #PB lines).
+// ene[15] gets enevcc(:,1); grad = dE/dx.
+// ---------------------------------------------------------------------------------------
+void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
+  const int n = c.n;
+  for (int k = 0; k < JP_MAXENE; ++k) ene[k] = 0.0;
+  std::fill(grad, grad + 3 * n, 0.0);
+
+  // bonds: dnebnd_PB (dnergv.f90:65-122)
+  for (const auto& b : c.bonds) {
+    double d[3] = {x[3 * b.i] - x[3 * b.j], x[3 * b.i + 1] - x[3 * b.j + 1], x[3 * b.i + 2] - x[3 * b.j + 2]};
+    minimg(c, d);
+    double r12 = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    double dif = r12 - b.r0;
+    double coef = b.k * dif;
+    ene[JP_E_BOND] += coef * dif;
+    coef = 2.0 * coef / r12;
+    for (int k = 0; k < 3; ++k) {
+      grad[3 * b.i + k] += coef * d[k];
+      grad[3 * b.j + k] -= coef * d[k];
+    }
+  }
+  // angles: dneang_PB (dnergv.f90:128-207)
+  for (const auto& a : c.angles) {
+    double d12[3], d32[3];
+    for (int k = 0; k < 3; ++k) {
+      d12[k] = x[3 * a.i + k] - x[3 * a.j + k];
+      d32[k] = x[3 * a.k + k] - x[3 * a.j + k];
+    }
+    minimg(c, d12);
+    minimg(c, d32);
+    double r12 = d12[0] * d12[0] + d12[1] * d12[1] + d12[2] * d12[2];
+    double r32 = d32[0] * d32[0] + d32[1] * d32[1] + d32[2] * d32[2];
+    double r12r32 = std::sqrt(1.0 / (r12 * r32));
+    double cost = d12[0] * d32[0] + d12[1] * d32[1] + d12[2] * d32[2];
+    r12 = 1.0 / r12;
+    r32 = 1.0 / r32;
+    cost = std::min(cost * r12r32, 1.0);
+    cost = std::max(cost, -1.0);
+    double theta = std::acos(cost);
+    double dif = theta - a.t0;
+    double coef = a.kf * dif;
+    ene[JP_E_ANGLE] += coef * dif;
+    double sint = std::max(std::sin(theta), kEps);
+    coef = -2.0 * coef / sint;
+    double w[6];
+    double rt = cost * r12;
+    for (int k = 0; k < 3; ++k) w[k] = coef * (d32[k] * r12r32 - d12[k] * rt);
+    rt = cost * r32;
+    for (int k = 0; k < 3; ++k) w[3 + k] = coef * (d12[k] * r12r32 - d32[k] * rt);
+    for (int k = 0; k < 3; ++k) {
+      grad[3 * a.i + k] += w[k];
+      grad[3 * a.j + k] -= (w[k] + w[3 + k]);
+      grad[3 * a.k + k] += w[3 + k];
+    }
+  }
+  // torsions / impropers: dnetor_PB (dnergv.f90:223-434)
+  auto tors = [&](const std::vector<Ctx::Tors>& T, int slot) {
+    for (const auto& t : T) {
+      const int* ia = t.a;
+      double d21[3], d32[3], d43[3];
+      for (int k = 0; k < 3; ++k) {
+        d21[k] = x[3 * ia[1] + k] - x[3 * ia[0] + k];
+        d32[k] = x[3 * ia[2] + k] - x[3 * ia[1] + k];
+        d43[k] = x[3 * ia[3] + k] - x[3 * ia[2] + k];
+      }
+      minimg(c, d21);
+      minimg(c, d32);
+      minimg(c, d43);
+      double p12[3] = {d21[1] * d32[2] - d32[1] * d21[2], d21[2] * d32[0] - d32[2] * d21[0],
+                       d21[0] * d32[1] - d32[0] * d21[1]};
+      double p23[3] = {d32[1] * d43[2] - d43[1] * d32[2], d32[2] * d43[0] - d43[2] * d32[0],
+                       d32[0] * d43[1] - d43[0] * d32[1]};
+      double r12 = p12[0] * p12[0] + p12[1] * p12[1] + p12[2] * p12[2];
+      double r23 = p23[0] * p23[0] + p23[1] * p23[1] + p23[2] * p23[2];
+      double r12r23 = std::sqrt(r12 * r23);
+      if (!(r12r23 > 0.0)) continue;
+      r12r23 = 1.0 / r12r23;
+      double s1223 = p12[0] * p23[0] + p12[1] * p23[1] + p12[2] * p23[2];
+      double cosp = s1223 * r12r23;
+      if (cosp > 1.0) cosp = 1.0;
+      else if (cosp < -1.0) cosp = -1.0;
+      double p123[3] = {p12[1] * p23[2] - p23[1] * p12[2], p12[2] * p23[0] - p23[2] * p12[0],
+                        p12[0] * p23[1] - p23[0] * p12[1]};
+      double s32123 = d32[0] * p123[0] + d32[1] * p123[1] + d32[2] * p123[2];
+      double phi = std::acos(cosp);
+      if (s32123 < 0.0) phi = 2.0 * kPi - phi;
+      double phimod = t.nrot * phi + t.phase;
+      double div = 1.0 / (double)t.div;
+      ene[slot] += t.k * (1.0 + std::cos(phimod)) * div;
+      double sinp = std::sin(phi);
+      int nrot = (int)anint(t.nrot);
+      double w0 = 0.0;
+      switch (nrot) {
+        case 1: w0 = 1.0; break;
+        case 2: w0 = 2.0 * cosp; break;
+        case 3: w0 = -4.0 * sinp * sinp + 3.0; break;
+        case 4: w0 = (-8.0 * sinp * sinp + 4.0) * cosp; break;
+        case 5: w0 = (16.0 * sinp * sinp - 20.0) * sinp * sinp + 5.0; break;
+        case 6: w0 = cosp * (6.0 + 32.0 * cosp * cosp * (cosp * cosp - 1.0)); break;
+        default: w0 = 0.0;
+      }
+      w0 = std::cos(t.phase) * t.nrot * t.k * div * w0 * r12r23;
+      double w1 = d21[0] + d32[0], w2 = d21[1] + d32[1], w3 = d21[2] + d32[2];
+      double q12 = s1223 / r12, q23 = s1223 / r23;
+      double w[9];
+      w[0] = d32[2] * p23[1] - d32[1] * p23[2] - q12 * (d32[2] * p12[1] - d32[1] * p12[2]);
+      w[1] = d32[0] * p23[2] - d32[2] * p23[0] - q12 * (d32[0] * p12[2] - d32[2] * p12[0]);
+      w[2] = d32[1] * p23[0] - d32[0] * p23[1] - q12 * (d32[1] * p12[0] - d32[0] * p12[1]);
+      w[3] = -w3 * p23[1] + d43[2] * p12[1] + w2 * p23[2] - d43[1] * p12[2] -
+             q12 * (-w3 * p12[1] + w2 * p12[2]) - q23 * (d43[2] * p23[1] - d43[1] * p23[2]);
+      w[4] = w3 * p23[0] - d43[2] * p12[0] - w1 * p23[2] + d43[0] * p12[2] -
+             q12 * (w3 * p12[0] - w1 * p12[2]) - q23 * (d43[0] * p23[2] - d43[2] * p23[0]);
+      w[5] = -w2 * p23[0] + d43[1] * p12[0] + w1 * p23[1] - d43[0] * p12[1] -
+             q12 * (-w2 * p12[0] + w1 * p12[1]) - q23 * (d43[1] * p23[0] - d43[0] * p23[1]);
+      w[6] = d32[2] * p12[1] - d32[1] * p12[2] - q23 * (d32[2] * p23[1] - d32[1] * p23[2]);
+      w[7] = d32[0] * p12[2] - d32[2] * p12[0] - q23 * (d32[0] * p23[2] - d32[2] * p23[0]);
+      w[8] = d32[1] * p12[0] - d32[0] * p12[1] - q23 * (d32[1] * p23[0] - d32[0] * p23[1]);
+      for (int k = 0; k < 9; ++k) w[k] *= w0;
+      for (int k = 0; k < 3; ++k) {
+        grad[3 * ia[0] + k] += w[k];
+        grad[3 * ia[1] + k] += w[3 + k];
+        grad[3 * ia[2] + k] -= (w[k] + w[3 + k] + w[6 + k]);
+        grad[3 * ia[3] + k] += w[6 + k];
+      }
+    }
+  };
+  tors(c.tors, JP_E_TORS);
+  tors(c.imprs, JP_E_IMPR);
+  // 1-4 vdW + electrostatics: dne14_PB (dnergv.f90:440-516)
+  for (const auto& p : c.p14) {
+    double d[3] = {x[3 * p.i] - x[3 * p.j], x[3 * p.i + 1] - x[3 * p.j + 1], x[3 * p.i + 2] - x[3 * p.j + 2]};
+    minimg(c, d);
+    double r14 = 1.0 / (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    double r141 = std::sqrt(r14);
+    double r146 = r14 * r14 * r14;
+    double r1412 = r146 * r146;
+    int ti = c.typ[p.i], tj = c.typ[p.j];
+    double co6 = c.c6[ti * c.ntype + tj] * r146;
+    double co12 = c.c12[ti * c.ntype + tj] * r1412;
+    ene[JP_E_VDW14] += p.svdw * (-co6 + co12);
+    double coef = r14 * p.svdw * (-2.0 * co12 + co6) * 6.0;
+    double w[3] = {coef * d[0], coef * d[1], coef * d[2]};
+    coef = p.sele * r141;
+    ene[JP_E_ELE14] += coef;
+    coef = coef * (-r14);
+    for (int k = 0; k < 3; ++k) {
+      w[k] += coef * d[k];
+      grad[3 * p.i + k] += w[k];
+      grad[3 * p.j + k] -= w[k];
+    }
+  }
+
+  // ZD + LJ pair loop: enear_ZD_redu_PB (enear.f90:107-257, #ZD #REDU #PB lines),
+  // per-thread gradient copies stand in for the OpenMP reduction(+:Tgrad).
+  const int nt = c.nthreads;
+  std::vector<double> tg((size_t)nt * 3 * n, 0.0);
+  double eel = 0.0, evdw = 0.0;
+  long long npair = 0;
+#pragma omp parallel num_threads(nt) reduction(+ : eel, evdw, npair)
+  {
+    double* G = tg.data() + (size_t)omp_get_thread_num() * 3 * n;
+#pragma omp for schedule(dynamic, 64)
+    for (int i = 0; i < n; ++i) {
+      const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
+      const double chgi = c.chgmod[i];
+      const int it1 = c.typ[i];
+      double gwx = 0, gwy = 0, gwz = 0;
+      for (int j : c.nb[i]) {
+        double d[3] = {xi - x[3 * j], yi - x[3 * j + 1], zi - x[3 * j + 2]};
+        minimg(c, d);
+        double dd2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        double dd2i = 1.0 / dd2;
+        double co = (dd2i - c.irlim2 >= 0.0) ? 1.0 : 0.0;   // sign(0.5,dd2i-irlim2)+0.5
+        double ddi = std::sqrt(dd2i);
+        double dd6i = dd2i * dd2i * dd2i * co;
+        double ee = chgi * c.chgmod[j] * co;
+        eel += ee * (ddi + c.bcoeff * dd2 - c.zcore);
+        int it2 = c.typ[j];
+        double v1 = c.c6[it2 * c.ntype + it1] * dd6i;
+        double v2 = c.c12[it2 * c.ntype + it1] * dd6i * dd6i;
+        evdw += -v1 + v2;
+        double cc = ee * (dd2i * ddi - c.fcoeff) + (-6.0 * v1 + 12.0 * v2) * dd2i;
+        double fx = d[0] * cc, fy = d[1] * cc, fz = d[2] * cc;
+        gwx += fx; gwy += fy; gwz += fz;
+        G[3 * j] += fx; G[3 * j + 1] += fy; G[3 * j + 2] += fz;
+        npair += (co > 0.0) ? 1 : 0;
+      }
+      G[3 * i] -= gwx; G[3 * i + 1] -= gwy; G[3 * i + 2] -= gwz;
+    }
+  }
+  for (int t = 0; t < nt; ++t) {
+    const double* G = tg.data() + (size_t)t * 3 * n;
+    for (int k = 0; k < 3 * n; ++k) grad[k] += G[k];
+  }
+  c.npair_last = npair;
+  // ZD excess of excluded pairs (enear.f90:518-555) and self term (enear.f90:571)
+  double eexc = 0.0;
+  for (const auto& e : c.excess) {
+    int a = e[0], b = e[1];
+    double d[3] = {x[3 * a] - x[3 * b], x[3 * a + 1] - x[3 * b + 1], x[3 * a + 2] - x[3 * b + 2]};
+    minimg(c, d);
+    double dd2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    double cc = c.chgmod[a] * c.chgmod[b];
+    eexc += cc * c.bcoeff * dd2;
+    cc *= c.fcoeff;
+    for (int k = 0; k < 3; ++k) {
+      grad[3 * a + k] += d[k] * cc;
+      grad[3 * b + k] -= d[k] * cc;
+    }
+  }
+  ene[JP_E_VDW15] += evdw;
+  ene[JP_E_ELE15] += eel + c.dself + eexc;
+  double tot = 0.0;
+  for (int k = 1; k < JP_MAXENE; ++k) tot += ene[k];
+  ene[JP_E_TOTAL] = tot;
+}
+
+// ---------------------------------------------------------------------------------------
+// SHAKE (shake.f90): shak2e (687-755), shak2i (568-681), shake3 (113-327), shake4 (333-562)
+// Returns 0, 1 (not converged) or -2 (singular).
+// ---------------------------------------------------------------------------------------
+const int kParlis[6][2] = {{0, 1}, {1, 2}, {2, 0}, {3, 0}, {2, 3}, {1, 3}};
+
+int ludeco(double A[6][6], int n, double epsl, int* ip) {  // simulu.f90 ludeco
+  for (int k = 0; k < n; ++k) ip[k] = k;
+  for (int k = 0; k < n; ++k) {
+    int l = k;
+    double al = std::fabs(A[ip[l]][k]);
+    for (int i = k + 1; i < n; ++i)
+      if (std::fabs(A[ip[i]][k]) > al) { l = i; al = std::fabs(A[ip[l]][k]); }
+    if (l != k) std::swap(ip[k], ip[l]);
+    if (std::fabs(A[ip[k]][k]) < epsl) return -1;
+    A[ip[k]][k] = 1.0 / A[ip[k]][k];
+    for (int i = k + 1; i < n; ++i) {
+      A[ip[i]][k] *= A[ip[k]][k];
+      for (int j = k + 1; j < n; ++j) A[ip[i]][j] -= A[ip[i]][k] * A[ip[k]][j];
+    }
+  }
+  return 0;
+}
+
+int simulu(double A[6][6], int n, const double* B, double* X) {  // simulu.f90 simulu
+  int ip[6];
+  if (ludeco(A, n, kEps * kEps * kEps, ip) != 0) return -1;
+  for (int i = 0; i < n; ++i) {
+    double t = B[ip[i]];
+    for (int j = 0; j < i; ++j) t -= A[ip[i]][j] * X[j];
+    X[i] = t;
+  }
+  for (int i = n - 1; i >= 0; --i) {
+    double t = X[i];
+    for (int j = i + 1; j < n; ++j) t -= A[ip[i]][j] * X[j];
+    X[i] = t * A[ip[i]][i];
+  }
+  return 0;
+}
+
+int shake_all(Ctx& c, double* r1, const double* r2) {
+  const double tol = c.prm.shake_tol;
+  const int maxit = c.prm.shake_maxit;
+  int ier = 0;
+  auto vec = [&](const double* r, int a, int b, double* d) {
+    for (int k = 0; k < 3; ++k) d[k] = r[3 * a + k] - r[3 * b + k];
+    minimg(c, d);
+  };
+  // two-atom groups
+  if (!c.sk2.empty()) {
+    if (c.prm.shake_method == JP_SHAKE_HBON) {   // shak2e: exact quadratic
+      for (const auto& g : c.sk2) {
+        int ia = g.a[0], ja = g.a[1];
+        double im1 = c.imass[ia], im2 = c.imass[ja];
+        double i3 = im1 + im2, i4 = i3 * i3;
+        double d1[3], d2[3];
+        vec(r1, ja, ia, d1);
+        vec(r2, ja, ia, d2);
+        double d1d1 = d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2];
+        double d1d2 = d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2];
+        double d2d2 = d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2];
+        double A = i4 * d2d2, B = i3 * d1d2, C = d1d1 - g.d2[0];
+        double G = (B - std::sqrt(B * B - C * A)) / A;
+        for (int k = 0; k < 3; ++k) {
+          r1[3 * ia + k] += im1 * G * d2[k];
+          r1[3 * ja + k] -= im2 * G * d2[k];
+        }
+      }
+    } else {                                     // shak2i: iterative
+      const int ng = (int)c.sk2.size();
+      std::vector<char> ok(ng, 0);
+      std::vector<double> d2s(3 * ng);
+      for (int q = 0; q < ng; ++q) vec(r2, c.sk2[q].a[0], c.sk2[q].a[1], &d2s[3 * q]);
+      bool conv = false;
+      for (int it = 0; it < maxit && !conv; ++it) {
+        for (int q = 0; q < ng; ++q) {
+          const auto& g = c.sk2[q];
+          double im1 = c.imass[g.a[0]], im2 = c.imass[g.a[1]];
+          double i3 = 0.5 / (im1 + im2);
+          double d1[3];
+          vec(r1, g.a[0], g.a[1], d1);
+          double dif = g.d2[0] - (d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
+          double inpro = d1[0] * d2s[3 * q] + d1[1] * d2s[3 * q + 1] + d1[2] * d2s[3 * q + 2];
+          double G = (dif * i3) / inpro;
+          for (int k = 0; k < 3; ++k) {
+            r1[3 * g.a[0] + k] += im1 * G * d2s[3 * q + k];
+            r1[3 * g.a[1] + k] -= im2 * G * d2s[3 * q + k];
+          }
+        }
+        int nok = 0;
+        for (int q = 0; q < ng; ++q) {
+          if (ok[q]) { ++nok; continue; }
+          const auto& g = c.sk2[q];
+          double d1[3];
+          vec(r1, g.a[0], g.a[1], d1);
+          double dif = g.d2[0] - (d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
+          ok[q] = std::fabs(dif / g.d2[0]) < tol;
+          nok += ok[q];
+        }
+        conv = (nok == ng);
+      }
+      if (!conv) return 1;
+    }
+  }
+  // three-atom (triangle) groups: shake3 Newton with closed-form 3x3 inverse
+  int numerr = 0, notconv = 0;
+  for (const auto& g : c.sk3) {
+    const int* a = g.a;
+    double im[3] = {c.imass[a[0]], c.imass[a[1]], c.imass[a[2]]};
+    double cg[3][3] = {{im[0] + im[1], -im[1], -im[0]},
+                       {-im[1], im[1] + im[2], -im[2]},
+                       {-im[0], -im[2], im[2] + im[0]}};
+    double d1[3][3], d2[3][3];
+    vec(r1, a[0], a[1], d1[0]); vec(r1, a[1], a[2], d1[1]); vec(r1, a[2], a[0], d1[2]);
+    vec(r2, a[0], a[1], d2[0]); vec(r2, a[1], a[2], d2[1]); vec(r2, a[2], a[0], d2[2]);
+    double G[6] = {0, 0, 0, 0, 0, 0};
+    bool ok = false;
+    for (int it = 0; it < maxit; ++it) {
+      double B[3];
+      for (int q = 0; q < 3; ++q) B[q] = g.d2[q] - (d1[q][0] * d1[q][0] + d1[q][1] * d1[q][1] + d1[q][2] * d1[q][2]);
+      if (std::fabs(B[0]) < tol * g.d2[0] && std::fabs(B[1]) < tol * g.d2[1] && std::fabs(B[2]) < tol * g.d2[2]) {
+        ok = true;
+        for (int k = 0; k < 3; ++k) {
+          r1[3 * a[0] + k] += im[0] * (G[3] * d2[0][k] - G[5] * d2[2][k]);
+          r1[3 * a[1] + k] += im[1] * (-G[3] * d2[0][k] + G[4] * d2[1][k]);
+          r1[3 * a[2] + k] += im[2] * (-G[4] * d2[1][k] + G[5] * d2[2][k]);
+        }
+        break;
+      }
+      double gf[3][3];
+      for (int ig = 0; ig < 3; ++ig)
+        for (int q = 0; q < 3; ++q)
+          gf[q][ig] = 2.0 * cg[q][ig] * (d1[q][0] * d2[ig][0] + d1[q][1] * d2[ig][1] + d1[q][2] * d2[ig][2]);
+      double deta = gf[0][0] * gf[1][1] * gf[2][2] + gf[0][1] * gf[1][2] * gf[2][0] + gf[0][2] * gf[1][0] * gf[2][1] -
+                    gf[0][0] * gf[1][2] * gf[2][1] - gf[0][1] * gf[1][0] * gf[2][2] - gf[0][2] * gf[1][1] * gf[2][0];
+      if (deta == 0.0) ++numerr;
+      else deta = 1.0 / deta;
+      double db[3][3];
+      db[0][0] = gf[1][1] * gf[2][2] - gf[1][2] * gf[2][1];
+      db[0][1] = gf[2][1] * gf[0][2] - gf[2][2] * gf[0][1];
+      db[0][2] = gf[0][1] * gf[1][2] - gf[0][2] * gf[1][1];
+      db[1][0] = gf[1][2] * gf[2][0] - gf[1][0] * gf[2][2];
+      db[1][1] = gf[2][2] * gf[0][0] - gf[2][0] * gf[0][2];
+      db[1][2] = gf[0][2] * gf[1][0] - gf[0][0] * gf[1][2];
+      db[2][0] = gf[1][0] * gf[2][1] - gf[1][1] * gf[2][0];
+      db[2][1] = gf[2][0] * gf[0][1] - gf[2][1] * gf[0][0];
+      db[2][2] = gf[0][0] * gf[1][1] - gf[0][1] * gf[1][0];
+      for (int q = 0; q < 3; ++q) G[q] = deta * (db[q][0] * B[0] + db[q][1] * B[1] + db[q][2] * B[2]);
+      for (int q = 0; q < 3; ++q) G[3 + q] += G[q];
+      for (int q = 0; q < 3; ++q)
+        for (int k = 0; k < 3; ++k)
+          d1[q][k] += cg[q][0] * d2[0][k] * G[0] + cg[q][1] * d2[1][k] * G[1] + cg[q][2] * d2[2][k] * G[2];
+    }
+    if (!ok) ++notconv;
+  }
+  if (numerr) return -2;
+  if (notconv) return 1;
+  // four-atom groups: shake4 Newton + LU (simulu)
+  for (const auto& g : c.sk4) {
+    const int* a = g.a;
+    double im[4] = {c.imass[a[0]], c.imass[a[1]], c.imass[a[2]], c.imass[a[3]]};
+    const double cg[6][6] = {
+        {im[0] + im[1], -im[1], -im[0], -im[0], 0.0, -im[1]},
+        {-im[1], im[1] + im[2], -im[2], 0.0, -im[2], im[1]},
+        {-im[0], -im[2], im[2] + im[0], im[0], im[2], 0.0},
+        {-im[0], 0.0, im[0], im[3] + im[0], -im[3], -im[3]},
+        {0.0, -im[2], im[2], -im[3], im[2] + im[3], im[3]},
+        {-im[1], im[1], 0.0, -im[3], im[3], im[1] + im[3]}};
+    const int nc = 6;
+    double d1[6][3], d2[6][3], wk[6][3], G[6] = {0, 0, 0, 0, 0, 0};
+    for (int q = 0; q < nc; ++q) {
+      vec(r1, a[kParlis[q][0]], a[kParlis[q][1]], d1[q]);
+      vec(r2, a[kParlis[q][0]], a[kParlis[q][1]], d2[q]);
+      for (int k = 0; k < 3; ++k) wk[q][k] = d1[q][k];
+    }
+    bool ok = false;
+    for (int it = 0; it < maxit; ++it) {
+      double B[6];
+      bool flg = true;
+      for (int q = 0; q < nc; ++q) {
+        B[q] = g.d2[q] - (wk[q][0] * wk[q][0] + wk[q][1] * wk[q][1] + wk[q][2] * wk[q][2]);
+        if (std::fabs(B[q]) >= tol * g.d2[q]) flg = false;
+      }
+      if (flg) {
+        ok = true;
+        for (int k = 0; k < 3; ++k) {
+          r1[3 * a[0] + k] += im[0] * (G[0] * d2[0][k] - G[2] * d2[2][k] - G[3] * d2[3][k]);
+          r1[3 * a[1] + k] += im[1] * (-G[0] * d2[0][k] + G[1] * d2[1][k] + G[5] * d2[5][k]);
+          r1[3 * a[2] + k] += im[2] * (-G[1] * d2[1][k] + G[2] * d2[2][k] + G[4] * d2[4][k]);
+          r1[3 * a[3] + k] += im[3] * (G[3] * d2[3][k] - G[4] * d2[4][k] - G[5] * d2[5][k]);
+        }
+        break;
+      }
+      double gf[6][6];
+      for (int ig = 0; ig < nc; ++ig)
+        for (int q = 0; q < nc; ++q)
+          gf[q][ig] = 2.0 * cg[q][ig] * (wk[q][0] * d2[ig][0] + wk[q][1] * d2[ig][1] + wk[q][2] * d2[ig][2]);
+      for (int ig = 0; ig < nc; ++ig)
+        for (int q = 0; q < nc; ++q) B[q] += gf[q][ig] * G[ig];
+      if (simulu(gf, nc, B, G) != 0) ++numerr;
+      for (int q = 0; q < nc; ++q)
+        for (int k = 0; k < 3; ++k) wk[q][k] = d1[q][k];
+      for (int ig = 0; ig < nc; ++ig)
+        for (int q = 0; q < nc; ++q)
+          for (int k = 0; k < 3; ++k) wk[q][k] += cg[q][ig] * d2[ig][k] * G[ig];
+    }
+    if (!ok) ++notconv;
+  }
+  if (numerr) return -2;
+  if (notconv) return 1;
+  return ier;
+}
+
+// caltmp (caltmp.f90:2-48): T of the whole system from v
+double caltmp(const Ctx& c, const double* v) {
+  double ek = 0.0;
+  for (int i = 0; i < c.n; ++i)
+    ek += c.mass[i] * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+  ek *= 1.0e7;
+  return ek / (kGas * (double)c.idnfre);
+}
+
+// caltmp2 (caltmp.f90:54-110): per sub-system temperatures
+void caltmp2(const Ctx& c, const double* v, double* tf) {
+  for (int s = 0; s < c.nsub; ++s) tf[s] = 0.0;
+  for (int i = 0; i < c.n; ++i)
+    tf[c.mol[i]] += c.mass[i] * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+  for (int s = 0; s < c.nsub; ++s) tf[s] = tf[s] * 1.0e7 / (c.nfrmol[s] * kGas);
+}
+
+// McMD weight d lnP/dE at energy e (verlethe.f90:196-230), returns dew (force scale)
+double mcmd_scale(const Ctx& c, double e) {
+  const jp_ge& g = c.ge;
+  double dprobl;
+  if (e <= g.celw) dprobl = g.alphalw;
+  else if (e >= g.ceup) dprobl = g.alphaup;
+  else {
+    double rt = (e - g.celw) / (g.ceup - g.celw);
+    int i = 0;
+    for (i = 0; i < g.nwindow; ++i)
+      if (rt < c.ge_high[i]) break;
+    if (i >= g.nwindow) i = g.nwindow - 1;
+    rt -= c.ge_low[i];
+    const double* cf = &c.ge_coef[(size_t)i * (g.ndeg + 1)];
+    dprobl = cf[0];
+    for (int j = 1; j <= g.ndeg; ++j) dprobl += cf[j] * std::pow(rt, j);
+  }
+  return (kGas / kJouCal) * 1.0e-3 * g.tempce * dprobl;
+}
+
+// One verlet step (verlet.f90:2-226), METHOD= MICR (no velocity scaling, no COM stop).
+int step_verlet(Ctx& c, double* ene) {
+  const int n = c.n;
+  std::vector<double> x0(c.cord);
+  energy_grad(c, c.cord.data(), ene, c.grad.data());
+  const double dt = c.prm.dt;
+  double rt = -dt * kConvcv;
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) c.vel[3 * i + k] += rt * c.grad[3 * i + k] / c.mass[i];
+  for (int i = 0; i < 3 * n; ++i) c.cord[i] += dt * c.vel[i];
+  if (c.prm.shake_method != JP_SHAKE_NONE) {
+    int ier = shake_all(c, c.cord.data(), x0.data());
+    if (ier != 0) return ier;
+    rt = 1.0 / dt;
+    for (int i = 0; i < 3 * n; ++i) c.vel[i] = (c.cord[i] - x0[i]) * rt;
+  }
+  return 0;
+}
+
+// One verlethe step (verlethe.f90:2-758), METHOD= CANO or GE (McMD), itmeth 1 or 2,
+// with the SHAKE <-> thermostat loop (icslop) and SHAKE-failure dt halving.
+int step_verlethe(Ctx& c, double* ene) {
+  const int n = c.n;
+  const double deltt = c.prm.dt;
+  const double temps = c.prm.temp, tmpsta = c.prm.temp_start;
+  const int idhtlp = c.prm.heat_loop;
+  const double i_idhtlp = idhtlp > 0 ? 1.0 / (double)idhtlp : 0.0;
+  const long long idloop = c.idloop;
+  const bool whole = (c.prm.tempco == 1);
+  const bool shk = (c.prm.shake_method != JP_SHAKE_NONE);
+  double Tdeltt = deltt;
+  int ishk = 0, jshk = 1;
+  std::vector<double> cordm1(3 * n), velback(3 * n), velt(3 * n), cordback(3 * n), forcec(3 * n);
+  std::vector<double> tf(c.nsub), chif(c.nsub);
+  auto target_t = [&]() {
+    if (idhtlp <= 0 || idloop > idhtlp) return temps;
+    return tmpsta + ((temps - tmpsta) * i_idhtlp) * (double)idloop;
+  };
+  for (;;) {
+    cordm1 = c.cord;
+    velback = c.vel;
+  redo:
+    energy_grad(c, c.cord.data(), ene, c.grad.data());
+    if (c.prm.method == JP_METHOD_CANO) {
+      if (c.prm.psetmp > kEps) {
+        double dew = temps / c.prm.psetmp;
+        for (auto& g : c.grad) g *= dew;
+      }
+    } else if (c.prm.method == JP_METHOD_GE) {
+      double dew = mcmd_scale(c, ene[JP_E_TOTAL]);
+      for (auto& g : c.grad) g *= dew;
+    }
+    double* g = c.grad.data();
+    // velocity at 1/2 dt without SHAKE force (verlethe.f90:390-398)
+    double rt = 0.5 * Tdeltt * kConvcv;
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) velt[3 * i + k] = c.vel[3 * i + k] - rt * g[3 * i + k] * c.imass[i];
+    // temperature control (verlethe.f90:400-470)
+    const double tt = target_t();
+    if (whole) {
+      double tempc = shk ? caltmp(c, velt.data()) : temps;
+      double chi = std::sqrt(tt / tempc);
+      double a = chi * Tdeltt * kConvcv, b = 2.0 * chi - 1.0;
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) c.vel[3 * i + k] = b * c.vel[3 * i + k] - a * g[3 * i + k] * c.imass[i];
+    } else {
+      if (shk) caltmp2(c, velt.data(), tf.data());
+      else std::fill(tf.begin(), tf.end(), temps);
+      for (int s = 0; s < c.nsub; ++s) chif[s] = std::sqrt(tt / tf[s]);
+      for (int i = 0; i < n; ++i) {
+        double chi = chif[c.mol[i]];
+        double a = chi * Tdeltt * kConvcv, b = 2.0 * chi - 1.0;
+        for (int k = 0; k < 3; ++k) c.vel[3 * i + k] = b * c.vel[3 * i + k] - a * g[3 * i + k] * c.imass[i];
+      }
+    }
+    for (int i = 0; i < 3 * n; ++i) c.cord[i] += Tdeltt * c.vel[i];
+    if (shk) {
+      std::fill(forcec.begin(), forcec.end(), 0.0);
+      bool retry = false;
+      for (int numite = 1; numite <= c.prm.icslop; ++numite) {
+        cordback = c.cord;
+        int ier = shake_all(c, c.cord.data(), cordm1.data());
+        if (ier != 0) {
+          c.cord = cordm1;
+          c.vel = velback;
+          if (Tdeltt < 0.01 * deltt) return JP_E_SHAKE_ABORT;
+          jshk *= 2; ishk *= 2;
+          Tdeltt *= 0.5;
+          retry = true;
+          break;
+        }
+        double ri = 1.0 / Tdeltt;
+        for (int i = 0; i < 3 * n; ++i) {
+          c.vel[i] = (c.cord[i] - cordm1[i]) * ri;
+          velt[i] = (velback[i] + c.vel[i]) * 0.5;
+        }
+        const double tshu = target_t();
+        if (whole) {
+          double tempc = caltmp(c, velt.data());
+          if (std::fabs(tempc - tshu) < c.prm.fcstol * tshu) break;
+        } else {
+          caltmp2(c, velt.data(), tf.data());
+          double mn = *std::min_element(tf.begin(), tf.end()), mx = *std::max_element(tf.begin(), tf.end());
+          if (std::max(std::fabs(mn - tshu), std::fabs(mx - tshu)) < c.prm.fcstol * tshu) break;
+        }
+        if (numite == c.prm.icslop) break;
+        double r2 = 1.0 / (Tdeltt * Tdeltt), h = 0.5 * Tdeltt;
+        for (int i = 0; i < n; ++i)
+          for (int k = 0; k < 3; ++k) {
+            int q = 3 * i + k;
+            forcec[q] += r2 * (c.cord[q] - cordback[q]);
+            velt[q] = h * (-kConvcv * g[q] * c.imass[i] + forcec[q]) + velback[q];
+          }
+        if (whole) {
+          double tempc = caltmp(c, velt.data());
+          double chi = std::sqrt(tt / tempc);
+          double a = chi * Tdeltt, b = 2.0 * chi - 1.0;
+          for (int i = 0; i < n; ++i)
+            for (int k = 0; k < 3; ++k) {
+              int q = 3 * i + k;
+              c.vel[q] = (-kConvcv * g[q] * c.imass[i] + forcec[q]) * a + velback[q] * b;
+            }
+        } else {
+          caltmp2(c, velt.data(), tf.data());
+          for (int s = 0; s < c.nsub; ++s) chif[s] = std::sqrt(tt / tf[s]);
+          for (int i = 0; i < n; ++i) {
+            double chi = chif[c.mol[i]];
+            double a = chi * Tdeltt, b = 2.0 * chi - 1.0;
+            for (int k = 0; k < 3; ++k) {
+              int q = 3 * i + k;
+              c.vel[q] = b * velback[q] + a * (-kConvcv * g[q] * c.imass[i] + forcec[q]);
+            }
+          }
+        }
+        for (int i = 0; i < 3 * n; ++i) c.cord[i] = cordm1[i] + Tdeltt * c.vel[i];
+      }
+      if (retry) goto redo;
+    }
+    ++ishk;
+    if (ishk == jshk) break;
+    if (ishk % 2 == 0) { jshk /= 2; ishk /= 2; Tdeltt *= 2.0; }
+  }
+  return 0;
+}
+
+template <class T>
+T* arr(const T* p, size_t n, std::vector<T>& store) {
+  store.assign(p, p + n);
+  return store.data();
+}
+
+}  // namespace
+
+// =======================================================================================
+// C ABI for the Python test harness
+// =======================================================================================
+extern "C" {
+
+void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
+  Ctx* c = new Ctx();
+  const int b = s->index_base;
+  const int n = s->natom;
+  c->n = n;
+  c->prm = *prm;
+  c->nthreads = nthreads > 0 ? nthreads : omp_get_max_threads();
+  for (int k = 0; k < 3; ++k) { c->box[k] = s->box[k]; c->invbox[k] = 1.0 / s->box[k]; }
+  c->mass.assign(s->mass, s->mass + n);
+  c->imass.resize(n);
+  for (int i = 0; i < n; ++i) c->imass[i] = 1.0 / c->mass[i];   // md.f90:62-71 ifxmass
+  c->chg.assign(s->charge, s->charge + n);
+  c->typ.resize(n);
+  for (int i = 0; i < n; ++i) c->typ[i] = s->atype[i] - b;
+  c->mol.assign(n, 0);
+  if (s->molecule && prm->tempco == 2) {
+    // sub-system ids renumbered densely in order, empty ids removed (md.f90:133-151)
+    std::vector<int> ids;
+    for (int i = 0; i < n; ++i) ids.push_back(s->molecule[i] - b);
+    std::vector<int> u(ids);
+    std::sort(u.begin(), u.end());
+    u.erase(std::unique(u.begin(), u.end()), u.end());
+    for (int i = 0; i < n; ++i) c->mol[i] = (int)(std::lower_bound(u.begin(), u.end(), ids[i]) - u.begin());
+  }
+  c->ntype = s->ntype;
+  c->c6.assign(s->c6, s->c6 + (size_t)s->ntype * s->ntype);
+  c->c12.assign(s->c12, s->c12 + (size_t)s->ntype * s->ntype);
+  // exclusions (inpcls.f90:229-290 itab14)
+  c->excl.assign(n, {});
+  for (int i = 0; i < n; ++i) {
+    for (int p = s->excl_ptr[i]; p < s->excl_ptr[i + 1]; ++p) c->excl[i].push_back(s->excl_idx[p] - b);
+    std::sort(c->excl[i].begin(), c->excl[i].end());
+  }
+  // chgmod (inpcls.f90:215-227)
+  c->ccoef = kEekcal / prm->dielectric;
+  const double fac = std::sqrt(c->ccoef);
+  c->chgmod.resize(n);
+  for (int i = 0; i < n; ++i) c->chgmod[i] = fac * c->chg[i];
+  // SHAKE groups (setshk.f90 redshk: fudshk = d^2; modshk orders 2,3,4-atom groups)
+  auto pairkey = [](int a, int bb) { return a < bb ? ((long long)a << 32) | bb : ((long long)bb << 32) | a; };
+  std::vector<long long> cpairs;
+  for (int gi = 0; gi < s->nshake; ++gi) {
+    Shake g;
+    g.n = s->shake_n[gi];
+    for (int k = 0; k < 4; ++k) g.a[k] = k < g.n ? s->shake_atoms[4 * gi + k] - b : -1;
+    int nc = g.n * (g.n - 1) / 2;
+    for (int q = 0; q < 6; ++q) g.d2[q] = q < nc ? s->shake_dist[6 * gi + q] * s->shake_dist[6 * gi + q] : 0.0;
+    for (int q = 0; q < nc; ++q) cpairs.push_back(pairkey(g.a[kParlis[q][0]], g.a[kParlis[q][1]]));
+    c->nconstr += nc;
+    if (g.n == 2) c->sk2.push_back(g);
+    else if (g.n == 3) c->sk3.push_back(g);
+    else c->sk4.push_back(g);
+  }
+  std::sort(cpairs.begin(), cpairs.end());
+  const bool shk = prm->shake_method != JP_SHAKE_NONE && s->nshake > 0;
+  if (!shk) { c->sk2.clear(); c->sk3.clear(); c->sk4.clear(); c->nconstr = 0; c->prm.shake_method = JP_SHAKE_NONE; }
+  auto constrained = [&](int a, int bb) { return shk && std::binary_search(cpairs.begin(), cpairs.end(), pairkey(a, bb)); };
+  // bonds / angles, dropping SHAKE-constrained ones (setshk.f90 reabnd/reaang)
+  for (int i = 0; i < s->nbond; ++i) {
+    int a = s->bond[2 * i] - b, bb = s->bond[2 * i + 1] - b;
+    if (constrained(a, bb)) continue;
+    c->bonds.push_back({a, bb, s->bond_k[i], s->bond_r0[i]});
+  }
+  for (int i = 0; i < s->nangle; ++i) {
+    int a = s->angle[3 * i] - b, m = s->angle[3 * i + 1] - b, z = s->angle[3 * i + 2] - b;
+    if (constrained(a, z)) continue;
+    c->angles.push_back({a, m, z, s->angle_k[i], s->angle_theta0[i]});
+  }
+  for (int i = 0; i < s->ntors; ++i) {
+    Ctx::Tors t;
+    for (int k = 0; k < 4; ++k) t.a[k] = s->tors[4 * i + k] - b;
+    t.k = s->tors_k[i]; t.nrot = s->tors_nrot[i]; t.phase = s->tors_phase[i]; t.div = s->tors_div[i];
+    c->tors.push_back(t);
+    // 1-4 pairs (incel.f90:972-987, mknopm inptpl.f90:453-462, incel.f90:1084-1087)
+    if (s->tors_nbf[i] == 1) {
+      int a1 = t.a[0], a4 = t.a[3];
+      int t1 = c->typ[a1], t4 = c->typ[a4];
+      double sv = std::min(s->s14_vdw[t1], s->s14_vdw[t4]);
+      double se = std::min(s->s14_ele[t1], s->s14_ele[t4]);
+      c->p14.push_back({a1, a4, sv, se * c->ccoef * c->chg[a1] * c->chg[a4]});
+    }
+  }
+  for (int i = 0; i < s->nimpr; ++i) {
+    Ctx::Tors t;
+    for (int k = 0; k < 4; ++k) t.a[k] = s->impr[4 * i + k] - b;
+    t.k = s->impr_k[i]; t.nrot = s->impr_nrot[i]; t.phase = s->impr_phase[i]; t.div = s->impr_div[i];
+    c->imprs.push_back(t);
+  }
+  // ZD constants, dself and excess list (incel.f90:29-39, :627-689)
+  c->rc = prm->cutoff;
+  c->rlim = c->rc + 1.5;
+  c->rlim2 = c->rlim * c->rlim;
+  c->irlim2 = 1.0 / (c->rc * c->rc);
+  {
+    double rtmp = 1.0 / c->rc;
+    c->zcore = 1.5 * rtmp;
+    c->fcoeff = rtmp * rtmp * rtmp;
+    c->bcoeff = 0.5 * c->fcoeff;
+  }
+  std::vector<double> dwork(c->chg);   // self term
+  auto addx = [&](int a, int bb) {
+    dwork[a] += c->chg[bb];
+    dwork[bb] += c->chg[a];
+    c->excess.push_back({a, bb});
+  };
+  for (int i = 0; i < s->nbond; ++i) addx(s->bond[2 * i] - b, s->bond[2 * i + 1] - b);
+  for (int i = 0; i < s->nangle; ++i) addx(s->angle[3 * i] - b, s->angle[3 * i + 2] - b);
+  for (int i = 0; i < s->ntors; ++i)
+    if (s->tors_nbf[i] == 1) addx(s->tors[4 * i] - b, s->tors[4 * i + 3] - b);
+  double ds = 0.0;
+  for (int i = 0; i < n; ++i) ds += c->chg[i] * dwork[i];
+  c->dself = -c->zcore * ds * 0.5 * c->ccoef;
+  // GE weight
+  if (s->ge) {
+    c->has_ge = true;
+    c->ge = *s->ge;
+    size_t nc = (size_t)s->ge->nwindow * (s->ge->ndeg + 1);
+    c->ge_coef.assign(s->ge->coef, s->ge->coef + nc);
+    c->ge_low.assign(s->ge->low, s->ge->low + s->ge->nwindow);
+    c->ge_high.assign(s->ge->high, s->ge->high + s->ge->nwindow);
+  }
+  // DOF (md.f90:116-131, :133-183); no COM stop
+  c->idnfre = 3 * n - c->nconstr;
+  c->nsub = 1;
+  for (int i = 0; i < n; ++i) c->nsub = std::max(c->nsub, c->mol[i] + 1);
+  c->nfrmol.assign(c->nsub, 0.0);
+  for (int i = 0; i < n; ++i) c->nfrmol[c->mol[i]] += 3.0;
+  for (const auto* v : {&c->sk2, &c->sk3, &c->sk4})
+    for (const auto& g : *v) c->nfrmol[c->mol[g.a[0]]] -= (double)(g.n * (g.n - 1) / 2);
+  // state
+  c->cord.assign(s->cord, s->cord + 3 * n);
+  c->vel.assign(3 * n, 0.0);
+  if (s->vel) c->vel.assign(s->vel, s->vel + 3 * n);
+  c->grad.assign(3 * n, 0.0);
+  build_list(*c);
+  return c;
+}
+
+void or_destroy(void* h) { delete (Ctx*)h; }
+
+void or_set_state(void* h, const double* cord, const double* vel) {
+  Ctx* c = (Ctx*)h;
+  if (cord) std::memcpy(c->cord.data(), cord, sizeof(double) * 3 * c->n);
+  if (vel) std::memcpy(c->vel.data(), vel, sizeof(double) * 3 * c->n);
+}
+
+void or_get_state(void* h, double* cord, double* vel) {
+  Ctx* c = (Ctx*)h;
+  if (cord) std::memcpy(cord, c->cord.data(), sizeof(double) * 3 * c->n);
+  if (vel) std::memcpy(vel, c->vel.data(), sizeof(double) * 3 * c->n);
+}
+
+void or_rebuild(void* h) { build_list(*(Ctx*)h); }
+
+long long or_npairs_listed(void* h) {
+  Ctx* c = (Ctx*)h;
+  long long s = 0;
+  for (auto& L : c->nb) s += (long long)L.size();
+  return s;
+}
+
+long long or_npairs_cut(void* h) { return ((Ctx*)h)->npair_last; }
+
+double or_dself(void* h) { return ((Ctx*)h)->dself; }
+int or_dof(void* h) { return ((Ctx*)h)->idnfre; }
+
+int or_energy_grad(void* h, const double* cord, double* ene, double* grad) {
+  Ctx* c = (Ctx*)h;
+  if (cord) std::memcpy(c->cord.data(), cord, sizeof(double) * 3 * c->n);
+  energy_grad(*c, c->cord.data(), ene, grad);
+  return 0;
+}
+
+int or_shake(void* h, double* r1, const double* r2) { return shake_all(*(Ctx*)h, r1, r2); }
+
+double or_temperature(void* h, const double* v) {
+  Ctx* c = (Ctx*)h;
+  return caltmp(*c, v ? v : c->vel.data());
+}
+
+// nsteps of runmd (md.f90:519-694): verlet or verlethe, then celprp every UPDATE steps.
+int or_run(void* h, int nsteps, double* ene_out, double* temp_out) {
+  Ctx* c = (Ctx*)h;
+  double ene[JP_MAXENE];
+  for (int s = 0; s < nsteps; ++s) {
+    c->idloop += 1;
+    int ier;
+    if (c->prm.method == JP_METHOD_MICR) ier = step_verlet(*c, ene);
+    else ier = step_verlethe(*c, ene);
+    if (ier != 0) return ier;
+    if (ene_out) std::memcpy(ene_out + (size_t)s * JP_MAXENE, ene, sizeof(ene));
+    if (temp_out) temp_out[s] = caltmp(*c, c->vel.data());
+    if (c->prm.update > 0 && c->idloop % c->prm.update == 0) build_list(*c);
+  }
+  return 0;
+}
+
+double or_mcmd_scale(void* h, double e) { return mcmd_scale(*(Ctx*)h, e); }
+
+}  // extern "C"
