@@ -51,6 +51,7 @@ struct jp_ctx {
   bool fp64 = false;
   bool minimg = true;
   int pair_warps = 0;
+  int cano_grid = 1;
   int hist_cap = 1024;
   long long idloop = 0;
   cudaStream_t st = nullptr;
@@ -124,6 +125,7 @@ void enqueue_rebuild(jp_ctx *c) {
   k_sort_bins<<<(c->nkeys + nt - 1) / nt, nt, 0, st>>>(P, c->nkeys);
   k_clear_slots<<<(c->nslot + nt - 1) / nt, nt, 0, st>>>(P, c->nslot, c->zc.nt1 - 1);
   k_fill_slots<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
+  k_excl_slots<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
   k_block_setup<<<(c->nblk * 32 + nt - 1) / nt, nt, 0, st>>>(P, c->nblk, c->qscale);
   if (c->fp64) k_fill_pos_d<<<(c->nslot + nt - 1) / nt, nt, 0, st>>>(P, c->nslot, c->qscale);
   const double rlim = c->prm.cutoff + 1.5;
@@ -131,7 +133,7 @@ void enqueue_rebuild(jp_ctx *c) {
   k_tile_scan_chunks<<<nwb, 128, 0, st>>>(P, c->nchunk, rlim * rlim, (float)rlim);
   scan_exclusive(P.chunk_cnt, P.chunk_off, c->nchunk + 1, c->scan_scratch, P.ntiles, st);
   k_tile_emit<<<nwb, 128, 0, st>>>(P, c->nchunk);
-  c->launches_rebuild = 14 + (c->fp64 ? 1 : 0);
+  c->launches_rebuild = 15 + (c->fp64 ? 1 : 0);
 }
 
 // ---- one MD step ------------------------------------------------------------------------
@@ -163,7 +165,7 @@ void enqueue_integrate(jp_ctx *c) {
   cudaMemsetAsync(P.kin_fix, 0, sizeof(long long) * c->nkin * c->nsub, c->st);
   launch_prepare(P, c->ic, c->nrep, c->st);
   if (c->prm.method == JP_METHOD_MICR) launch_micr(P, c->ic, c->nunit, c->fp64, c->st);
-  else launch_cano(P, c->ic, c->nunit, c->fp64, c->st);
+  else launch_cano(P, c->ic, c->nunit, c->fp64, c->cano_grid, c->st);
   launch_finish(P, c->ic, c->nrep, c->st);
 }
 
@@ -171,11 +173,7 @@ int launches_per_step(const jp_ctx *c) {
   int n = 1;                       // pair
   n += c->nterm > 0 ? 1 : 0;      // bonded
   n += 2;                          // prepare + finish
-  if (c->prm.method == JP_METHOD_MICR) n += 1;
-  else {
-    const bool shk = c->prm.shake_method != JP_SHAKE_NONE;
-    n += 1 + (shk ? 1 + c->prm.icslop + 2 * (c->prm.icslop - 1) : 0);
-  }
+  n += 1;                          // k_micr or the fused cooperative CANO/GE kernel
   return n;
 }
 
@@ -200,6 +198,7 @@ int check_status(jp_ctx *c) {
   CK(cudaMemcpy(&s, c->P.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
   if (s == 0) return JP_OK;
   CK(cudaMemset(c->P.status, 0, sizeof(unsigned)));
+  if (s & ERR_TIMEOUT) return JP_E_TIMEOUT;
   if (s & ERR_LIST_OVERFLOW) return JP_E_LIST_OVERFLOW;
   if (s & ERR_NONFINITE) return JP_E_NONFINITE;
   if (s & ERR_FIX_OVERFLOW) return JP_E_FIXED_OVERFLOW;
@@ -442,7 +441,9 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
         u.sub = sub0 + mol[i];
         ru.push_back(u);
       }
-    std::stable_sort(ru.begin(), ru.end(), [](const Unit &x, const Unit &y) { return x.sub < y.sub; });
+    std::stable_sort(ru.begin(), ru.end(), [](const Unit &x, const Unit &y) {
+      return x.sub != y.sub ? x.sub < y.sub : x.n < y.n;   // warps uniform in sub-system and group size
+    });
     R.unit0 = (int)units.size();
     R.nunit = (int)ru.size();
     units.insert(units.end(), ru.begin(), ru.end());
@@ -591,6 +592,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.grd, 3 * (size_t)N);
   e |= dput(c, &P.excl_ptr, hexp);
   e |= dput(c, &P.excl_idx, hexi);
+  e |= dalloc(c, &P.excl_slot, hexi.size());
   e |= dalloc(c, &P.pos_f, (size_t)c->nslot);
   e |= dalloc(c, &P.pos_d, (size_t)c->nslot);
   e |= dalloc(c, &P.off, 3 * (size_t)c->nslot);
@@ -625,6 +627,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.scale, (size_t)nrep);
   e |= dalloc(c, &P.done, (size_t)nrep);
   e |= dalloc(c, &P.status, 1);
+  e |= dalloc(c, &P.bar, 4);
   e |= dalloc(c, &P.pair_cnt, (size_t)nrep);
   e |= dalloc(c, &P.ene_hist, (size_t)c->hist_cap * nrep * JP_MAXENE);
   e |= dalloc(c, &P.temp_hist, (size_t)c->hist_cap * nrep);
@@ -660,6 +663,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   c->pair_warps = std::max(1, nsm) * 8 * 6;   // 6 blocks of 8 warps per SM
+  c->cano_grid = cano_grid(c->fp64, c->device);
   CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   CK(cudaEventCreate(&c->ev_a));
   CK(cudaEventCreate(&c->ev_b));

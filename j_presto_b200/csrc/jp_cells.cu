@@ -147,18 +147,22 @@ __global__ void k_fill_pos_d(DevPtrs P, int nslot, double qscale) {
   else P.pos_d[s] = make_double4(0.0, 0.0, 0.0, 0.0);
 }
 
-__device__ __forceinline__ bool excluded(const DevPtrs& P, int ai, int aj) {
-  int b = P.excl_ptr[ai], e = P.excl_ptr[ai + 1];
-  for (int p = b; p < e; ++p)
-    if (P.excl_idx[p] == aj) return true;
-  return false;
+// slot of every exclusion partner, refreshed after each sort: lets the tile build clear
+// excluded pairs per partner instead of searching the partner list per pair
+__global__ void k_excl_slots(DevPtrs P, int natom) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natom) return;
+  for (int p = P.excl_ptr[a]; p < P.excl_ptr[a + 1]; ++p) P.excl_slot[p] = P.slot_of[P.excl_idx[p]];
 }
+
+constexpr int kExclReg = 8;   // exclusion partners held in registers per i-atom
 
 // Tile list, pass A: one warp per chunk = (i-block, 32 consecutive candidate j-blocks
 // starting at j0 >= i, same replica).  Bounding-box test of the 32 candidates at once, then
 // for each survivor the exact mask; non-empty masks go to the chunk's scratch slots.
 __device__ __forceinline__ unsigned tile_mask(const DevPtrs& P, const Rep& R, int bi, int bj, int lane,
-                                              int ai, double xi, double yi, double zi, bool iexcl,
+                                              int ai, double xi, double yi, double zi,
+                                              const int (&ps)[kExclReg], int pb, int pe,
                                               double rlim2) {
   const int aj = P.satom[bj * kTile + lane];
   double xj = 0, yj = 0, zj = 0;
@@ -176,9 +180,17 @@ __device__ __forceinline__ unsigned tile_mask(const DevPtrs& P, const Rep& R, in
     dx -= R.box[0] * anint(dx * R.invbox[0]);
     dy -= R.box[1] * anint(dy * R.invbox[1]);
     dz -= R.box[2] * anint(dz * R.invbox[2]);
-    if (dx * dx + dy * dy + dz * dz <= rlim2) {
-      if (iexcl && excluded(P, ai, ak)) continue;
-      mask |= 1u << k;
+    if (dx * dx + dy * dy + dz * dz <= rlim2) mask |= 1u << k;
+  }
+  // 1-2/1-3/1-4 partners of the i-atom that sit in block bj: lane l sees slot
+  // bj*32 + ((l+k)&31) at bit k
+  if (mask) {
+#pragma unroll
+    for (int q = 0; q < kExclReg; ++q)
+      if ((ps[q] >> 5) == bj) mask &= ~(1u << (((ps[q] & 31) - lane) & 31));
+    for (int p = pb + kExclReg; p < pe; ++p) {
+      const int sp = P.excl_slot[p];
+      if ((sp >> 5) == bj) mask &= ~(1u << (((sp & 31) - lane) & 31));
     }
   }
   return mask;
@@ -210,12 +222,19 @@ __global__ void k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rl
   if (ball) {
     const int ai = P.satom[bi * kTile + lane];
     double xi = 0, yi = 0, zi = 0;
-    if (ai >= 0) { xi = P.x[3 * ai]; yi = P.x[3 * ai + 1]; zi = P.x[3 * ai + 2]; }
-    const bool iexcl = ai >= 0 && P.excl_ptr[ai + 1] > P.excl_ptr[ai];
+    int pb = 0, pe = 0;
+    int ps[kExclReg];
+    if (ai >= 0) {
+      xi = P.x[3 * ai]; yi = P.x[3 * ai + 1]; zi = P.x[3 * ai + 2];
+      pb = P.excl_ptr[ai];
+      pe = P.excl_ptr[ai + 1];
+    }
+#pragma unroll
+    for (int q = 0; q < kExclReg; ++q) ps[q] = pb + q < pe ? P.excl_slot[pb + q] : -64;
     while (ball) {
       const int b = __ffs(ball) - 1;
       ball &= ball - 1;
-      const unsigned m = tile_mask(P, R, bi, j0 + b, lane, ai, xi, yi, zi, iexcl, rlim2);
+      const unsigned m = tile_mask(P, R, bi, j0 + b, lane, ai, xi, yi, zi, ps, pb, pe, rlim2);
       if (__any_sync(0xffffffffu, m != 0)) {
         P.tmp_masks[((size_t)w * 32 + b) * 32 + lane] = m;
         nz |= 1u << b;

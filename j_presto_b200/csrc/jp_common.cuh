@@ -36,7 +36,7 @@ constexpr double kJouCal = 4.184;
 // error bits of the device status word
 enum : unsigned {
   ERR_SHAKE_NOCONV = 1u, ERR_SHAKE_SINGULAR = 2u, ERR_NONFINITE = 4u,
-  ERR_FIX_OVERFLOW = 8u, ERR_LIST_OVERFLOW = 16u, ERR_SORT = 32u
+  ERR_FIX_OVERFLOW = 8u, ERR_LIST_OVERFLOW = 16u, ERR_SORT = 32u, ERR_TIMEOUT = 64u
 };
 
 // per-replica constants
@@ -83,6 +83,7 @@ struct DevPtrs {
   double *grd;
   // exclusions (global atom ids)
   int *excl_ptr, *excl_idx;
+  int *excl_slot;                 // slot of each partner after the last sort
   // slots / blocks
   float4 *pos_f;
   double4 *pos_d;
@@ -118,6 +119,7 @@ struct DevPtrs {
   double *scale;                  // per replica force scale (GE / pseudo-T)
   int *done;                      // per replica SHAKE-thermostat loop finished
   unsigned *status;               // error bits
+  unsigned *bar;                  // grid barrier of the cooperative integrator [4]
   long long *pair_cnt;            // [nrep]
   double *ene_hist;               // [max_steps][nrep][15]
   double *temp_hist;              // [max_steps][nrep]

@@ -30,6 +30,10 @@ __device__ __forceinline__ void load_grad(const DevPtrs& P, int a, double s, dou
   }
 }
 
+__host__ __device__ __noinline__ int shake_group4(const Rep& R, const Unit& u, const double* im,
+                                                 double r1[4][3], const double r2[4][3],
+                                                 double tol, int maxit);
+
 // ---- SHAKE on one group (r1 constrained against reference r2) --------------------------
 // returns 0 converged, 1 not converged, -2 singular
 __host__ __device__ int shake_group(const Rep& R, const Unit& u, const double* im, double r1[4][3],
@@ -128,7 +132,15 @@ __host__ __device__ int shake_group(const Rep& R, const Unit& u, const double* i
     }
     return singular ? -2 : 1;
   }
-  // n == 4: shake4 (shake.f90:333-562): Newton with LU (simulu.f90)
+  return shake_group4(R, u, im, r1, r2, tol, maxit);
+}
+
+// n == 4: shake4 (shake.f90:333-562): Newton with LU (simulu.f90).  Kept out of line: only
+// X-H3 groups take it, and inlining its 6x6 system would raise the register demand of every
+// integration kernel.
+__host__ __device__ __noinline__ int shake_group4(const Rep& R, const Unit& u, const double* im,
+                                                 double r1[4][3], const double r2[4][3],
+                                                 double tol, int maxit) {
   const double cg[6][6] = {
       {im[0] + im[1], -im[1], -im[0], -im[0], 0.0, -im[1]},
       {-im[1], im[1] + im[2], -im[2], 0.0, -im[2], im[1]},
@@ -249,7 +261,9 @@ __device__ __forceinline__ double target_temp(const IntConst& c, long long idloo
 }
 
 __device__ __forceinline__ double sub_temp(const DevPtrs& P, const IntConst& c, int kslot, int sub) {
-  const double ek = (double)P.kin_fix[(size_t)kslot * c.nsub_total + sub] * kKinInv;
+  // L2-coherent load: inside the cooperative kernel other blocks wrote this sum before the
+  // last grid barrier, and L1 may still hold the line from an earlier phase
+  const double ek = (double)__ldcg(&P.kin_fix[(size_t)kslot * c.nsub_total + sub]) * kKinInv;
   return ek * 1.0e7 / (kGas * P.nfr[sub]);
 }
 
@@ -321,7 +335,7 @@ __global__ void k_prepare(DevPtrs P, IntConst c, int nrep) {
 
 // ---- METHOD= MICR: verlet.f90 fused with SHAKE, one thread per unit ---------------------
 template <bool FP64>
-__global__ void __launch_bounds__(128) k_micr(DevPtrs P, IntConst c, int nunit) {
+__global__ void __launch_bounds__(64) k_micr(DevPtrs P, IntConst c, int nunit) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double ke = 0.0;
   int sub = -1;
@@ -371,44 +385,38 @@ __global__ void __launch_bounds__(128) k_micr(DevPtrs P, IntConst c, int nunit) 
 }
 
 // ---- METHOD= CANO / GE: verlethe.f90 ----------------------------------------------------
+// The step's phases are device functions over one unit; k_cano_fused runs them in one
+// cooperative launch, separated by grid barriers where a phase needs the kinetic-energy
+// sums of the previous one.
+
 // phase 1 (verlethe.f90:380-398): back up x, v; velt = v - dt/2 c g/m; KE(velt) -> slot 0
 template <bool FP64>
-__global__ void __launch_bounds__(128) k_cano1(DevPtrs P, IntConst c, int nunit) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ double cano1_unit(const DevPtrs& P, const IntConst& c, const Unit& u) {
+  const double s = P.scale[u.rep];
+  const double rt = 0.5 * c.dt * kConvcv;
   double ke = 0.0;
-  int sub = -1;
-  if (t < nunit) {
-    const Unit u = P.units[t];
-    sub = u.sub;
-    const double s = P.scale[u.rep];
-    const double rt = 0.5 * c.dt * kConvcv;
-    JP_UNIT_LOOP(q) {
-      const int a = u.a[q];
-      double g[3];
-      load_grad<FP64>(P, a, s, g);
-      const double im = P.imass[a];
-      double vv = 0.0;
-      for (int k = 0; k < 3; ++k) {
-        const double v = P.v[3 * a + k];
-        P.x0[3 * a + k] = P.x[3 * a + k];
-        P.vback[3 * a + k] = v;
-        const double vt = v - rt * g[k] * im;
-        vv += vt * vt;
-      }
-      ke += P.mass[a] * vv;
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    double g[3];
+    load_grad<FP64>(P, a, s, g);
+    const double im = P.imass[a];
+    double vv = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const double v = P.v[3 * a + k];
+      P.x0[3 * a + k] = P.x[3 * a + k];
+      P.vback[3 * a + k] = v;
+      const double vt = v - rt * g[k] * im;
+      vv += vt * vt;
     }
+    ke += P.mass[a] * vv;
   }
-  if (__any_sync(0xffffffffu, t < nunit)) add_kin(P, c.nsub_total, 0, sub, ke);
+  return ke;
 }
 
 // phase 2 (verlethe.f90:400-516): chi from slot 0; v = (2chi-1)v - chi dt c g/m; x += dt v
 template <bool FP64>
-__global__ void __launch_bounds__(128) k_cano2(DevPtrs P, IntConst c, int nunit) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nunit) return;
-  const Unit u = P.units[t];
+__device__ __forceinline__ void cano2_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double tt) {
   const double s = P.scale[u.rep];
-  const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
   double tempc = c.temp;
   if (c.shake_method != JP_SHAKE_NONE) tempc = sub_temp(P, c, 0, u.sub);
   const double chi = sqrt(tt / tempc);
@@ -431,96 +439,72 @@ __global__ void __launch_bounds__(128) k_cano2(DevPtrs P, IntConst c, int nunit)
 // phase 3 of iteration `it` (verlethe.f90:524-612): SHAKE, v = (x-x0)/dt,
 // velt = (vback+v)/2, KE(velt) -> slot 2*it-1
 template <bool FP64>
-__global__ void __launch_bounds__(128) k_cano3(DevPtrs P, IntConst c, int nunit, int it) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  double ke = 0.0;
-  int sub = -1;
-  if (t < nunit) {
-    const Unit u = P.units[t];
-    const Rep& R = P.reps[u.rep];
-    const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
-    if (cano_active(P, c, R, it, false, tt)) {
-      sub = u.sub;
-      double x1[4][3], x0[4][3], im[4];
-      JP_UNIT_LOOP(q) {
-        const int a = u.a[q];
-        im[q] = P.imass[a];
-        for (int k = 0; k < 3; ++k) {
-          x1[q][k] = P.x[3 * a + k];
-          x0[q][k] = P.x0[3 * a + k];
-          P.xback[3 * a + k] = x1[q][k];
-        }
-      }
-      if (u.n >= 2) {
-        const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
-        if (ier) shake_status(P, ier);
-      }
-      const double ri = 1.0 / c.dt;
-      bool bad = false;
-      JP_UNIT_LOOP(q) {
-        const int a = u.a[q];
-        double vv = 0.0;
-        for (int k = 0; k < 3; ++k) {
-          const double v = (x1[q][k] - x0[q][k]) * ri;
-          P.v[3 * a + k] = v;
-          P.x[3 * a + k] = x1[q][k];
-          const double vt = 0.5 * (P.vback[3 * a + k] + v);
-          vv += vt * vt;
-          bad |= !isfinite(x1[q][k]);
-        }
-        ke += P.mass[a] * vv;
-        write_slot(P, a, x1[q], FP64);
-      }
-      if (bad) atomicOr(P.status, ERR_NONFINITE);
+__device__ __forceinline__ double cano3_unit(const DevPtrs& P, const IntConst& c, const Unit& u) {
+  const Rep& R = P.reps[u.rep];
+  double x1[4][3], x0[4][3], im[4];
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    im[q] = P.imass[a];
+    for (int k = 0; k < 3; ++k) {
+      x1[q][k] = P.x[3 * a + k];
+      x0[q][k] = P.x0[3 * a + k];
+      P.xback[3 * a + k] = x1[q][k];
     }
   }
-  if (__any_sync(0xffffffffu, t < nunit)) add_kin(P, c.nsub_total, 2 * it - 1, sub, ke);
+  if (u.n >= 2) {
+    const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
+    if (ier) shake_status(P, ier);
+  }
+  const double ri = 1.0 / c.dt;
+  bool bad = false;
+  double ke = 0.0;
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    double vv = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const double v = (x1[q][k] - x0[q][k]) * ri;
+      P.v[3 * a + k] = v;
+      P.x[3 * a + k] = x1[q][k];
+      const double vt = 0.5 * (P.vback[3 * a + k] + v);
+      vv += vt * vt;
+      bad |= !isfinite(x1[q][k]);
+    }
+    ke += P.mass[a] * vv;
+    write_slot(P, a, x1[q], FP64);
+  }
+  if (bad) atomicOr(P.status, ERR_NONFINITE);
+  return ke;
 }
 
 // phase 4 (verlethe.f90:625-640): forcec += (x - xback)/dt^2; velt; KE -> slot 2*it
 template <bool FP64>
-__global__ void __launch_bounds__(128) k_cano4(DevPtrs P, IntConst c, int nunit, int it) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ double cano4_unit(const DevPtrs& P, const IntConst& c, const Unit& u) {
+  const double s = P.scale[u.rep];
+  const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
   double ke = 0.0;
-  int sub = -1;
-  if (t < nunit) {
-    const Unit u = P.units[t];
-    const Rep& R = P.reps[u.rep];
-    const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
-    if (cano_active(P, c, R, it, true, tt)) {
-      sub = u.sub;
-      const double s = P.scale[u.rep];
-      const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
-      JP_UNIT_LOOP(q) {
-        const int a = u.a[q];
-        double g[3];
-        load_grad<FP64>(P, a, s, g);
-        const double im = P.imass[a];
-        double vv = 0.0;
-        for (int k = 0; k < 3; ++k) {
-          const int i = 3 * a + k;
-          const double fc = P.forcec[i] + r2 * (P.x[i] - P.xback[i]);
-          P.forcec[i] = fc;
-          const double vt = h * (-kConvcv * g[k] * im + fc) + P.vback[i];
-          vv += vt * vt;
-        }
-        ke += P.mass[a] * vv;
-      }
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    double g[3];
+    load_grad<FP64>(P, a, s, g);
+    const double im = P.imass[a];
+    double vv = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const int i = 3 * a + k;
+      const double fc = P.forcec[i] + r2 * (P.x[i] - P.xback[i]);
+      P.forcec[i] = fc;
+      const double vt = h * (-kConvcv * g[k] * im + fc) + P.vback[i];
+      vv += vt * vt;
     }
+    ke += P.mass[a] * vv;
   }
-  if (__any_sync(0xffffffffu, t < nunit)) add_kin(P, c.nsub_total, 2 * it, sub, ke);
+  return ke;
 }
 
 // phase 5 (verlethe.f90:641-718): chi from slot 2*it; v = chi dt (-c g/m + forcec) +
 // (2chi-1) vback; x = x0 + dt v
 template <bool FP64>
-__global__ void __launch_bounds__(128) k_cano5(DevPtrs P, IntConst c, int nunit, int it) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nunit) return;
-  const Unit u = P.units[t];
-  const Rep& R = P.reps[u.rep];
-  const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
-  if (!cano_active(P, c, R, it, true, tt)) return;
+__device__ __forceinline__ void cano5_unit(const DevPtrs& P, const IntConst& c, const Unit& u, int it,
+                                           double tt) {
   const double s = P.scale[u.rep];
   const double chi = sqrt(tt / sub_temp(P, c, 2 * it, u.sub));
   const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
@@ -534,6 +518,116 @@ __global__ void __launch_bounds__(128) k_cano5(DevPtrs P, IntConst c, int nunit,
       const double v = (-kConvcv * g[k] * im + P.forcec[i]) * a1 + P.vback[i] * b1;
       P.v[i] = v;
       P.x[i] = P.x0[i] + c.dt * v;
+    }
+  }
+}
+
+// Grid barrier for a cooperative launch (all blocks co-resident).  bar[0] arrivals,
+// bar[1] generation, bar[2] abort.  The wait is bounded (~1 s of SM clock): on timeout the
+// kernel records ERR_TIMEOUT, raises abort and every block returns at its next barrier.
+constexpr long long kBarrierCycles = 2000000000LL;
+
+__device__ __forceinline__ bool grid_barrier(const DevPtrs& P) {
+  __shared__ int s_ok;
+  unsigned* bar = P.bar;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    volatile unsigned* vb = bar;
+    const unsigned gen = vb[1];
+    __threadfence();
+    if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+      atomicExch(&bar[0], 0u);
+      __threadfence();
+      atomicAdd(&bar[1], 1u);
+    } else {
+      const long long t0 = clock64();
+      while (vb[1] == gen) {
+        if (vb[2] != 0u) { ok = 0; break; }
+        if (clock64() - t0 > kBarrierCycles) {
+          atomicOr(P.status, ERR_TIMEOUT);
+          atomicExch(&bar[2], 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// the whole SHAKE <-> thermostat step of verlethe for all replicas, one launch
+template <bool FP64>
+__global__ void __launch_bounds__(64) k_cano_fused(DevPtrs P, IntConst c, int nunit) {
+  const int nthr = gridDim.x * blockDim.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
+  const bool shk = c.shake_method != JP_SHAKE_NONE;
+  if (shk) {
+    for (int base = 0; base < nunit; base += nthr) {
+      const int t = base + gt;
+      double ke = 0.0;
+      int sub = -1;
+      if (t < nunit) {
+        const Unit u = P.units[t];
+        sub = u.sub;
+        ke = cano1_unit<FP64>(P, c, u);
+      }
+      add_kin(P, c.nsub_total, 0, sub, ke);
+    }
+    if (!grid_barrier(P)) return;
+  }
+  // phase 2, fused with phase 3 of the first iteration (both thread-local)
+  for (int base = 0; base < nunit; base += nthr) {
+    const int t = base + gt;
+    double ke = 0.0;
+    int sub = -1;
+    if (t < nunit) {
+      const Unit u = P.units[t];
+      cano2_unit<FP64>(P, c, u, tt);
+      if (shk) {
+        sub = u.sub;
+        ke = cano3_unit<FP64>(P, c, u);
+      }
+    }
+    if (shk) add_kin(P, c.nsub_total, 1, sub, ke);
+  }
+  if (!shk) return;
+  for (int it = 1; it < c.icslop; ++it) {
+    if (!grid_barrier(P)) return;
+    // phase 4 of `it` for replicas still iterating
+    for (int base = 0; base < nunit; base += nthr) {
+      const int t = base + gt;
+      double ke = 0.0;
+      int sub = -1;
+      if (t < nunit) {
+        const Unit u = P.units[t];
+        if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+          sub = u.sub;
+          ke = cano4_unit<FP64>(P, c, u);
+        }
+      }
+      add_kin(P, c.nsub_total, 2 * it, sub, ke);
+    }
+    if (!grid_barrier(P)) return;
+    // phase 5 of `it` fused with phase 3 of it+1
+    for (int base = 0; base < nunit; base += nthr) {
+      const int t = base + gt;
+      double ke = 0.0;
+      int sub = -1;
+      if (t < nunit) {
+        const Unit u = P.units[t];
+        if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+          cano5_unit<FP64>(P, c, u, it, tt);
+          sub = u.sub;
+          ke = cano3_unit<FP64>(P, c, u);
+        }
+      }
+      add_kin(P, c.nsub_total, 2 * it + 1, sub, ke);
     }
   }
 }
@@ -594,37 +688,36 @@ void launch_prepare(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t 
 }
 
 void launch_micr(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, cudaStream_t st) {
-  const int nb = (nunit + 127) / 128;
-  if (fp64) k_micr<true><<<nb, 128, 0, st>>>(P, c, nunit);
-  else k_micr<false><<<nb, 128, 0, st>>>(P, c, nunit);
+  const int nb = (nunit + 63) / 64;
+  if (fp64) k_micr<true><<<nb, 64, 0, st>>>(P, c, nunit);
+  else k_micr<false><<<nb, 64, 0, st>>>(P, c, nunit);
 }
 
-void launch_cano(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, cudaStream_t st) {
-  const int nb = (nunit + 127) / 128;
-  const bool shk = c.shake_method != JP_SHAKE_NONE;
-  if (fp64) {
-    if (shk) k_cano1<true><<<nb, 128, 0, st>>>(P, c, nunit);
-    k_cano2<true><<<nb, 128, 0, st>>>(P, c, nunit);
-    if (shk)
-      for (int it = 1; it <= c.icslop; ++it) {
-        k_cano3<true><<<nb, 128, 0, st>>>(P, c, nunit, it);
-        if (it < c.icslop) {
-          k_cano4<true><<<nb, 128, 0, st>>>(P, c, nunit, it);
-          k_cano5<true><<<nb, 128, 0, st>>>(P, c, nunit, it);
-        }
-      }
-  } else {
-    if (shk) k_cano1<false><<<nb, 128, 0, st>>>(P, c, nunit);
-    k_cano2<false><<<nb, 128, 0, st>>>(P, c, nunit);
-    if (shk)
-      for (int it = 1; it <= c.icslop; ++it) {
-        k_cano3<false><<<nb, 128, 0, st>>>(P, c, nunit, it);
-        if (it < c.icslop) {
-          k_cano4<false><<<nb, 128, 0, st>>>(P, c, nunit, it);
-          k_cano5<false><<<nb, 128, 0, st>>>(P, c, nunit, it);
-        }
-      }
-  }
+int cano_grid(bool fp64, int device) {
+  int nsm = 0, per = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  if (fp64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cano_fused<true>, 64, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cano_fused<false>, 64, 0);
+  return nsm * (per > 0 ? per : 1);
+}
+
+void launch_cano(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
+                 cudaStream_t st) {
+  cudaMemsetAsync(P.bar, 0, sizeof(unsigned) * 4, st);
+  const int want = (nunit + 63) / 64;
+  const int grid = want < grid_max ? (want > 0 ? want : 1) : grid_max;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(64);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (fp64) cudaLaunchKernelEx(&cfg, k_cano_fused<true>, P, c, nunit);
+  else cudaLaunchKernelEx(&cfg, k_cano_fused<false>, P, c, nunit);
 }
 
 void launch_finish(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t st) {

@@ -10,6 +10,7 @@ __global__ void k_scatter(DevPtrs P, int natom);
 __global__ void k_sort_bins(DevPtrs P, int nkeys);
 __global__ void k_clear_slots(DevPtrs P, int nslot, int dummy_type);
 __global__ void k_fill_slots(DevPtrs P, int natom);
+__global__ void k_excl_slots(DevPtrs P, int natom);
 __global__ void k_block_setup(DevPtrs P, int nblk, double qscale);
 __global__ void k_fill_pos_d(DevPtrs P, int nslot, double qscale);
 __global__ void k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rlimf);
@@ -51,7 +52,9 @@ struct IntConst {
 };
 void launch_prepare(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t st);
 void launch_micr(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, cudaStream_t st);
-void launch_cano(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, cudaStream_t st);
+int cano_grid(bool fp64, int device);   // co-resident blocks of the fused CANO kernel
+void launch_cano(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
+                 cudaStream_t st);
 void launch_finish(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t st);
 void launch_shake_only(const DevPtrs& P, const IntConst& c, int unit0, int nunit, cudaStream_t st);
 

@@ -157,6 +157,7 @@ def _build_polymer(top, nres, lo, hi, rng, box):
         idx["N"] = place(path[3 * r] + sg[0] * 0.41 * off, T_N)
         idx["CA"] = place(path[3 * r + 1] + sg[1] * 0.41 * off, T_C)
         idx["C"] = place(path[3 * r + 2] + sg[2] * 0.41 * off, T_C)
+        idx["atoms"] = [idx["N"], idx["CA"], idx["C"]]
         if prev_c is not None:
             top.bonds.append((prev_c, idx["N"]))
         top.bonds += [(idx["N"], idx["CA"]), (idx["CA"], idx["C"])]
@@ -174,6 +175,7 @@ def _build_polymer(top, nres, lo, hi, rng, box):
         top.bonds.append((idx["N"], idx["HN"]))
         top.shake.append((idx["N"], idx["HN"]))
         idx["HA"] = place(p_ca + 1.09 * (0.5 * sg[1] * off - 0.866 * zz), T_HC)
+        idx["atoms"] += [idx["O"], idx["HN"], idx["HA"]]
         top.bonds.append((idx["CA"], idx["HA"]))
         top.shake.append((idx["CA"], idx["HA"]))
     for idx in res:
@@ -194,6 +196,7 @@ def _build_polymer(top, nres, lo, hi, rng, box):
             prev_dir = (cands[best] - top.pos[anchor]) / 1.53
             nbrs = [anchor]
             heavy.append(a)
+            idx["atoms"].append(a)
             anchor = a
         # hydrogens: CH3 on the last heavy atom first, then CH2 down the chain
         caps = [2] * (len(heavy) - 1) + [3]
@@ -216,6 +219,7 @@ def _build_polymer(top, nres, lo, hi, rng, box):
                 h = place(cands[int(np.argmax(score))], T_HC)
                 top.bonds.append((a, h))
                 hs[a].append(h)
+                idx["atoms"].append(h)
                 nh -= 1
         for a in heavy:
             if hs[a]:
@@ -251,13 +255,22 @@ def _relax_solute(top, first, last, box, iters=400):
                 p13.add((nb[x], nb[y]))
     p13 = np.array(sorted(p13), int).reshape(-1, 2)
     d13 = np.where(isH[p13[:, 0]] & isH[p13[:, 1]], 1.6, 2.1) if len(p13) else np.zeros(0)
-    excl = set(map(tuple, bonds)) | set(map(tuple, bonds[:, ::-1])) | set(map(tuple, p13)) | \
-        set(map(tuple, p13[:, ::-1]))
-    iu, ju = np.triu_indices(n, 1)
-    keep = np.array([(i, j) not in excl for i, j in zip(iu, ju)])
-    iu, ju = iu[keep], ju[keep]
-    dmin = np.where(isH[iu] | isH[ju], 2.3, 2.9)
+    from scipy.spatial import cKDTree
+    ex_codes = np.unique(np.concatenate([np.minimum(bonds[:, 0], bonds[:, 1]) * n + np.maximum(bonds[:, 0], bonds[:, 1]),
+                                         np.minimum(p13[:, 0], p13[:, 1]) * n + np.maximum(p13[:, 0], p13[:, 1])]))
+    boxv = np.full(3, float(box)) if np.ndim(box) == 0 else np.asarray(box, float)
+    iu = ju = dmin = None
     for it in range(iters):
+        if it % 8 == 0:   # neighbour candidates within 3.5 A, periodic, 1-2/1-3 pairs removed
+            tree = cKDTree(np.mod(X, boxv), boxsize=boxv)
+            pr = tree.query_pairs(3.5, output_type="ndarray")
+            if len(pr):
+                a, b = np.minimum(pr[:, 0], pr[:, 1]), np.maximum(pr[:, 0], pr[:, 1])
+                keep = ~np.isin(a * n + b, ex_codes)
+                iu, ju = a[keep], b[keep]
+            else:
+                iu = ju = np.zeros(0, int)
+            dmin = np.where(isH[iu] | isH[ju], 2.3, 2.9)
         moved = False
         # non-bonded minimum distances
         d = X[iu] - X[ju]
@@ -293,16 +306,19 @@ def _relax_solute(top, first, last, box, iters=400):
 
 
 def _charges_polymer(top, first, last, residues, rng):
-    """q ~ N(0, 0.3) renormalised so each residue carries an integer charge."""
-    # atoms of residue r: from its N to the atom before the next residue's N
-    starts = [res["N"] for res in residues] + [last]
+    """Partial charges ~N(0, 0.3 e) renormalised so each residue carries an integer charge.
+    Hydrogens get small positive charges (|N(0, 0.15)| + 0.05): TIP3P water hydrogens carry
+    no Lennard-Jones repulsion, so a negatively charged solute hydrogen would let a water
+    hydrogen collapse onto it.  The heavy atoms absorb the renormalisation."""
     total = 0
-    for r in range(len(residues)):
-        ids = np.arange(starts[r], starts[r + 1])
+    for res in residues:
+        ids = np.array(res["atoms"])
+        isH = np.array([TYPES[top.typ[a]][0].startswith("H") for a in ids])
         q = rng.normal(0.0, 0.3, size=len(ids))
-        target = round(q.sum())
-        target = int(max(-1, min(1, target)))
-        q += (target - q.sum()) / len(ids)
+        q[isH] = np.abs(rng.normal(0.0, 0.15, size=int(isH.sum()))) + 0.05
+        target = int(max(-1, min(1, round(q.sum()))))
+        heavy = ~isH
+        q[heavy] += (target - q.sum()) / int(heavy.sum())
         for a, v in zip(ids, q):
             top.chg[a] = float(v)
         total += target
