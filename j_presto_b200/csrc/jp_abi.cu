@@ -41,6 +41,7 @@ struct jp_ctx {
   jp_params prm{};
   int device = 0;
   int natom = 0, nblk = 0, nslot = 0, nunit = 0, nterm = 0, nsub = 0, nkeys = 0, nkin = 8;
+  int ncol = 0;
   int tile_cap_total = 0, nchunk = 0;
   std::vector<Rep> reps;
   std::vector<int> rep_natom;
@@ -106,23 +107,20 @@ int dput(jp_ctx *c, T **p, const std::vector<T> &h) {
 
 constexpr double kEekcal = 332.06378;
 
-int ceil_log2(int v) {
-  int b = 0;
-  while ((1 << b) < v) ++b;
-  return b;
-}
-
 // ---- rebuild: cells + tiles -------------------------------------------------------------
 void enqueue_rebuild(jp_ctx *c) {
   DevPtrs &P = c->P;
   cudaStream_t st = c->st;
   const int nt = 256;
-  cudaMemsetAsync(P.hist, 0, sizeof(int) * c->nkeys, st);
-  cudaMemsetAsync(P.cursor, 0, sizeof(int) * c->nkeys, st);
+  cudaMemsetAsync(P.hist, 0, sizeof(int) * (c->nkeys + 1), st);
+  cudaMemsetAsync(P.cursor, 0, sizeof(int) * (c->nkeys + 1), st);
+  cudaMemsetAsync(P.rep_hmax, 0, sizeof(float) * 3 * c->nrep, st);
   k_cell_key<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
-  scan_exclusive(P.hist, P.hist_scan, c->nkeys, c->scan_scratch, nullptr, st);
+  scan_exclusive(P.hist, P.hist_scan, c->nkeys + 1, c->scan_scratch, nullptr, st);
   k_scatter<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
   k_sort_bins<<<(c->nkeys + nt - 1) / nt, nt, 0, st>>>(P, c->nkeys);
+  k_col_count<<<(c->ncol + nt - 1) / nt, nt, 0, st>>>(P, c->ncol);
+  scan_exclusive(P.col_nb, P.col_blk, c->ncol + 1, c->scan_scratch, nullptr, st);
   k_clear_slots<<<(c->nslot + nt - 1) / nt, nt, 0, st>>>(P, c->nslot, c->zc.nt1 - 1);
   k_fill_slots<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
   k_excl_slots<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
@@ -133,7 +131,7 @@ void enqueue_rebuild(jp_ctx *c) {
   k_tile_scan_chunks<<<nwb, 128, 0, st>>>(P, c->nchunk, rlim * rlim, (float)rlim);
   scan_exclusive(P.chunk_cnt, P.chunk_off, c->nchunk + 1, c->scan_scratch, P.ntiles, st);
   k_tile_emit<<<nwb, 128, 0, st>>>(P, c->nchunk);
-  c->launches_rebuild = 15 + (c->fp64 ? 1 : 0);
+  c->launches_rebuild = 19 + (c->fp64 ? 1 : 0);
 }
 
 // ---- one MD step ------------------------------------------------------------------------
@@ -341,7 +339,8 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       ljd[i * nt1 + j] = make_double2(sys[0].c6[i * ntype + j], sys[0].c12[i * ntype + j]);
       ljf[i * nt1 + j] = make_float2((float)sys[0].c6[i * ntype + j], (float)sys[0].c12[i * ntype + j]);
     }
-  int atom0 = 0, blk0 = 0, key0 = 0, sub0 = 0;
+  int atom0 = 0, blk0 = 0, key0 = 0, sub0 = 0, col0 = 0;
+  std::vector<int> hcol_rep;
   for (int r = 0; r < nrep; ++r) {
     const jp_system &s = sys[r];
     const int b = s.index_base;
@@ -351,16 +350,28 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     R.atom0 = atom0;
     R.natom = n;
     R.blk0 = blk0;
-    R.nblk = (n + kTile - 1) / kTile;
+    // xy columns of edge ~(32/density)^(1/3) so that 32 z-sorted atoms fill a near-cubic
+    // block; 0.25 A z bins inside a column
+    const double dens = n / (s.box[0] * s.box[1] * s.box[2]);
+    const double edge = std::cbrt((double)kTile / dens);
     for (int k = 0; k < 3; ++k) {
       R.box[k] = s.box[k];
       R.invbox[k] = 1.0 / s.box[k];
-      R.grid[k] = std::max(1, std::min(1024, (int)std::floor(s.box[k] / 2.4)));
+    }
+    for (int k = 0; k < 2; ++k) {
+      R.grid[k] = std::max(1, std::min(512, (int)std::lround(s.box[k] / edge)));
       R.cell[k] = s.box[k] / R.grid[k];
     }
-    R.keybits = ceil_log2(std::max(R.grid[0], std::max(R.grid[1], R.grid[2])));
+    R.grid[2] = std::max(1, (int)std::ceil(s.box[2] / 0.25));
+    R.cell[2] = s.box[2] / R.grid[2];
+    R.col0 = col0;
+    R.ncol = R.grid[0] * R.grid[1];
+    col0 += R.ncol;
+    for (int q = 0; q < R.ncol; ++q) hcol_rep.push_back(r);
     R.key0 = key0;
-    key0 += 1 << (3 * R.keybits);
+    key0 += R.ncol * R.grid[2];
+    // block capacity: every column wastes less than one block
+    R.nblk = (n + kTile - 1) / kTile + R.ncol;
     for (int i = 0; i < n; ++i) {
       for (int k = 0; k < 3; ++k) {
         hx.push_back(s.cord[3 * i + k]);
@@ -553,6 +564,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   c->nunit = (int)units.size();
   c->nsub = sub0;
   c->nkeys = key0;
+  c->ncol = col0;
   c->nkin = std::max(8, 2 * prm->icslop + 2);
   std::vector<Term> terms;
   for (auto &v2 : terms_by_kind) terms.insert(terms.end(), v2.begin(), v2.end());
@@ -613,9 +625,13 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.masks, (size_t)c->tile_cap_total * 32);
   e |= dalloc(c, &P.ntiles, 1);
   e |= dalloc(c, &P.key, (size_t)N);
-  e |= dalloc(c, &P.hist, (size_t)c->nkeys);
-  e |= dalloc(c, &P.hist_scan, (size_t)c->nkeys);
-  e |= dalloc(c, &P.cursor, (size_t)c->nkeys);
+  e |= dalloc(c, &P.hist, (size_t)c->nkeys + 1);        // +1: sentinel for the scan
+  e |= dalloc(c, &P.hist_scan, (size_t)c->nkeys + 1);
+  e |= dalloc(c, &P.cursor, (size_t)c->nkeys + 1);
+  e |= dput(c, &P.col_rep, hcol_rep);
+  e |= dalloc(c, &P.col_nb, (size_t)c->ncol + 1);
+  e |= dalloc(c, &P.col_blk, (size_t)c->ncol + 1);
+  e |= dalloc(c, &P.rep_hmax, 3 * (size_t)nrep);
   e |= dalloc(c, &P.sorted, (size_t)N);
   e |= dput(c, &P.units, units);
   e |= dput(c, &P.terms, terms);
@@ -634,7 +650,8 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.step_ctr, 2);
   e |= dput(c, &P.lj_f, ljf);
   e |= dput(c, &P.lj_d, ljd);
-  e |= dalloc(c, &c->scan_scratch, (size_t)std::max(c->nkeys, c->nchunk + 1) / 1024 + 2);
+  e |= dalloc(c, &c->scan_scratch,
+              (size_t)std::max(std::max(c->nkeys, c->ncol), c->nchunk) / 1024 + 4);
   if (e) { jp_destroy(c); return JP_E_CUDA; }
   // the tile-row prefix must cover the sentinel entry; row_cnt[nblk] stays 0
   // ---- constants ---------------------------------------------------------------------------
@@ -642,6 +659,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   c->zc.zcore = 1.5 / rc;
   c->zc.fcoeff = 1.0 / (rc * rc * rc);
   c->zc.bcoeff = 0.5 * c->zc.fcoeff;
+  c->zc.rlim = rc + 1.5;
   c->zc.nt1 = nt1;
   IntConst &ic = c->ic;
   ic.dt = prm->dt;

@@ -19,28 +19,21 @@
 
 namespace jp {
 
-__device__ __forceinline__ unsigned spread3(unsigned v) {
-  v &= 0x3ffu;
-  v = (v | (v << 16)) & 0x030000FFu;
-  v = (v | (v << 8)) & 0x0300F00Fu;
-  v = (v | (v << 4)) & 0x030C30C3u;
-  v = (v | (v << 2)) & 0x09249249u;
-  return v;
-}
-
+// Binning: atoms go to xy columns of edge ~(32/density)^(1/3) (~6.8 A for water) and,
+// inside a column, to 0.25 A z bins.  The key orders atoms by (replica, column, z), so each
+// column's atoms are z-sorted and a column cut into runs of 32 gives near-cubic blocks.
 __global__ void k_cell_key(DevPtrs P, int natom) {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= natom) return;
   const Rep R = P.reps[P.rep_of[a]];
-  unsigned c[3];
+  int c[3];
   for (int k = 0; k < 3; ++k) {
-    double x = P.x[3 * a + k];
-    double w = x - R.box[k] * floor(x * R.invbox[k]);
+    const double x = P.x[3 * a + k];
+    const double w = x - R.box[k] * floor(x * R.invbox[k]);
     int q = (int)(w / R.cell[k]);
-    q = q < 0 ? 0 : (q >= R.grid[k] ? R.grid[k] - 1 : q);
-    c[k] = (unsigned)q;
+    c[k] = q < 0 ? 0 : (q >= R.grid[k] ? R.grid[k] - 1 : q);
   }
-  unsigned key = (unsigned)R.key0 + (spread3(c[0]) | (spread3(c[1]) << 1) | (spread3(c[2]) << 2));
+  const unsigned key = (unsigned)(R.key0 + (c[1] * R.grid[0] + c[0]) * R.grid[2] + c[2]);
   P.key[a] = key;
   atomicAdd(&P.hist[key], 1);
 }
@@ -68,6 +61,17 @@ __global__ void k_sort_bins(DevPtrs P, int nkeys) {
   }
 }
 
+// blocks each column needs: ceil(atoms in column / 32)
+__global__ void k_col_count(DevPtrs P, int ncol) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  const int r = P.col_rep[c];
+  const Rep& R = P.reps[r];
+  const int k0 = R.key0 + (c - R.col0) * R.grid[2];
+  const int n = P.hist_scan[k0 + R.grid[2]] - P.hist_scan[k0];
+  P.col_nb[c] = (n + kTile - 1) / kTile;
+}
+
 __global__ void k_clear_slots(DevPtrs P, int nslot, int dummy_type) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nslot) return;
@@ -75,12 +79,18 @@ __global__ void k_clear_slots(DevPtrs P, int nslot, int dummy_type) {
   P.styp[s] = dummy_type;
 }
 
+// sorted position -> slot: block = replica's first block + blocks of the columns before this
+// one (a column never shares a block with another), lane = rank inside the column
 __global__ void k_fill_slots(DevPtrs P, int natom) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= natom) return;
-  int a = P.sorted[c];
+  const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos >= natom) return;
+  const int a = P.sorted[pos];
   const Rep& R = P.reps[P.rep_of[a]];
-  int slot = c - R.atom0 + kTile * R.blk0;
+  const int col = R.col0 + ((int)P.key[a] - R.key0) / R.grid[2];
+  const int kcol = R.key0 + (col - R.col0) * R.grid[2];
+  const int rank = pos - P.hist_scan[kcol];
+  const int blk = R.blk0 + (P.col_blk[col] - P.col_blk[R.col0]) + rank / kTile;
+  const int slot = blk * kTile + (rank % kTile);
   P.slot_of[a] = slot;
   P.satom[slot] = a;
   P.styp[slot] = P.typ[a];
@@ -119,9 +129,18 @@ __global__ void k_block_setup(DevPtrs P, int nblk, double qscale) {
     P.blk_ref[3 * warp + 1] = ref[1];
     P.blk_ref[3 * warp + 2] = ref[2];
     P.blk_ctr[warp] = make_float4((float)ref[0], (float)ref[1], (float)ref[2], 0.f);
+    // an empty block (capacity not used this rebuild) gets a -inf extent: it never passes
+    // the bounding-box test
     P.blk_half[warp] = make_float4((float)(0.5 * (hi[0] - lo[0])) + 1e-4f,
                                    (float)(0.5 * (hi[1] - lo[1])) + 1e-4f,
                                    (float)(0.5 * (hi[2] - lo[2])) + 1e-4f, 0.f);
+    if (lo[0] <= hi[0]) {   // largest block half-extent per replica (non-negative floats
+                            // order like their bit patterns)
+      const int r = P.blk_rep[warp];
+      for (int k = 0; k < 3; ++k)
+        atomicMax(reinterpret_cast<int*>(&P.rep_hmax[3 * r + k]),
+                  __float_as_int((float)(0.5 * (hi[k] - lo[k]))));
+    }
   }
   double o[3];
   for (int k = 0; k < 3; ++k) o[k] = ref[k] + R.box[k] * img[k];

@@ -45,10 +45,11 @@ struct Rep {
   int blk0, nblk;          // block range (slots [32*blk0, 32*(blk0+nblk)))
   int unit0, nunit;        // integration units
   int sub0, nsub;          // temperature sub-systems (global ids)
-  int key0, keybits;       // cell-key range start, Morton bits per dimension
-  int grid[3];
+  int key0;                // first sort key of the replica
+  int col0, ncol;          // first global xy column, number of columns
+  int grid[3];             // columns in x, in y; z bins per column
   double box[3], invbox[3];
-  double cell[3];          // cell edge per dimension
+  double cell[3];          // column edge in x, in y; z-bin height
   double dself;
   int ge_off, ge_nwin, ge_ndeg;   // offset into the GE coefficient array
   double ge_alphalw, ge_alphaup, ge_celw, ge_ceup, ge_tempce;
@@ -106,6 +107,9 @@ struct DevPtrs {
   unsigned *key;                  // per atom
   int *hist, *hist_scan, *cursor; // per key
   int *sorted;                    // compact order -> atom
+  int *col_rep;                   // replica of each xy column (static)
+  int *col_nb, *col_blk;          // blocks per column and their exclusive scan [ncol+1]
+  float *rep_hmax;                // largest block half-extent per replica [nrep][3]
   // units / terms
   Unit *units;
   Term *terms;

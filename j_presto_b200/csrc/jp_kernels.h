@@ -8,6 +8,7 @@ namespace jp {
 __global__ void k_cell_key(DevPtrs P, int natom);
 __global__ void k_scatter(DevPtrs P, int natom);
 __global__ void k_sort_bins(DevPtrs P, int nkeys);
+__global__ void k_col_count(DevPtrs P, int ncol);
 __global__ void k_clear_slots(DevPtrs P, int nslot, int dummy_type);
 __global__ void k_fill_slots(DevPtrs P, int natom);
 __global__ void k_excl_slots(DevPtrs P, int natom);
@@ -20,6 +21,7 @@ void scan_exclusive(const int* in, int* out, int n, int* scratch, int* total, cu
 // ZD pair constants
 struct ZdConst {
   double rc2, zcore, bcoeff, fcoeff;
+  double rlim;             // list radius rc + 1.5
   int nt1;                 // LJ table stride (ntype + 1 incl. the dummy type)
 };
 

@@ -39,14 +39,67 @@ __device__ __forceinline__ void flush_energy(const DevPtrs& P, int rep, double e
   }
 }
 
+// One 32x32 tile: lane = i atom; the j atoms are staged in the warp's shared-memory slice
+// and read at (lane + k) & 31 in step k; the j-force accumulators rotate one lane per step
+// (3 shuffles) so that after 32 steps each is back in the lane of its atom.
 template <bool MINIMG, bool COUNT>
+__device__ __forceinline__ void tile_mixed(const float4* __restrict__ sj_pos, const int* __restrict__ sj_typ,
+                                           const float2* __restrict__ s_lj, int nt1, float4 pi, int ti,
+                                           float4 sh, unsigned m, int lane, float bx, float by, float bz,
+                                           float ibx, float iby, float ibz, float rc2, float zb, float zf,
+                                           float zc, float& fix, float& fiy, float& fiz, float& gjx,
+                                           float& gjy, float& gjz, float& te, float& tl, int& tn) {
+  const float xi = pi.x + sh.x, yi = pi.y + sh.y, zi = pi.z + sh.z;
+  const int row = ti * nt1;
+#pragma unroll 4
+  for (int k = 0; k < 32; ++k) {
+    const int jl = (lane + k) & 31;
+    if (m & 1u) {
+      const float4 pj = sj_pos[jl];
+      float dx = xi - pj.x, dy = yi - pj.y, dz = zi - pj.z;
+      if (MINIMG) {
+        dx -= bx * rintf(dx * ibx);
+        dy -= by * rintf(dy * iby);
+        dz -= bz * rintf(dz * ibz);
+      }
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      if (r2 <= rc2) {
+        const float rinv = rsqrtf(r2);
+        const float r2inv = rinv * rinv;
+        const float r6inv = r2inv * r2inv * r2inv;
+        const float2 lj = s_lj[row + sj_typ[jl]];
+        const float qq = pi.w * pj.w;
+        const float v1 = lj.x * r6inv;
+        const float v2 = lj.y * r6inv * r6inv;
+        te = fmaf(qq, rinv + fmaf(zb, r2, -zc), te);
+        tl += v2 - v1;
+        const float fs = fmaf(qq, fmaf(rinv, r2inv, -zf), (12.f * v2 - 6.f * v1) * r2inv);
+        const float fx = dx * fs, fy = dy * fs, fz = dz * fs;
+        fix -= fx; fiy -= fy; fiz -= fz;
+        gjx += fx; gjy += fy; gjz += fz;
+        if (COUNT) ++tn;
+      }
+    }
+    m >>= 1;
+    const int src = (lane + 1) & 31;
+    gjx = __shfl_sync(0xffffffffu, gjx, src);
+    gjy = __shfl_sync(0xffffffffu, gjy, src);
+    gjz = __shfl_sync(0xffffffffu, gjz, src);
+  }
+}
+
+template <bool COUNT>
 __global__ void __launch_bounds__(kPairThreads)
 k_pair_mixed(DevPtrs P, ZdConst z) {
   extern __shared__ float2 s_lj[];
+  __shared__ float4 s_jpos[kPairThreads];
+  __shared__ int s_jtyp[kPairThreads];
   const int nlj = z.nt1 * z.nt1;
   for (int i = threadIdx.x; i < nlj; i += blockDim.x) s_lj[i] = P.lj_f[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
+  float4* sj_pos = s_jpos + (threadIdx.x & ~31);
+  int* sj_typ = s_jtyp + (threadIdx.x & ~31);
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const int T = *P.ntiles;
@@ -60,6 +113,7 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
   long long gix = 0, giy = 0, giz = 0;
   double eel = 0.0, elj = 0.0;
   long long npair = 0;
+  bool mi = true;
   float bx = 0.f, by = 0.f, bz = 0.f, ibx = 0.f, iby = 0.f, ibz = 0.f;
   for (int t = t0; t < t1; ++t) {
     const int2 ij = P.tiles[t];
@@ -84,57 +138,30 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
         const Rep& R = P.reps[rep];
         bx = (float)R.box[0]; by = (float)R.box[1]; bz = (float)R.box[2];
         ibx = (float)R.invbox[0]; iby = (float)R.invbox[1]; ibz = (float)R.invbox[2];
+        // Per-pair minimum image is needed only if a listed pair could reach half a box
+        // length: |d| <= rlim + 2*(h_i + h_j) + motion since the build (2 A margin).
+        mi = false;
+        for (int k = 0; k < 3; ++k)
+          if (0.5 * R.box[k] < z.rlim + 4.0 * (double)P.rep_hmax[3 * rep + k] + 2.0) mi = true;
       }
     }
     const float4 sh = P.tile_shift[t];
-    unsigned m = P.masks[(size_t)t * 32 + lane];
+    const unsigned m = P.masks[(size_t)t * 32 + lane];
     const int sj = ij.y * kTile + lane;
-    float4 pj = P.pos_f[sj];
-    int tj = P.styp[sj];
-    const float xi = pi.x + sh.x, yi = pi.y + sh.y, zi = pi.z + sh.z;
-    const int row = ti * z.nt1;
+    __syncwarp();
+    sj_pos[lane] = P.pos_f[sj];
+    sj_typ[lane] = P.styp[sj];
+    __syncwarp();
     float gjx = 0.f, gjy = 0.f, gjz = 0.f;
     float fix = 0.f, fiy = 0.f, fiz = 0.f;
     float te = 0.f, tl = 0.f;
     int tn = 0;
-#pragma unroll 4
-    for (int k = 0; k < 32; ++k) {
-      if (m & 1u) {
-        float dx = xi - pj.x, dy = yi - pj.y, dz = zi - pj.z;
-        if (MINIMG) {
-          dx -= bx * rintf(dx * ibx);
-          dy -= by * rintf(dy * iby);
-          dz -= bz * rintf(dz * ibz);
-        }
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        if (r2 <= rc2) {
-          const float rinv = rsqrtf(r2);
-          const float r2inv = rinv * rinv;
-          const float r6inv = r2inv * r2inv * r2inv;
-          const float2 lj = s_lj[row + tj];
-          const float qq = pi.w * pj.w;
-          const float v1 = lj.x * r6inv;
-          const float v2 = lj.y * r6inv * r6inv;
-          te = fmaf(qq, rinv + fmaf(zb, r2, -zc), te);
-          tl += v2 - v1;
-          const float fs = fmaf(qq, fmaf(rinv, r2inv, -zf), (12.f * v2 - 6.f * v1) * r2inv);
-          const float fx = dx * fs, fy = dy * fs, fz = dz * fs;
-          fix -= fx; fiy -= fy; fiz -= fz;
-          gjx += fx; gjy += fy; gjz += fz;
-          if (COUNT) ++tn;
-        }
-      }
-      m >>= 1;
-      const int src = (lane + 1) & 31;
-      pj.x = __shfl_sync(0xffffffffu, pj.x, src);
-      pj.y = __shfl_sync(0xffffffffu, pj.y, src);
-      pj.z = __shfl_sync(0xffffffffu, pj.z, src);
-      pj.w = __shfl_sync(0xffffffffu, pj.w, src);
-      tj = __shfl_sync(0xffffffffu, tj, src);
-      gjx = __shfl_sync(0xffffffffu, gjx, src);
-      gjy = __shfl_sync(0xffffffffu, gjy, src);
-      gjz = __shfl_sync(0xffffffffu, gjz, src);
-    }
+    if (mi)
+      tile_mixed<true, COUNT>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, lane, bx, by, bz, ibx, iby,
+                              ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn);
+    else
+      tile_mixed<false, COUNT>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, lane, bx, by, bz, ibx, iby,
+                               ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn);
     const int aj = P.satom[sj];
     if (aj >= 0 && (gjx != 0.f || gjy != 0.f || gjz != 0.f)) {
       atomic_add_ll(&P.frc[3 * aj + 0], to_fix((double)gjx, kFrcScale));
@@ -262,18 +289,13 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
   flush_energy(P, cur_rep, eel, elj, npair, COUNT);
 }
 
-void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool minimg, bool count,
+void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool, bool count,
                        cudaStream_t st) {
   const int wpb = kPairThreads / 32;
   const int nb = (nwarps + wpb - 1) / wpb;
   const size_t sh = sizeof(float2) * z.nt1 * z.nt1;
-  if (minimg) {
-    if (count) k_pair_mixed<true, true><<<nb, kPairThreads, sh, st>>>(P, z);
-    else k_pair_mixed<true, false><<<nb, kPairThreads, sh, st>>>(P, z);
-  } else {
-    if (count) k_pair_mixed<false, true><<<nb, kPairThreads, sh, st>>>(P, z);
-    else k_pair_mixed<false, false><<<nb, kPairThreads, sh, st>>>(P, z);
-  }
+  if (count) k_pair_mixed<true><<<nb, kPairThreads, sh, st>>>(P, z);
+  else k_pair_mixed<false><<<nb, kPairThreads, sh, st>>>(P, z);
 }
 
 void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, cudaStream_t st) {
