@@ -161,10 +161,7 @@ void enqueue_bonded(jp_ctx *c) {
 void enqueue_integrate(jp_ctx *c) {
   DevPtrs &P = c->P;
   cudaMemsetAsync(P.kin_fix, 0, sizeof(long long) * c->nkin * c->nsub, c->st);
-  launch_prepare(P, c->ic, c->nrep, c->st);
-  if (c->prm.method == JP_METHOD_MICR) launch_micr(P, c->ic, c->nunit, c->fp64, c->st);
-  else launch_cano(P, c->ic, c->nunit, c->fp64, c->cano_grid, c->st);
-  launch_finish(P, c->ic, c->nrep, c->st);
+  launch_integrate(P, c->ic, c->nunit, c->fp64, c->cano_grid, c->st);
 }
 
 int launches_per_step(const jp_ctx *c) {

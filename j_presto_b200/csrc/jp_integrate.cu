@@ -8,6 +8,8 @@
 // is FP64.  Kinetic-energy sums for the thermostat are 64-bit fixed point (order
 // independent); all replicas are processed by the same launches and each replica keeps
 // its own temperatures, SHAKE<->thermostat iteration count and force scale.
+#include <algorithm>
+
 #include "jp_kernels.h"
 
 namespace jp {
@@ -35,10 +37,12 @@ __host__ __device__ __noinline__ int shake_group4(const Rep& R, const Unit& u, c
                                                  double tol, int maxit);
 
 // ---- SHAKE on one group (r1 constrained against reference r2) --------------------------
-// returns 0 converged, 1 not converged, -2 singular
-__host__ __device__ int shake_group(const Rep& R, const Unit& u, const double* im, double r1[4][3],
-                           const double r2[4][3], int method, double tol, int maxit) {
-  const int n = u.n;
+// returns 0 converged, 1 not converged, -2 singular.  2- and 3-atom groups: inlined, works on
+// register arrays; 4-atom groups: shake_group4, out of line.
+__host__ __device__ __forceinline__ int shake_small(const Rep& R, int n, const double* len2,
+                                                    const double* im, double (*r1)[3],
+                                                    const double (*r2)[3], int method, double tol,
+                                                    int maxit) {
   if (n == 2) {
     double d1[3], d2[3];
     if (method == JP_SHAKE_HBON) {   // shak2e (shake.f90:687-755): exact quadratic
@@ -49,7 +53,7 @@ __host__ __device__ int shake_group(const Rep& R, const Unit& u, const double* i
       const double d1d1 = d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2];
       const double d1d2 = d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2];
       const double d2d2 = d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2];
-      const double A = i4 * d2d2, B = i3 * d1d2, C = d1d1 - u.d2[0];
+      const double A = i4 * d2d2, B = i3 * d1d2, C = d1d1 - len2[0];
       const double G = (B - sqrt(B * B - C * A)) / A;
       for (int k = 0; k < 3; ++k) {
         r1[0][k] += im[0] * G * d2[k];
@@ -64,7 +68,7 @@ __host__ __device__ int shake_group(const Rep& R, const Unit& u, const double* i
     for (int it = 0; it < maxit; ++it) {
       for (int k = 0; k < 3; ++k) d1[k] = r1[0][k] - r1[1][k];
       mimg(R, d1);
-      double dif = u.d2[0] - (d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
+      double dif = len2[0] - (d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
       const double inpro = d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2];
       const double G = dif * i3 / inpro;
       for (int k = 0; k < 3; ++k) {
@@ -73,8 +77,8 @@ __host__ __device__ int shake_group(const Rep& R, const Unit& u, const double* i
       }
       for (int k = 0; k < 3; ++k) d1[k] = r1[0][k] - r1[1][k];
       mimg(R, d1);
-      dif = u.d2[0] - (d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
-      if (fabs(dif / u.d2[0]) < tol) return 0;
+      dif = len2[0] - (d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
+      if (fabs(dif / len2[0]) < tol) return 0;
     }
     return 1;
   }
@@ -96,8 +100,8 @@ __host__ __device__ int shake_group(const Rep& R, const Unit& u, const double* i
     bool singular = false;
     for (int it = 0; it < maxit; ++it) {
       double B[3];
-      for (int q = 0; q < 3; ++q) B[q] = u.d2[q] - (d1[q][0] * d1[q][0] + d1[q][1] * d1[q][1] + d1[q][2] * d1[q][2]);
-      if (fabs(B[0]) < tol * u.d2[0] && fabs(B[1]) < tol * u.d2[1] && fabs(B[2]) < tol * u.d2[2]) {
+      for (int q = 0; q < 3; ++q) B[q] = len2[q] - (d1[q][0] * d1[q][0] + d1[q][1] * d1[q][1] + d1[q][2] * d1[q][2]);
+      if (fabs(B[0]) < tol * len2[0] && fabs(B[1]) < tol * len2[1] && fabs(B[2]) < tol * len2[2]) {
         for (int k = 0; k < 3; ++k) {
           r1[0][k] += im[0] * (G[3] * d2[0][k] - G[5] * d2[2][k]);
           r1[1][k] += im[1] * (-G[3] * d2[0][k] + G[4] * d2[1][k]);
@@ -132,7 +136,33 @@ __host__ __device__ int shake_group(const Rep& R, const Unit& u, const double* i
     }
     return singular ? -2 : 1;
   }
+  return 1;
+}
+
+__host__ __device__ int shake_group(const Rep& R, const Unit& u, const double* im, double r1[4][3],
+                                    const double r2[4][3], int method, double tol, int maxit) {
+  if (u.n <= 3) return shake_small(R, u.n, u.d2, im, r1, r2, method, tol, maxit);
   return shake_group4(R, u, im, r1, r2, tol, maxit);
+}
+
+// coefficient matrix coeg of shake4 (shake.f90:363-398): entry (q, ig) from the inverse
+// masses; evaluated at each use (static q, ig fold to one add or a sign) instead of being
+// held as a 6x6 array
+__host__ __device__ __forceinline__ double cg4(int q, int ig, const double* im) {
+  switch (q * 6 + ig) {
+    case 0: return im[0] + im[1];  case 1: return -im[1];  case 2: return -im[0];
+    case 3: return -im[0];         case 4: return 0.0;     case 5: return -im[1];
+    case 6: return -im[1];         case 7: return im[1] + im[2];  case 8: return -im[2];
+    case 9: return 0.0;            case 10: return -im[2]; case 11: return im[1];
+    case 12: return -im[0];        case 13: return -im[2]; case 14: return im[2] + im[0];
+    case 15: return im[0];         case 16: return im[2];  case 17: return 0.0;
+    case 18: return -im[0];        case 19: return 0.0;    case 20: return im[0];
+    case 21: return im[3] + im[0]; case 22: return -im[3]; case 23: return -im[3];
+    case 24: return 0.0;           case 25: return -im[2]; case 26: return im[2];
+    case 27: return -im[3];        case 28: return im[2] + im[3]; case 29: return im[3];
+    case 30: return -im[1];        case 31: return im[1];  case 32: return 0.0;
+    case 33: return -im[3];        case 34: return im[3];  default: return im[1] + im[3];
+  }
 }
 
 // n == 4: shake4 (shake.f90:333-562): Newton with LU (simulu.f90).  Kept out of line: only
@@ -141,13 +171,6 @@ __host__ __device__ int shake_group(const Rep& R, const Unit& u, const double* i
 __host__ __device__ __noinline__ int shake_group4(const Rep& R, const Unit& u, const double* im,
                                                  double r1[4][3], const double r2[4][3],
                                                  double tol, int maxit) {
-  const double cg[6][6] = {
-      {im[0] + im[1], -im[1], -im[0], -im[0], 0.0, -im[1]},
-      {-im[1], im[1] + im[2], -im[2], 0.0, -im[2], im[1]},
-      {-im[0], -im[2], im[2] + im[0], im[0], im[2], 0.0},
-      {-im[0], 0.0, im[0], im[3] + im[0], -im[3], -im[3]},
-      {0.0, -im[2], im[2], -im[3], im[2] + im[3], im[3]},
-      {-im[1], im[1], 0.0, -im[3], im[3], im[1] + im[3]}};
   const int pa[6][2] = {{0, 1}, {1, 2}, {2, 0}, {3, 0}, {2, 3}, {1, 3}};
   double d1[6][3], d2[6][3], wk[6][3], G[6] = {0, 0, 0, 0, 0, 0};
   for (int q = 0; q < 6; ++q) {
@@ -177,46 +200,66 @@ __host__ __device__ __noinline__ int shake_group4(const Rep& R, const Unit& u, c
       return singular ? -2 : 0;
     }
     double A[6][6];
+#pragma unroll
     for (int ig = 0; ig < 6; ++ig)
+#pragma unroll
       for (int q = 0; q < 6; ++q)
-        A[q][ig] = 2.0 * cg[q][ig] * (wk[q][0] * d2[ig][0] + wk[q][1] * d2[ig][1] + wk[q][2] * d2[ig][2]);
+        A[q][ig] = 2.0 * cg4(q, ig, im) * (wk[q][0] * d2[ig][0] + wk[q][1] * d2[ig][1] + wk[q][2] * d2[ig][2]);
     for (int ig = 0; ig < 6; ++ig)
       for (int q = 0; q < 6; ++q) B[q] += A[q][ig] * G[ig];
-    // LU with partial pivoting through a row permutation (simulu.f90 ludeco + solve)
-    int ip[6] = {0, 1, 2, 3, 4, 5};
+    // LU with partial pivoting (simulu.f90 ludeco + solve): the same pivot choice and
+    // elimination order as md_run's row-permutation form, with the pivot row swapped in
+    // registers (static indices only, so nothing goes to local memory)
     bool lu_ok = true;
-    for (int k = 0; k < 6 && lu_ok; ++k) {
-      int l = k;
-      double al = fabs(A[ip[l]][k]);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      int pr = k;
+      double al = fabs(A[k][k]);
+#pragma unroll
       for (int i = k + 1; i < 6; ++i)
-        if (fabs(A[ip[i]][k]) > al) { l = i; al = fabs(A[ip[l]][k]); }
-      if (l != k) { int t = ip[k]; ip[k] = ip[l]; ip[l] = t; }
-      if (fabs(A[ip[k]][k]) < 1.0e-30) { lu_ok = false; break; }
-      A[ip[k]][k] = 1.0 / A[ip[k]][k];
+        if (fabs(A[i][k]) > al) { pr = i; al = fabs(A[i][k]); }
+#pragma unroll
       for (int i = k + 1; i < 6; ++i) {
-        A[ip[i]][k] *= A[ip[k]][k];
-        for (int j = k + 1; j < 6; ++j) A[ip[i]][j] -= A[ip[i]][k] * A[ip[k]][j];
+        const bool sw = (pr == i);
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+          const double t = A[k][j];
+          A[k][j] = sw ? A[i][j] : t;
+          A[i][j] = sw ? t : A[i][j];
+        }
+        const double tb = B[k];
+        B[k] = sw ? B[i] : tb;
+        B[i] = sw ? tb : B[i];
       }
+      if (fabs(A[k][k]) < 1.0e-30) lu_ok = false;
+      const double piv = 1.0 / A[k][k];
+#pragma unroll
+      for (int i = k + 1; i < 6; ++i) {
+        const double f = A[i][k] * piv;
+#pragma unroll
+        for (int j = k + 1; j < 6; ++j) A[i][j] -= f * A[k][j];
+        B[i] -= f * B[k];
+      }
+      A[k][k] = piv;
     }
     if (!lu_ok) {
       singular = true;
     } else {
-      for (int i = 0; i < 6; ++i) {
-        double t = B[ip[i]];
-        for (int j = 0; j < i; ++j) t -= A[ip[i]][j] * G[j];
-        G[i] = t;
-      }
+#pragma unroll
       for (int i = 5; i >= 0; --i) {
-        double t = G[i];
-        for (int j = i + 1; j < 6; ++j) t -= A[ip[i]][j] * G[j];
-        G[i] = t * A[ip[i]][i];
+        double t = B[i];
+#pragma unroll
+        for (int j = i + 1; j < 6; ++j) t -= A[i][j] * G[j];
+        G[i] = t * A[i][i];
       }
     }
     for (int q = 0; q < 6; ++q)
       for (int k = 0; k < 3; ++k) wk[q][k] = d1[q][k];
+#pragma unroll
     for (int ig = 0; ig < 6; ++ig)
+#pragma unroll
       for (int q = 0; q < 6; ++q)
-        for (int k = 0; k < 3; ++k) wk[q][k] += cg[q][ig] * d2[ig][k] * G[ig];
+        for (int k = 0; k < 3; ++k) wk[q][k] += cg4(q, ig, im) * d2[ig][k] * G[ig];
   }
   return singular ? -2 : 1;
 }
@@ -291,25 +334,14 @@ __device__ bool cano_active(const DevPtrs& P, const IntConst& c, const Rep& R, i
   return true;
 }
 
-// ---- per-replica preparation: energies of this step, force scale ----------------------
-__global__ void k_prepare(DevPtrs P, IntConst c, int nrep) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nrep) return;
+// ---- per-replica preparation --------------------------------------------------------
+// force scale of replica r for this step: McMD weight (verlethe.f90:196-238) from the total
+// potential energy, or the pseudo-temperature factor (verlet.f90:118-142)
+__device__ double rep_scale(const DevPtrs& P, const IntConst& c, int r) {
   const Rep& R = P.reps[r];
-  double e[JP_MAXENE];
-  double tot = 0.0;
-  for (int k = 1; k < JP_MAXENE; ++k) {
-    e[k] = (double)P.ene_fix[r * 16 + k] * kEneInv;
-    if (k == JP_E_ELE15) e[k] += R.dself;
-    tot += e[k];
-  }
-  e[0] = tot;
-  const int h = P.step_ctr[1];
-  double* out = P.ene_hist + ((size_t)h * nrep + r) * JP_MAXENE;
-  for (int k = 0; k < JP_MAXENE; ++k) out[k] = e[k];
-  double s = 1.0;
   if (c.method == JP_METHOD_GE && R.ge_nwin > 0) {
-    // McMD weight (verlethe.f90:196-238)
+    double tot = R.dself;
+    for (int k = 1; k < JP_MAXENE; ++k) tot += (double)__ldcg(&P.ene_fix[r * 16 + k]) * kEneInv;
     double dprobl;
     if (tot <= R.ge_celw) dprobl = R.ge_alphalw;
     else if (tot >= R.ge_ceup) dprobl = R.ge_alphaup;
@@ -326,73 +358,164 @@ __global__ void k_prepare(DevPtrs P, IntConst c, int nrep) {
       dprobl = cc[0];
       for (int j = 1; j <= R.ge_ndeg; ++j) dprobl += cc[j] * pow(rt, (double)j);
     }
-    s = (kGas / kJouCal) * 1.0e-3 * R.ge_tempce * dprobl;
-  } else if (c.psetmp > 1.0e-10) {
-    s = c.temp / c.psetmp;
+    return (kGas / kJouCal) * 1.0e-3 * R.ge_tempce * dprobl;
   }
-  P.scale[r] = s;
+  if (c.psetmp > 1.0e-10) return c.temp / c.psetmp;
+  return 1.0;
 }
 
-// ---- METHOD= MICR: verlet.f90 fused with SHAKE, one thread per unit ---------------------
-template <bool FP64>
-__global__ void __launch_bounds__(64) k_micr(DevPtrs P, IntConst c, int nunit) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  double ke = 0.0;
-  int sub = -1;
-  if (t < nunit) {
-    const Unit u = P.units[t];
-    const Rep& R = P.reps[u.rep];
-    sub = u.sub;
-    const double s = P.scale[u.rep];
-    const double rt = -c.dt * kConvcv;
-    double x0[4][3], x1[4][3], vb[4][3], im[4];
-    JP_UNIT_LOOP(q) {
-      const int a = u.a[q];
-      double g[3];
-      load_grad<FP64>(P, a, s, g);
-      im[q] = P.imass[a];
-      for (int k = 0; k < 3; ++k) {
-        x0[q][k] = P.x[3 * a + k];
-        vb[q][k] = P.v[3 * a + k];
-        const double v = vb[q][k] + rt * g[k] * im[q];
-        x1[q][k] = x0[q][k] + c.dt * v;
-        P.v[3 * a + k] = v;
-      }
-    }
-    if (u.n >= 2 && c.shake_method != JP_SHAKE_NONE) {
-      const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
-      if (ier) shake_status(P, ier);
-      const double ri = 1.0 / c.dt;
-      JP_UNIT_LOOP(q)
-        for (int k = 0; k < 3; ++k) P.v[3 * u.a[q] + k] = (x1[q][k] - x0[q][k]) * ri;
-    }
-    bool bad = false;
-    JP_UNIT_LOOP(q) {
-      const int a = u.a[q];
-      double vv = 0.0;
-      for (int k = 0; k < 3; ++k) {
-        P.x[3 * a + k] = x1[q][k];
-        const double vm = 0.5 * (vb[q][k] + P.v[3 * a + k]);
-        vv += vm * vm;
-        bad |= !isfinite(x1[q][k]);
-      }
-      ke += P.mass[a] * vv;
-      write_slot(P, a, x1[q], FP64);
-    }
-    if (bad) atomicOr(P.status, ERR_NONFINITE);
+// energies of this step (time t) into the per-step history: eneval(15) of dnergy
+__device__ void write_ene_hist(const DevPtrs& P, const IntConst& c, int r) {
+  const Rep& R = P.reps[r];
+  double e[JP_MAXENE];
+  double tot = 0.0;
+  for (int k = 1; k < JP_MAXENE; ++k) {
+    e[k] = (double)__ldcg(&P.ene_fix[r * 16 + k]) * kEneInv;
+    if (k == JP_E_ELE15) e[k] += R.dself;
+    tot += e[k];
   }
-  if (__any_sync(0xffffffffu, t < nunit)) add_kin(P, c.nsub_total, c.nkin - 1, sub, ke);
+  e[0] = tot;
+  double* out = P.ene_hist + ((size_t)P.step_ctr[1] * c.nrep + r) * JP_MAXENE;
+  for (int k = 0; k < JP_MAXENE; ++k) out[k] = e[k];
+}
+
+// Grid barrier for a cooperative launch (all blocks co-resident).  bar[0] arrivals,
+// bar[1] generation, bar[2] abort.  The wait is bounded (~1 s of SM clock): on timeout the
+// kernel records ERR_TIMEOUT, raises abort and every block returns at its next barrier.
+constexpr long long kBarrierCycles = 2000000000LL;
+
+__device__ __forceinline__ bool grid_barrier(const DevPtrs& P) {
+  __shared__ int s_ok;
+  unsigned* bar = P.bar;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    volatile unsigned* vb = bar;
+    const unsigned gen = vb[1];
+    __threadfence();
+    if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+      atomicExch(&bar[0], 0u);
+      __threadfence();
+      atomicAdd(&bar[1], 1u);
+    } else {
+      const long long t0 = clock64();
+      while (vb[1] == gen) {
+        if (vb[2] != 0u) { ok = 0; break; }
+        if (clock64() - t0 > kBarrierCycles) {
+          atomicOr(P.status, ERR_TIMEOUT);
+          atomicExch(&bar[2], 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// end of step, block 0 after the final barrier: temperature of each replica (the kinetic
+// slot of the last SHAKE pass, i.e. of (v(t-dt/2)+v(t+dt/2))/2) and the step counters
+__device__ void finish_block(const DevPtrs& P, const IntConst& c, double tt) {
+  const int h = P.step_ctr[1];
+  for (int r = threadIdx.x; r < c.nrep; r += blockDim.x) {
+    const Rep& R = P.reps[r];
+    int ks = c.nkin - 1;   // MICR
+    if (c.method != JP_METHOD_MICR && c.shake_method != JP_SHAKE_NONE) {
+      int q = 1;
+      for (; q < c.icslop; ++q)
+        if (cano_conv(P, c, R, q, tt)) break;
+      ks = 2 * q - 1;
+    }
+    double ek = 0.0, nf = 0.0;
+    for (int s = R.sub0; s < R.sub0 + R.nsub; ++s) {
+      ek += (double)__ldcg(&P.kin_fix[(size_t)ks * c.nsub_total + s]) * kKinInv;
+      nf += P.nfr[s];
+    }
+    P.temp_hist[(size_t)h * c.nrep + r] =
+        (c.method == JP_METHOD_MICR || c.shake_method != JP_SHAKE_NONE) ? ek * 1.0e7 / (kGas * nf) : -1.0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    P.step_ctr[0] += 1;
+    P.step_ctr[1] += 1;
+  }
+}
+
+// ---- METHOD= MICR: verlet.f90 fused with SHAKE, one cooperative launch ------------------
+template <bool FP64>
+__device__ __forceinline__ double micr_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s) {
+  const Rep& R = P.reps[u.rep];
+  const double rt = -c.dt * kConvcv;
+  double x0[4][3], x1[4][3], vb[4][3], im[4];
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    double g[3];
+    load_grad<FP64>(P, a, s, g);
+    im[q] = P.imass[a];
+    for (int k = 0; k < 3; ++k) {
+      x0[q][k] = P.x[3 * a + k];
+      vb[q][k] = P.v[3 * a + k];
+      const double v = vb[q][k] + rt * g[k] * im[q];
+      x1[q][k] = x0[q][k] + c.dt * v;
+      P.v[3 * a + k] = v;
+    }
+  }
+  if (u.n >= 2 && c.shake_method != JP_SHAKE_NONE) {
+    const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
+    if (ier) shake_status(P, ier);
+    const double ri = 1.0 / c.dt;
+    JP_UNIT_LOOP(q)
+      for (int k = 0; k < 3; ++k) P.v[3 * u.a[q] + k] = (x1[q][k] - x0[q][k]) * ri;
+  }
+  bool bad = false;
+  double ke = 0.0;
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    double vv = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      P.x[3 * a + k] = x1[q][k];
+      const double vm = 0.5 * (vb[q][k] + P.v[3 * a + k]);
+      vv += vm * vm;
+      bad |= !isfinite(x1[q][k]);
+    }
+    ke += P.mass[a] * vv;
+    write_slot(P, a, x1[q], FP64);
+  }
+  if (bad) atomicOr(P.status, ERR_NONFINITE);
+  return ke;
+}
+
+template <bool FP64>
+__global__ void __launch_bounds__(64) k_micr_fused(DevPtrs P, IntConst c, int nunit) {
+  const int nthr = gridDim.x * blockDim.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gt < c.nrep) write_ene_hist(P, c, gt);
+  for (int base = 0; base < nunit; base += nthr) {
+    const int t = base + gt;
+    double ke = 0.0;
+    int sub = -1;
+    if (t < nunit) {
+      const Unit u = P.units[t];
+      sub = u.sub;
+      ke = micr_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
+    }
+    add_kin(P, c.nsub_total, c.nkin - 1, sub, ke);
+  }
+  if (!grid_barrier(P)) return;
+  if (blockIdx.x == 0) finish_block(P, c, c.temp);
 }
 
 // ---- METHOD= CANO / GE: verlethe.f90 ----------------------------------------------------
-// The step's phases are device functions over one unit; k_cano_fused runs them in one
-// cooperative launch, separated by grid barriers where a phase needs the kinetic-energy
-// sums of the previous one.
+// Streaming form: one unit's state lives in global memory between phases (any number of
+// units per thread; also used for 4-atom groups by the register-resident form).
 
 // phase 1 (verlethe.f90:380-398): back up x, v; velt = v - dt/2 c g/m; KE(velt) -> slot 0
 template <bool FP64>
-__device__ __forceinline__ double cano1_unit(const DevPtrs& P, const IntConst& c, const Unit& u) {
-  const double s = P.scale[u.rep];
+__device__ __noinline__ double cano1_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s) {
   const double rt = 0.5 * c.dt * kConvcv;
   double ke = 0.0;
   JP_UNIT_LOOP(q) {
@@ -415,8 +538,8 @@ __device__ __forceinline__ double cano1_unit(const DevPtrs& P, const IntConst& c
 
 // phase 2 (verlethe.f90:400-516): chi from slot 0; v = (2chi-1)v - chi dt c g/m; x += dt v
 template <bool FP64>
-__device__ __forceinline__ void cano2_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double tt) {
-  const double s = P.scale[u.rep];
+__device__ __noinline__ void cano2_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
+                                        double tt) {
   double tempc = c.temp;
   if (c.shake_method != JP_SHAKE_NONE) tempc = sub_temp(P, c, 0, u.sub);
   const double chi = sqrt(tt / tempc);
@@ -436,10 +559,10 @@ __device__ __forceinline__ void cano2_unit(const DevPtrs& P, const IntConst& c, 
   }
 }
 
-// phase 3 of iteration `it` (verlethe.f90:524-612): SHAKE, v = (x-x0)/dt,
-// velt = (vback+v)/2, KE(velt) -> slot 2*it-1
+// phase 3 of an iteration (verlethe.f90:524-612): SHAKE, v = (x-x0)/dt,
+// velt = (vback+v)/2, KE(velt)
 template <bool FP64>
-__device__ __forceinline__ double cano3_unit(const DevPtrs& P, const IntConst& c, const Unit& u) {
+__device__ __noinline__ double cano3_unit(const DevPtrs& P, const IntConst& c, const Unit& u) {
   const Rep& R = P.reps[u.rep];
   double x1[4][3], x0[4][3], im[4];
   JP_UNIT_LOOP(q) {
@@ -476,10 +599,9 @@ __device__ __forceinline__ double cano3_unit(const DevPtrs& P, const IntConst& c
   return ke;
 }
 
-// phase 4 (verlethe.f90:625-640): forcec += (x - xback)/dt^2; velt; KE -> slot 2*it
+// phase 4 (verlethe.f90:625-640): forcec += (x - xback)/dt^2; velt; KE
 template <bool FP64>
-__device__ __forceinline__ double cano4_unit(const DevPtrs& P, const IntConst& c, const Unit& u) {
-  const double s = P.scale[u.rep];
+__device__ __noinline__ double cano4_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s) {
   const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
   double ke = 0.0;
   JP_UNIT_LOOP(q) {
@@ -503,9 +625,8 @@ __device__ __forceinline__ double cano4_unit(const DevPtrs& P, const IntConst& c
 // phase 5 (verlethe.f90:641-718): chi from slot 2*it; v = chi dt (-c g/m + forcec) +
 // (2chi-1) vback; x = x0 + dt v
 template <bool FP64>
-__device__ __forceinline__ void cano5_unit(const DevPtrs& P, const IntConst& c, const Unit& u, int it,
-                                           double tt) {
-  const double s = P.scale[u.rep];
+__device__ __noinline__ void cano5_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
+                                        int it, double tt) {
   const double chi = sqrt(tt / sub_temp(P, c, 2 * it, u.sub));
   const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
   JP_UNIT_LOOP(q) {
@@ -522,145 +643,308 @@ __device__ __forceinline__ void cano5_unit(const DevPtrs& P, const IntConst& c, 
   }
 }
 
-// Grid barrier for a cooperative launch (all blocks co-resident).  bar[0] arrivals,
-// bar[1] generation, bar[2] abort.  The wait is bounded (~1 s of SM clock): on timeout the
-// kernel records ERR_TIMEOUT, raises abort and every block returns at its next barrier.
-constexpr long long kBarrierCycles = 2000000000LL;
+// Resident form: a 1-3 atom unit keeps its state through every phase of the step on chip:
+// positions x, x0, v(t-dt/2), forcec and the shift of the last SHAKE pass in shared memory
+// (component-major, 9 values per state per thread), scalars in registers.  v(t+dt/2) is
+// recomputed from x and x0 after each SHAKE pass; the scaled gradient is re-read (it is not
+// written during the step).
+constexpr int kIntThreads = 64;
 
-__device__ __forceinline__ bool grid_barrier(const DevPtrs& P) {
-  __shared__ int s_ok;
-  unsigned* bar = P.bar;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    volatile unsigned* vb = bar;
-    const unsigned gen = vb[1];
-    __threadfence();
-    if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
-      atomicExch(&bar[0], 0u);
-      __threadfence();
-      atomicAdd(&bar[1], 1u);
-    } else {
-      const long long t0 = clock64();
-      while (vb[1] == gen) {
-        if (vb[2] != 0u) { ok = 0; break; }
-        if (clock64() - t0 > kBarrierCycles) {
-          atomicOr(P.status, ERR_TIMEOUT);
-          atomicExch(&bar[2], 1u);
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
-      }
-    }
-    __threadfence();
-    s_ok = ok;
+struct UnitScal {
+  int n, sub, rep;
+  int a[3];
+  double d2[3], im[3], m[3];
+};
+
+struct UnitSmem {
+  double x[9][kIntThreads], x0[9][kIntThreads], vb[9][kIntThreads];
+  double dxs[9][kIntThreads], fc[9][kIntThreads];
+};
+
+template <bool FP64>
+__device__ __forceinline__ void ru_grad(const DevPtrs& P, const UnitScal& U, int q, double s, double* g) {
+  if (FP64) {
+    for (int k = 0; k < 3; ++k) g[k] = __ldg(&P.grd[3 * U.a[q] + k]) * s;
+  } else {
+    for (int k = 0; k < 3; ++k) g[k] = (double)__ldg(&P.frc[3 * U.a[q] + k]) * kFrcInv * s;
   }
-  __syncthreads();
-  return s_ok != 0;
 }
 
-// the whole SHAKE <-> thermostat step of verlethe for all replicas, one launch
+__device__ __forceinline__ void ru_load(const DevPtrs& P, const Unit& u, UnitScal& U, UnitSmem& S,
+                                        int tid) {
+  U.n = u.n; U.sub = u.sub; U.rep = u.rep;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    U.d2[q] = u.d2[q];
+    const bool on = q < u.n;
+    const int a = on ? u.a[q] : u.a[0];
+    U.a[q] = a;
+    U.im[q] = on ? P.imass[a] : 0.0;
+    U.m[q] = on ? P.mass[a] : 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      S.x[3 * q + k][tid] = P.x[3 * a + k];
+      S.vb[3 * q + k][tid] = P.v[3 * a + k];
+    }
+  }
+}
+
+// phase 1: x0 = x, KE of v(t-dt/2) - dt/2 c g/m
 template <bool FP64>
-__global__ void __launch_bounds__(64) k_cano_fused(DevPtrs P, IntConst c, int nunit) {
+__device__ __forceinline__ double ru_cano1(const DevPtrs& P, const IntConst& c, const UnitScal& U,
+                                           UnitSmem& S, int tid, double s) {
+  const double rt = 0.5 * c.dt * kConvcv;
+  double ke = 0.0;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double g[3];
+    ru_grad<FP64>(P, U, q, s, g);
+    double vv = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      S.x0[3 * q + k][tid] = S.x[3 * q + k][tid];
+      const double vt = S.vb[3 * q + k][tid] - rt * g[k] * U.im[q];
+      vv += vt * vt;
+    }
+    ke += U.m[q] * vv;
+  }
+  return ke;
+}
+
+// phase 3: SHAKE + KE of (v(t-dt/2) + v(t+dt/2))/2
+__device__ __forceinline__ double ru_cano3(const DevPtrs& P, const IntConst& c, const UnitScal& U,
+                                           UnitSmem& S, int tid) {
+  double x[3][3], x0[3][3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      x[q][k] = S.x[3 * q + k][tid];
+      x0[q][k] = S.x0[3 * q + k][tid];
+    }
+  if (U.n >= 2) {
+    const int ier = shake_small(P.reps[U.rep], U.n, U.d2, U.im, x, x0, c.shake_method,
+                                c.shake_tol, c.shake_maxit);
+    if (ier) shake_status(P, ier);
+  }
+  const double ri = 1.0 / c.dt;
+  double ke = 0.0;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double vv = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int i = 3 * q + k;
+      S.dxs[i][tid] = x[q][k] - S.x[i][tid];
+      S.x[i][tid] = x[q][k];
+      const double vt = 0.5 * (S.vb[i][tid] + (x[q][k] - x0[q][k]) * ri);
+      vv += vt * vt;
+    }
+    ke += U.m[q] * vv;
+  }
+  return ke;
+}
+
+// whole step for all replicas, one launch; units of 1-3 atoms held in registers when every
+// unit has its own thread (RESIDENT), else streamed through global memory
+template <bool FP64, bool RESIDENT>
+__global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst c, int nunit) {
   const int nthr = gridDim.x * blockDim.x;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
   const bool shk = c.shake_method != JP_SHAKE_NONE;
-  if (shk) {
-    for (int base = 0; base < nunit; base += nthr) {
-      const int t = base + gt;
+  if (gt < c.nrep) write_ene_hist(P, c, gt);
+  if (RESIDENT) {
+    // ---------------- one unit per thread --------------------------------------------
+    __shared__ UnitSmem S;
+    const int tid = threadIdx.x;
+    const bool have = gt < nunit;
+    Unit u;
+    u.n = 0; u.sub = -1; u.rep = 0;
+    if (have) u = P.units[gt];
+    const bool reg = have && u.n <= 3;
+    const double s = have ? rep_scale(P, c, u.rep) : 1.0;
+    UnitScal U;
+    if (reg) ru_load(P, u, U, S, tid);
+    const int sub = have ? u.sub : -1;
+    if (shk) {
       double ke = 0.0;
-      int sub = -1;
-      if (t < nunit) {
-        const Unit u = P.units[t];
-        sub = u.sub;
-        ke = cano1_unit<FP64>(P, c, u);
-      }
+      if (reg) ke = ru_cano1<FP64>(P, c, U, S, tid, s);
+      else if (have) ke = cano1_unit<FP64>(P, c, u, s);
       add_kin(P, c.nsub_total, 0, sub, ke);
+      if (!grid_barrier(P)) return;
     }
-    if (!grid_barrier(P)) return;
-  }
-  // phase 2, fused with phase 3 of the first iteration (both thread-local)
-  for (int base = 0; base < nunit; base += nthr) {
-    const int t = base + gt;
-    double ke = 0.0;
-    int sub = -1;
-    if (t < nunit) {
-      const Unit u = P.units[t];
-      cano2_unit<FP64>(P, c, u, tt);
-      if (shk) {
-        sub = u.sub;
-        ke = cano3_unit<FP64>(P, c, u);
+    // phase 2 (+ phase 3 of the first SHAKE pass)
+    {
+      double ke = 0.0;
+      if (reg) {
+        const double tempc = shk ? sub_temp(P, c, 0, U.sub) : c.temp;
+        const double chi = sqrt(tt / tempc);
+        const double a1 = chi * c.dt * kConvcv, b1 = 2.0 * chi - 1.0;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          double g[3];
+          ru_grad<FP64>(P, U, q, s, g);
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const int i = 3 * q + k;
+            const double v = b1 * S.vb[i][tid] - a1 * g[k] * U.im[q];
+            S.x[i][tid] += c.dt * v;
+            S.fc[i][tid] = 0.0;
+            if (!shk) S.dxs[i][tid] = v;   // no SHAKE: the new velocity, stored below
+          }
+        }
+        if (shk) ke = ru_cano3(P, c, U, S, tid);
+      } else if (have) {
+        cano2_unit<FP64>(P, c, u, s, tt);
+        if (shk) ke = cano3_unit<FP64>(P, c, u);
+      }
+      if (shk) add_kin(P, c.nsub_total, 1, sub, ke);
+    }
+    if (shk) {
+      for (int it = 1; it < c.icslop; ++it) {
+        if (!grid_barrier(P)) return;
+        const bool act = have && cano_active(P, c, P.reps[u.rep], it, true, tt);
+        double ke = 0.0;
+        if (act) {   // phase 4
+          if (reg) {
+            const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              double g[3];
+              ru_grad<FP64>(P, U, q, s, g);
+              double vv = 0.0;
+#pragma unroll
+              for (int k = 0; k < 3; ++k) {
+                const int i = 3 * q + k;
+                const double fc = S.fc[i][tid] + r2 * S.dxs[i][tid];
+                S.fc[i][tid] = fc;
+                const double vt = h * (-kConvcv * g[k] * U.im[q] + fc) + S.vb[i][tid];
+                vv += vt * vt;
+              }
+              ke += U.m[q] * vv;
+            }
+          } else {
+            ke = cano4_unit<FP64>(P, c, u, s);
+          }
+        }
+        add_kin(P, c.nsub_total, 2 * it, act ? sub : -1, ke);
+        if (!grid_barrier(P)) return;
+        ke = 0.0;
+        if (act) {   // phase 5 + phase 3 of the next pass
+          if (reg) {
+            const double chi = sqrt(tt / sub_temp(P, c, 2 * it, U.sub));
+            const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              double g[3];
+              ru_grad<FP64>(P, U, q, s, g);
+#pragma unroll
+              for (int k = 0; k < 3; ++k) {
+                const int i = 3 * q + k;
+                const double v = (-kConvcv * g[k] * U.im[q] + S.fc[i][tid]) * a1 + S.vb[i][tid] * b1;
+                S.x[i][tid] = S.x0[i][tid] + c.dt * v;
+              }
+            }
+            ke = ru_cano3(P, c, U, S, tid);
+          } else {
+            cano5_unit<FP64>(P, c, u, s, it, tt);
+            ke = cano3_unit<FP64>(P, c, u);
+          }
+        }
+        add_kin(P, c.nsub_total, 2 * it + 1, act ? sub : -1, ke);
       }
     }
-    if (shk) add_kin(P, c.nsub_total, 1, sub, ke);
-  }
-  if (!shk) return;
-  for (int it = 1; it < c.icslop; ++it) {
-    if (!grid_barrier(P)) return;
-    // phase 4 of `it` for replicas still iterating
-    for (int base = 0; base < nunit; base += nthr) {
-      const int t = base + gt;
-      double ke = 0.0;
-      int sub = -1;
-      if (t < nunit) {
-        const Unit u = P.units[t];
-        if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
-          sub = u.sub;
-          ke = cano4_unit<FP64>(P, c, u);
+    if (reg) {   // the unit's new state back to memory
+      bool bad = false;
+      const double ri = 1.0 / c.dt;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        if (q < U.n) {
+          const int a = U.a[q];
+          double xq[3];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const int i = 3 * q + k;
+            xq[k] = S.x[i][tid];
+            P.x[3 * a + k] = xq[k];
+            P.v[3 * a + k] = shk ? (xq[k] - S.x0[i][tid]) * ri : S.dxs[i][tid];
+            bad |= !isfinite(xq[k]);
+          }
+          write_slot(P, a, xq, FP64);
         }
       }
-      add_kin(P, c.nsub_total, 2 * it, sub, ke);
+      if (bad) atomicOr(P.status, ERR_NONFINITE);
     }
-    if (!grid_barrier(P)) return;
-    // phase 5 of `it` fused with phase 3 of it+1
+  } else {
+    // ---------------- streaming: grid-stride over units ------------------------------
+    if (shk) {
+      for (int base = 0; base < nunit; base += nthr) {
+        const int t = base + gt;
+        double ke = 0.0;
+        int sub = -1;
+        if (t < nunit) {
+          const Unit u = P.units[t];
+          sub = u.sub;
+          ke = cano1_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
+        }
+        add_kin(P, c.nsub_total, 0, sub, ke);
+      }
+      if (!grid_barrier(P)) return;
+    }
     for (int base = 0; base < nunit; base += nthr) {
       const int t = base + gt;
       double ke = 0.0;
       int sub = -1;
       if (t < nunit) {
         const Unit u = P.units[t];
-        if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
-          cano5_unit<FP64>(P, c, u, it, tt);
+        cano2_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), tt);
+        if (shk) {
           sub = u.sub;
           ke = cano3_unit<FP64>(P, c, u);
         }
       }
-      add_kin(P, c.nsub_total, 2 * it + 1, sub, ke);
+      if (shk) add_kin(P, c.nsub_total, 1, sub, ke);
+    }
+    if (shk) {
+      for (int it = 1; it < c.icslop; ++it) {
+        if (!grid_barrier(P)) return;
+        for (int base = 0; base < nunit; base += nthr) {
+          const int t = base + gt;
+          double ke = 0.0;
+          int sub = -1;
+          if (t < nunit) {
+            const Unit u = P.units[t];
+            if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+              sub = u.sub;
+              ke = cano4_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
+            }
+          }
+          add_kin(P, c.nsub_total, 2 * it, sub, ke);
+        }
+        if (!grid_barrier(P)) return;
+        for (int base = 0; base < nunit; base += nthr) {
+          const int t = base + gt;
+          double ke = 0.0;
+          int sub = -1;
+          if (t < nunit) {
+            const Unit u = P.units[t];
+            if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+              cano5_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
+              sub = u.sub;
+              ke = cano3_unit<FP64>(P, c, u);
+            }
+          }
+          add_kin(P, c.nsub_total, 2 * it + 1, sub, ke);
+        }
+      }
     }
   }
+  if (!grid_barrier(P)) return;
+  if (blockIdx.x == 0) finish_block(P, c, tt);
 }
 
-// ---- end of step: temperatures, counters --------------------------------------------------
-__global__ void k_finish(DevPtrs P, IntConst c, int nrep) {
-  const int h = P.step_ctr[1];
-  for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
-    const Rep& R = P.reps[r];
-    int ks = c.nkin - 1;   // MICR: KE of (v(t-dt/2)+v(t+dt/2))/2
-    if (c.method != JP_METHOD_MICR && c.shake_method != JP_SHAKE_NONE) {
-      const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
-      int q = 1;
-      for (; q < c.icslop; ++q)
-        if (cano_conv(P, c, R, q, tt)) break;
-      ks = 2 * q - 1;
-    }
-    double ek = 0.0, nf = 0.0;
-    for (int s = R.sub0; s < R.sub0 + R.nsub; ++s) {
-      ek += (double)P.kin_fix[(size_t)ks * c.nsub_total + s] * kKinInv;
-      nf += P.nfr[s];
-    }
-    P.temp_hist[(size_t)h * nrep + r] = (c.method == JP_METHOD_MICR || c.shake_method != JP_SHAKE_NONE)
-                                            ? ek * 1.0e7 / (kGas * nf) : -1.0;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    P.step_ctr[0] += 1;
-    P.step_ctr[1] += 1;
-  }
-}
-
-// ---- standalone SHAKE (test hook): r1 constrained against r2, positions in x / x0 -------
+// ---- standalone SHAKE (test hook): r1 constrained against r2, positions in xback / x0 -----
 __global__ void k_shake_only(DevPtrs P, IntConst c, int unit0, int nunit) {
   const int tt = blockIdx.x * blockDim.x + threadIdx.x;
   if (tt >= nunit) return;
@@ -683,29 +967,32 @@ __global__ void k_shake_only(DevPtrs P, IntConst c, int unit0, int nunit) {
     for (int k = 0; k < 3; ++k) P.xback[3 * u.a[q] + k] = x1[q][k];
 }
 
-void launch_prepare(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t st) {
-  k_prepare<<<(nrep + 127) / 128, 128, 0, st>>>(P, c, nrep);
-}
-
-void launch_micr(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, cudaStream_t st) {
-  const int nb = (nunit + 63) / 64;
-  if (fp64) k_micr<true><<<nb, 64, 0, st>>>(P, c, nunit);
-  else k_micr<false><<<nb, 64, 0, st>>>(P, c, nunit);
-}
-
-int cano_grid(bool fp64, int device) {
+// ---- launches -----------------------------------------------------------------------------
+template <class K>
+static int coop_grid(K kernel, int device) {
   int nsm = 0, per = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  if (fp64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cano_fused<true>, 64, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cano_fused<false>, 64, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 64, 0);
   return nsm * (per > 0 ? per : 1);
 }
 
-void launch_cano(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
-                 cudaStream_t st) {
-  cudaMemsetAsync(P.bar, 0, sizeof(unsigned) * 4, st);
-  const int want = (nunit + 63) / 64;
-  const int grid = want < grid_max ? (want > 0 ? want : 1) : grid_max;
+int cano_grid(bool fp64, int device) {
+  // the smallest co-resident grid among the integration kernels of this precision
+  int g;
+  if (fp64) {
+    g = coop_grid(k_cano_fused<true, true>, device);
+    g = std::min(g, coop_grid(k_cano_fused<true, false>, device));
+    g = std::min(g, coop_grid(k_micr_fused<true>, device));
+  } else {
+    g = coop_grid(k_cano_fused<false, true>, device);
+    g = std::min(g, coop_grid(k_cano_fused<false, false>, device));
+    g = std::min(g, coop_grid(k_micr_fused<false>, device));
+  }
+  return g;
+}
+
+template <class... Args>
+static void coop_launch(void (*kernel)(Args...), int grid, cudaStream_t st, Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(64);
@@ -716,12 +1003,25 @@ void launch_cano(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int 
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (fp64) cudaLaunchKernelEx(&cfg, k_cano_fused<true>, P, c, nunit);
-  else cudaLaunchKernelEx(&cfg, k_cano_fused<false>, P, c, nunit);
+  cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-void launch_finish(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t st) {
-  k_finish<<<1, 1024, 0, st>>>(P, c, nrep);
+void launch_integrate(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
+                      cudaStream_t st) {
+  cudaMemsetAsync(P.bar, 0, sizeof(unsigned) * 4, st);
+  const int want = std::max(1, (nunit + 63) / 64);
+  const int grid = std::min(want, grid_max);
+  const bool resident = want <= grid_max;
+  if (c.method == JP_METHOD_MICR) {
+    if (fp64) coop_launch(k_micr_fused<true>, grid, st, P, c, nunit);
+    else coop_launch(k_micr_fused<false>, grid, st, P, c, nunit);
+  } else if (resident) {
+    if (fp64) coop_launch(k_cano_fused<true, true>, grid, st, P, c, nunit);
+    else coop_launch(k_cano_fused<false, true>, grid, st, P, c, nunit);
+  } else {
+    if (fp64) coop_launch(k_cano_fused<true, false>, grid, st, P, c, nunit);
+    else coop_launch(k_cano_fused<false, false>, grid, st, P, c, nunit);
+  }
 }
 
 void launch_shake_only(const DevPtrs& P, const IntConst& c, int unit0, int nunit, cudaStream_t st) {

@@ -52,12 +52,11 @@ struct IntConst {
   int natom;
   int nkin;                // kinetic-sum slots; the last one is MICR's
 };
-void launch_prepare(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t st);
-void launch_micr(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, cudaStream_t st);
-int cano_grid(bool fp64, int device);   // co-resident blocks of the fused CANO kernel
-void launch_cano(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
-                 cudaStream_t st);
-void launch_finish(const DevPtrs& P, const IntConst& c, int nrep, cudaStream_t st);
+int cano_grid(bool fp64, int device);   // co-resident blocks of the integration kernels
+// one cooperative launch: energies of the step, force scale, verlet (MICR) or verlethe
+// (CANO/GE) with SHAKE, temperatures and step counters
+void launch_integrate(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
+                      cudaStream_t st);
 void launch_shake_only(const DevPtrs& P, const IntConst& c, int unit0, int nunit, cudaStream_t st);
 
 }  // namespace jp

@@ -16,6 +16,7 @@ WORKLOADS = {
     "c2": systems.config_c2,
     "c3": systems.config_c3,
     "small": lambda: systems.solvated_polymer(6, 700, seed=11),
+    "w7000": lambda: systems.water_box(7000, 62.0, seed=9),
 }
 
 
@@ -26,12 +27,13 @@ def main():
     ap.add_argument("--method", default="cano", choices=["micr", "cano"])
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--direct", action="store_true")
+    ap.add_argument("--tempco", type=int, default=2, choices=[1, 2])
     a = ap.parse_args()
     build.build()
     top = WORKLOADS[a.workload]()
     prec = abi.JP_PREC_MIXED if a.precision == "mixed" else abi.JP_PREC_FP64
     meth = abi.JP_METHOD_CANO if a.method == "cano" else abi.JP_METHOD_MICR
-    with engine.Engine(top, precision=prec, method=meth) as e:
+    with engine.Engine(top, precision=prec, method=meth, tempco=a.tempco) as e:
         e.set_timing(a.direct)
         e.step(a.steps, energies=False, temps=False)
         tot, ph, ln = e.last_timing()
