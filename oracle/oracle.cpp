@@ -6,9 +6,10 @@
 //
 // Every routine cites the md_run source (src_md_run/<file>:<line>) it follows.  The
 // reference itself cannot be compiled in this environment (no Fortran compiler), and the
-// reference ships no tests or golden vectors, so the oracle is pinned by hand-derived
-// known-answer tests under tests/golden/ and by analytic identities (finite-difference
-// gradients, energy conservation); see DESIGN.md "parity pinning".
+// reference ships no tests or golden vectors, so parity against the reference is
+// unpinned: the oracle is checked against known-answer vectors derived independently from
+// the closed-form formulas (tests/golden/) and against analytic identities
+// (finite-difference gradients, energy conservation, constraint satisfaction).
 //
 // Build: oracle/Makefile -> oracle/liboracle.so (C ABI, see or_* below).
 
