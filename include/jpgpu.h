@@ -4,7 +4,8 @@
  * The reference (j_presto md_run, Fortran 90 + OpenMP) has no plugin or FFI layer: its
  * routines share state through modules.  Each entry point below replaces one reference call
  * site, named in its comment as file:line inside src_md_run/.  A Fortran driver binds these
- * through iso_c_binding; the bundled Python/ctypes host does the same.
+ * through iso_c_binding (a bind(C) interface per entry point); the bundled Python/ctypes
+ * host does the same.
  *
  * Conventions
  *   - Units follow md_run: Angstrom, fs, amu, kcal/mol, e.  Velocities in Angstrom/fs.
@@ -56,7 +57,8 @@ enum {
   JP_E_FIXED_OVERFLOW = -201,     /* a force contribution left the 64-bit fixed-point range */
   JP_E_CUDA = -300,               /* CUDA runtime error */
   JP_E_NO_DEVICE = -301,
-  JP_E_TIMEOUT = -302             /* a bounded device wait ran out */
+  JP_E_TIMEOUT = -302,            /* a bounded device wait ran out */
+  JP_E_NOALLOC_LIMIT = -110       /* natom above JP_NOALLOC_MAX_ATOMS (jp_nonbond_noalloc) */
 };
 
 /* Generalized-ensemble weight (.nf file, md_run inmcmd.f90:22-40; verlethe.f90:196-321). */
@@ -198,6 +200,38 @@ int jp_calibrate_fp32(int32_t device, double *tflops);
 
 const char *jp_strerror(int code);
 void jp_destroy(jp_ctx *ctx);
+
+/* Largest system jp_nonbond_noalloc accepts: its static scratch array holds
+ * 32 + 3 * JP_NOALLOC_MAX_ATOMS doubles (384.25 KiB) on each device. */
+#define JP_NOALLOC_MAX_ATOMS 16384
+
+/* No counterpart in the reference: an entry point that allocates no device memory, for
+ * callers that cannot allocate.  The ZD + LJ non-bonded part of dnergy -- the pair terms
+ * within `cutoff` under the minimum image, the ZD excess of every excluded pair and the ZD
+ * self term -- of ONE system given entirely in caller-owned DEVICE buffers, by an
+ * O(N^2) all-pairs variant of the FP64 tile kernel (no pair list).
+ *   cord[natom][3], charge[natom] (e), atype[natom], c6/c12[ntype][ntype] as in jp_system,
+ *   excl_ptr[natom+1] / excl_idx: symmetric exclusion CSR as in jp_system (the ZD excess
+ *   is applied to each excluded pair once), index_base 0 or 1 for atype and excl_idx;
+ *   box[3] is a HOST array, each edge > 2 * cutoff.
+ *   Outputs (device): grad[natom][3] = dE/dx; ene[0] = ZD Coulomb (jp_energy_grad's
+ *   JP_E_ELE15 slot, self term included), ene[1] = LJ (JP_E_VDW15).
+ *   stream: a cudaStream_t of the current device (NULL = legacy default stream).
+ * Work runs on `stream` in the current device's context; the call returns after it has
+ * finished.  natom > JP_NOALLOC_MAX_ATOMS returns JP_E_NOALLOC_LIMIT before any device
+ * work; an atom or type index out of range returns JP_E_INVALID, a non-finite result
+ * JP_E_NONFINITE.
+ * Scratch: one static device array shared by every call on a device; each call clears it
+ * on `stream` first.  Calls whose device work overlaps (different streams or host threads
+ * on one device) race on it and corrupt each other's results: serialise them.  The first
+ * call on each device looks up that device's copy of the array (cudaGetSymbolAddress,
+ * which may load the library's module); make that first call before any stream capture.
+ * Calls no cudaMalloc, cudaFree or other allocating routine. */
+int jp_nonbond_noalloc(int32_t natom, const double *cord, const double *charge,
+                       const int32_t *atype, int32_t ntype, const double *c6, const double *c12,
+                       const int32_t *excl_ptr, const int32_t *excl_idx, int32_t index_base,
+                       const double box[3], double cutoff, double dielectric, double *grad,
+                       double *ene, void *stream);
 
 #ifdef __cplusplus
 }

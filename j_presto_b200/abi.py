@@ -21,6 +21,8 @@ JP_E_LIST_OVERFLOW = -151
 JP_E_NONFINITE = -200
 JP_E_CUDA = -300
 JP_E_NO_DEVICE = -301
+JP_E_NOALLOC_LIMIT = -110
+JP_NOALLOC_MAX_ATOMS = 16384
 
 # energy slot names (md_run main.f90:157-159 cyenam order)
 ENERGY_NAMES = ["TOTAL", "BOND", "ANGLE", "TORSION", "IMPROPER", "VDW14", "ELEC14",

@@ -14,7 +14,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libjpgpu.so")
-SOURCES = ["jp_cells.cu", "jp_pair.cu", "jp_bonded.cu", "jp_integrate.cu", "jp_calib.cu", "jp_abi.cu"]
+SOURCES = ["jp_cells.cu", "jp_pair.cu", "jp_bonded.cu", "jp_integrate.cu", "jp_calib.cu", "jp_abi.cu",
+           "jp_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

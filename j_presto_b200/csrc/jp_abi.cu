@@ -295,6 +295,7 @@ const char *jp_strerror(int code) {
     case JP_E_CUDA: return g_last_err;
     case JP_E_NO_DEVICE: return "no CUDA device";
     case JP_E_TIMEOUT: return "device wait timed out";
+    case JP_E_NOALLOC_LIMIT: return "natom above JP_NOALLOC_MAX_ATOMS, the static scratch size";
     default: return "unknown error";
   }
 }

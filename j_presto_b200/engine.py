@@ -20,7 +20,7 @@ _lib = None
 EXPORTS = ["jp_default_params", "jp_create", "jp_rebuild_cells", "jp_energy_grad", "jp_step",
            "jp_shake", "jp_get_state", "jp_set_state", "jp_pair_count", "jp_set_timing",
            "jp_last_timing", "jp_launch_counts", "jp_list_stats", "jp_calibrate_fp32",
-           "jp_strerror", "jp_destroy"]
+           "jp_strerror", "jp_destroy", "jp_nonbond_noalloc"]
 
 
 class JpError(RuntimeError):
@@ -58,6 +58,9 @@ def lib():
         L.jp_strerror.restype = C.c_char_p
         L.jp_destroy.argtypes = [vp]
         L.jp_destroy.restype = None
+        # all array arguments are device addresses except box (host double[3])
+        L.jp_nonbond_noalloc.argtypes = [ip, vp, vp, vp, ip, vp, vp, vp, vp, ip, dp, C.c_double,
+                                         C.c_double, vp, vp, vp]
         _lib = L
     return _lib
 
