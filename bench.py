@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload: the solvated-polymer system (159-residue chain + 7,000 waters + ions, 22,784
+Workload: the solvated-polymer system (159-residue chain + 7,000 waters + ions, 22,860
 atoms, 62 A cubic PBC cell, zero-dipole cut-off 12 A, SHAKE on X-H and rigid waters,
 METHOD= CANO at 300 K, 2 fs), synthetic and seeded.  One step = one md_run MD step
 (forces, Hoover-Evans thermostat with the SHAKE<->thermostat loop, SHAKE) with the pair
@@ -39,7 +39,11 @@ METRIC = "aggregate ns/day & pairs/s: mixed vs FP64 GPU path at ≤1e-5 RMS forc
 DT_FS = 2.0
 FLOPS_PER_PAIR = 52          # FP32 flops per pair interaction within rc (FMA = 2)
 L2_FLUSH_BYTES = 256 << 20   # > 126 MB L2
-WORKLOAD = ("solvated polymer: 159-residue chain + 7,000 waters + Na+/Cl-, 22,784 atoms, "
+PAIR_PROFILE = os.path.join(ROOT, "profiles", "k_pair_mixed_c2.md")
+
+
+def workload_name(natom):
+    return (f"solvated polymer: 159-residue chain + 7,000 waters + Na+/Cl-, {natom:,} atoms, "
             "62 A cubic PBC, ZD cut-off 12 A (list 13.5 A, UPDATE 10), SHAKE X-H + rigid "
             "water, METHOD= CANO 300 K, dt 2 fs")
 
@@ -95,10 +99,11 @@ class Clocks:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+        time.sleep(0.5)          # nvidia-smi start-up, so that sampling covers the region
         return self
 
     def __exit__(self, *a):
@@ -132,12 +137,18 @@ class Clocks:
 
 
 def ncu_traffic():
-    """Per-launch DRAM bytes of the pair kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "pair_mixed_c2.json")
-    if os.path.exists(p):
-        d = json.load(open(p))
-        return d.get("dram_bytes_per_launch"), d.get("source")
+    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the pair
+    kernel, from the committed ncu summary's `dram_bytes_per_launch:` line."""
+    if os.path.exists(PAIR_PROFILE):
+        for line in open(PAIR_PROFILE):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0]), os.path.relpath(PAIR_PROFILE, ROOT)
     return None, None
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    return json.load(open(p)) if os.path.exists(p) else {}
 
 
 def cpu_baseline(top, budget_s=15.0):
@@ -184,7 +195,7 @@ def run_reference(args, rank):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ns/day", "n_gpus": args.gpus,
             "steps": done, "warmup": w, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "atoms": int(top["natom"])},
+            "config": {"workload": workload_name(int(top["natom"])), "atoms": int(top["natom"])},
             "cpu_baseline": {"value": v, "unit": "ns/day", "cores": nth, "kind": "port",
                              "sample": f"{done} CANO steps, oracle/oracle.cpp OpenMP FP64 "
                                        "(md_run itself needs a Fortran compiler, absent)"},
@@ -207,7 +218,7 @@ def timed_loop(eng, steps, flush_buf):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
@@ -285,6 +296,7 @@ def main():
     peak = engine.calibrate_fp32(dev)
     achieved = FLOPS_PER_PAIR * pairs / (pair_ms * 1e-3) / 1e12
     traffic, tsrc = ncu_traffic()
+    hbm_peak = measured_peaks().get("hbm_gbs")
     cpu = None if args.no_cpu else cpu_baseline(top)
     clocks = clk.summary()
     nreb = args.steps // 10
@@ -292,7 +304,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "atoms": int(n), "precision": "FP32 pair arithmetic, "
+        "config": {"workload": workload_name(int(n)), "atoms": int(n), "precision": "FP32 pair arithmetic, "
                    "64-bit fixed-point force/energy accumulation, FP64 integrate+SHAKE",
                    "l2": "flushed (256 MB write) between timed steps", "replicas_per_gpu": 1,
                    "parallelism": f"replicas x{world}"},
@@ -314,6 +326,10 @@ def main():
         "roofline": {"bound": "fp32", "kernel": "k_pair_mixed", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": traffic, "traffic_source": tsrc,
+                     "hbm": None if traffic is None or not hbm_peak else
+                     {"achieved_gbs": traffic / (pair_ms * 1e-3) / 1e9, "peak_gbs": hbm_peak,
+                      "frac": traffic / (pair_ms * 1e-3) / 1e9 / hbm_peak,
+                      "note": "ncu DRAM bytes per launch / CUDA-event launch time, of measured"},
                      "note": f"{FLOPS_PER_PAIR} FP32 flops per pair within rc x pairs per launch / "
                              "CUDA-event launch time; peak = FP32 FMA loop measured in this run "
                              "(MEASURED_PEAKS.json lists HBM and bf16 tensor peaks only)"},

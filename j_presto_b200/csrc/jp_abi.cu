@@ -167,8 +167,7 @@ void enqueue_integrate(jp_ctx *c) {
 int launches_per_step(const jp_ctx *c) {
   int n = 1;                       // pair
   n += c->nterm > 0 ? 1 : 0;      // bonded
-  n += 2;                          // prepare + finish
-  n += 1;                          // k_micr or the fused cooperative CANO/GE kernel
+  n += 1;                          // the fused cooperative MICR or CANO/GE kernel
   return n;
 }
 

@@ -76,35 +76,30 @@ def _perp(v, rng):
 
 
 def _serpentine(npts, step, lo, hi, rowgap):
-    """Points along a boustrophedon path inside the box [lo, hi]^3, spaced `step`."""
-    span = hi - lo
-    nrow_y = max(1, int(span // rowgap))
-    pts = []
-    x_dir, y_i, z_i = 1, 0, 0
-    x = lo
-    y = lo + 0.5 * rowgap
-    z = lo + 0.5 * rowgap
-    while len(pts) < npts:
-        pts.append((x, y, z))
-        nx = x + x_dir * step
-        if lo <= nx <= hi:
-            x = nx
-            continue
-        # turn: move along y by rowgap (sampled at `step`)
-        x_dir = -x_dir
-        ny = y + rowgap
-        if ny > hi:
-            ny = lo + 0.5 * rowgap
-            z += rowgap
-            if z > hi:
-                raise ValueError("polymer does not fit in the box")
-        nseg = max(1, int(round(abs(ny - y) / step)))
-        for s in range(1, nseg):
-            if len(pts) >= npts:
-                break
-            pts.append((x, y + (ny - y) * s / nseg, z))
-        y = ny
-    return np.array(pts[:npts])
+    """`npts` points spaced `step` (arc length) along a 3-D boustrophedon inside the box
+    [lo, hi]^3: rows along x, stepped by `rowgap` in y, layers stepped by `rowgap` in z,
+    the y order reversed on every other layer so each turn is one short straight leg."""
+    nrow = max(1, int((hi - lo) // rowgap))
+    rows = lo + 0.5 * rowgap + rowgap * np.arange(nrow)
+    way = []
+    k = 0
+    for iz, z in enumerate(rows):
+        for y in (rows if iz % 2 == 0 else rows[::-1]):
+            xa, xb = (lo, hi) if k % 2 == 0 else (hi, lo)
+            way += [(xa, y, z), (xb, y, z)]
+            k += 1
+    way = np.array(way, float)
+    seg = np.diff(way, axis=0)
+    slen = np.linalg.norm(seg, axis=1)
+    keep = slen > 1e-9
+    seg, slen, base = seg[keep], slen[keep], way[:-1][keep]
+    cum = np.concatenate([[0.0], np.cumsum(slen)])
+    s_at = step * np.arange(npts)
+    if s_at[-1] > cum[-1]:
+        raise ValueError("polymer does not fit in the box")
+    i = np.minimum(np.searchsorted(cum, s_at, side="right") - 1, len(slen) - 1)
+    t = (s_at - cum[i]) / slen[i]
+    return base[i] + t[:, None] * seg[i]
 
 
 def _build_polymer(top, nres, lo, hi, rng, box):
@@ -231,11 +226,13 @@ def _build_polymer(top, nres, lo, hi, rng, box):
     return res
 
 
-def _relax_solute(top, first, last, box, iters=400):
-    """Position-based clash relief of the solute: bonds keep their built lengths, 1-3
-    pairs are kept at >= 2.1 A (>= 1.6 A between hydrogens) and every other pair at
+def _relax_solute(top, first, last, box, iters=3000):
+    """Position-based relaxation of the solute: bonds keep their built lengths, every 1-3
+    pair is pulled to the distance of an ideal valence angle at its centre (120 deg at N
+    and at the carbonyl C, 109.47 deg elsewhere), and every other pair is kept at
     >= 2.9 A between heavy atoms, >= 2.3 A with a hydrogen.  Bonded equilibrium values are
-    taken from the relaxed geometry afterwards, so the start carries no bonded strain."""
+    taken from the relaxed geometry afterwards, so the start carries no bonded strain and
+    no angle sits near 180 deg (where torsion gradients are singular)."""
     n = last - first
     if n < 2:
         return
@@ -244,17 +241,28 @@ def _relax_solute(top, first, last, box, iters=400):
     bonds = np.array([(a - first, b - first) for a, b in top.bonds
                       if first <= a < last and first <= b < last], int).reshape(-1, 2)
     L0 = np.linalg.norm(X[bonds[:, 0]] - X[bonds[:, 1]], axis=1)
+    # heavy-atom bonds of the path's corners come out stretched or squeezed
+    heavy_bond = ~isH[bonds[:, 0]] & ~isH[bonds[:, 1]]
+    L0 = np.where(heavy_bond, np.clip(L0, 1.33, 1.53), L0)
     nbr = [set() for _ in range(n)]
     for a, b in bonds:
         nbr[a].add(b); nbr[b].add(a)
-    p13 = set()
+    blen = {}
+    for (a, b), l0 in zip(bonds, L0):
+        blen[(a, b)] = blen[(b, a)] = l0
+    typ = [top.typ[first + i] for i in range(n)]
+    sp2 = [typ[j] == T_N or (typ[j] == T_C and any(typ[b] == T_O for b in nbr[j]))
+           for j in range(n)]
+    t13 = {}
     for j in range(n):
         nb = sorted(nbr[j])
+        c = math.cos(math.radians(120.0 if sp2[j] else 109.47))
         for x in range(len(nb)):
             for y in range(x + 1, len(nb)):
-                p13.add((nb[x], nb[y]))
-    p13 = np.array(sorted(p13), int).reshape(-1, 2)
-    d13 = np.where(isH[p13[:, 0]] & isH[p13[:, 1]], 1.6, 2.1) if len(p13) else np.zeros(0)
+                la, lc = blen[(nb[x], j)], blen[(nb[y], j)]
+                t13[(nb[x], nb[y])] = math.sqrt(la * la + lc * lc - 2.0 * la * lc * c)
+    p13 = np.array(sorted(t13), int).reshape(-1, 2)
+    d13 = np.array([t13[tuple(k)] for k in p13]) if len(p13) else np.zeros(0)
     from scipy.spatial import cKDTree
     ex_codes = np.unique(np.concatenate([np.minimum(bonds[:, 0], bonds[:, 1]) * n + np.maximum(bonds[:, 0], bonds[:, 1]),
                                          np.minimum(p13[:, 0], p13[:, 1]) * n + np.maximum(p13[:, 0], p13[:, 1])]))
@@ -282,15 +290,15 @@ def _relax_solute(top, first, last, box, iters=400):
             f = (0.5 * (dmin[bad] - r[bad]) / np.maximum(r[bad], 1e-6))[:, None] * d[bad]
             np.add.at(X, iu[bad], 0.5 * f)
             np.add.at(X, ju[bad], -0.5 * f)
-        # 1-3 minimum distances
+        # 1-3 distances of the ideal valence angles
         if len(p13):
             d = X[p13[:, 0]] - X[p13[:, 1]]
             d -= box * np.round(d / box)
             r = np.linalg.norm(d, axis=1)
-            bad = r < d13
+            bad = np.abs(r - d13) > 1e-3
             if bad.any():
                 moved = True
-                f = (0.5 * (d13[bad] - r[bad]) / np.maximum(r[bad], 1e-6))[:, None] * d[bad]
+                f = (0.25 * (d13[bad] - r[bad]) / np.maximum(r[bad], 1e-6))[:, None] * d[bad]
                 np.add.at(X, p13[bad, 0], f)
                 np.add.at(X, p13[bad, 1], -f)
         # bond lengths
