@@ -631,6 +631,10 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.rep_hmax, 3 * (size_t)nrep);
   e |= dalloc(c, &P.sorted, (size_t)N);
   e |= dput(c, &P.units, units);
+  std::vector<int> small_idx, quad_idx;
+  for (int i = 0; i < (int)units.size(); ++i) (units[i].n == 4 ? quad_idx : small_idx).push_back(i);
+  e |= dput(c, &P.small_idx, small_idx);
+  e |= dput(c, &P.quad_idx, quad_idx);
   e |= dput(c, &P.terms, terms);
   e |= dput(c, &P.reps, reps);
   e |= dput(c, &P.ge_coef, hge);
@@ -675,6 +679,10 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   ic.nsub_total = c->nsub;
   ic.natom = N;
   ic.nkin = c->nkin;
+  ic.nsmall = (int)small_idx.size();
+  ic.nquad = (int)quad_idx.size();
+  ic.qbase = (ic.nsmall + 31) / 32 * 32;
+  ic.nvirt = ic.qbase + (8 * ic.nquad + 31) / 32 * 32;
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   c->pair_warps = std::max(1, nsm) * 8 * 6;   // 6 blocks of 8 warps per SM

@@ -112,6 +112,7 @@ struct DevPtrs {
   float *rep_hmax;                // largest block half-extent per replica [nrep][3]
   // units / terms
   Unit *units;
+  int *small_idx, *quad_idx;      // units of 1-3 atoms / of 4 atoms, in unit order
   Term *terms;
   // replicas
   Rep *reps;

@@ -379,35 +379,30 @@ __device__ void write_ene_hist(const DevPtrs& P, const IntConst& c, int r) {
   for (int k = 0; k < JP_MAXENE; ++k) out[k] = e[k];
 }
 
-// Grid barrier for a cooperative launch (all blocks co-resident).  bar[0] arrivals,
-// bar[1] generation, bar[2] abort.  The wait is bounded (~1 s of SM clock): on timeout the
-// kernel records ERR_TIMEOUT, raises abort and every block returns at its next barrier.
+// Grid barrier for a cooperative launch (all blocks co-resident).  bar[0] counts arrivals
+// over the whole launch (never reset inside it): barrier number e is passed once it reaches
+// e * gridDim.x.  bar[2] is the abort flag.  The wait is bounded (~1 s of SM clock): on
+// timeout the kernel records ERR_TIMEOUT, raises abort and every block returns at its next
+// barrier.  `epoch` is the block's arrival target, advanced by each call.
 constexpr long long kBarrierCycles = 2000000000LL;
 
-__device__ __forceinline__ bool grid_barrier(const DevPtrs& P) {
+__device__ __forceinline__ bool grid_barrier(const DevPtrs& P, unsigned& epoch) {
   __shared__ int s_ok;
-  unsigned* bar = P.bar;
   __syncthreads();
+  epoch += gridDim.x;
   if (threadIdx.x == 0) {
     int ok = 1;
-    volatile unsigned* vb = bar;
-    const unsigned gen = vb[1];
+    volatile unsigned* vb = P.bar;
     __threadfence();
-    if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
-      atomicExch(&bar[0], 0u);
-      __threadfence();
-      atomicAdd(&bar[1], 1u);
-    } else {
-      const long long t0 = clock64();
-      while (vb[1] == gen) {
-        if (vb[2] != 0u) { ok = 0; break; }
-        if (clock64() - t0 > kBarrierCycles) {
-          atomicOr(P.status, ERR_TIMEOUT);
-          atomicExch(&bar[2], 1u);
-          ok = 0;
-          break;
-        }
-        __nanosleep(32);
+    atomicAdd(&P.bar[0], 1u);
+    const long long t0 = clock64();
+    while (vb[0] < epoch) {
+      if (vb[2] != 0u) { ok = 0; break; }
+      if (clock64() - t0 > kBarrierCycles) {
+        atomicOr(P.status, ERR_TIMEOUT);
+        atomicExch(&P.bar[2], 1u);
+        ok = 0;
+        break;
       }
     }
     __threadfence();
@@ -417,7 +412,7 @@ __device__ __forceinline__ bool grid_barrier(const DevPtrs& P) {
   return s_ok != 0;
 }
 
-// end of step, block 0 after the final barrier: temperature of each replica (the kinetic
+// end of step, one block after all others have finished: temperature of each replica (the kinetic
 // slot of the last SHAKE pass, i.e. of (v(t-dt/2)+v(t+dt/2))/2) and the step counters
 __device__ void finish_block(const DevPtrs& P, const IntConst& c, double tt) {
   const int h = P.step_ctr[1];
@@ -443,6 +438,28 @@ __device__ void finish_block(const DevPtrs& P, const IntConst& c, double tt) {
     P.step_ctr[0] += 1;
     P.step_ctr[1] += 1;
   }
+}
+
+// is any replica still iterating the SHAKE <-> thermostat loop at pass `it`?  The same answer
+// in every block: all read the kinetic sums completed before the last grid barrier.
+__device__ bool any_active(const DevPtrs& P, const IntConst& c, int it, double tt) {
+  int act = 0;
+  for (int r = threadIdx.x; r < c.nrep; r += blockDim.x)
+    act |= cano_active(P, c, P.reps[r], it, true, tt) ? 1 : 0;
+  return __syncthreads_or(act) != 0;
+}
+
+// the last block to finish the step computes the temperatures and advances the step counters
+__device__ void finish_last(const DevPtrs& P, const IntConst& c, double tt) {
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&P.bar[3], 1u) == gridDim.x - 1;
+    __threadfence();
+  }
+  __syncthreads();
+  if (s_last) finish_block(P, c, tt);
 }
 
 // ---- METHOD= MICR: verlet.f90 fused with SHAKE, one cooperative launch ------------------
@@ -505,8 +522,7 @@ __global__ void __launch_bounds__(64) k_micr_fused(DevPtrs P, IntConst c, int nu
     }
     add_kin(P, c.nsub_total, c.nkin - 1, sub, ke);
   }
-  if (!grid_barrier(P)) return;
-  if (blockIdx.x == 0) finish_block(P, c, c.temp);
+  finish_last(P, c, c.temp);
 }
 
 // ---- METHOD= CANO / GE: verlethe.f90 ----------------------------------------------------
@@ -662,11 +678,11 @@ struct UnitSmem {
 };
 
 template <bool FP64>
-__device__ __forceinline__ void ru_grad(const DevPtrs& P, const UnitScal& U, int q, double s, double* g) {
+__device__ __forceinline__ void ru_grad(const DevPtrs& P, int a, double s, double* g) {
   if (FP64) {
-    for (int k = 0; k < 3; ++k) g[k] = __ldg(&P.grd[3 * U.a[q] + k]) * s;
+    for (int k = 0; k < 3; ++k) g[k] = __ldg(&P.grd[3 * a + k]) * s;
   } else {
-    for (int k = 0; k < 3; ++k) g[k] = (double)__ldg(&P.frc[3 * U.a[q] + k]) * kFrcInv * s;
+    for (int k = 0; k < 3; ++k) g[k] = (double)__ldg(&P.frc[3 * a + k]) * kFrcInv * s;
   }
 }
 
@@ -698,7 +714,7 @@ __device__ __forceinline__ double ru_cano1(const DevPtrs& P, const IntConst& c, 
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     double g[3];
-    ru_grad<FP64>(P, U, q, s, g);
+    ru_grad<FP64>(P, U.a[q], s, g);
     double vv = 0.0;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -709,6 +725,26 @@ __device__ __forceinline__ double ru_cano1(const DevPtrs& P, const IntConst& c, 
     ke += U.m[q] * vv;
   }
   return ke;
+}
+
+// phase 2: v = (2chi-1) v - chi dt c g/m; x += dt v; forcec = 0
+template <bool FP64>
+__device__ __forceinline__ void ru_cano2(const DevPtrs& P, const IntConst& c, const UnitScal& U,
+                                         UnitSmem& S, int tid, double s, double chi, bool shk) {
+  const double a1 = chi * c.dt * kConvcv, b1 = 2.0 * chi - 1.0;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double g[3];
+    ru_grad<FP64>(P, U.a[q], s, g);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int i = 3 * q + k;
+      const double v = b1 * S.vb[i][tid] - a1 * g[k] * U.im[q];
+      S.x[i][tid] += c.dt * v;
+      S.fc[i][tid] = 0.0;
+      if (!shk) S.dxs[i][tid] = v;   // no SHAKE: the new velocity, stored at the end
+    }
+  }
 }
 
 // phase 3: SHAKE + KE of (v(t-dt/2) + v(t+dt/2))/2
@@ -745,117 +781,560 @@ __device__ __forceinline__ double ru_cano3(const DevPtrs& P, const IntConst& c, 
   return ke;
 }
 
-// whole step for all replicas, one launch; units of 1-3 atoms held in registers when every
-// unit has its own thread (RESIDENT), else streamed through global memory
+// phase 4: forcec += (x - xback)/dt^2; KE of dt/2 (-c g/m + forcec) + v(t-dt/2)
+template <bool FP64>
+__device__ __forceinline__ double ru_cano4(const DevPtrs& P, const IntConst& c, const UnitScal& U,
+                                           UnitSmem& S, int tid, double s) {
+  const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
+  double ke = 0.0;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double g[3];
+    ru_grad<FP64>(P, U.a[q], s, g);
+    double vv = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int i = 3 * q + k;
+      const double fc = S.fc[i][tid] + r2 * S.dxs[i][tid];
+      S.fc[i][tid] = fc;
+      const double vt = h * (-kConvcv * g[k] * U.im[q] + fc) + S.vb[i][tid];
+      vv += vt * vt;
+    }
+    ke += U.m[q] * vv;
+  }
+  return ke;
+}
+
+// phase 5: v = chi dt (-c g/m + forcec) + (2chi-1) v(t-dt/2); x = x0 + dt v
+template <bool FP64>
+__device__ __forceinline__ void ru_cano5(const DevPtrs& P, const IntConst& c, const UnitScal& U,
+                                         UnitSmem& S, int tid, double s, double chi) {
+  const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double g[3];
+    ru_grad<FP64>(P, U.a[q], s, g);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int i = 3 * q + k;
+      const double v = (-kConvcv * g[k] * U.im[q] + S.fc[i][tid]) * a1 + S.vb[i][tid] * b1;
+      S.x[i][tid] = S.x0[i][tid] + c.dt * v;
+    }
+  }
+}
+
+// ---- 4-atom SHAKE groups: eight lanes per group ------------------------------------------
+// Lanes 0-3 of an aligned group of 8 hold the group's atoms (state in the shared-memory slot
+// of the lane, component 0-2); lanes 0-5 hold its constraints in md_run's pair order
+// (shake.f90 parlis: 1-2, 2-3, 3-1, 4-1, 3-4, 2-4).  Warps that carry 4-atom groups carry
+// nothing else, so every lane of such a warp runs the same code and the width-8 shuffles
+// below are always warp-convergent.
+struct QLane {
+  int sl;            // lane in the group (0-7)
+  int a;             // atom of this lane (sl < 4), else -1
+  int sub, rep;      // -1 / 0 for lanes of an empty group
+  bool grp;          // the group exists
+  double im, m;      // inverse mass, mass of the atom (0 without one)
+  double len2;       // squared length of constraint sl (sl < 6)
+};
+
+__device__ __forceinline__ QLane ql_make(const DevPtrs& P, const IntConst& c, int v) {
+  QLane q;
+  const int g = (v - c.qbase) >> 3;
+  q.sl = v & 7;
+  q.grp = g < c.nquad;
+  q.a = -1; q.sub = -1; q.rep = 0; q.im = 0.0; q.m = 0.0; q.len2 = 1.0;
+  if (q.grp) {
+    const Unit& u = P.units[P.quad_idx[g]];
+    q.sub = u.sub;
+    q.rep = u.rep;
+    if (q.sl < 4) {
+      q.a = u.a[q.sl];
+      q.im = P.imass[q.a];
+      q.m = P.mass[q.a];
+    }
+    if (q.sl < 6) q.len2 = u.d2[q.sl];
+  }
+  return q;
+}
+
+__device__ __forceinline__ double sum8(double v) {
+  v += __shfl_xor_sync(0xffffffffu, v, 4, 8);
+  v += __shfl_xor_sync(0xffffffffu, v, 2, 8);
+  v += __shfl_xor_sync(0xffffffffu, v, 1, 8);
+  return v;
+}
+
+// kinetic sum of a quad warp: one value per group (replicated in its 8 lanes)
+__device__ __forceinline__ void add_kin_quad(const DevPtrs& P, int nsub_total, int kslot, int sub,
+                                             double ke_grp) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  long long* dst = P.kin_fix + (size_t)kslot * nsub_total;
+  const int s0 = __shfl_sync(full, sub, 0);
+  double e = (lane & 7) == 0 ? ke_grp : 0.0;
+  if (__all_sync(full, sub == s0)) {
+    e += __shfl_xor_sync(full, e, 8);
+    e += __shfl_xor_sync(full, e, 16);
+    if (lane == 0 && s0 >= 0) atomic_add_ll(&dst[s0], to_fix(e, kKinScale));
+  } else if ((lane & 7) == 0 && sub >= 0 && ke_grp != 0.0) {
+    atomic_add_ll(&dst[sub], to_fix(ke_grp, kKinScale));
+  }
+}
+
+// shake4 (shake.f90:333-562) for one group spread over its 8 lanes: each constraint lane
+// builds its row of the Newton matrix, the LU with partial pivoting (simulu) eliminates the
+// rows held by the lanes that are not yet pivots, and back substitution broadcasts G one
+// entry at a time.  Same iteration, pivot rule, elimination arithmetic and convergence test
+// as the serial form.  x (in/out) and x0 are this lane's atom (lanes 0-3).  Returns 0, 1 (not
+// converged) or -2 (singular), the same value in all lanes of the group.
+__device__ int quad_shake(const Rep& R, const QLane& q, double x[3], const double x0[3], double tol,
+                          int maxit) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int sl = q.sl;
+  const int pi_ = sl == 0 ? 0 : sl == 1 ? 1 : sl == 2 ? 2 : sl == 3 ? 3 : sl == 4 ? 2 : 1;
+  const int pj_ = sl == 0 ? 1 : sl == 1 ? 2 : sl == 2 ? 0 : sl == 3 ? 0 : 3;
+  const bool con = q.grp && sl < 6;
+  double d1[3], d2[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double xi = __shfl_sync(full, x[k], pi_, 8), xj = __shfl_sync(full, x[k], pj_, 8);
+    const double yi = __shfl_sync(full, x0[k], pi_, 8), yj = __shfl_sync(full, x0[k], pj_, 8);
+    d1[k] = xi - xj;
+    d2[k] = yi - yj;
+  }
+  mimg(R, d1);
+  mimg(R, d2);
+  double D2[6][3], im4[4], cr[6];
+#pragma unroll
+  for (int ig = 0; ig < 6; ++ig)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) D2[ig][k] = __shfl_sync(full, d2[k], ig, 8);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) im4[a] = __shfl_sync(full, q.im, a, 8);
+#pragma unroll
+  for (int ig = 0; ig < 6; ++ig) cr[ig] = sl < 6 ? cg4(sl, ig, im4) : 0.0;
+  double wk[3] = {d1[0], d1[1], d1[2]};
+  double G[6] = {0, 0, 0, 0, 0, 0};
+  bool done = !q.grp;
+  bool singular = false;
+  int ret = 0;
+  for (int it = 0; it < maxit; ++it) {
+    const double B0 = q.len2 - (wk[0] * wk[0] + wk[1] * wk[1] + wk[2] * wk[2]);
+    const bool bad = con && fabs(B0) >= tol * q.len2;
+    const unsigned gbits = (__ballot_sync(full, bad) >> (lane & 24)) & 0xffu;
+    if (!done && gbits == 0u) {   // converged: 3) modify r1 (shake.f90:478-489)
+      done = true;
+      ret = singular ? -2 : 0;
+      if (sl < 4) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          double w;
+          if (sl == 0) w = G[0] * D2[0][k] - G[2] * D2[2][k] - G[3] * D2[3][k];
+          else if (sl == 1) w = -G[0] * D2[0][k] + G[1] * D2[1][k] + G[5] * D2[5][k];
+          else if (sl == 2) w = -G[1] * D2[1][k] + G[2] * D2[2][k] + G[4] * D2[4][k];
+          else w = G[3] * D2[3][k] - G[4] * D2[4][k] - G[5] * D2[5][k];
+          x[k] += q.im * w;
+        }
+      }
+    }
+    if (__all_sync(full, done)) return q.grp ? ret : 0;
+    // gradient matrix row of this constraint and the right-hand side
+    double A[6];
+#pragma unroll
+    for (int ig = 0; ig < 6; ++ig)
+      A[ig] = 2.0 * cr[ig] * (wk[0] * D2[ig][0] + wk[1] * D2[ig][1] + wk[2] * D2[ig][2]);
+    double B = B0;
+#pragma unroll
+    for (int ig = 0; ig < 6; ++ig) B += A[ig] * G[ig];
+    // LU with partial pivoting over the constraint lanes
+    bool used = !con;
+    bool lu_ok = true;
+    int perm[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      double bv = used ? -1.0 : fabs(A[k]);
+      int bl = sl;
+#pragma unroll
+      for (int off = 4; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(full, bv, off, 8);
+        const int ol = __shfl_xor_sync(full, bl, off, 8);
+        if (ov > bv || (ov == bv && ol < bl)) { bv = ov; bl = ol; }
+      }
+      perm[k] = bl;
+      double pk[6];
+#pragma unroll
+      for (int j = k; j < 6; ++j) pk[j] = __shfl_sync(full, A[j], bl, 8);
+      const double pb = __shfl_sync(full, B, bl, 8);
+      if (fabs(pk[k]) < 1.0e-30) lu_ok = false;
+      const double piv = 1.0 / pk[k];
+      if (sl == bl) {
+        used = true;
+        A[k] = piv;
+      } else if (!used) {
+        const double f = A[k] * piv;
+#pragma unroll
+        for (int j = k + 1; j < 6; ++j) A[j] -= f * pk[j];
+        B -= f * pb;
+      }
+    }
+    // back substitution: every lane of the warp runs the shuffles (lu_ok and done differ
+    // between the groups of a warp); only a live group with a regular matrix takes the result
+    const bool take = lu_ok && !done;
+    if (!lu_ok && !done) singular = true;
+#pragma unroll
+    for (int i = 5; i >= 0; --i) {
+      double t = B;
+#pragma unroll
+      for (int j = i + 1; j < 6; ++j) t -= A[j] * G[j];
+      const double gi = __shfl_sync(full, t * A[i], perm[i], 8);
+      if (take) G[i] = gi;
+    }
+    if (!done) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double w = d1[k];
+#pragma unroll
+        for (int ig = 0; ig < 6; ++ig) w += cr[ig] * D2[ig][k] * G[ig];
+        wk[k] = w;
+      }
+    }
+  }
+  if (!done) ret = singular ? -2 : 1;
+  return q.grp ? ret : 0;
+}
+
+// the per-atom phases of a quad lane, on its shared-memory slot (component 0-2)
+template <bool FP64>
+__device__ __forceinline__ double q_cano1(const DevPtrs& P, const IntConst& c, const QLane& q,
+                                          UnitSmem& S, int tid, double s) {
+  double ke = 0.0;
+  if (q.a >= 0) {
+    const double rt = 0.5 * c.dt * kConvcv;
+    double g[3];
+    ru_grad<FP64>(P, q.a, s, g);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      S.x0[k][tid] = S.x[k][tid];
+      const double vt = S.vb[k][tid] - rt * g[k] * q.im;
+      ke += vt * vt;
+    }
+    ke *= q.m;
+  }
+  return sum8(ke);
+}
+
+template <bool FP64>
+__device__ __forceinline__ void q_cano2(const DevPtrs& P, const IntConst& c, const QLane& q,
+                                        UnitSmem& S, int tid, double s, double chi) {
+  if (q.a < 0) return;
+  const double a1 = chi * c.dt * kConvcv, b1 = 2.0 * chi - 1.0;
+  double g[3];
+  ru_grad<FP64>(P, q.a, s, g);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double v = b1 * S.vb[k][tid] - a1 * g[k] * q.im;
+    S.x[k][tid] += c.dt * v;
+    S.fc[k][tid] = 0.0;
+  }
+}
+
+__device__ __forceinline__ double q_cano3(const DevPtrs& P, const IntConst& c, const QLane& q,
+                                          UnitSmem& S, int tid) {
+  double x[3], x0[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    x[k] = S.x[k][tid];
+    x0[k] = S.x0[k][tid];
+  }
+  const int ier = quad_shake(P.reps[q.rep], q, x, x0, c.shake_tol, c.shake_maxit);
+  if (ier && q.sl == 0) shake_status(P, ier);
+  double ke = 0.0;
+  if (q.a >= 0) {
+    const double ri = 1.0 / c.dt;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      S.dxs[k][tid] = x[k] - S.x[k][tid];
+      S.x[k][tid] = x[k];
+      const double vt = 0.5 * (S.vb[k][tid] + (x[k] - x0[k]) * ri);
+      ke += vt * vt;
+    }
+    ke *= q.m;
+  }
+  return sum8(ke);
+}
+
+template <bool FP64>
+__device__ __forceinline__ double q_cano4(const DevPtrs& P, const IntConst& c, const QLane& q,
+                                          UnitSmem& S, int tid, double s) {
+  double ke = 0.0;
+  if (q.a >= 0) {
+    const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
+    double g[3];
+    ru_grad<FP64>(P, q.a, s, g);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double fc = S.fc[k][tid] + r2 * S.dxs[k][tid];
+      S.fc[k][tid] = fc;
+      const double vt = h * (-kConvcv * g[k] * q.im + fc) + S.vb[k][tid];
+      ke += vt * vt;
+    }
+    ke *= q.m;
+  }
+  return sum8(ke);
+}
+
+template <bool FP64>
+__device__ __forceinline__ void q_cano5(const DevPtrs& P, const IntConst& c, const QLane& q,
+                                        UnitSmem& S, int tid, double s, double chi) {
+  if (q.a < 0) return;
+  const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
+  double g[3];
+  ru_grad<FP64>(P, q.a, s, g);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double v = (-kConvcv * g[k] * q.im + S.fc[k][tid]) * a1 + S.vb[k][tid] * b1;
+    S.x[k][tid] = S.x0[k][tid] + c.dt * v;
+  }
+}
+
+// streaming form of a quad lane: its slot is filled from and returned to the atom arrays
+// around each phase (x, x0, v(t-dt/2) = vback, forcec, and x - xback for the SHAKE shift)
+__device__ __forceinline__ void q_fetch(const DevPtrs& P, const QLane& q, UnitSmem& S, int tid,
+                                        bool first) {
+  if (q.a < 0) return;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int i = 3 * q.a + k;
+    S.x[k][tid] = P.x[i];
+    if (first) {
+      S.vb[k][tid] = P.v[i];
+      S.fc[k][tid] = 0.0;
+      S.dxs[k][tid] = 0.0;
+    } else {
+      S.x0[k][tid] = P.x0[i];
+      S.vb[k][tid] = P.vback[i];
+      S.fc[k][tid] = P.forcec[i];
+      S.dxs[k][tid] = P.x[i] - P.xback[i];
+    }
+  }
+}
+
+__device__ __forceinline__ void q_spill(const DevPtrs& P, const IntConst& c, const QLane& q,
+                                        UnitSmem& S, int tid, bool fp64) {
+  if (q.a < 0) return;
+  const double ri = 1.0 / c.dt;
+  double xq[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int i = 3 * q.a + k;
+    xq[k] = S.x[k][tid];
+    P.x[i] = xq[k];
+    P.x0[i] = S.x0[k][tid];
+    P.vback[i] = S.vb[k][tid];
+    P.forcec[i] = S.fc[k][tid];
+    P.xback[i] = xq[k] - S.dxs[k][tid];
+    P.v[i] = (xq[k] - S.x0[k][tid]) * ri;
+  }
+  if (!isfinite(xq[0]) || !isfinite(xq[1]) || !isfinite(xq[2])) atomicOr(P.status, ERR_NONFINITE);
+  write_slot(P, q.a, xq, fp64);
+}
+
+// Whole step for all replicas, one launch.  Virtual lanes: [0, nsmall) one 1-3 atom unit
+// each; [qbase, nvirt) eight lanes per 4-atom group.  RESIDENT: one virtual lane per thread
+// and all unit state on chip for the whole step; else grid-stride over the virtual lanes
+// with the state in the atom arrays between phases.
 template <bool FP64, bool RESIDENT>
 __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst c, int nunit) {
+  __shared__ UnitSmem S;
   const int nthr = gridDim.x * blockDim.x;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int tid = threadIdx.x;
   const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
   const bool shk = c.shake_method != JP_SHAKE_NONE;
+  unsigned epoch = 0;
   if (gt < c.nrep) write_ene_hist(P, c, gt);
+  const int nv = RESIDENT ? nthr : c.nvirt;
+  // RESIDENT state of this thread's lane
+  UnitScal U;
+  QLane Q;
+  bool small = false, quad = false;
+  double s = 1.0;
   if (RESIDENT) {
-    // ---------------- one unit per thread --------------------------------------------
-    __shared__ UnitSmem S;
-    const int tid = threadIdx.x;
-    const bool have = gt < nunit;
-    Unit u;
-    u.n = 0; u.sub = -1; u.rep = 0;
-    if (have) u = P.units[gt];
-    const bool reg = have && u.n <= 3;
-    const double s = have ? rep_scale(P, c, u.rep) : 1.0;
-    UnitScal U;
-    if (reg) ru_load(P, u, U, S, tid);
-    const int sub = have ? u.sub : -1;
-    if (shk) {
-      double ke = 0.0;
-      if (reg) ke = ru_cano1<FP64>(P, c, U, S, tid, s);
-      else if (have) ke = cano1_unit<FP64>(P, c, u, s);
-      add_kin(P, c.nsub_total, 0, sub, ke);
-      if (!grid_barrier(P)) return;
+    const int v = gt;
+    small = v < c.nsmall;
+    quad = v >= c.qbase && v < c.nvirt;
+    if (small) {
+      const Unit u = P.units[P.small_idx[v]];
+      ru_load(P, u, U, S, tid);
+      s = rep_scale(P, c, u.rep);
+    } else if (quad) {
+      Q = ql_make(P, c, v);
+      q_fetch(P, Q, S, tid, true);
+      s = rep_scale(P, c, Q.rep);
     }
-    // phase 2 (+ phase 3 of the first SHAKE pass)
-    {
-      double ke = 0.0;
-      if (reg) {
-        const double tempc = shk ? sub_temp(P, c, 0, U.sub) : c.temp;
-        const double chi = sqrt(tt / tempc);
-        const double a1 = chi * c.dt * kConvcv, b1 = 2.0 * chi - 1.0;
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          double g[3];
-          ru_grad<FP64>(P, U, q, s, g);
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            const int i = 3 * q + k;
-            const double v = b1 * S.vb[i][tid] - a1 * g[k] * U.im[q];
-            S.x[i][tid] += c.dt * v;
-            S.fc[i][tid] = 0.0;
-            if (!shk) S.dxs[i][tid] = v;   // no SHAKE: the new velocity, stored below
-          }
+  }
+  // phase 1 (verlethe.f90:380-398)
+  if (shk) {
+    for (int base = 0; base < nv; base += nthr) {
+      const int v = base + gt;
+      if (RESIDENT) {
+        if (quad) {   // warp-uniform: one kinetic-sum call site per warp kind
+          add_kin_quad(P, c.nsub_total, 0, Q.sub, q_cano1<FP64>(P, c, Q, S, tid, s));
+        } else {
+          const double ke = small ? ru_cano1<FP64>(P, c, U, S, tid, s) : 0.0;
+          add_kin(P, c.nsub_total, 0, small ? U.sub : -1, ke);
         }
-        if (shk) ke = ru_cano3(P, c, U, S, tid);
-      } else if (have) {
-        cano2_unit<FP64>(P, c, u, s, tt);
-        if (shk) ke = cano3_unit<FP64>(P, c, u);
+      } else if (v >= c.qbase) {
+        const QLane q = ql_make(P, c, v);
+        q_fetch(P, q, S, tid, true);
+        const double ke = q_cano1<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep));
+        q_spill(P, c, q, S, tid, FP64);
+        add_kin_quad(P, c.nsub_total, 0, q.sub, ke);
+      } else {
+        double ke = 0.0;
+        int sub = -1;
+        if (v < c.nsmall) {
+          const Unit u = P.units[P.small_idx[v]];
+          sub = u.sub;
+          ke = cano1_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
+        }
+        add_kin(P, c.nsub_total, 0, sub, ke);
+      }
+    }
+    if (!grid_barrier(P, epoch)) return;
+  }
+  // phase 2 (verlethe.f90:400-516) + phase 3 of the first SHAKE pass
+  for (int base = 0; base < nv; base += nthr) {
+    const int v = base + gt;
+    if (RESIDENT) {
+      if (quad) {
+        const double chi = Q.grp ? sqrt(tt / sub_temp(P, c, 0, Q.sub)) : 1.0;
+        q_cano2<FP64>(P, c, Q, S, tid, s, chi);
+        add_kin_quad(P, c.nsub_total, 1, Q.sub, q_cano3(P, c, Q, S, tid));
+      } else {
+        double ke = 0.0;
+        if (small) {
+          const double chi = sqrt(tt / (shk ? sub_temp(P, c, 0, U.sub) : c.temp));
+          ru_cano2<FP64>(P, c, U, S, tid, s, chi, shk);
+          if (shk) ke = ru_cano3(P, c, U, S, tid);
+        }
+        if (shk) add_kin(P, c.nsub_total, 1, small ? U.sub : -1, ke);
+      }
+    } else if (v >= c.qbase) {
+      const QLane q = ql_make(P, c, v);
+      q_fetch(P, q, S, tid, false);
+      const double chi = q.grp ? sqrt(tt / sub_temp(P, c, 0, q.sub)) : 1.0;
+      q_cano2<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep), chi);
+      const double ke = q_cano3(P, c, q, S, tid);
+      q_spill(P, c, q, S, tid, FP64);
+      add_kin_quad(P, c.nsub_total, 1, q.sub, ke);
+    } else {
+      double ke = 0.0;
+      int sub = -1;
+      if (v < c.nsmall) {
+        const Unit u = P.units[P.small_idx[v]];
+        cano2_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), tt);
+        if (shk) {
+          sub = u.sub;
+          ke = cano3_unit<FP64>(P, c, u);
+        }
       }
       if (shk) add_kin(P, c.nsub_total, 1, sub, ke);
     }
-    if (shk) {
-      for (int it = 1; it < c.icslop; ++it) {
-        if (!grid_barrier(P)) return;
-        const bool act = have && cano_active(P, c, P.reps[u.rep], it, true, tt);
-        double ke = 0.0;
-        if (act) {   // phase 4
-          if (reg) {
-            const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-              double g[3];
-              ru_grad<FP64>(P, U, q, s, g);
-              double vv = 0.0;
-#pragma unroll
-              for (int k = 0; k < 3; ++k) {
-                const int i = 3 * q + k;
-                const double fc = S.fc[i][tid] + r2 * S.dxs[i][tid];
-                S.fc[i][tid] = fc;
-                const double vt = h * (-kConvcv * g[k] * U.im[q] + fc) + S.vb[i][tid];
-                vv += vt * vt;
-              }
-              ke += U.m[q] * vv;
-            }
+  }
+  if (shk) {
+    for (int it = 1; it < c.icslop; ++it) {
+      if (!grid_barrier(P, epoch)) return;
+      if (!any_active(P, c, it, tt)) break;
+      // phase 4 (verlethe.f90:625-640)
+      for (int base = 0; base < nv; base += nthr) {
+        const int v = base + gt;
+        if (RESIDENT) {
+          if (quad) {
+            const bool act = Q.grp && cano_active(P, c, P.reps[Q.rep], it, true, tt);
+            const double ke = q_cano4<FP64>(P, c, Q, S, tid, s);
+            add_kin_quad(P, c.nsub_total, 2 * it, act ? Q.sub : -1, act ? ke : 0.0);
           } else {
-            ke = cano4_unit<FP64>(P, c, u, s);
+            const bool act = small && cano_active(P, c, P.reps[U.rep], it, true, tt);
+            const double ke = act ? ru_cano4<FP64>(P, c, U, S, tid, s) : 0.0;
+            add_kin(P, c.nsub_total, 2 * it, act ? U.sub : -1, ke);
           }
-        }
-        add_kin(P, c.nsub_total, 2 * it, act ? sub : -1, ke);
-        if (!grid_barrier(P)) return;
-        ke = 0.0;
-        if (act) {   // phase 5 + phase 3 of the next pass
-          if (reg) {
-            const double chi = sqrt(tt / sub_temp(P, c, 2 * it, U.sub));
-            const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-              double g[3];
-              ru_grad<FP64>(P, U, q, s, g);
-#pragma unroll
-              for (int k = 0; k < 3; ++k) {
-                const int i = 3 * q + k;
-                const double v = (-kConvcv * g[k] * U.im[q] + S.fc[i][tid]) * a1 + S.vb[i][tid] * b1;
-                S.x[i][tid] = S.x0[i][tid] + c.dt * v;
-              }
+        } else if (v >= c.qbase) {
+          const QLane q = ql_make(P, c, v);
+          const bool act = q.grp && cano_active(P, c, P.reps[q.rep], it, true, tt);
+          q_fetch(P, q, S, tid, false);
+          const double ke = q_cano4<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep));
+          if (act) q_spill(P, c, q, S, tid, FP64);
+          add_kin_quad(P, c.nsub_total, 2 * it, act ? q.sub : -1, act ? ke : 0.0);
+        } else {
+          double ke = 0.0;
+          int sub = -1;
+          if (v < c.nsmall) {
+            const Unit u = P.units[P.small_idx[v]];
+            if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+              sub = u.sub;
+              ke = cano4_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
             }
-            ke = ru_cano3(P, c, U, S, tid);
-          } else {
-            cano5_unit<FP64>(P, c, u, s, it, tt);
-            ke = cano3_unit<FP64>(P, c, u);
           }
+          add_kin(P, c.nsub_total, 2 * it, sub, ke);
         }
-        add_kin(P, c.nsub_total, 2 * it + 1, act ? sub : -1, ke);
+      }
+      if (!grid_barrier(P, epoch)) return;
+      // phase 5 (verlethe.f90:641-718) + phase 3 of the next SHAKE pass
+      for (int base = 0; base < nv; base += nthr) {
+        const int v = base + gt;
+        if (RESIDENT) {
+          if (!quad) {
+            const bool act = small && cano_active(P, c, P.reps[U.rep], it, true, tt);
+            double ke = 0.0;
+            if (act) {
+              ru_cano5<FP64>(P, c, U, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, U.sub)));
+              ke = ru_cano3(P, c, U, S, tid);
+            }
+            add_kin(P, c.nsub_total, 2 * it + 1, act ? U.sub : -1, ke);
+          } else {
+            // the whole warp runs the SHAKE (its shuffles); inactive groups keep their state
+            const bool act = Q.grp && cano_active(P, c, P.reps[Q.rep], it, true, tt);
+            double sx[3], sdx[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { sx[k] = S.x[k][tid]; sdx[k] = S.dxs[k][tid]; }
+            if (act) q_cano5<FP64>(P, c, Q, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, Q.sub)));
+            const double ke = q_cano3(P, c, Q, S, tid);
+            if (!act && Q.a >= 0) {
+#pragma unroll
+              for (int k = 0; k < 3; ++k) { S.x[k][tid] = sx[k]; S.dxs[k][tid] = sdx[k]; }
+            }
+            add_kin_quad(P, c.nsub_total, 2 * it + 1, act ? Q.sub : -1, act ? ke : 0.0);
+          }
+        } else if (v >= c.qbase) {
+          const QLane q = ql_make(P, c, v);
+          const bool act = q.grp && cano_active(P, c, P.reps[q.rep], it, true, tt);
+          q_fetch(P, q, S, tid, false);
+          if (act) q_cano5<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep),
+                                 sqrt(tt / sub_temp(P, c, 2 * it, q.sub)));
+          const double ke = q_cano3(P, c, q, S, tid);
+          if (act) q_spill(P, c, q, S, tid, FP64);
+          add_kin_quad(P, c.nsub_total, 2 * it + 1, act ? q.sub : -1, act ? ke : 0.0);
+        } else {
+          double ke = 0.0;
+          int sub = -1;
+          if (v < c.nsmall) {
+            const Unit u = P.units[P.small_idx[v]];
+            if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+              cano5_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
+              sub = u.sub;
+              ke = cano3_unit<FP64>(P, c, u);
+            }
+          }
+          add_kin(P, c.nsub_total, 2 * it + 1, sub, ke);
+        }
       }
     }
-    if (reg) {   // the unit's new state back to memory
+  }
+  if (RESIDENT) {   // the lane's new state back to memory
+    if (small) {
       bool bad = false;
       const double ri = 1.0 / c.dt;
 #pragma unroll
@@ -875,73 +1354,11 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
         }
       }
       if (bad) atomicOr(P.status, ERR_NONFINITE);
-    }
-  } else {
-    // ---------------- streaming: grid-stride over units ------------------------------
-    if (shk) {
-      for (int base = 0; base < nunit; base += nthr) {
-        const int t = base + gt;
-        double ke = 0.0;
-        int sub = -1;
-        if (t < nunit) {
-          const Unit u = P.units[t];
-          sub = u.sub;
-          ke = cano1_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
-        }
-        add_kin(P, c.nsub_total, 0, sub, ke);
-      }
-      if (!grid_barrier(P)) return;
-    }
-    for (int base = 0; base < nunit; base += nthr) {
-      const int t = base + gt;
-      double ke = 0.0;
-      int sub = -1;
-      if (t < nunit) {
-        const Unit u = P.units[t];
-        cano2_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), tt);
-        if (shk) {
-          sub = u.sub;
-          ke = cano3_unit<FP64>(P, c, u);
-        }
-      }
-      if (shk) add_kin(P, c.nsub_total, 1, sub, ke);
-    }
-    if (shk) {
-      for (int it = 1; it < c.icslop; ++it) {
-        if (!grid_barrier(P)) return;
-        for (int base = 0; base < nunit; base += nthr) {
-          const int t = base + gt;
-          double ke = 0.0;
-          int sub = -1;
-          if (t < nunit) {
-            const Unit u = P.units[t];
-            if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
-              sub = u.sub;
-              ke = cano4_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
-            }
-          }
-          add_kin(P, c.nsub_total, 2 * it, sub, ke);
-        }
-        if (!grid_barrier(P)) return;
-        for (int base = 0; base < nunit; base += nthr) {
-          const int t = base + gt;
-          double ke = 0.0;
-          int sub = -1;
-          if (t < nunit) {
-            const Unit u = P.units[t];
-            if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
-              cano5_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
-              sub = u.sub;
-              ke = cano3_unit<FP64>(P, c, u);
-            }
-          }
-          add_kin(P, c.nsub_total, 2 * it + 1, sub, ke);
-        }
-      }
+    } else if (quad) {
+      q_spill(P, c, Q, S, tid, FP64);
     }
   }
-  if (!grid_barrier(P)) return;
-  if (blockIdx.x == 0) finish_block(P, c, tt);
+  finish_last(P, c, tt);
 }
 
 // ---- standalone SHAKE (test hook): r1 constrained against r2, positions in xback / x0 -----
@@ -1009,7 +1426,8 @@ static void coop_launch(void (*kernel)(Args...), int grid, cudaStream_t st, Args
 void launch_integrate(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
                       cudaStream_t st) {
   cudaMemsetAsync(P.bar, 0, sizeof(unsigned) * 4, st);
-  const int want = std::max(1, (nunit + 63) / 64);
+  const int lanes = c.method == JP_METHOD_MICR ? nunit : c.nvirt;
+  const int want = std::max(1, (lanes + kIntThreads - 1) / kIntThreads);
   const int grid = std::min(want, grid_max);
   const bool resident = want <= grid_max;
   if (c.method == JP_METHOD_MICR) {

@@ -51,6 +51,9 @@ struct IntConst {
   int nsub_total;
   int natom;
   int nkin;                // kinetic-sum slots; the last one is MICR's
+  // virtual lanes of the CANO/GE kernel: [0, nsmall) one 1-3 atom unit each (small_idx),
+  // [qbase, nvirt) eight lanes per 4-atom group (quad_idx); qbase and nvirt are multiples of 32
+  int nsmall, nquad, qbase, nvirt;
 };
 int cano_grid(bool fp64, int device);   // co-resident blocks of the integration kernels
 // one cooperative launch: energies of the step, force scale, verlet (MICR) or verlethe
