@@ -72,6 +72,23 @@ typedef struct jp_ge {
   double lower, upper;       /* ALSD linear wall slopes (LMD only) */
 } jp_ge;
 
+/* Capacity of a replica's weight and of its energy histogram (fixed when the context is
+ * created, so the weight can be replaced between runs without re-capturing anything). */
+#define JP_GE_MAX_WINDOWS 16
+#define JP_GE_MAX_DEG 15
+#define JP_GE_MAX_BINS 4096
+
+/* One McMD weight iteration (GEprep distrib_MULT + lstsquare_final), see jp_ge_fit. */
+typedef struct jp_ge_fit_params {
+  double emin, emax;         /* minE, maxE of the histogram (distrib_MULT) */
+  int32_t nbin, nbor;        /* nBIN bins in [emin, emax] plus nBOR border bins each side */
+  double next_emin, next_emax; /* nxminE, nxmaxE: energy range of the new weight */
+  double next_temp;          /* nxT: its temperature T0 */
+  int32_t nwindow, ndeg;     /* Nwindow, NfitDIM of the new polynomial */
+  int32_t ignore_empty;      /* igndat: drop bins with no estimate (weights sqrt(count)) */
+  int32_t neglect_low, neglect_high;  /* FneglectL/H: leave the border bins out of the fit */
+} jp_ge_fit_params;
+
 /* One replica's system: topology, parameters and coordinates.
  * Mirrors md_run's COMBAS/COMERG/COMMIS module arrays. */
 typedef struct jp_system {
@@ -197,6 +214,36 @@ int jp_list_stats(jp_ctx *ctx, int64_t *ntiles, int64_t *npairs_listed, int64_t 
 /* FP32 FMA throughput of `device` in TFLOP/s (best of 5 timed FMA-chain launches): the
  * peak the pair kernel's FP32 arithmetic is measured against. */
 int jp_calibrate_fp32(int32_t device, double *tflops);
+
+/* McMD iteration support (GEprep, src_GEprep/distrib_MULT.f90:60-445).
+ * jp_ge_hist_setup: from now on every MD step adds the potential energy E(t) of `replica`
+ * (-1 = all) to an energy histogram of nbin + 2 nbor bins of width (emax-emin)/nbin starting
+ * nbor bins below emin (distrib_MULT's binning, including its bin-index truncation);
+ * nbin + 2 nbor <= JP_GE_MAX_BINS; nbin = 0 switches it off.  Counts start at zero.
+ * jp_ge_hist_get: the counts [nbin + 2 nbor] as doubles; clear != 0 zeroes them. */
+int jp_ge_hist_setup(jp_ctx *ctx, int32_t replica, double emin, double emax, int32_t nbin,
+                     int32_t nbor);
+int jp_ge_hist_get(jp_ctx *ctx, int32_t replica, double *counts, int32_t clear);
+
+/* Replace the McMD weight of `replica` (the .nf read by inmcmd.f90) for the following steps;
+ * nwindow <= JP_GE_MAX_WINDOWS, ndeg <= JP_GE_MAX_DEG.  METHOD= GE contexts only. */
+int jp_ge_set(jp_ctx *ctx, int32_t replica, const jp_ge *ge);
+
+/* Host only.  lstsquare_final.f90: weighted least-squares fit of Y(X) by `nwindow`
+ * polynomials of degree `ndim` on equal windows of [minv, maxv] (X ascending), continuous in
+ * value and slope; coe[nwindow][ndim+1], low/high[nwindow] out; resid[2] (nullable) the
+ * weighted residual error and its spread (Resierr, Resierr2). */
+int jp_lstsq_windows(int32_t nwindow, int32_t ndat, int32_t ndim, double minv, double maxv,
+                     const double *X, const double *Y, const double *wei, double *coe,
+                     double *low, double *high, double *resid);
+
+/* Host only.  distrib_MULT.f90:286-445: from a histogram hist[nbin + 2 nbor] sampled with the
+ * weight `old`, the differential density of states d lnN/dE = d lnP/dE + (d lnN/dE of old),
+ * fitted on [next_emin, next_emax]; the new weight goes to `out`, whose coefficient arrays
+ * are the caller's coef[nwindow][ndeg+1], low/high[nwindow]; resid[2] nullable.  Run
+ * weights (fw) and flatness acceleration of GEprep are not supported (all weights 1). */
+int jp_ge_fit(const double *hist, const jp_ge_fit_params *fp, const jp_ge *old, double *coef,
+              double *low, double *high, jp_ge *out, double *resid);
 
 const char *jp_strerror(int code);
 void jp_destroy(jp_ctx *ctx);

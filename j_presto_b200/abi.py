@@ -41,6 +41,16 @@ class JpGe(C.Structure):
                 ("tempce", C.c_double), ("lower", C.c_double), ("upper", C.c_double)]
 
 
+JP_GE_MAX_WINDOWS, JP_GE_MAX_DEG, JP_GE_MAX_BINS = 16, 15, 4096
+
+
+class JpGeFitParams(C.Structure):
+    _fields_ = [("emin", C.c_double), ("emax", C.c_double), ("nbin", C.c_int32), ("nbor", C.c_int32),
+                ("next_emin", C.c_double), ("next_emax", C.c_double), ("next_temp", C.c_double),
+                ("nwindow", C.c_int32), ("ndeg", C.c_int32), ("ignore_empty", C.c_int32),
+                ("neglect_low", C.c_int32), ("neglect_high", C.c_int32)]
+
+
 class JpSystem(C.Structure):
     _fields_ = [
         ("natom", C.c_int32), ("index_base", C.c_int32), ("box", C.c_double * 3),
@@ -159,3 +169,18 @@ def make_systems(tops, keep):
     for i, t in enumerate(tops):
         arr[i] = make_system(t, keep)
     return arr
+
+
+def make_ge(nf, keep):
+    """JpGe from a weight dict {coef [nwin][ndeg+1], low, high, alphalw, alphaup, celw, ceup,
+    tempce[, lower, upper]}; arrays appended to `keep`."""
+    g = JpGe()
+    coef = np.ascontiguousarray(nf["coef"], np.float64)
+    g.nwindow, g.ndeg = coef.shape[0], coef.shape[1] - 1
+    g.coef = _ptr(coef, C.c_double, keep)
+    g.low = _ptr(np.ascontiguousarray(nf["low"], np.float64), C.c_double, keep)
+    g.high = _ptr(np.ascontiguousarray(nf["high"], np.float64), C.c_double, keep)
+    for k in ("alphalw", "alphaup", "celw", "ceup", "tempce"):
+        setattr(g, k, float(nf[k]))
+    g.lower, g.upper = float(nf.get("lower", 0.0)), float(nf.get("upper", 0.0))
+    return g

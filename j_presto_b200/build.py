@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libjpgpu.so")
 SOURCES = ["jp_cells.cu", "jp_pair.cu", "jp_bonded.cu", "jp_integrate.cu", "jp_calib.cu", "jp_abi.cu",
-           "jp_noalloc.cu"]
+           "jp_noalloc.cu", "jp_gefit.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -44,7 +44,7 @@ def build(verbose=False, ptxas_v=False, force=False):
         flags += ["-Xptxas", "-v"]
     for s in SOURCES:
         src = os.path.join(CSRC, s)
-        obj = os.path.join(OBJ, s.replace(".cu", ".o"))
+        obj = os.path.join(OBJ, os.path.splitext(s)[0] + ".o")
         objs.append(obj)
         if force or ptxas_v or _stale(obj, [src] + headers):
             cmd = [nvcc()] + ARCH + flags + ["-c", src, "-o", obj]

@@ -106,6 +106,17 @@ int dput(jp_ctx *c, T **p, const std::vector<T> &h) {
 }
 
 constexpr double kEekcal = 332.06378;
+constexpr int kGeCap = JP_GE_MAX_WINDOWS * (JP_GE_MAX_DEG + 3);   // doubles per replica
+
+// a .nf weight in the device layout: per window [low, high, c0..cndeg]
+void pack_ge(const jp_ge &g, double *dst) {
+  int o = 0;
+  for (int w = 0; w < g.nwindow; ++w) {
+    dst[o++] = g.low[w];
+    dst[o++] = g.high[w];
+    for (int k = 0; k <= g.ndeg; ++k) dst[o++] = g.coef[w * (g.ndeg + 1) + k];
+  }
+}
 
 // ---- rebuild: cells + tiles -------------------------------------------------------------
 void enqueue_rebuild(jp_ctx *c) {
@@ -248,7 +259,8 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
     for (int g = 0; g < s.nshake; ++g)
       for (int k = 0; k < s.shake_n[g]; ++k)
         if (!okatom(s.shake_atoms[4 * g + k])) return JP_E_INVALID;
-    if (s.ge && (s.ge->nwindow < 1 || s.ge->ndeg < 0 || !s.ge->coef || !s.ge->low || !s.ge->high))
+    if (s.ge && (s.ge->nwindow < 1 || s.ge->ndeg < 0 || s.ge->nwindow > JP_GE_MAX_WINDOWS ||
+                 s.ge->ndeg > JP_GE_MAX_DEG || !s.ge->coef || !s.ge->low || !s.ge->high))
       return JP_E_INVALID;
   }
   return 0;
@@ -535,9 +547,11 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     double ds = 0.0;
     for (int i = 0; i < n; ++i) ds += s.charge[i] * dwork[i];
     R.dself = -(1.5 / rc) * ds * 0.5 * ccoef;
-    // GE weight: per window [low, high, c0..cndeg]
+    // GE weight: a fixed slot per replica, per window [low, high, c0..cndeg]
+    R.ge_off = r * kGeCap;
+    R.hist_off = r * JP_GE_MAX_BINS;
+    hge.resize((size_t)(r + 1) * kGeCap, 0.0);
     if (s.ge) {
-      R.ge_off = (int)hge.size();
       R.ge_nwin = s.ge->nwindow;
       R.ge_ndeg = s.ge->ndeg;
       R.ge_alphalw = s.ge->alphalw;
@@ -545,11 +559,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       R.ge_celw = s.ge->celw;
       R.ge_ceup = s.ge->ceup;
       R.ge_tempce = s.ge->tempce;
-      for (int w = 0; w < s.ge->nwindow; ++w) {
-        hge.push_back(s.ge->low[w]);
-        hge.push_back(s.ge->high[w]);
-        for (int k = 0; k <= s.ge->ndeg; ++k) hge.push_back(s.ge->coef[w * (s.ge->ndeg + 1) + k]);
-      }
+      pack_ge(*s.ge, hge.data() + R.ge_off);
     }
     atom0 += n;
     blk0 += R.nblk;
@@ -638,6 +648,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dput(c, &P.terms, terms);
   e |= dput(c, &P.reps, reps);
   e |= dput(c, &P.ge_coef, hge);
+  e |= dalloc(c, &P.ge_hist, (size_t)nrep * JP_GE_MAX_BINS);
   e |= dalloc(c, &P.ene_fix, 16 * (size_t)nrep);
   e |= dalloc(c, &P.kin_fix, (size_t)c->nkin * c->nsub);
   e |= dput(c, &P.nfr, hnfr);
@@ -781,6 +792,60 @@ int jp_energy_grad(jp_ctx *c, int32_t r, const double *cord, double *eneval, dou
     }
   }
   return check_status(c);
+}
+
+int jp_ge_hist_setup(jp_ctx *c, int32_t r, double emin, double emax, int32_t nbin, int32_t nbor) {
+  if (!c || r < -1 || r >= c->nrep || nbin < 0 || nbor < 0) return JP_E_INVALID;
+  if (nbin > 0 && (!(emax > emin) || nbin + 2 * nbor > JP_GE_MAX_BINS)) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  for (int q = (r < 0 ? 0 : r); q < (r < 0 ? c->nrep : r + 1); ++q) {
+    Rep &R = c->reps[q];
+    const double de = nbin > 0 ? (emax - emin) / nbin : 1.0;
+    R.hist_n = nbin > 0 ? nbin + 2 * nbor : 0;
+    R.hist_min = emin - de * nbor;
+    R.hist_inv = 1.0 / de;
+    CK(cudaMemset(c->P.ge_hist + R.hist_off, 0, sizeof(unsigned long long) * JP_GE_MAX_BINS));
+    CK(cudaMemcpy(c->P.reps + q, &R, sizeof(Rep), cudaMemcpyHostToDevice));
+  }
+  return JP_OK;
+}
+
+int jp_ge_hist_get(jp_ctx *c, int32_t r, double *counts, int32_t clear) {
+  if (!c || r < 0 || r >= c->nrep || !counts) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  const Rep &R = c->reps[r];
+  std::vector<unsigned long long> h(R.hist_n);
+  if (R.hist_n > 0)
+    CK(cudaMemcpy(h.data(), c->P.ge_hist + R.hist_off, sizeof(unsigned long long) * R.hist_n,
+                  cudaMemcpyDeviceToHost));
+  for (int i = 0; i < R.hist_n; ++i) counts[i] = (double)h[i];
+  if (clear) CK(cudaMemset(c->P.ge_hist + R.hist_off, 0, sizeof(unsigned long long) * JP_GE_MAX_BINS));
+  return JP_OK;
+}
+
+int jp_ge_set(jp_ctx *c, int32_t r, const jp_ge *g) {
+  if (!c || r < 0 || r >= c->nrep || !g) return JP_E_INVALID;
+  if (c->prm.method != JP_METHOD_GE) return JP_E_INVALID;
+  if (g->nwindow < 1 || g->nwindow > JP_GE_MAX_WINDOWS || g->ndeg < 0 || g->ndeg > JP_GE_MAX_DEG ||
+      !g->coef || !g->low || !g->high || !(g->ceup > g->celw))
+    return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  Rep &R = c->reps[r];
+  std::vector<double> slot(kGeCap, 0.0);
+  pack_ge(*g, slot.data());
+  R.ge_nwin = g->nwindow;
+  R.ge_ndeg = g->ndeg;
+  R.ge_alphalw = g->alphalw;
+  R.ge_alphaup = g->alphaup;
+  R.ge_celw = g->celw;
+  R.ge_ceup = g->ceup;
+  R.ge_tempce = g->tempce;
+  CK(cudaMemcpy(c->P.ge_coef + R.ge_off, slot.data(), sizeof(double) * kGeCap, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->P.reps + r, &R, sizeof(Rep), cudaMemcpyHostToDevice));
+  return JP_OK;
 }
 
 int jp_pair_count(jp_ctx *c, int32_t r, int64_t *count) {

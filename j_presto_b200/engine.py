@@ -20,7 +20,8 @@ _lib = None
 EXPORTS = ["jp_default_params", "jp_create", "jp_rebuild_cells", "jp_energy_grad", "jp_step",
            "jp_shake", "jp_get_state", "jp_set_state", "jp_pair_count", "jp_set_timing",
            "jp_last_timing", "jp_launch_counts", "jp_list_stats", "jp_calibrate_fp32",
-           "jp_strerror", "jp_destroy", "jp_nonbond_noalloc"]
+           "jp_strerror", "jp_destroy", "jp_nonbond_noalloc", "jp_ge_hist_setup",
+           "jp_ge_hist_get", "jp_ge_set", "jp_lstsq_windows", "jp_ge_fit"]
 
 
 class JpError(RuntimeError):
@@ -58,6 +59,12 @@ def lib():
         L.jp_strerror.restype = C.c_char_p
         L.jp_destroy.argtypes = [vp]
         L.jp_destroy.restype = None
+        L.jp_ge_hist_setup.argtypes = [vp, ip, C.c_double, C.c_double, ip, ip]
+        L.jp_ge_hist_get.argtypes = [vp, ip, dp, ip]
+        L.jp_ge_set.argtypes = [vp, ip, C.POINTER(abi.JpGe)]
+        L.jp_lstsq_windows.argtypes = [ip, ip, ip, C.c_double, C.c_double, dp, dp, dp, dp, dp, dp, dp]
+        L.jp_ge_fit.argtypes = [dp, C.POINTER(abi.JpGeFitParams), C.POINTER(abi.JpGe), dp, dp, dp,
+                                C.POINTER(abi.JpGe), dp]
         # all array arguments are device addresses except box (host double[3])
         L.jp_nonbond_noalloc.argtypes = [ip, vp, vp, vp, ip, vp, vp, vp, vp, ip, dp, C.c_double,
                                          C.c_double, vp, vp, vp]
@@ -73,6 +80,34 @@ def _chk(code, where, warn_ok=False):
     if code < 0 or (code > 0 and not warn_ok):
         raise JpError(code, where)
     return code
+
+
+def lstsq_windows(x, y, w, nwindow, ndeg, minv=0.0, maxv=1.0):
+    """lstsquare_final: windowed weighted polynomial fit; returns (coef, low, high, resid)."""
+    x, y, w = (np.ascontiguousarray(a, np.float64) for a in (x, y, w))
+    coef = np.zeros((nwindow, ndeg + 1))
+    low, high, resid = np.zeros(nwindow), np.zeros(nwindow), np.zeros(2)
+    _chk(lib().jp_lstsq_windows(nwindow, len(x), ndeg, minv, maxv, _dp(x), _dp(y), _dp(w),
+                                _dp(coef), _dp(low), _dp(high), _dp(resid)), "jp_lstsq_windows")
+    return coef, low, high, resid
+
+
+def ge_fit(hist, old_nf, emin, emax, nbin, nbor, next_emin, next_emax, next_temp, nwindow, ndeg,
+           ignore_empty=True, neglect_low=False, neglect_high=False):
+    """One McMD weight iteration (distrib_MULT): new weight dict and residual errors."""
+    keep = []
+    h = np.ascontiguousarray(hist, np.float64)
+    fp = abi.JpGeFitParams(emin, emax, nbin, nbor, next_emin, next_emax, next_temp, nwindow, ndeg,
+                           int(ignore_empty), int(neglect_low), int(neglect_high))
+    old = abi.make_ge(old_nf, keep)
+    coef = np.zeros((nwindow, ndeg + 1))
+    low, high, resid = np.zeros(nwindow), np.zeros(nwindow), np.zeros(2)
+    out = abi.JpGe()
+    _chk(lib().jp_ge_fit(_dp(h), C.byref(fp), C.byref(old), _dp(coef), _dp(low), _dp(high),
+                         C.byref(out), _dp(resid)), "jp_ge_fit")
+    nf = dict(coef=coef, low=low, high=high, alphalw=out.alphalw, alphaup=out.alphaup,
+              celw=out.celw, ceup=out.ceup, tempce=out.tempce, lower=out.lower, upper=out.upper)
+    return nf, resid
 
 
 def calibrate_fp32(device=0):
@@ -93,6 +128,7 @@ class Engine:
         self.natoms = [int(t["natom"]) for t in tops]
         self.params = params if params is not None else abi.default_params(**kw)
         self._keep = []
+        self._hist_n = {}
         self._sys = abi.make_systems(tops, self._keep)
         h = C.c_void_p()
         _chk(lib().jp_create(self._sys, self.nrep, C.byref(self.params), C.byref(h)), "jp_create")
@@ -136,6 +172,23 @@ class Engine:
         g = np.zeros((n, 3))
         _chk(lib().jp_energy_grad(self._h, rep, _dp(c), _dp(e), _dp(g)), "jp_energy_grad")
         return e, g
+
+    # ---- McMD iteration ----
+    def ge_hist_setup(self, emin, emax, nbin, nbor, rep=-1):
+        _chk(lib().jp_ge_hist_setup(self._h, rep, emin, emax, nbin, nbor), "jp_ge_hist_setup")
+        for r in (range(self.nrep) if rep < 0 else [rep]):
+            self._hist_n[r] = nbin + 2 * nbor if nbin > 0 else 0
+
+    def ge_hist_get(self, rep=0, clear=False):
+        n = int(self._hist_n.get(rep, abi.JP_GE_MAX_BINS))
+        h = np.zeros(abi.JP_GE_MAX_BINS)
+        _chk(lib().jp_ge_hist_get(self._h, rep, _dp(h), int(clear)), "jp_ge_hist_get")
+        return h[:n]
+
+    def ge_set(self, nf, rep=0):
+        keep = []
+        g = abi.make_ge(nf, keep)
+        _chk(lib().jp_ge_set(self._h, rep, C.byref(g)), "jp_ge_set")
 
     def pair_count(self, rep=0):
         v = C.c_int64()
