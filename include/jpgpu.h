@@ -245,6 +245,39 @@ int jp_lstsq_windows(int32_t nwindow, int32_t ndat, int32_t ndim, double minv, d
 int jp_ge_fit(const double *hist, const jp_ge_fit_params *fp, const jp_ge *old, double *coef,
               double *low, double *high, jp_ge *out, double *resid);
 
+/* Host only.  The fit data of jp_ge_fit (distrib_MULT.f90:322-420): points x (reduced energy
+ * of the next range), y = d lnN/dE and weights w, each of capacity nbin + 2 nbor; *ndat out. */
+int jp_ge_dlnn(const double *hist, const jp_ge_fit_params *fp, const jp_ge *old, double *x,
+               double *y, double *w, int32_t *ndat);
+
+/* Weight surrogate network: nin -> 64 -> 64 -> nout (tanh), FP32, nin, nout <= 2.  It stands
+ * in for the polynomial of jp_ge_fit (nin = nout = 1: reduced energy -> d lnN/dE; ALSD:
+ * (E, lambda) -> its two derivatives).  Parameters are one flat float vector of
+ * jp_mlp_nparam(nin, nout) entries (layout in csrc/jp_mlp.cuh).
+ * jp_mlp_init: Glorot-uniform weights from `seed`, input/target normalisation from the data
+ *   of each of nnet networks (samples off[k]..off[k+1]-1 of x[][nin], y[][nout]).
+ * jp_mlp_train: `epochs` full-batch Adam steps (learning rate lr) of all nnet networks at once
+ *   on `device`, one CUDA block per network, minimising sum w (net - y)^2 / sum w in
+ *   normalised units; params in/out [nnet][np]; loss[nnet] at the final parameters;
+ *   grad[nnet][np] (nullable) the gradient there (epochs = 0: at the given parameters).
+ * jp_mlp_forward: y[n][nout] of one network at x[n][nin] on `device`. */
+#define JP_MLP_HIDDEN 64
+#define JP_MLP_MAXIO 2
+int32_t jp_mlp_nparam(int32_t nin, int32_t nout);
+int jp_mlp_init(int32_t nin, int32_t nout, int32_t nnet, const float *x, const float *y,
+                const int32_t *off, uint64_t seed, float *params);
+int jp_mlp_train(int32_t nin, int32_t nout, int32_t nnet, const float *x, const float *y,
+                 const float *w, const int32_t *off, int32_t epochs, float lr, int32_t device,
+                 float *params, float *loss, float *grad);
+int jp_mlp_forward(int32_t nin, int32_t nout, const float *params, const float *x, int32_t n,
+                   int32_t device, float *y);
+
+/* McMD force scaling by the network instead of the polynomial for `replica` (METHOD= GE):
+ * inside [celw, ceup] of its current weight d lnN/dE = net(x), x the reduced energy;
+ * outside, alphalw / alphaup as before.  params: jp_mlp_nparam(1, 1) floats, or NULL to go
+ * back to the polynomial.  The next jp_step re-captures its step graph. */
+int jp_ge_set_mlp(jp_ctx *ctx, int32_t replica, const float *params);
+
 const char *jp_strerror(int code);
 void jp_destroy(jp_ctx *ctx);
 

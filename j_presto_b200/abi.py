@@ -151,13 +151,7 @@ def make_system(top, keep, cord=None, vel=None):
                         else np.zeros(6), C.c_double, keep)
     ge = top.get("ge")
     if ge is not None:
-        g = JpGe(nwindow=int(ge["nwindow"]), ndeg=int(ge["ndeg"]),
-                 alphalw=float(ge["alphalw"]), alphaup=float(ge["alphaup"]),
-                 celw=float(ge["celw"]), ceup=float(ge["ceup"]), tempce=float(ge["tempce"]),
-                 lower=float(ge.get("lower", 0.0)), upper=float(ge.get("upper", 0.0)))
-        g.coef = _ptr(np.asarray(ge["coef"]).reshape(-1), C.c_double, keep)
-        g.low = _ptr(ge["low"], C.c_double, keep)
-        g.high = _ptr(ge["high"], C.c_double, keep)
+        g = make_ge(ge, keep)
         keep.append(g)
         s.ge = C.pointer(g)
     return s
@@ -175,8 +169,10 @@ def make_ge(nf, keep):
     """JpGe from a weight dict {coef [nwin][ndeg+1], low, high, alphalw, alphaup, celw, ceup,
     tempce[, lower, upper]}; arrays appended to `keep`."""
     g = JpGe()
-    coef = np.ascontiguousarray(nf["coef"], np.float64)
-    g.nwindow, g.ndeg = coef.shape[0], coef.shape[1] - 1
+    coef = np.asarray(nf["coef"], np.float64)
+    nwin = int(nf.get("nwindow", coef.shape[0] if coef.ndim == 2 else 1))
+    coef = np.ascontiguousarray(coef.reshape(nwin, -1))
+    g.nwindow, g.ndeg = nwin, coef.shape[1] - 1
     g.coef = _ptr(coef, C.c_double, keep)
     g.low = _ptr(np.ascontiguousarray(nf["low"], np.float64), C.c_double, keep)
     g.high = _ptr(np.ascontiguousarray(nf["high"], np.float64), C.c_double, keep)

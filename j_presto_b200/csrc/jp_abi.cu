@@ -172,13 +172,21 @@ void enqueue_bonded(jp_ctx *c) {
 void enqueue_integrate(jp_ctx *c) {
   DevPtrs &P = c->P;
   cudaMemsetAsync(P.kin_fix, 0, sizeof(long long) * c->nkin * c->nsub, c->st);
+  if (c->ic.ge_prescaled) launch_ge_scale(P, c->ic, c->st);
   launch_integrate(P, c->ic, c->nunit, c->fp64, c->cano_grid, c->st);
+}
+
+void drop_graphs(jp_ctx *c) {
+  if (c->g_step) cudaGraphExecDestroy(c->g_step);
+  if (c->g_rebuild) cudaGraphExecDestroy(c->g_rebuild);
+  c->g_step = c->g_rebuild = nullptr;
 }
 
 int launches_per_step(const jp_ctx *c) {
   int n = 1;                       // pair
   n += c->nterm > 0 ? 1 : 0;      // bonded
   n += 1;                          // the fused cooperative MICR or CANO/GE kernel
+  n += c->ic.ge_prescaled ? 1 : 0; // k_ge_scale
   return n;
 }
 
@@ -649,6 +657,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dput(c, &P.reps, reps);
   e |= dput(c, &P.ge_coef, hge);
   e |= dalloc(c, &P.ge_hist, (size_t)nrep * JP_GE_MAX_BINS);
+  e |= dalloc(c, &P.mlp, (size_t)nrep * kMlpSlot);
   e |= dalloc(c, &P.ene_fix, 16 * (size_t)nrep);
   e |= dalloc(c, &P.kin_fix, (size_t)c->nkin * c->nsub);
   e |= dput(c, &P.nfr, hnfr);
@@ -694,6 +703,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   ic.nquad = (int)quad_idx.size();
   ic.qbase = (ic.nsmall + 31) / 32 * 32;
   ic.nvirt = ic.qbase + (8 * ic.nquad + 31) / 32 * 32;
+  ic.ge_prescaled = 0;
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   c->pair_warps = std::max(1, nsm) * 8 * 6;   // 6 blocks of 8 warps per SM
@@ -845,6 +855,27 @@ int jp_ge_set(jp_ctx *c, int32_t r, const jp_ge *g) {
   R.ge_tempce = g->tempce;
   CK(cudaMemcpy(c->P.ge_coef + R.ge_off, slot.data(), sizeof(double) * kGeCap, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->P.reps + r, &R, sizeof(Rep), cudaMemcpyHostToDevice));
+  return JP_OK;
+}
+
+int jp_ge_set_mlp(jp_ctx *c, int32_t r, const float *params) {
+  if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
+  if (c->prm.method != JP_METHOD_GE) return JP_E_INVALID;
+  const int np = jp_mlp_nparam(1, 1);
+  if (np < 0 || np > kMlpSlot) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  Rep &R = c->reps[r];
+  R.mlp_on = params ? 1 : 0;
+  if (params) CK(cudaMemcpy(c->P.mlp + (size_t)r * kMlpSlot, params, sizeof(float) * np,
+                            cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->P.reps + r, &R, sizeof(Rep), cudaMemcpyHostToDevice));
+  int any = 0;
+  for (int q = 0; q < c->nrep; ++q) any |= c->reps[q].mlp_on;
+  if (any != c->ic.ge_prescaled) {   // the step graph changes: capture it again
+    c->ic.ge_prescaled = any;
+    drop_graphs(c);
+  }
   return JP_OK;
 }
 

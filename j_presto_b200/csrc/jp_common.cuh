@@ -55,6 +55,8 @@ struct Rep {
   double ge_alphalw, ge_alphaup, ge_celw, ge_ceup, ge_tempce;
   int hist_off, hist_n;           // energy histogram slot and bin count (0 = off)
   double hist_min, hist_inv;      // lower edge of bin 0 and 1 / bin width
+  int mlp_on;                     // McMD weight from the surrogate network instead of the polynomial
+  int pad_;
 };
 
 // integration unit: a SHAKE group (2-4 atoms) or a lone atom (n = 1)
@@ -120,6 +122,7 @@ struct DevPtrs {
   Rep *reps;
   double *ge_coef;                // JP_GE_MAX_WINDOWS * (JP_GE_MAX_DEG + 3) per replica
   unsigned long long *ge_hist;    // JP_GE_MAX_BINS per replica
+  float *mlp;                     // surrogate network parameters, kMlpSlot per replica
   // accumulators
   long long *ene_fix;             // [nrep][16]
   long long *kin_fix;             // [nslots_kin][nsub_total]

@@ -240,12 +240,11 @@ extern "C" int jp_lstsq_windows(int32_t nwindow, int32_t ndat, int32_t ndim, dou
   return JP_OK;
 }
 
-extern "C" int jp_ge_fit(const double *hist, const jp_ge_fit_params *fp, const jp_ge *old,
-                         double *coef, double *low, double *high, jp_ge *out, double *resid) {
-  if (!hist || !fp || !old || !coef || !low || !high || !out) return JP_E_INVALID;
-  const int nbin = fp->nbin, nbor = fp->nbor, nw = fp->nwindow, nd = fp->ndeg;
-  if (nbin < 2 || nbor < 0 || nw < 1 || nw > JP_GE_MAX_WINDOWS || nd < 1 || nd > JP_GE_MAX_DEG ||
-      !(fp->emax > fp->emin) || !(fp->next_emax > fp->next_emin))
+extern "C" int jp_ge_dlnn(const double *hist, const jp_ge_fit_params *fp, const jp_ge *old,
+                          double *xo, double *yo, double *wo, int32_t *ndat) {
+  if (!hist || !fp || !old || !xo || !yo || !wo || !ndat) return JP_E_INVALID;
+  const int nbin = fp->nbin, nbor = fp->nbor;
+  if (nbin < 2 || nbor < 0 || !(fp->emax > fp->emin) || !(fp->next_emax > fp->next_emin))
     return JP_E_INVALID;
   if (old->nwindow < 1 || old->ndeg < 0 || !old->coef || !old->low || !old->high ||
       !(old->ceup > old->celw))
@@ -284,22 +283,41 @@ extern "C" int jp_ge_fit(const double *hist, const jp_ge_fit_params *fp, const j
   // data on the next range
   const int ist = fp->neglect_low ? nbor : 0;
   const int ien = fp->neglect_high ? nbor + nbin - 1 : nab - 2;
-  std::vector<double> X, Y, W;
+  int n = 0;
   for (int i = ist; i <= ien; ++i) {
     const double x2 = (ee[i] + 0.5 * de - fp->next_emin) / (fp->next_emax - fp->next_emin);
     const double cnt = hist[i] + hist[i + 1];
+    double wv;
     if (fp->ignore_empty) {
       if (dlnn[i] == 0.0) continue;
-      X.push_back(x2); Y.push_back(dlnn[i]); W.push_back(std::sqrt(cnt));
+      wv = std::sqrt(cnt);
     } else {
       if (dlnn[i] == 0.0 && (x2 < old->celw || x2 > old->ceup)) continue;
-      X.push_back(x2); Y.push_back(dlnn[i]); W.push_back(std::max(std::sqrt(cnt), 1.0));
+      wv = std::max(std::sqrt(cnt), 1.0);
     }
+    xo[n] = x2; yo[n] = dlnn[i]; wo[n] = wv;
+    ++n;
   }
-  if ((int)X.size() < 2 * nw * (nd + 1)) return JP_E_INVALID;
+  *ndat = n;
+  return JP_OK;
+}
+
+extern "C" int jp_ge_fit(const double *hist, const jp_ge_fit_params *fp, const jp_ge *old,
+                         double *coef, double *low, double *high, jp_ge *out, double *resid) {
+  if (!hist || !fp || !old || !coef || !low || !high || !out) return JP_E_INVALID;
+  const int nw = fp->nwindow, nd = fp->ndeg;
+  if (fp->nbin < 2 || fp->nbor < 0 || nw < 1 || nw > JP_GE_MAX_WINDOWS || nd < 1 ||
+      nd > JP_GE_MAX_DEG)
+    return JP_E_INVALID;
+  const int cap = fp->nbin + 2 * fp->nbor;
+  std::vector<double> X(cap), Y(cap), W(cap);
+  int32_t ndat = 0;
+  const int rd = jp_ge_dlnn(hist, fp, old, X.data(), Y.data(), W.data(), &ndat);
+  if (rd) return rd;
+  if (ndat < 2 * nw * (nd + 1)) return JP_E_INVALID;
   double r[2] = {0.0, 0.0};
-  const int rc = jp_lstsq_windows(nw, (int)X.size(), nd, 0.0, 1.0, X.data(), Y.data(), W.data(), coef,
-                                  low, high, r);
+  const int rc = jp_lstsq_windows(nw, ndat, nd, 0.0, 1.0, X.data(), Y.data(), W.data(), coef, low,
+                                  high, r);
   if (rc) return rc;
   if (resid) { resid[0] = r[0]; resid[1] = r[1]; }
   double upd = coef[(size_t)(nw - 1) * (nd + 1)];

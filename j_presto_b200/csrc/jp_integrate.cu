@@ -11,6 +11,7 @@
 #include <algorithm>
 
 #include "jp_kernels.h"
+#include "jp_mlp.cuh"
 
 namespace jp {
 
@@ -337,7 +338,14 @@ __device__ bool cano_active(const DevPtrs& P, const IntConst& c, const Rep& R, i
 // ---- per-replica preparation --------------------------------------------------------
 // force scale of replica r for this step: McMD weight (verlethe.f90:196-238) from the total
 // potential energy, or the pseudo-temperature factor (verlet.f90:118-142)
-__device__ double rep_scale(const DevPtrs& P, const IntConst& c, int r) {
+__device__ double rep_scale_poly(const DevPtrs& P, const IntConst& c, int r);
+
+__device__ __forceinline__ double rep_scale(const DevPtrs& P, const IntConst& c, int r) {
+  if (c.ge_prescaled) return __ldcg(&P.scale[r]);
+  return rep_scale_poly(P, c, r);
+}
+
+__device__ double rep_scale_poly(const DevPtrs& P, const IntConst& c, int r) {
   const Rep& R = P.reps[r];
   if (c.method == JP_METHOD_GE && R.ge_nwin > 0) {
     double tot = R.dself;
@@ -362,6 +370,38 @@ __device__ double rep_scale(const DevPtrs& P, const IntConst& c, int r) {
   }
   if (c.psetmp > 1.0e-10) return c.temp / c.psetmp;
   return 1.0;
+}
+
+// k_ge_scale: one warp per replica.  McMD replicas with the surrogate network evaluate
+// d lnN/dE = net(x) at the reduced energy x inside [celw, ceup] (alphalw / alphaup outside,
+// as verlethe.f90:196-238 does for the polynomial); all others as rep_scale_poly.
+__global__ void __launch_bounds__(32) k_ge_scale(DevPtrs P, IntConst c) {
+  const int r = blockIdx.x;
+  const Rep& R = P.reps[r];
+  double s;
+  if (c.method == JP_METHOD_GE && R.ge_nwin > 0 && R.mlp_on) {
+    double tot = R.dself;
+    for (int k = 1; k < JP_MAXENE; ++k) tot += (double)__ldcg(&P.ene_fix[r * 16 + k]) * kEneInv;
+    double dprobl;
+    if (tot <= R.ge_celw) {
+      dprobl = R.ge_alphalw;
+    } else if (tot >= R.ge_ceup) {
+      dprobl = R.ge_alphaup;
+    } else {
+      const float x = (float)((tot - R.ge_celw) / (R.ge_ceup - R.ge_celw));
+      float y;
+      mlp_forward_warp(P.mlp + (size_t)r * kMlpSlot, 1, 1, &x, &y);
+      dprobl = (double)y;
+    }
+    s = (kGas / kJouCal) * 1.0e-3 * R.ge_tempce * dprobl;
+  } else {
+    s = rep_scale_poly(P, c, r);
+  }
+  if (threadIdx.x == 0) P.scale[r] = s;
+}
+
+void launch_ge_scale(const DevPtrs& P, const IntConst& c, cudaStream_t st) {
+  k_ge_scale<<<c.nrep, 32, 0, st>>>(P, c);
 }
 
 // energies of this step (time t) into the per-step history: eneval(15) of dnergy

@@ -54,6 +54,7 @@ struct IntConst {
   // virtual lanes of the CANO/GE kernel: [0, nsmall) one 1-3 atom unit each (small_idx),
   // [qbase, nvirt) eight lanes per 4-atom group (quad_idx); qbase and nvirt are multiples of 32
   int nsmall, nquad, qbase, nvirt;
+  int ge_prescaled;        // force scales computed by k_ge_scale before the integration kernel
 };
 int cano_grid(bool fp64, int device);   // co-resident blocks of the integration kernels
 // one cooperative launch: energies of the step, force scale, verlet (MICR) or verlethe
@@ -61,5 +62,8 @@ int cano_grid(bool fp64, int device);   // co-resident blocks of the integration
 void launch_integrate(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
                       cudaStream_t st);
 void launch_shake_only(const DevPtrs& P, const IntConst& c, int unit0, int nunit, cudaStream_t st);
+// per-replica force scale of this step (McMD polynomial or surrogate network) into P.scale
+void launch_ge_scale(const DevPtrs& P, const IntConst& c, cudaStream_t st);
+constexpr int kMlpSlot = 4400;   // floats per replica >= jp_mlp_nparam(1, 1)
 
 }  // namespace jp

@@ -21,7 +21,8 @@ EXPORTS = ["jp_default_params", "jp_create", "jp_rebuild_cells", "jp_energy_grad
            "jp_shake", "jp_get_state", "jp_set_state", "jp_pair_count", "jp_set_timing",
            "jp_last_timing", "jp_launch_counts", "jp_list_stats", "jp_calibrate_fp32",
            "jp_strerror", "jp_destroy", "jp_nonbond_noalloc", "jp_ge_hist_setup",
-           "jp_ge_hist_get", "jp_ge_set", "jp_lstsq_windows", "jp_ge_fit"]
+           "jp_ge_hist_get", "jp_ge_set", "jp_lstsq_windows", "jp_ge_fit", "jp_ge_dlnn",
+           "jp_mlp_nparam", "jp_mlp_init", "jp_mlp_train", "jp_mlp_forward", "jp_ge_set_mlp"]
 
 
 class JpError(RuntimeError):
@@ -65,6 +66,16 @@ def lib():
         L.jp_lstsq_windows.argtypes = [ip, ip, ip, C.c_double, C.c_double, dp, dp, dp, dp, dp, dp, dp]
         L.jp_ge_fit.argtypes = [dp, C.POINTER(abi.JpGeFitParams), C.POINTER(abi.JpGe), dp, dp, dp,
                                 C.POINTER(abi.JpGe), dp]
+        fp_ = C.POINTER(C.c_float)
+        L.jp_ge_dlnn.argtypes = [dp, C.POINTER(abi.JpGeFitParams), C.POINTER(abi.JpGe), dp, dp, dp,
+                                 C.POINTER(C.c_int32)]
+        L.jp_mlp_nparam.argtypes = [ip, ip]
+        L.jp_mlp_nparam.restype = C.c_int32
+        L.jp_mlp_init.argtypes = [ip, ip, ip, fp_, fp_, C.POINTER(C.c_int32), C.c_uint64, fp_]
+        L.jp_mlp_train.argtypes = [ip, ip, ip, fp_, fp_, fp_, C.POINTER(C.c_int32), ip, C.c_float, ip,
+                                   fp_, fp_, fp_]
+        L.jp_mlp_forward.argtypes = [ip, ip, fp_, fp_, ip, ip, fp_]
+        L.jp_ge_set_mlp.argtypes = [vp, ip, fp_]
         # all array arguments are device addresses except box (host double[3])
         L.jp_nonbond_noalloc.argtypes = [ip, vp, vp, vp, ip, vp, vp, vp, vp, ip, dp, C.c_double,
                                          C.c_double, vp, vp, vp]
@@ -108,6 +119,68 @@ def ge_fit(hist, old_nf, emin, emax, nbin, nbor, next_emin, next_emax, next_temp
     nf = dict(coef=coef, low=low, high=high, alphalw=out.alphalw, alphaup=out.alphaup,
               celw=out.celw, ceup=out.ceup, tempce=out.tempce, lower=out.lower, upper=out.upper)
     return nf, resid
+
+
+def _fp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _fit_params(emin, emax, nbin, nbor, next_emin, next_emax, next_temp, nwindow, ndeg,
+                ignore_empty=True, neglect_low=False, neglect_high=False):
+    return abi.JpGeFitParams(emin, emax, nbin, nbor, next_emin, next_emax, next_temp, nwindow,
+                             ndeg, int(ignore_empty), int(neglect_low), int(neglect_high))
+
+
+def ge_dlnn(hist, old_nf, emin, emax, nbin, nbor, next_emin, next_emax, **kw):
+    """The (x, y = d lnN/dE, w) points the McMD weight fit takes (distrib_MULT)."""
+    keep = []
+    h = np.ascontiguousarray(hist, np.float64)
+    fp = _fit_params(emin, emax, nbin, nbor, next_emin, next_emax, 300.0, 1, 1, **kw)
+    old = abi.make_ge(old_nf, keep)
+    cap = nbin + 2 * nbor
+    x, y, w = np.zeros(cap), np.zeros(cap), np.zeros(cap)
+    n = C.c_int32()
+    _chk(lib().jp_ge_dlnn(_dp(h), C.byref(fp), C.byref(old), _dp(x), _dp(y), _dp(w), C.byref(n)),
+         "jp_ge_dlnn")
+    return x[:n.value].copy(), y[:n.value].copy(), w[:n.value].copy()
+
+
+def mlp_nparam(nin=1, nout=1):
+    return int(lib().jp_mlp_nparam(nin, nout))
+
+
+def mlp_train(data, nin=1, nout=1, epochs=3000, lr=1e-3, seed=1, device=0, params=None,
+              grad=False):
+    """Train one surrogate network per (x[n][nin], y[n][nout], w[n]) dataset, all in one launch.
+    Returns (params [nnet][np], loss [nnet], grad [nnet][np] or None)."""
+    xs = [np.asarray(d[0], np.float32).reshape(len(d[0]), nin) for d in data]
+    ys = [np.asarray(d[1], np.float32).reshape(len(d[1]), nout) for d in data]
+    ws = [np.asarray(d[2], np.float32).reshape(-1) for d in data]
+    off = np.zeros(len(data) + 1, np.int32)
+    off[1:] = np.cumsum([len(w) for w in ws])
+    X = np.ascontiguousarray(np.concatenate(xs)); Y = np.ascontiguousarray(np.concatenate(ys))
+    W = np.ascontiguousarray(np.concatenate(ws))
+    npar = mlp_nparam(nin, nout)
+    if params is None:
+        params = np.zeros((len(data), npar), np.float32)
+        _chk(lib().jp_mlp_init(nin, nout, len(data), _fp(X), _fp(Y),
+                               off.ctypes.data_as(C.POINTER(C.c_int32)), seed, _fp(params)),
+             "jp_mlp_init")
+    params = np.ascontiguousarray(params, np.float32).reshape(len(data), npar).copy()
+    loss = np.zeros(len(data), np.float32)
+    g = np.zeros_like(params) if grad else None
+    _chk(lib().jp_mlp_train(nin, nout, len(data), _fp(X), _fp(Y), _fp(W),
+                            off.ctypes.data_as(C.POINTER(C.c_int32)), int(epochs), float(lr), device,
+                            _fp(params), _fp(loss), _fp(g)), "jp_mlp_train")
+    return params, loss, g
+
+
+def mlp_forward(params, x, nin=1, nout=1, device=0):
+    p = np.ascontiguousarray(params, np.float32).reshape(-1)
+    X = np.ascontiguousarray(np.asarray(x, np.float32).reshape(-1, nin))
+    y = np.zeros((X.shape[0], nout), np.float32)
+    _chk(lib().jp_mlp_forward(nin, nout, _fp(p), _fp(X), X.shape[0], device, _fp(y)), "jp_mlp_forward")
+    return y
 
 
 def calibrate_fp32(device=0):
@@ -189,6 +262,10 @@ class Engine:
         keep = []
         g = abi.make_ge(nf, keep)
         _chk(lib().jp_ge_set(self._h, rep, C.byref(g)), "jp_ge_set")
+
+    def ge_set_mlp(self, params, rep=0):
+        p = None if params is None else np.ascontiguousarray(params, np.float32).reshape(-1)
+        _chk(lib().jp_ge_set_mlp(self._h, rep, _fp(p)), "jp_ge_set_mlp")
 
     def pair_count(self, rep=0):
         v = C.c_int64()
