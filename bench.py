@@ -203,6 +203,50 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def c4_measure(dev, steps=20, warmup=3):
+    """C4: 64 uneven McMD replicas (8-30-residue chains in 600-9,000 waters), batched in one
+    mixed-precision context (one CUDA graph per step) against the same 64 run one after the
+    other on the FP64 path.  Both device-timed over `steps` steps after `warmup`."""
+    from j_presto_b200 import abi, engine, systems
+    reps = systems.config_c4(workers=os.cpu_count())
+    natoms = [int(t["natom"]) for t in reps]
+    for t in reps:                       # a placeholder to create the McMD contexts
+        t["ge"] = systems.mcmd_weight(-1.0e7, 1.0e7)
+    kw = dict(method=abi.JP_METHOD_GE, device=dev)
+    eng = engine.Engine(reps, precision=abi.JP_PREC_MIXED, **kw)
+    weights = []
+    for r, t in enumerate(reps):         # 280-700 K over a range around each start energy
+        e0 = eng.energy_grad(r)[0][0]
+        w = systems.mcmd_weight(e0 - 0.1 * natoms[r], e0 + 0.3 * natoms[r])
+        weights.append(w)
+        eng.ge_set(w, r)
+    eng.step(warmup, energies=False, temps=False)
+    eng.step(steps, energies=False, temps=False)
+    t_mix = eng.last_timing()[0] / 1e3
+    per_step, _ = eng.launch_counts()
+    eng.close()
+    t64 = 0.0
+    for r, t in enumerate(reps):
+        t["ge"] = weights[r]
+        e = engine.Engine(t, precision=abi.JP_PREC_FP64, **kw)
+        e.step(warmup, energies=False, temps=False)
+        e.step(steps, energies=False, temps=False)
+        t64 += e.last_timing()[0] / 1e3
+        e.close()
+    n = len(reps)
+    mix = ns_per_day(steps * n, t_mix)
+    fp64 = ns_per_day(steps * n, t64)
+    return {"workload": f"{n} McMD replicas (METHOD= GE, degree-8 weights 280-700 K): 8-30-residue "
+                        f"chains in 600-9,000 waters, {min(natoms):,}-{max(natoms):,} atoms, "
+                        f"{sum(natoms):,} in total, 2 fs, SHAKE X-H + rigid water",
+            "atoms": sum(natoms), "replicas": n, "steps": steps,
+            "mixed_batched": {"value": mix, "unit": "ns/day (aggregate)",
+                              "ms_per_step": 1e3 * t_mix / steps, "launches_per_step": per_step},
+            "fp64_back_to_back": {"value": fp64, "unit": "ns/day (aggregate)",
+                                  "ms_per_step": 1e3 * t64 / steps},
+            "speedup": mix / fp64}
+
+
 def timed_loop(eng, steps, flush_buf):
     """K device-timed steps, L2 flushed between steps; returns per-step ms."""
     import torch
@@ -222,6 +266,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
+    ap.add_argument("--no-c4", action="store_true", help="skip the 64-replica batched McMD line")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local = dist_setup(args.gpus)
@@ -298,6 +343,7 @@ def main():
     traffic, tsrc = ncu_traffic()
     hbm_peak = measured_peaks().get("hbm_gbs")
     cpu = None if args.no_cpu else cpu_baseline(top)
+    c4 = None if (args.no_c4 or world > 1) else c4_measure(dev)
     clocks = clk.summary()
     nreb = args.steps // 10
     line = {
@@ -334,6 +380,7 @@ def main():
                              "CUDA-event launch time; peak = FP32 FMA loop measured in this run "
                              "(MEASURED_PEAKS.json lists HBM and bf16 tensor peaks only)"},
         "cpu_baseline": cpu,
+        "c4_batched_mcmd": c4,
     }
     print(json.dumps(line), flush=True)
     barrier()

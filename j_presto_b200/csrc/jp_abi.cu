@@ -706,7 +706,8 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   ic.ge_prescaled = 0;
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  c->pair_warps = std::max(1, nsm) * 8 * 6;   // 6 blocks of 8 warps per SM
+  // one wave: every warp resident at once, each with an equal share of the tiles
+  c->pair_warps = std::max(1, nsm) * (256 / 32) * pair_blocks_per_sm(c->fp64, c->zc.nt1);
   c->cano_grid = cano_grid(c->fp64, c->device);
   CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   CK(cudaEventCreate(&c->ev_a));

@@ -29,6 +29,8 @@ struct ZdConst {
 void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool minimg, bool count,
                        cudaStream_t st);
 void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, cudaStream_t st);
+// co-resident blocks per SM of the (non-counting) pair kernel: the grid is one full wave
+int pair_blocks_per_sm(bool fp64, int nt1);
 void launch_update_pos(const DevPtrs& P, int nslot, bool fp64, double qscale, cudaStream_t st);
 
 // bonded (jp_bonded.cu)

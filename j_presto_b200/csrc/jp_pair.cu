@@ -289,6 +289,17 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
   flush_energy(P, cur_rep, eel, elj, npair, COUNT);
 }
 
+int pair_blocks_per_sm(bool fp64, int nt1) {
+  int per = 0;
+  if (fp64)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_fp64<false>, kPairThreads,
+                                                  sizeof(double2) * nt1 * nt1);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_mixed<false>, kPairThreads,
+                                                  sizeof(float2) * nt1 * nt1);
+  return per > 0 ? per : 1;
+}
+
 void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool, bool count,
                        cudaStream_t st) {
   const int wpb = kPairThreads / 32;

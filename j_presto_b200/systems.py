@@ -559,18 +559,29 @@ def config_c3(seed=3):
     return solvated_polymer(0, 33000, box=100.0, seed=seed, nion_pairs=100)
 
 
-def config_c4(nrep=64, seed=4, small=False):
+def _c4_one(args):
+    nres, nwat, seed = args
+    return solvated_polymer(nres, nwat, seed=seed)
+
+
+def config_c4(nrep=64, seed=4, small=False, workers=None):
     """64 uneven replicas: 8-30-residue chains in 600-9,000 waters (2k-30k atoms).
-    small=True shrinks the water counts tenfold for CPU tests."""
+    small=True shrinks the water counts tenfold for CPU tests.  workers > 1 builds the
+    replicas in a process pool started with `spawn` (safe next to CUDA)."""
     rng = np.random.default_rng(seed)
-    reps = []
+    jobs = []
     for r in range(nrep):
         nres = int(rng.integers(8, 31))
         nwat = int(rng.integers(600, 9001))
         if small:
             nwat = max(300, nwat // 10)
-        reps.append(solvated_polymer(nres, nwat, seed=seed * 1000 + r))
-    return reps
+        jobs.append((nres, nwat, seed * 1000 + r))
+    if workers and workers > 1:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(_c4_one, jobs))
+    return [_c4_one(j) for j in jobs]
 
 
 def config_c5(nrep=32, seed=5, nwat=3000):
