@@ -3,8 +3,9 @@
     python -m j_presto_b200.profile --workload c2 --precision mixed --steps 20 [--direct]
 
 --direct launches every kernel individually (timing mode) instead of replaying CUDA graphs.
-Workloads: c1 (3,000 waters, 31 A), c1p (1,000 waters), c2 (solvated polymer, 22,784
-atoms), c3 (33,000 waters + 200 ions), small (6-residue chain in 700 waters).
+Workloads: c1 (3,000 waters, 31 A), c1p (1,000 waters), c2 (solvated polymer, 22,860
+atoms), c3 (33,000 waters + 200 ions), c4 (64 McMD replicas, 1.06 M atoms), small
+(6-residue chain in 700 waters), w7000 (7,000 waters, 62 A).
 """
 import argparse
 
@@ -17,6 +18,7 @@ WORKLOADS = {
     "c3": systems.config_c3,
     "small": lambda: systems.solvated_polymer(6, 700, seed=11),
     "w7000": lambda: systems.water_box(7000, 62.0, seed=9),
+    "c4": None,   # 64 McMD replicas, built below
 }
 
 
@@ -30,15 +32,23 @@ def main():
     ap.add_argument("--tempco", type=int, default=2, choices=[1, 2])
     a = ap.parse_args()
     build.build()
-    top = WORKLOADS[a.workload]()
     prec = abi.JP_PREC_MIXED if a.precision == "mixed" else abi.JP_PREC_FP64
     meth = abi.JP_METHOD_CANO if a.method == "cano" else abi.JP_METHOD_MICR
+    if a.workload == "c4":
+        import os
+        top = systems.config_c4(workers=os.cpu_count())
+        for t in top:
+            t["ge"] = systems.mcmd_weight(-1.0e7, 1.0e7)
+        meth = abi.JP_METHOD_GE
+    else:
+        top = WORKLOADS[a.workload]()
     with engine.Engine(top, precision=prec, method=meth, tempco=a.tempco) as e:
         e.set_timing(a.direct)
         e.step(a.steps, energies=False, temps=False)
         tot, ph, ln = e.last_timing()
         nt, nl, ns = e.list_stats()
-    print(f"{a.workload} natom={top['natom']} steps={a.steps} ms/step={tot / a.steps:.4f} "
+    natom = sum(t["natom"] for t in top) if isinstance(top, list) else top["natom"]
+    print(f"{a.workload} natom={natom} steps={a.steps} ms/step={tot / a.steps:.4f} "
           f"tiles={nt} listed={nl} phases_ms={[round(p, 4) for p in ph]} launches={ln}")
 
 
