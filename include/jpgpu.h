@@ -129,6 +129,8 @@ typedef struct jp_system {
   const double *shake_dist;    /* [nshake][6] target distances d0 in md_run pair order
                                   (1,2),(2,3),(3,1),(4,1),(3,4),(2,4) -- setshk.f90 redshk */
   const jp_ge *ge;             /* McMD weight for METHOD= GE; NULL otherwise */
+  const int32_t *cluster;      /* [natom] 1 = atom of the lambda-scaled cluster (CLUSTA
+                                  residues, inpcls.f90 icls = 1), else 0; NULL = none */
 } jp_system;
 
 /* Run parameters shared by all replicas of a context (md.inp EXE> MD keywords). */
@@ -150,7 +152,20 @@ typedef struct jp_params {
   double fcstol;         /* their tolerance (md_run default 1e-3) */
   double psetmp;         /* PSETMP pseudo temperature; 0 = off */
   int32_t device;        /* CUDA device ordinal */
+  /* Adaptive lambda square dynamics (ALSD, CLSTMETHOD= LMD / LMD2, inpcls.f90, verlethe.f90
+   * :110-165, :240-321): with jp_system.cluster set, every term of class AA / AB / BB
+   * (both / one / no atom in the cluster) enters the forces times lambda^2 / lambda / 1
+   * (LMD) or lambda / sqrt(lambda) / 1 (LMD2); lambda moves under
+   * f = -2 E_AA lambda - E_AB - dew (LMD), dew the McMD weight in lambda (METHOD= GE). */
+  int32_t alsd;          /* JP_ALSD_* */
+  double lambda0;        /* initial lambda (LAMBDA) */
+  double lambda_mass;    /* its mass; 0 = total mass of the cluster (inpcls.f90:350-360) */
+  int32_t lambda_temp_control;  /* lambda velocity coupled to the thermostat (l_temp_control) */
+  int32_t scale_terms;   /* SCALET: JP_SCALE_* bits; non-bonded terms are always scaled */
 } jp_params;
+
+enum { JP_ALSD_NONE = 0, JP_ALSD_LMD = 1, JP_ALSD_LMD2 = 2 };
+enum { JP_SCALE_BOND = 1, JP_SCALE_ANGLE = 2, JP_SCALE_TORS = 4, JP_SCALE_IMPR = 8 };
 
 typedef struct jp_ctx jp_ctx;
 
@@ -189,6 +204,11 @@ int jp_shake(jp_ctx *ctx, int32_t replica, double *r1, const double *r2);
  * (outrst.f90:56-61, monmd.f90).  Any pointer may be NULL. */
 int jp_get_state(jp_ctx *ctx, int32_t replica, double *cord, double *vel);
 int jp_set_state(jp_ctx *ctx, int32_t replica, const double *cord, const double *vel);
+
+/* ALSD state of one replica: lam2 = {lambda, lambda velocity}; ecls (nullable) = the
+ * energies of classes AA, AB, BB (unscaled) at the last force evaluation. */
+int jp_get_lambda(jp_ctx *ctx, int32_t replica, double *lam2, double *ecls);
+int jp_set_lambda(jp_ctx *ctx, int32_t replica, double lambda, double lambda_v);
 
 /* Number of pair interactions within the cut-off evaluated at the last force call
  * (counts r <= rc among listed pairs, one per unordered pair), per replica. */

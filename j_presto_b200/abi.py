@@ -11,6 +11,8 @@ JP_MAXENE = 15
 JP_PREC_FP64, JP_PREC_MIXED = 0, 1
 JP_METHOD_CONS, JP_METHOD_MICR, JP_METHOD_CANO, JP_METHOD_GE = 1, 2, 3, 4
 JP_SHAKE_NONE, JP_SHAKE_HBON, JP_SHAKE_ALLB = 0, 1, 2
+JP_ALSD_NONE, JP_ALSD_LMD, JP_ALSD_LMD2 = 0, 1, 2
+JP_SCALE_BOND, JP_SCALE_ANGLE, JP_SCALE_TORS, JP_SCALE_IMPR = 1, 2, 4, 8
 # return codes (md_run ier convention: >0 warning, <0 fatal)
 JP_OK = 0
 JP_W_SHAKE_NOT_CONVERGED = 1
@@ -65,7 +67,7 @@ class JpSystem(C.Structure):
         ("nimpr", C.c_int32), ("impr", _ip), ("impr_k", _dp), ("impr_nrot", _dp),
         ("impr_phase", _dp), ("impr_div", _ip),
         ("nshake", C.c_int32), ("shake_n", _ip), ("shake_atoms", _ip), ("shake_dist", _dp),
-        ("ge", C.POINTER(JpGe)),
+        ("ge", C.POINTER(JpGe)), ("cluster", _ip),
     ]
 
 
@@ -77,6 +79,8 @@ class JpParams(C.Structure):
         ("tempco", C.c_int32), ("shake_method", C.c_int32), ("shake_tol", C.c_double),
         ("shake_maxit", C.c_int32), ("icslop", C.c_int32), ("fcstol", C.c_double),
         ("psetmp", C.c_double), ("device", C.c_int32),
+        ("alsd", C.c_int32), ("lambda0", C.c_double), ("lambda_mass", C.c_double),
+        ("lambda_temp_control", C.c_int32), ("scale_terms", C.c_int32),
     ]
 
 
@@ -85,7 +89,8 @@ def default_params(**kw):
     p = JpParams(precision=JP_PREC_MIXED, method=JP_METHOD_CANO, dt=2.0, cutoff=12.0,
                  dielectric=1.0, update=10, temp=300.0, temp_start=300.0, heat_loop=0,
                  tempco=2, shake_method=JP_SHAKE_HBON, shake_tol=1e-6, shake_maxit=1000,
-                 icslop=3, fcstol=1e-3, psetmp=0.0, device=0)
+                 icslop=3, fcstol=1e-3, psetmp=0.0, device=0, alsd=JP_ALSD_NONE, lambda0=1.0,
+                 lambda_mass=0.0, lambda_temp_control=0, scale_terms=0)
     for k, v in kw.items():
         if not hasattr(p, k):
             raise KeyError(k)
@@ -149,6 +154,8 @@ def make_system(top, keep, cord=None, vel=None):
                          else np.zeros(4, np.int32), C.c_int32, keep)
     s.shake_dist = _ptr(np.asarray(top["shake_dist"]).reshape(-1) if len(sh_n)
                         else np.zeros(6), C.c_double, keep)
+    cl = top.get("cluster")
+    s.cluster = None if cl is None else _ptr(np.asarray(cl, np.int32), C.c_int32, keep)
     ge = top.get("ge")
     if ge is not None:
         g = make_ge(ge, keep)

@@ -52,6 +52,7 @@ struct jp_ctx {
   bool fp64 = false;
   bool minimg = true;
   int pair_warps = 0;
+  bool alsd = false;
   int cano_grid = 1;
   int hist_cap = 1024;
   long long idloop = 0;
@@ -152,12 +153,13 @@ void enqueue_zero(jp_ctx *c, bool count) {
   if (c->fp64) cudaMemsetAsync(P.grd, 0, sizeof(double) * 3 * c->natom, st);
   else cudaMemsetAsync(P.frc, 0, sizeof(long long) * 3 * c->natom, st);
   cudaMemsetAsync(P.ene_fix, 0, sizeof(long long) * 16 * c->nrep, st);
+  if (c->alsd) cudaMemsetAsync(P.ene_cls, 0, sizeof(long long) * 4 * c->nrep, st);
   if (count) cudaMemsetAsync(P.pair_cnt, 0, sizeof(long long) * c->nrep, st);
 }
 
 void enqueue_pair(jp_ctx *c, bool count) {
-  if (c->fp64) launch_pair_fp64(c->P, c->zc, c->pair_warps, count, c->st);
-  else launch_pair_mixed(c->P, c->zc, c->pair_warps, c->minimg, count, c->st);
+  if (c->fp64) launch_pair_fp64(c->P, c->zc, c->pair_warps, count, c->alsd, c->st);
+  else launch_pair_mixed(c->P, c->zc, c->pair_warps, c->minimg, count, c->alsd, c->st);
 }
 
 void enqueue_forces(jp_ctx *c, bool count) {
@@ -166,7 +168,7 @@ void enqueue_forces(jp_ctx *c, bool count) {
 }
 
 void enqueue_bonded(jp_ctx *c) {
-  launch_bonded(c->P, c->nterm, c->fp64, c->zc.bcoeff, c->zc.fcoeff, c->st);
+  launch_bonded(c->P, c->nterm, c->fp64, c->zc.bcoeff, c->zc.fcoeff, c->alsd, c->st);
 }
 
 void enqueue_integrate(jp_ctx *c) {
@@ -226,6 +228,11 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
   if (prm->method != JP_METHOD_MICR && prm->method != JP_METHOD_CANO && prm->method != JP_METHOD_GE)
     return JP_E_INVALID;
   if (prm->precision != JP_PREC_FP64 && prm->precision != JP_PREC_MIXED) return JP_E_INVALID;
+  if (prm->alsd < JP_ALSD_NONE || prm->alsd > JP_ALSD_LMD2) return JP_E_INVALID;
+  if (prm->alsd != JP_ALSD_NONE) {   // verlethe only; lambda^(1/2) needs lambda > 0
+    if (prm->method == JP_METHOD_MICR || !std::isfinite(prm->lambda0)) return JP_E_INVALID;
+    if (prm->alsd == JP_ALSD_LMD2 && !(prm->lambda0 > 0.0)) return JP_E_INVALID;
+  }
   const double rlim = prm->cutoff + 1.5;
   for (int r = 0; r < nrep; ++r) {
     const jp_system &s = sys[r];
@@ -298,6 +305,11 @@ void jp_default_params(jp_params *p) {
   p->fcstol = 1.0e-3;              // main.f90:167
   p->psetmp = 0.0;
   p->device = 0;
+  p->alsd = JP_ALSD_NONE;
+  p->lambda0 = 1.0;
+  p->lambda_mass = 0.0;
+  p->lambda_temp_control = 0;
+  p->scale_terms = 0;
 }
 
 const char *jp_strerror(int code) {
@@ -345,7 +357,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   std::vector<int> htyp, hrep, hexp{0}, hexi;
   std::vector<Unit> units;
   std::vector<Term> terms_by_kind[6];
-  std::vector<double> hnfr, hge;
+  std::vector<double> hnfr, hge, hlam;
   std::vector<Rep> reps(nrep);
   const int ntype = sys[0].ntype;
   const int nt1 = ntype + 1;
@@ -389,6 +401,12 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     key0 += R.ncol * R.grid[2];
     // block capacity: every column wastes less than one block
     R.nblk = (n + kTile - 1) / kTile + R.ncol;
+    // ALSD cluster (inpcls.f90 icls): the atom's class bit rides in bit 30 of its LJ type
+    const bool ralsd = prm->alsd != JP_ALSD_NONE && s.cluster;
+    std::vector<int> inA(n, 0);
+    if (ralsd)
+      for (int i = 0; i < n; ++i) inA[i] = s.cluster[i] ? 1 : 0;
+    auto pcls = [&](int a1, int a2) { return ralsd ? 2 - inA[a1] - inA[a2] : 2; };
     for (int i = 0; i < n; ++i) {
       for (int k = 0; k < 3; ++k) {
         hx.push_back(s.cord[3 * i + k]);
@@ -397,7 +415,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       hmass.push_back(s.mass[i]);
       himass.push_back(1.0 / s.mass[i]);
       hchg.push_back(s.charge[i]);
-      htyp.push_back(s.atype[i] - b);
+      htyp.push_back((s.atype[i] - b) | (inA[i] << 30));
       hrep.push_back(r);
     }
     // exclusions
@@ -413,12 +431,14 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     std::vector<int> mol(n, 0);
     int nmol = 1;
     if (s.molecule && prm->tempco == 2) {
+      // with clusters each molecule splits into its cluster and non-cluster part (md.f90
+      // ixamol2 = (ixamol - 1) * nfrag + icls, renumbered densely)
+      auto key = [&](int i) { return ralsd ? 2 * (s.molecule[i] - b) + (inA[i] ? 0 : 1) : s.molecule[i] - b; };
       std::vector<int> u;
-      for (int i = 0; i < n; ++i) u.push_back(s.molecule[i] - b);
+      for (int i = 0; i < n; ++i) u.push_back(key(i));
       std::sort(u.begin(), u.end());
       u.erase(std::unique(u.begin(), u.end()), u.end());
-      for (int i = 0; i < n; ++i)
-        mol[i] = (int)(std::lower_bound(u.begin(), u.end(), s.molecule[i] - b) - u.begin());
+      for (int i = 0; i < n; ++i) mol[i] = (int)(std::lower_bound(u.begin(), u.end(), key(i)) - u.begin());
       nmol = (int)u.size();
     }
     R.sub0 = sub0;
@@ -454,6 +474,10 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
             in_group[u.a[k] - atom0] = 1;
           }
           u.sub = sub0 + mol[u.a[0] - atom0];
+          // a group's atoms share one temperature (they do when sub-systems follow
+          // molecules and residues); a group split across sub-systems is rejected
+          for (int k = 1; k < ng; ++k)
+            if (mol[u.a[k] - atom0] != mol[u.a[0] - atom0]) { delete c; return JP_E_INVALID; }
           nfr[mol[u.a[0] - atom0]] -= (double)nc;
           ru.push_back(u);
         }
@@ -475,6 +499,31 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     R.unit0 = (int)units.size();
     R.nunit = (int)ru.size();
     units.insert(units.end(), ru.begin(), ru.end());
+    // ALSD lambda: mass (inpcls.f90:350-360), its degree of freedom (md.f90:122-123,
+    // :220-228) and the sub-system whose temperature holds its kinetic term (caltmp/caltmp2)
+    R.lam_mode = ralsd ? prm->alsd : JP_ALSD_NONE;
+    R.lam_ke_sub = -1;
+    if (ralsd) {
+      R.lam_m = prm->lambda_mass;
+      if (!(R.lam_m > 0.0)) {
+        R.lam_m = 0.0;
+        for (int i = 0; i < n; ++i) if (inA[i]) R.lam_m += s.mass[i];
+      }
+      R.lam_im = R.lam_m > 0.0 ? 1.0 / R.lam_m : 0.0;
+      R.lam_tc = prm->lambda_temp_control ? 1 : 0;
+      const bool dof = R.lam_tc && prm->method == JP_METHOD_GE;
+      if (prm->tempco == 1) {
+        R.lam_ke_sub = R.sub0;
+        if (dof) nfr[0] += 1.0;
+      } else if (dof) {
+        int best = 0;
+        for (int q = 1; q < nmol; ++q) if (nfr[q] > nfr[best]) best = q;
+        nfr[best] += 1.0;
+        R.lam_ke_sub = R.sub0 + best;
+      }
+    }
+    hlam.push_back(prm->lambda0);
+    hlam.push_back(0.0);
     for (double f : nfr) hnfr.push_back(f);
     sub0 += nmol;
     auto constrained = [&](int a1, int a2) {
@@ -482,21 +531,29 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     };
     // bonded terms
     std::vector<double> dwork(s.charge, s.charge + n);
+    std::vector<double> dwk((size_t)3 * n, 0.0);   // the same by class (incel.f90:629-654)
+    for (int i = 0; i < n; ++i) dwk[(size_t)pcls(i, i) * n + i] += s.charge[i];
+    const int sct = prm->scale_terms;
     auto mkterm = [&](int kind) {
       Term t;
       std::memset(&t, 0, sizeof(t));
       t.kind = kind;
       t.rep = r;
       t.idiv = 1;
+      t.cls = 2;
       return t;
     };
     auto excess = [&](int a1, int a2) {   // incel.f90:635-654, :665-688
       dwork[a1] += s.charge[a2];
       dwork[a2] += s.charge[a1];
+      const int cl = pcls(a1, a2);
+      dwk[(size_t)cl * n + a1] += s.charge[a2];
+      dwk[(size_t)cl * n + a2] += s.charge[a1];
       Term t = mkterm(T_EXCESS);
       t.a[0] = atom0 + a1;
       t.a[1] = atom0 + a2;
       t.p0 = ccoef * s.charge[a1] * s.charge[a2];
+      t.cls = cl;
       terms_by_kind[T_EXCESS].push_back(t);
     };
     for (int i = 0; i < s.nbond; ++i) {
@@ -508,6 +565,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       t.a[1] = atom0 + a2;
       t.p0 = s.bond_k[i];
       t.p1 = s.bond_r0[i];
+      if (sct & JP_SCALE_BOND) t.cls = pcls(a1, a2);   // incel.f90:705-712
       terms_by_kind[T_BOND].push_back(t);
     }
     for (int i = 0; i < s.nangle; ++i) {
@@ -520,6 +578,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       t.a[2] = atom0 + a3;
       t.p0 = s.angle_k[i];
       t.p1 = s.angle_theta0[i];
+      if (sct & JP_SCALE_ANGLE) t.cls = pcls(a1, a3);  // :735-742
       terms_by_kind[T_ANGLE].push_back(t);
     }
     for (int i = 0; i < s.ntors; ++i) {
@@ -529,6 +588,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       t.p1 = s.tors_nrot[i];
       t.p2 = s.tors_phase[i];
       t.idiv = s.tors_div[i];
+      if (sct & JP_SCALE_TORS) t.cls = pcls(s.tors[4 * i + 1] - b, s.tors[4 * i + 2] - b);   // :838-845
       terms_by_kind[T_TORS].push_back(t);
       if (s.tors_nbf && s.tors_nbf[i] == 1) {
         const int a1 = s.tors[4 * i] - b, a4 = s.tors[4 * i + 3] - b;
@@ -540,6 +600,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
         p.a[2] = t1 * nt1 + t4;   // LJ table index
         p.p0 = std::min(s.s14_vdw[t1], s.s14_vdw[t4]);
         p.p1 = std::min(s.s14_ele[t1], s.s14_ele[t4]) * ccoef * s.charge[a1] * s.charge[a4];
+        p.cls = pcls(a1, a4);   // :758-787
         terms_by_kind[T_P14].push_back(p);
       }
     }
@@ -550,11 +611,21 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       t.p1 = s.impr_nrot[i];
       t.p2 = s.impr_phase[i];
       t.idiv = s.impr_div[i];
+      if ((sct & JP_SCALE_IMPR) && ralsd) {   // n_matrix(min icls, max icls), :911-917
+        int na = 0;
+        for (int k = 0; k < 4; ++k) na += inA[s.impr[4 * i + k] - b];
+        t.cls = na == 4 ? 0 : (na > 0 ? 1 : 2);
+      }
       terms_by_kind[T_IMPR].push_back(t);
     }
     double ds = 0.0;
     for (int i = 0; i < n; ++i) ds += s.charge[i] * dwork[i];
     R.dself = -(1.5 / rc) * ds * 0.5 * ccoef;
+    for (int k = 0; k < 3; ++k) {
+      double d = 0.0;
+      for (int i = 0; i < n; ++i) d += s.charge[i] * dwk[(size_t)k * n + i];
+      R.dself_cls[k] = -(1.5 / rc) * d * 0.5 * ccoef;
+    }
     // GE weight: a fixed slot per replica, per window [low, high, c0..cndeg]
     R.ge_off = r * kGeCap;
     R.hist_off = r * JP_GE_MAX_BINS;
@@ -567,6 +638,8 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       R.ge_celw = s.ge->celw;
       R.ge_ceup = s.ge->ceup;
       R.ge_tempce = s.ge->tempce;
+      R.ge_lower = s.ge->lower;
+      R.ge_upper = s.ge->upper;
       pack_ge(*s.ge, hge.data() + R.ge_off);
     }
     atom0 += n;
@@ -658,6 +731,8 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dput(c, &P.ge_coef, hge);
   e |= dalloc(c, &P.ge_hist, (size_t)nrep * JP_GE_MAX_BINS);
   e |= dalloc(c, &P.mlp, (size_t)nrep * kMlpSlot);
+  e |= dput(c, &P.lam, hlam);
+  e |= dalloc(c, &P.ene_cls, (size_t)nrep * 4);
   e |= dalloc(c, &P.ene_fix, 16 * (size_t)nrep);
   e |= dalloc(c, &P.kin_fix, (size_t)c->nkin * c->nsub);
   e |= dput(c, &P.nfr, hnfr);
@@ -704,6 +779,9 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   ic.qbase = (ic.nsmall + 31) / 32 * 32;
   ic.nvirt = ic.qbase + (8 * ic.nquad + 31) / 32 * 32;
   ic.ge_prescaled = 0;
+  ic.alsd = 0;
+  for (int r = 0; r < nrep; ++r) ic.alsd |= reps[r].lam_mode != 0;
+  c->alsd = ic.alsd != 0;
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   // one wave: every warp resident at once, each with an equal share of the tiles
@@ -854,6 +932,8 @@ int jp_ge_set(jp_ctx *c, int32_t r, const jp_ge *g) {
   R.ge_celw = g->celw;
   R.ge_ceup = g->ceup;
   R.ge_tempce = g->tempce;
+  R.ge_lower = g->lower;
+  R.ge_upper = g->upper;
   CK(cudaMemcpy(c->P.ge_coef + R.ge_off, slot.data(), sizeof(double) * kGeCap, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->P.reps + r, &R, sizeof(Rep), cudaMemcpyHostToDevice));
   return JP_OK;
@@ -877,6 +957,29 @@ int jp_ge_set_mlp(jp_ctx *c, int32_t r, const float *params) {
     c->ic.ge_prescaled = any;
     drop_graphs(c);
   }
+  return JP_OK;
+}
+
+int jp_get_lambda(jp_ctx *c, int32_t r, double *lam2, double *ecls) {
+  if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  if (lam2) CK(cudaMemcpy(lam2, c->P.lam + 2 * r, sizeof(double) * 2, cudaMemcpyDeviceToHost));
+  if (ecls) {
+    long long ef[4] = {0, 0, 0, 0};
+    if (c->alsd) CK(cudaMemcpy(ef, c->P.ene_cls + 4 * (size_t)r, sizeof(ef), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 3; ++k) ecls[k] = (double)ef[k] * kEneInv + c->reps[r].dself_cls[k];
+  }
+  return JP_OK;
+}
+
+int jp_set_lambda(jp_ctx *c, int32_t r, double lambda, double lambda_v) {
+  if (!c || r < 0 || r >= c->nrep || !std::isfinite(lambda) || !std::isfinite(lambda_v))
+    return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  const double v[2] = {lambda, lambda_v};
+  CK(cudaMemcpy(c->P.lam + 2 * r, v, sizeof(v), cudaMemcpyHostToDevice));
   return JP_OK;
 }
 

@@ -19,7 +19,9 @@ struct Img {
 };
 
 template <bool FP64>
-__device__ __forceinline__ void add_grad(const DevPtrs& P, int a, double gx, double gy, double gz) {
+__device__ __forceinline__ void add_grad(const DevPtrs& P, double fs, int a, double gx, double gy,
+                                         double gz) {
+  gx *= fs; gy *= fs; gz *= fs;   // ALSD class weight (1 otherwise)
   if (FP64) {
     atomicAdd(&P.grd[3 * a + 0], gx);
     atomicAdd(&P.grd[3 * a + 1], gy);
@@ -45,15 +47,34 @@ __device__ __forceinline__ void add_energy(const DevPtrs& P, int rep, int slot, 
   }
 }
 
+// warp-aggregated add of a term's energy to its replica's ALSD class total
+__device__ __forceinline__ void add_cls_energy(const DevPtrs& P, int rep, int cls, double e) {
+  const int key = rep * 4 + cls;
+  const unsigned full = 0xffffffffu;
+  const int k0 = __shfl_sync(full, key, 0);
+  if (__all_sync(full, key == k0)) {
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(full, e, o);
+    if ((threadIdx.x & 31) == 0 && e != 0.0) atomic_add_ll(&P.ene_cls[key], to_fix(e, kEneScale));
+  } else if (e != 0.0) {
+    atomic_add_ll(&P.ene_cls[key], to_fix(e, kEneScale));
+  }
+}
+
 template <bool FP64>
-__global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb, double zf) {
+__global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb, double zf,
+                                                int alsd) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double e1 = 0.0, e2 = 0.0;
-  int slot1 = JP_E_BOND, slot2 = -1, rep = 0;
+  int slot1 = JP_E_BOND, slot2 = -1, rep = 0, cls = 2;
   if (t < nterm) {
     const Term T = P.terms[t];
     rep = T.rep;
     const Rep& R = P.reps[rep];
+    double fs = 1.0;
+    if (alsd && R.lam_mode) {
+      cls = T.cls;
+      fs = lam_factor(R.lam_mode, P.lam[2 * rep], cls);
+    }
     Img im;
     for (int k = 0; k < 3; ++k) { im.b[k] = R.box[k]; im.ib[k] = R.invbox[k]; }
     const double* x = P.x;
@@ -67,8 +88,8 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
         double coef = T.p0 * dif;
         e1 = coef * dif;
         coef = 2.0 * coef / r12;
-        add_grad<FP64>(P, T.a[0], coef * d[0], coef * d[1], coef * d[2]);
-        add_grad<FP64>(P, T.a[1], -coef * d[0], -coef * d[1], -coef * d[2]);
+        add_grad<FP64>(P, fs, T.a[0], coef * d[0], coef * d[1], coef * d[2]);
+        add_grad<FP64>(P, fs, T.a[1], -coef * d[0], -coef * d[1], -coef * d[2]);
         slot1 = JP_E_BOND;
         break;
       }
@@ -99,9 +120,9 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
         for (int k = 0; k < 3; ++k) w[k] = coef * (d32[k] * r12r32 - d12[k] * rt);
         rt = cost * r32;
         for (int k = 0; k < 3; ++k) w[3 + k] = coef * (d12[k] * r12r32 - d32[k] * rt);
-        add_grad<FP64>(P, T.a[0], w[0], w[1], w[2]);
-        add_grad<FP64>(P, T.a[1], -(w[0] + w[3]), -(w[1] + w[4]), -(w[2] + w[5]));
-        add_grad<FP64>(P, T.a[2], w[3], w[4], w[5]);
+        add_grad<FP64>(P, fs, T.a[0], w[0], w[1], w[2]);
+        add_grad<FP64>(P, fs, T.a[1], -(w[0] + w[3]), -(w[1] + w[4]), -(w[2] + w[5]));
+        add_grad<FP64>(P, fs, T.a[2], w[3], w[4], w[5]);
         slot1 = JP_E_ANGLE;
         break;
       }
@@ -164,10 +185,10 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
         w[7] = d32[0] * p12[2] - d32[2] * p12[0] - q23 * (d32[0] * p23[2] - d32[2] * p23[0]);
         w[8] = d32[1] * p12[0] - d32[0] * p12[1] - q23 * (d32[1] * p23[0] - d32[0] * p23[1]);
         for (int k = 0; k < 9; ++k) w[k] *= w0;
-        add_grad<FP64>(P, T.a[0], w[0], w[1], w[2]);
-        add_grad<FP64>(P, T.a[1], w[3], w[4], w[5]);
-        add_grad<FP64>(P, T.a[2], -(w[0] + w[3] + w[6]), -(w[1] + w[4] + w[7]), -(w[2] + w[5] + w[8]));
-        add_grad<FP64>(P, T.a[3], w[6], w[7], w[8]);
+        add_grad<FP64>(P, fs, T.a[0], w[0], w[1], w[2]);
+        add_grad<FP64>(P, fs, T.a[1], w[3], w[4], w[5]);
+        add_grad<FP64>(P, fs, T.a[2], -(w[0] + w[3] + w[6]), -(w[1] + w[4] + w[7]), -(w[2] + w[5] + w[8]));
+        add_grad<FP64>(P, fs, T.a[3], w[6], w[7], w[8]);
         break;
       }
       case T_P14: {
@@ -190,8 +211,8 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
         e2 = coef;
         coef *= -r14;
         for (int k = 0; k < 3; ++k) w[k] += coef * d[k];
-        add_grad<FP64>(P, T.a[0], w[0], w[1], w[2]);
-        add_grad<FP64>(P, T.a[1], -w[0], -w[1], -w[2]);
+        add_grad<FP64>(P, fs, T.a[0], w[0], w[1], w[2]);
+        add_grad<FP64>(P, fs, T.a[1], -w[0], -w[1], -w[2]);
         break;
       }
       case T_EXCESS: {
@@ -203,8 +224,8 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
         double cc = T.p0;   // chgmod(a)*chgmod(b)
         e1 = cc * zb * dd2;
         cc *= zf;
-        add_grad<FP64>(P, T.a[0], d[0] * cc, d[1] * cc, d[2] * cc);
-        add_grad<FP64>(P, T.a[1], -d[0] * cc, -d[1] * cc, -d[2] * cc);
+        add_grad<FP64>(P, fs, T.a[0], d[0] * cc, d[1] * cc, d[2] * cc);
+        add_grad<FP64>(P, fs, T.a[1], -d[0] * cc, -d[1] * cc, -d[2] * cc);
         break;
       }
     }
@@ -214,14 +235,16 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
     add_energy(P, rep, slot1, e1);
     const bool has2 = __any_sync(0xffffffffu, slot2 >= 0);
     if (has2) add_energy(P, rep, slot2 >= 0 ? slot2 : JP_E_ELE14, e2);
+    if (alsd) add_cls_energy(P, rep, cls, e1 + e2);
   }
 }
 
-void launch_bonded(const DevPtrs& P, int nterm, bool fp64, double zb, double zf, cudaStream_t st) {
+void launch_bonded(const DevPtrs& P, int nterm, bool fp64, double zb, double zf, bool alsd,
+                   cudaStream_t st) {
   if (nterm <= 0) return;
   const int nb = (nterm + 255) / 256;
-  if (fp64) k_bonded<true><<<nb, 256, 0, st>>>(P, nterm, zb, zf);
-  else k_bonded<false><<<nb, 256, 0, st>>>(P, nterm, zb, zf);
+  if (fp64) k_bonded<true><<<nb, 256, 0, st>>>(P, nterm, zb, zf, alsd ? 1 : 0);
+  else k_bonded<false><<<nb, 256, 0, st>>>(P, nterm, zb, zf, alsd ? 1 : 0);
 }
 
 }  // namespace jp

@@ -53,11 +53,26 @@ struct Rep {
   double dself;
   int ge_off, ge_nwin, ge_ndeg;   // offset into the GE coefficient array
   double ge_alphalw, ge_alphaup, ge_celw, ge_ceup, ge_tempce;
+  double ge_lower, ge_upper;      // ALSD linear walls below celw / above ceup
   int hist_off, hist_n;           // energy histogram slot and bin count (0 = off)
   double hist_min, hist_inv;      // lower edge of bin 0 and 1 / bin width
   int mlp_on;                     // McMD weight from the surrogate network instead of the polynomial
+  // ALSD (cluster classes AA / AB / BB scaled by powers of lambda)
+  int lam_mode;                   // JP_ALSD_*; 0 = off
+  int lam_ke_sub;                 // sub-system whose temperature holds lambda's kinetic term, -1 none
+  int lam_tc;                     // lambda velocity coupled to the thermostat
   int pad_;
+  double lam_m, lam_im;           // lambda mass and its inverse
+  double dself_cls[3];            // ZD self term by class
 };
+
+// class weight of a term (verlethe.f90:116-163): class 0 = AA, 1 = AB, 2 = BB
+__host__ __device__ __forceinline__ double lam_factor(int mode, double lam, int cls) {
+  if (mode == JP_ALSD_NONE || cls == 2) return 1.0;
+  if (cls == 0) return mode == JP_ALSD_LMD ? lam * lam : lam;
+  return mode == JP_ALSD_LMD ? lam : sqrt(lam);
+}
+constexpr int kTypeMask = 0xffff;   // LJ type in the low bits of typ/styp; bit 30 = cluster atom
 
 // integration unit: a SHAKE group (2-4 atoms) or a lone atom (n = 1)
 struct Unit {
@@ -76,7 +91,7 @@ struct Term {
   int a[4];
   double p0, p1, p2;       // bond: k, r0 | angle: k, t0 | tors: k, nrot, phase | 14: svdw, sele
   int idiv;
-  int pad;
+  int cls;                 // ALSD class 0 = AA, 1 = AB, 2 = BB
 };
 
 struct DevPtrs {
@@ -123,6 +138,8 @@ struct DevPtrs {
   double *ge_coef;                // JP_GE_MAX_WINDOWS * (JP_GE_MAX_DEG + 3) per replica
   unsigned long long *ge_hist;    // JP_GE_MAX_BINS per replica
   float *mlp;                     // surrogate network parameters, kMlpSlot per replica
+  double *lam;                    // ALSD lambda and its velocity [nrep][2]
+  long long *ene_cls;             // class energies AA, AB, BB (fixed point) [nrep][4]
   // accumulators
   long long *ene_fix;             // [nrep][16]
   long long *kin_fix;             // [nslots_kin][nsub_total]

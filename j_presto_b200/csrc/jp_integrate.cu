@@ -347,6 +347,7 @@ __device__ __forceinline__ double rep_scale(const DevPtrs& P, const IntConst& c,
 
 __device__ double rep_scale_poly(const DevPtrs& P, const IntConst& c, int r) {
   const Rep& R = P.reps[r];
+  if (R.lam_mode) return 1.0;   // ALSD: the weight acts on lambda, forces go by class
   if (c.method == JP_METHOD_GE && R.ge_nwin > 0) {
     double tot = R.dself;
     for (int k = 1; k < JP_MAXENE; ++k) tot += (double)__ldcg(&P.ene_fix[r * 16 + k]) * kEneInv;
@@ -370,6 +371,75 @@ __device__ double rep_scale_poly(const DevPtrs& P, const IntConst& c, int r) {
   }
   if (c.psetmp > 1.0e-10) return c.temp / c.psetmp;
   return 1.0;
+}
+
+// ---- ALSD lambda (verlethe.f90:240-321, :400-450, :516-530) -----------------------------
+// McMD weight in lambda: the polynomial in lambda itself (window search on lambda, no
+// reduction) plus the linear walls; returns dew
+__device__ double alsd_dew(const DevPtrs& P, const Rep& R, double lam) {
+  const double* cf = P.ge_coef + R.ge_off;   // per window: low, high, c0..cndeg
+  const int stride = R.ge_ndeg + 3;
+  int i = R.ge_nwin - 1;
+  for (int j = 0; j < R.ge_nwin; ++j)
+    if (lam < cf[j * stride + 1]) { i = j; break; }
+  const double rt = lam - cf[i * stride];
+  const double* cc = cf + i * stride + 2;
+  double dprobl = cc[0];
+  for (int j = 1; j <= R.ge_ndeg; ++j) dprobl += cc[j] * pow(rt, (double)j);
+  if (lam < R.ge_celw) dprobl += R.ge_lower * (R.ge_celw - lam);
+  else if (lam > R.ge_ceup) dprobl += R.ge_upper * (lam - R.ge_ceup);
+  return (kGas / kJouCal) * 1.0e-3 * R.ge_tempce * dprobl;
+}
+
+// lambda of one replica through one step, carried by one thread
+struct LamStep {
+  double lam, lv, lvback, lf, lvt;
+};
+
+__device__ __forceinline__ void lam_add_ke(const DevPtrs& P, const IntConst& c, const Rep& R, int kslot,
+                                           double lvt) {
+  if (R.lam_ke_sub >= 0)
+    atomic_add_ll(&P.kin_fix[(size_t)kslot * c.nsub_total + R.lam_ke_sub],
+                  to_fix(R.lam_m * lvt * lvt, kKinScale));
+}
+
+// phase 1: the lambda force from the class energies and lambda's half-step velocity
+__device__ void lam_begin(const DevPtrs& P, const IntConst& c, int r, LamStep& L, bool shk) {
+  const Rep& R = P.reps[r];
+  L.lam = P.lam[2 * r];
+  L.lv = P.lam[2 * r + 1];
+  L.lvback = L.lv;
+  L.lf = 0.0;
+  if (c.method == JP_METHOD_GE) {
+    const double eaa = (double)__ldcg(&P.ene_cls[4 * r]) * kEneInv + R.dself_cls[0];
+    const double eab = (double)__ldcg(&P.ene_cls[4 * r + 1]) * kEneInv + R.dself_cls[1];
+    const double dew = alsd_dew(P, R, L.lam);
+    L.lf = R.lam_mode == JP_ALSD_LMD ? -2.0 * eaa * L.lam - eab - dew
+                                     : -eaa - 0.5 * eab / sqrt(L.lam) - dew;
+  }
+  L.lvt = L.lv;
+  if (R.lam_im != 0.0) L.lvt = L.lv + 0.5 * c.dt * kConvcv * L.lf * R.lam_im;
+  if (shk) lam_add_ke(P, c, R, 0, L.lvt);
+}
+
+// phase 2: thermostat-coupled (or free) velocity update, position, the loop's velocity
+__device__ void lam_advance(const DevPtrs& P, const IntConst& c, int r, LamStep& L, double tt,
+                            bool shk) {
+  const Rep& R = P.reps[r];
+  const double step = c.dt * kConvcv * L.lf * R.lam_im;
+  bool coupled = R.lam_tc && R.lam_im != 0.0;
+  int sub = R.lam_ke_sub;
+  if (c.tempco == 1) sub = R.sub0;
+  else coupled = coupled && sub >= 0;
+  if (coupled) {
+    const double chi = sqrt(tt / (shk ? sub_temp(P, c, 0, sub) : c.temp));
+    L.lv = (2.0 * chi - 1.0) * L.lv + chi * step;
+  } else {
+    L.lv += step;
+  }
+  L.lam += c.dt * L.lv;
+  L.lvt = (L.lvback + L.lv) * 0.5;
+  if (shk) lam_add_ke(P, c, R, 1, L.lvt);
 }
 
 // k_ge_scale: one warp per replica.  McMD replicas with the surrogate network evaluate
@@ -1199,6 +1269,10 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
   const bool shk = c.shake_method != JP_SHAKE_NONE;
   unsigned epoch = 0;
   if (gt < c.nrep) write_ene_hist(P, c, gt);
+  // ALSD: thread r carries lambda of replica r (c.alsd: some replica has clusters)
+  LamStep L{};
+  const bool lam_thread = c.alsd && gt < c.nrep && P.reps[gt].lam_mode != 0;
+  if (lam_thread) lam_begin(P, c, gt, L, shk);
   const int nv = RESIDENT ? nthr : c.nvirt;
   // RESIDENT state of this thread's lane
   UnitScal U;
@@ -1249,6 +1323,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
     }
     if (!grid_barrier(P, epoch)) return;
   }
+  if (lam_thread) lam_advance(P, c, gt, L, tt, shk);
   // phase 2 (verlethe.f90:400-516) + phase 3 of the first SHAKE pass
   for (int base = 0; base < nv; base += nthr) {
     const int v = base + gt;
@@ -1292,6 +1367,12 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
     for (int it = 1; it < c.icslop; ++it) {
       if (!grid_barrier(P, epoch)) return;
       if (!any_active(P, c, it, tt)) break;
+      // lambda's velocity stays (v_back + v)/2 through the loop (verlethe.f90:529)
+      const bool lam_act = lam_thread && cano_active(P, c, P.reps[gt], it, true, tt);
+      if (lam_act) {
+        lam_add_ke(P, c, P.reps[gt], 2 * it, L.lvt);
+        lam_add_ke(P, c, P.reps[gt], 2 * it + 1, L.lvt);
+      }
       // phase 4 (verlethe.f90:625-640)
       for (int base = 0; base < nv; base += nthr) {
         const int v = base + gt;
@@ -1401,6 +1482,10 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
     } else if (quad) {
       q_spill(P, c, Q, S, tid, FP64);
     }
+  }
+  if (lam_thread) {
+    P.lam[2 * gt] = L.lam;
+    P.lam[2 * gt + 1] = L.lv;
   }
   finish_last(P, c, tt);
 }

@@ -27,14 +27,16 @@ struct ZdConst {
 
 // pair kernels (jp_pair.cu)
 void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool minimg, bool count,
-                       cudaStream_t st);
-void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, cudaStream_t st);
+                       bool alsd, cudaStream_t st);
+void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, bool alsd,
+                      cudaStream_t st);
 // co-resident blocks per SM of the (non-counting) pair kernel: the grid is one full wave
 int pair_blocks_per_sm(bool fp64, int nt1);
 void launch_update_pos(const DevPtrs& P, int nslot, bool fp64, double qscale, cudaStream_t st);
 
 // bonded (jp_bonded.cu)
-void launch_bonded(const DevPtrs& P, int nterm, bool fp64, double zb, double zf, cudaStream_t st);
+void launch_bonded(const DevPtrs& P, int nterm, bool fp64, double zb, double zf, bool alsd,
+                   cudaStream_t st);
 
 // integration (jp_integrate.cu)
 struct IntConst {
@@ -57,6 +59,7 @@ struct IntConst {
   // [qbase, nvirt) eight lanes per 4-atom group (quad_idx); qbase and nvirt are multiples of 32
   int nsmall, nquad, qbase, nvirt;
   int ge_prescaled;        // force scales computed by k_ge_scale before the integration kernel
+  int alsd;                // some replica runs ALSD (lambda carried by the integration kernel)
 };
 int cano_grid(bool fp64, int device);   // co-resident blocks of the integration kernels
 // one cooperative launch: energies of the step, force scale, verlet (MICR) or verlethe

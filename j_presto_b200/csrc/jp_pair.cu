@@ -24,6 +24,21 @@ namespace jp {
 
 constexpr int kPairThreads = 256;
 
+// ALSD class energies of a replica: AA and AB accumulated, BB the rest of the pair energy
+__device__ __forceinline__ void flush_cls(const DevPtrs& P, int rep, double eaa, double eab,
+                                          double etot) {
+  for (int o = 16; o > 0; o >>= 1) {
+    eaa += __shfl_xor_sync(0xffffffffu, eaa, o);
+    eab += __shfl_xor_sync(0xffffffffu, eab, o);
+    etot += __shfl_xor_sync(0xffffffffu, etot, o);
+  }
+  if ((threadIdx.x & 31) == 0 && rep >= 0) {
+    atomic_add_ll(&P.ene_cls[rep * 4 + 0], to_fix(eaa, kEneScale));
+    atomic_add_ll(&P.ene_cls[rep * 4 + 1], to_fix(eab, kEneScale));
+    atomic_add_ll(&P.ene_cls[rep * 4 + 2], to_fix(etot - eaa - eab, kEneScale));
+  }
+}
+
 __device__ __forceinline__ void flush_energy(const DevPtrs& P, int rep, double eel, double elj,
                                              long long npair, bool count) {
   for (int o = 16; o > 0; o >>= 1) {
@@ -42,15 +57,18 @@ __device__ __forceinline__ void flush_energy(const DevPtrs& P, int rep, double e
 // One 32x32 tile: lane = i atom; the j atoms are staged in the warp's shared-memory slice
 // and read at (lane + k) & 31 in step k; the j-force accumulators rotate one lane per step
 // (3 shuffles) so that after 32 steps each is back in the lane of its atom.
-template <bool MINIMG, bool COUNT>
+// ALSD: ci = cluster bit of the i atom; a pair with nA cluster atoms has its force times
+// f2 (nA = 2, class AA), f1 (AB) or 1 (BB), and its energy also goes to ea (AA) / eb (AB).
+template <bool MINIMG, bool COUNT, bool ALSD>
 __device__ __forceinline__ void tile_mixed(const float4* __restrict__ sj_pos, const int* __restrict__ sj_typ,
                                            const float2* __restrict__ s_lj, int nt1, float4 pi, int ti,
                                            float4 sh, unsigned m, int lane, float bx, float by, float bz,
                                            float ibx, float iby, float ibz, float rc2, float zb, float zf,
                                            float zc, float& fix, float& fiy, float& fiz, float& gjx,
-                                           float& gjy, float& gjz, float& te, float& tl, int& tn) {
+                                           float& gjy, float& gjz, float& te, float& tl, int& tn,
+                                           int ci, float f1, float f2, float& ea, float& eb) {
   const float xi = pi.x + sh.x, yi = pi.y + sh.y, zi = pi.z + sh.z;
-  const int row = ti * nt1;
+  const int row = (ALSD ? (ti & kTypeMask) : ti) * nt1;
 #pragma unroll 4
   for (int k = 0; k < 32; ++k) {
     const int jl = (lane + k) & 31;
@@ -67,13 +85,26 @@ __device__ __forceinline__ void tile_mixed(const float4* __restrict__ sj_pos, co
         const float rinv = rsqrtf(r2);
         const float r2inv = rinv * rinv;
         const float r6inv = r2inv * r2inv * r2inv;
-        const float2 lj = s_lj[row + sj_typ[jl]];
+        const int tjr = sj_typ[jl];
+        const float2 lj = s_lj[row + (ALSD ? (tjr & kTypeMask) : tjr)];
         const float qq = pi.w * pj.w;
         const float v1 = lj.x * r6inv;
         const float v2 = lj.y * r6inv * r6inv;
-        te = fmaf(qq, rinv + fmaf(zb, r2, -zc), te);
-        tl += v2 - v1;
-        const float fs = fmaf(qq, fmaf(rinv, r2inv, -zf), (12.f * v2 - 6.f * v1) * r2inv);
+        float fs;
+        if (ALSD) {
+          const float e = qq * (rinv + fmaf(zb, r2, -zc)) + (v2 - v1);
+          te = fmaf(qq, rinv + fmaf(zb, r2, -zc), te);
+          tl += v2 - v1;
+          const int na = ci + (tjr >> 30);
+          if (na == 2) ea += e;
+          else if (na == 1) eb += e;
+          fs = (na == 2 ? f2 : na == 1 ? f1 : 1.f) *
+               fmaf(qq, fmaf(rinv, r2inv, -zf), (12.f * v2 - 6.f * v1) * r2inv);
+        } else {
+          te = fmaf(qq, rinv + fmaf(zb, r2, -zc), te);
+          tl += v2 - v1;
+          fs = fmaf(qq, fmaf(rinv, r2inv, -zf), (12.f * v2 - 6.f * v1) * r2inv);
+        }
         const float fx = dx * fs, fy = dy * fs, fz = dz * fs;
         fix -= fx; fiy -= fy; fiz -= fz;
         gjx += fx; gjy += fy; gjz += fz;
@@ -88,7 +119,7 @@ __device__ __forceinline__ void tile_mixed(const float4* __restrict__ sj_pos, co
   }
 }
 
-template <bool COUNT>
+template <bool COUNT, bool ALSD>
 __global__ void __launch_bounds__(kPairThreads)
 k_pair_mixed(DevPtrs P, ZdConst z) {
   extern __shared__ float2 s_lj[];
@@ -111,10 +142,11 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
   int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
   float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
   long long gix = 0, giy = 0, giz = 0;
-  double eel = 0.0, elj = 0.0;
+  double eel = 0.0, elj = 0.0, eaa = 0.0, eab = 0.0;
   long long npair = 0;
   bool mi = true;
   float bx = 0.f, by = 0.f, bz = 0.f, ibx = 0.f, iby = 0.f, ibz = 0.f;
+  float f1 = 1.f, f2 = 1.f;
   for (int t = t0; t < t1; ++t) {
     const int2 ij = P.tiles[t];
     if (ij.x != cur_bi) {
@@ -131,13 +163,21 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
       ai = P.satom[s];
       const int rep = P.blk_rep[cur_bi];
       if (rep != cur_rep) {
-        if (cur_rep >= 0) flush_energy(P, cur_rep, eel, elj, npair, COUNT);
-        eel = elj = 0.0;
+        if (cur_rep >= 0) {
+          if (ALSD) flush_cls(P, cur_rep, eaa, eab, eel + elj);
+          flush_energy(P, cur_rep, eel, elj, npair, COUNT);
+        }
+        eel = elj = eaa = eab = 0.0;
         npair = 0;
         cur_rep = rep;
         const Rep& R = P.reps[rep];
         bx = (float)R.box[0]; by = (float)R.box[1]; bz = (float)R.box[2];
         ibx = (float)R.invbox[0]; iby = (float)R.invbox[1]; ibz = (float)R.invbox[2];
+        if (ALSD) {
+          const double lam = P.lam[2 * rep];
+          f1 = (float)lam_factor(R.lam_mode, lam, 1);
+          f2 = (float)lam_factor(R.lam_mode, lam, 0);
+        }
         // Per-pair minimum image is needed only if a listed pair could reach half a box
         // length: |d| <= rlim + 2*(h_i + h_j) + motion since the build (2 A margin).
         mi = false;
@@ -154,14 +194,17 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     __syncwarp();
     float gjx = 0.f, gjy = 0.f, gjz = 0.f;
     float fix = 0.f, fiy = 0.f, fiz = 0.f;
-    float te = 0.f, tl = 0.f;
+    float te = 0.f, tl = 0.f, ea = 0.f, eb = 0.f;
     int tn = 0;
+    const int ci = ALSD ? (ti >> 30) : 0;
     if (mi)
-      tile_mixed<true, COUNT>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, lane, bx, by, bz, ibx, iby,
-                              ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn);
+      tile_mixed<true, COUNT, ALSD>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, lane, bx, by, bz, ibx,
+                                    iby, ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn,
+                                    ci, f1, f2, ea, eb);
     else
-      tile_mixed<false, COUNT>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, lane, bx, by, bz, ibx, iby,
-                               ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn);
+      tile_mixed<false, COUNT, ALSD>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, lane, bx, by, bz, ibx,
+                                     iby, ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl,
+                                     tn, ci, f1, f2, ea, eb);
     const int aj = P.satom[sj];
     if (aj >= 0 && (gjx != 0.f || gjy != 0.f || gjz != 0.f)) {
       atomic_add_ll(&P.frc[3 * aj + 0], to_fix((double)gjx, kFrcScale));
@@ -173,6 +216,7 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     giz += to_fix((double)fiz, kFrcScale);
     eel += (double)te;
     elj += (double)tl;
+    if (ALSD) { eaa += (double)ea; eab += (double)eb; }
     if (COUNT) npair += tn;
   }
   if (ai >= 0 && (gix | giy | giz)) {
@@ -180,10 +224,11 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     atomic_add_ll(&P.frc[3 * ai + 1], giy);
     atomic_add_ll(&P.frc[3 * ai + 2], giz);
   }
+  if (ALSD) flush_cls(P, cur_rep, eaa, eab, eel + elj);
   flush_energy(P, cur_rep, eel, elj, npair, COUNT);
 }
 
-template <bool COUNT>
+template <bool COUNT, bool ALSD>
 __global__ void __launch_bounds__(kPairThreads)
 k_pair_fp64(DevPtrs P, ZdConst z) {
   extern __shared__ double2 s_ljd[];
@@ -202,9 +247,10 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
   int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
   double4 pi = make_double4(0, 0, 0, 0);
   double gix = 0, giy = 0, giz = 0;
-  double eel = 0.0, elj = 0.0;
+  double eel = 0.0, elj = 0.0, eaa = 0.0, eab = 0.0;
   long long npair = 0;
   double bx = 0, by = 0, bz = 0, ibx = 0, iby = 0, ibz = 0;
+  double f1 = 1.0, f2 = 1.0;
   for (int t = t0; t < t1; ++t) {
     const int2 ij = P.tiles[t];
     if (ij.x != cur_bi) {
@@ -221,20 +267,28 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
       ai = P.satom[s];
       const int rep = P.blk_rep[cur_bi];
       if (rep != cur_rep) {
-        if (cur_rep >= 0) flush_energy(P, cur_rep, eel, elj, npair, COUNT);
-        eel = elj = 0.0;
+        if (cur_rep >= 0) {
+          if (ALSD) flush_cls(P, cur_rep, eaa, eab, eel + elj);
+          flush_energy(P, cur_rep, eel, elj, npair, COUNT);
+        }
+        eel = elj = eaa = eab = 0.0;
         npair = 0;
         cur_rep = rep;
         const Rep& R = P.reps[rep];
         bx = R.box[0]; by = R.box[1]; bz = R.box[2];
         ibx = R.invbox[0]; iby = R.invbox[1]; ibz = R.invbox[2];
+        if (ALSD) {
+          f1 = lam_factor(R.lam_mode, P.lam[2 * rep], 1);
+          f2 = lam_factor(R.lam_mode, P.lam[2 * rep], 0);
+        }
       }
     }
     unsigned m = P.masks[(size_t)t * 32 + lane];
     const int sj = ij.y * kTile + lane;
     double4 pj = P.pos_d[sj];
     int tj = P.styp[sj];
-    const int row = ti * z.nt1;
+    const int row = (ALSD ? (ti & kTypeMask) : ti) * z.nt1;
+    const int ci = ALSD ? (ti >> 30) : 0;
     double gjx = 0, gjy = 0, gjz = 0;
     int tn = 0;
 #pragma unroll 2
@@ -250,12 +304,18 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
           const double ddi = sqrt(dd2i);
           const double dd6i = dd2i * dd2i * dd2i;
           const double ee = pi.w * pj.w;
-          eel += ee * (ddi + z.bcoeff * dd2 - z.zcore);
-          const double2 lj = s_ljd[row + tj];
+          const double epair = ee * (ddi + z.bcoeff * dd2 - z.zcore);
+          eel += epair;
+          const double2 lj = s_ljd[row + (ALSD ? (tj & kTypeMask) : tj)];
           const double v1 = lj.x * dd6i;
           const double v2 = lj.y * dd6i * dd6i;
           elj += -v1 + v2;
-          const double cc = ee * (dd2i * ddi - z.fcoeff) + (-6.0 * v1 + 12.0 * v2) * dd2i;
+          double cc = ee * (dd2i * ddi - z.fcoeff) + (-6.0 * v1 + 12.0 * v2) * dd2i;
+          if (ALSD) {
+            const int na = ci + (tj >> 30);
+            if (na == 2) { eaa += epair + (-v1 + v2); cc *= f2; }
+            else if (na == 1) { eab += epair + (-v1 + v2); cc *= f1; }
+          }
           const double fx = dx * cc, fy = dy * cc, fz = dz * cc;
           gix -= fx; giy -= fy; giz -= fz;
           gjx += fx; gjy += fy; gjz += fz;
@@ -286,35 +346,47 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
     atomicAdd(&P.grd[3 * ai + 1], giy);
     atomicAdd(&P.grd[3 * ai + 2], giz);
   }
+  if (ALSD) flush_cls(P, cur_rep, eaa, eab, eel + elj);
   flush_energy(P, cur_rep, eel, elj, npair, COUNT);
 }
 
 int pair_blocks_per_sm(bool fp64, int nt1) {
   int per = 0;
   if (fp64)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_fp64<false>, kPairThreads,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_fp64<false, false>, kPairThreads,
                                                   sizeof(double2) * nt1 * nt1);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_mixed<false>, kPairThreads,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_mixed<false, false>, kPairThreads,
                                                   sizeof(float2) * nt1 * nt1);
   return per > 0 ? per : 1;
 }
 
-void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool, bool count,
+void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool, bool count, bool alsd,
                        cudaStream_t st) {
   const int wpb = kPairThreads / 32;
   const int nb = (nwarps + wpb - 1) / wpb;
   const size_t sh = sizeof(float2) * z.nt1 * z.nt1;
-  if (count) k_pair_mixed<true><<<nb, kPairThreads, sh, st>>>(P, z);
-  else k_pair_mixed<false><<<nb, kPairThreads, sh, st>>>(P, z);
+  if (alsd) {
+    if (count) k_pair_mixed<true, true><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_mixed<false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+  } else {
+    if (count) k_pair_mixed<true, false><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_mixed<false, false><<<nb, kPairThreads, sh, st>>>(P, z);
+  }
 }
 
-void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, cudaStream_t st) {
+void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, bool alsd,
+                      cudaStream_t st) {
   const int wpb = kPairThreads / 32;
   const int nb = (nwarps + wpb - 1) / wpb;
   const size_t sh = sizeof(double2) * z.nt1 * z.nt1;
-  if (count) k_pair_fp64<true><<<nb, kPairThreads, sh, st>>>(P, z);
-  else k_pair_fp64<false><<<nb, kPairThreads, sh, st>>>(P, z);
+  if (alsd) {
+    if (count) k_pair_fp64<true, true><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_fp64<false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+  } else {
+    if (count) k_pair_fp64<true, false><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_fp64<false, false><<<nb, kPairThreads, sh, st>>>(P, z);
+  }
 }
 
 // slot positions from the master coordinates (after an external coordinate change)

@@ -22,7 +22,8 @@ EXPORTS = ["jp_default_params", "jp_create", "jp_rebuild_cells", "jp_energy_grad
            "jp_last_timing", "jp_launch_counts", "jp_list_stats", "jp_calibrate_fp32",
            "jp_strerror", "jp_destroy", "jp_nonbond_noalloc", "jp_ge_hist_setup",
            "jp_ge_hist_get", "jp_ge_set", "jp_lstsq_windows", "jp_ge_fit", "jp_ge_dlnn",
-           "jp_mlp_nparam", "jp_mlp_init", "jp_mlp_train", "jp_mlp_forward", "jp_ge_set_mlp"]
+           "jp_mlp_nparam", "jp_mlp_init", "jp_mlp_train", "jp_mlp_forward", "jp_ge_set_mlp",
+           "jp_get_lambda", "jp_set_lambda"]
 
 
 class JpError(RuntimeError):
@@ -76,6 +77,8 @@ def lib():
                                    fp_, fp_, fp_]
         L.jp_mlp_forward.argtypes = [ip, ip, fp_, fp_, ip, ip, fp_]
         L.jp_ge_set_mlp.argtypes = [vp, ip, fp_]
+        L.jp_get_lambda.argtypes = [vp, ip, dp, dp]
+        L.jp_set_lambda.argtypes = [vp, ip, C.c_double, C.c_double]
         # all array arguments are device addresses except box (host double[3])
         L.jp_nonbond_noalloc.argtypes = [ip, vp, vp, vp, ip, vp, vp, vp, vp, ip, dp, C.c_double,
                                          C.c_double, vp, vp, vp]
@@ -262,6 +265,16 @@ class Engine:
         keep = []
         g = abi.make_ge(nf, keep)
         _chk(lib().jp_ge_set(self._h, rep, C.byref(g)), "jp_ge_set")
+
+    # ---- ALSD ----
+    def get_lambda(self, rep=0):
+        """(lambda, lambda velocity), class energies (AA, AB, BB) of the last force call."""
+        l2, ec = np.zeros(2), np.zeros(3)
+        _chk(lib().jp_get_lambda(self._h, rep, _dp(l2), _dp(ec)), "jp_get_lambda")
+        return l2, ec
+
+    def set_lambda(self, lam, lam_v=0.0, rep=0):
+        _chk(lib().jp_set_lambda(self._h, rep, float(lam), float(lam_v)), "jp_set_lambda")
 
     def ge_set_mlp(self, params, rep=0):
         p = None if params is None else np.ascontiguousarray(params, np.float32).reshape(-1)

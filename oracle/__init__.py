@@ -49,6 +49,10 @@ def lib():
         L.or_run.argtypes = [vp, C.c_int, dp, dp]
         L.or_mcmd_scale.argtypes = [vp, C.c_double]
         L.or_mcmd_scale.restype = C.c_double
+        L.or_get_lambda.argtypes = [vp, dp, dp]
+        L.or_get_lambda.restype = None
+        L.or_set_lambda.argtypes = [vp, C.c_double, C.c_double]
+        L.or_set_lambda.restype = None
         _lib = L
     return _lib
 
@@ -128,3 +132,12 @@ class Oracle:
 
     def mcmd_scale(self, e):
         return lib().or_mcmd_scale(self._h, float(e))
+
+    def get_lambda(self):
+        """(lambda, lambda velocity), class energies (AA, AB, BB) of the last force call."""
+        l2, ec = np.zeros(2), np.zeros(3)
+        lib().or_get_lambda(self._h, _dp(l2), _dp(ec))
+        return l2, ec
+
+    def set_lambda(self, lam, lam_v=0.0):
+        lib().or_set_lambda(self._h, float(lam), float(lam_v))

@@ -52,19 +52,35 @@ struct Ctx {
   int ntype = 0;
   std::vector<double> c6, c12;
   std::vector<std::vector<int>> excl;  // sorted partner list per atom
-  struct Bond { int i, j; double k, r0; };
-  struct Angle { int i, j, k; double kf, t0; };
-  struct Tors { int a[4]; double k, nrot, phase; int div; };
-  struct P14 { int i, j; double svdw, sele; };
+  // cls: ALSD class of the term, 0 = AA, 1 = AB, 2 = BB (n_matrix, inpcls.f90:297-325);
+  // 2 for every term without clusters
+  struct Bond { int i, j; double k, r0; int cls; };
+  struct Angle { int i, j, k; double kf, t0; int cls; };
+  struct Tors { int a[4]; double k, nrot, phase; int div; int cls; };
+  struct P14 { int i, j; double svdw, sele; int cls; };
   std::vector<Bond> bonds;       // active bonds (SHAKE-constrained removed)
   std::vector<Angle> angles;     // active angles
   std::vector<Tors> tors, imprs;
   std::vector<P14> p14;
-  std::vector<std::array<int, 2>> excess;
+  std::vector<std::array<int, 3>> excess;   // (i, j, cls)
   std::vector<Shake> sk2, sk3, sk4;
   int nconstr = 0;
   // ---- ZD constants (incel.f90:29-39, :655-662) ----
   double rc, rlim, rlim2, irlim2, zcore, fcoeff, bcoeff, ccoef, dself;
+  // ---- ALSD (inpcls.f90, verlethe.f90:110-165, :240-321, :400-450) ----
+  int alsd = 0;
+  std::vector<int> inA;               // 1 = atom of the lambda-scaled cluster
+  double lam = 1.0, lam_v = 0.0, lam_m = 0.0, lam_im = 0.0;
+  bool lam_tc = false, lam_dof = false;
+  int ifg_lambda = -1;                // sub-system carrying lambda's degree of freedom
+  double ecls[3] = {0.0, 0.0, 0.0};   // class energies (unscaled) of the last force call
+  double dself_cls[3] = {0.0, 0.0, 0.0};
+  int pcls(int a, int b) const { return alsd ? 2 - inA[a] - inA[b] : 2; }
+  void factors(double* f) const {     // class weights of the gradient
+    if (alsd == JP_ALSD_LMD) { f[0] = lam * lam; f[1] = lam; f[2] = 1.0; }
+    else if (alsd == JP_ALSD_LMD2) { f[0] = lam; f[1] = std::sqrt(lam); f[2] = 1.0; }
+    else { f[0] = f[1] = f[2] = 1.0; }
+  }
   // ---- run parameters ----
   jp_params prm;
   jp_ge ge{};
@@ -156,6 +172,12 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
   const int n = c.n;
   for (int k = 0; k < JP_MAXENE; ++k) ene[k] = 0.0;
   std::fill(grad, grad + 3 * n, 0.0);
+  // ALSD: term gradients enter times f[class] (verlethe.f90:116-163: grad(:,:,3) =
+  // lambda^2 grad(:,:,1) + lambda grad(:,:,2) + grad(:,:,3)); class energies unscaled
+  double f[3];
+  c.factors(f);
+  double* ec = c.ecls;
+  for (int k = 0; k < 3; ++k) ec[k] = c.dself_cls[k];
 
   // bonds: dnebnd_PB (dnergv.f90:65-122)
   for (const auto& b : c.bonds) {
@@ -165,7 +187,8 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
     double dif = r12 - b.r0;
     double coef = b.k * dif;
     ene[JP_E_BOND] += coef * dif;
-    coef = 2.0 * coef / r12;
+    ec[b.cls] += coef * dif;
+    coef = f[b.cls] * 2.0 * coef / r12;
     for (int k = 0; k < 3; ++k) {
       grad[3 * b.i + k] += coef * d[k];
       grad[3 * b.j + k] -= coef * d[k];
@@ -192,8 +215,9 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
     double dif = theta - a.t0;
     double coef = a.kf * dif;
     ene[JP_E_ANGLE] += coef * dif;
+    ec[a.cls] += coef * dif;
     double sint = std::max(std::sin(theta), kEps);
-    coef = -2.0 * coef / sint;
+    coef = -f[a.cls] * 2.0 * coef / sint;
     double w[6];
     double rt = cost * r12;
     for (int k = 0; k < 3; ++k) w[k] = coef * (d32[k] * r12r32 - d12[k] * rt);
@@ -239,6 +263,7 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
       double phimod = t.nrot * phi + t.phase;
       double div = 1.0 / (double)t.div;
       ene[slot] += t.k * (1.0 + std::cos(phimod)) * div;
+      ec[t.cls] += t.k * (1.0 + std::cos(phimod)) * div;
       double sinp = std::sin(phi);
       int nrot = (int)anint(t.nrot);
       double w0 = 0.0;
@@ -251,7 +276,7 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
         case 6: w0 = cosp * (6.0 + 32.0 * cosp * cosp * (cosp * cosp - 1.0)); break;
         default: w0 = 0.0;
       }
-      w0 = std::cos(t.phase) * t.nrot * t.k * div * w0 * r12r23;
+      w0 = f[t.cls] * std::cos(t.phase) * t.nrot * t.k * div * w0 * r12r23;
       double w1 = d21[0] + d32[0], w2 = d21[1] + d32[1], w3 = d21[2] + d32[2];
       double q12 = s1223 / r12, q23 = s1223 / r23;
       double w[9];
@@ -290,15 +315,17 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
     double co6 = c.c6[ti * c.ntype + tj] * r146;
     double co12 = c.c12[ti * c.ntype + tj] * r1412;
     ene[JP_E_VDW14] += p.svdw * (-co6 + co12);
+    ec[p.cls] += p.svdw * (-co6 + co12);
     double coef = r14 * p.svdw * (-2.0 * co12 + co6) * 6.0;
     double w[3] = {coef * d[0], coef * d[1], coef * d[2]};
     coef = p.sele * r141;
     ene[JP_E_ELE14] += coef;
+    ec[p.cls] += coef;
     coef = coef * (-r14);
     for (int k = 0; k < 3; ++k) {
       w[k] += coef * d[k];
-      grad[3 * p.i + k] += w[k];
-      grad[3 * p.j + k] -= w[k];
+      grad[3 * p.i + k] += f[p.cls] * w[k];
+      grad[3 * p.j + k] -= f[p.cls] * w[k];
     }
   }
 
@@ -307,8 +334,9 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
   const int nt = c.nthreads;
   std::vector<double> tg((size_t)nt * 3 * n, 0.0);
   double eel = 0.0, evdw = 0.0;
+  double ec0 = 0.0, ec1 = 0.0, ec2 = 0.0;
   long long npair = 0;
-#pragma omp parallel num_threads(nt) reduction(+ : eel, evdw, npair)
+#pragma omp parallel num_threads(nt) reduction(+ : eel, evdw, npair, ec0, ec1, ec2)
   {
     double* G = tg.data() + (size_t)omp_get_thread_num() * 3 * n;
 #pragma omp for schedule(dynamic, 64)
@@ -326,12 +354,15 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
         double ddi = std::sqrt(dd2i);
         double dd6i = dd2i * dd2i * dd2i * co;
         double ee = chgi * c.chgmod[j] * co;
-        eel += ee * (ddi + c.bcoeff * dd2 - c.zcore);
+        const double epair = ee * (ddi + c.bcoeff * dd2 - c.zcore);
+        eel += epair;
         int it2 = c.typ[j];
         double v1 = c.c6[it2 * c.ntype + it1] * dd6i;
         double v2 = c.c12[it2 * c.ntype + it1] * dd6i * dd6i;
         evdw += -v1 + v2;
-        double cc = ee * (dd2i * ddi - c.fcoeff) + (-6.0 * v1 + 12.0 * v2) * dd2i;
+        const int pc = c.pcls(i, j);
+        (pc == 0 ? ec0 : pc == 1 ? ec1 : ec2) += epair + (-v1 + v2);
+        double cc = f[pc] * (ee * (dd2i * ddi - c.fcoeff) + (-6.0 * v1 + 12.0 * v2) * dd2i);
         double fx = d[0] * cc, fy = d[1] * cc, fz = d[2] * cc;
         gwx += fx; gwy += fy; gwz += fz;
         G[3 * j] += fx; G[3 * j + 1] += fy; G[3 * j + 2] += fz;
@@ -345,6 +376,7 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
     for (int k = 0; k < 3 * n; ++k) grad[k] += G[k];
   }
   c.npair_last = npair;
+  ec[0] += ec0; ec[1] += ec1; ec[2] += ec2;
   // ZD excess of excluded pairs (enear.f90:518-555) and self term (enear.f90:571)
   double eexc = 0.0;
   for (const auto& e : c.excess) {
@@ -354,7 +386,8 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
     double dd2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
     double cc = c.chgmod[a] * c.chgmod[b];
     eexc += cc * c.bcoeff * dd2;
-    cc *= c.fcoeff;
+    ec[e[2]] += cc * c.bcoeff * dd2;
+    cc *= f[e[2]] * c.fcoeff;
     for (int k = 0; k < 3; ++k) {
       grad[3 * a + k] += d[k] * cc;
       grad[3 * b + k] -= d[k] * cc;
@@ -581,8 +614,10 @@ int shake_all(Ctx& c, double* r1, const double* r2) {
 }
 
 // caltmp (caltmp.f90:2-48): T of the whole system from v
-double caltmp(const Ctx& c, const double* v) {
-  double ek = 0.0;
+// caltmp (caltmp.f90:1-48): ek starts with lambda's kinetic term l_mas*l_vel^2 (zero
+// without ALSD)
+double caltmp(const Ctx& c, const double* v, double lvt = 0.0) {
+  double ek = c.lam_m * lvt * lvt;
   for (int i = 0; i < c.n; ++i)
     ek += c.mass[i] * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
   ek *= 1.0e7;
@@ -590,10 +625,11 @@ double caltmp(const Ctx& c, const double* v) {
 }
 
 // caltmp2 (caltmp.f90:54-110): per sub-system temperatures
-void caltmp2(const Ctx& c, const double* v, double* tf) {
+void caltmp2(const Ctx& c, const double* v, double* tf, double lvt = 0.0) {
   for (int s = 0; s < c.nsub; ++s) tf[s] = 0.0;
   for (int i = 0; i < c.n; ++i)
     tf[c.mol[i]] += c.mass[i] * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+  if (c.lam_tc && c.ifg_lambda >= 0) tf[c.ifg_lambda] += c.lam_m * lvt * lvt;   // caltmp.f90:98-99
   for (int s = 0; s < c.nsub; ++s) tf[s] = tf[s] * 1.0e7 / (c.nfrmol[s] * kGas);
 }
 
@@ -614,6 +650,23 @@ double mcmd_scale(const Ctx& c, double e) {
     dprobl = cf[0];
     for (int j = 1; j <= g.ndeg; ++j) dprobl += cf[j] * std::pow(rt, j);
   }
+  return (kGas / kJouCal) * 1.0e-3 * g.tempce * dprobl;
+}
+
+// ALSD weight d lnP/dlambda (verlethe.f90:240-262): polynomial in lambda itself (window
+// search on lambda, no reduction) plus the linear walls below celw / above ceup; dew
+double alsd_dew(const Ctx& c) {
+  const jp_ge& g = c.ge;
+  const double lam = c.lam;
+  int i = g.nwindow - 1;
+  for (int j = 0; j < g.nwindow; ++j)
+    if (lam < c.ge_high[j]) { i = j; break; }
+  const double rt = lam - c.ge_low[i];
+  const double* cf = &c.ge_coef[(size_t)i * (g.ndeg + 1)];
+  double dprobl = cf[0];
+  for (int j = 1; j <= g.ndeg; ++j) dprobl += cf[j] * std::pow(rt, j);
+  if (lam < g.celw) dprobl += g.lower * (g.celw - lam);
+  else if (lam > g.ceup) dprobl += g.upper * (lam - g.ceup);
   return (kGas / kJouCal) * 1.0e-3 * g.tempce * dprobl;
 }
 
@@ -655,12 +708,23 @@ int step_verlethe(Ctx& c, double* ene) {
     if (idhtlp <= 0 || idloop > idhtlp) return temps;
     return tmpsta + ((temps - tmpsta) * i_idhtlp) * (double)idloop;
   };
+  double lmd_back = c.lam, lmd_vback = c.lam_v, lambda_f = 0.0;
   for (;;) {
     cordm1 = c.cord;
     velback = c.vel;
+    lmd_back = c.lam;
+    lmd_vback = c.lam_v;
   redo:
+    lambda_f = 0.0;
     energy_grad(c, c.cord.data(), ene, c.grad.data());
-    if (c.prm.method == JP_METHOD_CANO) {
+    if (c.alsd) {
+      // forces already combined by class (energy_grad); lambda force (verlethe.f90:289-320)
+      if (c.prm.method == JP_METHOD_GE) {
+        const double dew = alsd_dew(c);
+        if (c.alsd == JP_ALSD_LMD) lambda_f = -2.0 * c.ecls[0] * c.lam - c.ecls[1] - dew;
+        else lambda_f = -c.ecls[0] - 0.5 * c.ecls[1] / std::sqrt(c.lam) - dew;
+      }
+    } else if (c.prm.method == JP_METHOD_CANO) {
       if (c.prm.psetmp > kEps) {
         double dew = temps / c.prm.psetmp;
         for (auto& g : c.grad) g *= dew;
@@ -674,16 +738,23 @@ int step_verlethe(Ctx& c, double* ene) {
     double rt = 0.5 * Tdeltt * kConvcv;
     for (int i = 0; i < n; ++i)
       for (int k = 0; k < 3; ++k) velt[3 * i + k] = c.vel[3 * i + k] - rt * g[3 * i + k] * c.imass[i];
+    double lambda_vt = c.lam_v;
+    if (c.lam_im != 0.0) lambda_vt = c.lam_v + rt * lambda_f * c.lam_im;   // :403-404
     // temperature control (verlethe.f90:400-470)
     const double tt = target_t();
+    const double lstep = Tdeltt * kConvcv * lambda_f * c.lam_im;
     if (whole) {
-      double tempc = shk ? caltmp(c, velt.data()) : temps;
+      double tempc = shk ? caltmp(c, velt.data(), lambda_vt) : temps;
       double chi = std::sqrt(tt / tempc);
       double a = chi * Tdeltt * kConvcv, b = 2.0 * chi - 1.0;
       for (int i = 0; i < n; ++i)
         for (int k = 0; k < 3; ++k) c.vel[3 * i + k] = b * c.vel[3 * i + k] - a * g[3 * i + k] * c.imass[i];
+      if (c.lam_im != 0.0) {   // :439-445
+        if (c.lam_tc) c.lam_v = b * c.lam_v + a * lambda_f * c.lam_im;
+        else c.lam_v = c.lam_v + lstep;
+      }
     } else {
-      if (shk) caltmp2(c, velt.data(), tf.data());
+      if (shk) caltmp2(c, velt.data(), tf.data(), lambda_vt);
       else std::fill(tf.begin(), tf.end(), temps);
       for (int s = 0; s < c.nsub; ++s) chif[s] = std::sqrt(tt / tf[s]);
       for (int i = 0; i < n; ++i) {
@@ -691,8 +762,17 @@ int step_verlethe(Ctx& c, double* ene) {
         double a = chi * Tdeltt * kConvcv, b = 2.0 * chi - 1.0;
         for (int k = 0; k < 3; ++k) c.vel[3 * i + k] = b * c.vel[3 * i + k] - a * g[3 * i + k] * c.imass[i];
       }
+      // :475-481; without a lambda sub-system (CANO) the uncoupled update is taken
+      if (c.lam_tc && c.ifg_lambda >= 0) {
+        const double chi = chif[c.ifg_lambda];
+        c.lam_v = (2.0 * chi - 1.0) * c.lam_v + chi * Tdeltt * kConvcv * lambda_f * c.lam_im;
+      } else {
+        c.lam_v = c.lam_v + lstep;
+      }
     }
     for (int i = 0; i < 3 * n; ++i) c.cord[i] += Tdeltt * c.vel[i];
+    c.lam = c.lam + Tdeltt * c.lam_v;                                        // :516
+    lambda_vt = (lmd_vback + c.lam_v) * 0.5;                                 // :529
     if (shk) {
       std::fill(forcec.begin(), forcec.end(), 0.0);
       bool retry = false;
@@ -702,6 +782,8 @@ int step_verlethe(Ctx& c, double* ene) {
         if (ier != 0) {
           c.cord = cordm1;
           c.vel = velback;
+          c.lam = lmd_back;
+          c.lam_v = lmd_vback;
           if (Tdeltt < 0.01 * deltt) return JP_E_SHAKE_ABORT;
           jshk *= 2; ishk *= 2;
           Tdeltt *= 0.5;
@@ -715,10 +797,10 @@ int step_verlethe(Ctx& c, double* ene) {
         }
         const double tshu = target_t();
         if (whole) {
-          double tempc = caltmp(c, velt.data());
+          double tempc = caltmp(c, velt.data(), lambda_vt);
           if (std::fabs(tempc - tshu) < c.prm.fcstol * tshu) break;
         } else {
-          caltmp2(c, velt.data(), tf.data());
+          caltmp2(c, velt.data(), tf.data(), lambda_vt);
           double mn = *std::min_element(tf.begin(), tf.end()), mx = *std::max_element(tf.begin(), tf.end());
           if (std::max(std::fabs(mn - tshu), std::fabs(mx - tshu)) < c.prm.fcstol * tshu) break;
         }
@@ -731,7 +813,7 @@ int step_verlethe(Ctx& c, double* ene) {
             velt[q] = h * (-kConvcv * g[q] * c.imass[i] + forcec[q]) + velback[q];
           }
         if (whole) {
-          double tempc = caltmp(c, velt.data());
+          double tempc = caltmp(c, velt.data(), lambda_vt);
           double chi = std::sqrt(tt / tempc);
           double a = chi * Tdeltt, b = 2.0 * chi - 1.0;
           for (int i = 0; i < n; ++i)
@@ -740,7 +822,7 @@ int step_verlethe(Ctx& c, double* ene) {
               c.vel[q] = (-kConvcv * g[q] * c.imass[i] + forcec[q]) * a + velback[q] * b;
             }
         } else {
-          caltmp2(c, velt.data(), tf.data());
+          caltmp2(c, velt.data(), tf.data(), lambda_vt);
           for (int s = 0; s < c.nsub; ++s) chif[s] = std::sqrt(tt / tf[s]);
           for (int i = 0; i < n; ++i) {
             double chi = chif[c.mol[i]];
@@ -790,10 +872,16 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
   c->typ.resize(n);
   for (int i = 0; i < n; ++i) c->typ[i] = s->atype[i] - b;
   c->mol.assign(n, 0);
+  c->alsd = (prm->alsd != JP_ALSD_NONE && s->cluster) ? prm->alsd : 0;
+  c->inA.assign(n, 0);
+  if (c->alsd)
+    for (int i = 0; i < n; ++i) c->inA[i] = s->cluster[i] ? 1 : 0;
   if (s->molecule && prm->tempco == 2) {
-    // sub-system ids renumbered densely in order, empty ids removed (md.f90:133-151)
+    // sub-system ids renumbered densely in order, empty ids removed (md.f90:133-151);
+    // with clusters each molecule splits into its cluster and non-cluster part (ixamol2)
     std::vector<int> ids;
-    for (int i = 0; i < n; ++i) ids.push_back(s->molecule[i] - b);
+    for (int i = 0; i < n; ++i)
+      ids.push_back(c->alsd ? 2 * (s->molecule[i] - b) + (c->inA[i] ? 0 : 1) : s->molecule[i] - b);
     std::vector<int> u(ids);
     std::sort(u.begin(), u.end());
     u.erase(std::unique(u.begin(), u.end()), u.end());
@@ -836,17 +924,20 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
   for (int i = 0; i < s->nbond; ++i) {
     int a = s->bond[2 * i] - b, bb = s->bond[2 * i + 1] - b;
     if (constrained(a, bb)) continue;
-    c->bonds.push_back({a, bb, s->bond_k[i], s->bond_r0[i]});
+    const int cl = (prm->scale_terms & JP_SCALE_BOND) ? c->pcls(a, bb) : 2;   // incel.f90:705-712
+    c->bonds.push_back({a, bb, s->bond_k[i], s->bond_r0[i], cl});
   }
   for (int i = 0; i < s->nangle; ++i) {
     int a = s->angle[3 * i] - b, m = s->angle[3 * i + 1] - b, z = s->angle[3 * i + 2] - b;
     if (constrained(a, z)) continue;
-    c->angles.push_back({a, m, z, s->angle_k[i], s->angle_theta0[i]});
+    const int cl = (prm->scale_terms & JP_SCALE_ANGLE) ? c->pcls(a, z) : 2;   // :735-742
+    c->angles.push_back({a, m, z, s->angle_k[i], s->angle_theta0[i], cl});
   }
   for (int i = 0; i < s->ntors; ++i) {
     Ctx::Tors t;
     for (int k = 0; k < 4; ++k) t.a[k] = s->tors[4 * i + k] - b;
     t.k = s->tors_k[i]; t.nrot = s->tors_nrot[i]; t.phase = s->tors_phase[i]; t.div = s->tors_div[i];
+    t.cls = (prm->scale_terms & JP_SCALE_TORS) ? c->pcls(t.a[1], t.a[2]) : 2;   // :838-845
     c->tors.push_back(t);
     // 1-4 pairs (incel.f90:972-987, mknopm inptpl.f90:453-462, incel.f90:1084-1087)
     if (s->tors_nbf[i] == 1) {
@@ -854,13 +945,19 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
       int t1 = c->typ[a1], t4 = c->typ[a4];
       double sv = std::min(s->s14_vdw[t1], s->s14_vdw[t4]);
       double se = std::min(s->s14_ele[t1], s->s14_ele[t4]);
-      c->p14.push_back({a1, a4, sv, se * c->ccoef * c->chg[a1] * c->chg[a4]});
+      c->p14.push_back({a1, a4, sv, se * c->ccoef * c->chg[a1] * c->chg[a4], c->pcls(a1, a4)});
     }
   }
   for (int i = 0; i < s->nimpr; ++i) {
     Ctx::Tors t;
     for (int k = 0; k < 4; ++k) t.a[k] = s->impr[4 * i + k] - b;
     t.k = s->impr_k[i]; t.nrot = s->impr_nrot[i]; t.phase = s->impr_phase[i]; t.div = s->impr_div[i];
+    t.cls = 2;
+    if ((prm->scale_terms & JP_SCALE_IMPR) && c->alsd) {   // n_matrix(min icls, max icls) :911-917
+      int na = 0;
+      for (int k = 0; k < 4; ++k) na += c->inA[t.a[k]];
+      t.cls = na == 4 ? 0 : (na > 0 ? 1 : 2);
+    }
     c->imprs.push_back(t);
   }
   // ZD constants, dself and excess list (incel.f90:29-39, :627-689)
@@ -875,10 +972,15 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
     c->bcoeff = 0.5 * c->fcoeff;
   }
   std::vector<double> dwork(c->chg);   // self term
+  std::vector<double> dwk((size_t)3 * n, 0.0);   // per class (incel.f90:629-654)
+  for (int i = 0; i < n; ++i) dwk[(size_t)c->pcls(i, i) * n + i] += c->chg[i];
   auto addx = [&](int a, int bb) {
     dwork[a] += c->chg[bb];
     dwork[bb] += c->chg[a];
-    c->excess.push_back({a, bb});
+    const int cl = c->pcls(a, bb);
+    dwk[(size_t)cl * n + a] += c->chg[bb];
+    dwk[(size_t)cl * n + bb] += c->chg[a];
+    c->excess.push_back({a, bb, cl});
   };
   for (int i = 0; i < s->nbond; ++i) addx(s->bond[2 * i] - b, s->bond[2 * i + 1] - b);
   for (int i = 0; i < s->nangle; ++i) addx(s->angle[3 * i] - b, s->angle[3 * i + 2] - b);
@@ -887,6 +989,11 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
   double ds = 0.0;
   for (int i = 0; i < n; ++i) ds += c->chg[i] * dwork[i];
   c->dself = -c->zcore * ds * 0.5 * c->ccoef;
+  for (int k = 0; k < 3; ++k) {
+    double d = 0.0;
+    for (int i = 0; i < n; ++i) d += c->chg[i] * dwk[(size_t)k * n + i];
+    c->dself_cls[k] = -c->zcore * d * 0.5 * c->ccoef;
+  }
   // GE weight
   if (s->ge) {
     c->has_ge = true;
@@ -904,6 +1011,26 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
   for (int i = 0; i < n; ++i) c->nfrmol[c->mol[i]] += 3.0;
   for (const auto* v : {&c->sk2, &c->sk3, &c->sk4})
     for (const auto& g : *v) c->nfrmol[c->mol[g.a[0]]] -= (double)(g.n * (g.n - 1) / 2);
+  // lambda: mass (inpcls.f90:350-360) and its degree of freedom (md.f90:122-123, :220-228)
+  if (c->alsd) {
+    c->lam = prm->lambda0;
+    c->lam_v = 0.0;
+    c->lam_m = prm->lambda_mass;
+    if (!(c->lam_m > 0.0)) {
+      c->lam_m = 0.0;
+      for (int i = 0; i < n; ++i) if (c->inA[i]) c->lam_m += c->mass[i];
+    }
+    c->lam_im = c->lam_m > 0.0 ? 1.0 / c->lam_m : 0.0;
+    c->lam_tc = prm->lambda_temp_control != 0;
+    c->lam_dof = c->lam_tc && prm->method == JP_METHOD_GE;
+    if (c->lam_dof) {
+      c->idnfre += 1;
+      int best = 0;
+      for (int s2 = 1; s2 < c->nsub; ++s2) if (c->nfrmol[s2] > c->nfrmol[best]) best = s2;
+      c->ifg_lambda = best;
+      c->nfrmol[best] += 1.0;
+    }
+  }
   // state
   c->cord.assign(s->cord, s->cord + 3 * n);
   c->vel.assign(3 * n, 0.0);
@@ -973,5 +1100,17 @@ int or_run(void* h, int nsteps, double* ene_out, double* temp_out) {
 }
 
 double or_mcmd_scale(void* h, double e) { return mcmd_scale(*(Ctx*)h, e); }
+
+void or_get_lambda(void* h, double* lam2, double* ecls) {
+  Ctx* c = (Ctx*)h;
+  if (lam2) { lam2[0] = c->lam; lam2[1] = c->lam_v; }
+  if (ecls) for (int k = 0; k < 3; ++k) ecls[k] = c->ecls[k];
+}
+
+void or_set_lambda(void* h, double lam, double lam_v) {
+  Ctx* c = (Ctx*)h;
+  c->lam = lam;
+  c->lam_v = lam_v;
+}
 
 }  // extern "C"
