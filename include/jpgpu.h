@@ -58,7 +58,9 @@ enum {
   JP_E_CUDA = -300,               /* CUDA runtime error */
   JP_E_NO_DEVICE = -301,
   JP_E_TIMEOUT = -302,            /* a bounded device wait ran out */
-  JP_E_NOALLOC_LIMIT = -110       /* natom above JP_NOALLOC_MAX_ATOMS (jp_nonbond_noalloc) */
+  JP_E_NOALLOC_LIMIT = -110,      /* natom above JP_NOALLOC_MAX_ATOMS (jp_nonbond_noalloc) */
+  JP_E_STOP_MASS = -121,          /* remotv ier=-1: the stopped atoms have no mass */
+  JP_E_STOP_SINGULAR = -122       /* remotv ier=-2: their inertia tensor is singular */
 };
 
 /* Generalized-ensemble weight (.nf file, md_run inmcmd.f90:22-40; verlethe.f90:196-321). */
@@ -136,7 +138,7 @@ typedef struct jp_system {
 /* Run parameters shared by all replicas of a context (md.inp EXE> MD keywords). */
 typedef struct jp_params {
   int32_t precision;     /* JP_PREC_FP64 or JP_PREC_MIXED */
-  int32_t method;        /* METHOD= (JP_METHOD_MICR / CANO / GE) */
+  int32_t method;        /* METHOD= (JP_METHOD_CONS / MICR / CANO / GE) */
   double dt;             /* TIMEST (fs) */
   double cutoff;         /* CUTLEN (Angstrom), ZD cut-off */
   double dielectric;     /* DIEVAL */
@@ -162,10 +164,22 @@ typedef struct jp_params {
   double lambda_mass;    /* its mass; 0 = total mass of the cluster (inpcls.f90:350-360) */
   int32_t lambda_temp_control;  /* lambda velocity coupled to the thermostat (l_temp_control) */
   int32_t scale_terms;   /* SCALET: JP_SCALE_* bits; non-bonded terms are always scaled */
+  /* METHOD= CONS (verlet.f90:31-34, :172-176, scalet.f90): before each position update the
+   * velocities are scaled by sqrt(1 + dt/taut (T0/T - 1)), at most 2, T the temperature
+   * of v(t-dt/2) over all degrees of freedom. */
+  double taut;           /* TAUTEM relaxation time (fs), > 0 for METHOD= CONS */
+  /* STOPCE (remotv.f90, called by verlet.f90:157-158 and verlethe.f90:490-492, :706-709):
+   * after each velocity update the centre-of-mass translation and/or rotation of the first
+   * stop_natom atoms is removed, positions at time t giving the centre and the inertia
+   * tensor; the degrees of freedom drop by 3 / 6 (md.f90:116-121, :186-216). */
+  int32_t stop_center;   /* JP_STOP_TRANS / ROT / BOTH; JP_STOP_NONE (or 0) = off */
+  int32_t stop_natom;    /* ixcend(nstpcn): atoms 1..stop_natom; 0 = the leading atoms that
+                            share atom 1's molecule id (all atoms without molecule ids) */
 } jp_params;
 
 enum { JP_ALSD_NONE = 0, JP_ALSD_LMD = 1, JP_ALSD_LMD2 = 2 };
 enum { JP_SCALE_BOND = 1, JP_SCALE_ANGLE = 2, JP_SCALE_TORS = 4, JP_SCALE_IMPR = 8 };
+enum { JP_STOP_TRANS = 1, JP_STOP_ROT = 2, JP_STOP_BOTH = 3, JP_STOP_NONE = 4 };   /* STOPCE */
 
 typedef struct jp_ctx jp_ctx;
 
@@ -221,6 +235,11 @@ int jp_pair_count(jp_ctx *ctx, int32_t replica, int64_t *count);
  * phase: [0] pair kernel, [1] bonded, [2] integrate+SHAKE, [3] list rebuild, plus
  * launches[0..3] = number of launches timed per phase (nullable arrays). */
 int jp_set_timing(jp_ctx *ctx, int enable);
+
+/* Caps the integration kernel's grid at `blocks` (0 = the co-resident maximum, the default).
+ * A step whose integration lanes exceed the grid runs the grid-stride form, with the unit
+ * state in the atom arrays between phases, as large systems do.  Test and tuning hook. */
+int jp_set_grid_limit(jp_ctx *ctx, int32_t blocks);
 int jp_last_timing(jp_ctx *ctx, double *total_ms, double *phase_ms4, int32_t *launches4);
 
 /* Kernel launches per jp_step step (excluding list rebuilds) and per list rebuild. */

@@ -174,6 +174,7 @@ void enqueue_bonded(jp_ctx *c) {
 void enqueue_integrate(jp_ctx *c) {
   DevPtrs &P = c->P;
   cudaMemsetAsync(P.kin_fix, 0, sizeof(long long) * c->nkin * c->nsub, c->st);
+  if (c->ic.stop) cudaMemsetAsync(P.com, 0, sizeof(double) * c->ic.ncom * c->ic.nrep * 16, c->st);
   if (c->ic.ge_prescaled) launch_ge_scale(P, c->ic, c->st);
   launch_integrate(P, c->ic, c->nunit, c->fp64, c->cano_grid, c->st);
 }
@@ -217,6 +218,8 @@ int check_status(jp_ctx *c) {
   if (s & ERR_LIST_OVERFLOW) return JP_E_LIST_OVERFLOW;
   if (s & ERR_NONFINITE) return JP_E_NONFINITE;
   if (s & ERR_FIX_OVERFLOW) return JP_E_FIXED_OVERFLOW;
+  if (s & ERR_STOP_MASS) return JP_E_STOP_MASS;
+  if (s & ERR_STOP_SINGULAR) return JP_E_STOP_SINGULAR;
   if (s & ERR_SHAKE_SINGULAR) return JP_E_SHAKE_SINGULAR;
   if (s & ERR_SHAKE_NOCONV) return JP_W_SHAKE_NOT_CONVERGED;
   return JP_E_INVALID;
@@ -225,12 +228,13 @@ int check_status(jp_ctx *c) {
 int validate(const jp_system *sys, int nrep, const jp_params *prm) {
   if (!sys || nrep <= 0 || !prm) return JP_E_INVALID;
   if (prm->cutoff <= 0.0 || prm->dt <= 0.0 || prm->dielectric <= 0.0) return JP_E_INVALID;
-  if (prm->method != JP_METHOD_MICR && prm->method != JP_METHOD_CANO && prm->method != JP_METHOD_GE)
-    return JP_E_INVALID;
+  if (prm->method < JP_METHOD_CONS || prm->method > JP_METHOD_GE) return JP_E_INVALID;
+  if (prm->method == JP_METHOD_CONS && !(prm->taut > 0.0)) return JP_E_INVALID;
+  if (prm->stop_center < 0 || prm->stop_center > JP_STOP_NONE || prm->stop_natom < 0) return JP_E_INVALID;
   if (prm->precision != JP_PREC_FP64 && prm->precision != JP_PREC_MIXED) return JP_E_INVALID;
   if (prm->alsd < JP_ALSD_NONE || prm->alsd > JP_ALSD_LMD2) return JP_E_INVALID;
   if (prm->alsd != JP_ALSD_NONE) {   // verlethe only; lambda^(1/2) needs lambda > 0
-    if (prm->method == JP_METHOD_MICR || !std::isfinite(prm->lambda0)) return JP_E_INVALID;
+    if (prm->method <= JP_METHOD_MICR || !std::isfinite(prm->lambda0)) return JP_E_INVALID;
     if (prm->alsd == JP_ALSD_LMD2 && !(prm->lambda0 > 0.0)) return JP_E_INVALID;
   }
   const double rlim = prm->cutoff + 1.5;
@@ -241,6 +245,7 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
     for (int k = 0; k < 3; ++k)
       if (!(s.box[k] > 2.0 * rlim)) return JP_E_INVALID;   // unique minimum image
     if (s.ntype != sys[0].ntype) return JP_E_INVALID;
+    if (prm->stop_natom > s.natom) return JP_E_INVALID;
     const size_t nt2 = (size_t)s.ntype * s.ntype;
     for (size_t q = 0; q < nt2; ++q)
       if (s.c6[q] != sys[0].c6[q] || s.c12[q] != sys[0].c12[q]) return JP_E_INVALID;
@@ -310,6 +315,9 @@ void jp_default_params(jp_params *p) {
   p->lambda_mass = 0.0;
   p->lambda_temp_control = 0;
   p->scale_terms = 0;
+  p->taut = 40.0;                  // inpmd.f90:125 reaele(11)
+  p->stop_center = JP_STOP_NONE;   // inpmd.f90:124 intele(8)=4
+  p->stop_natom = 0;
 }
 
 const char *jp_strerror(int code) {
@@ -327,6 +335,8 @@ const char *jp_strerror(int code) {
     case JP_E_NO_DEVICE: return "no CUDA device";
     case JP_E_TIMEOUT: return "device wait timed out";
     case JP_E_NOALLOC_LIMIT: return "natom above JP_NOALLOC_MAX_ATOMS, the static scratch size";
+    case JP_E_STOP_MASS: return "centre-of-mass stop: the stopped atoms have no mass";
+    case JP_E_STOP_SINGULAR: return "centre-of-mass stop: inertia tensor of the stopped atoms is singular";
     default: return "unknown error";
   }
 }
@@ -493,6 +503,30 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
         u.sub = sub0 + mol[i];
         ru.push_back(u);
       }
+    // centre-of-mass stop (md.f90:116-121, :186-216): 3 (translation or rotation) or 6 fewer
+    // degrees of freedom, taken from the sub-systems of the first molecule in proportion to
+    // their DOF; the stopped atoms are the first stop_natom (ixcend(nstpcn))
+    R.stop_n = 0;
+    if (prm->stop_center >= JP_STOP_TRANS && prm->stop_center <= JP_STOP_BOTH) {
+      int lead = n;   // leading atoms with atom 1's molecule id
+      if (s.molecule) {
+        lead = 1;
+        while (lead < n && s.molecule[lead] == s.molecule[0]) ++lead;
+      }
+      R.stop_n = prm->stop_natom > 0 ? prm->stop_natom : lead;
+      const double drop = prm->stop_center == JP_STOP_BOTH ? 6.0 : 3.0;
+      int ifrg = 0;
+      for (int i = 0; i < lead; ++i) ifrg = std::max(ifrg, mol[i] + 1);
+      if (ifrg >= 2) {
+        double sum = 0.0;
+        for (int q = 0; q < ifrg; ++q) sum += nfr[q];
+        std::vector<double> ratio(ifrg);
+        for (int q = 0; q < ifrg; ++q) ratio[q] = nfr[q] / sum;
+        for (int q = 0; q < ifrg; ++q) nfr[q] -= drop * ratio[q];
+      } else {
+        nfr[0] -= drop;
+      }
+    }
     std::stable_sort(ru.begin(), ru.end(), [](const Unit &x, const Unit &y) {
       return x.sub != y.sub ? x.sub < y.sub : x.n < y.n;   // warps uniform in sub-system and group size
     });
@@ -733,6 +767,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.mlp, (size_t)nrep * kMlpSlot);
   e |= dput(c, &P.lam, hlam);
   e |= dalloc(c, &P.ene_cls, (size_t)nrep * 4);
+  e |= dalloc(c, &P.com, (size_t)std::max(1, prm->icslop) * nrep * 16);
   e |= dalloc(c, &P.ene_fix, 16 * (size_t)nrep);
   e |= dalloc(c, &P.kin_fix, (size_t)c->nkin * c->nsub);
   e |= dput(c, &P.nfr, hnfr);
@@ -779,6 +814,9 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   ic.qbase = (ic.nsmall + 31) / 32 * 32;
   ic.nvirt = ic.qbase + (8 * ic.nquad + 31) / 32 * 32;
   ic.ge_prescaled = 0;
+  ic.stop = (prm->stop_center >= JP_STOP_TRANS && prm->stop_center <= JP_STOP_BOTH) ? prm->stop_center : 0;
+  ic.ncom = std::max(1, prm->icslop);
+  ic.taut = prm->taut;
   ic.alsd = 0;
   for (int r = 0; r < nrep; ++r) ic.alsd |= reps[r].lam_mode != 0;
   c->alsd = ic.alsd != 0;
@@ -995,6 +1033,15 @@ int jp_pair_count(jp_ctx *c, int32_t r, int64_t *count) {
 int jp_set_timing(jp_ctx *c, int enable) {
   if (!c) return JP_E_INVALID;
   c->tm.enabled = enable != 0;
+  return JP_OK;
+}
+
+int jp_set_grid_limit(jp_ctx *c, int32_t blocks) {
+  if (!c || blocks < 0) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  const int full = cano_grid(c->fp64, c->device);
+  c->cano_grid = blocks > 0 ? std::min((int)blocks, full) : full;
+  drop_graphs(c);
   return JP_OK;
 }
 

@@ -36,7 +36,8 @@ constexpr double kJouCal = 4.184;
 // error bits of the device status word
 enum : unsigned {
   ERR_SHAKE_NOCONV = 1u, ERR_SHAKE_SINGULAR = 2u, ERR_NONFINITE = 4u,
-  ERR_FIX_OVERFLOW = 8u, ERR_LIST_OVERFLOW = 16u, ERR_SORT = 32u, ERR_TIMEOUT = 64u
+  ERR_FIX_OVERFLOW = 8u, ERR_LIST_OVERFLOW = 16u, ERR_SORT = 32u, ERR_TIMEOUT = 64u,
+  ERR_STOP_MASS = 128u, ERR_STOP_SINGULAR = 256u
 };
 
 // per-replica constants
@@ -61,7 +62,7 @@ struct Rep {
   int lam_mode;                   // JP_ALSD_*; 0 = off
   int lam_ke_sub;                 // sub-system whose temperature holds lambda's kinetic term, -1 none
   int lam_tc;                     // lambda velocity coupled to the thermostat
-  int pad_;
+  int stop_n;                     // centre-of-mass stop: atoms [atom0, atom0 + stop_n); 0 = off
   double lam_m, lam_im;           // lambda mass and its inverse
   double dself_cls[3];            // ZD self term by class
 };
@@ -140,6 +141,7 @@ struct DevPtrs {
   float *mlp;                     // surrogate network parameters, kMlpSlot per replica
   double *lam;                    // ALSD lambda and its velocity [nrep][2]
   long long *ene_cls;             // class energies AA, AB, BB (fixed point) [nrep][4]
+  double *com;                    // centre-of-mass stop sums [ncom][nrep][16]
   // accumulators
   long long *ene_fix;             // [nrep][16]
   long long *kin_fix;             // [nslots_kin][nsub_total]

@@ -533,7 +533,7 @@ __device__ void finish_block(const DevPtrs& P, const IntConst& c, double tt) {
   for (int r = threadIdx.x; r < c.nrep; r += blockDim.x) {
     const Rep& R = P.reps[r];
     int ks = c.nkin - 1;   // MICR
-    if (c.method != JP_METHOD_MICR && c.shake_method != JP_SHAKE_NONE) {
+    if (c.method > JP_METHOD_MICR && c.shake_method != JP_SHAKE_NONE) {   // verlethe
       int q = 1;
       for (; q < c.icslop; ++q)
         if (cano_conv(P, c, R, q, tt)) break;
@@ -545,7 +545,7 @@ __device__ void finish_block(const DevPtrs& P, const IntConst& c, double tt) {
       nf += P.nfr[s];
     }
     P.temp_hist[(size_t)h * c.nrep + r] =
-        (c.method == JP_METHOD_MICR || c.shake_method != JP_SHAKE_NONE) ? ek * 1.0e7 / (kGas * nf) : -1.0;
+        (c.method <= JP_METHOD_MICR || c.shake_method != JP_SHAKE_NONE) ? ek * 1.0e7 / (kGas * nf) : -1.0;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -574,6 +574,124 @@ __device__ void finish_last(const DevPtrs& P, const IntConst& c, double tt) {
   }
   __syncthreads();
   if (s_last) finish_block(P, c, tt);
+}
+
+// ---- centre-of-mass stop (remotv.f90:2-131) ----------------------------------------------
+// One reduction per velocity update: over the stopped atoms of a replica, with positions at
+// time t (x0) and the velocity just updated (v), the sums
+//   [0] m, [1-3] m x0, [4-6] m v, [7-9] m x0_k^2, [10] m x0 y0, [11] m y0 z0, [12] m z0 x0,
+//   [13-15] m (x0 cross v).
+// Centre, inertia tensor about the centre (parallel-axis shift) and angular momentum about
+// the centre follow from them, so the correction v -= tv + w x (x0 - centre) needs one grid
+// barrier.  The sums are FP64 atomics (their order, hence the last bits, varies run to run).
+constexpr int kCom = 16;
+
+__device__ __forceinline__ bool stopped(const Rep& R, int a) { return a - R.atom0 < R.stop_n; }
+
+__device__ __forceinline__ void com_terms(double m, const double* x0, const double* v, double* w) {
+  w[0] += m;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    w[1 + k] += m * x0[k];
+    w[4 + k] += m * v[k];
+    w[7 + k] += m * x0[k] * x0[k];
+  }
+  w[10] += m * x0[0] * x0[1];
+  w[11] += m * x0[1] * x0[2];
+  w[12] += m * x0[2] * x0[0];
+  w[13] += m * (x0[1] * v[2] - x0[2] * v[1]);
+  w[14] += m * (x0[2] * v[0] - x0[0] * v[2]);
+  w[15] += m * (x0[0] * v[1] - x0[1] * v[0]);
+}
+
+// adds each lane's sums to slot `slot` of replica `rep` (-1: the lane has none).  Called by
+// all 32 lanes of a warp at one site.
+__device__ void com_add(const DevPtrs& P, const IntConst& c, int slot, int rep, const double* w) {
+  const unsigned full = 0xffffffffu;
+  const unsigned has = __ballot_sync(full, rep >= 0);
+  if (has == 0u) return;
+  const int r0 = __shfl_sync(full, rep, __ffs(has) - 1);
+  double* dst = P.com + (size_t)slot * c.nrep * kCom;
+  if (__all_sync(full, rep < 0 || rep == r0)) {
+#pragma unroll
+    for (int k = 0; k < kCom; ++k) {
+      double v = rep >= 0 ? w[k] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(full, v, o);
+      if ((threadIdx.x & 31) == 0) atomicAdd(&dst[(size_t)r0 * kCom + k], v);
+    }
+  } else if (rep >= 0) {
+    for (int k = 0; k < kCom; ++k) atomicAdd(&dst[(size_t)rep * kCom + k], w[k]);
+  }
+}
+
+struct ComFix {
+  double cen[3], tv[3], w[3];   // centre, translation and angular velocity to remove
+};
+
+// remotv's translational velocity (STOPCE 1, 3) and angular velocity (2, 3) of replica `rep`
+// from the completed sums of slot `slot`.  False (error recorded) without mass or with a
+// singular inertia tensor; the determinant test is relative to the tensor's scale, as the
+// sums are shifted by the parallel-axis theorem.
+__device__ bool com_fix(const DevPtrs& P, const IntConst& c, int slot, int rep, ComFix& F) {
+  const double* s = P.com + ((size_t)slot * c.nrep + rep) * kCom;
+  double q[kCom];
+#pragma unroll
+  for (int k = 0; k < kCom; ++k) q[k] = __ldcg(&s[k]);
+  if (!(q[0] > 0.0)) {
+    atomicOr(P.status, ERR_STOP_MASS);
+    return false;
+  }
+  const double M = q[0], im = 1.0 / M;
+  const bool tr = c.stop == JP_STOP_TRANS || c.stop == JP_STOP_BOTH;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    F.cen[k] = q[1 + k] * im;
+    F.tv[k] = tr ? q[4 + k] * im : 0.0;
+    F.w[k] = 0.0;
+  }
+  if (c.stop == JP_STOP_ROT || c.stop == JP_STOP_BOTH) {
+    const double* r = F.cen;
+    const double cxx = q[7] - M * r[0] * r[0], cyy = q[8] - M * r[1] * r[1], czz = q[9] - M * r[2] * r[2];
+    const double cxy = q[10] - M * r[0] * r[1], cyz = q[11] - M * r[1] * r[2], czx = q[12] - M * r[2] * r[0];
+    const double ixx = cyy + czz, iyy = czz + cxx, izz = cxx + cyy;
+    const double ixy = -cxy, iyz = -cyz, izx = -czx;
+    const double det = ixx * iyy * izz + 2.0 * ixy * iyz * izx - iyz * iyz * ixx - izx * izx * iyy -
+                       ixy * ixy * izz;
+    const double tr3 = (ixx + iyy + izz) * (1.0 / 3.0);
+    if (!(fabs(det) > 1.0e-12 * tr3 * tr3 * tr3)) {
+      atomicOr(P.status, ERR_STOP_SINGULAR);
+      return false;
+    }
+    const double id = 1.0 / det;
+    const double i11 = (iyy * izz - iyz * iyz) * id, i12 = (iyz * izx - izz * ixy) * id;
+    const double i13 = (ixy * iyz - izx * iyy) * id, i22 = (izz * ixx - izx * izx) * id;
+    const double i23 = (izx * ixy - ixx * iyz) * id, i33 = (ixx * iyy - ixy * ixy) * id;
+    // angular momentum about the centre: sum m x0 x v - centre x sum m v
+    const double l0 = q[13] - (r[1] * q[6] - r[2] * q[5]);
+    const double l1 = q[14] - (r[2] * q[4] - r[0] * q[6]);
+    const double l2 = q[15] - (r[0] * q[5] - r[1] * q[4]);
+    F.w[0] = i11 * l0 + i12 * l1 + i13 * l2;
+    F.w[1] = i12 * l0 + i22 * l1 + i23 * l2;
+    F.w[2] = i13 * l0 + i23 * l1 + i33 * l2;
+  }
+  return true;
+}
+
+// velocity to remove from an atom at x0: tv + w x (x0 - centre)
+__device__ __forceinline__ void com_delta(const ComFix& F, const double* x0, double* d) {
+  const double r0 = x0[0] - F.cen[0], r1 = x0[1] - F.cen[1], r2 = x0[2] - F.cen[2];
+  d[0] = F.tv[0] + F.w[1] * r2 - F.w[2] * r1;
+  d[1] = F.tv[1] + F.w[2] * r0 - F.w[0] * r2;
+  d[2] = F.tv[2] + F.w[0] * r1 - F.w[1] * r0;
+}
+
+// does a unit of n atoms a[0..n) (n <= NA) hold a stopped atom?
+template <int NA>
+__device__ __forceinline__ bool unit_stopped(const Rep& R, int n, const int* a) {
+  bool any = false;
+#pragma unroll
+  for (int q = 0; q < NA; ++q) any |= q < n && stopped(R, a[q]);
+  return any;
 }
 
 // ---- METHOD= MICR: verlet.f90 fused with SHAKE, one cooperative launch ------------------
@@ -620,11 +738,148 @@ __device__ __forceinline__ double micr_unit(const DevPtrs& P, const IntConst& c,
   return ke;
 }
 
+// METHOD= CONS and the centre-of-mass stop split the step at grid barriers:
+// (CONS) temperature of v(t-dt/2) | velocity update, its centre-of-mass sums | the
+// correction, Berendsen factor, positions, SHAKE.  v(t-dt/2) waits in vback.
 template <bool FP64>
+__device__ __forceinline__ int micr_vel(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
+                                        double* w) {
+  const Rep& R = P.reps[u.rep];
+  const double rt = -c.dt * kConvcv;
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < kCom; ++k) w[k] = 0.0;
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    double g[3], x0[3], v[3];
+    load_grad<FP64>(P, a, s, g);
+    const double im = P.imass[a];
+    for (int k = 0; k < 3; ++k) {
+      const double vb = P.v[3 * a + k];
+      P.vback[3 * a + k] = vb;
+      v[k] = vb + rt * g[k] * im;
+      P.v[3 * a + k] = v[k];
+      x0[k] = P.x[3 * a + k];
+    }
+    if (c.stop && stopped(R, a)) {
+      com_terms(P.mass[a], x0, v, w);
+      any = true;
+    }
+  }
+  return any ? u.rep : -1;
+}
+
+// Berendsen factor of scalet.f90:30-45 from the temperature of v(t-dt/2) (kinetic slot 0,
+// all degrees of freedom of the replica); 1 when that temperature is not positive
+__device__ double berendsen(const DevPtrs& P, const IntConst& c, const Rep& R) {
+  double ek = 0.0, nf = 0.0;
+  for (int s = R.sub0; s < R.sub0 + R.nsub; ++s) {
+    ek += (double)__ldcg(&P.kin_fix[s]) * kKinInv;
+    nf += P.nfr[s];
+  }
+  const double tempc = ek * 1.0e7 / (kGas * nf);
+  if (!(tempc > 0.0)) return 1.0;
+  const double lam = sqrt(1.0 + (c.dt / c.taut) * (c.temp / tempc - 1.0));
+  return lam >= 2.0 ? 2.0 : lam;
+}
+
+template <bool FP64>
+__device__ __forceinline__ double micr_pos(const DevPtrs& P, const IntConst& c, const Unit& u) {
+  const Rep& R = P.reps[u.rep];
+  ComFix F;
+  const bool fix = c.stop && unit_stopped<4>(R, u.n, u.a) && com_fix(P, c, 0, u.rep, F);
+  const double lam = c.method == JP_METHOD_CONS ? berendsen(P, c, R) : 1.0;
+  double x0[4][3], x1[4][3], vb[4][3], im[4];
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    im[q] = P.imass[a];
+    double d[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < 3; ++k) x0[q][k] = P.x[3 * a + k];
+    if (fix && stopped(R, a)) com_delta(F, x0[q], d);
+    for (int k = 0; k < 3; ++k) {
+      vb[q][k] = P.vback[3 * a + k];
+      const double v = (P.v[3 * a + k] - d[k]) * lam;
+      x1[q][k] = x0[q][k] + c.dt * v;
+      P.v[3 * a + k] = v;
+    }
+  }
+  if (u.n >= 2 && c.shake_method != JP_SHAKE_NONE) {
+    const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
+    if (ier) shake_status(P, ier);
+    const double ri = 1.0 / c.dt;
+    JP_UNIT_LOOP(q)
+      for (int k = 0; k < 3; ++k) P.v[3 * u.a[q] + k] = (x1[q][k] - x0[q][k]) * ri;
+  }
+  bool bad = false;
+  double ke = 0.0;
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    double vv = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      P.x[3 * a + k] = x1[q][k];
+      const double vm = 0.5 * (vb[q][k] + P.v[3 * a + k]);
+      vv += vm * vm;
+      bad |= !isfinite(x1[q][k]);
+    }
+    ke += P.mass[a] * vv;
+    write_slot(P, a, x1[q], FP64);
+  }
+  if (bad) atomicOr(P.status, ERR_NONFINITE);
+  return ke;
+}
+
+// SPLIT: METHOD= CONS or the centre-of-mass stop (a separate instantiation, so that the
+// plain MICR kernel keeps its register allocation)
+template <bool FP64, bool SPLIT>
 __global__ void __launch_bounds__(64) k_micr_fused(DevPtrs P, IntConst c, int nunit) {
   const int nthr = gridDim.x * blockDim.x;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   if (gt < c.nrep) write_ene_hist(P, c, gt);
+  if (SPLIT) {
+    unsigned epoch = 0;
+    if (c.method == JP_METHOD_CONS) {   // verlet.f90:31-34
+      for (int base = 0; base < nunit; base += nthr) {
+        const int t = base + gt;
+        double ke = 0.0;
+        int sub = -1;
+        if (t < nunit) {
+          const Unit u = P.units[t];
+          sub = u.sub;
+          JP_UNIT_LOOP(q) {
+            const int a = u.a[q];
+            const double* v = P.v + 3 * a;
+            ke += P.mass[a] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+          }
+        }
+        add_kin(P, c.nsub_total, 0, sub, ke);
+      }
+      if (!grid_barrier(P, epoch)) return;
+    }
+    for (int base = 0; base < nunit; base += nthr) {   // verlet.f90:144-154
+      const int t = base + gt;
+      double w[kCom];
+      int rep = -1;
+      if (t < nunit) {
+        const Unit u = P.units[t];
+        rep = micr_vel<FP64>(P, c, u, rep_scale(P, c, u.rep), w);
+      }
+      if (c.stop) com_add(P, c, 0, rep, w);
+    }
+    if (c.stop && !grid_barrier(P, epoch)) return;
+    for (int base = 0; base < nunit; base += nthr) {   // verlet.f90:157-215
+      const int t = base + gt;
+      double ke = 0.0;
+      int sub = -1;
+      if (t < nunit) {
+        const Unit u = P.units[t];
+        sub = u.sub;
+        ke = micr_pos<FP64>(P, c, u);
+      }
+      add_kin(P, c.nsub_total, c.nkin - 1, sub, ke);
+    }
+    finish_last(P, c, c.temp);
+    return;
+  }
   for (int base = 0; base < nunit; base += nthr) {
     const int t = base + gt;
     double ke = 0.0;
@@ -1255,11 +1510,130 @@ __device__ __forceinline__ void q_spill(const DevPtrs& P, const IntConst& c, con
   write_slot(P, q.a, xq, fp64);
 }
 
+// Centre-of-mass stop in the CANO/GE kernel (verlethe.f90:490-492, :706-709).  After a
+// velocity update a lane holds x0 (time t) and x = x0 + dt v; its stopped atoms add their sums
+// (v recovered as (x - x0)/dt), and after the grid barrier the correction moves x by
+// -dt (tv + w x (x0 - centre)) (and v without SHAKE), which is the remotv-corrected velocity
+// carried into the position update.
+__device__ __forceinline__ int com_small(const DevPtrs& P, const IntConst& c, const UnitScal& U,
+                                         const UnitSmem& S, int tid, double* w) {
+  const Rep& R = P.reps[U.rep];
+  const double ri = 1.0 / c.dt;
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < kCom; ++k) w[k] = 0.0;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    if (q < U.n && stopped(R, U.a[q])) {
+      double x0[3], v[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        x0[k] = S.x0[3 * q + k][tid];
+        v[k] = (S.x[3 * q + k][tid] - x0[k]) * ri;
+      }
+      com_terms(U.m[q], x0, v, w);
+      any = true;
+    }
+  }
+  return any ? U.rep : -1;
+}
+
+__device__ __forceinline__ void fix_small(const DevPtrs& P, const IntConst& c, int slot, const UnitScal& U,
+                                          UnitSmem& S, int tid, bool shk) {
+  const Rep& R = P.reps[U.rep];
+  ComFix F;
+  if (!unit_stopped<3>(R, U.n, U.a) || !com_fix(P, c, slot, U.rep, F)) return;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    if (q < U.n && stopped(R, U.a[q])) {
+      double x0[3], d[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) x0[k] = S.x0[3 * q + k][tid];
+      com_delta(F, x0, d);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        S.x[3 * q + k][tid] -= c.dt * d[k];
+        if (!shk) S.dxs[3 * q + k][tid] -= d[k];
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int com_quad(const DevPtrs& P, const IntConst& c, const QLane& q,
+                                        const UnitSmem& S, int tid, double* w) {
+#pragma unroll
+  for (int k = 0; k < kCom; ++k) w[k] = 0.0;
+  if (q.a < 0 || !stopped(P.reps[q.rep], q.a)) return -1;
+  const double ri = 1.0 / c.dt;
+  double x0[3], v[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    x0[k] = S.x0[k][tid];
+    v[k] = (S.x[k][tid] - x0[k]) * ri;
+  }
+  com_terms(q.m, x0, v, w);
+  return q.rep;
+}
+
+__device__ __forceinline__ void fix_quad(const DevPtrs& P, const IntConst& c, int slot, const QLane& q,
+                                         UnitSmem& S, int tid) {
+  ComFix F;
+  if (q.a < 0 || !stopped(P.reps[q.rep], q.a) || !com_fix(P, c, slot, q.rep, F)) return;
+  double x0[3], d[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) x0[k] = S.x0[k][tid];
+  com_delta(F, x0, d);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) S.x[k][tid] -= c.dt * d[k];
+}
+
+// streaming form: the unit's x0 and x in the atom arrays
+__device__ __forceinline__ int com_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double* w) {
+  const Rep& R = P.reps[u.rep];
+  const double ri = 1.0 / c.dt;
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < kCom; ++k) w[k] = 0.0;
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    if (stopped(R, a)) {
+      double x0[3], v[3];
+      for (int k = 0; k < 3; ++k) {
+        x0[k] = P.x0[3 * a + k];
+        v[k] = (P.x[3 * a + k] - x0[k]) * ri;
+      }
+      com_terms(P.mass[a], x0, v, w);
+      any = true;
+    }
+  }
+  return any ? u.rep : -1;
+}
+
+__device__ __forceinline__ void fix_unit(const DevPtrs& P, const IntConst& c, int slot, const Unit& u,
+                                         bool shk, bool fp64) {
+  const Rep& R = P.reps[u.rep];
+  ComFix F;
+  if (!unit_stopped<4>(R, u.n, u.a) || !com_fix(P, c, slot, u.rep, F)) return;
+  JP_UNIT_LOOP(q) {
+    const int a = u.a[q];
+    if (stopped(R, a)) {
+      double x0[3], d[3];
+      for (int k = 0; k < 3; ++k) x0[k] = P.x0[3 * a + k];
+      com_delta(F, x0, d);
+      for (int k = 0; k < 3; ++k) {
+        P.x[3 * a + k] -= c.dt * d[k];
+        if (!shk) P.v[3 * a + k] -= d[k];
+      }
+      if (!shk) write_slot(P, a, P.x + 3 * a, fp64);
+    }
+  }
+}
+
 // Whole step for all replicas, one launch.  Virtual lanes: [0, nsmall) one 1-3 atom unit
 // each; [qbase, nvirt) eight lanes per 4-atom group.  RESIDENT: one virtual lane per thread
 // and all unit state on chip for the whole step; else grid-stride over the virtual lanes
 // with the state in the atom arrays between phases.
-template <bool FP64, bool RESIDENT>
+template <bool FP64, bool RESIDENT, bool STOP>
 __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst c, int nunit) {
   __shared__ UnitSmem S;
   const int nthr = gridDim.x * blockDim.x;
@@ -1293,8 +1667,8 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
       s = rep_scale(P, c, Q.rep);
     }
   }
-  // phase 1 (verlethe.f90:380-398)
-  if (shk) {
+  // phase 1 (verlethe.f90:380-398); with the centre-of-mass stop also without SHAKE (x0)
+  if (shk || STOP) {
     for (int base = 0; base < nv; base += nthr) {
       const int v = base + gt;
       if (RESIDENT) {
@@ -1324,43 +1698,95 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
     if (!grid_barrier(P, epoch)) return;
   }
   if (lam_thread) lam_advance(P, c, gt, L, tt, shk);
-  // phase 2 (verlethe.f90:400-516) + phase 3 of the first SHAKE pass
+  // phase 2 (verlethe.f90:400-516) + phase 3 of the first SHAKE pass; the centre-of-mass
+  // stop puts its sums and a grid barrier between the two (com slot 0)
+  constexpr bool split = STOP;   // c.stop != 0
   for (int base = 0; base < nv; base += nthr) {
     const int v = base + gt;
+    double w[kCom];
     if (RESIDENT) {
       if (quad) {
         const double chi = Q.grp ? sqrt(tt / sub_temp(P, c, 0, Q.sub)) : 1.0;
         q_cano2<FP64>(P, c, Q, S, tid, s, chi);
-        add_kin_quad(P, c.nsub_total, 1, Q.sub, q_cano3(P, c, Q, S, tid));
+        if (split) com_add(P, c, 0, com_quad(P, c, Q, S, tid, w), w);
+        else add_kin_quad(P, c.nsub_total, 1, Q.sub, q_cano3(P, c, Q, S, tid));
       } else {
         double ke = 0.0;
         if (small) {
           const double chi = sqrt(tt / (shk ? sub_temp(P, c, 0, U.sub) : c.temp));
           ru_cano2<FP64>(P, c, U, S, tid, s, chi, shk);
-          if (shk) ke = ru_cano3(P, c, U, S, tid);
+          if (shk && !split) ke = ru_cano3(P, c, U, S, tid);
         }
-        if (shk) add_kin(P, c.nsub_total, 1, small ? U.sub : -1, ke);
+        if (split) com_add(P, c, 0, small ? com_small(P, c, U, S, tid, w) : -1, w);
+        else if (shk) add_kin(P, c.nsub_total, 1, small ? U.sub : -1, ke);
       }
     } else if (v >= c.qbase) {
       const QLane q = ql_make(P, c, v);
       q_fetch(P, q, S, tid, false);
       const double chi = q.grp ? sqrt(tt / sub_temp(P, c, 0, q.sub)) : 1.0;
       q_cano2<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep), chi);
-      const double ke = q_cano3(P, c, q, S, tid);
-      q_spill(P, c, q, S, tid, FP64);
-      add_kin_quad(P, c.nsub_total, 1, q.sub, ke);
+      if (split) {
+        const int rep = com_quad(P, c, q, S, tid, w);
+        q_spill(P, c, q, S, tid, FP64);
+        com_add(P, c, 0, rep, w);
+      } else {
+        const double ke = q_cano3(P, c, q, S, tid);
+        q_spill(P, c, q, S, tid, FP64);
+        add_kin_quad(P, c.nsub_total, 1, q.sub, ke);
+      }
     } else {
       double ke = 0.0;
-      int sub = -1;
+      int sub = -1, rep = -1;
       if (v < c.nsmall) {
         const Unit u = P.units[P.small_idx[v]];
         cano2_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), tt);
-        if (shk) {
+        if (split) {
+          rep = com_unit(P, c, u, w);
+        } else if (shk) {
           sub = u.sub;
           ke = cano3_unit<FP64>(P, c, u);
         }
       }
-      if (shk) add_kin(P, c.nsub_total, 1, sub, ke);
+      if (split) com_add(P, c, 0, rep, w);
+      else if (shk) add_kin(P, c.nsub_total, 1, sub, ke);
+    }
+  }
+  if (split) {
+    if (!grid_barrier(P, epoch)) return;
+    for (int base = 0; base < nv; base += nthr) {   // the correction, then phase 3
+      const int v = base + gt;
+      if (RESIDENT) {
+        if (quad) {
+          fix_quad(P, c, 0, Q, S, tid);
+          add_kin_quad(P, c.nsub_total, 1, Q.sub, q_cano3(P, c, Q, S, tid));
+        } else {
+          double ke = 0.0;
+          if (small) {
+            fix_small(P, c, 0, U, S, tid, shk);
+            if (shk) ke = ru_cano3(P, c, U, S, tid);
+          }
+          if (shk) add_kin(P, c.nsub_total, 1, small ? U.sub : -1, ke);
+        }
+      } else if (v >= c.qbase) {
+        const QLane q = ql_make(P, c, v);
+        q_fetch(P, q, S, tid, false);
+        fix_quad(P, c, 0, q, S, tid);
+        const double ke = q_cano3(P, c, q, S, tid);
+        q_spill(P, c, q, S, tid, FP64);
+        add_kin_quad(P, c.nsub_total, 1, q.sub, ke);
+      } else {
+        double ke = 0.0;
+        int sub = -1;
+        if (v < c.nsmall) {
+          const Unit u = P.units[P.small_idx[v]];
+          fix_unit(P, c, 0, u, shk, FP64);
+          if (shk) {
+            sub = u.sub;
+            ke = cano3_unit<FP64>(P, c, u);
+          }
+        }
+        if (shk) add_kin(P, c.nsub_total, 1, sub, ke);
+      }
     }
   }
   if (shk) {
@@ -1407,9 +1833,90 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
         }
       }
       if (!grid_barrier(P, epoch)) return;
-      // phase 5 (verlethe.f90:641-718) + phase 3 of the next SHAKE pass
+      // phase 5 (verlethe.f90:641-718) + phase 3 of the next SHAKE pass; with the
+      // centre-of-mass stop: phase 5 and the sums (com slot it), barrier, correction + phase 3
+      if (split) {
+        for (int base = 0; base < nv; base += nthr) {
+          const int v = base + gt;
+          double w[kCom];
+          int rep = -1;
+          if (RESIDENT) {
+            if (!quad) {
+              if (small && cano_active(P, c, P.reps[U.rep], it, true, tt)) {
+                ru_cano5<FP64>(P, c, U, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, U.sub)));
+                rep = com_small(P, c, U, S, tid, w);
+              }
+            } else if (Q.grp && cano_active(P, c, P.reps[Q.rep], it, true, tt)) {
+              q_cano5<FP64>(P, c, Q, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, Q.sub)));
+              rep = com_quad(P, c, Q, S, tid, w);
+            }
+          } else if (v >= c.qbase) {
+            const QLane q = ql_make(P, c, v);
+            if (q.grp && cano_active(P, c, P.reps[q.rep], it, true, tt)) {
+              q_fetch(P, q, S, tid, false);
+              q_cano5<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep), sqrt(tt / sub_temp(P, c, 2 * it, q.sub)));
+              rep = com_quad(P, c, q, S, tid, w);
+              q_spill(P, c, q, S, tid, FP64);
+            }
+          } else if (v < c.nsmall) {
+            const Unit u = P.units[P.small_idx[v]];
+            if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+              cano5_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
+              rep = com_unit(P, c, u, w);
+            }
+          }
+          com_add(P, c, it, rep, w);
+        }
+        if (!grid_barrier(P, epoch)) return;
+      }
       for (int base = 0; base < nv; base += nthr) {
         const int v = base + gt;
+        if (split) {   // the correction, then phase 3 (phase 5 ran above)
+          if (RESIDENT) {
+            if (!quad) {
+              const bool act = small && cano_active(P, c, P.reps[U.rep], it, true, tt);
+              double ke = 0.0;
+              if (act) {
+                fix_small(P, c, it, U, S, tid, shk);
+                ke = ru_cano3(P, c, U, S, tid);
+              }
+              add_kin(P, c.nsub_total, 2 * it + 1, act ? U.sub : -1, ke);
+            } else {
+              const bool act = Q.grp && cano_active(P, c, P.reps[Q.rep], it, true, tt);
+              double sx[3], sdx[3];
+#pragma unroll
+              for (int k = 0; k < 3; ++k) { sx[k] = S.x[k][tid]; sdx[k] = S.dxs[k][tid]; }
+              if (act) fix_quad(P, c, it, Q, S, tid);
+              const double ke = q_cano3(P, c, Q, S, tid);
+              if (!act && Q.a >= 0) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) { S.x[k][tid] = sx[k]; S.dxs[k][tid] = sdx[k]; }
+              }
+              add_kin_quad(P, c.nsub_total, 2 * it + 1, act ? Q.sub : -1, act ? ke : 0.0);
+            }
+          } else if (v >= c.qbase) {
+            const QLane q = ql_make(P, c, v);
+            const bool act = q.grp && cano_active(P, c, P.reps[q.rep], it, true, tt);
+            q_fetch(P, q, S, tid, false);
+            if (act) fix_quad(P, c, it, q, S, tid);
+            const double ke = q_cano3(P, c, q, S, tid);
+            if (act) q_spill(P, c, q, S, tid, FP64);
+            add_kin_quad(P, c.nsub_total, 2 * it + 1, act ? q.sub : -1, act ? ke : 0.0);
+          } else {
+            double ke = 0.0;
+            int sub = -1;
+            if (v < c.nsmall) {
+              const Unit u = P.units[P.small_idx[v]];
+              if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+                fix_unit(P, c, it, u, shk, FP64);
+                sub = u.sub;
+                ke = cano3_unit<FP64>(P, c, u);
+              }
+            }
+            add_kin(P, c.nsub_total, 2 * it + 1, sub, ke);
+          }
+          continue;
+        }
         if (RESIDENT) {
           if (!quad) {
             const bool act = small && cano_active(P, c, P.reps[U.rep], it, true, tt);
@@ -1526,13 +2033,19 @@ int cano_grid(bool fp64, int device) {
   // the smallest co-resident grid among the integration kernels of this precision
   int g;
   if (fp64) {
-    g = coop_grid(k_cano_fused<true, true>, device);
-    g = std::min(g, coop_grid(k_cano_fused<true, false>, device));
-    g = std::min(g, coop_grid(k_micr_fused<true>, device));
+    g = coop_grid(k_cano_fused<true, true, false>, device);
+    g = std::min(g, coop_grid(k_cano_fused<true, false, false>, device));
+    g = std::min(g, coop_grid(k_cano_fused<true, true, true>, device));
+    g = std::min(g, coop_grid(k_cano_fused<true, false, true>, device));
+    g = std::min(g, coop_grid(k_micr_fused<true, false>, device));
+    g = std::min(g, coop_grid(k_micr_fused<true, true>, device));
   } else {
-    g = coop_grid(k_cano_fused<false, true>, device);
-    g = std::min(g, coop_grid(k_cano_fused<false, false>, device));
-    g = std::min(g, coop_grid(k_micr_fused<false>, device));
+    g = coop_grid(k_cano_fused<false, true, false>, device);
+    g = std::min(g, coop_grid(k_cano_fused<false, false, false>, device));
+    g = std::min(g, coop_grid(k_cano_fused<false, true, true>, device));
+    g = std::min(g, coop_grid(k_cano_fused<false, false, true>, device));
+    g = std::min(g, coop_grid(k_micr_fused<false, false>, device));
+    g = std::min(g, coop_grid(k_micr_fused<false, true>, device));
   }
   return g;
 }
@@ -1555,19 +2068,22 @@ static void coop_launch(void (*kernel)(Args...), int grid, cudaStream_t st, Args
 void launch_integrate(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
                       cudaStream_t st) {
   cudaMemsetAsync(P.bar, 0, sizeof(unsigned) * 4, st);
-  const int lanes = c.method == JP_METHOD_MICR ? nunit : c.nvirt;
+  const bool verlet = c.method <= JP_METHOD_MICR;   // MICR or CONS
+  const int lanes = verlet ? nunit : c.nvirt;
   const int want = std::max(1, (lanes + kIntThreads - 1) / kIntThreads);
   const int grid = std::min(want, grid_max);
   const bool resident = want <= grid_max;
-  if (c.method == JP_METHOD_MICR) {
-    if (fp64) coop_launch(k_micr_fused<true>, grid, st, P, c, nunit);
-    else coop_launch(k_micr_fused<false>, grid, st, P, c, nunit);
+  const bool stop = c.stop != 0;
+  if (verlet) {
+    const bool split = stop || c.method == JP_METHOD_CONS;
+    if (fp64) coop_launch(split ? k_micr_fused<true, true> : k_micr_fused<true, false>, grid, st, P, c, nunit);
+    else coop_launch(split ? k_micr_fused<false, true> : k_micr_fused<false, false>, grid, st, P, c, nunit);
   } else if (resident) {
-    if (fp64) coop_launch(k_cano_fused<true, true>, grid, st, P, c, nunit);
-    else coop_launch(k_cano_fused<false, true>, grid, st, P, c, nunit);
+    if (fp64) coop_launch(stop ? k_cano_fused<true, true, true> : k_cano_fused<true, true, false>, grid, st, P, c, nunit);
+    else coop_launch(stop ? k_cano_fused<false, true, true> : k_cano_fused<false, true, false>, grid, st, P, c, nunit);
   } else {
-    if (fp64) coop_launch(k_cano_fused<true, false>, grid, st, P, c, nunit);
-    else coop_launch(k_cano_fused<false, false>, grid, st, P, c, nunit);
+    if (fp64) coop_launch(stop ? k_cano_fused<true, false, true> : k_cano_fused<true, false, false>, grid, st, P, c, nunit);
+    else coop_launch(stop ? k_cano_fused<false, false, true> : k_cano_fused<false, false, false>, grid, st, P, c, nunit);
   }
 }
 

@@ -60,6 +60,9 @@ struct IntConst {
   int nsmall, nquad, qbase, nvirt;
   int ge_prescaled;        // force scales computed by k_ge_scale before the integration kernel
   int alsd;                // some replica runs ALSD (lambda carried by the integration kernel)
+  int stop;                // STOPCE 1 translation, 2 rotation, 3 both; 0 = off
+  int ncom;                // centre-of-mass sum slots (one per velocity update of a step)
+  double taut;             // METHOD= CONS relaxation time (fs)
 };
 int cano_grid(bool fp64, int device);   // co-resident blocks of the integration kernels
 // one cooperative launch: energies of the step, force scale, verlet (MICR) or verlethe

@@ -23,7 +23,7 @@ EXPORTS = ["jp_default_params", "jp_create", "jp_rebuild_cells", "jp_energy_grad
            "jp_strerror", "jp_destroy", "jp_nonbond_noalloc", "jp_ge_hist_setup",
            "jp_ge_hist_get", "jp_ge_set", "jp_lstsq_windows", "jp_ge_fit", "jp_ge_dlnn",
            "jp_mlp_nparam", "jp_mlp_init", "jp_mlp_train", "jp_mlp_forward", "jp_ge_set_mlp",
-           "jp_get_lambda", "jp_set_lambda"]
+           "jp_get_lambda", "jp_set_lambda", "jp_set_grid_limit"]
 
 
 class JpError(RuntimeError):
@@ -52,6 +52,7 @@ def lib():
         L.jp_set_state.argtypes = [vp, ip, dp, dp]
         L.jp_pair_count.argtypes = [vp, ip, C.POINTER(C.c_int64)]
         L.jp_set_timing.argtypes = [vp, C.c_int]
+        L.jp_set_grid_limit.argtypes = [vp, C.c_int32]
         L.jp_last_timing.argtypes = [vp, dp, dp, C.POINTER(C.c_int32)]
         L.jp_launch_counts.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.jp_list_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
@@ -302,6 +303,11 @@ class Engine:
     # ---- timing ----
     def set_timing(self, on):
         _chk(lib().jp_set_timing(self._h, 1 if on else 0), "jp_set_timing")
+
+    def set_grid_limit(self, blocks):
+        """Cap the integration grid (0 = co-resident maximum); a smaller grid than the
+        system's lanes selects the grid-stride form of the integrator."""
+        _chk(lib().jp_set_grid_limit(self._h, int(blocks)), "jp_set_grid_limit")
 
     def last_timing(self):
         tot = C.c_double()

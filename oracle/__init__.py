@@ -53,6 +53,8 @@ def lib():
         L.or_get_lambda.restype = None
         L.or_set_lambda.argtypes = [vp, C.c_double, C.c_double]
         L.or_set_lambda.restype = None
+        L.or_remotv.argtypes = [vp, dp, dp]
+        L.or_nfrmol.argtypes = [vp, dp]
         _lib = L
     return _lib
 
@@ -141,3 +143,15 @@ class Oracle:
 
     def set_lambda(self, lam, lam_v=0.0):
         lib().or_set_lambda(self._h, float(lam), float(lam_v))
+
+    def remotv(self, xp, vel):
+        """remotv applied to a copy of `vel` with positions `xp`; (ier, new velocities)."""
+        v = np.ascontiguousarray(vel, np.float64).copy()
+        ier = lib().or_remotv(self._h, _dp(np.ascontiguousarray(xp, np.float64)), _dp(v))
+        return ier, v
+
+    def nfrmol(self):
+        n = lib().or_nfrmol(self._h, None)
+        out = np.zeros(n)
+        lib().or_nfrmol(self._h, _dp(out))
+        return out

@@ -88,6 +88,7 @@ struct Ctx {
   bool has_ge = false;
   // ---- DOF (md.f90:116-228) ----
   int idnfre = 0;
+  int stop_n = 0;               // centre-of-mass stop: atoms 0..stop_n-1 (ixcend(nstpcn))
   int nsub = 1;
   std::vector<double> nfrmol;   // per sub-system DOF
   // ---- pair list: half list (j listed under i) of pairs within rlim at build ----
@@ -670,15 +671,95 @@ double alsd_dew(const Ctx& c) {
   return (kGas / kJouCal) * 1.0e-3 * g.tempce * dprobl;
 }
 
-// One verlet step (verlet.f90:2-226), METHOD= MICR (no velocity scaling, no COM stop).
+// remotv (remotv.f90:2-131): remove the centre-of-mass translation (STOPCE 1, 3) and/or
+// rotation (2, 3) of atoms 0..stop_n-1 from c.vel, centre and inertia from positions xp.
+// Direct sums over the atoms, as the reference forms them.  Returns 0, -1 (no mass) or -2
+// (singular inertia tensor).
+int remotv(Ctx& c, const double* xp) {
+  const int na = c.stop_n, idf = c.prm.stop_center;
+  double tot = 0.0;
+  for (int i = 0; i < na; ++i) tot += c.mass[i];
+  if (tot <= 0.0) return -1;
+  tot = 1.0 / tot;
+  double cen[3] = {0, 0, 0}, tv[3] = {0, 0, 0}, av[3] = {0, 0, 0};
+  for (int i = 0; i < na; ++i)
+    for (int k = 0; k < 3; ++k) {
+      cen[k] += c.mass[i] * xp[3 * i + k];
+      if (idf == JP_STOP_TRANS || idf == JP_STOP_BOTH) tv[k] += c.mass[i] * c.vel[3 * i + k];
+    }
+  for (int k = 0; k < 3; ++k) { cen[k] *= tot; tv[k] *= tot; }
+  std::vector<double> d((size_t)3 * na);
+  for (int i = 0; i < na; ++i)
+    for (int k = 0; k < 3; ++k) d[3 * i + k] = xp[3 * i + k] - cen[k];
+  if (idf == JP_STOP_ROT || idf == JP_STOP_BOTH) {
+    double ixx = 0, iyy = 0, izz = 0, ixy = 0, iyz = 0, izx = 0;
+    for (int i = 0; i < na; ++i) {
+      const double m = c.mass[i], dx = d[3 * i], dy = d[3 * i + 1], dz = d[3 * i + 2];
+      ixx += m * (dy * dy + dz * dz);
+      iyy += m * (dz * dz + dx * dx);
+      izz += m * (dx * dx + dy * dy);
+      ixy -= m * dx * dy;
+      iyz -= m * dy * dz;
+      izx -= m * dz * dx;
+    }
+    double det = ixx * iyy * izz + 2.0 * ixy * iyz * izx - iyz * iyz * ixx - izx * izx * iyy - ixy * ixy * izz;
+    if (det == 0.0) return -2;
+    det = 1.0 / det;
+    double inv[3][3];
+    inv[0][0] = (iyy * izz - iyz * iyz) * det;
+    inv[0][1] = inv[1][0] = (iyz * izx - izz * ixy) * det;
+    inv[0][2] = inv[2][0] = (ixy * iyz - izx * iyy) * det;
+    inv[1][1] = (izz * ixx - izx * izx) * det;
+    inv[1][2] = inv[2][1] = (izx * ixy - ixx * iyz) * det;
+    inv[2][2] = (ixx * iyy - ixy * ixy) * det;
+    for (int i = 0; i < na; ++i) {   // angular velocity: inverse tensor times angular momentum
+      const double* v = &c.vel[3 * i];
+      const double dx = d[3 * i], dy = d[3 * i + 1], dz = d[3 * i + 2];
+      const double l[3] = {dy * v[2] - dz * v[1], dz * v[0] - dx * v[2], dx * v[1] - dy * v[0]};
+      for (int k = 0; k < 3; ++k)
+        av[k] += c.mass[i] * (inv[k][0] * l[0] + inv[k][1] * l[1] + inv[k][2] * l[2]);
+    }
+  }
+  for (int i = 0; i < na; ++i) {
+    double* v = &c.vel[3 * i];
+    const double dx = d[3 * i], dy = d[3 * i + 1], dz = d[3 * i + 2];
+    v[0] = v[0] - av[1] * dz + av[2] * dy - tv[0];
+    v[1] = v[1] - av[2] * dx + av[0] * dz - tv[1];
+    v[2] = v[2] - av[0] * dy + av[1] * dx - tv[2];
+  }
+  return 0;
+}
+
+inline bool stop_on(const Ctx& c) {
+  return c.prm.stop_center >= JP_STOP_TRANS && c.prm.stop_center <= JP_STOP_BOTH && c.stop_n > 0;
+}
+
+// error code of the engine for remotv's ier
+inline int remotv_code(int ier) { return ier == -1 ? JP_E_STOP_MASS : JP_E_STOP_SINGULAR; }
+
+// One verlet step (verlet.f90:2-226), METHOD= MICR or CONS: pseudo-temperature force scale,
+// velocity update, centre-of-mass stop, Berendsen scaling (scalet.f90), positions, SHAKE.
 int step_verlet(Ctx& c, double* ene) {
   const int n = c.n;
   std::vector<double> x0(c.cord);
+  const bool cons = c.prm.method == JP_METHOD_CONS;
+  const double tempc = cons ? caltmp(c, c.vel.data()) : 0.0;   // T of v(t-dt/2), verlet.f90:31-34
   energy_grad(c, c.cord.data(), ene, c.grad.data());
+  if (c.prm.psetmp > kEps)   // verlet.f90:118-142
+    for (auto& g : c.grad) g *= c.prm.temp / c.prm.psetmp;
   const double dt = c.prm.dt;
   double rt = -dt * kConvcv;
   for (int i = 0; i < n; ++i)
     for (int k = 0; k < 3; ++k) c.vel[3 * i + k] += rt * c.grad[3 * i + k] / c.mass[i];
+  if (stop_on(c)) {
+    const int ier = remotv(c, x0.data());
+    if (ier) return remotv_code(ier);
+  }
+  if (cons && tempc > 0.0) {   // scalet.f90:30-45
+    double lam = std::sqrt(1.0 + (dt / c.prm.taut) * (c.prm.temp / tempc - 1.0));
+    if (lam >= 2.0) lam = 2.0;
+    for (auto& v : c.vel) v *= lam;
+  }
   for (int i = 0; i < 3 * n; ++i) c.cord[i] += dt * c.vel[i];
   if (c.prm.shake_method != JP_SHAKE_NONE) {
     int ier = shake_all(c, c.cord.data(), x0.data());
@@ -770,6 +851,10 @@ int step_verlethe(Ctx& c, double* ene) {
         c.lam_v = c.lam_v + lstep;
       }
     }
+    if (stop_on(c)) {   // verlethe.f90:490-492, positions at time t
+      const int ier = remotv(c, c.cord.data());
+      if (ier) return remotv_code(ier);
+    }
     for (int i = 0; i < 3 * n; ++i) c.cord[i] += Tdeltt * c.vel[i];
     c.lam = c.lam + Tdeltt * c.lam_v;                                        // :516
     lambda_vt = (lmd_vback + c.lam_v) * 0.5;                                 // :529
@@ -832,6 +917,10 @@ int step_verlethe(Ctx& c, double* ene) {
               c.vel[q] = b * velback[q] + a * (-kConvcv * g[q] * c.imass[i] + forcec[q]);
             }
           }
+        }
+        if (stop_on(c)) {   // verlethe.f90:706-709
+          const int ier = remotv(c, cordm1.data());
+          if (ier) return remotv_code(ier);
         }
         for (int i = 0; i < 3 * n; ++i) c.cord[i] = cordm1[i] + Tdeltt * c.vel[i];
       }
@@ -1003,7 +1092,7 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
     c->ge_low.assign(s->ge->low, s->ge->low + s->ge->nwindow);
     c->ge_high.assign(s->ge->high, s->ge->high + s->ge->nwindow);
   }
-  // DOF (md.f90:116-131, :133-183); no COM stop
+  // DOF (md.f90:116-131, :133-183)
   c->idnfre = 3 * n - c->nconstr;
   c->nsub = 1;
   for (int i = 0; i < n; ++i) c->nsub = std::max(c->nsub, c->mol[i] + 1);
@@ -1011,6 +1100,29 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
   for (int i = 0; i < n; ++i) c->nfrmol[c->mol[i]] += 3.0;
   for (const auto* v : {&c->sk2, &c->sk3, &c->sk4})
     for (const auto& g : *v) c->nfrmol[c->mol[g.a[0]]] -= (double)(g.n * (g.n - 1) / 2);
+  // centre-of-mass stop (md.f90:116-121, :186-216): 3 or 6 fewer, taken from the
+  // sub-systems of the first molecule in proportion to their DOF
+  if (prm->stop_center >= JP_STOP_TRANS && prm->stop_center <= JP_STOP_BOTH) {
+    int iatm = n;   // leading atoms with atom 1's molecule id
+    if (s->molecule) {
+      iatm = 1;
+      while (iatm < n && s->molecule[iatm] == s->molecule[0]) ++iatm;
+    }
+    c->stop_n = prm->stop_natom > 0 ? prm->stop_natom : iatm;
+    const int drop = prm->stop_center == JP_STOP_BOTH ? 6 : 3;
+    c->idnfre -= drop;
+    int ifrg = 0;
+    for (int i = 0; i < iatm; ++i) ifrg = std::max(ifrg, c->mol[i] + 1);
+    if (ifrg >= 2) {
+      double sum = 0.0;
+      for (int q = 0; q < ifrg; ++q) sum += c->nfrmol[q];
+      std::vector<double> ratio(ifrg);
+      for (int q = 0; q < ifrg; ++q) ratio[q] = c->nfrmol[q] / sum;
+      for (int q = 0; q < ifrg; ++q) c->nfrmol[q] -= drop * ratio[q];
+    } else {
+      c->nfrmol[0] -= drop;
+    }
+  }
   // lambda: mass (inpcls.f90:350-360) and its degree of freedom (md.f90:122-123, :220-228)
   if (c->alsd) {
     c->lam = prm->lambda0;
@@ -1089,7 +1201,7 @@ int or_run(void* h, int nsteps, double* ene_out, double* temp_out) {
   for (int s = 0; s < nsteps; ++s) {
     c->idloop += 1;
     int ier;
-    if (c->prm.method == JP_METHOD_MICR) ier = step_verlet(*c, ene);
+    if (c->prm.method <= JP_METHOD_MICR) ier = step_verlet(*c, ene);
     else ier = step_verlethe(*c, ene);
     if (ier != 0) return ier;
     if (ene_out) std::memcpy(ene_out + (size_t)s * JP_MAXENE, ene, sizeof(ene));
@@ -1100,6 +1212,25 @@ int or_run(void* h, int nsteps, double* ene_out, double* temp_out) {
 }
 
 double or_mcmd_scale(void* h, double e) { return mcmd_scale(*(Ctx*)h, e); }
+
+// remotv on a given velocity set (in/out) with positions xp; returns ier (0, -1, -2).
+// Test hook.
+int or_remotv(void* h, const double* xp, double* vel) {
+  Ctx* c = (Ctx*)h;
+  std::vector<double> keep(c->vel);
+  std::memcpy(c->vel.data(), vel, sizeof(double) * 3 * c->n);
+  const int ier = remotv(*c, xp);
+  std::memcpy(vel, c->vel.data(), sizeof(double) * 3 * c->n);
+  c->vel.swap(keep);
+  return ier;
+}
+
+// DOF of each sub-system (nfrmol); returns their number
+int or_nfrmol(void* h, double* out) {
+  Ctx* c = (Ctx*)h;
+  if (out) std::memcpy(out, c->nfrmol.data(), sizeof(double) * c->nsub);
+  return c->nsub;
+}
 
 void or_get_lambda(void* h, double* lam2, double* ecls) {
   Ctx* c = (Ctx*)h;
