@@ -60,7 +60,9 @@ enum {
   JP_E_TIMEOUT = -302,            /* a bounded device wait ran out */
   JP_E_NOALLOC_LIMIT = -110,      /* natom above JP_NOALLOC_MAX_ATOMS (jp_nonbond_noalloc) */
   JP_E_STOP_MASS = -121,          /* remotv ier=-1: the stopped atoms have no mass */
-  JP_E_STOP_SINGULAR = -122       /* remotv ier=-2: their inertia tensor is singular */
+  JP_E_STOP_SINGULAR = -122,      /* remotv ier=-2: their inertia tensor is singular */
+  JP_E_FREE_WINDOW = -130         /* BOUNDA= NO: an atom left the window the context was
+                                     built for (re-create it from the current state) */
 };
 
 /* Generalized-ensemble weight (.nf file, md_run inmcmd.f90:22-40; verlethe.f90:196-321). */
@@ -175,11 +177,20 @@ typedef struct jp_params {
   int32_t stop_center;   /* JP_STOP_TRANS / ROT / BOTH; JP_STOP_NONE (or 0) = off */
   int32_t stop_natom;    /* ixcend(nstpcn): atoms 1..stop_natom; 0 = the leading atoms that
                             share atom 1's molecule id (all atoms without molecule ids) */
+  /* CAL15M (cmmdo.f90:27-74): JP_CAL15M_ZD (zero-dipole, the default) or JP_CAL15M_ATOM
+   * (atom cut-off, enear_ACT_*: E = qi qj / r and the LJ term for r <= CUTLEN, no self or
+   * excess term). */
+  int32_t cal15m;
+  /* BOUNDA (inpmd.f90:72): JP_BOUND_PBC (the box of jp_system) or JP_BOUND_NONE (no
+   * boundary, the *_CB variants: no minimum image; the box of jp_system is ignored). */
+  int32_t bounda;
 } jp_params;
 
 enum { JP_ALSD_NONE = 0, JP_ALSD_LMD = 1, JP_ALSD_LMD2 = 2 };
 enum { JP_SCALE_BOND = 1, JP_SCALE_ANGLE = 2, JP_SCALE_TORS = 4, JP_SCALE_IMPR = 8 };
 enum { JP_STOP_TRANS = 1, JP_STOP_ROT = 2, JP_STOP_BOTH = 3, JP_STOP_NONE = 4 };   /* STOPCE */
+enum { JP_CAL15M_CMM = 1, JP_CAL15M_ATOM = 2, JP_CAL15M_ZD = 4 };                  /* CAL15M */
+enum { JP_BOUND_NONE = 0, JP_BOUND_PBC = 1 };                                       /* BOUNDA */
 
 typedef struct jp_ctx jp_ctx;
 

@@ -8,12 +8,15 @@ import ctypes as C
 import numpy as np
 
 JP_MAXENE = 15
+JP_E_TOTAL, JP_E_VDW15, JP_E_ELE15 = 0, 7, 8   # eneval slots
 JP_PREC_FP64, JP_PREC_MIXED = 0, 1
 JP_METHOD_CONS, JP_METHOD_MICR, JP_METHOD_CANO, JP_METHOD_GE = 1, 2, 3, 4
 JP_SHAKE_NONE, JP_SHAKE_HBON, JP_SHAKE_ALLB = 0, 1, 2
 JP_ALSD_NONE, JP_ALSD_LMD, JP_ALSD_LMD2 = 0, 1, 2
 JP_SCALE_BOND, JP_SCALE_ANGLE, JP_SCALE_TORS, JP_SCALE_IMPR = 1, 2, 4, 8
 JP_STOP_TRANS, JP_STOP_ROT, JP_STOP_BOTH, JP_STOP_NONE = 1, 2, 3, 4
+JP_CAL15M_CMM, JP_CAL15M_ATOM, JP_CAL15M_ZD = 1, 2, 4
+JP_BOUND_NONE, JP_BOUND_PBC = 0, 1
 # return codes (md_run ier convention: >0 warning, <0 fatal)
 JP_OK = 0
 JP_W_SHAKE_NOT_CONVERGED = 1
@@ -27,6 +30,7 @@ JP_E_NO_DEVICE = -301
 JP_E_NOALLOC_LIMIT = -110
 JP_E_STOP_MASS = -121
 JP_E_STOP_SINGULAR = -122
+JP_E_FREE_WINDOW = -130
 JP_NOALLOC_MAX_ATOMS = 16384
 
 # energy slot names (md_run main.f90:157-159 cyenam order)
@@ -85,6 +89,7 @@ class JpParams(C.Structure):
         ("alsd", C.c_int32), ("lambda0", C.c_double), ("lambda_mass", C.c_double),
         ("lambda_temp_control", C.c_int32), ("scale_terms", C.c_int32),
         ("taut", C.c_double), ("stop_center", C.c_int32), ("stop_natom", C.c_int32),
+        ("cal15m", C.c_int32), ("bounda", C.c_int32),
     ]
 
 
@@ -95,7 +100,8 @@ def default_params(**kw):
                  tempco=2, shake_method=JP_SHAKE_HBON, shake_tol=1e-6, shake_maxit=1000,
                  icslop=3, fcstol=1e-3, psetmp=0.0, device=0, alsd=JP_ALSD_NONE, lambda0=1.0,
                  lambda_mass=0.0, lambda_temp_control=0, scale_terms=0, taut=40.0,
-                 stop_center=JP_STOP_NONE, stop_natom=0)
+                 stop_center=JP_STOP_NONE, stop_natom=0, cal15m=JP_CAL15M_ZD,
+                 bounda=JP_BOUND_PBC)
     for k, v in kw.items():
         if not hasattr(p, k):
             raise KeyError(k)

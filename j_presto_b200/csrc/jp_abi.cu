@@ -218,6 +218,7 @@ int check_status(jp_ctx *c) {
   if (s & ERR_LIST_OVERFLOW) return JP_E_LIST_OVERFLOW;
   if (s & ERR_NONFINITE) return JP_E_NONFINITE;
   if (s & ERR_FIX_OVERFLOW) return JP_E_FIXED_OVERFLOW;
+  if (s & ERR_FREE_WINDOW) return JP_E_FREE_WINDOW;
   if (s & ERR_STOP_MASS) return JP_E_STOP_MASS;
   if (s & ERR_STOP_SINGULAR) return JP_E_STOP_SINGULAR;
   if (s & ERR_SHAKE_SINGULAR) return JP_E_SHAKE_SINGULAR;
@@ -231,6 +232,8 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
   if (prm->method < JP_METHOD_CONS || prm->method > JP_METHOD_GE) return JP_E_INVALID;
   if (prm->method == JP_METHOD_CONS && !(prm->taut > 0.0)) return JP_E_INVALID;
   if (prm->stop_center < 0 || prm->stop_center > JP_STOP_NONE || prm->stop_natom < 0) return JP_E_INVALID;
+  if (prm->cal15m != JP_CAL15M_ZD && prm->cal15m != JP_CAL15M_ATOM) return JP_E_INVALID;
+  if (prm->bounda != JP_BOUND_PBC && prm->bounda != JP_BOUND_NONE) return JP_E_INVALID;
   if (prm->precision != JP_PREC_FP64 && prm->precision != JP_PREC_MIXED) return JP_E_INVALID;
   if (prm->alsd < JP_ALSD_NONE || prm->alsd > JP_ALSD_LMD2) return JP_E_INVALID;
   if (prm->alsd != JP_ALSD_NONE) {   // verlethe only; lambda^(1/2) needs lambda > 0
@@ -242,8 +245,9 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
     const jp_system &s = sys[r];
     if (s.natom <= 0 || !s.cord || !s.mass || !s.charge || !s.atype || !s.c6 || !s.c12 || !s.excl_ptr)
       return JP_E_INVALID;
-    for (int k = 0; k < 3; ++k)
-      if (!(s.box[k] > 2.0 * rlim)) return JP_E_INVALID;   // unique minimum image
+    if (prm->bounda == JP_BOUND_PBC)
+      for (int k = 0; k < 3; ++k)
+        if (!(s.box[k] > 2.0 * rlim)) return JP_E_INVALID;   // unique minimum image
     if (s.ntype != sys[0].ntype) return JP_E_INVALID;
     if (prm->stop_natom > s.natom) return JP_E_INVALID;
     const size_t nt2 = (size_t)s.ntype * s.ntype;
@@ -318,6 +322,8 @@ void jp_default_params(jp_params *p) {
   p->taut = 40.0;                  // inpmd.f90:125 reaele(11)
   p->stop_center = JP_STOP_NONE;   // inpmd.f90:124 intele(8)=4
   p->stop_natom = 0;
+  p->cal15m = JP_CAL15M_ZD;
+  p->bounda = JP_BOUND_PBC;
 }
 
 const char *jp_strerror(int code) {
@@ -335,6 +341,7 @@ const char *jp_strerror(int code) {
     case JP_E_NO_DEVICE: return "no CUDA device";
     case JP_E_TIMEOUT: return "device wait timed out";
     case JP_E_NOALLOC_LIMIT: return "natom above JP_NOALLOC_MAX_ATOMS, the static scratch size";
+    case JP_E_FREE_WINDOW: return "BOUNDA= NO: an atom left the window of the context (re-create it)";
     case JP_E_STOP_MASS: return "centre-of-mass stop: the stopped atoms have no mass";
     case JP_E_STOP_SINGULAR: return "centre-of-mass stop: inertia tensor of the stopped atoms is singular";
     default: return "unknown error";
@@ -389,20 +396,43 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     R.atom0 = atom0;
     R.natom = n;
     R.blk0 = blk0;
+    // BOUNDA= NO: a periodic box in which no two atoms of the replica can be half a box
+    // apart, so that minimum image is the identity and the periodic cell list, tiles and
+    // kernels give exactly the free-boundary pair set (the *_CB variants).  The atoms must
+    // stay in a window around their initial bounding box (checked at each list rebuild).
+    double box[3], vol = 1.0;
+    R.free_bnd = prm->bounda == JP_BOUND_NONE ? 1 : 0;
+    for (int k = 0; k < 3; ++k) {
+      box[k] = s.box[k];
+      if (R.free_bnd) {
+        double lo = s.cord[k], hi = s.cord[k];
+        for (int i = 1; i < n; ++i) {
+          lo = std::min(lo, s.cord[3 * i + k]);
+          hi = std::max(hi, s.cord[3 * i + k]);
+        }
+        const double half = 0.5 * (hi - lo) + 10.0 + 0.1 * (hi - lo);
+        R.win_lo[k] = 0.5 * (lo + hi) - half;
+        R.win_hi[k] = 0.5 * (lo + hi) + half;
+        box[k] = std::max(4.0 * half + 2.0, 2.0 * rlim + 2.0);   // separations < 2 half < box / 2
+        vol *= std::max(hi - lo, 10.0);
+      } else {
+        vol *= box[k];
+      }
+    }
     // xy columns of edge ~(32/density)^(1/3) so that 32 z-sorted atoms fill a near-cubic
     // block; 0.25 A z bins inside a column
-    const double dens = n / (s.box[0] * s.box[1] * s.box[2]);
+    const double dens = n / vol;
     const double edge = std::cbrt((double)kTile / dens);
     for (int k = 0; k < 3; ++k) {
-      R.box[k] = s.box[k];
-      R.invbox[k] = 1.0 / s.box[k];
+      R.box[k] = box[k];
+      R.invbox[k] = 1.0 / box[k];
     }
     for (int k = 0; k < 2; ++k) {
-      R.grid[k] = std::max(1, std::min(512, (int)std::lround(s.box[k] / edge)));
-      R.cell[k] = s.box[k] / R.grid[k];
+      R.grid[k] = std::max(1, std::min(512, (int)std::lround(box[k] / edge)));
+      R.cell[k] = box[k] / R.grid[k];
     }
-    R.grid[2] = std::max(1, (int)std::ceil(s.box[2] / 0.25));
-    R.cell[2] = s.box[2] / R.grid[2];
+    R.grid[2] = std::max(1, (int)std::ceil(box[2] / 0.25));
+    R.cell[2] = box[2] / R.grid[2];
     R.col0 = col0;
     R.ncol = R.grid[0] * R.grid[1];
     col0 += R.ncol;
@@ -577,7 +607,9 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       t.cls = 2;
       return t;
     };
+    const bool zd = prm->cal15m == JP_CAL15M_ZD;   // ATOM: no self or excess term
     auto excess = [&](int a1, int a2) {   // incel.f90:635-654, :665-688
+      if (!zd) return;
       dwork[a1] += s.charge[a2];
       dwork[a2] += s.charge[a1];
       const int cl = pcls(a1, a2);
@@ -654,11 +686,11 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     }
     double ds = 0.0;
     for (int i = 0; i < n; ++i) ds += s.charge[i] * dwork[i];
-    R.dself = -(1.5 / rc) * ds * 0.5 * ccoef;
+    R.dself = zd ? -(1.5 / rc) * ds * 0.5 * ccoef : 0.0;
     for (int k = 0; k < 3; ++k) {
       double d = 0.0;
       for (int i = 0; i < n; ++i) d += s.charge[i] * dwk[(size_t)k * n + i];
-      R.dself_cls[k] = -(1.5 / rc) * d * 0.5 * ccoef;
+      R.dself_cls[k] = zd ? -(1.5 / rc) * d * 0.5 * ccoef : 0.0;
     }
     // GE weight: a fixed slot per replica, per window [low, high, c0..cndeg]
     R.ge_off = r * kGeCap;
@@ -786,9 +818,12 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   if (e) { jp_destroy(c); return JP_E_CUDA; }
   // the tile-row prefix must cover the sentinel entry; row_cnt[nblk] stays 0
   // ---- constants ---------------------------------------------------------------------------
+  // ZD constants (incel.f90:655-658); the atom cut-off is the same pair formula with all
+  // three zero: E = qi qj / r, F = qi qj / r^3 d (enear.f90 #ACT lines)
+  const bool zd = prm->cal15m == JP_CAL15M_ZD;
   c->zc.rc2 = rc * rc;
-  c->zc.zcore = 1.5 / rc;
-  c->zc.fcoeff = 1.0 / (rc * rc * rc);
+  c->zc.zcore = zd ? 1.5 / rc : 0.0;
+  c->zc.fcoeff = zd ? 1.0 / (rc * rc * rc) : 0.0;
   c->zc.bcoeff = 0.5 * c->zc.fcoeff;
   c->zc.rlim = rc + 1.5;
   c->zc.nt1 = nt1;

@@ -27,12 +27,15 @@ __global__ void k_cell_key(DevPtrs P, int natom) {
   if (a >= natom) return;
   const Rep R = P.reps[P.rep_of[a]];
   int c[3];
+  bool out = false;
   for (int k = 0; k < 3; ++k) {
     const double x = P.x[3 * a + k];
+    out |= R.free_bnd && !(x >= R.win_lo[k] && x <= R.win_hi[k]);
     const double w = x - R.box[k] * floor(x * R.invbox[k]);
     int q = (int)(w / R.cell[k]);
     c[k] = q < 0 ? 0 : (q >= R.grid[k] ? R.grid[k] - 1 : q);
   }
+  if (out) atomicOr(P.status, ERR_FREE_WINDOW);
   const unsigned key = (unsigned)(R.key0 + (c[1] * R.grid[0] + c[0]) * R.grid[2] + c[2]);
   P.key[a] = key;
   atomicAdd(&P.hist[key], 1);

@@ -37,7 +37,7 @@ constexpr double kJouCal = 4.184;
 enum : unsigned {
   ERR_SHAKE_NOCONV = 1u, ERR_SHAKE_SINGULAR = 2u, ERR_NONFINITE = 4u,
   ERR_FIX_OVERFLOW = 8u, ERR_LIST_OVERFLOW = 16u, ERR_SORT = 32u, ERR_TIMEOUT = 64u,
-  ERR_STOP_MASS = 128u, ERR_STOP_SINGULAR = 256u
+  ERR_STOP_MASS = 128u, ERR_STOP_SINGULAR = 256u, ERR_FREE_WINDOW = 512u
 };
 
 // per-replica constants
@@ -65,6 +65,10 @@ struct Rep {
   int stop_n;                     // centre-of-mass stop: atoms [atom0, atom0 + stop_n); 0 = off
   double lam_m, lam_im;           // lambda mass and its inverse
   double dself_cls[3];            // ZD self term by class
+  // BOUNDA= NO: the periodic box is a container large enough that minimum image is the
+  // identity while every atom stays in [win_lo, win_hi]
+  int free_bnd;
+  double win_lo[3], win_hi[3];
 };
 
 // class weight of a term (verlethe.f90:116-163): class 0 = AA, 1 = AB, 2 = BB

@@ -877,19 +877,18 @@ __global__ void __launch_bounds__(64) k_micr_fused(DevPtrs P, IntConst c, int nu
       }
       add_kin(P, c.nsub_total, c.nkin - 1, sub, ke);
     }
-    finish_last(P, c, c.temp);
-    return;
-  }
-  for (int base = 0; base < nunit; base += nthr) {
-    const int t = base + gt;
-    double ke = 0.0;
-    int sub = -1;
-    if (t < nunit) {
-      const Unit u = P.units[t];
-      sub = u.sub;
-      ke = micr_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
+  } else {
+    for (int base = 0; base < nunit; base += nthr) {
+      const int t = base + gt;
+      double ke = 0.0;
+      int sub = -1;
+      if (t < nunit) {
+        const Unit u = P.units[t];
+        sub = u.sub;
+        ke = micr_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
+      }
+      add_kin(P, c.nsub_total, c.nkin - 1, sub, ke);
     }
-    add_kin(P, c.nsub_total, c.nkin - 1, sub, ke);
   }
   finish_last(P, c, c.temp);
 }

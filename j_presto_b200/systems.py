@@ -476,9 +476,11 @@ def water_box(nwat, box, seed=1, jitter=0.3, temp=300.0):
     return _finalize(top, np.full(3, float(box)), temp, rng)
 
 
-def solvated_polymer(nres, nwat, box=None, seed=2, nion_pairs=0, temp=300.0):
+def solvated_polymer(nres, nwat, box=None, seed=2, nion_pairs=0, temp=300.0, sphere=None):
     """A `nres`-residue chain plus `nwat` waters and Na+/Cl- (neutralising, plus
-    `nion_pairs` extra pairs) in a cubic PBC box."""
+    `nion_pairs` extra pairs) in a cubic PBC box; with `sphere` (a radius) the chain is
+    built inside a cube of half-edge 0.8 radius and the solvent fills the sphere only (a
+    droplet around the box centre)."""
     rng = np.random.default_rng(seed)
     top = _Top(rng)
     if box is None:
@@ -486,7 +488,10 @@ def solvated_polymer(nres, nwat, box=None, seed=2, nion_pairs=0, temp=300.0):
         # a unique minimum image needs box > 2 (rc + 1.5) = 27 A at the 12 A ZD cut-off
         box = max(vol ** (1.0 / 3.0), 28.0)
     pad = 2.0
-    residues = _build_polymer(top, nres, pad, box - pad, rng, box) if nres else []
+    lo, hi = pad, box - pad
+    if sphere is not None:
+        lo, hi = 0.5 * box - 0.8 * sphere, 0.5 * box + 0.8 * sphere
+    residues = _build_polymer(top, nres, lo, hi, rng, box) if nres else []
     nsol = len(top.pos)
     net = _charges_polymer(top, 0, nsol, residues, rng) if nres else 0
     n_na = nion_pairs + max(0, -net)
@@ -496,6 +501,8 @@ def solvated_polymer(nres, nwat, box=None, seed=2, nion_pairs=0, temp=300.0):
     ncube = need
     while True:
         sites, a = _lattice(box, ncube)
+        if sphere is not None:
+            sites = sites[np.linalg.norm(sites - 0.5 * box, axis=1) < sphere - 1.0]
         if nsol:
             ok = np.ones(len(sites), bool)
             for c0 in range(0, len(sites), 4096):
@@ -519,6 +526,15 @@ def solvated_polymer(nres, nwat, box=None, seed=2, nion_pairs=0, temp=300.0):
         else:
             top.add(p, T_CL, -1.0, MOL_CL)
     return _finalize(top, np.full(3, float(box)), temp, rng)
+
+
+def droplet(nres, nwat, seed=6, temp=300.0):
+    """A chain and `nwat` waters in a sphere at water density, for BOUNDA= NO (the box only
+    holds the construction: periodic images are never near)."""
+    vol = (nwat + 4.0 * nres) / WATER_DENSITY
+    radius = (3.0 * vol / (4.0 * math.pi)) ** (1.0 / 3.0) + 1.5
+    box = 2.0 * radius + 30.0
+    return solvated_polymer(nres, nwat, box=box, seed=seed, temp=temp, sphere=radius)
 
 
 def mcmd_weight(e_min, e_max, ndeg=8, t_lo=280.0, t_hi=700.0, tempce=300.0):

@@ -89,6 +89,7 @@ struct Ctx {
   // ---- DOF (md.f90:116-228) ----
   int idnfre = 0;
   int stop_n = 0;               // centre-of-mass stop: atoms 0..stop_n-1 (ixcend(nstpcn))
+  bool pbc = true;              // BOUNDA= PBC; false: no boundary (*_CB variants)
   int nsub = 1;
   std::vector<double> nfrmol;   // per sub-system DOF
   // ---- pair list: half list (j listed under i) of pairs within rlim at build ----
@@ -100,7 +101,9 @@ struct Ctx {
   int nthreads = 1;
 };
 
+// minimum image (the *_PB variants); the identity with BOUNDA= NO (*_CB)
 inline void minimg(const Ctx& c, double* d) {
+  if (!c.pbc) return;
   for (int k = 0; k < 3; ++k) d[k] -= c.box[k] * anint(d[k] * c.invbox[k]);
 }
 
@@ -114,9 +117,10 @@ void build_list(Ctx& c) {
   const int n = c.n;
   c.nb.assign(n, {});
   const double* x = c.cord.data();
-  int g[3];
-  for (int k = 0; k < 3; ++k) g[k] = std::max(1, (int)std::floor(c.box[k] / c.rlim));
-  const bool brute = (g[0] < 3 || g[1] < 3 || g[2] < 3);
+  int g[3] = {1, 1, 1};
+  if (c.pbc)
+    for (int k = 0; k < 3; ++k) g[k] = std::max(1, (int)std::floor(c.box[k] / c.rlim));
+  const bool brute = !c.pbc || (g[0] < 3 || g[1] < 3 || g[2] < 3);   // all pairs without a box
   std::vector<int> cellof(n), head, next(n, -1);
   if (!brute) {
     head.assign(g[0] * g[1] * g[2], -1);
@@ -953,6 +957,7 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
   c->n = n;
   c->prm = *prm;
   c->nthreads = nthreads > 0 ? nthreads : omp_get_max_threads();
+  c->pbc = prm->bounda == JP_BOUND_PBC;
   for (int k = 0; k < 3; ++k) { c->box[k] = s->box[k]; c->invbox[k] = 1.0 / s->box[k]; }
   c->mass.assign(s->mass, s->mass + n);
   c->imass.resize(n);
@@ -1060,10 +1065,15 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
     c->fcoeff = rtmp * rtmp * rtmp;
     c->bcoeff = 0.5 * c->fcoeff;
   }
+  // CAL15M= ATOM (enear.f90 #ACT lines): E = qi qj co / r, F = qi qj co / r^3 d, which is
+  // the ZD formula with zcore = bcoeff = fcoeff = 0; no self or excess term (#ZD only)
+  const bool zd = prm->cal15m == JP_CAL15M_ZD;
+  if (!zd) c->zcore = c->fcoeff = c->bcoeff = 0.0;
   std::vector<double> dwork(c->chg);   // self term
   std::vector<double> dwk((size_t)3 * n, 0.0);   // per class (incel.f90:629-654)
   for (int i = 0; i < n; ++i) dwk[(size_t)c->pcls(i, i) * n + i] += c->chg[i];
   auto addx = [&](int a, int bb) {
+    if (!zd) return;
     dwork[a] += c->chg[bb];
     dwork[bb] += c->chg[a];
     const int cl = c->pcls(a, bb);
