@@ -177,13 +177,18 @@ typedef struct jp_params {
   int32_t stop_center;   /* JP_STOP_TRANS / ROT / BOTH; JP_STOP_NONE (or 0) = off */
   int32_t stop_natom;    /* ixcend(nstpcn): atoms 1..stop_natom; 0 = the leading atoms that
                             share atom 1's molecule id (all atoms without molecule ids) */
-  /* CAL15M (cmmdo.f90:27-74): JP_CAL15M_ZD (zero-dipole, the default) or JP_CAL15M_ATOM
+  /* CAL15M (cmmdo.f90:27-74): JP_CAL15M_ZD (zero-dipole, the default), JP_CAL15M_ATOM
    * (atom cut-off, enear_ACT_*: E = qi qj / r and the LJ term for r <= CUTLEN, no self or
-   * excess term). */
+   * excess term) or JP_CAL15M_CMM (cell multipole method, BOUNDA= NO only: exact Coulomb
+   * and LJ between atoms of neighbouring level-1 cells, LJ out to CUTLEN from the cells
+   * within CUTLEN, and the far field of up to 5 cell levels by multipoles). */
   int32_t cal15m;
   /* BOUNDA (inpmd.f90:72): JP_BOUND_PBC (the box of jp_system) or JP_BOUND_NONE (no
    * boundary, the *_CB variants: no minimum image; the box of jp_system is ignored). */
   int32_t bounda;
+  int32_t cmm_levels;    /* CELLVL: cell levels of the CMM (raised to fit the system, <= 5) */
+  double cmm_cell;       /* CELSIZ: edge of a level-1 CMM cell (Angstrom) */
+  int32_t cmm_update;    /* CMMUPD: far-field interval (steps); UPDATE must be a multiple */
 } jp_params;
 
 enum { JP_ALSD_NONE = 0, JP_ALSD_LMD = 1, JP_ALSD_LMD2 = 2 };

@@ -89,7 +89,8 @@ class JpParams(C.Structure):
         ("alsd", C.c_int32), ("lambda0", C.c_double), ("lambda_mass", C.c_double),
         ("lambda_temp_control", C.c_int32), ("scale_terms", C.c_int32),
         ("taut", C.c_double), ("stop_center", C.c_int32), ("stop_natom", C.c_int32),
-        ("cal15m", C.c_int32), ("bounda", C.c_int32),
+        ("cal15m", C.c_int32), ("bounda", C.c_int32), ("cmm_levels", C.c_int32),
+        ("cmm_cell", C.c_double), ("cmm_update", C.c_int32),
     ]
 
 
@@ -101,7 +102,7 @@ def default_params(**kw):
                  icslop=3, fcstol=1e-3, psetmp=0.0, device=0, alsd=JP_ALSD_NONE, lambda0=1.0,
                  lambda_mass=0.0, lambda_temp_control=0, scale_terms=0, taut=40.0,
                  stop_center=JP_STOP_NONE, stop_natom=0, cal15m=JP_CAL15M_ZD,
-                 bounda=JP_BOUND_PBC)
+                 bounda=JP_BOUND_PBC, cmm_levels=3, cmm_cell=6.0, cmm_update=5)
     for k, v in kw.items():
         if not hasattr(p, k):
             raise KeyError(k)

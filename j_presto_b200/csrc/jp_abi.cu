@@ -324,6 +324,9 @@ void jp_default_params(jp_params *p) {
   p->stop_natom = 0;
   p->cal15m = JP_CAL15M_ZD;
   p->bounda = JP_BOUND_PBC;
+  p->cmm_levels = 3;               // inpinp.f90:86 intele(16)
+  p->cmm_cell = 6.0;               // inpinp.f90:86 reaele(17)
+  p->cmm_update = 5;               // inpmd.f90:151 intele(66)
 }
 
 const char *jp_strerror(int code) {

@@ -55,6 +55,10 @@ def lib():
         L.or_set_lambda.restype = None
         L.or_remotv.argtypes = [vp, dp, dp]
         L.or_nfrmol.argtypes = [vp, dp]
+        L.or_cmm_level.argtypes = [vp, C.c_int, dp, C.POINTER(C.c_int), dp]
+        L.or_cmm_nlev.argtypes = [vp]
+        L.or_cmm_far.argtypes = [vp, dp]
+        L.or_cmm_far.restype = C.c_double
         _lib = L
     return _lib
 
@@ -149,6 +153,26 @@ class Oracle:
         v = np.ascontiguousarray(vel, np.float64).copy()
         ier = lib().or_remotv(self._h, _dp(np.ascontiguousarray(xp, np.float64)), _dp(v))
         return ier, v
+
+    def cmm_levels(self):
+        """Per CMM level (1..nlev): (multipoles [nv^3][13], populations [nv^3], centres
+        [nv][3]); cells x fastest."""
+        out = []
+        for l in range(1, lib().or_cmm_nlev(self._h) + 1):
+            nv = lib().or_cmm_level(self._h, l, None, None, None)
+            pot = np.zeros((nv ** 3, 13))
+            pop = np.zeros(nv ** 3, np.int32)
+            cen = np.zeros((nv, 3))
+            lib().or_cmm_level(self._h, l, _dp(pot), pop.ctypes.data_as(C.POINTER(C.c_int)),
+                               _dp(cen))
+            out.append((pot, pop, cen))
+        return out
+
+    def cmm_far(self):
+        """(far-field energy, its gradient [natom][3]) of the last force call (CMM)."""
+        g = np.zeros((self.n, 3))
+        e = lib().or_cmm_far(self._h, _dp(g))
+        return e, g
 
     def nfrmol(self):
         n = lib().or_nfrmol(self._h, None)

@@ -94,6 +94,19 @@ struct Ctx {
   std::vector<double> nfrmol;   // per sub-system DOF
   // ---- pair list: half list (j listed under i) of pairs within rlim at build ----
   std::vector<std::vector<int>> nb;
+  // ---- CMM (CAL15M= CMM): levels 1..nlev (index 0 unused) ----
+  bool cmm = false;
+  int nlev = 0, idelay = 0, nv[6] = {0, 0, 0, 0, 0, 0};
+  double siz[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<double> cen[6];            // [3][nv] cell centres per level (celpar_CB)
+  std::vector<int> pop[6];               // atoms per cell [nv^3], x fastest
+  std::vector<double> pot[6];            // 13 coefficients per cell (celpol)
+  std::vector<int> cell1;                // level-1 cell (1-based ix, iy, iz) of each atom
+  std::vector<std::vector<char>> nbt;    // per listed pair: 1 = Coulomb + LJ, 0 = LJ only
+  std::vector<double> gwk;               // far-field gradient of the last update
+  double ecmm = 0.0;                     // its energy (sum over levels)
+  bool itwin = true;                     // recompute the far field at the next force call
+  int cmm_err = 0;                       // error of the last rebuild (an atom off the grid)
   // ---- state ----
   std::vector<double> cord, vel, grad;
   long long idloop = 0;
@@ -113,7 +126,13 @@ inline void minimg(const Ctx& c, double* d) {
 // the itab14 removal (cutoff.f90:50-96).  A plain cell grid replaces the reference's
 // cell hierarchy; the resulting pair SET is the same.
 // ---------------------------------------------------------------------------------------
+int cmm_rebuild(Ctx& c);
+
 void build_list(Ctx& c) {
+  if (c.cmm) {
+    c.cmm_err = cmm_rebuild(c);
+    return;
+  }
   const int n = c.n;
   c.nb.assign(n, {});
   const double* x = c.cord.data();
@@ -166,6 +185,218 @@ void build_list(Ctx& c) {
       std::sort(L.begin(), L.end());
     }
   }
+}
+
+// ---------------------------------------------------------------------------------------
+// CMM (CAL15M= CMM, BOUNDA= NO).  Cell geometry of incel.f90:41-57 / mk_c (:1245-1276),
+// re-centred on the atoms' centroid at each rebuild (celpar.f90 celpar_CB :36-53); atom
+// cells as celpar.f90:90-116; level populations celoth.f90; multipoles celpol.f90 (level 1
+// from the atoms, then level to level); near tables neartb.f90 (Coulomb + LJ between atoms
+// of neighbouring level-1 cells; LJ only for cells up to idelay apart and dd < rc^2 at the
+// rebuild; 1-2/1-3/1-4 partners removed); far field cmmdo.f90:80-170, :181-290 over the
+// cell lists of mk_cm (incel.f90:1098-1240).
+// ---------------------------------------------------------------------------------------
+inline int cidx(const Ctx& c, int l, int ix, int iy, int iz) {   // 1-based indices
+  return ((iz - 1) * c.nv[l] + (iy - 1)) * c.nv[l] + (ix - 1);
+}
+
+inline int lvup(int i) { return (i + 1) / 2; }
+
+// returns 0 or JP_E_CELL_OVERFLOW (an atom outside the level-1 grid, celpar ier=28)
+int cmm_rebuild(Ctx& c) {
+  const int n = c.n;
+  const double* x = c.cord.data();
+  double cord0[3];
+  const double rtmp = 1.0 / (double)n;
+  for (int k = 0; k < 3; ++k) {
+    double sum = 0.0;
+    for (int i = 0; i < n; ++i) sum += x[3 * i + k];
+    cord0[k] = sum * rtmp;
+  }
+  for (int l = 1; l <= c.nlev; ++l) {
+    const int m = c.nv[l];
+    c.cen[l].assign(3 * m, 0.0);
+    const double r = -0.5 * (m + 1);
+    for (int i = 1; i <= m; ++i)
+      for (int k = 0; k < 3; ++k) c.cen[l][3 * (i - 1) + k] = c.siz[l] * ((double)i + r) + cord0[k];
+    c.pop[l].assign((size_t)m * m * m, 0);
+    c.pot[l].assign((size_t)13 * m * m * m, 0.0);
+  }
+  // level-1 cells of the atoms
+  const double half = c.siz[1] * 0.5, rr = 1.0 / c.siz[1];
+  const double org[3] = {c.cen[1][0] - half, c.cen[1][1] - half, c.cen[1][2] - half};
+  const int nv1 = c.nv[1];
+  c.cell1.assign(3 * n, 0);
+  std::vector<std::vector<int>> members((size_t)nv1 * nv1 * nv1);
+  for (int i = 0; i < n; ++i) {
+    int m[3];
+    for (int k = 0; k < 3; ++k) {
+      m[k] = (int)((x[3 * i + k] - org[k]) * rr) + 1;   // Fortran int(): toward zero
+      if (m[k] < 1 || m[k] > nv1) return JP_E_CELL_OVERFLOW;
+      c.cell1[3 * i + k] = m[k];
+    }
+    const int id = cidx(c, 1, m[0], m[1], m[2]);
+    c.pop[1][id] += 1;
+    members[id].push_back(i);
+  }
+  // populations of the upper levels (celoth)
+  for (int l = 2; l <= c.nlev; ++l)
+    for (int iz = 1; iz <= c.nv[l - 1]; ++iz)
+      for (int iy = 1; iy <= c.nv[l - 1]; ++iy)
+        for (int ix = 1; ix <= c.nv[l - 1]; ++ix)
+          c.pop[l][cidx(c, l, lvup(ix), lvup(iy), lvup(iz))] += c.pop[l - 1][cidx(c, l - 1, ix, iy, iz)];
+  // level-1 multipoles about the cell centres, raw charges (celpol.f90:27-80)
+  for (int iz = 1; iz <= nv1; ++iz)
+    for (int iy = 1; iy <= nv1; ++iy)
+      for (int ix = 1; ix <= nv1; ++ix) {
+        const int id = cidx(c, 1, ix, iy, iz);
+        if (members[id].empty()) continue;
+        const double g[3] = {c.cen[1][3 * (ix - 1)], c.cen[1][3 * (iy - 1) + 1], c.cen[1][3 * (iz - 1) + 2]};
+        double qz = 0, rx = 0, ry = 0, rz = 0, rxx = 0, ryy = 0, rzz = 0, rxy = 0, ryz = 0, rzx = 0;
+        for (int a : members[id]) {
+          const double cc = c.chg[a];
+          const double dx = x[3 * a] - g[0], dy = x[3 * a + 1] - g[1], dz = x[3 * a + 2] - g[2];
+          qz += cc;
+          rx += cc * dx; ry += cc * dy; rz += cc * dz;
+          const double dxx = dx * dx, dyy = dy * dy, dzz = dz * dz;
+          rxx += cc * (2 * dxx - dyy - dzz);
+          ryy += cc * (2 * dyy - dzz - dxx);
+          rzz += cc * (2 * dzz - dxx - dyy);
+          rxy += cc * dx * dy; ryz += cc * dy * dz; rzx += cc * dz * dx;
+        }
+        double* q = &c.pot[1][(size_t)13 * id];
+        const double v[13] = {qz, rx, ry, rz, rxx * 0.5, ryy * 0.5, rzz * 0.5, rxx, ryy, rzz,
+                              rxy * 3.0, ryz * 3.0, rzx * 3.0};
+        for (int k = 0; k < 13; ++k) q[k] = v[k];
+      }
+  // level l-1 -> l, children in celpol's order (x fastest), shifted to the parent centre
+  for (int l = 2; l <= c.nlev; ++l)
+    for (int iz = 1; iz <= c.nv[l]; ++iz)
+      for (int iy = 1; iy <= c.nv[l]; ++iy)
+        for (int ix = 1; ix <= c.nv[l]; ++ix) {
+          const int id = cidx(c, l, ix, iy, iz);
+          if (c.pop[l][id] == 0) continue;
+          double qz = 0, rx = 0, ry = 0, rz = 0, rxx = 0, ryy = 0, rzz = 0, rxy = 0, ryz = 0, rzx = 0;
+          for (int jj = 0; jj < 8; ++jj) {
+            const int mx = 2 * ix - 1 + (jj & 1), my = 2 * iy - 1 + ((jj >> 1) & 1), mz = 2 * iz - 1 + ((jj >> 2) & 1);
+            const int cid = cidx(c, l - 1, mx, my, mz);
+            if (c.pop[l - 1][cid] == 0) continue;
+            const double* p = &c.pot[l - 1][(size_t)13 * cid];
+            const double qq = p[0];
+            qz += qq;
+            const double xx = c.cen[l - 1][3 * (mx - 1)] - c.cen[l][3 * (ix - 1)];
+            const double yy = c.cen[l - 1][3 * (my - 1) + 1] - c.cen[l][3 * (iy - 1) + 1];
+            const double zz = c.cen[l - 1][3 * (mz - 1) + 2] - c.cen[l][3 * (iz - 1) + 2];
+            const double ax = p[1], ay = p[2], az = p[3];
+            rx += ax + qq * xx; ry += ay + qq * yy; rz += az + qq * zz;
+            const double dxx = xx * xx, dyy = yy * yy, dzz = zz * zz;
+            const double xax = xx * ax, yay = yy * ay, zaz = zz * az;
+            rxx += p[4] + 2 * xax - yay - zaz + qq * (dxx - 0.5 * (dyy + dzz));
+            ryy += p[5] + 2 * yay - zaz - xax + qq * (dyy - 0.5 * (dzz + dxx));
+            rzz += p[6] + 2 * zaz - xax - yay + qq * (dzz - 0.5 * (dxx + dyy));
+            rxy += p[10] * 0.5 + (yy * ax + xx * ay + xx * yy * qq) * 1.5;
+            ryz += p[11] * 0.5 + (zz * ay + yy * az + yy * zz * qq) * 1.5;
+            rzx += p[12] * 0.5 + (xx * az + zz * ax + zz * xx * qq) * 1.5;
+          }
+          double* q = &c.pot[l][(size_t)13 * id];
+          const double v[13] = {qz, rx, ry, rz, rxx, ryy, rzz, rxx * 2.0, ryy * 2.0, rzz * 2.0,
+                                rxy * 2.0, ryz * 2.0, rzx * 2.0};
+          for (int k = 0; k < 13; ++k) q[k] = v[k];
+        }
+  // near tables (neartb): all pairs of neighbouring cells, LJ-only pairs out to idelay cells
+  c.nb.assign(n, {});
+  c.nbt.assign(n, {});
+  const double rc2 = c.rc * c.rc;
+#pragma omp parallel for schedule(dynamic, 32)
+  for (int i = 0; i < n; ++i) {
+    for (int j = i + 1; j < n; ++j) {
+      int cheb = 0;
+      for (int k = 0; k < 3; ++k) cheb = std::max(cheb, std::abs(c.cell1[3 * i + k] - c.cell1[3 * j + k]));
+      char kind;
+      if (cheb <= 1) {
+        kind = 1;
+      } else if (c.idelay > 1 && cheb <= c.idelay) {
+        const double dx = x[3 * i] - x[3 * j], dy = x[3 * i + 1] - x[3 * j + 1], dz = x[3 * i + 2] - x[3 * j + 2];
+        if (!(dx * dx + dy * dy + dz * dz < rc2)) continue;
+        kind = 0;
+      } else {
+        continue;
+      }
+      if (std::binary_search(c.excl[i].begin(), c.excl[i].end(), j)) continue;
+      c.nb[i].push_back(j);
+      c.nbt[i].push_back(kind);
+    }
+  }
+  return 0;
+}
+
+// far field of every atom (cmmdo.f90:85-160, compute_particle_multipole :181-290) into
+// c.gwk (gradient) and c.ecmm (energy), from the multipoles of the last rebuild
+void cmm_far(Ctx& c, const double* x) {
+  const int n = c.n;
+  c.gwk.assign(3 * (size_t)n, 0.0);
+  double ecmm[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < n; ++i) {
+    int a[3] = {c.cell1[3 * i], c.cell1[3 * i + 1], c.cell1[3 * i + 2]};
+    double gx = 0, gy = 0, gz = 0;
+    for (int l = 1; l <= c.nlev; ++l) {
+      if (l > 1)
+        for (int k = 0; k < 3; ++k) a[k] = lvup(a[k]);
+      const int m = c.nv[l];
+      int lo[3], hi[3], nlo[3], nhi[3];
+      for (int k = 0; k < 3; ++k) {
+        nlo[k] = std::max(1, a[k] - 1);
+        nhi[k] = std::min(m, a[k] + 1);
+        if (l < c.nlev) {   // children of the parent's neighbours (mk_cm)
+          const int p = lvup(a[k]), m1 = c.nv[l + 1];
+          lo[k] = std::max(1, p - 1) * 2 - 1;
+          hi[k] = std::min(m1, p + 1) * 2;
+        } else {            // the top level: every cell
+          lo[k] = 1;
+          hi[k] = m;
+        }
+      }
+      double e = 0.0;
+      for (int kz = lo[2]; kz <= hi[2]; ++kz)
+        for (int ky = lo[1]; ky <= hi[1]; ++ky)
+          for (int kx = lo[0]; kx <= hi[0]; ++kx) {
+            if (kx >= nlo[0] && kx <= nhi[0] && ky >= nlo[1] && ky <= nhi[1] && kz >= nlo[2] && kz <= nhi[2])
+              continue;
+            const int id = cidx(c, l, kx, ky, kz);
+            if (c.pop[l][id] == 0) continue;
+            const double* q = &c.pot[l][(size_t)13 * id];
+            const double dx = x[3 * i] - c.cen[l][3 * (kx - 1)];
+            const double dy = x[3 * i + 1] - c.cen[l][3 * (ky - 1) + 1];
+            const double dz = x[3 * i + 2] - c.cen[l][3 * (kz - 1) + 2];
+            const double dx2 = dx * dx, dy2 = dy * dy, dz2 = dz * dz;
+            const double dd2i = 1.0 / (dx2 + dy2 + dz2);
+            const double ddi = std::sqrt(dd2i);
+            const double dd3i = ddi * dd2i, dd5i = dd3i * dd2i;
+            const double dxy = dx * dy, dyz = dy * dz, dzx = dz * dx;
+            const double aa1 = q[1] * dx + q[2] * dy + q[3] * dz;
+            const double aa2 = q[4] * dx2 + q[5] * dy2 + q[6] * dz2 + q[10] * dxy + q[11] * dyz + q[12] * dzx;
+            e += q[0] * ddi + aa1 * dd3i + aa2 * dd5i;
+            const double bbx = (q[0] * dx - q[1]) * dd3i, bby = (q[0] * dy - q[2]) * dd3i,
+                         bbz = (q[0] * dz - q[3]) * dd3i;
+            const double c2x = q[7] * dx + q[10] * dy + q[12] * dz;
+            const double c2y = q[10] * dx + q[8] * dy + q[11] * dz;
+            const double c2z = q[12] * dx + q[11] * dy + q[9] * dz;
+            const double cc4 = aa1 * 3.0 + aa2 * dd2i * 5.0;
+            gx += -bbx + (c2x - cc4 * dx) * dd5i;
+            gy += -bby + (c2y - cc4 * dy) * dd5i;
+            gz += -bbz + (c2z - cc4 * dz) * dd5i;
+          }
+      ecmm[l] += c.ccoef * c.chg[i] * e;   // chgmod2 = ccoef * charge (inpcls.f90:223)
+    }
+    const double q2 = c.ccoef * c.chg[i];
+    c.gwk[3 * i] = gx * q2;
+    c.gwk[3 * i + 1] = gy * q2;
+    c.gwk[3 * i + 2] = gz * q2;
+  }
+  double tot = 0.0;
+  for (int l = 1; l <= c.nlev; ++l) tot += ecmm[l] * 0.5;
+  c.ecmm = tot;
+  c.itwin = false;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -350,15 +581,21 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
       const double chgi = c.chgmod[i];
       const int it1 = c.typ[i];
       double gwx = 0, gwy = 0, gwz = 0;
-      for (int j : c.nb[i]) {
+      for (size_t q = 0; q < c.nb[i].size(); ++q) {
+        const int j = c.nb[i][q];
         double d[3] = {xi - x[3 * j], yi - x[3 * j + 1], zi - x[3 * j + 2]};
         minimg(c, d);
         double dd2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
         double dd2i = 1.0 / dd2;
         double co = (dd2i - c.irlim2 >= 0.0) ? 1.0 : 0.0;   // sign(0.5,dd2i-irlim2)+0.5
+        double coel = co;
+        if (c.cmm) {   // enear_CMM: no cut-off; the LJ-only table has no Coulomb term
+          co = 1.0;
+          coel = c.nbt[i][q] ? 1.0 : 0.0;
+        }
         double ddi = std::sqrt(dd2i);
         double dd6i = dd2i * dd2i * dd2i * co;
-        double ee = chgi * c.chgmod[j] * co;
+        double ee = chgi * c.chgmod[j] * coel;
         const double epair = ee * (ddi + c.bcoeff * dd2 - c.zcore);
         eel += epair;
         int it2 = c.typ[j];
@@ -371,7 +608,7 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
         double fx = d[0] * cc, fy = d[1] * cc, fz = d[2] * cc;
         gwx += fx; gwy += fy; gwz += fz;
         G[3 * j] += fx; G[3 * j + 1] += fy; G[3 * j + 2] += fz;
-        npair += (co > 0.0) ? 1 : 0;
+        npair += (coel > 0.0) ? 1 : 0;
       }
       G[3 * i] -= gwx; G[3 * i + 1] -= gwy; G[3 * i + 2] -= gwz;
     }
@@ -397,6 +634,11 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
       grad[3 * a + k] += d[k] * cc;
       grad[3 * b + k] -= d[k] * cc;
     }
+  }
+  if (c.cmm) {   // far field: recomputed when itwin is set, else the last one again
+    if (c.itwin) cmm_far(c, x);
+    for (int k = 0; k < 3 * n; ++k) grad[k] += c.gwk[k];
+    eel += c.ecmm;
   }
   ene[JP_E_VDW15] += evdw;
   ene[JP_E_ELE15] += eel + c.dself + eexc;
@@ -1153,6 +1395,30 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
       c->nfrmol[best] += 1.0;
     }
   }
+  // CMM geometry (incel.f90:29-57): rlim = CUTLEN, level sizes, nlev raised to the extent
+  c->cmm = prm->cal15m == JP_CAL15M_CMM;
+  if (c->cmm) {
+    double ext = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      double lo = s->cord[k], hi = s->cord[k];
+      for (int i = 1; i < n; ++i) {
+        lo = std::min(lo, s->cord[3 * i + k]);
+        hi = std::max(hi, s->cord[3 * i + k]);
+      }
+      ext = std::max(ext, hi - lo);
+    }
+    int nlev = prm->cmm_levels;
+    const double cminsiz = prm->cmm_cell;
+    if (std::ldexp(1.0, nlev + 1) * cminsiz < ext)
+      nlev = (int)std::ceil(std::log(ext / cminsiz) / std::log(2.0) - 1.0);
+    c->nlev = nlev;
+    for (int l = 1; l <= nlev; ++l) {
+      c->nv[l] = 4 << (nlev - l);
+      c->siz[l] = cminsiz * (double)(1 << (l - 1));
+    }
+    c->idelay = (int)std::ceil(c->rc / c->siz[1]);
+    c->itwin = true;
+  }
   // state
   c->cord.assign(s->cord, s->cord + 3 * n);
   c->vel.assign(3 * n, 0.0);
@@ -1193,8 +1459,34 @@ int or_dof(void* h) { return ((Ctx*)h)->idnfre; }
 int or_energy_grad(void* h, const double* cord, double* ene, double* grad) {
   Ctx* c = (Ctx*)h;
   if (cord) std::memcpy(c->cord.data(), cord, sizeof(double) * 3 * c->n);
+  const bool keep = c->itwin;
+  c->itwin = true;   // a single-point evaluation takes the far field at these coordinates
   energy_grad(*c, c->cord.data(), ene, grad);
+  c->itwin = keep;   // and leaves the step loop's far-field cadence as it was
   return 0;
+}
+
+// CMM state of level l (1-based): returns nv (0 without CMM); pot [nv^3][13], pop [nv^3],
+// cen [nv][3] (each nullable).  Test hook.
+int or_cmm_level(void* h, int l, double* pot, int* pop, double* cen) {
+  Ctx* c = (Ctx*)h;
+  if (!c->cmm || l < 1 || l > c->nlev) return 0;
+  const size_t nc = (size_t)c->nv[l] * c->nv[l] * c->nv[l];
+  if (pot) std::memcpy(pot, c->pot[l].data(), sizeof(double) * 13 * nc);
+  if (pop) std::memcpy(pop, c->pop[l].data(), sizeof(int) * nc);
+  if (cen) std::memcpy(cen, c->cen[l].data(), sizeof(double) * 3 * c->nv[l]);
+  return c->nv[l];
+}
+
+int or_cmm_nlev(void* h) { return ((Ctx*)h)->cmm ? ((Ctx*)h)->nlev : 0; }
+
+// far-field energy of the last force call; gwk (nullable) [natom][3] its gradient.
+// Test hook.
+double or_cmm_far(void* h, double* gwk) {
+  Ctx* c = (Ctx*)h;
+  if (!c->cmm) return 0.0;
+  if (gwk) std::memcpy(gwk, c->gwk.data(), sizeof(double) * 3 * c->n);
+  return c->ecmm;
 }
 
 int or_shake(void* h, double* r1, const double* r2) { return shake_all(*(Ctx*)h, r1, r2); }
@@ -1216,7 +1508,12 @@ int or_run(void* h, int nsteps, double* ene_out, double* temp_out) {
     if (ier != 0) return ier;
     if (ene_out) std::memcpy(ene_out + (size_t)s * JP_MAXENE, ene, sizeof(ene));
     if (temp_out) temp_out[s] = caltmp(*c, c->vel.data());
-    if (c->prm.update > 0 && c->idloop % c->prm.update == 0) build_list(*c);
+    if (c->prm.update > 0 && c->idloop % c->prm.update == 0) {
+      build_list(*c);
+      if (c->cmm_err) return c->cmm_err;
+    }
+    // CMM far-field marker for the next step (md.f90:680-684)
+    if (c->cmm) c->itwin = c->idloop % c->prm.cmm_update == 0;
   }
   return 0;
 }
