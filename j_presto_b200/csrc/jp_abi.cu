@@ -53,6 +53,9 @@ struct jp_ctx {
   bool minimg = true;
   int pair_warps = 0;
   bool alsd = false;
+  bool cmm = false;                 // CAL15M= CMM
+  int cmm_ncell[6] = {0, 0, 0, 0, 0, 0};   // cells per level over all replicas
+  int cmm_nlev = 0;                 // most levels of any replica
   int cano_grid = 1;
   int hist_cap = 1024;
   long long idloop = 0;
@@ -127,6 +130,16 @@ void enqueue_rebuild(jp_ctx *c) {
   cudaMemsetAsync(P.hist, 0, sizeof(int) * (c->nkeys + 1), st);
   cudaMemsetAsync(P.cursor, 0, sizeof(int) * (c->nkeys + 1), st);
   cudaMemsetAsync(P.rep_hmax, 0, sizeof(float) * 3 * c->nrep, st);
+  int ncmm = 0;
+  if (c->cmm) {   // celpar_CB + celoth + celpol: cells and multipoles at this rebuild
+    int ntot = 0;
+    for (int l = 1; l <= c->cmm_nlev; ++l) ntot += c->cmm_ncell[l];
+    cudaMemsetAsync(P.cmm_c0, 0, sizeof(double) * 3 * c->nrep, st);
+    cudaMemsetAsync(P.cmm_pop, 0, sizeof(int) * ntot, st);
+    cudaMemsetAsync(P.cmm_raw, 0, sizeof(double) * 10 * c->cmm_ncell[1], st);
+    launch_cmm_rebuild(P, c->natom, c->nrep, c->cmm_ncell[1], c->cmm_ncell, c->cmm_nlev, st);
+    ncmm = 3 + std::max(0, c->cmm_nlev - 1);
+  }
   k_cell_key<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
   scan_exclusive(P.hist, P.hist_scan, c->nkeys + 1, c->scan_scratch, nullptr, st);
   k_scatter<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
@@ -138,12 +151,13 @@ void enqueue_rebuild(jp_ctx *c) {
   k_excl_slots<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
   k_block_setup<<<(c->nblk * 32 + nt - 1) / nt, nt, 0, st>>>(P, c->nblk, c->qscale);
   if (c->fp64) k_fill_pos_d<<<(c->nslot + nt - 1) / nt, nt, 0, st>>>(P, c->nslot, c->qscale);
-  const double rlim = c->prm.cutoff + 1.5;
+  const double rlim = c->zc.rlim;   // rc + 1.5; CMM: the farthest near-field pair
+  const double rc = c->prm.cutoff;
   const int nwb = (c->nchunk * 32 + 127) / 128;
-  k_tile_scan_chunks<<<nwb, 128, 0, st>>>(P, c->nchunk, rlim * rlim, (float)rlim);
+  launch_tile_scan(P, c->nchunk, rlim * rlim, (float)rlim, rc * rc, c->cmm, st);
   scan_exclusive(P.chunk_cnt, P.chunk_off, c->nchunk + 1, c->scan_scratch, P.ntiles, st);
-  k_tile_emit<<<nwb, 128, 0, st>>>(P, c->nchunk);
-  c->launches_rebuild = 19 + (c->fp64 ? 1 : 0);
+  k_tile_emit<<<nwb, 128, 0, st>>>(P, c->nchunk, c->cmm ? 1 : 0);
+  c->launches_rebuild = 19 + (c->fp64 ? 1 : 0) + ncmm;
 }
 
 // ---- one MD step ------------------------------------------------------------------------
@@ -157,14 +171,17 @@ void enqueue_zero(jp_ctx *c, bool count) {
   if (count) cudaMemsetAsync(P.pair_cnt, 0, sizeof(long long) * c->nrep, st);
 }
 
-void enqueue_pair(jp_ctx *c, bool count) {
+// the non-bonded forces: pair tiles, and with CMM the far field (recomputed every CMMUPD
+// steps by the step counter, or always with force_far: a single-point evaluation)
+void enqueue_pair(jp_ctx *c, bool count, bool force_far = false) {
   if (c->fp64) launch_pair_fp64(c->P, c->zc, c->pair_warps, count, c->alsd, c->st);
   else launch_pair_mixed(c->P, c->zc, c->pair_warps, c->minimg, count, c->alsd, c->st);
+  if (c->cmm) launch_cmm_far(c->P, c->natom, c->nrep, c->fp64, force_far, c->qscale * c->qscale, c->st);
 }
 
-void enqueue_forces(jp_ctx *c, bool count) {
+void enqueue_forces(jp_ctx *c, bool count, bool force_far = false) {
   enqueue_zero(c, count);
-  enqueue_pair(c, count);
+  enqueue_pair(c, count, force_far);
 }
 
 void enqueue_bonded(jp_ctx *c) {
@@ -190,6 +207,7 @@ int launches_per_step(const jp_ctx *c) {
   n += c->nterm > 0 ? 1 : 0;      // bonded
   n += 1;                          // the fused cooperative MICR or CANO/GE kernel
   n += c->ic.ge_prescaled ? 1 : 0; // k_ge_scale
+  n += c->cmm ? 2 : 0;             // k_cmm_far, k_cmm_energy
   return n;
 }
 
@@ -219,6 +237,7 @@ int check_status(jp_ctx *c) {
   if (s & ERR_NONFINITE) return JP_E_NONFINITE;
   if (s & ERR_FIX_OVERFLOW) return JP_E_FIXED_OVERFLOW;
   if (s & ERR_FREE_WINDOW) return JP_E_FREE_WINDOW;
+  if (s & ERR_CMM_GRID) return JP_E_CELL_OVERFLOW;
   if (s & ERR_STOP_MASS) return JP_E_STOP_MASS;
   if (s & ERR_STOP_SINGULAR) return JP_E_STOP_SINGULAR;
   if (s & ERR_SHAKE_SINGULAR) return JP_E_SHAKE_SINGULAR;
@@ -232,7 +251,14 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
   if (prm->method < JP_METHOD_CONS || prm->method > JP_METHOD_GE) return JP_E_INVALID;
   if (prm->method == JP_METHOD_CONS && !(prm->taut > 0.0)) return JP_E_INVALID;
   if (prm->stop_center < 0 || prm->stop_center > JP_STOP_NONE || prm->stop_natom < 0) return JP_E_INVALID;
-  if (prm->cal15m != JP_CAL15M_ZD && prm->cal15m != JP_CAL15M_ATOM) return JP_E_INVALID;
+  if (prm->cal15m != JP_CAL15M_ZD && prm->cal15m != JP_CAL15M_ATOM && prm->cal15m != JP_CAL15M_CMM)
+    return JP_E_INVALID;
+  if (prm->cal15m == JP_CAL15M_CMM) {   // inpmd.f90:283-288, :525-528; CMM without clusters
+    if (prm->bounda != JP_BOUND_NONE || prm->alsd != JP_ALSD_NONE) return JP_E_INVALID;
+    if (!(prm->cmm_cell > 0.0) || prm->cmm_levels < 1 || prm->cmm_levels > 5 || prm->cmm_update < 1)
+      return JP_E_INVALID;
+    if (prm->update > 0 && prm->update % prm->cmm_update != 0) return JP_E_INVALID;
+  }
   if (prm->bounda != JP_BOUND_PBC && prm->bounda != JP_BOUND_NONE) return JP_E_INVALID;
   if (prm->precision != JP_PREC_FP64 && prm->precision != JP_PREC_MIXED) return JP_E_INVALID;
   if (prm->alsd < JP_ALSD_NONE || prm->alsd > JP_ALSD_LMD2) return JP_E_INVALID;
@@ -421,6 +447,31 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       } else {
         vol *= box[k];
       }
+    }
+    // CMM cell levels (incel.f90:29-57): nlev raised until 2^(nlev+1) CELSIZ covers the
+    // largest extent; nv = 4 * 2^(nlev-l) cells of edge CELSIZ * 2^(l-1) per level
+    R.cmm = prm->cal15m == JP_CAL15M_CMM ? 1 : 0;
+    if (R.cmm) {
+      double ext = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        double lo = s.cord[k], hi = s.cord[k];
+        for (int i = 1; i < n; ++i) {
+          lo = std::min(lo, s.cord[3 * i + k]);
+          hi = std::max(hi, s.cord[3 * i + k]);
+        }
+        ext = std::max(ext, hi - lo);
+      }
+      int nlev = prm->cmm_levels;
+      if (std::ldexp(1.0, nlev + 1) * prm->cmm_cell < ext)
+        nlev = (int)std::ceil(std::log(ext / prm->cmm_cell) / std::log(2.0) - 1.0);
+      if (nlev > 5) { delete c; return JP_E_INVALID; }
+      R.nlev = nlev;
+      for (int l = 1; l <= nlev; ++l) {
+        R.nv[l] = 4 << (nlev - l);
+        R.siz[l] = prm->cmm_cell * (double)(1 << (l - 1));
+      }
+      R.idelay = (int)std::ceil(rc / R.siz[1]);
+      R.cmm_upd = prm->cmm_update;
     }
     // xy columns of edge ~(32/density)^(1/3) so that 32 z-sorted atoms fill a near-cubic
     // block; 0.25 A z bins inside a column
@@ -714,6 +765,22 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     atom0 += n;
     blk0 += R.nblk;
   }
+  // CMM cells of all replicas, level-major: level 1 of every replica, then level 2, ...
+  c->cmm = prm->cal15m == JP_CAL15M_CMM;
+  if (c->cmm) {
+    int off = 0;
+    for (int l = 1; l <= 5; ++l) {
+      const int base = off;
+      for (int r = 0; r < nrep; ++r) {
+        Rep &R = reps[r];
+        if (!R.cmm || l > R.nlev) continue;
+        R.cell_off[l] = off;
+        off += R.nv[l] * R.nv[l] * R.nv[l];
+        c->cmm_nlev = std::max(c->cmm_nlev, R.nlev);
+      }
+      c->cmm_ncell[l] = off - base;
+    }
+  }
   c->reps = reps;
   c->natom = atom0;
   c->nblk = blk0;
@@ -780,6 +847,20 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.tiles, (size_t)c->tile_cap_total);
   e |= dalloc(c, &P.tile_shift, (size_t)c->tile_cap_total);
   e |= dalloc(c, &P.masks, (size_t)c->tile_cap_total * 32);
+  if (c->cmm) {
+    int ntot = 0;
+    for (int l = 1; l <= 5; ++l) ntot += c->cmm_ncell[l];
+    e |= dalloc(c, &P.masks_el, (size_t)c->tile_cap_total * 32);
+    e |= dalloc(c, &P.tmp_masks_el, (size_t)c->tile_cap_total * 32);
+    e |= dalloc(c, &P.cmm_cell, (size_t)N);
+    e |= dalloc(c, &P.gwk, 3 * (size_t)N);
+    e |= dalloc(c, &P.cmm_pop, (size_t)ntot);
+    e |= dalloc(c, &P.cmm_pot, 13 * (size_t)ntot);
+    e |= dalloc(c, &P.cmm_raw, 10 * (size_t)c->cmm_ncell[1]);
+    e |= dalloc(c, &P.cmm_c0, 3 * (size_t)nrep);
+    e |= dalloc(c, &P.cmm_e, (size_t)nrep);
+    e |= dalloc(c, &P.cmm_enew, (size_t)nrep);
+  }
   e |= dalloc(c, &P.ntiles, 1);
   e |= dalloc(c, &P.key, (size_t)N);
   e |= dalloc(c, &P.hist, (size_t)c->nkeys + 1);        // +1: sentinel for the scan
@@ -829,6 +910,13 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   c->zc.fcoeff = zd ? 1.0 / (rc * rc * rc) : 0.0;
   c->zc.bcoeff = 0.5 * c->zc.fcoeff;
   c->zc.rlim = rc + 1.5;
+  c->zc.cmm = c->cmm ? 1 : 0;
+  if (c->cmm) {   // near field without cut-off, out to two level-1 cells along a diagonal
+    double s1 = 0.0;
+    for (int r = 0; r < nrep; ++r) s1 = std::max(s1, c->reps[r].siz[1]);
+    c->zc.rc2 = 1.0e30;
+    c->zc.rlim = std::max(2.0 * std::sqrt(3.0) * s1, rc) * 1.0001 + 0.01;
+  }
   c->zc.nt1 = nt1;
   IntConst &ic = c->ic;
   ic.dt = prm->dt;
@@ -930,7 +1018,7 @@ int jp_energy_grad(jp_ctx *c, int32_t r, const double *cord, double *eneval, dou
                        cudaMemcpyHostToDevice, c->st));
     launch_update_pos(c->P, c->nslot, c->fp64, c->qscale, c->st);
   }
-  enqueue_forces(c, true);
+  enqueue_forces(c, true, true);
   enqueue_bonded(c);
   CK(cudaStreamSynchronize(c->st));
   CK(cudaGetLastError());

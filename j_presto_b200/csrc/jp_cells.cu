@@ -182,27 +182,50 @@ constexpr int kExclReg = 8;   // exclusion partners held in registers per i-atom
 // Tile list, pass A: one warp per chunk = (i-block, 32 consecutive candidate j-blocks
 // starting at j0 >= i, same replica).  Bounding-box test of the 32 candidates at once, then
 // for each survivor the exact mask; non-empty masks go to the chunk's scratch slots.
+// CMM: level-1 cells ci / cj (packed 0-based x | y << 8 | z << 16, -1 = off the grid);
+// neighbours (neartb.f90 first table) set mask and mel, cells up to idelay apart with
+// r^2 < rc2 at the rebuild (neartb.f90:330-370, the LJ-only table) set mask only
+template <bool CMM>
 __device__ __forceinline__ unsigned tile_mask(const DevPtrs& P, const Rep& R, int bi, int bj, int lane,
                                               int ai, double xi, double yi, double zi,
                                               const int (&ps)[kExclReg], int pb, int pe,
-                                              double rlim2) {
+                                              double rlim2, int ci, double rc2, unsigned& mel) {
   const int aj = P.satom[bj * kTile + lane];
   double xj = 0, yj = 0, zj = 0;
-  if (aj >= 0) { xj = P.x[3 * aj]; yj = P.x[3 * aj + 1]; zj = P.x[3 * aj + 2]; }
+  int cj = -1;
+  if (aj >= 0) {
+    xj = P.x[3 * aj]; yj = P.x[3 * aj + 1]; zj = P.x[3 * aj + 2];
+    if (CMM) cj = P.cmm_cell[aj];
+  }
   unsigned mask = 0;
+  mel = 0;
   for (int k = 0; k < 32; ++k) {
     const int src = (lane + k) & 31;
     const double xk = __shfl_sync(0xffffffffu, xj, src);
     const double yk = __shfl_sync(0xffffffffu, yj, src);
     const double zk = __shfl_sync(0xffffffffu, zj, src);
     const int ak = __shfl_sync(0xffffffffu, aj, src);
+    const int ck = CMM ? __shfl_sync(0xffffffffu, cj, src) : 0;
     if (ai < 0 || ak < 0) continue;
     if (bj == bi && (k == 0 || k > 16 || (k == 16 && lane >= 16))) continue;
     double dx = xi - xk, dy = yi - yk, dz = zi - zk;
     dx -= R.box[0] * anint(dx * R.invbox[0]);
     dy -= R.box[1] * anint(dy * R.invbox[1]);
     dz -= R.box[2] * anint(dz * R.invbox[2]);
-    if (dx * dx + dy * dy + dz * dz <= rlim2) mask |= 1u << k;
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (CMM) {
+      if (ci < 0 || ck < 0) continue;
+      const int cheb = max(abs((ci & 255) - (ck & 255)),
+                           max(abs(((ci >> 8) & 255) - ((ck >> 8) & 255)), abs((ci >> 16) - (ck >> 16))));
+      if (cheb <= 1) {
+        mask |= 1u << k;
+        mel |= 1u << k;
+      } else if (R.idelay > 1 && cheb <= R.idelay && d2 < rc2) {
+        mask |= 1u << k;
+      }
+    } else if (d2 <= rlim2) {
+      mask |= 1u << k;
+    }
   }
   // 1-2/1-3/1-4 partners of the i-atom that sit in block bj: lane l sees slot
   // bj*32 + ((l+k)&31) at bit k
@@ -215,10 +238,12 @@ __device__ __forceinline__ unsigned tile_mask(const DevPtrs& P, const Rep& R, in
       if ((sp >> 5) == bj) mask &= ~(1u << (((sp & 31) - lane) & 31));
     }
   }
+  mel &= mask;
   return mask;
 }
 
-__global__ void k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rlimf) {
+template <bool CMM>
+__global__ void k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rlimf, double rc2) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= nchunk) return;
@@ -244,21 +269,25 @@ __global__ void k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rl
   if (ball) {
     const int ai = P.satom[bi * kTile + lane];
     double xi = 0, yi = 0, zi = 0;
-    int pb = 0, pe = 0;
+    int pb = 0, pe = 0, ci = -1;
     int ps[kExclReg];
     if (ai >= 0) {
       xi = P.x[3 * ai]; yi = P.x[3 * ai + 1]; zi = P.x[3 * ai + 2];
       pb = P.excl_ptr[ai];
       pe = P.excl_ptr[ai + 1];
+      if (CMM) ci = P.cmm_cell[ai];
     }
 #pragma unroll
     for (int q = 0; q < kExclReg; ++q) ps[q] = pb + q < pe ? P.excl_slot[pb + q] : -64;
     while (ball) {
       const int b = __ffs(ball) - 1;
       ball &= ball - 1;
-      const unsigned m = tile_mask(P, R, bi, j0 + b, lane, ai, xi, yi, zi, ps, pb, pe, rlim2);
+      unsigned mel;
+      const unsigned m = tile_mask<CMM>(P, R, bi, j0 + b, lane, ai, xi, yi, zi, ps, pb, pe, rlim2,
+                                        ci, rc2, mel);
       if (__any_sync(0xffffffffu, m != 0)) {
         P.tmp_masks[((size_t)w * 32 + b) * 32 + lane] = m;
+        if (CMM) P.tmp_masks_el[((size_t)w * 32 + b) * 32 + lane] = mel;
         nz |= 1u << b;
       }
     }
@@ -270,7 +299,14 @@ __global__ void k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rl
 }
 
 // pass C: copy non-empty tiles to the dense list at the scanned offsets (row-major, j order)
-__global__ void k_tile_emit(DevPtrs P, int nchunk) {
+void launch_tile_scan(const DevPtrs& P, int nchunk, double rlim2, float rlimf, double rc2, bool cmm,
+                      cudaStream_t st) {
+  const int nwb = (nchunk * 32 + 127) / 128;
+  if (cmm) k_tile_scan_chunks<true><<<nwb, 128, 0, st>>>(P, nchunk, rlim2, rlimf, rc2);
+  else k_tile_scan_chunks<false><<<nwb, 128, 0, st>>>(P, nchunk, rlim2, rlimf, rc2);
+}
+
+__global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= nchunk) return;
@@ -283,6 +319,7 @@ __global__ void k_tile_emit(DevPtrs P, int nchunk) {
     const int b = __ffs(nz) - 1;
     nz &= nz - 1;
     P.masks[(size_t)t * 32 + lane] = P.tmp_masks[((size_t)w * 32 + b) * 32 + lane];
+    if (cmm) P.masks_el[(size_t)t * 32 + lane] = P.tmp_masks_el[((size_t)w * 32 + b) * 32 + lane];
     if (lane == 0) {
       const int bj = j0 + b;
       P.tiles[t] = make_int2(bi, bj);

@@ -37,7 +37,7 @@ constexpr double kJouCal = 4.184;
 enum : unsigned {
   ERR_SHAKE_NOCONV = 1u, ERR_SHAKE_SINGULAR = 2u, ERR_NONFINITE = 4u,
   ERR_FIX_OVERFLOW = 8u, ERR_LIST_OVERFLOW = 16u, ERR_SORT = 32u, ERR_TIMEOUT = 64u,
-  ERR_STOP_MASS = 128u, ERR_STOP_SINGULAR = 256u, ERR_FREE_WINDOW = 512u
+  ERR_STOP_MASS = 128u, ERR_STOP_SINGULAR = 256u, ERR_FREE_WINDOW = 512u, ERR_CMM_GRID = 1024u
 };
 
 // per-replica constants
@@ -69,6 +69,11 @@ struct Rep {
   // identity while every atom stays in [win_lo, win_hi]
   int free_bnd;
   double win_lo[3], win_hi[3];
+  // CMM (CAL15M= CMM): levels 1..nlev (index 0 unused), nv cells per axis, edge siz;
+  // cell_off = first global cell of the level in the CMM cell arrays (x fastest)
+  int cmm, nlev, idelay, cmm_upd;
+  int nv[6], cell_off[6];
+  double siz[6];
 };
 
 // class weight of a term (verlethe.f90:116-163): class 0 = AA, 1 = AB, 2 = BB
@@ -146,6 +151,15 @@ struct DevPtrs {
   double *lam;                    // ALSD lambda and its velocity [nrep][2]
   long long *ene_cls;             // class energies AA, AB, BB (fixed point) [nrep][4]
   double *com;                    // centre-of-mass stop sums [ncom][nrep][16]
+  // CMM: per atom its level-1 cell (0-based ix | iy << 8 | iz << 16) and far-field gradient;
+  // per cell (all levels, all replicas) population and 13 multipole coefficients; level-1
+  // raw sums; per replica the centroid sums and the far-field energy (last and being built)
+  int *cmm_cell;
+  double *gwk;
+  int *cmm_pop;
+  double *cmm_pot, *cmm_raw, *cmm_c0;
+  long long *cmm_e, *cmm_enew;
+  unsigned *masks_el, *tmp_masks_el;   // CMM tiles: pairs with the Coulomb term
   // accumulators
   long long *ene_fix;             // [nrep][16]
   long long *kin_fix;             // [nslots_kin][nsub_total]

@@ -14,16 +14,27 @@ __global__ void k_fill_slots(DevPtrs P, int natom);
 __global__ void k_excl_slots(DevPtrs P, int natom);
 __global__ void k_block_setup(DevPtrs P, int nblk, double qscale);
 __global__ void k_fill_pos_d(DevPtrs P, int nslot, double qscale);
-__global__ void k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rlimf);
-__global__ void k_tile_emit(DevPtrs P, int nchunk);
+// CMM: masks from the level-1 cells (neighbours: Coulomb + LJ into masks and masks_el;
+// cells up to idelay apart and r^2 < rc2: LJ only) instead of the list radius
+void launch_tile_scan(const DevPtrs& P, int nchunk, double rlim2, float rlimf, double rc2, bool cmm,
+                      cudaStream_t st);
+__global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm);
 void scan_exclusive(const int* in, int* out, int n, int* scratch, int* total, cudaStream_t st);
 
 // ZD pair constants
 struct ZdConst {
   double rc2, zcore, bcoeff, fcoeff;
-  double rlim;             // list radius rc + 1.5
+  double rlim;             // list radius rc + 1.5 (CMM: the farthest listed pair)
   int nt1;                 // LJ table stride (ntype + 1 incl. the dummy type)
+  int cmm;                 // CMM near field: no cut-off, Coulomb only where masks_el says
 };
+
+// cell multipole method (jp_cmm.cu): cells and multipoles at a list rebuild (before the tile
+// scan), and the far field of a step (every cmm_upd steps, or always with force)
+void launch_cmm_rebuild(const DevPtrs& P, int natom, int nrep, int ncell1, const int* ncell_lvl,
+                        int nlev_max, cudaStream_t st);
+void launch_cmm_far(const DevPtrs& P, int natom, int nrep, bool fp64, bool force, double ccoef,
+                    cudaStream_t st);
 
 // pair kernels (jp_pair.cu)
 void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool minimg, bool count,

@@ -59,10 +59,12 @@ __device__ __forceinline__ void flush_energy(const DevPtrs& P, int rep, double e
 // (3 shuffles) so that after 32 steps each is back in the lane of its atom.
 // ALSD: ci = cluster bit of the i atom; a pair with nA cluster atoms has its force times
 // f2 (nA = 2, class AA), f1 (AB) or 1 (BB), and its energy also goes to ea (AA) / eb (AB).
-template <bool MINIMG, bool COUNT, bool ALSD>
+// CMM: no cut-off (rc2 is huge) and the Coulomb term only for the pairs of `me` (the
+// neighbouring-cell pairs; the rest of the tile's pairs are LJ only)
+template <bool MINIMG, bool COUNT, bool ALSD, bool CMM>
 __device__ __forceinline__ void tile_mixed(const float4* __restrict__ sj_pos, const int* __restrict__ sj_typ,
                                            const float2* __restrict__ s_lj, int nt1, float4 pi, int ti,
-                                           float4 sh, unsigned m, int lane, float bx, float by, float bz,
+                                           float4 sh, unsigned m, unsigned me, int lane, float bx, float by, float bz,
                                            float ibx, float iby, float ibz, float rc2, float zb, float zf,
                                            float zc, float& fix, float& fiy, float& fiz, float& gjx,
                                            float& gjy, float& gjz, float& te, float& tl, int& tn,
@@ -87,7 +89,7 @@ __device__ __forceinline__ void tile_mixed(const float4* __restrict__ sj_pos, co
         const float r6inv = r2inv * r2inv * r2inv;
         const int tjr = sj_typ[jl];
         const float2 lj = s_lj[row + (ALSD ? (tjr & kTypeMask) : tjr)];
-        const float qq = pi.w * pj.w;
+        const float qq = CMM ? ((me & 1u) ? pi.w * pj.w : 0.f) : pi.w * pj.w;
         const float v1 = lj.x * r6inv;
         const float v2 = lj.y * r6inv * r6inv;
         float fs;
@@ -108,10 +110,11 @@ __device__ __forceinline__ void tile_mixed(const float4* __restrict__ sj_pos, co
         const float fx = dx * fs, fy = dy * fs, fz = dz * fs;
         fix -= fx; fiy -= fy; fiz -= fz;
         gjx += fx; gjy += fy; gjz += fz;
-        if (COUNT) ++tn;
+        if (COUNT && (!CMM || (me & 1u))) ++tn;
       }
     }
     m >>= 1;
+    if (CMM) me >>= 1;
     const int src = (lane + 1) & 31;
     gjx = __shfl_sync(0xffffffffu, gjx, src);
     gjy = __shfl_sync(0xffffffffu, gjy, src);
@@ -119,7 +122,7 @@ __device__ __forceinline__ void tile_mixed(const float4* __restrict__ sj_pos, co
   }
 }
 
-template <bool COUNT, bool ALSD>
+template <bool COUNT, bool ALSD, bool CMM>
 __global__ void __launch_bounds__(kPairThreads)
 k_pair_mixed(DevPtrs P, ZdConst z) {
   extern __shared__ float2 s_lj[];
@@ -187,6 +190,7 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     }
     const float4 sh = P.tile_shift[t];
     const unsigned m = P.masks[(size_t)t * 32 + lane];
+    const unsigned me = CMM ? P.masks_el[(size_t)t * 32 + lane] : 0u;
     const int sj = ij.y * kTile + lane;
     __syncwarp();
     sj_pos[lane] = P.pos_f[sj];
@@ -198,11 +202,11 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     int tn = 0;
     const int ci = ALSD ? (ti >> 30) : 0;
     if (mi)
-      tile_mixed<true, COUNT, ALSD>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, lane, bx, by, bz, ibx,
+      tile_mixed<true, COUNT, ALSD, CMM>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, me, lane, bx, by, bz, ibx,
                                     iby, ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn,
                                     ci, f1, f2, ea, eb);
     else
-      tile_mixed<false, COUNT, ALSD>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, lane, bx, by, bz, ibx,
+      tile_mixed<false, COUNT, ALSD, CMM>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, me, lane, bx, by, bz, ibx,
                                      iby, ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl,
                                      tn, ci, f1, f2, ea, eb);
     const int aj = P.satom[sj];
@@ -228,7 +232,7 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
   flush_energy(P, cur_rep, eel, elj, npair, COUNT);
 }
 
-template <bool COUNT, bool ALSD>
+template <bool COUNT, bool ALSD, bool CMM>
 __global__ void __launch_bounds__(kPairThreads)
 k_pair_fp64(DevPtrs P, ZdConst z) {
   extern __shared__ double2 s_ljd[];
@@ -284,6 +288,7 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
       }
     }
     unsigned m = P.masks[(size_t)t * 32 + lane];
+    unsigned me = CMM ? P.masks_el[(size_t)t * 32 + lane] : 0u;
     const int sj = ij.y * kTile + lane;
     double4 pj = P.pos_d[sj];
     int tj = P.styp[sj];
@@ -303,7 +308,7 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
         if (dd2i - irlim2 >= 0.0) {
           const double ddi = sqrt(dd2i);
           const double dd6i = dd2i * dd2i * dd2i;
-          const double ee = pi.w * pj.w;
+          const double ee = CMM ? ((me & 1u) ? pi.w * pj.w : 0.0) : pi.w * pj.w;
           const double epair = ee * (ddi + z.bcoeff * dd2 - z.zcore);
           eel += epair;
           const double2 lj = s_ljd[row + (ALSD ? (tj & kTypeMask) : tj)];
@@ -319,10 +324,11 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
           const double fx = dx * cc, fy = dy * cc, fz = dz * cc;
           gix -= fx; giy -= fy; giz -= fz;
           gjx += fx; gjy += fy; gjz += fz;
-          if (COUNT) ++tn;
+          if (COUNT && (!CMM || (me & 1u))) ++tn;
         }
       }
       m >>= 1;
+      if (CMM) me >>= 1;
       const int src = (lane + 1) & 31;
       pj.x = __shfl_sync(0xffffffffu, pj.x, src);
       pj.y = __shfl_sync(0xffffffffu, pj.y, src);
@@ -353,10 +359,10 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
 int pair_blocks_per_sm(bool fp64, int nt1) {
   int per = 0;
   if (fp64)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_fp64<false, false>, kPairThreads,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_fp64<false, false, false>, kPairThreads,
                                                   sizeof(double2) * nt1 * nt1);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_mixed<false, false>, kPairThreads,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_mixed<false, false, false>, kPairThreads,
                                                   sizeof(float2) * nt1 * nt1);
   return per > 0 ? per : 1;
 }
@@ -366,12 +372,15 @@ void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool, boo
   const int wpb = kPairThreads / 32;
   const int nb = (nwarps + wpb - 1) / wpb;
   const size_t sh = sizeof(float2) * z.nt1 * z.nt1;
-  if (alsd) {
-    if (count) k_pair_mixed<true, true><<<nb, kPairThreads, sh, st>>>(P, z);
-    else k_pair_mixed<false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+  if (z.cmm) {
+    if (count) k_pair_mixed<true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_mixed<false, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+  } else if (alsd) {
+    if (count) k_pair_mixed<true, true, false><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_mixed<false, true, false><<<nb, kPairThreads, sh, st>>>(P, z);
   } else {
-    if (count) k_pair_mixed<true, false><<<nb, kPairThreads, sh, st>>>(P, z);
-    else k_pair_mixed<false, false><<<nb, kPairThreads, sh, st>>>(P, z);
+    if (count) k_pair_mixed<true, false, false><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_mixed<false, false, false><<<nb, kPairThreads, sh, st>>>(P, z);
   }
 }
 
@@ -380,12 +389,15 @@ void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count
   const int wpb = kPairThreads / 32;
   const int nb = (nwarps + wpb - 1) / wpb;
   const size_t sh = sizeof(double2) * z.nt1 * z.nt1;
-  if (alsd) {
-    if (count) k_pair_fp64<true, true><<<nb, kPairThreads, sh, st>>>(P, z);
-    else k_pair_fp64<false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+  if (z.cmm) {
+    if (count) k_pair_fp64<true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_fp64<false, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+  } else if (alsd) {
+    if (count) k_pair_fp64<true, true, false><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_fp64<false, true, false><<<nb, kPairThreads, sh, st>>>(P, z);
   } else {
-    if (count) k_pair_fp64<true, false><<<nb, kPairThreads, sh, st>>>(P, z);
-    else k_pair_fp64<false, false><<<nb, kPairThreads, sh, st>>>(P, z);
+    if (count) k_pair_fp64<true, false, false><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_fp64<false, false, false><<<nb, kPairThreads, sh, st>>>(P, z);
   }
 }
 

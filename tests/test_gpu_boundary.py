@@ -75,7 +75,8 @@ def test_leaving_the_window_is_reported(eng_mod, drop):
         assert ex.value.code == abi.JP_E_FREE_WINDOW
 
 
-def test_cmm_is_rejected(eng_mod, drop):
+def test_cmm_needs_the_free_boundary(eng_mod, drop):
     with pytest.raises(eng_mod.JpError) as ex:
-        eng_mod.Engine(drop, precision=MIXED, cal15m=abi.JP_CAL15M_CMM, bounda=NONE)
+        eng_mod.Engine(dict(drop, box=np.full(3, 80.0)), precision=MIXED, cal15m=abi.JP_CAL15M_CMM,
+                       bounda=PBC)
     assert ex.value.code == abi.JP_E_INVALID
