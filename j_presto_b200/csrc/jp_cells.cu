@@ -25,7 +25,7 @@ namespace jp {
 __global__ void k_cell_key(DevPtrs P, int natom) {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= natom) return;
-  const Rep R = P.reps[P.rep_of[a]];
+  const Rep& R = P.reps[P.rep_of[a]];
   int c[3];
   bool out = false;
   for (int k = 0; k < 3; ++k) {
@@ -106,7 +106,7 @@ __global__ void k_block_setup(DevPtrs P, int nblk, double qscale) {
   if (warp >= nblk) return;
   const int slot = warp * kTile + lane;
   const int a = P.satom[slot];
-  const Rep R = P.reps[P.blk_rep[warp]];
+  const Rep& R = P.reps[P.blk_rep[warp]];
   double w[3] = {0, 0, 0}, img[3] = {0, 0, 0};
   double lo[3], hi[3];
   for (int k = 0; k < 3; ++k) {
@@ -199,6 +199,9 @@ __device__ __forceinline__ unsigned tile_mask(const DevPtrs& P, const Rep& R, in
   }
   unsigned mask = 0;
   mel = 0;
+  const double bx = R.box[0], by = R.box[1], bz = R.box[2];
+  const double ibx = R.invbox[0], iby = R.invbox[1], ibz = R.invbox[2];
+  const int idelay = R.idelay;
   for (int k = 0; k < 32; ++k) {
     const int src = (lane + k) & 31;
     const double xk = __shfl_sync(0xffffffffu, xj, src);
@@ -209,9 +212,9 @@ __device__ __forceinline__ unsigned tile_mask(const DevPtrs& P, const Rep& R, in
     if (ai < 0 || ak < 0) continue;
     if (bj == bi && (k == 0 || k > 16 || (k == 16 && lane >= 16))) continue;
     double dx = xi - xk, dy = yi - yk, dz = zi - zk;
-    dx -= R.box[0] * anint(dx * R.invbox[0]);
-    dy -= R.box[1] * anint(dy * R.invbox[1]);
-    dz -= R.box[2] * anint(dz * R.invbox[2]);
+    dx -= bx * anint(dx * ibx);
+    dy -= by * anint(dy * iby);
+    dz -= bz * anint(dz * ibz);
     const double d2 = dx * dx + dy * dy + dz * dz;
     if (CMM) {
       if (ci < 0 || ck < 0) continue;
@@ -220,7 +223,7 @@ __device__ __forceinline__ unsigned tile_mask(const DevPtrs& P, const Rep& R, in
       if (cheb <= 1) {
         mask |= 1u << k;
         mel |= 1u << k;
-      } else if (R.idelay > 1 && cheb <= R.idelay && d2 < rc2) {
+      } else if (idelay > 1 && cheb <= idelay && d2 < rc2) {
         mask |= 1u << k;
       }
     } else if (d2 <= rlim2) {
@@ -242,13 +245,68 @@ __device__ __forceinline__ unsigned tile_mask(const DevPtrs& P, const Rep& R, in
   return mask;
 }
 
+// Fast form of the mask (no CMM, large box): lane = j atom; the i block is read from shared
+// memory one atom per step (a broadcast) and a ballot gives that i atom's row of the tile at
+// once; lane i keeps row i and rotates it into the kernels' layout (bit k = j (i + k) & 31).
+// Coordinates are wrapped (x - box floor(x / box)) and the tile's image is the block
+// references' minimum image n, exact for every pair the list can hold when box/2 > list
+// radius + block extents (the condition of the pair kernels' per-tile shift).
+struct IStage {
+  double x[kTile], y[kTile], z[kTile];
+};
+
+__device__ __forceinline__ unsigned tile_mask_fast(const DevPtrs& P, const Rep& R, int bi, int bj, int lane,
+                                                   int ai, const IStage& S, const int (&ps)[kExclReg],
+                                                   int pb, int pe, double rlim2) {
+  const int aj = P.satom[bj * kTile + lane];
+  double xj = 0.0, yj = 0.0, zj = 0.0;
+  if (aj >= 0) {
+    double w[3];
+    for (int k = 0; k < 3; ++k) {
+      const double x = P.x[3 * aj + k];
+      const double n = anint((P.blk_ref[3 * bi + k] - P.blk_ref[3 * bj + k]) * R.invbox[k]);
+      w[k] = (x - R.box[k] * floor(x * R.invbox[k])) + R.box[k] * n;
+    }
+    xj = w[0]; yj = w[1]; zj = w[2];
+  }
+  unsigned row = 0;
+#pragma unroll 8
+  for (int i = 0; i < kTile; ++i) {
+    const double dx = S.x[i] - xj, dy = S.y[i] - yj, dz = S.z[i] - zj;
+    const bool in = aj >= 0 && dx * dx + dy * dy + dz * dz <= rlim2;
+    const unsigned b = __ballot_sync(0xffffffffu, in);
+    if (lane == i) row = b;
+  }
+  if (ai < 0) row = 0;
+  unsigned mask = __funnelshift_r(row, row, lane);
+  if (bj == bi) mask &= lane < 16 ? 0x1fffeu : 0xfffeu;   // each unordered pair once, no self pair
+  if (mask) {
+#pragma unroll
+    for (int q = 0; q < kExclReg; ++q)
+      if ((ps[q] >> 5) == bj) mask &= ~(1u << (((ps[q] & 31) - lane) & 31));
+    for (int p = pb + kExclReg; p < pe; ++p) {
+      const int sp = P.excl_slot[p];
+      if ((sp >> 5) == bj) mask &= ~(1u << (((sp & 31) - lane) & 31));
+    }
+  }
+  return mask;
+}
+
 template <bool CMM>
-__global__ void k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rlimf, double rc2) {
+__global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rlimf,
+                                                          double rc2) {
+  __shared__ IStage s_i[4];
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= nchunk) return;
   const int bi = P.chunk_i[w], j0 = P.chunk_j0[w];
-  const Rep R = P.reps[P.blk_rep[bi]];
+  const int rep = P.blk_rep[bi];
+  const Rep& R = P.reps[rep];
+  // exact when a pair within the list radius cannot be another image than the blocks':
+  // box/2 > list radius + the two blocks' half extents (largest of the replica)
+  bool fast = !CMM;
+  for (int k = 0; k < 3; ++k)
+    if (!(0.5 * R.box[k] > sqrt(rlim2) + 2.0 * (double)P.rep_hmax[3 * rep + k] + 0.01)) fast = false;
   const int bend = R.blk0 + R.nblk;
   const float4 ci = P.blk_ctr[bi], hi = P.blk_half[bi];
   const int bj = j0 + lane;
@@ -279,12 +337,20 @@ __global__ void k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rl
     }
 #pragma unroll
     for (int q = 0; q < kExclReg; ++q) ps[q] = pb + q < pe ? P.excl_slot[pb + q] : -64;
+    IStage& S = s_i[threadIdx.x >> 5];
+    if (fast) {   // the i block, wrapped, for the broadcast reads
+      S.x[lane] = xi - R.box[0] * floor(xi * R.invbox[0]);
+      S.y[lane] = yi - R.box[1] * floor(yi * R.invbox[1]);
+      S.z[lane] = zi - R.box[2] * floor(zi * R.invbox[2]);
+      __syncwarp();
+    }
     while (ball) {
       const int b = __ffs(ball) - 1;
       ball &= ball - 1;
-      unsigned mel;
-      const unsigned m = tile_mask<CMM>(P, R, bi, j0 + b, lane, ai, xi, yi, zi, ps, pb, pe, rlim2,
-                                        ci, rc2, mel);
+      unsigned mel = 0;
+      const unsigned m = fast ? tile_mask_fast(P, R, bi, j0 + b, lane, ai, S, ps, pb, pe, rlim2)
+                              : tile_mask<CMM>(P, R, bi, j0 + b, lane, ai, xi, yi, zi, ps, pb, pe, rlim2,
+                                               ci, rc2, mel);
       if (__any_sync(0xffffffffu, m != 0)) {
         P.tmp_masks[((size_t)w * 32 + b) * 32 + lane] = m;
         if (CMM) P.tmp_masks_el[((size_t)w * 32 + b) * 32 + lane] = mel;
