@@ -166,7 +166,7 @@ void enqueue_zero(jp_ctx *c, bool count) {
   cudaStream_t st = c->st;
   if (c->fp64) cudaMemsetAsync(P.grd, 0, sizeof(double) * 3 * c->natom, st);
   else cudaMemsetAsync(P.frc, 0, sizeof(long long) * 3 * c->natom, st);
-  cudaMemsetAsync(P.ene_fix, 0, sizeof(long long) * 16 * c->nrep, st);
+  cudaMemsetAsync(P.ene_fix, 0, sizeof(long long) * (16 * c->nrep + 1), st);   // + tile counter
   if (c->alsd) cudaMemsetAsync(P.ene_cls, 0, sizeof(long long) * 4 * c->nrep, st);
   if (count) cudaMemsetAsync(P.pair_cnt, 0, sizeof(long long) * c->nrep, st);
 }
@@ -884,7 +884,8 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dput(c, &P.lam, hlam);
   e |= dalloc(c, &P.ene_cls, (size_t)nrep * 4);
   e |= dalloc(c, &P.com, (size_t)std::max(1, prm->icslop) * nrep * 16);
-  e |= dalloc(c, &P.ene_fix, 16 * (size_t)nrep);
+  e |= dalloc(c, &P.ene_fix, 16 * (size_t)nrep + 1);
+  if (!e) P.tile_ctr = reinterpret_cast<int *>(P.ene_fix + 16 * (size_t)nrep);
   e |= dalloc(c, &P.kin_fix, (size_t)c->nkin * c->nsub);
   e |= dput(c, &P.nfr, hnfr);
   e |= dalloc(c, &P.scale, (size_t)nrep);

@@ -161,7 +161,8 @@ struct DevPtrs {
   long long *cmm_e, *cmm_enew;
   unsigned *masks_el, *tmp_masks_el;   // CMM tiles: pairs with the Coulomb term
   // accumulators
-  long long *ene_fix;             // [nrep][16]
+  long long *ene_fix;             // [nrep][16], then the pair kernels' tile counter
+  int *tile_ctr;                  // next unclaimed tile (zeroed with ene_fix every step)
   long long *kin_fix;             // [nslots_kin][nsub_total]
   double *nfr;                    // DOF per sub-system
   double *scale;                  // per replica force scale (GE / pseudo-T)

@@ -23,6 +23,7 @@
 namespace jp {
 
 constexpr int kPairThreads = 256;
+constexpr int kPairClaim = 4;   // tiles a warp claims at a time (mixed path)
 
 // ALSD class energies of a replica: AA and AB accumulated, BB the rest of the pair energy
 __device__ __forceinline__ void flush_cls(const DevPtrs& P, int rep, double eaa, double eab,
@@ -36,6 +37,33 @@ __device__ __forceinline__ void flush_cls(const DevPtrs& P, int rep, double eaa,
     atomic_add_ll(&P.ene_cls[rep * 4 + 0], to_fix(eaa, kEneScale));
     atomic_add_ll(&P.ene_cls[rep * 4 + 1], to_fix(eab, kEneScale));
     atomic_add_ll(&P.ene_cls[rep * 4 + 2], to_fix(etot - eaa - eab, kEneScale));
+  }
+}
+
+// the same with 64-bit fixed-point sums (order independent: the mixed kernel's warps take
+// their tiles dynamically, so a warp's set of tiles changes from run to run)
+__device__ __forceinline__ void flush_fix(const DevPtrs& P, int rep, long long eel, long long elj,
+                                          long long eaa, long long eab, long long npair, bool count,
+                                          bool alsd) {
+  for (int o = 16; o > 0; o >>= 1) {
+    eel += __shfl_xor_sync(0xffffffffu, eel, o);
+    elj += __shfl_xor_sync(0xffffffffu, elj, o);
+    if (alsd) {
+      eaa += __shfl_xor_sync(0xffffffffu, eaa, o);
+      eab += __shfl_xor_sync(0xffffffffu, eab, o);
+    }
+    if (count) npair += __shfl_xor_sync(0xffffffffu, npair, o);
+  }
+  if ((threadIdx.x & 31) == 0 && rep >= 0) {
+    atomic_add_ll(&P.ene_fix[rep * 16 + JP_E_ELE15], eel);
+    atomic_add_ll(&P.ene_fix[rep * 16 + JP_E_VDW15], elj);
+    if (alsd) {
+      atomic_add_ll(&P.ene_cls[rep * 4 + 0], eaa);
+      atomic_add_ll(&P.ene_cls[rep * 4 + 1], eab);
+      atomic_add_ll(&P.ene_cls[rep * 4 + 2], eel + elj - eaa - eab);
+    }
+    if (count) atomicAdd(reinterpret_cast<unsigned long long*>(&P.pair_cnt[rep]),
+                         static_cast<unsigned long long>(npair));
   }
 }
 
@@ -134,22 +162,24 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
   const int lane = threadIdx.x & 31;
   float4* sj_pos = s_jpos + (threadIdx.x & ~31);
   int* sj_typ = s_jtyp + (threadIdx.x & ~31);
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
   const int T = *P.ntiles;
-  const int chunk = (T + nw - 1) / nw;
-  const int t0 = gw * chunk;
-  const int t1 = min(T, t0 + chunk);
-  if (t0 >= t1) return;
   const float rc2 = (float)z.rc2, zb = (float)z.bcoeff, zf = (float)z.fcoeff, zc = (float)z.zcore;
   int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
   float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
   long long gix = 0, giy = 0, giz = 0;
-  double eel = 0.0, elj = 0.0, eaa = 0.0, eab = 0.0;
+  long long eel = 0, elj = 0, eaa = 0, eab = 0;   // fixed point, per tile
   long long npair = 0;
   bool mi = true;
   float bx = 0.f, by = 0.f, bz = 0.f, ibx = 0.f, iby = 0.f, ibz = 0.f;
   float f1 = 1.f, f2 = 1.f;
+  // tiles are claimed kPairClaim at a time from a global counter (row order: consecutive
+  // tiles mostly share their i block), so warps finish together whatever their tiles hold
+  for (;;) {
+  int t0 = 0;
+  if (lane == 0) t0 = atomicAdd(P.tile_ctr, kPairClaim);
+  t0 = __shfl_sync(0xffffffffu, t0, 0);
+  if (t0 >= T) break;
+  const int t1 = min(T, t0 + kPairClaim);
   for (int t = t0; t < t1; ++t) {
     const int2 ij = P.tiles[t];
     if (ij.x != cur_bi) {
@@ -167,10 +197,9 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
       const int rep = P.blk_rep[cur_bi];
       if (rep != cur_rep) {
         if (cur_rep >= 0) {
-          if (ALSD) flush_cls(P, cur_rep, eaa, eab, eel + elj);
-          flush_energy(P, cur_rep, eel, elj, npair, COUNT);
+          flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
         }
-        eel = elj = eaa = eab = 0.0;
+        eel = elj = eaa = eab = 0;
         npair = 0;
         cur_rep = rep;
         const Rep& R = P.reps[rep];
@@ -218,18 +247,18 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     gix += to_fix((double)fix, kFrcScale);
     giy += to_fix((double)fiy, kFrcScale);
     giz += to_fix((double)fiz, kFrcScale);
-    eel += (double)te;
-    elj += (double)tl;
-    if (ALSD) { eaa += (double)ea; eab += (double)eb; }
+    eel += to_fix((double)te, kEneScale);
+    elj += to_fix((double)tl, kEneScale);
+    if (ALSD) { eaa += to_fix((double)ea, kEneScale); eab += to_fix((double)eb, kEneScale); }
     if (COUNT) npair += tn;
+  }
   }
   if (ai >= 0 && (gix | giy | giz)) {
     atomic_add_ll(&P.frc[3 * ai + 0], gix);
     atomic_add_ll(&P.frc[3 * ai + 1], giy);
     atomic_add_ll(&P.frc[3 * ai + 2], giz);
   }
-  if (ALSD) flush_cls(P, cur_rep, eaa, eab, eel + elj);
-  flush_energy(P, cur_rep, eel, elj, npair, COUNT);
+  flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
 }
 
 template <bool COUNT, bool ALSD, bool CMM>
