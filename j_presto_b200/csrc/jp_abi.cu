@@ -190,8 +190,6 @@ void enqueue_bonded(jp_ctx *c) {
 
 void enqueue_integrate(jp_ctx *c) {
   DevPtrs &P = c->P;
-  cudaMemsetAsync(P.kin_fix, 0, sizeof(long long) * c->nkin * c->nsub, c->st);
-  if (c->ic.stop) cudaMemsetAsync(P.com, 0, sizeof(double) * c->ic.ncom * c->ic.nrep * 16, c->st);
   if (c->ic.ge_prescaled) launch_ge_scale(P, c->ic, c->st);
   launch_integrate(P, c->ic, c->nunit, c->fp64, c->cano_grid, c->st);
 }
@@ -232,6 +230,10 @@ int check_status(jp_ctx *c) {
   CK(cudaMemcpy(&s, c->P.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
   if (s == 0) return JP_OK;
   CK(cudaMemset(c->P.status, 0, sizeof(unsigned)));
+  // an integration that stopped early left its barrier and sums: clear them for the next
+  CK(cudaMemset(c->P.bar, 0, sizeof(unsigned) * 4));
+  CK(cudaMemset(c->P.kin_fix, 0, sizeof(long long) * c->nkin * c->nsub));
+  if (c->ic.stop) CK(cudaMemset(c->P.com, 0, sizeof(double) * c->ic.ncom * c->ic.nrep * 16));
   if (s & ERR_TIMEOUT) return JP_E_TIMEOUT;
   if (s & ERR_LIST_OVERFLOW) return JP_E_LIST_OVERFLOW;
   if (s & ERR_NONFINITE) return JP_E_NONFINITE;

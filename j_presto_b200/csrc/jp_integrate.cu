@@ -15,6 +15,8 @@
 
 namespace jp {
 
+constexpr int kCom = 16;   // centre-of-mass stop sums per replica and slot
+
 // Loop over the 1-4 atoms of an integration unit.  The trip count is fixed at 4 and fully
 // unrolled with a guard: the per-unit arrays then live in registers.  (A runtime trip count
 // over these small local arrays produced wrong values on sm_100a with nvcc 12.9.)
@@ -548,9 +550,19 @@ __device__ void finish_block(const DevPtrs& P, const IntConst& c, double tt) {
         (c.method <= JP_METHOD_MICR || c.shake_method != JP_SHAKE_NONE) ? ek * 1.0e7 / (kGas * nf) : -1.0;
   }
   __syncthreads();
+  // the next step starts from zero kinetic (and centre-of-mass) sums and a fresh barrier:
+  // every other block has left its last barrier and read its last sum
+  const int nk = c.nkin * c.nsub_total;
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) P.kin_fix[i] = 0;
+  if (c.stop)
+    for (int i = threadIdx.x; i < c.ncom * c.nrep * kCom; i += blockDim.x) P.com[i] = 0.0;
   if (threadIdx.x == 0) {
     P.step_ctr[0] += 1;
     P.step_ctr[1] += 1;
+    P.bar[0] = 0u;
+    P.bar[1] = 0u;
+    P.bar[2] = 0u;
+    P.bar[3] = 0u;
   }
 }
 
@@ -584,8 +596,6 @@ __device__ void finish_last(const DevPtrs& P, const IntConst& c, double tt) {
 // Centre, inertia tensor about the centre (parallel-axis shift) and angular momentum about
 // the centre follow from them, so the correction v -= tv + w x (x0 - centre) needs one grid
 // barrier.  The sums are FP64 atomics (their order, hence the last bits, varies run to run).
-constexpr int kCom = 16;
-
 __device__ __forceinline__ bool stopped(const Rep& R, int a) { return a - R.atom0 < R.stop_n; }
 
 __device__ __forceinline__ void com_terms(double m, const double* x0, const double* v, double* w) {
@@ -2066,7 +2076,8 @@ static void coop_launch(void (*kernel)(Args...), int grid, cudaStream_t st, Args
 
 void launch_integrate(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
                       cudaStream_t st) {
-  cudaMemsetAsync(P.bar, 0, sizeof(unsigned) * 4, st);
+  // bar, the kinetic sums and the centre-of-mass sums are zero here: created so, and reset
+  // by the last block of the previous integration (or by the host after an error)
   const bool verlet = c.method <= JP_METHOD_MICR;   // MICR or CONS
   const int lanes = verlet ? nunit : c.nvirt;
   const int want = std::max(1, (lanes + kIntThreads - 1) / kIntThreads);

@@ -23,7 +23,7 @@
 namespace jp {
 
 constexpr int kPairThreads = 256;
-constexpr int kPairClaim = 4;   // tiles a warp claims at a time (mixed path)
+constexpr int kPairClaim = 1;   // tiles a warp claims at a time (mixed path)
 
 // ALSD class energies of a replica: AA and AB accumulated, BB the rest of the pair energy
 __device__ __forceinline__ void flush_cls(const DevPtrs& P, int rep, double eaa, double eab,
