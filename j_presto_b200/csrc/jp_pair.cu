@@ -14,34 +14,22 @@
 // steps every lane has seen every j and each j-force is back in the lane that loaded it.
 // Newton's third law: each unordered pair is evaluated once.
 //
-// Mixed path: FP32 pair arithmetic on block-local coordinates (|x| < ~10 A), forces summed
-// per tile in FP32 then added as 64-bit fixed point (2^-32 kcal/mol/A) with integer
-// atomics -- order independent, so results are bit-identical run to run.
-// FP64 path: the same tiles in FP64 with absolute coordinates and FP64 atomics.
+// Warps take tiles one at a time from a global counter, so all finish together whatever
+// their tiles hold (tile work varies with the mask).
+// Mixed path: FP32 pair arithmetic on block-local coordinates (|x| < ~10 A), forces and
+// energies summed per tile in FP32 then added as 64-bit fixed point (2^-32 kcal/mol/A) with
+// integer atomics -- order independent, so results are bit-identical run to run.
+// FP64 path: the same tiles in FP64 with absolute coordinates and FP64 force atomics.
 #include "jp_kernels.h"
 
 namespace jp {
 
 constexpr int kPairThreads = 256;
-constexpr int kPairClaim = 1;   // tiles a warp claims at a time (mixed path)
+constexpr int kPairClaim = 1;   // tiles a warp claims at a time
 
-// ALSD class energies of a replica: AA and AB accumulated, BB the rest of the pair energy
-__device__ __forceinline__ void flush_cls(const DevPtrs& P, int rep, double eaa, double eab,
-                                          double etot) {
-  for (int o = 16; o > 0; o >>= 1) {
-    eaa += __shfl_xor_sync(0xffffffffu, eaa, o);
-    eab += __shfl_xor_sync(0xffffffffu, eab, o);
-    etot += __shfl_xor_sync(0xffffffffu, etot, o);
-  }
-  if ((threadIdx.x & 31) == 0 && rep >= 0) {
-    atomic_add_ll(&P.ene_cls[rep * 4 + 0], to_fix(eaa, kEneScale));
-    atomic_add_ll(&P.ene_cls[rep * 4 + 1], to_fix(eab, kEneScale));
-    atomic_add_ll(&P.ene_cls[rep * 4 + 2], to_fix(etot - eaa - eab, kEneScale));
-  }
-}
-
-// the same with 64-bit fixed-point sums (order independent: the mixed kernel's warps take
-// their tiles dynamically, so a warp's set of tiles changes from run to run)
+// a warp's energies (ELE15, VDW15; ALSD class AA / AB, BB the rest) and pair count into the
+// replica's slots: 64-bit fixed point, summed per tile, so the totals do not depend on which
+// warp took which tile (the kernels claim their tiles dynamically)
 __device__ __forceinline__ void flush_fix(const DevPtrs& P, int rep, long long eel, long long elj,
                                           long long eaa, long long eab, long long npair, bool count,
                                           bool alsd) {
@@ -62,21 +50,6 @@ __device__ __forceinline__ void flush_fix(const DevPtrs& P, int rep, long long e
       atomic_add_ll(&P.ene_cls[rep * 4 + 1], eab);
       atomic_add_ll(&P.ene_cls[rep * 4 + 2], eel + elj - eaa - eab);
     }
-    if (count) atomicAdd(reinterpret_cast<unsigned long long*>(&P.pair_cnt[rep]),
-                         static_cast<unsigned long long>(npair));
-  }
-}
-
-__device__ __forceinline__ void flush_energy(const DevPtrs& P, int rep, double eel, double elj,
-                                             long long npair, bool count) {
-  for (int o = 16; o > 0; o >>= 1) {
-    eel += __shfl_xor_sync(0xffffffffu, eel, o);
-    elj += __shfl_xor_sync(0xffffffffu, elj, o);
-    if (count) npair += __shfl_xor_sync(0xffffffffu, npair, o);
-  }
-  if ((threadIdx.x & 31) == 0 && rep >= 0) {
-    atomic_add_ll(&P.ene_fix[rep * 16 + JP_E_ELE15], to_fix(eel, kEneScale));
-    atomic_add_ll(&P.ene_fix[rep * 16 + JP_E_VDW15], to_fix(elj, kEneScale));
     if (count) atomicAdd(reinterpret_cast<unsigned long long*>(&P.pair_cnt[rep]),
                          static_cast<unsigned long long>(npair));
   }
@@ -269,22 +242,22 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
   for (int i = threadIdx.x; i < nlj; i += blockDim.x) s_ljd[i] = P.lj_d[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
   const int T = *P.ntiles;
-  const int chunk = (T + nw - 1) / nw;
-  const int t0 = gw * chunk;
-  const int t1 = min(T, t0 + chunk);
-  if (t0 >= t1) return;
   const double irlim2 = 1.0 / z.rc2;
   int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
   double4 pi = make_double4(0, 0, 0, 0);
   double gix = 0, giy = 0, giz = 0;
-  double eel = 0.0, elj = 0.0, eaa = 0.0, eab = 0.0;
+  long long eel = 0, elj = 0, eaa = 0, eab = 0;   // fixed point, per tile
   long long npair = 0;
   double bx = 0, by = 0, bz = 0, ibx = 0, iby = 0, ibz = 0;
   double f1 = 1.0, f2 = 1.0;
-  for (int t = t0; t < t1; ++t) {
+  // tiles claimed one at a time, as in the mixed kernel
+  for (;;) {
+  int t = 0;
+  if (lane == 0) t = atomicAdd(P.tile_ctr, 1);
+  t = __shfl_sync(0xffffffffu, t, 0);
+  if (t >= T) break;
+  {
     const int2 ij = P.tiles[t];
     if (ij.x != cur_bi) {
       if (ai >= 0) {
@@ -301,10 +274,9 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
       const int rep = P.blk_rep[cur_bi];
       if (rep != cur_rep) {
         if (cur_rep >= 0) {
-          if (ALSD) flush_cls(P, cur_rep, eaa, eab, eel + elj);
-          flush_energy(P, cur_rep, eel, elj, npair, COUNT);
+          flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
         }
-        eel = elj = eaa = eab = 0.0;
+        eel = elj = eaa = eab = 0;
         npair = 0;
         cur_rep = rep;
         const Rep& R = P.reps[rep];
@@ -325,6 +297,7 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
     const int ci = ALSD ? (ti >> 30) : 0;
     double gjx = 0, gjy = 0, gjz = 0;
     int tn = 0;
+    double te = 0.0, tl = 0.0, ta = 0.0, tb = 0.0;   // this tile's energies
 #pragma unroll 2
     for (int k = 0; k < 32; ++k) {
       if (m & 1u) {
@@ -339,16 +312,16 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
           const double dd6i = dd2i * dd2i * dd2i;
           const double ee = CMM ? ((me & 1u) ? pi.w * pj.w : 0.0) : pi.w * pj.w;
           const double epair = ee * (ddi + z.bcoeff * dd2 - z.zcore);
-          eel += epair;
+          te += epair;
           const double2 lj = s_ljd[row + (ALSD ? (tj & kTypeMask) : tj)];
           const double v1 = lj.x * dd6i;
           const double v2 = lj.y * dd6i * dd6i;
-          elj += -v1 + v2;
+          tl += -v1 + v2;
           double cc = ee * (dd2i * ddi - z.fcoeff) + (-6.0 * v1 + 12.0 * v2) * dd2i;
           if (ALSD) {
             const int na = ci + (tj >> 30);
-            if (na == 2) { eaa += epair + (-v1 + v2); cc *= f2; }
-            else if (na == 1) { eab += epair + (-v1 + v2); cc *= f1; }
+            if (na == 2) { ta += epair + (-v1 + v2); cc *= f2; }
+            else if (na == 1) { tb += epair + (-v1 + v2); cc *= f1; }
           }
           const double fx = dx * cc, fy = dy * cc, fz = dz * cc;
           gix -= fx; giy -= fy; giz -= fz;
@@ -375,14 +348,17 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
       atomicAdd(&P.grd[3 * aj + 2], gjz);
     }
     if (COUNT) npair += tn;
+    eel += to_fix(te, kEneScale);
+    elj += to_fix(tl, kEneScale);
+    if (ALSD) { eaa += to_fix(ta, kEneScale); eab += to_fix(tb, kEneScale); }
+  }
   }
   if (ai >= 0) {
     atomicAdd(&P.grd[3 * ai + 0], gix);
     atomicAdd(&P.grd[3 * ai + 1], giy);
     atomicAdd(&P.grd[3 * ai + 2], giz);
   }
-  if (ALSD) flush_cls(P, cur_rep, eaa, eab, eel + elj);
-  flush_energy(P, cur_rep, eel, elj, npair, COUNT);
+  flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
 }
 
 int pair_blocks_per_sm(bool fp64, int nt1) {
