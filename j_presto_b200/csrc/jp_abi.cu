@@ -60,6 +60,8 @@ struct jp_ctx {
   int hist_cap = 1024;
   long long idloop = 0;
   cudaStream_t st = nullptr;
+  cudaStream_t st2 = nullptr;       // the bonded kernel's branch of the step graph
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaGraphExec_t g_step = nullptr, g_rebuild = nullptr;
   int *scan_scratch = nullptr;
   std::vector<void *> allocs;
@@ -215,8 +217,16 @@ int capture(jp_ctx *c, cudaGraphExec_t *out, bool rebuild) {
   if (rebuild) {
     enqueue_rebuild(c);
   } else {
-    enqueue_forces(c, false);
-    enqueue_bonded(c);
+    // the bonded terms run beside the pair tiles (both only add into the force and energy
+    // accumulators, as order-independent integer sums on the mixed path), joined before the
+    // integration
+    enqueue_zero(c, false);
+    CK(cudaEventRecord(c->ev_fork, c->st));
+    CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
+    launch_bonded(c->P, c->nterm, c->fp64, c->zc.bcoeff, c->zc.fcoeff, c->alsd, c->st2);
+    CK(cudaEventRecord(c->ev_join, c->st2));
+    enqueue_pair(c, false);
+    CK(cudaStreamWaitEvent(c->st, c->ev_join, 0));
     enqueue_integrate(c);
   }
   CK(cudaStreamEndCapture(c->st, &g));
@@ -955,6 +965,9 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   c->pair_warps = std::max(1, nsm) * (256 / 32) * pair_blocks_per_sm(c->fp64, c->zc.nt1);
   c->cano_grid = cano_grid(c->fp64, c->device);
   CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
   CK(cudaEventCreate(&c->ev_a));
   CK(cudaEventCreate(&c->ev_b));
   enqueue_rebuild(c);
@@ -976,6 +989,9 @@ void jp_destroy(jp_ctx *c) {
   if (c->ev_a) cudaEventDestroy(c->ev_a);
   if (c->ev_b) cudaEventDestroy(c->ev_b);
   if (c->st) cudaStreamDestroy(c->st);
+  if (c->st2) cudaStreamDestroy(c->st2);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   delete c;
 }
 

@@ -568,11 +568,25 @@ __device__ void finish_block(const DevPtrs& P, const IntConst& c, double tt) {
 
 // is any replica still iterating the SHAKE <-> thermostat loop at pass `it`?  The same answer
 // in every block: all read the kinetic sums completed before the last grid barrier.
-__device__ bool any_active(const DevPtrs& P, const IntConst& c, int it, double tt) {
+// The block also keeps each replica's answer in s_act (replicas below kActCache), so the
+// lanes of the pass read a shared flag instead of re-reading the kinetic sums.
+constexpr int kActCache = 1024;
+
+__device__ bool any_active(const DevPtrs& P, const IntConst& c, int it, double tt,
+                           unsigned char* s_act) {
   int act = 0;
-  for (int r = threadIdx.x; r < c.nrep; r += blockDim.x)
-    act |= cano_active(P, c, P.reps[r], it, true, tt) ? 1 : 0;
-  return __syncthreads_or(act) != 0;
+  for (int r = threadIdx.x; r < c.nrep; r += blockDim.x) {
+    const bool a = cano_active(P, c, P.reps[r], it, true, tt);
+    if (r < kActCache) s_act[r] = a ? 1 : 0;
+    act |= a ? 1 : 0;
+  }
+  return __syncthreads_or(act) != 0;   // also publishes s_act to the block
+}
+
+// is replica r still iterating at pass `it` (after any_active filled s_act)?
+__device__ __forceinline__ bool rep_active(const DevPtrs& P, const IntConst& c, const unsigned char* s_act,
+                                           int r, int it, double tt) {
+  return r < kActCache ? s_act[r] != 0 : cano_active(P, c, P.reps[r], it, true, tt);
 }
 
 // the last block to finish the step computes the temperatures and advances the step counters
@@ -1236,6 +1250,18 @@ __device__ __forceinline__ QLane ql_make(const DevPtrs& P, const IntConst& c, in
   return q;
 }
 
+// 1/a by Newton's iteration for the reciprocal, y <- y + y (1 - a y), from the hardware's
+// approximate reciprocal: each step squares the relative error, two give full double
+// precision (within an ulp of the rounded quotient) for the normal, well-scaled pivots of
+// the 4-atom SHAKE solve, at a fraction of an IEEE division's latency
+__device__ __forceinline__ double recip_nr(double a) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+  y = fma(y, fma(-a, y, 1.0), y);
+  y = fma(y, fma(-a, y, 1.0), y);
+  return y;
+}
+
 __device__ __forceinline__ double sum8(double v) {
   v += __shfl_xor_sync(0xffffffffu, v, 4, 8);
   v += __shfl_xor_sync(0xffffffffu, v, 2, 8);
@@ -1346,7 +1372,7 @@ __device__ int quad_shake(const Rep& R, const QLane& q, double x[3], const doubl
       for (int j = k; j < 6; ++j) pk[j] = __shfl_sync(full, A[j], bl, 8);
       const double pb = __shfl_sync(full, B, bl, 8);
       if (fabs(pk[k]) < 1.0e-30) lu_ok = false;
-      const double piv = 1.0 / pk[k];
+      const double piv = recip_nr(pk[k]);
       if (sl == bl) {
         used = true;
         A[k] = piv;
@@ -1645,6 +1671,7 @@ __device__ __forceinline__ void fix_unit(const DevPtrs& P, const IntConst& c, in
 template <bool FP64, bool RESIDENT, bool STOP>
 __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst c, int nunit) {
   __shared__ UnitSmem S;
+  __shared__ unsigned char s_act[kActCache];   // replicas still in the SHAKE<->thermostat loop
   const int nthr = gridDim.x * blockDim.x;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int tid = threadIdx.x;
@@ -1801,9 +1828,9 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
   if (shk) {
     for (int it = 1; it < c.icslop; ++it) {
       if (!grid_barrier(P, epoch)) return;
-      if (!any_active(P, c, it, tt)) break;
+      if (!any_active(P, c, it, tt, s_act)) break;
       // lambda's velocity stays (v_back + v)/2 through the loop (verlethe.f90:529)
-      const bool lam_act = lam_thread && cano_active(P, c, P.reps[gt], it, true, tt);
+      const bool lam_act = lam_thread && rep_active(P, c, s_act, gt, it, tt);
       if (lam_act) {
         lam_add_ke(P, c, P.reps[gt], 2 * it, L.lvt);
         lam_add_ke(P, c, P.reps[gt], 2 * it + 1, L.lvt);
@@ -1813,17 +1840,17 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
         const int v = base + gt;
         if (RESIDENT) {
           if (quad) {
-            const bool act = Q.grp && cano_active(P, c, P.reps[Q.rep], it, true, tt);
+            const bool act = Q.grp && rep_active(P, c, s_act, Q.rep, it, tt);
             const double ke = q_cano4<FP64>(P, c, Q, S, tid, s);
             add_kin_quad(P, c.nsub_total, 2 * it, act ? Q.sub : -1, act ? ke : 0.0);
           } else {
-            const bool act = small && cano_active(P, c, P.reps[U.rep], it, true, tt);
+            const bool act = small && rep_active(P, c, s_act, U.rep, it, tt);
             const double ke = act ? ru_cano4<FP64>(P, c, U, S, tid, s) : 0.0;
             add_kin(P, c.nsub_total, 2 * it, act ? U.sub : -1, ke);
           }
         } else if (v >= c.qbase) {
           const QLane q = ql_make(P, c, v);
-          const bool act = q.grp && cano_active(P, c, P.reps[q.rep], it, true, tt);
+          const bool act = q.grp && rep_active(P, c, s_act, q.rep, it, tt);
           q_fetch(P, q, S, tid, false);
           const double ke = q_cano4<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep));
           if (act) q_spill(P, c, q, S, tid, FP64);
@@ -1833,7 +1860,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
           int sub = -1;
           if (v < c.nsmall) {
             const Unit u = P.units[P.small_idx[v]];
-            if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+            if (rep_active(P, c, s_act, u.rep, it, tt)) {
               sub = u.sub;
               ke = cano4_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
             }
@@ -1851,17 +1878,17 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
           int rep = -1;
           if (RESIDENT) {
             if (!quad) {
-              if (small && cano_active(P, c, P.reps[U.rep], it, true, tt)) {
+              if (small && rep_active(P, c, s_act, U.rep, it, tt)) {
                 ru_cano5<FP64>(P, c, U, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, U.sub)));
                 rep = com_small(P, c, U, S, tid, w);
               }
-            } else if (Q.grp && cano_active(P, c, P.reps[Q.rep], it, true, tt)) {
+            } else if (Q.grp && rep_active(P, c, s_act, Q.rep, it, tt)) {
               q_cano5<FP64>(P, c, Q, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, Q.sub)));
               rep = com_quad(P, c, Q, S, tid, w);
             }
           } else if (v >= c.qbase) {
             const QLane q = ql_make(P, c, v);
-            if (q.grp && cano_active(P, c, P.reps[q.rep], it, true, tt)) {
+            if (q.grp && rep_active(P, c, s_act, q.rep, it, tt)) {
               q_fetch(P, q, S, tid, false);
               q_cano5<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep), sqrt(tt / sub_temp(P, c, 2 * it, q.sub)));
               rep = com_quad(P, c, q, S, tid, w);
@@ -1869,7 +1896,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
             }
           } else if (v < c.nsmall) {
             const Unit u = P.units[P.small_idx[v]];
-            if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+            if (rep_active(P, c, s_act, u.rep, it, tt)) {
               cano5_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
               rep = com_unit(P, c, u, w);
             }
@@ -1883,7 +1910,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
         if (split) {   // the correction, then phase 3 (phase 5 ran above)
           if (RESIDENT) {
             if (!quad) {
-              const bool act = small && cano_active(P, c, P.reps[U.rep], it, true, tt);
+              const bool act = small && rep_active(P, c, s_act, U.rep, it, tt);
               double ke = 0.0;
               if (act) {
                 fix_small(P, c, it, U, S, tid, shk);
@@ -1891,7 +1918,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
               }
               add_kin(P, c.nsub_total, 2 * it + 1, act ? U.sub : -1, ke);
             } else {
-              const bool act = Q.grp && cano_active(P, c, P.reps[Q.rep], it, true, tt);
+              const bool act = Q.grp && rep_active(P, c, s_act, Q.rep, it, tt);
               double sx[3], sdx[3];
 #pragma unroll
               for (int k = 0; k < 3; ++k) { sx[k] = S.x[k][tid]; sdx[k] = S.dxs[k][tid]; }
@@ -1905,7 +1932,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
             }
           } else if (v >= c.qbase) {
             const QLane q = ql_make(P, c, v);
-            const bool act = q.grp && cano_active(P, c, P.reps[q.rep], it, true, tt);
+            const bool act = q.grp && rep_active(P, c, s_act, q.rep, it, tt);
             q_fetch(P, q, S, tid, false);
             if (act) fix_quad(P, c, it, q, S, tid);
             const double ke = q_cano3(P, c, q, S, tid);
@@ -1916,7 +1943,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
             int sub = -1;
             if (v < c.nsmall) {
               const Unit u = P.units[P.small_idx[v]];
-              if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+              if (rep_active(P, c, s_act, u.rep, it, tt)) {
                 fix_unit(P, c, it, u, shk, FP64);
                 sub = u.sub;
                 ke = cano3_unit<FP64>(P, c, u);
@@ -1928,7 +1955,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
         }
         if (RESIDENT) {
           if (!quad) {
-            const bool act = small && cano_active(P, c, P.reps[U.rep], it, true, tt);
+            const bool act = small && rep_active(P, c, s_act, U.rep, it, tt);
             double ke = 0.0;
             if (act) {
               ru_cano5<FP64>(P, c, U, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, U.sub)));
@@ -1937,7 +1964,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
             add_kin(P, c.nsub_total, 2 * it + 1, act ? U.sub : -1, ke);
           } else {
             // the whole warp runs the SHAKE (its shuffles); inactive groups keep their state
-            const bool act = Q.grp && cano_active(P, c, P.reps[Q.rep], it, true, tt);
+            const bool act = Q.grp && rep_active(P, c, s_act, Q.rep, it, tt);
             double sx[3], sdx[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) { sx[k] = S.x[k][tid]; sdx[k] = S.dxs[k][tid]; }
@@ -1951,7 +1978,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
           }
         } else if (v >= c.qbase) {
           const QLane q = ql_make(P, c, v);
-          const bool act = q.grp && cano_active(P, c, P.reps[q.rep], it, true, tt);
+          const bool act = q.grp && rep_active(P, c, s_act, q.rep, it, tt);
           q_fetch(P, q, S, tid, false);
           if (act) q_cano5<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep),
                                  sqrt(tt / sub_temp(P, c, 2 * it, q.sub)));
@@ -1963,7 +1990,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
           int sub = -1;
           if (v < c.nsmall) {
             const Unit u = P.units[P.small_idx[v]];
-            if (cano_active(P, c, P.reps[u.rep], it, true, tt)) {
+            if (rep_active(P, c, s_act, u.rep, it, tt)) {
               cano5_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
               sub = u.sub;
               ke = cano3_unit<FP64>(P, c, u);
