@@ -217,10 +217,11 @@ int capture(jp_ctx *c, cudaGraphExec_t *out, bool rebuild) {
   if (rebuild) {
     enqueue_rebuild(c);
   } else {
-    // the bonded terms run beside the pair tiles (both only add into the force and energy
-    // accumulators, as order-independent integer sums on the mixed path), joined before the
-    // integration
-    enqueue_zero(c, false);
+    // forces and energy slots start at zero (the integration of the previous step, or the
+    // call that last used them, left them so); the bonded terms run beside the pair tiles
+    // (both only add into the accumulators, as order-independent integer sums on the mixed
+    // path), joined before the integration
+    if (c->alsd) cudaMemsetAsync(c->P.ene_cls, 0, sizeof(long long) * 4 * c->nrep, c->st);
     CK(cudaEventRecord(c->ev_fork, c->st));
     CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
     launch_bonded(c->P, c->nterm, c->fp64, c->zc.bcoeff, c->zc.fcoeff, c->alsd, c->st2);
@@ -240,8 +241,11 @@ int check_status(jp_ctx *c) {
   CK(cudaMemcpy(&s, c->P.status, sizeof(unsigned), cudaMemcpyDeviceToHost));
   if (s == 0) return JP_OK;
   CK(cudaMemset(c->P.status, 0, sizeof(unsigned)));
-  // an integration that stopped early left its barrier and sums: clear them for the next
+  // an integration that stopped early left its barrier, sums and accumulators: clear them
   CK(cudaMemset(c->P.bar, 0, sizeof(unsigned) * 4));
+  if (c->fp64) CK(cudaMemset(c->P.grd, 0, sizeof(double) * 3 * c->natom));
+  else CK(cudaMemset(c->P.frc, 0, sizeof(long long) * 3 * c->natom));
+  CK(cudaMemset(c->P.ene_fix, 0, sizeof(long long) * (16 * c->nrep + 1)));
   CK(cudaMemset(c->P.kin_fix, 0, sizeof(long long) * c->nkin * c->nsub));
   if (c->ic.stop) CK(cudaMemset(c->P.com, 0, sizeof(double) * c->ic.ncom * c->ic.nrep * 16));
   if (s & ERR_TIMEOUT) return JP_E_TIMEOUT;
@@ -1063,6 +1067,12 @@ int jp_energy_grad(jp_ctx *c, int32_t r, const double *cord, double *eneval, dou
       for (size_t i = 0; i < g.size(); ++i) grad[i] = (double)g[i] * kFrcInv;
     }
   }
+  // steps start from zero force and energy accumulators; the class energies stay readable
+  // (jp_get_lambda) until the next step clears them
+  if (c->fp64) CK(cudaMemsetAsync(c->P.grd, 0, sizeof(double) * 3 * c->natom, c->st));
+  else CK(cudaMemsetAsync(c->P.frc, 0, sizeof(long long) * 3 * c->natom, c->st));
+  CK(cudaMemsetAsync(c->P.ene_fix, 0, sizeof(long long) * (16 * c->nrep + 1), c->st));
+  CK(cudaStreamSynchronize(c->st));
   return check_status(c);
 }
 

@@ -376,27 +376,29 @@ __global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= nchunk) return;
-  unsigned nz = P.chunk_nz[w];
+  const unsigned nz = P.chunk_nz[w];
   if (!nz) return;
   const int bi = P.chunk_i[w], j0 = P.chunk_j0[w];
-  const Rep& R = P.reps[P.blk_rep[bi]];
-  int t = P.chunk_off[w];
-  while (nz) {
-    const int b = __ffs(nz) - 1;
-    nz &= nz - 1;
-    P.masks[(size_t)t * 32 + lane] = P.tmp_masks[((size_t)w * 32 + b) * 32 + lane];
-    if (cmm) P.masks_el[(size_t)t * 32 + lane] = P.tmp_masks_el[((size_t)w * 32 + b) * 32 + lane];
-    if (lane == 0) {
-      const int bj = j0 + b;
-      P.tiles[t] = make_int2(bi, bj);
-      double s[3];
-      for (int k = 0; k < 3; ++k) {
-        const double d = P.blk_ref[3 * bi + k] - P.blk_ref[3 * bj + k];
-        s[k] = d - R.box[k] * anint(d * R.invbox[k]);
-      }
-      P.tile_shift[t] = make_float4((float)s[0], (float)s[1], (float)s[2], 0.f);
+  const int t0 = P.chunk_off[w];
+  const int cnt = __popc(nz);
+  if (lane < cnt) {   // lane q: the chunk's q-th tile, its block pair and image shift
+    const Rep& R = P.reps[P.blk_rep[bi]];
+    const int bj = j0 + (int)__fns(nz, 0, lane + 1);
+    P.tiles[t0 + lane] = make_int2(bi, bj);
+    float sh[3];
+    for (int k = 0; k < 3; ++k) {
+      const double d = P.blk_ref[3 * bi + k] - P.blk_ref[3 * bj + k];
+      sh[k] = (float)(d - R.box[k] * anint(d * R.invbox[k]));
     }
-    ++t;
+    P.tile_shift[t0 + lane] = make_float4(sh[0], sh[1], sh[2], 0.f);
+  }
+  unsigned m = nz;   // masks: one coalesced row of 32 per tile
+#pragma unroll 4
+  for (int q = 0; q < cnt; ++q) {
+    const int b = __ffs(m) - 1;
+    m &= m - 1;
+    P.masks[(size_t)(t0 + q) * 32 + lane] = P.tmp_masks[((size_t)w * 32 + b) * 32 + lane];
+    if (cmm) P.masks_el[(size_t)(t0 + q) * 32 + lane] = P.tmp_masks_el[((size_t)w * 32 + b) * 32 + lane];
   }
 }
 

@@ -267,6 +267,17 @@ __host__ __device__ __noinline__ int shake_group4(const Rep& R, const Unit& u, c
   return singular ? -2 : 1;
 }
 
+// An atom's force accumulator back to zero once its owner has read it for the last time in
+// the step: the next step's pair, bonded and far-field kernels add into zeros (no memset).
+template <bool FP64>
+__device__ __forceinline__ void zero_force(const DevPtrs& P, int a) {
+  if (FP64) {
+    P.grd[3 * a] = 0.0; P.grd[3 * a + 1] = 0.0; P.grd[3 * a + 2] = 0.0;
+  } else {
+    P.frc[3 * a] = 0; P.frc[3 * a + 1] = 0; P.frc[3 * a + 2] = 0;
+  }
+}
+
 __device__ __forceinline__ void shake_status(const DevPtrs& P, int ier) {
   if (ier == 1) atomicOr(P.status, ERR_SHAKE_NOCONV);
   else if (ier == -2) atomicOr(P.status, ERR_SHAKE_SINGULAR);
@@ -554,6 +565,9 @@ __device__ void finish_block(const DevPtrs& P, const IntConst& c, double tt) {
   // every other block has left its last barrier and read its last sum
   const int nk = c.nkin * c.nsub_total;
   for (int i = threadIdx.x; i < nk; i += blockDim.x) P.kin_fix[i] = 0;
+  // the step's energies have been read (write_ene_hist, the force scale); the pair kernels'
+  // tile counter follows them
+  for (int i = threadIdx.x; i < 16 * c.nrep + 1; i += blockDim.x) P.ene_fix[i] = 0;
   if (c.stop)
     for (int i = threadIdx.x; i < c.ncom * c.nrep * kCom; i += blockDim.x) P.com[i] = 0.0;
   if (threadIdx.x == 0) {
@@ -886,6 +900,7 @@ __global__ void __launch_bounds__(64) k_micr_fused(DevPtrs P, IntConst c, int nu
       if (t < nunit) {
         const Unit u = P.units[t];
         rep = micr_vel<FP64>(P, c, u, rep_scale(P, c, u.rep), w);
+        JP_UNIT_LOOP(q) zero_force<FP64>(P, u.a[q]);
       }
       if (c.stop) com_add(P, c, 0, rep, w);
     }
@@ -910,6 +925,7 @@ __global__ void __launch_bounds__(64) k_micr_fused(DevPtrs P, IntConst c, int nu
         const Unit u = P.units[t];
         sub = u.sub;
         ke = micr_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
+        JP_UNIT_LOOP(q) zero_force<FP64>(P, u.a[q]);
       }
       add_kin(P, c.nsub_total, c.nkin - 1, sub, ke);
     }
@@ -2022,8 +2038,25 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
         }
       }
       if (bad) atomicOr(P.status, ERR_NONFINITE);
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        if (q < U.n) zero_force<FP64>(P, U.a[q]);
     } else if (quad) {
       q_spill(P, c, Q, S, tid, FP64);
+      if (Q.a >= 0) zero_force<FP64>(P, Q.a);
+    }
+  } else {   // grid-stride form: each thread clears the atoms of the lanes it ran
+    for (int base = 0; base < nv; base += nthr) {
+      const int v = base + gt;
+      if (v >= c.qbase) {
+        if (v < c.nvirt) {
+          const QLane q = ql_make(P, c, v);
+          if (q.a >= 0) zero_force<FP64>(P, q.a);
+        }
+      } else if (v < c.nsmall) {
+        const Unit u = P.units[P.small_idx[v]];
+        JP_UNIT_LOOP(q) zero_force<FP64>(P, u.a[q]);
+      }
     }
   }
   if (lam_thread) {
