@@ -76,6 +76,22 @@ typedef struct jp_ge {
   double lower, upper;       /* ALSD linear wall slopes (LMD only) */
 } jp_ge;
 
+/* Frozen external environment of a CMM run (EXTCMM=, setextCMM.f90 / enear_extCMM.f90): the
+ * level-1 multipoles of the cells of a surrounding system, on the same cell grid as the
+ * simulated one, which is then centred on `center` instead of the atoms' centroid (celpar.f90
+ * :54-70).  Each atom interacts with the occupied external cells among its own level-1 cell
+ * and its 26 neighbours: the multipole expansion, softened inside 1.5 CELSIZ of the cell
+ * centre (enear_extCMM.f90:58-164).  Only 4 cell levels are supported (setextCMM.f90:20). */
+typedef struct jp_ext_cmm {
+  int32_t nlev;              /* cell levels of the file: must equal the run's (4) */
+  double cell;               /* its level-1 cell size: must equal CELSIZ */
+  double center[3];          /* grid centre (celx, cely, celz) */
+  const uint8_t *flag;       /* [nv1^3] 1 = external cell occupied (exflag1), x fastest */
+  const double *pot;         /* [nv1^3][13] its multipoles in the engine's layout: q, p_x..z,
+                                Q_xx/2, Q_yy/2, Q_zz/2, Q_xx, Q_yy, Q_zz, Q_xy, Q_yz, Q_zx
+                                (setextCMM.f90:44-68 forms this from the file's 10 arrays) */
+} jp_ext_cmm;
+
 /* Capacity of a replica's weight and of its energy histogram (fixed when the context is
  * created, so the weight can be replaced between runs without re-capturing anything). */
 #define JP_GE_MAX_WINDOWS 16
@@ -135,6 +151,7 @@ typedef struct jp_system {
   const jp_ge *ge;             /* McMD weight for METHOD= GE; NULL otherwise */
   const int32_t *cluster;      /* [natom] 1 = atom of the lambda-scaled cluster (CLUSTA
                                   residues, inpcls.f90 icls = 1), else 0; NULL = none */
+  const jp_ext_cmm *ext_cmm;   /* EXTCMM= environment (CAL15M= CMM only); NULL = none */
 } jp_system;
 
 /* Run parameters shared by all replicas of a context (md.inp EXE> MD keywords). */

@@ -50,6 +50,11 @@ class JpGe(C.Structure):
                 ("tempce", C.c_double), ("lower", C.c_double), ("upper", C.c_double)]
 
 
+class JpExtCmm(C.Structure):
+    _fields_ = [("nlev", C.c_int32), ("cell", C.c_double), ("center", C.c_double * 3),
+                ("flag", C.POINTER(C.c_uint8)), ("pot", _dp)]
+
+
 JP_GE_MAX_WINDOWS, JP_GE_MAX_DEG, JP_GE_MAX_BINS = 16, 15, 4096
 
 
@@ -74,7 +79,7 @@ class JpSystem(C.Structure):
         ("nimpr", C.c_int32), ("impr", _ip), ("impr_k", _dp), ("impr_nrot", _dp),
         ("impr_phase", _dp), ("impr_div", _ip),
         ("nshake", C.c_int32), ("shake_n", _ip), ("shake_atoms", _ip), ("shake_dist", _dp),
-        ("ge", C.POINTER(JpGe)), ("cluster", _ip),
+        ("ge", C.POINTER(JpGe)), ("cluster", _ip), ("ext_cmm", C.POINTER(JpExtCmm)),
     ]
 
 
@@ -168,6 +173,17 @@ def make_system(top, keep, cord=None, vel=None):
                         else np.zeros(6), C.c_double, keep)
     cl = top.get("cluster")
     s.cluster = None if cl is None else _ptr(np.asarray(cl, np.int32), C.c_int32, keep)
+    ex = top.get("ext_cmm")   # dict(nlev, cell, center[3], flag[nv^3] 0/1, pot[nv^3][13])
+    if ex is not None:
+        flag = np.ascontiguousarray(np.asarray(ex["flag"]).reshape(-1), np.uint8)
+        pot = np.ascontiguousarray(np.asarray(ex["pot"], np.float64).reshape(-1))
+        keep += [flag, pot]
+        e = JpExtCmm(nlev=int(ex["nlev"]), cell=float(ex["cell"]),
+                     center=(C.c_double * 3)(*[float(v) for v in ex["center"]]),
+                     flag=flag.ctypes.data_as(C.POINTER(C.c_uint8)),
+                     pot=pot.ctypes.data_as(_dp))
+        keep.append(e)
+        s.ext_cmm = C.pointer(e)
     ge = top.get("ge")
     if ge is not None:
         g = make_ge(ge, keep)

@@ -488,6 +488,16 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       }
       R.idelay = (int)std::ceil(rc / R.siz[1]);
       R.cmm_upd = prm->cmm_update;
+      if (s.ext_cmm) {   // setextCMM.f90:17-33: 4 levels, the same grid as the file's
+        const jp_ext_cmm &x = *s.ext_cmm;
+        if (x.nlev != 4 || nlev != 4 || !x.flag || !x.pot ||
+            !(std::fabs(x.cell - prm->cmm_cell) <= 1e-9 * prm->cmm_cell)) { delete c; return JP_E_INVALID; }
+        R.ext = 1;
+        for (int k = 0; k < 3; ++k) R.ext_c0[k] = x.center[k];
+      }
+    } else if (s.ext_cmm) {
+      delete c;
+      return JP_E_INVALID;   // an external environment belongs to a CMM run
     }
     // xy columns of edge ~(32/density)^(1/3) so that 32 z-sorted atoms fill a near-cubic
     // block; 0.25 A z bins inside a column
@@ -876,6 +886,21 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     e |= dalloc(c, &P.cmm_c0, 3 * (size_t)nrep);
     e |= dalloc(c, &P.cmm_e, (size_t)nrep);
     e |= dalloc(c, &P.cmm_enew, (size_t)nrep);
+    e |= dalloc(c, &P.ene_ext, (size_t)nrep);
+    // external environments on the level-1 cells (zeros for replicas without one)
+    std::vector<unsigned char> hflag((size_t)c->cmm_ncell[1], 0);
+    std::vector<double> hpot((size_t)13 * c->cmm_ncell[1], 0.0);
+    for (int r = 0; r < nrep; ++r) {
+      const Rep &R = c->reps[r];
+      if (!R.ext) continue;
+      const size_t nc = (size_t)R.nv[1] * R.nv[1] * R.nv[1];
+      for (size_t q = 0; q < nc; ++q) {
+        hflag[R.cell_off[1] + q] = sys[r].ext_cmm->flag[q] ? 1 : 0;
+        for (int k = 0; k < 13; ++k) hpot[(R.cell_off[1] + q) * 13 + k] = sys[r].ext_cmm->pot[q * 13 + k];
+      }
+    }
+    e |= dput(c, &P.ext_flag, hflag);
+    e |= dput(c, &P.ext_pot, hpot);
   }
   e |= dalloc(c, &P.ntiles, 1);
   e |= dalloc(c, &P.key, (size_t)N);

@@ -29,9 +29,10 @@ __device__ __forceinline__ double cmm_cen(const Rep& R, const double* c0, int l,
   return R.siz[l] * ((double)i + r) + c0[k];
 }
 
+// the grid centre: the atoms' centroid at the last rebuild, or the external environment's
 __device__ __forceinline__ void cmm_centroid(const DevPtrs& P, const Rep& R, int rep, double* c0) {
   const double rtmp = 1.0 / (double)R.natom;
-  for (int k = 0; k < 3; ++k) c0[k] = __ldcg(&P.cmm_c0[3 * rep + k]) * rtmp;
+  for (int k = 0; k < 3; ++k) c0[k] = R.ext ? R.ext_c0[k] : __ldcg(&P.cmm_c0[3 * rep + k]) * rtmp;
 }
 
 // replica and local index of global cell g of level l (-1: no CMM replica holds it)
@@ -52,7 +53,7 @@ __global__ void k_cmm_centroid(DevPtrs P, int natom) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= natom) return;
   const int rep = P.rep_of[a];
-  if (!P.reps[rep].cmm) return;
+  if (!P.reps[rep].cmm || P.reps[rep].ext) return;
   for (int k = 0; k < 3; ++k) atomicAdd(&P.cmm_c0[3 * rep + k], P.x[3 * a + k]);
 }
 
@@ -234,6 +235,80 @@ __device__ double cmm_far_atom(const DevPtrs& P, const Rep& R, const double* c0,
   return e;
 }
 
+// external environment of one atom (enear_extCMM.f90:58-164): the occupied external cells
+// among its level-1 cell and the 26 around it; within R = 1.5 cell sizes of a cell centre the
+// expansion on that sphere, blended inward by a cubic in r.  Returns the energy per unit
+// charge (before md_run's factor 0.5), gradient per unit charge in g.
+__device__ double cmm_ext_atom(const DevPtrs& P, const Rep& R, const double* c0, int cell,
+                               const double* x, double* g) {
+  const int nv1 = R.nv[1];
+  const int mx = (cell & 255) + 1, my = ((cell >> 8) & 255) + 1, mz = ((cell >> 16) & 255) + 1;
+  const double RR = 1.5 * R.siz[1], RR2 = RR * RR, RR_2 = 3.0 * R.siz[1];
+  const double iRR = 1.0 / RR, iRR3 = iRR * iRR * iRR, iRR5 = iRR3 * iRR * iRR;
+  const double i3RR5 = 3.0 * iRR5, i5RR7 = 5.0 * iRR5 * iRR * iRR;
+  double e = 0.0;
+  g[0] = g[1] = g[2] = 0.0;
+  for (int jz = max(1, mz - 1); jz <= min(nv1, mz + 1); ++jz)
+    for (int jy = max(1, my - 1); jy <= min(nv1, my + 1); ++jy)
+      for (int jx = max(1, mx - 1); jx <= min(nv1, mx + 1); ++jx) {
+        const int id = R.cell_off[1] + ((jz - 1) * nv1 + (jy - 1)) * nv1 + (jx - 1);
+        if (!P.ext_flag[id]) continue;
+        const double* q = P.ext_pot + (size_t)id * 13;
+        double dx = x[0] - cmm_cen(R, c0, 1, jx, 0);
+        double dy = x[1] - cmm_cen(R, c0, 1, jy, 1);
+        double dz = x[2] - cmm_cen(R, c0, 1, jz, 2);
+        const double dd2 = dx * dx + dy * dy + dz * dz;
+        double ec, f[3];
+        if (dd2 < RR2) {
+          const double scal = sqrt(RR2 / dd2);
+          dx *= scal; dy *= scal; dz *= scal;
+          const double aa1 = q[1] * dx + q[2] * dy + q[3] * dz;
+          const double aa2 = q[4] * dx * dx + q[5] * dy * dy + q[6] * dz * dz + q[10] * dx * dy +
+                             q[11] * dy * dz + q[12] * dz * dx;
+          const double e0 = q[0] * iRR + aa1 * iRR3 + aa2 * iRR5;
+          const double c4 = aa1 * i3RR5 + aa2 * i5RR7;
+          f[0] = -(q[0] * dx - q[1]) * iRR3 + (q[7] * dx + q[10] * dy + q[12] * dz) * iRR5 - c4 * dx;
+          f[1] = -(q[0] * dy - q[2]) * iRR3 + (q[10] * dx + q[8] * dy + q[11] * dz) * iRR5 - c4 * dy;
+          f[2] = -(q[0] * dz - q[3]) * iRR3 + (q[12] * dx + q[11] * dy + q[9] * dz) * iRR5 - c4 * dz;
+          const double fn = sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+          const double r = sqrt(dd2), b = fn * r;
+          const double sf = r * iRR3 * (6.0 * e0 * (r - RR) + b * (3.0 * r - RR_2)) / fn;
+          for (int k = 0; k < 3; ++k) f[k] *= sf;
+          const double t = r * iRR;
+          ec = (2.0 * e0 + b) * t * t * t - (3.0 * e0 + b) * t * t + 2.0 * e0;
+        } else {
+          const double d2i = 1.0 / dd2, di = sqrt(d2i), d3i = di * d2i, d5i = d3i * d2i;
+          const double d7i = d5i * d2i;
+          const double aa1 = q[1] * dx + q[2] * dy + q[3] * dz;
+          const double aa2 = q[4] * dx * dx + q[5] * dy * dy + q[6] * dz * dz + q[10] * dx * dy +
+                             q[11] * dy * dz + q[12] * dz * dx;
+          ec = q[0] * di + aa1 * d3i + aa2 * d5i;
+          const double c4 = aa1 * 3.0 * d5i + aa2 * 5.0 * d7i;
+          f[0] = -(q[0] * dx - q[1]) * d3i + (q[7] * dx + q[10] * dy + q[12] * dz) * d5i - c4 * dx;
+          f[1] = -(q[0] * dy - q[2]) * d3i + (q[10] * dx + q[8] * dy + q[11] * dz) * d5i - c4 * dy;
+          f[2] = -(q[0] * dz - q[3]) * d3i + (q[12] * dx + q[11] * dy + q[9] * dz) * d5i - c4 * dz;
+        }
+        e += ec;
+        for (int k = 0; k < 3; ++k) g[k] += f[k];
+      }
+  return e;
+}
+
+// warp sum of each lane's energy into a replica's fixed-point slot (rep -1: nothing)
+__device__ __forceinline__ void warp_energy(long long* dst, int rep, double e) {
+  const unsigned full = 0xffffffffu;
+  const unsigned has = __ballot_sync(full, rep >= 0);
+  if (has == 0u) return;
+  const int r0 = __shfl_sync(full, rep, __ffs(has) - 1);
+  if (__all_sync(full, rep < 0 || rep == r0)) {
+    double v = rep >= 0 ? e : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(full, v, o);
+    if ((threadIdx.x & 31) == 0) atomic_add_ll(&dst[r0], to_fix(v, kEneScale));
+  } else if (rep >= 0) {
+    atomic_add_ll(&dst[rep], to_fix(e, kEneScale));
+  }
+}
+
 __device__ __forceinline__ bool cmm_due(const DevPtrs& P, const Rep& R, bool force) {
   return force || (P.step_ctr[0] % R.cmm_upd) == 0;
 }
@@ -241,42 +316,39 @@ __device__ __forceinline__ bool cmm_due(const DevPtrs& P, const Rep& R, bool for
 // far field of each atom when due (into gwk, energy into cmm_enew), then gwk into the forces
 __global__ void k_cmm_far(DevPtrs P, int natom, int fp64, int force, double ccoef) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  int rep = -1;
-  double e = 0.0;
+  int rep = -1, rep_x = -1;
+  double e = 0.0, ex = 0.0;
   if (a < natom) {
     const int r = P.rep_of[a];
     const Rep& R = P.reps[r];
     if (R.cmm) {
       const int cell = P.cmm_cell[a];
+      const double q2 = ccoef * P.chg[a];   // chgmod2 (inpcls.f90:223)
+      double c0[3], x[3], g[3];
+      cmm_centroid(P, R, r, c0);
+      for (int k = 0; k < 3; ++k) x[k] = P.x[3 * a + k];
       if (cmm_due(P, R, force != 0) && cell >= 0) {
-        double c0[3], x[3], g[3];
-        cmm_centroid(P, R, r, c0);
-        for (int k = 0; k < 3; ++k) x[k] = P.x[3 * a + k];
-        const double q2 = ccoef * P.chg[a];   // chgmod2 (inpcls.f90:223)
         e = 0.5 * q2 * cmm_far_atom(P, R, c0, cell, x, g);
         for (int k = 0; k < 3; ++k) P.gwk[3 * a + k] = g[k] * q2;
         rep = r;
       }
       if (cell >= 0) {
+        double gx[3] = {0.0, 0.0, 0.0};
+        if (R.ext) {   // the external environment, every step (cmmdo.f90:82)
+          ex = 0.5 * q2 * cmm_ext_atom(P, R, c0, cell, x, gx);
+          rep_x = r;
+        }
         for (int k = 0; k < 3; ++k) {
-          const double gk = P.gwk[3 * a + k];
+          const double gk = P.gwk[3 * a + k] + gx[k] * q2;
           if (fp64) atomicAdd(&P.grd[3 * a + k], gk);
           else atomic_add_ll(&P.frc[3 * a + k], to_fix(gk, kFrcScale));
         }
       }
     }
   }
-  // warp-level energy sum (one replica per warp as a rule; mixed warps add per lane)
-  const unsigned full = 0xffffffffu;
-  const unsigned has = __ballot_sync(full, rep >= 0);
-  if (has == 0u) return;
-  const int r0 = __shfl_sync(full, rep, __ffs(has) - 1);
-  if (__all_sync(full, rep < 0 || rep == r0)) {
-    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(full, e, o);
-    if ((threadIdx.x & 31) == 0) atomic_add_ll(&P.cmm_enew[r0], to_fix(e, kEneScale));
-  } else if (rep >= 0) {
-    atomic_add_ll(&P.cmm_enew[rep], to_fix(e, kEneScale));
-  }
+  // warp-level energy sums (one replica per warp as a rule; mixed warps add per lane)
+  warp_energy(P.cmm_enew, rep, e);
+  warp_energy(P.ene_ext, rep_x, ex);
 }
 
 // the far-field energy of the step into ELE15: the new sum when due, else the last one
@@ -288,7 +360,8 @@ __global__ void k_cmm_energy(DevPtrs P, int nrep, int force) {
       P.cmm_e[r] = P.cmm_enew[r];
       P.cmm_enew[r] = 0;
     }
-    atomic_add_ll(&P.ene_fix[r * 16 + JP_E_ELE15], P.cmm_e[r]);
+    atomic_add_ll(&P.ene_fix[r * 16 + JP_E_ELE15], P.cmm_e[r] + P.ene_ext[r]);
+    P.ene_ext[r] = 0;
   }
 }
 

@@ -74,6 +74,8 @@ struct Rep {
   int cmm, nlev, idelay, cmm_upd;
   int nv[6], cell_off[6];
   double siz[6];
+  int ext;                        // EXTCMM= environment on the level-1 cells (ext_flag, ext_pot)
+  double ext_c0[3];               // its grid centre, used instead of the atoms' centroid
 };
 
 // class weight of a term (verlethe.f90:116-163): class 0 = AA, 1 = AB, 2 = BB
@@ -159,7 +161,10 @@ struct DevPtrs {
   int *cmm_pop;
   double *cmm_pot, *cmm_raw, *cmm_c0;
   long long *cmm_e, *cmm_enew;
+  long long *ene_ext;             // EXTCMM energy of the step, per replica (fixed point)
   unsigned *masks_el, *tmp_masks_el;   // CMM tiles: pairs with the Coulomb term
+  unsigned char *ext_flag;        // EXTCMM: occupied external level-1 cells (CMM cell index)
+  double *ext_pot;                // their 13 coefficients
   // accumulators
   long long *ene_fix;             // [nrep][16], then the pair kernels' tile counter
   int *tile_ctr;                  // next unclaimed tile (zeroed with ene_fix every step)

@@ -106,6 +106,11 @@ struct Ctx {
   std::vector<double> gwk;               // far-field gradient of the last update
   double ecmm = 0.0;                     // its energy (sum over levels)
   bool itwin = true;                     // recompute the far field at the next force call
+  bool ext = false;                      // EXTCMM= environment on the level-1 grid
+  double ext_c0[3] = {0, 0, 0};          // its grid centre
+  std::vector<unsigned char> ext_flag;   // [nv1^3] occupied external cells
+  std::vector<double> ext_pot;           // [nv1^3][13]
+  double eext = 0.0;                     // its energy at the last force call
   int cmm_err = 0;                       // error of the last rebuild (an atom off the grid)
   // ---- state ----
   std::vector<double> cord, vel, grad;
@@ -211,7 +216,7 @@ int cmm_rebuild(Ctx& c) {
   for (int k = 0; k < 3; ++k) {
     double sum = 0.0;
     for (int i = 0; i < n; ++i) sum += x[3 * i + k];
-    cord0[k] = sum * rtmp;
+    cord0[k] = c.ext ? c.ext_c0[k] : sum * rtmp;   // EXTCMM: the file's centre (celpar.f90:54-70)
   }
   for (int l = 1; l <= c.nlev; ++l) {
     const int m = c.nv[l];
@@ -328,6 +333,67 @@ int cmm_rebuild(Ctx& c) {
     }
   }
   return 0;
+}
+
+// external environment (enear_extCMM.f90:2-174): each atom against the occupied external
+// cells among its level-1 cell and the 26 around it (clipped to the grid); within 1.5 cell
+// sizes of a cell centre the expansion is taken on that sphere and blended inward
+// (:58-125), beyond it the plain expansion (:126-160).  Returns the energy (times 0.5, as
+// md_run adds it), gradient added to grad.
+double cmm_ext(Ctx& c, const double* x, double* grad) {
+  const int nv1 = c.nv[1];
+  const double RR = 1.5 * c.siz[1], RR2 = RR * RR, RR_2 = 3.0 * c.siz[1];
+  const double iRR = 1.0 / RR, iRR3 = iRR * iRR * iRR, iRR5 = iRR3 * iRR * iRR;
+  const double i3RR5 = 3.0 * iRR5, i5RR7 = 5.0 * iRR5 * iRR * iRR;
+  double etot = 0.0;
+  for (int i = 0; i < c.n; ++i) {
+    const int mx = c.cell1[3 * i], my = c.cell1[3 * i + 1], mz = c.cell1[3 * i + 2];
+    const double q2 = c.ccoef * c.chg[i];
+    for (int jz = std::max(1, mz - 1); jz <= std::min(nv1, mz + 1); ++jz)
+      for (int jy = std::max(1, my - 1); jy <= std::min(nv1, my + 1); ++jy)
+        for (int jx = std::max(1, mx - 1); jx <= std::min(nv1, mx + 1); ++jx) {
+          const int id = cidx(c, 1, jx, jy, jz);
+          if (!c.ext_flag[id]) continue;
+          const double* q = &c.ext_pot[(size_t)13 * id];
+          double dx = x[3 * i] - c.cen[1][3 * (jx - 1)];
+          double dy = x[3 * i + 1] - c.cen[1][3 * (jy - 1) + 1];
+          double dz = x[3 * i + 2] - c.cen[1][3 * (jz - 1) + 2];
+          const double dd2 = dx * dx + dy * dy + dz * dz;
+          double e, f[3];
+          if (dd2 < RR2) {
+            const double scal = std::sqrt(RR2 / dd2);
+            dx *= scal; dy *= scal; dz *= scal;
+            const double aa1 = q[1] * dx + q[2] * dy + q[3] * dz;
+            const double aa2 = q[4] * dx * dx + q[5] * dy * dy + q[6] * dz * dz + q[10] * dx * dy +
+                               q[11] * dy * dz + q[12] * dz * dx;
+            const double e0 = q[0] * iRR + aa1 * iRR3 + aa2 * iRR5;
+            const double c4 = aa1 * i3RR5 + aa2 * i5RR7;
+            f[0] = -(q[0] * dx - q[1]) * iRR3 + (q[7] * dx + q[10] * dy + q[12] * dz) * iRR5 - c4 * dx;
+            f[1] = -(q[0] * dy - q[2]) * iRR3 + (q[10] * dx + q[8] * dy + q[11] * dz) * iRR5 - c4 * dy;
+            f[2] = -(q[0] * dz - q[3]) * iRR3 + (q[12] * dx + q[11] * dy + q[9] * dz) * iRR5 - c4 * dz;
+            const double fn = std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+            const double r = std::sqrt(dd2), b = fn * r;
+            const double sf = r * iRR3 * (6.0 * e0 * (r - RR) + b * (3.0 * r - RR_2)) / fn;
+            for (int k = 0; k < 3; ++k) f[k] *= sf;
+            const double t = r * iRR;
+            e = (2.0 * e0 + b) * t * t * t - (3.0 * e0 + b) * t * t + 2.0 * e0;
+          } else {
+            const double d2i = 1.0 / dd2, di = std::sqrt(d2i), d3i = di * d2i, d5i = d3i * d2i;
+            const double d7i = d5i * d2i;
+            const double aa1 = q[1] * dx + q[2] * dy + q[3] * dz;
+            const double aa2 = q[4] * dx * dx + q[5] * dy * dy + q[6] * dz * dz + q[10] * dx * dy +
+                               q[11] * dy * dz + q[12] * dz * dx;
+            e = q[0] * di + aa1 * d3i + aa2 * d5i;
+            const double c4 = aa1 * 3.0 * d5i + aa2 * 5.0 * d7i;
+            f[0] = -(q[0] * dx - q[1]) * d3i + (q[7] * dx + q[10] * dy + q[12] * dz) * d5i - c4 * dx;
+            f[1] = -(q[0] * dy - q[2]) * d3i + (q[10] * dx + q[8] * dy + q[11] * dz) * d5i - c4 * dy;
+            f[2] = -(q[0] * dz - q[3]) * d3i + (q[12] * dx + q[11] * dy + q[9] * dz) * d5i - c4 * dz;
+          }
+          etot += e * q2;
+          for (int k = 0; k < 3; ++k) grad[3 * i + k] += f[k] * q2;
+        }
+  }
+  return 0.5 * etot;
 }
 
 // far field of every atom (cmmdo.f90:85-160, compute_particle_multipole :181-290) into
@@ -639,6 +705,10 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
     if (c.itwin) cmm_far(c, x);
     for (int k = 0; k < 3 * n; ++k) grad[k] += c.gwk[k];
     eel += c.ecmm;
+    if (c.ext) {   // the external environment, every force call (cmmdo.f90:82)
+      c.eext = cmm_ext(c, x, grad);
+      eel += c.eext;
+    }
   }
   ene[JP_E_VDW15] += evdw;
   ene[JP_E_ELE15] += eel + c.dself + eexc;
@@ -1418,6 +1488,13 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
     }
     c->idelay = (int)std::ceil(c->rc / c->siz[1]);
     c->itwin = true;
+    if (s->ext_cmm) {   // setextCMM.f90: the file's level-1 cells on this grid
+      const int nc = c->nv[1] * c->nv[1] * c->nv[1];
+      c->ext = true;
+      for (int k = 0; k < 3; ++k) c->ext_c0[k] = s->ext_cmm->center[k];
+      c->ext_flag.assign(s->ext_cmm->flag, s->ext_cmm->flag + nc);
+      c->ext_pot.assign(s->ext_cmm->pot, s->ext_cmm->pot + (size_t)13 * nc);
+    }
   }
   // state
   c->cord.assign(s->cord, s->cord + 3 * n);
