@@ -342,6 +342,9 @@ def main():
     achieved = FLOPS_PER_PAIR * pairs / (pair_ms * 1e-3) / 1e12
     traffic, tsrc = ncu_traffic()
     hbm_peak = measured_peaks().get("hbm_gbs")
+    hbm_src = "of measured"
+    if not hbm_peak:   # the pool's earlier copy-bandwidth measurement
+        hbm_peak, hbm_src = 6650.0, "of fallback (MEASURED_PEAKS.json absent)"
     cpu = None if args.no_cpu else cpu_baseline(top)
     c4 = None if (args.no_c4 or world > 1) else c4_measure(dev)
     clocks = clk.summary()
@@ -375,7 +378,7 @@ def main():
                      "hbm": None if traffic is None or not hbm_peak else
                      {"achieved_gbs": traffic / (pair_ms * 1e-3) / 1e9, "peak_gbs": hbm_peak,
                       "frac": traffic / (pair_ms * 1e-3) / 1e9 / hbm_peak,
-                      "note": "ncu DRAM bytes per launch / CUDA-event launch time, of measured"},
+                      "note": "ncu DRAM bytes per launch / CUDA-event launch time, " + hbm_src},
                      "note": f"{FLOPS_PER_PAIR} FP32 flops per pair within rc x pairs per launch / "
                              "CUDA-event launch time; peak = FP32 FMA loop measured in this run "
                              "(MEASURED_PEAKS.json lists HBM and bf16 tensor peaks only)"},
