@@ -152,6 +152,15 @@ typedef struct jp_system {
   const int32_t *cluster;      /* [natom] 1 = atom of the lambda-scaled cluster (CLUSTA
                                   residues, inpcls.f90 icls = 1), else 0; NULL = none */
   const jp_ext_cmm *ext_cmm;   /* EXTCMM= environment (CAL15M= CMM only); NULL = none */
+  /* Hydrogen-bond 10-12 term (md_run iyeflg(10), on when a type pair has iyppid = 2,
+   * incel.f90:170-171; CAL15M= ZD and ATOM): a listed 1-5 pair whose types are marked
+   * in hbond keeps its Coulomb term but has E = C12h/r^12 - C10/r^10 instead of the 12-6
+   * term, with the same cut-off, summed into JP_E_HBOND (cutoff.f90:98-154 splits the
+   * pairs off, enear.f90:330-516 evaluates them).  1-4 pairs keep c6/c12 (dnergv.f90:490).
+   * The three tables are shared by all replicas, like c6/c12.  NULL hbond = no such pair. */
+  const int32_t *hbond;        /* [ntype][ntype] 1 = iyppid 2, else 0; symmetric */
+  const double *c10;           /* [ntype][ntype] fynbpp(3,:,:) of the marked pairs */
+  const double *c12h;          /* [ntype][ntype] fynbpp(4,:,:) of the marked pairs */
 } jp_system;
 
 /* Run parameters shared by all replicas of a context (md.inp EXE> MD keywords). */

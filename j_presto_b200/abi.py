@@ -8,7 +8,7 @@ import ctypes as C
 import numpy as np
 
 JP_MAXENE = 15
-JP_E_TOTAL, JP_E_VDW15, JP_E_ELE15 = 0, 7, 8   # eneval slots
+JP_E_TOTAL, JP_E_VDW14, JP_E_VDW15, JP_E_ELE15, JP_E_HBOND = 0, 5, 7, 8, 9   # eneval slots
 JP_PREC_FP64, JP_PREC_MIXED = 0, 1
 JP_METHOD_CONS, JP_METHOD_MICR, JP_METHOD_CANO, JP_METHOD_GE = 1, 2, 3, 4
 JP_SHAKE_NONE, JP_SHAKE_HBON, JP_SHAKE_ALLB = 0, 1, 2
@@ -80,6 +80,7 @@ class JpSystem(C.Structure):
         ("impr_phase", _dp), ("impr_div", _ip),
         ("nshake", C.c_int32), ("shake_n", _ip), ("shake_atoms", _ip), ("shake_dist", _dp),
         ("ge", C.POINTER(JpGe)), ("cluster", _ip), ("ext_cmm", C.POINTER(JpExtCmm)),
+        ("hbond", _ip), ("c10", _dp), ("c12h", _dp),
     ]
 
 
@@ -184,6 +185,10 @@ def make_system(top, keep, cord=None, vel=None):
                      pot=pot.ctypes.data_as(_dp))
         keep.append(e)
         s.ext_cmm = C.pointer(e)
+    if top.get("hbond") is not None:   # [ntype][ntype] 0/1 flags and the 10-12 tables
+        s.hbond = _ptr(np.asarray(top["hbond"], np.int32), C.c_int32, keep)
+        s.c10 = _ptr(top["c10"], C.c_double, keep)
+        s.c12h = _ptr(top["c12h"], C.c_double, keep)
     ge = top.get("ge")
     if ge is not None:
         g = make_ge(ge, keep)

@@ -54,6 +54,8 @@ struct jp_ctx {
   int pair_warps = 0;
   bool alsd = false;
   bool cmm = false;                 // CAL15M= CMM
+  bool hbond = false;               // some type pair has the 10-12 H-bond term
+  int hb_cap = 0;                   // capacity of the H-bond pair list
   int cmm_ncell[6] = {0, 0, 0, 0, 0, 0};   // cells per level over all replicas
   int cmm_nlev = 0;                 // most levels of any replica
   int cano_grid = 1;
@@ -159,7 +161,8 @@ void enqueue_rebuild(jp_ctx *c) {
   launch_tile_scan(P, c->nchunk, rlim * rlim, (float)rlim, rc * rc, c->cmm, st);
   scan_exclusive(P.chunk_cnt, P.chunk_off, c->nchunk + 1, c->scan_scratch, P.ntiles, st);
   k_tile_emit<<<nwb, 128, 0, st>>>(P, c->nchunk, c->cmm ? 1 : 0);
-  c->launches_rebuild = 19 + (c->fp64 ? 1 : 0) + ncmm;
+  if (c->hbond) launch_hb_list(P, c->hb_cap, c->zc.nt1, c->nblk, st);
+  c->launches_rebuild = 19 + (c->fp64 ? 1 : 0) + ncmm + (c->hbond ? 1 : 0);
 }
 
 // ---- one MD step ------------------------------------------------------------------------
@@ -178,6 +181,7 @@ void enqueue_zero(jp_ctx *c, bool count) {
 void enqueue_pair(jp_ctx *c, bool count, bool force_far = false) {
   if (c->fp64) launch_pair_fp64(c->P, c->zc, c->pair_warps, count, c->alsd, c->st);
   else launch_pair_mixed(c->P, c->zc, c->pair_warps, c->minimg, count, c->alsd, c->st);
+  if (c->hbond) launch_hbond(c->P, c->hb_cap, c->zc.rc2, c->zc.nt1, c->fp64, c->alsd, c->st);
   if (c->cmm) launch_cmm_far(c->P, c->natom, c->nrep, c->fp64, force_far, c->qscale * c->qscale, c->st);
 }
 
@@ -208,6 +212,7 @@ int launches_per_step(const jp_ctx *c) {
   n += 1;                          // the fused cooperative MICR or CANO/GE kernel
   n += c->ic.ge_prescaled ? 1 : 0; // k_ge_scale
   n += c->cmm ? 2 : 0;             // k_cmm_far, k_cmm_energy
+  n += c->hbond ? 1 : 0;           // k_hbond
   return n;
 }
 
@@ -295,6 +300,26 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
     const size_t nt2 = (size_t)s.ntype * s.ntype;
     for (size_t q = 0; q < nt2; ++q)
       if (s.c6[q] != sys[0].c6[q] || s.c12[q] != sys[0].c12[q]) return JP_E_INVALID;
+    // H-bond tables: 0/1 flags, symmetric, finite parameters, the same in every replica;
+    // the 10-12 pairs belong to the cut-off variants (enear_ZD_*, enear_ACT_*) only
+    if ((s.hbond == nullptr) != (sys[0].hbond == nullptr)) return JP_E_INVALID;
+    if (s.hbond) {
+      if (!s.c10 || !s.c12h) return JP_E_INVALID;
+      const int nt = s.ntype;
+      bool any = false;
+      for (int i = 0; i < nt; ++i)
+        for (int j = 0; j < nt; ++j) {
+          const size_t q = (size_t)i * nt + j, qt = (size_t)j * nt + i;
+          const int f = s.hbond[q];
+          if ((f != 0 && f != 1) || f != s.hbond[qt] || f != sys[0].hbond[q]) return JP_E_INVALID;
+          if (!f) continue;
+          any = true;
+          if (!std::isfinite(s.c10[q]) || !std::isfinite(s.c12h[q]) || s.c10[q] != s.c10[qt] ||
+              s.c12h[q] != s.c12h[qt] || s.c10[q] != sys[0].c10[q] || s.c12h[q] != sys[0].c12h[q])
+            return JP_E_INVALID;
+        }
+      if (any && prm->cal15m == JP_CAL15M_CMM) return JP_E_INVALID;
+    }
     for (int i = 0; i < s.ntors; ++i) {
       int n = (int)std::lround(s.tors_nrot[i]);
       if (n < 1 || n > 6 || s.tors_div[i] == 0) return JP_E_INVALID;
@@ -425,11 +450,28 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   const int nt1 = ntype + 1;
   std::vector<float2> ljf(nt1 * nt1, make_float2(0.f, 0.f));
   std::vector<double2> ljd(nt1 * nt1, make_double2(0.0, 0.0));
+  // H-bond type pairs: (C10, C12h) and their flags; the pair kernels' 12-6 table is zero
+  // there (those pairs keep only their Coulomb term in the tiles), the 1-4 table is not
+  std::vector<double2> hbt(nt1 * nt1, make_double2(0.0, 0.0));
+  std::vector<int> hbp(nt1 * nt1, 0), hbty(nt1, 0);
   for (int i = 0; i < ntype; ++i)
     for (int j = 0; j < ntype; ++j) {
-      ljd[i * nt1 + j] = make_double2(sys[0].c6[i * ntype + j], sys[0].c12[i * ntype + j]);
-      ljf[i * nt1 + j] = make_float2((float)sys[0].c6[i * ntype + j], (float)sys[0].c12[i * ntype + j]);
+      const int q = i * ntype + j;
+      ljd[i * nt1 + j] = make_double2(sys[0].c6[q], sys[0].c12[q]);
+      ljf[i * nt1 + j] = make_float2((float)sys[0].c6[q], (float)sys[0].c12[q]);
+      if (sys[0].hbond && sys[0].hbond[q]) {
+        hbt[i * nt1 + j] = make_double2(sys[0].c10[q], sys[0].c12h[q]);
+        hbp[i * nt1 + j] = 1;
+        hbty[i] = 1;
+      }
     }
+  const std::vector<double2> lj14 = ljd;
+  for (int q = 0; q < nt1 * nt1; ++q)
+    if (hbp[q]) {
+      ljd[q] = make_double2(0.0, 0.0);
+      ljf[q] = make_float2(0.f, 0.f);
+    }
+  c->hbond = std::find(hbp.begin(), hbp.end(), 1) != hbp.end();
   int atom0 = 0, blk0 = 0, key0 = 0, sub0 = 0, col0 = 0;
   std::vector<int> hcol_rep;
   for (int r = 0; r < nrep; ++r) {
@@ -939,6 +981,21 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.step_ctr, 2);
   e |= dput(c, &P.lj_f, ljf);
   e |= dput(c, &P.lj_d, ljd);
+  e |= dput(c, &P.lj14, lj14);
+  if (c->hbond) {
+    // listed pairs of an atom are bounded by the atoms within the list radius at a density
+    // of 0.2 per A^3 (liquid water holds 0.1); each marked pair is counted at both atoms
+    long long nhb = 0;
+    for (int a = 0; a < N; ++a) nhb += hbty[htyp[a] & kTypeMask];
+    const double rl = rc + 1.5;
+    const long long per = (long long)std::ceil(0.2 * 4.0 / 3.0 * std::acos(-1.0) * rl * rl * rl);
+    c->hb_cap = (int)std::min<long long>(std::max<long long>(nhb * per, 1024), 1LL << 30);
+    e |= dput(c, &P.hb_tab, hbt);
+    e |= dput(c, &P.hb_pair, hbp);
+    e |= dput(c, &P.hb_type, hbty);
+    e |= dalloc(c, &P.hb_list, (size_t)c->hb_cap);
+    e |= dalloc(c, &P.hb_n, 1);
+  }
   e |= dalloc(c, &c->scan_scratch,
               (size_t)std::max(std::max(c->nkeys, c->ncol), c->nchunk) / 1024 + 4);
   if (e) { jp_destroy(c); return JP_E_CUDA; }

@@ -19,48 +19,6 @@ struct Img {
 };
 
 template <bool FP64>
-__device__ __forceinline__ void add_grad(const DevPtrs& P, double fs, int a, double gx, double gy,
-                                         double gz) {
-  gx *= fs; gy *= fs; gz *= fs;   // ALSD class weight (1 otherwise)
-  if (FP64) {
-    atomicAdd(&P.grd[3 * a + 0], gx);
-    atomicAdd(&P.grd[3 * a + 1], gy);
-    atomicAdd(&P.grd[3 * a + 2], gz);
-  } else {
-    atomic_add_ll(&P.frc[3 * a + 0], to_fix(gx, kFrcScale));
-    atomic_add_ll(&P.frc[3 * a + 1], to_fix(gy, kFrcScale));
-    atomic_add_ll(&P.frc[3 * a + 2], to_fix(gz, kFrcScale));
-  }
-}
-
-// warp-aggregated energy add keyed by (replica, slot)
-__device__ __forceinline__ void add_energy(const DevPtrs& P, int rep, int slot, double e) {
-  const int key = rep * 16 + slot;
-  const unsigned full = 0xffffffffu;
-  const int k0 = __shfl_sync(full, key, 0);
-  const bool uni = __all_sync(full, key == k0);
-  if (uni) {
-    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(full, e, o);
-    if ((threadIdx.x & 31) == 0) atomic_add_ll(&P.ene_fix[key], to_fix(e, kEneScale));
-  } else if (e != 0.0) {
-    atomic_add_ll(&P.ene_fix[key], to_fix(e, kEneScale));
-  }
-}
-
-// warp-aggregated add of a term's energy to its replica's ALSD class total
-__device__ __forceinline__ void add_cls_energy(const DevPtrs& P, int rep, int cls, double e) {
-  const int key = rep * 4 + cls;
-  const unsigned full = 0xffffffffu;
-  const int k0 = __shfl_sync(full, key, 0);
-  if (__all_sync(full, key == k0)) {
-    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(full, e, o);
-    if ((threadIdx.x & 31) == 0 && e != 0.0) atomic_add_ll(&P.ene_cls[key], to_fix(e, kEneScale));
-  } else if (e != 0.0) {
-    atomic_add_ll(&P.ene_cls[key], to_fix(e, kEneScale));
-  }
-}
-
-template <bool FP64>
 __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb, double zf,
                                                 int alsd) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -202,7 +160,7 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
         const double r146 = r14 * r14 * r14;
         const double r1412 = r146 * r146;
         // p0 = svdw, p1 = sele*ccoef*q1*q4, a[2] = LJ table index
-        const double2 lj = P.lj_d[T.a[2]];
+        const double2 lj = P.lj14[T.a[2]];
         const double co6 = lj.x * r146, co12 = lj.y * r1412;
         e1 = T.p0 * (-co6 + co12);
         double coef = r14 * T.p0 * (-2.0 * co12 + co6) * 6.0;

@@ -178,9 +178,17 @@ struct DevPtrs {
   double *ene_hist;               // [max_steps][nrep][15]
   double *temp_hist;              // [max_steps][nrep]
   int *step_ctr;                  // device step counter (idloop)
-  // LJ table
-  float2 *lj_f;                   // (C6, C12) [(nt+1)^2]
+  // LJ tables [(nt+1)^2]: the pair kernels' (C6, C12), zero for H-bond type pairs; the
+  // 1-4 terms' (C6, C12) of every type pair
+  float2 *lj_f;
   double2 *lj_d;
+  double2 *lj14;
+  // H-bond 10-12 term: (C10, C12h) and flag per type pair, flag per type; the listed
+  // H-bond pairs (atom ids) of the last rebuild and their count
+  double2 *hb_tab;
+  int *hb_pair, *hb_type;
+  int2 *hb_list;
+  int *hb_n;
 };
 
 __device__ __forceinline__ long long to_fix(double v, double scale) {
@@ -192,5 +200,49 @@ __device__ __forceinline__ void atomic_add_ll(long long *p, long long v) {
 }
 
 __host__ __device__ __forceinline__ double anint(double x) { return round(x); }
+
+// gradient of one atom from a term evaluated in FP64, times its ALSD class weight fs:
+// FP64 atomics on the FP64 path, 64-bit fixed point on the mixed path
+template <bool FP64>
+__device__ __forceinline__ void add_grad(const DevPtrs& P, double fs, int a, double gx, double gy,
+                                         double gz) {
+  gx *= fs; gy *= fs; gz *= fs;   // ALSD class weight (1 otherwise)
+  if (FP64) {
+    atomicAdd(&P.grd[3 * a + 0], gx);
+    atomicAdd(&P.grd[3 * a + 1], gy);
+    atomicAdd(&P.grd[3 * a + 2], gz);
+  } else {
+    atomic_add_ll(&P.frc[3 * a + 0], to_fix(gx, kFrcScale));
+    atomic_add_ll(&P.frc[3 * a + 1], to_fix(gy, kFrcScale));
+    atomic_add_ll(&P.frc[3 * a + 2], to_fix(gz, kFrcScale));
+  }
+}
+
+// warp-aggregated energy add keyed by (replica, slot)
+__device__ __forceinline__ void add_energy(const DevPtrs& P, int rep, int slot, double e) {
+  const int key = rep * 16 + slot;
+  const unsigned full = 0xffffffffu;
+  const int k0 = __shfl_sync(full, key, 0);
+  const bool uni = __all_sync(full, key == k0);
+  if (uni) {
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(full, e, o);
+    if ((threadIdx.x & 31) == 0) atomic_add_ll(&P.ene_fix[key], to_fix(e, kEneScale));
+  } else if (e != 0.0) {
+    atomic_add_ll(&P.ene_fix[key], to_fix(e, kEneScale));
+  }
+}
+
+// warp-aggregated add of a term's energy to its replica's ALSD class total
+__device__ __forceinline__ void add_cls_energy(const DevPtrs& P, int rep, int cls, double e) {
+  const int key = rep * 4 + cls;
+  const unsigned full = 0xffffffffu;
+  const int k0 = __shfl_sync(full, key, 0);
+  if (__all_sync(full, key == k0)) {
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(full, e, o);
+    if ((threadIdx.x & 31) == 0 && e != 0.0) atomic_add_ll(&P.ene_cls[key], to_fix(e, kEneScale));
+  } else if (e != 0.0) {
+    atomic_add_ll(&P.ene_cls[key], to_fix(e, kEneScale));
+  }
+}
 
 }  // namespace jp

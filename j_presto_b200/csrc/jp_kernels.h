@@ -45,6 +45,11 @@ void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count
 int pair_blocks_per_sm(bool fp64, int nt1);
 void launch_update_pos(const DevPtrs& P, int nslot, bool fp64, double qscale, cudaStream_t st);
 
+// H-bond 10-12 pairs (jp_hbond.cu): their list at a rebuild (after the tile list), their
+// term at every force evaluation
+void launch_hb_list(const DevPtrs& P, int cap, int nt1, int nblk, cudaStream_t st);
+void launch_hbond(const DevPtrs& P, int cap, double rc2, int nt1, bool fp64, bool alsd, cudaStream_t st);
+
 // bonded (jp_bonded.cu)
 void launch_bonded(const DevPtrs& P, int nterm, bool fp64, double zb, double zf, bool alsd,
                    cudaStream_t st);

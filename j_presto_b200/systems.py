@@ -537,6 +537,26 @@ def droplet(nres, nwat, seed=6, temp=300.0):
     return solvated_polymer(nres, nwat, box=box, seed=seed, temp=temp, sphere=radius)
 
 
+HBOND_PAIRS = ((T_H, T_O), (T_H, T_OW), (T_HW, T_O))   # donor H -- acceptor O
+
+
+def with_hbond(top, pairs=HBOND_PAIRS, r0=1.9, depth=0.5):
+    """A copy of `top` whose type pairs `pairs` take the 10-12 H-bond term
+    E = C12h/r^12 - C10/r^10 (iyppid = 2), with its minimum -depth kcal/mol at r0 A:
+    C10 = 6 depth r0^10, C12h = C10 r0^2 / 1.2."""
+    nt = int(top["ntype"])
+    hb = np.zeros((nt, nt), np.int32)
+    c10 = np.zeros((nt, nt))
+    c12h = np.zeros((nt, nt))
+    a10 = 6.0 * depth * r0 ** 10
+    for i, j in pairs:
+        for p, q in ((i, j), (j, i)):
+            hb[p, q] = 1
+            c10[p, q] = a10
+            c12h[p, q] = a10 * r0 * r0 / 1.2
+    return dict(top, hbond=hb, c10=c10, c12h=c12h)
+
+
 def mcmd_weight(e_min, e_max, ndeg=8, t_lo=280.0, t_hi=700.0, tempce=300.0):
     """McMD .nf weight with d ln n/dE = 1/(R T(E)), T linear from t_lo at e_min to t_hi at
     e_max, fitted by a degree-`ndeg` polynomial in x = (E - celw)/(ceup - celw) and

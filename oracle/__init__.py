@@ -75,6 +75,9 @@ class Oracle:
         self.top = top
         self.n = int(top["natom"])
         self.params = params if params is not None else abi.default_params(**kw)
+        hb = top.get("hbond")
+        if hb is not None and np.any(hb) and self.params.cal15m == abi.JP_CAL15M_CMM:
+            raise ValueError("the H-bond 10-12 pairs are restated for CAL15M= ZD and ATOM only")
         self._sys = abi.make_system(top, self._keep)
         self._h = lib().or_create(C.byref(self._sys), C.byref(self.params), int(nthreads))
 

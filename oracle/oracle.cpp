@@ -51,6 +51,9 @@ struct Ctx {
   std::vector<int> typ, mol;
   int ntype = 0;
   std::vector<double> c6, c12;
+  // H-bond type pairs (iyppid = 2) and their 10-12 parameters fynbpp(3:4,:,:); empty = none
+  std::vector<int> hbp;
+  std::vector<double> c10, c12h;
   std::vector<std::vector<int>> excl;  // sorted partner list per atom
   // cls: ALSD class of the term, 0 = AA, 1 = AB, 2 = BB (n_matrix, inpcls.f90:297-325);
   // 2 for every term without clusters
@@ -635,10 +638,10 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
   // per-thread gradient copies stand in for the OpenMP reduction(+:Tgrad).
   const int nt = c.nthreads;
   std::vector<double> tg((size_t)nt * 3 * n, 0.0);
-  double eel = 0.0, evdw = 0.0;
+  double eel = 0.0, evdw = 0.0, ehb = 0.0;
   double ec0 = 0.0, ec1 = 0.0, ec2 = 0.0;
   long long npair = 0;
-#pragma omp parallel num_threads(nt) reduction(+ : eel, evdw, npair, ec0, ec1, ec2)
+#pragma omp parallel num_threads(nt) reduction(+ : eel, evdw, ehb, npair, ec0, ec1, ec2)
   {
     double* G = tg.data() + (size_t)omp_get_thread_num() * 3 * n;
 #pragma omp for schedule(dynamic, 64)
@@ -665,12 +668,25 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
         const double epair = ee * (ddi + c.bcoeff * dd2 - c.zcore);
         eel += epair;
         int it2 = c.typ[j];
-        double v1 = c.c6[it2 * c.ntype + it1] * dd6i;
-        double v2 = c.c12[it2 * c.ntype + it1] * dd6i * dd6i;
-        evdw += -v1 + v2;
+        const int tp = it2 * c.ntype + it1;
+        double v1, v2, p1;
+        if (!c.hbp.empty() && c.hbp[tp]) {
+          // the itbhyd pairs (cutoff.f90:98-154): 10-12 instead of 12-6, into ehydcn
+          // (enear.f90:415-440, #ZD / #ACT lines)
+          const double dd10i = dd2i * dd2i * dd2i * dd2i * dd2i * co;
+          v1 = c.c10[tp] * dd10i;
+          v2 = c.c12h[tp] * dd10i * dd2i;
+          p1 = 10.0;
+          ehb += -v1 + v2;
+        } else {
+          v1 = c.c6[tp] * dd6i;
+          v2 = c.c12[tp] * dd6i * dd6i;
+          p1 = 6.0;
+          evdw += -v1 + v2;
+        }
         const int pc = c.pcls(i, j);
         (pc == 0 ? ec0 : pc == 1 ? ec1 : ec2) += epair + (-v1 + v2);
-        double cc = f[pc] * (ee * (dd2i * ddi - c.fcoeff) + (-6.0 * v1 + 12.0 * v2) * dd2i);
+        double cc = f[pc] * (ee * (dd2i * ddi - c.fcoeff) + (-p1 * v1 + 12.0 * v2) * dd2i);
         double fx = d[0] * cc, fy = d[1] * cc, fz = d[2] * cc;
         gwx += fx; gwy += fy; gwz += fz;
         G[3 * j] += fx; G[3 * j + 1] += fy; G[3 * j + 2] += fz;
@@ -711,6 +727,7 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
     }
   }
   ene[JP_E_VDW15] += evdw;
+  ene[JP_E_HBOND] += ehb;
   ene[JP_E_ELE15] += eel + c.dself + eexc;
   double tot = 0.0;
   for (int k = 1; k < JP_MAXENE; ++k) tot += ene[k];
@@ -1296,6 +1313,12 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
   c->ntype = s->ntype;
   c->c6.assign(s->c6, s->c6 + (size_t)s->ntype * s->ntype);
   c->c12.assign(s->c12, s->c12 + (size_t)s->ntype * s->ntype);
+  if (s->hbond) {
+    const size_t nt2 = (size_t)s->ntype * s->ntype;
+    c->hbp.assign(s->hbond, s->hbond + nt2);
+    c->c10.assign(s->c10, s->c10 + nt2);
+    c->c12h.assign(s->c12h, s->c12h + nt2);
+  }
   // exclusions (inpcls.f90:229-290 itab14)
   c->excl.assign(n, {});
   for (int i = 0; i < n; ++i) {
