@@ -32,7 +32,8 @@ extern "C" {
 /* energy slot indices (0-based) of eneval/enevcc, md_run dnergy.f90:17-35 */
 enum {
   JP_E_TOTAL = 0, JP_E_BOND = 1, JP_E_ANGLE = 2, JP_E_TORS = 3, JP_E_IMPR = 4,
-  JP_E_VDW14 = 5, JP_E_ELE14 = 6, JP_E_VDW15 = 7, JP_E_ELE15 = 8, JP_E_HBOND = 9
+  JP_E_VDW14 = 5, JP_E_ELE14 = 6, JP_E_VDW15 = 7, JP_E_ELE15 = 8, JP_E_HBOND = 9,
+  JP_E_POSRES = 10, JP_E_DISTRES = 11, JP_E_DIHERES = 12, JP_E_CAP = 13
 };
 
 /* precision of the force path */
@@ -109,6 +110,49 @@ typedef struct jp_ge_fit_params {
   int32_t neglect_low, neglect_high;  /* FneglectL/H: leave the border bins out of the fit */
 } jp_ge_fit_params;
 
+/* Restraints and the spherical CAP boundary of one replica (dneres.f90 dneres_PB/_CB,
+ * called from dnergy.f90:70-74).  The caller reads psr/dsr/dhr/CAPbound files as md_run
+ * does and passes the finished force constants.  Atom indices use jp_system.index_base.
+ * Energies go to the slots md_run uses (enevcc(11..14)): JP_E_POSRES .. JP_E_CAP; with
+ * ALSD they belong to class BB and are not scaled (grad(:,:,nfrg)). */
+typedef struct jp_restraints {
+  /* POSITI (dposc, dneres.f90:48-101): E = 1/2 sum k |x - ref|^2, minimum image under
+   * BOUNDA= PBC; k = fugcns = (mass *) delta * boltzk * T * w (psr.f90:214-216, inpmd.f90:547) */
+  int32_t npos;
+  const int32_t *pos_atom;     /* [npos] iugpnt */
+  const double *pos_k;         /* [npos] fugcns (kcal/mol/A^2) */
+  const double *pos_ref;       /* [npos][3] fucord of those atoms */
+  /* DISTAN (ddistc, dneres.f90:107-221): R = <r^-6>^(-1/6) over all pairs of group i x
+   * group j (minimum image); E = k_up (R^2 - up^2)^2 if R > up, k_lo (R^2 - lo^2)^2 if
+   * R < lo, else 0; k = boltzk * T * w / 2 * fudupr / fudlow */
+  int32_t ndist;
+  const int32_t *dist_iptr;    /* [ndist+1] CSR of group i's atoms (iuipnt) */
+  const int32_t *dist_iatom;
+  const int32_t *dist_jptr;    /* [ndist+1] CSR of group j's atoms (iujpnt) */
+  const int32_t *dist_jatom;
+  const double *dist_lo, *dist_up;     /* furlow, furupr (A) */
+  const double *dist_klo, *dist_kup;
+  /* DIHEDR (dcdihe, dneres.f90:227-378): phi in [0, 2 pi) as the torsion term defines it;
+   * outside [lo, up] E = k (phi - wall)^2 from the nearer wall, across 2 pi;
+   * k_up = boltzk T w / (2 fudelu^2), k_lo = boltzk T w / (2 fudell^2) */
+  int32_t ndihe;
+  const int32_t *dihe_atom;    /* [ndihe][4] iudhcp */
+  const double *dihe_lo, *dihe_up;     /* fucdlw, fucdup (radian, 0 <= lo <= up < 2 pi) */
+  const double *dihe_klo, *dihe_kup;
+  /* SETBOU sphere CAP (dnecap iufcap = 1, capshp = 1, dnecap.f90:80-122, :428-437), no
+   * minimum image: the centre of mass C of each group (a range of atoms, chains of the
+   * INCLUDE list) has E = 1/2 k (|C - centre| - radius)^2 outside the sphere, its gradient
+   * shared by the atoms in proportion to their mass; each listed solute atom has
+   * E = 1/2 k_atom (|x - centre| - radius_atom)^2 outside radius_atom = radius - BUFFER */
+  int32_t ncap_group;
+  const int32_t *cap_group;    /* [ncap_group][2] first and last atom (fechn) */
+  int32_t ncap_atom;
+  const int32_t *cap_atom;     /* [ncap_atom] iamcap */
+  double cap_center[3];        /* fxcbou */
+  double cap_radius, cap_k;            /* furcap, fukcap */
+  double cap_atom_radius, cap_atom_k;  /* furcap_pro, fukcap_pro */
+} jp_restraints;
+
 /* One replica's system: topology, parameters and coordinates.
  * Mirrors md_run's COMBAS/COMERG/COMMIS module arrays. */
 typedef struct jp_system {
@@ -161,6 +205,7 @@ typedef struct jp_system {
   const int32_t *hbond;        /* [ntype][ntype] 1 = iyppid 2, else 0; symmetric */
   const double *c10;           /* [ntype][ntype] fynbpp(3,:,:) of the marked pairs */
   const double *c12h;          /* [ntype][ntype] fynbpp(4,:,:) of the marked pairs */
+  const jp_restraints *restraints;   /* POSITI / DISTAN / DIHEDR / SETBOU; NULL = none */
 } jp_system;
 
 /* Run parameters shared by all replicas of a context (md.inp EXE> MD keywords). */

@@ -9,6 +9,7 @@ import numpy as np
 
 JP_MAXENE = 15
 JP_E_TOTAL, JP_E_VDW14, JP_E_VDW15, JP_E_ELE15, JP_E_HBOND = 0, 5, 7, 8, 9   # eneval slots
+JP_E_POSRES, JP_E_DISTRES, JP_E_DIHERES, JP_E_CAP = 10, 11, 12, 13
 JP_PREC_FP64, JP_PREC_MIXED = 0, 1
 JP_METHOD_CONS, JP_METHOD_MICR, JP_METHOD_CANO, JP_METHOD_GE = 1, 2, 3, 4
 JP_SHAKE_NONE, JP_SHAKE_HBON, JP_SHAKE_ALLB = 0, 1, 2
@@ -65,6 +66,19 @@ class JpGeFitParams(C.Structure):
                 ("neglect_low", C.c_int32), ("neglect_high", C.c_int32)]
 
 
+class JpRestraints(C.Structure):
+    _fields_ = [
+        ("npos", C.c_int32), ("pos_atom", _ip), ("pos_k", _dp), ("pos_ref", _dp),
+        ("ndist", C.c_int32), ("dist_iptr", _ip), ("dist_iatom", _ip), ("dist_jptr", _ip),
+        ("dist_jatom", _ip), ("dist_lo", _dp), ("dist_up", _dp), ("dist_klo", _dp), ("dist_kup", _dp),
+        ("ndihe", C.c_int32), ("dihe_atom", _ip), ("dihe_lo", _dp), ("dihe_up", _dp),
+        ("dihe_klo", _dp), ("dihe_kup", _dp),
+        ("ncap_group", C.c_int32), ("cap_group", _ip), ("ncap_atom", C.c_int32), ("cap_atom", _ip),
+        ("cap_center", C.c_double * 3), ("cap_radius", C.c_double), ("cap_k", C.c_double),
+        ("cap_atom_radius", C.c_double), ("cap_atom_k", C.c_double),
+    ]
+
+
 class JpSystem(C.Structure):
     _fields_ = [
         ("natom", C.c_int32), ("index_base", C.c_int32), ("box", C.c_double * 3),
@@ -80,7 +94,7 @@ class JpSystem(C.Structure):
         ("impr_phase", _dp), ("impr_div", _ip),
         ("nshake", C.c_int32), ("shake_n", _ip), ("shake_atoms", _ip), ("shake_dist", _dp),
         ("ge", C.POINTER(JpGe)), ("cluster", _ip), ("ext_cmm", C.POINTER(JpExtCmm)),
-        ("hbond", _ip), ("c10", _dp), ("c12h", _dp),
+        ("hbond", _ip), ("c10", _dp), ("c12h", _dp), ("restraints", C.POINTER(JpRestraints)),
     ]
 
 
@@ -189,12 +203,56 @@ def make_system(top, keep, cord=None, vel=None):
         s.hbond = _ptr(np.asarray(top["hbond"], np.int32), C.c_int32, keep)
         s.c10 = _ptr(top["c10"], C.c_double, keep)
         s.c12h = _ptr(top["c12h"], C.c_double, keep)
+    if top.get("restraints") is not None:
+        s.restraints = C.pointer(make_restraints(top["restraints"], keep))
     ge = top.get("ge")
     if ge is not None:
         g = make_ge(ge, keep)
         keep.append(g)
         s.ge = C.pointer(g)
     return s
+
+
+def make_restraints(rd, keep):
+    """JpRestraints from a dict: pos=(atoms, k, ref[n][3]); dist=(igroups, jgroups, lo, up,
+    klo, kup) with the groups as lists of atom lists; dihe=(atoms[n][4], lo, up, klo, kup);
+    cap=dict(center, radius, k, groups[n][2] first/last atom, atoms, atom_radius, atom_k)."""
+    r = JpRestraints()
+    if rd.get("pos") is not None:
+        atoms, k, ref = rd["pos"]
+        r.npos = len(atoms)
+        r.pos_atom = _ptr(atoms, C.c_int32, keep)
+        r.pos_k = _ptr(k, C.c_double, keep)
+        r.pos_ref = _ptr(np.asarray(ref, np.float64).reshape(-1), C.c_double, keep)
+    if rd.get("dist") is not None:
+        ig, jg, lo, up, klo, kup = rd["dist"]
+        r.ndist = len(ig)
+        r.dist_iptr = _ptr(np.concatenate([[0], np.cumsum([len(g) for g in ig])]), C.c_int32, keep)
+        r.dist_iatom = _ptr(np.concatenate([np.asarray(g, np.int32) for g in ig]), C.c_int32, keep)
+        r.dist_jptr = _ptr(np.concatenate([[0], np.cumsum([len(g) for g in jg])]), C.c_int32, keep)
+        r.dist_jatom = _ptr(np.concatenate([np.asarray(g, np.int32) for g in jg]), C.c_int32, keep)
+        r.dist_lo, r.dist_up = _ptr(lo, C.c_double, keep), _ptr(up, C.c_double, keep)
+        r.dist_klo, r.dist_kup = _ptr(klo, C.c_double, keep), _ptr(kup, C.c_double, keep)
+    if rd.get("dihe") is not None:
+        atoms, lo, up, klo, kup = rd["dihe"]
+        r.ndihe = len(atoms)
+        r.dihe_atom = _ptr(np.asarray(atoms, np.int32).reshape(-1), C.c_int32, keep)
+        r.dihe_lo, r.dihe_up = _ptr(lo, C.c_double, keep), _ptr(up, C.c_double, keep)
+        r.dihe_klo, r.dihe_kup = _ptr(klo, C.c_double, keep), _ptr(kup, C.c_double, keep)
+    cap = rd.get("cap")
+    if cap is not None:
+        groups = np.asarray(cap.get("groups", np.zeros((0, 2))), np.int32).reshape(-1, 2)
+        atoms = np.asarray(cap.get("atoms", []), np.int32)
+        r.ncap_group = len(groups)
+        r.cap_group = _ptr(groups.reshape(-1), C.c_int32, keep) if len(groups) else None
+        r.ncap_atom = len(atoms)
+        r.cap_atom = _ptr(atoms, C.c_int32, keep) if len(atoms) else None
+        r.cap_center[:] = [float(v) for v in cap["center"]]
+        r.cap_radius, r.cap_k = float(cap["radius"]), float(cap["k"])
+        r.cap_atom_radius = float(cap.get("atom_radius", 0.0))
+        r.cap_atom_k = float(cap.get("atom_k", 0.0))
+    keep.append(r)
+    return r
 
 
 def make_systems(tops, keep):

@@ -56,6 +56,7 @@ struct jp_ctx {
   bool cmm = false;                 // CAL15M= CMM
   bool hbond = false;               // some type pair has the 10-12 H-bond term
   int hb_cap = 0;                   // capacity of the H-bond pair list
+  int nres = 0;                     // restraint and CAP terms
   int cmm_ncell[6] = {0, 0, 0, 0, 0, 0};   // cells per level over all replicas
   int cmm_nlev = 0;                 // most levels of any replica
   int cano_grid = 1;
@@ -192,6 +193,7 @@ void enqueue_forces(jp_ctx *c, bool count, bool force_far = false) {
 
 void enqueue_bonded(jp_ctx *c) {
   launch_bonded(c->P, c->nterm, c->fp64, c->zc.bcoeff, c->zc.fcoeff, c->alsd, c->st);
+  launch_restraints(c->P, c->nres, c->fp64, c->alsd, c->st);
 }
 
 void enqueue_integrate(jp_ctx *c) {
@@ -213,6 +215,7 @@ int launches_per_step(const jp_ctx *c) {
   n += c->ic.ge_prescaled ? 1 : 0; // k_ge_scale
   n += c->cmm ? 2 : 0;             // k_cmm_far, k_cmm_energy
   n += c->hbond ? 1 : 0;           // k_hbond
+  n += c->nres > 0 ? 1 : 0;        // k_restraints
   return n;
 }
 
@@ -230,6 +233,7 @@ int capture(jp_ctx *c, cudaGraphExec_t *out, bool rebuild) {
     CK(cudaEventRecord(c->ev_fork, c->st));
     CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
     launch_bonded(c->P, c->nterm, c->fp64, c->zc.bcoeff, c->zc.fcoeff, c->alsd, c->st2);
+    launch_restraints(c->P, c->nres, c->fp64, c->alsd, c->st2);
     CK(cudaEventRecord(c->ev_join, c->st2));
     enqueue_pair(c, false);
     CK(cudaStreamWaitEvent(c->st, c->ev_join, 0));
@@ -350,6 +354,53 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
     for (int g = 0; g < s.nshake; ++g)
       for (int k = 0; k < s.shake_n[g]; ++k)
         if (!okatom(s.shake_atoms[4 * g + k])) return JP_E_INVALID;
+    if (s.restraints) {   // every array present for its count, indices in range, finite values
+      const jp_restraints &q = *s.restraints;
+      auto fin = [](double v) { return std::isfinite(v); };
+      if (q.npos < 0 || q.ndist < 0 || q.ndihe < 0 || q.ncap_group < 0 || q.ncap_atom < 0)
+        return JP_E_INVALID;
+      if (q.npos && (!q.pos_atom || !q.pos_k || !q.pos_ref)) return JP_E_INVALID;
+      for (int i = 0; i < q.npos; ++i)
+        if (!okatom(q.pos_atom[i]) || !fin(q.pos_k[i]) || !fin(q.pos_ref[3 * i]) ||
+            !fin(q.pos_ref[3 * i + 1]) || !fin(q.pos_ref[3 * i + 2]))
+          return JP_E_INVALID;
+      if (q.ndist && (!q.dist_iptr || !q.dist_iatom || !q.dist_jptr || !q.dist_jatom || !q.dist_lo ||
+                      !q.dist_up || !q.dist_klo || !q.dist_kup || q.dist_iptr[0] != 0 || q.dist_jptr[0] != 0))
+        return JP_E_INVALID;
+      for (int i = 0; i < q.ndist; ++i) {
+        // non-empty groups without a common atom (r = 0 would make <r^-6> infinite)
+        if (q.dist_iptr[i + 1] <= q.dist_iptr[i] || q.dist_jptr[i + 1] <= q.dist_jptr[i]) return JP_E_INVALID;
+        if (!fin(q.dist_lo[i]) || !fin(q.dist_up[i]) || !(q.dist_lo[i] <= q.dist_up[i]) ||
+            !fin(q.dist_klo[i]) || !fin(q.dist_kup[i]))
+          return JP_E_INVALID;
+        for (int p = q.dist_iptr[i]; p < q.dist_iptr[i + 1]; ++p) {
+          if (!okatom(q.dist_iatom[p])) return JP_E_INVALID;
+          for (int u = q.dist_jptr[i]; u < q.dist_jptr[i + 1]; ++u)
+            if (!okatom(q.dist_jatom[u]) || q.dist_jatom[u] == q.dist_iatom[p]) return JP_E_INVALID;
+        }
+      }
+      if (q.ndihe && (!q.dihe_atom || !q.dihe_lo || !q.dihe_up || !q.dihe_klo || !q.dihe_kup))
+        return JP_E_INVALID;
+      for (int i = 0; i < q.ndihe; ++i) {
+        for (int k = 0; k < 4; ++k) if (!okatom(q.dihe_atom[4 * i + k])) return JP_E_INVALID;
+        if (!fin(q.dihe_lo[i]) || !fin(q.dihe_up[i]) || !(q.dihe_lo[i] <= q.dihe_up[i]) ||
+            !fin(q.dihe_klo[i]) || !fin(q.dihe_kup[i]))
+          return JP_E_INVALID;
+      }
+      if (q.ncap_group || q.ncap_atom) {   // dnecap is called from dneres_CB only
+        if (prm->bounda != JP_BOUND_NONE) return JP_E_INVALID;
+        if (!fin(q.cap_center[0]) || !fin(q.cap_center[1]) || !fin(q.cap_center[2]) ||
+            !(q.cap_radius >= 0.0) || !(q.cap_atom_radius >= 0.0) || !fin(q.cap_radius) ||
+            !fin(q.cap_atom_radius) || !fin(q.cap_k) || !fin(q.cap_atom_k))
+          return JP_E_INVALID;
+        if ((q.ncap_group && !q.cap_group) || (q.ncap_atom && !q.cap_atom)) return JP_E_INVALID;
+        for (int i = 0; i < q.ncap_group; ++i)
+          if (!okatom(q.cap_group[2 * i]) || !okatom(q.cap_group[2 * i + 1]) ||
+              q.cap_group[2 * i] > q.cap_group[2 * i + 1])
+            return JP_E_INVALID;
+        for (int i = 0; i < q.ncap_atom; ++i) if (!okatom(q.cap_atom[i])) return JP_E_INVALID;
+      }
+    }
     if (s.ge && (s.ge->nwindow < 1 || s.ge->ndeg < 0 || s.ge->nwindow > JP_GE_MAX_WINDOWS ||
                  s.ge->ndeg > JP_GE_MAX_DEG || !s.ge->coef || !s.ge->low || !s.ge->high))
       return JP_E_INVALID;
@@ -473,6 +524,8 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     }
   c->hbond = std::find(hbp.begin(), hbp.end(), 1) != hbp.end();
   int atom0 = 0, blk0 = 0, key0 = 0, sub0 = 0, col0 = 0;
+  std::vector<Restr> hres;          // restraints and CAP terms of all replicas
+  std::vector<int> hres_idx;        // atoms of the distance-restraint groups
   std::vector<int> hcol_rep;
   for (int r = 0; r < nrep; ++r) {
     const jp_system &s = sys[r];
@@ -830,6 +883,65 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       R.ge_upper = s.ge->upper;
       pack_ge(*s.ge, hge.data() + R.ge_off);
     }
+    if (s.restraints) {   // dneres: POSITI, DISTAN, DIHEDR, SETBOU sphere CAP
+      const jp_restraints &q = *s.restraints;
+      auto item = [&](int kind) {
+        Restr t;
+        std::memset(&t, 0, sizeof(t));
+        t.kind = kind;
+        t.rep = r;
+        return t;
+      };
+      for (int i = 0; i < q.npos; ++i) {
+        Restr t = item(R_POS);
+        t.a[0] = atom0 + q.pos_atom[i] - b;
+        for (int k = 0; k < 3; ++k) t.p[k] = q.pos_ref[3 * i + k];
+        t.p[3] = q.pos_k[i];
+        hres.push_back(t);
+      }
+      for (int i = 0; i < q.ndist; ++i) {
+        Restr t = item(R_DIST);
+        t.a[0] = (int)hres_idx.size();
+        for (int p = q.dist_iptr[i]; p < q.dist_iptr[i + 1]; ++p) hres_idx.push_back(atom0 + q.dist_iatom[p] - b);
+        t.a[1] = t.a[2] = (int)hres_idx.size();
+        for (int p = q.dist_jptr[i]; p < q.dist_jptr[i + 1]; ++p) hres_idx.push_back(atom0 + q.dist_jatom[p] - b);
+        t.a[3] = (int)hres_idx.size();
+        t.p[0] = q.dist_lo[i];
+        t.p[1] = q.dist_up[i];
+        t.p[2] = q.dist_klo[i];
+        t.p[3] = q.dist_kup[i];
+        hres.push_back(t);
+      }
+      for (int i = 0; i < q.ndihe; ++i) {
+        Restr t = item(R_DIHE);
+        for (int k = 0; k < 4; ++k) t.a[k] = atom0 + q.dihe_atom[4 * i + k] - b;
+        t.p[0] = q.dihe_lo[i];
+        t.p[1] = q.dihe_up[i];
+        t.p[2] = q.dihe_klo[i];
+        t.p[3] = q.dihe_kup[i];
+        hres.push_back(t);
+      }
+      for (int i = 0; i < q.ncap_group; ++i) {
+        Restr t = item(R_CAPG);
+        t.a[0] = atom0 + q.cap_group[2 * i] - b;
+        t.a[1] = atom0 + q.cap_group[2 * i + 1] - b;
+        double m = 0.0;
+        for (int a = q.cap_group[2 * i] - b; a <= q.cap_group[2 * i + 1] - b; ++a) m += s.mass[a];
+        for (int k = 0; k < 3; ++k) t.p[k] = q.cap_center[k];
+        t.p[3] = q.cap_radius;
+        t.p[4] = q.cap_k;
+        t.p[5] = 1.0 / m;
+        hres.push_back(t);
+      }
+      for (int i = 0; i < q.ncap_atom; ++i) {
+        Restr t = item(R_CAPA);
+        t.a[0] = atom0 + q.cap_atom[i] - b;
+        for (int k = 0; k < 3; ++k) t.p[k] = q.cap_center[k];
+        t.p[3] = q.cap_atom_radius;
+        t.p[4] = q.cap_atom_k;
+        hres.push_back(t);
+      }
+    }
     atom0 += n;
     blk0 += R.nblk;
   }
@@ -982,6 +1094,11 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dput(c, &P.lj_f, ljf);
   e |= dput(c, &P.lj_d, ljd);
   e |= dput(c, &P.lj14, lj14);
+  c->nres = (int)hres.size();
+  if (c->nres) {
+    e |= dput(c, &P.restr, hres);
+    if (!hres_idx.empty()) e |= dput(c, &P.res_idx, hres_idx);
+  }
   if (c->hbond) {
     // listed pairs of an atom are bounded by the atoms within the list radius at a density
     // of 0.2 per A^3 (liquid water holds 0.1); each marked pair is counted at both atoms

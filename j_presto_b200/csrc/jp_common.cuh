@@ -106,6 +106,17 @@ struct Term {
   int cls;                 // ALSD class 0 = AA, 1 = AB, 2 = BB
 };
 
+// restraint or CAP term of one replica (jp_restraint.cu); atoms are global ids
+enum : int { R_POS = 0, R_DIST = 1, R_DIHE = 2, R_CAPG = 3, R_CAPA = 4 };
+struct Restr {
+  int kind;
+  int rep;
+  int a[4];        // POS, CAPA: atom | DIST: group i = res_idx[a0, a1), group j = res_idx[a2, a3)
+                   // | DIHE: the four atoms | CAPG: first and last atom of the group
+  double p[6];     // POS: ref xyz, k | DIST, DIHE: lo, up, k_lo, k_up
+                   // | CAPG, CAPA: centre xyz, radius, k (CAPG: p[5] = 1 / group mass)
+};
+
 struct DevPtrs {
   // atoms
   double *x, *v, *x0, *vback, *xback, *forcec;
@@ -189,6 +200,9 @@ struct DevPtrs {
   int *hb_pair, *hb_type;
   int2 *hb_list;
   int *hb_n;
+  // restraints and CAP terms, and the atoms of the distance-restraint groups
+  Restr *restr;
+  int *res_idx;
 };
 
 __device__ __forceinline__ long long to_fix(double v, double scale) {

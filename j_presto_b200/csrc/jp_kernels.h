@@ -50,6 +50,9 @@ void launch_update_pos(const DevPtrs& P, int nslot, bool fp64, double qscale, cu
 void launch_hb_list(const DevPtrs& P, int cap, int nt1, int nblk, cudaStream_t st);
 void launch_hbond(const DevPtrs& P, int cap, double rc2, int nt1, bool fp64, bool alsd, cudaStream_t st);
 
+// restraints and CAP boundary (jp_restraint.cu)
+void launch_restraints(const DevPtrs& P, int n, bool fp64, bool alsd, cudaStream_t st);
+
 // bonded (jp_bonded.cu)
 void launch_bonded(const DevPtrs& P, int nterm, bool fp64, double zb, double zf, bool alsd,
                    cudaStream_t st);

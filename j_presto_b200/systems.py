@@ -557,6 +557,63 @@ def with_hbond(top, pairs=HBOND_PAIRS, r0=1.9, depth=0.5):
     return dict(top, hbond=hb, c10=c10, c12h=c12h)
 
 
+def with_restraints(top, seed=3, cap=False, kt=0.596):
+    """A copy of `top` with restraints on its solute, as psr/dsr/dhr files would give them
+    (constants folded as md_run folds them, kt = boltzk * 300 K): position restraints on
+    the first heavy atoms, pulled 0.3 A off their reference; distance restraints between
+    solute atoms and atom pairs, half of them violated; dihedral restraints on backbone-like
+    quadruples whose [lo, up] misses the current angle.  cap=True adds the sphere CAP of
+    the included waters (centre of mass of each O-H-H triple) and of the solute heavy atoms
+    around the centroid, for BOUNDA= NO."""
+    rng = np.random.default_rng(seed)
+    x = np.asarray(top["cord"], float)
+    t = np.asarray(top["atype"])
+    heavy = np.flatnonzero(np.isin(t, (T_C, T_N, T_O)))
+    pos_atoms = heavy[:12]
+    ref = x[pos_atoms] + rng.normal(size=(len(pos_atoms), 3)) * 0.3
+    rd = dict(pos=(pos_atoms.astype(np.int32), np.full(len(pos_atoms), 5.0), ref))
+    ig, jg, lo, up = [], [], [], []
+    for k in range(6):
+        a, b = heavy[3 * k], heavy[3 * k + 10]
+        grp_i = [a] if k % 2 == 0 else [a, heavy[3 * k + 1]]
+        grp_j = [b]
+        r = np.linalg.norm(x[a] - x[b])
+        ig.append(grp_i)
+        jg.append(grp_j)
+        if k % 3 == 0:
+            lo.append(r + 1.0); up.append(r + 3.0)       # too short: the lower wall
+        elif k % 3 == 1:
+            lo.append(r - 4.0); up.append(r - 1.0)       # too long: the upper wall
+        else:
+            lo.append(r - 1.0); up.append(r + 1.0)       # satisfied
+    nd = len(ig)
+    dscc = kt * 0.5
+    rd["dist"] = (ig, jg, np.array(lo), np.array(up), np.full(nd, dscc * 0.2), np.full(nd, dscc * 0.3))
+    quads, dlo, dup = [], [], []
+    for k in range(4):
+        q = heavy[2 * k:2 * k + 4]
+        b1, b2, b3 = x[q[1]] - x[q[0]], x[q[2]] - x[q[1]], x[q[3]] - x[q[2]]
+        n1, n2 = np.cross(b1, b2), np.cross(b2, b3)
+        phi = np.arctan2(np.dot(np.cross(n1, n2), b2) / np.linalg.norm(b2), np.dot(n1, n2)) % (2 * np.pi)
+        w = np.radians(40.0)
+        c0 = (phi + np.radians(60.0 + 30.0 * k)) % (2 * np.pi)   # a window away from phi
+        quads.append(q)
+        dlo.append(max(0.0, c0 - w / 2))
+        dup.append(min(2 * np.pi - 1e-9, c0 + w / 2))
+    nh = len(quads)
+    dhk = kt * 1.0 / 2.0
+    rd["dihe"] = (np.array(quads, np.int32), np.array(dlo), np.array(dup),
+                  np.full(nh, dhk / np.radians(10.0) ** 2), np.full(nh, dhk / np.radians(10.0) ** 2))
+    if cap:
+        ow = np.flatnonzero(t == T_OW)
+        centre = x.mean(0)
+        rmax = np.linalg.norm(x - centre, axis=1).max()
+        rd["cap"] = dict(center=centre, radius=0.85 * rmax, k=2.0,
+                         groups=np.stack([ow, ow + 2], 1).astype(np.int32),
+                         atoms=heavy.astype(np.int32), atom_radius=0.85 * rmax - 4.0, atom_k=2.0)
+    return dict(top, restraints=rd)
+
+
 def mcmd_weight(e_min, e_max, ndeg=8, t_lo=280.0, t_hi=700.0, tempce=300.0):
     """McMD .nf weight with d ln n/dE = 1/(R T(E)), T linear from t_lo at e_min to t_hi at
     e_max, fitted by a degree-`ndeg` polynomial in x = (E - celw)/(ceup - celw) and

@@ -51,6 +51,16 @@ struct Ctx {
   std::vector<int> typ, mol;
   int ntype = 0;
   std::vector<double> c6, c12;
+  // restraints (dneres.f90) and the sphere CAP (dnecap.f90); atom indices 0-based
+  struct PosRes { int a; double k, ref[3]; };
+  struct DistRes { std::vector<int> gi, gj; double lo, up, klo, kup; };
+  struct DiheRes { int a[4]; double lo, up, klo, kup; };
+  std::vector<PosRes> posres;
+  std::vector<DistRes> distres;
+  std::vector<DiheRes> diheres;
+  std::vector<std::pair<int, int>> cap_groups;   // first, last atom (fechn)
+  std::vector<int> cap_atoms;                    // iamcap
+  double cap_c[3] = {0, 0, 0}, cap_r = 0, cap_k = 0, cap_ra = 0, cap_ka = 0;
   // H-bond type pairs (iyppid = 2) and their 10-12 parameters fynbpp(3:4,:,:); empty = none
   std::vector<int> hbp;
   std::vector<double> c10, c12h;
@@ -469,6 +479,151 @@ void cmm_far(Ctx& c, const double* x) {
 }
 
 // ---------------------------------------------------------------------------------------
+// dneres_PB / dneres_CB (dneres.f90:2-43): position (dposc :48-101), distance (ddistc
+// :107-221) and dihedral (dcdihe :227-378) restraints, then the sphere CAP (dnecap.f90
+// :80-122, :428-437; called from dneres_CB only).  Gradients unscaled (grad(:,:,nfrg)),
+// energies into enevcc(11..14) and the BB class.
+// ---------------------------------------------------------------------------------------
+void restraints(Ctx& c, const double* x, double* ene, double* grad) {
+  double epos = 0.0;
+  for (const auto& r : c.posres) {
+    double d[3];
+    for (int k = 0; k < 3; ++k) d[k] = x[3 * r.a + k] - r.ref[k];
+    minimg(c, d);
+    epos += r.k * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    for (int k = 0; k < 3; ++k) grad[3 * r.a + k] += r.k * d[k];
+  }
+  epos *= 0.5;
+  double enoe = 0.0;
+  for (const auto& r : c.distres) {
+    auto sep = [&](int p, int q, double* d) {
+      for (int k = 0; k < 3; ++k) d[k] = x[3 * p + k] - x[3 * q + k];
+      minimg(c, d);
+      return d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    };
+    const double npair = (double)(r.gi.size() * r.gj.size());
+    double tot = 0.0, d[3];
+    for (int p : r.gi)
+      for (int q : r.gj) {
+        const double r2 = sep(p, q, d);
+        tot += 1.0 / (r2 * r2 * r2);
+      }
+    const double rave = std::pow(tot / npair, -1.0 / 6.0);
+    double r0 = 1.0, cst = 0.0;
+    if (rave > r.up) { r0 = r.up; cst = r.kup; }
+    else if (rave < r.lo) { r0 = r.lo; cst = r.klo; }
+    const double dr2 = rave * rave - r0 * r0;
+    enoe += cst * dr2 * dr2;
+    if (rave >= r.lo && rave <= r.up) continue;
+    const double coef = 4.0 * cst * dr2 * std::pow(rave, 8) / npair;
+    for (int side = 0; side < 2; ++side) {
+      const auto& A = side ? r.gj : r.gi;
+      const auto& B = side ? r.gi : r.gj;
+      for (int p : A) {
+        double td[3] = {0, 0, 0};
+        for (int q : B) {
+          const double r2 = sep(p, q, d);
+          const double r8i = 1.0 / (r2 * r2 * r2 * r2);
+          for (int k = 0; k < 3; ++k) td[k] += d[k] * r8i;
+        }
+        for (int k = 0; k < 3; ++k) grad[3 * p + k] += coef * td[k];
+      }
+    }
+  }
+  double edhc = 0.0;
+  for (const auto& r : c.diheres) {
+    const int* ia = r.a;
+    double d21[3], d32[3], d43[3];
+    for (int k = 0; k < 3; ++k) {
+      d21[k] = x[3 * ia[1] + k] - x[3 * ia[0] + k];
+      d32[k] = x[3 * ia[2] + k] - x[3 * ia[1] + k];
+      d43[k] = x[3 * ia[3] + k] - x[3 * ia[2] + k];
+    }
+    minimg(c, d21);
+    minimg(c, d32);
+    minimg(c, d43);
+    double p12[3] = {d21[1] * d32[2] - d32[1] * d21[2], d21[2] * d32[0] - d32[2] * d21[0],
+                     d21[0] * d32[1] - d32[0] * d21[1]};
+    double p23[3] = {d32[1] * d43[2] - d43[1] * d32[2], d32[2] * d43[0] - d43[2] * d32[0],
+                     d32[0] * d43[1] - d43[0] * d32[1]};
+    double r12 = p12[0] * p12[0] + p12[1] * p12[1] + p12[2] * p12[2];
+    double r23 = p23[0] * p23[0] + p23[1] * p23[1] + p23[2] * p23[2];
+    double r12r23 = std::sqrt(r12 * r23);
+    if (r12r23 <= 0.0) continue;
+    r12r23 = 1.0 / r12r23;
+    const double s1223 = p12[0] * p23[0] + p12[1] * p23[1] + p12[2] * p23[2];
+    const double cosp = std::max(std::min(s1223 * r12r23, 1.0), -1.0);
+    const double p123[3] = {p12[1] * p23[2] - p23[1] * p12[2], p12[2] * p23[0] - p23[2] * p12[0],
+                            p12[0] * p23[1] - p23[0] * p12[1]};
+    const double s32123 = d32[0] * p123[0] + d32[1] * p123[1] + d32[2] * p123[2];
+    double phi = std::acos(cosp);
+    if (s32123 < 0.0) phi = 2.0 * kPi - phi;
+    double phi0 = 0.0, phi1 = 0.0, cons0 = 0.0, cons1 = 0.0;
+    if (phi > r.up) { phi0 = r.up; phi1 = r.lo + 2.0 * kPi; cons0 = r.kup; cons1 = r.klo; }
+    else if (phi < r.lo) { phi0 = r.up - 2.0 * kPi; phi1 = r.lo; cons0 = r.kup; cons1 = r.klo; }
+    const double dl0 = phi - phi0, dl1 = phi1 - phi;
+    double dphi, cst;
+    if (dl0 < dl1) { dphi = dl0; cst = cons0; }
+    else { dphi = -dl1; cst = cons1; }
+    edhc += cst * dphi * dphi;
+    if (std::fabs(phi) < kEps || std::fabs(phi - kPi) < kEps) continue;
+    const double q12 = s1223 / r12, q23 = s1223 / r23;
+    const double wr = -2.0 * cst * dphi / std::sin(phi) * r12r23;
+    const double w1 = d21[0] + d32[0], w2 = d21[1] + d32[1], w3 = d21[2] + d32[2];
+    double w[9];
+    w[0] = d32[2] * p23[1] - d32[1] * p23[2] - q12 * (d32[2] * p12[1] - d32[1] * p12[2]);
+    w[1] = d32[0] * p23[2] - d32[2] * p23[0] - q12 * (d32[0] * p12[2] - d32[2] * p12[0]);
+    w[2] = d32[1] * p23[0] - d32[0] * p23[1] - q12 * (d32[1] * p12[0] - d32[0] * p12[1]);
+    w[3] = -w3 * p23[1] + d43[2] * p12[1] + w2 * p23[2] - d43[1] * p12[2] -
+           q12 * (-w3 * p12[1] + w2 * p12[2]) - q23 * (d43[2] * p23[1] - d43[1] * p23[2]);
+    w[4] = w3 * p23[0] - d43[2] * p12[0] - w1 * p23[2] + d43[0] * p12[2] -
+           q12 * (w3 * p12[0] - w1 * p12[2]) - q23 * (d43[0] * p23[2] - d43[2] * p23[0]);
+    w[5] = -w2 * p23[0] + d43[1] * p12[0] + w1 * p23[1] - d43[0] * p12[1] -
+           q12 * (-w2 * p12[0] + w1 * p12[1]) - q23 * (d43[1] * p23[0] - d43[0] * p23[1]);
+    w[6] = d32[2] * p12[1] - d32[1] * p12[2] - q23 * (d32[2] * p23[1] - d32[1] * p23[2]);
+    w[7] = d32[0] * p12[2] - d32[2] * p12[0] - q23 * (d32[0] * p23[2] - d32[2] * p23[0]);
+    w[8] = d32[1] * p12[0] - d32[0] * p12[1] - q23 * (d32[1] * p23[0] - d32[0] * p23[1]);
+    for (int k = 0; k < 3; ++k) {
+      grad[3 * ia[0] + k] += wr * w[k];
+      grad[3 * ia[1] + k] += wr * w[3 + k];
+      grad[3 * ia[2] + k] -= wr * (w[k] + w[3 + k] + w[6 + k]);
+      grad[3 * ia[3] + k] += wr * w[6 + k];
+    }
+  }
+  double ecap = 0.0;
+  for (const auto& g : c.cap_groups) {   // centre of mass of each included chain
+    double m = 0.0, C[3] = {0, 0, 0};
+    for (int a = g.first; a <= g.second; ++a) {
+      m += c.mass[a];
+      for (int k = 0; k < 3; ++k) C[k] += c.mass[a] * x[3 * a + k];
+    }
+    for (int k = 0; k < 3; ++k) C[k] = C[k] / m - c.cap_c[k];
+    const double dist = C[0] * C[0] + C[1] * C[1] + C[2] * C[2];
+    if (dist <= c.cap_r * c.cap_r) continue;
+    const double d = std::sqrt(dist), over = d - c.cap_r;
+    ecap += c.cap_k * over * over;
+    const double rt = c.cap_k * over / d;
+    for (int a = g.first; a <= g.second; ++a)
+      for (int k = 0; k < 3; ++k) grad[3 * a + k] += C[k] * rt * (c.mass[a] / m);
+  }
+  for (int a : c.cap_atoms) {
+    double T[3];
+    for (int k = 0; k < 3; ++k) T[k] = x[3 * a + k] - c.cap_c[k];
+    const double dist = T[0] * T[0] + T[1] * T[1] + T[2] * T[2];
+    if (dist <= c.cap_ra * c.cap_ra) continue;
+    const double d = std::sqrt(dist), over = d - c.cap_ra;
+    ecap += c.cap_ka * over * over;
+    for (int k = 0; k < 3; ++k) grad[3 * a + k] += c.cap_ka * over / d * T[k];
+  }
+  ecap *= 0.5;
+  ene[JP_E_POSRES] += epos;
+  ene[JP_E_DISTRES] += enoe;
+  ene[JP_E_DIHERES] += edhc;
+  ene[JP_E_CAP] += ecap;
+  c.ecls[2] += epos + enoe + edhc + ecap;
+}
+
+// ---------------------------------------------------------------------------------------
 // dnergy (dnergy.f90:2-84) -> dnergv_PB (dnergv.f90:2-59): bonds, angles, torsions,
 // impropers, 1-4, then cmmdo -> enear_ZD_redu_PB (enear.f90, #ZD #REDU #PB lines).
 // ene[15] gets enevcc(:,1); grad = dE/dx.
@@ -633,6 +788,8 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
       grad[3 * p.j + k] -= f[p.cls] * w[k];
     }
   }
+
+  restraints(c, x, ene, grad);
 
   // ZD + LJ pair loop: enear_ZD_redu_PB (enear.f90:107-257, #ZD #REDU #PB lines),
   // per-thread gradient copies stand in for the OpenMP reduction(+:Tgrad).
@@ -1318,6 +1475,31 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
     c->hbp.assign(s->hbond, s->hbond + nt2);
     c->c10.assign(s->c10, s->c10 + nt2);
     c->c12h.assign(s->c12h, s->c12h + nt2);
+  }
+  if (s->restraints) {
+    const jp_restraints& q = *s->restraints;
+    for (int i = 0; i < q.npos; ++i)
+      c->posres.push_back({q.pos_atom[i] - b, q.pos_k[i],
+                           {q.pos_ref[3 * i], q.pos_ref[3 * i + 1], q.pos_ref[3 * i + 2]}});
+    for (int i = 0; i < q.ndist; ++i) {
+      Ctx::DistRes d;
+      for (int p = q.dist_iptr[i]; p < q.dist_iptr[i + 1]; ++p) d.gi.push_back(q.dist_iatom[p] - b);
+      for (int p = q.dist_jptr[i]; p < q.dist_jptr[i + 1]; ++p) d.gj.push_back(q.dist_jatom[p] - b);
+      d.lo = q.dist_lo[i]; d.up = q.dist_up[i]; d.klo = q.dist_klo[i]; d.kup = q.dist_kup[i];
+      c->distres.push_back(d);
+    }
+    for (int i = 0; i < q.ndihe; ++i) {
+      Ctx::DiheRes d;
+      for (int k = 0; k < 4; ++k) d.a[k] = q.dihe_atom[4 * i + k] - b;
+      d.lo = q.dihe_lo[i]; d.up = q.dihe_up[i]; d.klo = q.dihe_klo[i]; d.kup = q.dihe_kup[i];
+      c->diheres.push_back(d);
+    }
+    for (int i = 0; i < q.ncap_group; ++i)
+      c->cap_groups.push_back({q.cap_group[2 * i] - b, q.cap_group[2 * i + 1] - b});
+    for (int i = 0; i < q.ncap_atom; ++i) c->cap_atoms.push_back(q.cap_atom[i] - b);
+    for (int k = 0; k < 3; ++k) c->cap_c[k] = q.cap_center[k];
+    c->cap_r = q.cap_radius; c->cap_k = q.cap_k;
+    c->cap_ra = q.cap_atom_radius; c->cap_ka = q.cap_atom_k;
   }
   // exclusions (inpcls.f90:229-290 itab14)
   c->excl.assign(n, {});
