@@ -62,8 +62,10 @@ enum {
   JP_E_NOALLOC_LIMIT = -110,      /* natom above JP_NOALLOC_MAX_ATOMS (jp_nonbond_noalloc) */
   JP_E_STOP_MASS = -121,          /* remotv ier=-1: the stopped atoms have no mass */
   JP_E_STOP_SINGULAR = -122,      /* remotv ier=-2: their inertia tensor is singular */
-  JP_E_FREE_WINDOW = -130         /* BOUNDA= NO: an atom left the window the context was
+  JP_E_FREE_WINDOW = -130,        /* BOUNDA= NO: an atom left the window the context was
                                      built for (re-create it from the current state) */
+  JP_E_MIN_STEP = -140            /* steep.f90:235-243 ier=-2: the step length fell below
+                                     1e-10 A per degree of freedom */
 };
 
 /* Generalized-ensemble weight (.nf file, md_run inmcmd.f90:22-40; verlethe.f90:196-321). */
@@ -406,6 +408,38 @@ int jp_ge_set_mlp(jp_ctx *ctx, int32_t replica, const float *params);
 
 const char *jp_strerror(int code);
 void jp_destroy(jp_ctx *ctx);
+
+/* Energy minimisation (EXE> MIN, mini.f90 runmin -> steep.f90 steep/linsrd): steepest
+ * descent with an adaptive step length.  Each iteration moves every atom along
+ * -grad/|grad| (the whole replica's gradient normalised) by the step length, applies SHAKE
+ * to the moved positions when the context has SHAKE groups, evaluates dnergy, and
+ * multiplies the step length by `up` when the energy fell, else by `down`; the move is kept
+ * either way.  It stops when the RMS gradient sqrt(sum |g|^2 / natom) <= convgr (checked
+ * before each move), after max_loop iterations, when the step length falls below 1e-10 A
+ * per degree of freedom (JP_E_MIN_STEP) or when SHAKE fails.  The pair list is rebuilt
+ * every `update` iterations and once at the end.  METHOD= CONJ is not built. */
+enum { JP_MIN_STEEP = 1 };
+typedef struct jp_min_params {
+  int32_t method;        /* JP_MIN_STEEP (METHOD= STEE) */
+  int32_t max_loop;      /* LOOPLI: iterations (force evaluations after the first), >= 1 */
+  int32_t update;        /* UPDATE: list rebuild interval in iterations (default 10) */
+  double convgr;         /* CONVGR: RMS gradient threshold, kcal/mol/A (default 0.1) */
+  double step0;          /* ISTEPL: initial step length per atom, A (default 0.01); the
+                            step length starts at step0 * sqrt(natom) */
+  double up, down;       /* step-length factors (md_run defaults 1.2 and 0.6) */
+} jp_min_params;
+
+void jp_default_min_params(jp_min_params *p);
+
+/* Minimise every replica of the context at once, each with its own step length and stop
+ * condition (md_run minimises one system; replicas here are independent).  Per replica
+ * (arrays of nrep, each may be NULL): iters = iterations done, eneval[JP_MAXENE] = the
+ * energies of the last evaluation, rmsf = its RMS gradient, state = 0 still running at
+ * max_loop, 1 converged, 2 step length too small.  Returns JP_OK, JP_E_MIN_STEP if any
+ * replica ended with state 2, or the SHAKE codes (a SHAKE failure stops every replica).
+ * Velocities are left as they were. */
+int jp_minimize(jp_ctx *ctx, const jp_min_params *mp, int32_t *iters, double *eneval,
+                double *rmsf, int32_t *state);
 
 /* Largest system jp_nonbond_noalloc accepts: its static scratch array holds
  * 32 + 3 * JP_NOALLOC_MAX_ATOMS doubles (384.25 KiB) on each device. */

@@ -79,6 +79,26 @@ class JpRestraints(C.Structure):
     ]
 
 
+JP_MIN_STEEP = 1
+JP_E_MIN_STEP = -140
+
+
+class JpMinParams(C.Structure):
+    _fields_ = [("method", C.c_int32), ("max_loop", C.c_int32), ("update", C.c_int32),
+                ("convgr", C.c_double), ("step0", C.c_double), ("up", C.c_double), ("down", C.c_double)]
+
+
+def min_params(**kw):
+    """jp_min_params with md_run's EXE> MIN defaults (inpmin.f90), overridden by kw."""
+    p = JpMinParams(method=JP_MIN_STEEP, max_loop=1000, update=10, convgr=0.1, step0=0.01, up=1.2,
+                    down=0.6)
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
 class JpSystem(C.Structure):
     _fields_ = [
         ("natom", C.c_int32), ("index_base", C.c_int32), ("box", C.c_double * 3),

@@ -16,7 +16,7 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libjpgpu.so")
 SOURCES = ["jp_cells.cu", "jp_pair.cu", "jp_bonded.cu", "jp_integrate.cu", "jp_calib.cu", "jp_abi.cu",
            "jp_noalloc.cu", "jp_gefit.cpp", "jp_mlp.cu", "jp_cmm.cu", "jp_hbond.cu",
-           "jp_restraint.cu"]
+           "jp_restraint.cu", "jp_minimize.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -465,6 +465,7 @@ const char *jp_strerror(int code) {
     case JP_E_FREE_WINDOW: return "BOUNDA= NO: an atom left the window of the context (re-create it)";
     case JP_E_STOP_MASS: return "centre-of-mass stop: the stopped atoms have no mass";
     case JP_E_STOP_SINGULAR: return "centre-of-mass stop: inertia tensor of the stopped atoms is singular";
+    case JP_E_MIN_STEP: return "minimisation: the step length fell below 1e-10 A per degree of freedom";
     default: return "unknown error";
   }
 }
@@ -1388,6 +1389,100 @@ int jp_set_timing(jp_ctx *c, int enable) {
   if (!c) return JP_E_INVALID;
   c->tm.enabled = enable != 0;
   return JP_OK;
+}
+
+void jp_default_min_params(jp_min_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->method = JP_MIN_STEEP;   // inpmin.f90 defaults: METHOD= STEE, UPDATE 10, CONVGR 0.1,
+  p->max_loop = 1000;         // ISTEPL 0.01, step-length factors 1.2 / 0.6
+  p->update = 10;
+  p->convgr = 0.1;
+  p->step0 = 0.01;
+  p->up = 1.2;
+  p->down = 0.6;
+}
+
+int jp_minimize(jp_ctx *c, const jp_min_params *mp, int32_t *iters, double *eneval, double *rmsf,
+                int32_t *state) {
+  if (!c || !mp) return JP_E_INVALID;
+  if (mp->method != JP_MIN_STEEP || mp->max_loop < 1 || mp->update < 0 || !(mp->convgr >= 0.0) ||
+      !(mp->step0 > 0.0) || !(mp->up > 0.0) || !(mp->down > 0.0) || !std::isfinite(mp->convgr) ||
+      !std::isfinite(mp->step0) || !std::isfinite(mp->up) || !std::isfinite(mp->down))
+    return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  if (!c->P.mins && dalloc(c, &c->P.mins, (size_t)c->nrep)) return JP_E_CUDA;
+  DevPtrs &P = c->P;
+  cudaStream_t st = c->st;
+  const bool shake = c->prm.shake_method != JP_SHAKE_NONE && c->nunit > 0;
+  const int nmax = mp->max_loop;
+  CK(cudaMemsetAsync(P.mins, 0, sizeof(MinState) * c->nrep, st));
+  // the first evaluation (mini.f90 inimin) at the current positions
+  enqueue_zero(c, false);
+  enqueue_pair(c, false, true);
+  enqueue_bonded(c);
+  launch_min_init(P, c->natom, c->nrep, c->fp64, mp->step0, mp->convgr, st);
+  // one linsrd iteration of every replica, replayed as a graph
+  cudaGraph_t g;
+  cudaGraphExec_t gx = nullptr;
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  launch_min_move(P, c->natom, c->fp64, nmax, shake, st);
+  if (shake) {
+    launch_shake_only(P, c->ic, 0, c->nunit, st);
+    launch_min_commit(P, c->natom, nmax, st);
+  }
+  launch_update_pos(P, c->nslot, c->fp64, c->qscale, st);
+  enqueue_zero(c, false);
+  enqueue_pair(c, false, true);   // CMM: the far field at every evaluation
+  enqueue_bonded(c);
+  launch_min_decide(P, c->natom, c->nrep, c->fp64, nmax, mp->up, mp->down, mp->convgr, st);
+  CK(cudaStreamEndCapture(st, &g));
+  const cudaError_t ie = cudaGraphInstantiate(&gx, g, 0);
+  cudaGraphDestroy(g);
+  CK(ie);
+  std::vector<MinState> hs(c->nrep);
+  int it = 0;
+  cudaError_t err = cudaSuccess;
+  while (it < nmax && err == cudaSuccess) {
+    const int chunk = std::min(nmax - it, 64);
+    for (int k = 0; k < chunk && err == cudaSuccess; ++k) {
+      err = cudaGraphLaunch(gx, st);
+      ++it;
+      if (mp->update > 0 && it % mp->update == 0) enqueue_rebuild(c);   // steep.f90:51-54
+    }
+    if (err != cudaSuccess) break;
+    unsigned stat = 0;
+    err = cudaMemcpyAsync(&stat, P.status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(hs.data(), P.mins, sizeof(MinState) * c->nrep,
+                                                  cudaMemcpyDeviceToHost, st);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    if (err != cudaSuccess || stat != 0) break;
+    bool running = false;
+    for (const MinState &m : hs) running |= m.state == 0 && m.iters < nmax;
+    if (!running) break;
+  }
+  cudaGraphExecDestroy(gx);
+  CK(err);
+  // leave what the MD step expects: zero accumulators and a list built at these positions
+  if (c->fp64) CK(cudaMemsetAsync(P.grd, 0, sizeof(double) * 3 * c->natom, st));
+  else CK(cudaMemsetAsync(P.frc, 0, sizeof(long long) * 3 * c->natom, st));
+  CK(cudaMemsetAsync(P.ene_fix, 0, sizeof(long long) * (16 * c->nrep + 1), st));
+  enqueue_rebuild(c);
+  CK(cudaMemcpyAsync(hs.data(), P.mins, sizeof(MinState) * c->nrep, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  CK(cudaGetLastError());
+  bool step_err = false;
+  for (int r = 0; r < c->nrep; ++r) {
+    const MinState &m = hs[r];
+    if (iters) iters[r] = m.iters;
+    if (rmsf) rmsf[r] = m.rmsf;
+    if (state) state[r] = m.state;
+    if (eneval) std::memcpy(eneval + (size_t)r * JP_MAXENE, m.ene, sizeof(m.ene));
+    step_err |= m.state == 2;
+  }
+  const int rs = check_status(c);
+  if (rs != JP_OK) return rs;
+  return step_err ? JP_E_MIN_STEP : JP_OK;
 }
 
 int jp_set_grid_limit(jp_ctx *c, int32_t blocks) {

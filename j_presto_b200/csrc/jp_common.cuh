@@ -117,6 +117,17 @@ struct Restr {
                    // | CAPG, CAPA: centre xyz, radius, k (CAPG: p[5] = 1 / group mass)
 };
 
+// steepest-descent minimisation state of one replica (jp_minimize.cu)
+struct MinState {
+  double stp;               // step length (A, whole replica)
+  double e_old;             // total energy of the last evaluation
+  double gsum, gsum_new;    // sum |g|^2 of the last evaluation / being summed
+  double rmsf;              // sqrt(gsum / natom)
+  int state;                // 0 running, 1 converged, 2 step length too small
+  int iters;                // iterations done
+  double ene[JP_MAXENE];    // energies of the last evaluation
+};
+
 struct DevPtrs {
   // atoms
   double *x, *v, *x0, *vback, *xback, *forcec;
@@ -203,6 +214,7 @@ struct DevPtrs {
   // restraints and CAP terms, and the atoms of the distance-restraint groups
   Restr *restr;
   int *res_idx;
+  MinState *mins;                 // [nrep], allocated by the first jp_minimize
 };
 
 __device__ __forceinline__ long long to_fix(double v, double scale) {

@@ -53,6 +53,14 @@ void launch_hbond(const DevPtrs& P, int cap, double rc2, int nt1, bool fp64, boo
 // restraints and CAP boundary (jp_restraint.cu)
 void launch_restraints(const DevPtrs& P, int n, bool fp64, bool alsd, cudaStream_t st);
 
+// steepest-descent minimisation (jp_minimize.cu)
+void launch_min_init(const DevPtrs& P, int natom, int nrep, bool fp64, double step0, double convgr,
+                     cudaStream_t st);
+void launch_min_move(const DevPtrs& P, int natom, bool fp64, int max_loop, bool shake, cudaStream_t st);
+void launch_min_commit(const DevPtrs& P, int natom, int max_loop, cudaStream_t st);
+void launch_min_decide(const DevPtrs& P, int natom, int nrep, bool fp64, int max_loop, double up,
+                       double down, double convgr, cudaStream_t st);
+
 // bonded (jp_bonded.cu)
 void launch_bonded(const DevPtrs& P, int nterm, bool fp64, double zb, double zf, bool alsd,
                    cudaStream_t st);

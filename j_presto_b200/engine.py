@@ -23,7 +23,8 @@ EXPORTS = ["jp_default_params", "jp_create", "jp_rebuild_cells", "jp_energy_grad
            "jp_strerror", "jp_destroy", "jp_nonbond_noalloc", "jp_ge_hist_setup",
            "jp_ge_hist_get", "jp_ge_set", "jp_lstsq_windows", "jp_ge_fit", "jp_ge_dlnn",
            "jp_mlp_nparam", "jp_mlp_init", "jp_mlp_train", "jp_mlp_forward", "jp_ge_set_mlp",
-           "jp_get_lambda", "jp_set_lambda", "jp_set_grid_limit"]
+           "jp_get_lambda", "jp_set_lambda", "jp_set_grid_limit", "jp_default_min_params",
+           "jp_minimize"]
 
 
 class JpError(RuntimeError):
@@ -80,6 +81,10 @@ def lib():
         L.jp_ge_set_mlp.argtypes = [vp, ip, fp_]
         L.jp_get_lambda.argtypes = [vp, ip, dp, dp]
         L.jp_set_lambda.argtypes = [vp, ip, C.c_double, C.c_double]
+        L.jp_default_min_params.argtypes = [C.POINTER(abi.JpMinParams)]
+        L.jp_default_min_params.restype = None
+        L.jp_minimize.argtypes = [vp, C.POINTER(abi.JpMinParams), C.POINTER(C.c_int32), dp, dp,
+                                  C.POINTER(C.c_int32)]
         # all array arguments are device addresses except box (host double[3])
         L.jp_nonbond_noalloc.argtypes = [ip, vp, vp, vp, ip, vp, vp, vp, vp, ip, dp, C.c_double,
                                          C.c_double, vp, vp, vp]
@@ -293,6 +298,20 @@ class Engine:
         code = _chk(lib().jp_step(self._h, int(nsteps), _dp(e), _dp(t)), "jp_step", warn_ok)
         self.last_code = code
         return e, t
+
+    def minimize(self, warn_ok=False, **kw):
+        """Steepest descent of every replica (jp_minimize); kw override the md_run defaults
+        (max_loop, update, convgr, step0, up, down).  Returns per replica (iters, energies,
+        rms gradient, state); JpError for JP_E_MIN_STEP or a SHAKE failure."""
+        mp = abi.min_params(**kw)
+        it = np.zeros(self.nrep, np.int32)
+        st = np.zeros(self.nrep, np.int32)
+        e = np.zeros((self.nrep, abi.JP_MAXENE))
+        rm = np.zeros(self.nrep)
+        code = lib().jp_minimize(self._h, C.byref(mp), it.ctypes.data_as(C.POINTER(C.c_int32)), _dp(e),
+                                 _dp(rm), st.ctypes.data_as(C.POINTER(C.c_int32)))
+        self.last_code = _chk(code, "jp_minimize", warn_ok)
+        return it, e, rm, st
 
     def shake(self, r1, r2, rep=0):
         r1 = np.ascontiguousarray(r1, np.float64).copy()

@@ -47,6 +47,9 @@ def lib():
         L.or_temperature.argtypes = [vp, dp]
         L.or_temperature.restype = C.c_double
         L.or_run.argtypes = [vp, C.c_int, dp, dp]
+        ipp = C.POINTER(C.c_int)
+        L.or_minimize.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                  ipp, dp, dp, ipp]
         L.or_mcmd_scale.argtypes = [vp, C.c_double]
         L.or_mcmd_scale.restype = C.c_double
         L.or_get_lambda.argtypes = [vp, dp, dp]
@@ -147,6 +150,15 @@ class Oracle:
         l2, ec = np.zeros(2), np.zeros(3)
         lib().or_get_lambda(self._h, _dp(l2), _dp(ec))
         return l2, ec
+
+    def minimize(self, max_loop=1000, update=10, convgr=0.1, step0=0.01, up=1.2, down=0.6):
+        """steep (steep.f90) on this replica: (ier, iters, energies, rms gradient, state)."""
+        it, st = C.c_int(), C.c_int()
+        e = np.zeros(abi.JP_MAXENE)
+        rm = C.c_double()
+        ier = lib().or_minimize(self._h, int(max_loop), int(update), float(convgr), float(step0),
+                                float(up), float(down), C.byref(it), _dp(e), C.byref(rm), C.byref(st))
+        return ier, it.value, e, rm.value, st.value
 
     def set_lambda(self, lam, lam_v=0.0):
         lib().or_set_lambda(self._h, float(lam), float(lam_v))

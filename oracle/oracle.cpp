@@ -1778,6 +1778,61 @@ double or_temperature(void* h, const double* v) {
   return caltmp(*c, v ? v : c->vel.data());
 }
 
+// steepest-descent minimisation: steep (steep.f90:2-92) with linsrd (:98-246), RMS gradient
+// by calrsf (calrsf.f90), search direction by mksrdg (-grad / |grad|).  All atoms variable;
+// returns ier (0, steep's -2 for a vanishing step, SHAKE's code); iters, ene, rmsf, state
+// (0 loop limit, 1 converged, 2 step too small) describe the end.
+int or_minimize(void* h, int max_loop, int update, double convgr, double step0, double up, double down,
+                int* iters, double* ene_out, double* rmsf_out, int* state) {
+  Ctx* c = (Ctx*)h;
+  const int n = c->n;
+  double* x = c->cord.data();
+  std::vector<double> g(3 * (size_t)n), xref;
+  double ene[JP_MAXENE];
+  auto evaluate = [&]() {
+    c->itwin = true;
+    energy_grad(*c, x, ene, g.data());
+  };
+  auto gsum = [&]() {
+    double s2 = 0.0;
+    for (double v : g) s2 += v * v;
+    return s2;
+  };
+  evaluate();
+  double stp = step0 * std::sqrt((double)n);
+  int iloop = 0, ier = 0, st = 0;
+  double rmsf = std::sqrt(gsum() / n);
+  const bool shake = c->prm.shake_method != JP_SHAKE_NONE && !(c->sk2.empty() && c->sk3.empty() && c->sk4.empty());
+  for (;;) {
+    if (rmsf <= convgr) { st = 1; break; }
+    const double conv = -1.0 / std::sqrt(gsum());
+    const double epold = ene[JP_E_TOTAL];
+    if (shake) xref.assign(x, x + 3 * (size_t)n);
+    for (int k = 0; k < 3 * n; ++k) x[k] += stp * conv * g[k];
+    if (shake) {
+      ier = shake_all(*c, x, xref.data());
+      if (ier != 0) break;
+    }
+    ++iloop;
+    evaluate();
+    rmsf = std::sqrt(gsum() / n);
+    if (ene[JP_E_TOTAL] < epold) {
+      stp *= up;
+    } else {
+      stp *= down;
+      if (stp / std::sqrt(3.0 * n) < kEps) { st = 2; ier = -2; break; }
+    }
+    if (update > 0 && iloop % update == 0) build_list(*c);
+    if (iloop == max_loop) break;
+  }
+  if (iters) *iters = iloop;
+  if (ene_out) std::memcpy(ene_out, ene, sizeof(ene));
+  if (rmsf_out) *rmsf_out = rmsf;
+  if (state) *state = st;
+  build_list(*c);
+  return ier;
+}
+
 // nsteps of runmd (md.f90:519-694): verlet or verlethe, then celprp every UPDATE steps.
 int or_run(void* h, int nsteps, double* ene_out, double* temp_out) {
   Ctx* c = (Ctx*)h;
