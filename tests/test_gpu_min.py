@@ -4,8 +4,9 @@ convergence, replicas minimised together equal to each alone, MD continuing from
 minimised state, the stop on a vanishing step and the parameter checks.
 
 Tolerances: FP64 positions within 1e-8 A and energies 1e-8 relative of the oracle after the
-same number of iterations (the step-length decisions compare energies, which agree to far
-better than the differences between successive iterations).
+same number of iterations (with SHAKE, its convergence tolerance: 1e-6 A, energies 1e-6
+relative); the step-length decisions compare energies, which agree to far better than the
+differences between successive iterations.
 """
 import numpy as np
 import pytest
@@ -43,10 +44,16 @@ def _pair(eng_mod, top, nloop, prm=None, **kw):
 
 @pytest.mark.parametrize("shake", [abi.JP_SHAKE_NONE, abi.JP_SHAKE_HBON])
 def test_fp64_iterations_vs_oracle(eng_mod, poly, shake):
-    xo, eo, ro, x, ene, rm = _pair(eng_mod, poly, 25, shake_method=shake)
-    assert np.abs(x - xo).max() < 1e-8
-    np.testing.assert_allclose(ene, eo, rtol=1e-8, atol=1e-7)
-    np.testing.assert_allclose(rm, ro, rtol=1e-8)
+    """ISTEPL 0.002: with the default 0.01 the step length grows to moves that the SHAKE of
+    the reference cannot follow on this unrelaxed system (the exact two-atom solution has
+    no real root), in the engine and the oracle alike."""
+    xo, eo, ro, x, ene, rm = _pair(eng_mod, poly, 25, prm=dict(step0=0.002), shake_method=shake)
+    # with SHAKE each iteration's constraint solution is exact only to COVSHK (1e-6 of d0^2),
+    # and the iterative 3-atom solutions may stop one iteration apart: 1e-6 A
+    exact = shake == abi.JP_SHAKE_NONE
+    assert np.abs(x - xo).max() < (1e-8 if exact else 1e-6)
+    np.testing.assert_allclose(ene, eo, rtol=1e-8 if exact else 1e-6, atol=1e-7 if exact else 1e-4)
+    np.testing.assert_allclose(rm, ro, rtol=1e-8 if exact else 1e-5)
 
 
 def test_restraints_enter_the_minimisation(eng_mod, poly):
@@ -58,13 +65,15 @@ def test_restraints_enter_the_minimisation(eng_mod, poly):
 
 def test_converges_then_md_continues(eng_mod, poly):
     """Minimise to convergence, then 5 MD steps: the engine leaves zero accumulators and a
-    list built at the minimised positions, as the oracle's rebuild does."""
-    o = oracle.Oracle(poly, method=CANO)
+    list built at the minimised positions, as the oracle's rebuild does.  Without SHAKE:
+    steepest descent does not project the constraint forces out of the gradient, so with
+    SHAKE the RMS gradient stalls well above this threshold."""
+    o = oracle.Oracle(poly, method=CANO, shake_method=NOSHAKE)
     ier, it, eo, ro, so = o.minimize(max_loop=400, convgr=8.0)
     assert ier == 0 and so == 1
     assert o.run(5)[0] == 0
     xo = o.get_state()[0]
-    with eng_mod.Engine(poly, precision=FP64, method=CANO) as e:
+    with eng_mod.Engine(poly, precision=FP64, method=CANO, shake_method=NOSHAKE) as e:
         its, ene, rm, st = e.minimize(max_loop=400, convgr=8.0)
         assert its[0] == it and st[0] == 1 and rm[0] <= 8.0
         e.step(5)
@@ -74,7 +83,7 @@ def test_converges_then_md_continues(eng_mod, poly):
 
 def test_replicas_minimise_independently(eng_mod, poly):
     other = dict(systems.solvated_polymer(20, 1500, seed=11))
-    kw = dict(max_loop=15, update=5, convgr=0.0)
+    kw = dict(max_loop=15, update=5, convgr=0.0, step0=0.002)
     singles = []
     for t in (poly, other):
         with eng_mod.Engine(t, precision=FP64, method=CANO) as e:
@@ -91,9 +100,10 @@ def test_replicas_minimise_independently(eng_mod, poly):
 def test_mixed_path_lowers_the_energy(eng_mod, poly):
     o = oracle.Oracle(poly, method=CANO)
     e0 = o.energy_grad()[0][0]
-    ier, it, eo, _, _ = o.minimize(max_loop=60)
+    ier, it, eo, _, _ = o.minimize(max_loop=60, step0=0.002)
+    assert ier == 0
     with eng_mod.Engine(poly, precision=MIXED, method=CANO) as e:
-        its, ene, rm, st = e.minimize(max_loop=60)
+        its, ene, rm, st = e.minimize(max_loop=60, step0=0.002)
     assert its[0] == 60 and st[0] == 0
     assert ene[0][0] < e0 - 0.5 * (e0 - eo[0])
 
@@ -101,7 +111,7 @@ def test_mixed_path_lowers_the_energy(eng_mod, poly):
 def test_vanishing_step_and_bad_parameters(eng_mod, poly):
     with eng_mod.Engine(poly, precision=FP64, method=CANO, shake_method=NOSHAKE) as e:
         with pytest.raises(eng_mod.JpError) as ex:
-            e.minimize(max_loop=10, step0=3.0, down=1e-12, convgr=0.0)
+            e.minimize(max_loop=10, step0=0.1, down=1e-12, convgr=0.0)   # E rises 2.8e3 -> 2.2e4
         assert ex.value.code == abi.JP_E_MIN_STEP
         for bad in (dict(max_loop=0), dict(step0=0.0), dict(convgr=-1.0), dict(method=2)):
             with pytest.raises(eng_mod.JpError) as ex:
