@@ -47,6 +47,8 @@ def lib():
         L.or_temperature.argtypes = [vp, dp]
         L.or_temperature.restype = C.c_double
         L.or_run.argtypes = [vp, C.c_int, dp, dp]
+        L.or_first_force.argtypes = [vp, dp, dp, dp]
+        L.or_first_force.restype = None
         ipp = C.POINTER(C.c_int)
         L.or_minimize.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                   ipp, dp, dp, ipp]
@@ -150,6 +152,15 @@ class Oracle:
         l2, ec = np.zeros(2), np.zeros(3)
         lib().or_get_lambda(self._h, _dp(l2), _dp(ec))
         return l2, ec
+
+    def first_force(self):
+        """(eneval, lambda_f, grad) as md_run's FDEBUG dumps them at the first step: the
+        gradient after verlethe's scaling (pseudo temperature, McMD weight, ALSD classes)."""
+        e = np.zeros(abi.JP_MAXENE)
+        g = np.zeros((self.n, 3))
+        lf = C.c_double()
+        lib().or_first_force(self._h, _dp(e), C.byref(lf), _dp(g))
+        return e, lf.value, g
 
     def minimize(self, max_loop=1000, update=10, convgr=0.1, step0=0.01, up=1.2, down=0.6):
         """steep (steep.f90) on this replica: (ier, iters, energies, rms gradient, state)."""

@@ -1262,6 +1262,32 @@ int step_verlet(Ctx& c, double* ene) {
 
 // One verlethe step (verlethe.f90:2-758), METHOD= CANO or GE (McMD), itmeth 1 or 2,
 // with the SHAKE <-> thermostat loop (icslop) and SHAKE-failure dt halving.
+// dnergy and verlethe's scaling of the gradient (verlethe.f90:103-321): the pseudo
+// temperature (CANO), the McMD weight (GE) or the ALSD class combination (done inside
+// energy_grad) with the lambda force; c.grad gets the gradient the integration uses, the
+// return value is lambda_f.  This is the state that FDEBUG dumps (verlethe.f90:325-387).
+double verlethe_force(Ctx& c, double* ene) {
+  double lambda_f = 0.0;
+  energy_grad(c, c.cord.data(), ene, c.grad.data());
+  if (c.alsd) {
+    // forces already combined by class (energy_grad); lambda force (verlethe.f90:289-320)
+    if (c.prm.method == JP_METHOD_GE) {
+      const double dew = alsd_dew(c);
+      if (c.alsd == JP_ALSD_LMD) lambda_f = -2.0 * c.ecls[0] * c.lam - c.ecls[1] - dew;
+      else lambda_f = -c.ecls[0] - 0.5 * c.ecls[1] / std::sqrt(c.lam) - dew;
+    }
+  } else if (c.prm.method == JP_METHOD_CANO) {
+    if (c.prm.psetmp > kEps) {
+      double dew = c.prm.temp / c.prm.psetmp;
+      for (auto& g : c.grad) g *= dew;
+    }
+  } else if (c.prm.method == JP_METHOD_GE) {
+    double dew = mcmd_scale(c, ene[JP_E_TOTAL]);
+    for (auto& g : c.grad) g *= dew;
+  }
+  return lambda_f;
+}
+
 int step_verlethe(Ctx& c, double* ene) {
   const int n = c.n;
   const double deltt = c.prm.dt;
@@ -1286,24 +1312,7 @@ int step_verlethe(Ctx& c, double* ene) {
     lmd_back = c.lam;
     lmd_vback = c.lam_v;
   redo:
-    lambda_f = 0.0;
-    energy_grad(c, c.cord.data(), ene, c.grad.data());
-    if (c.alsd) {
-      // forces already combined by class (energy_grad); lambda force (verlethe.f90:289-320)
-      if (c.prm.method == JP_METHOD_GE) {
-        const double dew = alsd_dew(c);
-        if (c.alsd == JP_ALSD_LMD) lambda_f = -2.0 * c.ecls[0] * c.lam - c.ecls[1] - dew;
-        else lambda_f = -c.ecls[0] - 0.5 * c.ecls[1] / std::sqrt(c.lam) - dew;
-      }
-    } else if (c.prm.method == JP_METHOD_CANO) {
-      if (c.prm.psetmp > kEps) {
-        double dew = temps / c.prm.psetmp;
-        for (auto& g : c.grad) g *= dew;
-      }
-    } else if (c.prm.method == JP_METHOD_GE) {
-      double dew = mcmd_scale(c, ene[JP_E_TOTAL]);
-      for (auto& g : c.grad) g *= dew;
-    }
+    lambda_f = verlethe_force(c, ene);
     double* g = c.grad.data();
     // velocity at 1/2 dt without SHAKE force (verlethe.f90:390-398)
     double rt = 0.5 * Tdeltt * kConvcv;
@@ -1772,6 +1781,21 @@ double or_cmm_far(void* h, double* gwk) {
 }
 
 int or_shake(void* h, double* r1, const double* r2) { return shake_all(*(Ctx*)h, r1, r2); }
+
+// what md_run's FDEBUG dumps to 1stp_force.bin at the first step (verlethe.f90:382-387):
+// eneval, lambda_f and the gradient after verlethe's scaling, at the current coordinates
+// (METHOD= CANO / GE; MICR and CONS have no dump: the plain gradient and lambda_f = 0)
+void or_first_force(void* h, double* ene, double* lambda_f, double* grad) {
+  Ctx* c = (Ctx*)h;
+  const bool keep = c->itwin;
+  c->itwin = true;
+  double lf = 0.0;
+  if (c->prm.method >= JP_METHOD_CANO) lf = verlethe_force(*c, ene);
+  else energy_grad(*c, c->cord.data(), ene, c->grad.data());
+  c->itwin = keep;
+  if (lambda_f) *lambda_f = lf;
+  if (grad) std::memcpy(grad, c->grad.data(), sizeof(double) * 3 * c->n);
+}
 
 double or_temperature(void* h, const double* v) {
   Ctx* c = (Ctx*)h;
