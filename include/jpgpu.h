@@ -208,6 +208,10 @@ typedef struct jp_system {
   const double *c10;           /* [ntype][ntype] fynbpp(3,:,:) of the marked pairs */
   const double *c12h;          /* [ntype][ntype] fynbpp(4,:,:) of the marked pairs */
   const jp_restraints *restraints;   /* POSITI / DISTAN / DIHEDR / SETBOU; NULL = none */
+  const int32_t *tors_unscaled;  /* [ntors] 1 = the torsion stays in class BB (unscaled) even
+                                    with JP_SCALE_TORS: SCALET's peptide-bond exemption
+                                    (scale_tor 2/3, incel.f90:846-866), which the caller
+                                    decides from atom and residue names; NULL = none */
 } jp_system;
 
 /* Run parameters shared by all replicas of a context (md.inp EXE> MD keywords). */

@@ -115,6 +115,7 @@ class JpSystem(C.Structure):
         ("nshake", C.c_int32), ("shake_n", _ip), ("shake_atoms", _ip), ("shake_dist", _dp),
         ("ge", C.POINTER(JpGe)), ("cluster", _ip), ("ext_cmm", C.POINTER(JpExtCmm)),
         ("hbond", _ip), ("c10", _dp), ("c12h", _dp), ("restraints", C.POINTER(JpRestraints)),
+        ("tors_unscaled", _ip),
     ]
 
 
@@ -223,6 +224,8 @@ def make_system(top, keep, cord=None, vel=None):
         s.hbond = _ptr(np.asarray(top["hbond"], np.int32), C.c_int32, keep)
         s.c10 = _ptr(top["c10"], C.c_double, keep)
         s.c12h = _ptr(top["c12h"], C.c_double, keep)
+    if top.get("tors_unscaled") is not None:
+        s.tors_unscaled = _ptr(top["tors_unscaled"], C.c_int32, keep)
     if top.get("restraints") is not None:
         s.restraints = C.pointer(make_restraints(top["restraints"], keep))
     ge = top.get("ge")

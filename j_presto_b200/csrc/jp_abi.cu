@@ -830,7 +830,8 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       t.p1 = s.tors_nrot[i];
       t.p2 = s.tors_phase[i];
       t.idiv = s.tors_div[i];
-      if (sct & JP_SCALE_TORS) t.cls = pcls(s.tors[4 * i + 1] - b, s.tors[4 * i + 2] - b);   // :838-845
+      if ((sct & JP_SCALE_TORS) && !(s.tors_unscaled && s.tors_unscaled[i]))   // :838-866
+        t.cls = pcls(s.tors[4 * i + 1] - b, s.tors[4 * i + 2] - b);
       terms_by_kind[T_TORS].push_back(t);
       if (s.tors_nbf && s.tors_nbf[i] == 1) {
         const int a1 = s.tors[4 * i] - b, a4 = s.tors[4 * i + 3] - b;

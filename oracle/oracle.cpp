@@ -1557,7 +1557,10 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
     Ctx::Tors t;
     for (int k = 0; k < 4; ++k) t.a[k] = s->tors[4 * i + k] - b;
     t.k = s->tors_k[i]; t.nrot = s->tors_nrot[i]; t.phase = s->tors_phase[i]; t.div = s->tors_div[i];
-    t.cls = (prm->scale_terms & JP_SCALE_TORS) ? c->pcls(t.a[1], t.a[2]) : 2;   // :838-845
+    // class of the central pair (incel.f90:838-845); SCALET's peptide-bond exemption
+    // (scale_tor 2/3, :846-866) keeps the marked torsions unscaled
+    const bool fixed = s->tors_unscaled && s->tors_unscaled[i];
+    t.cls = ((prm->scale_terms & JP_SCALE_TORS) && !fixed) ? c->pcls(t.a[1], t.a[2]) : 2;
     c->tors.push_back(t);
     // 1-4 pairs (incel.f90:972-987, mknopm inptpl.f90:453-462, incel.f90:1084-1087)
     if (s->tors_nbf[i] == 1) {

@@ -99,3 +99,20 @@ def test_shake_group_across_subsystems_is_rejected(eng_mod, clustered):
     with pytest.raises(eng_mod.JpError) as ex:
         eng_mod.Engine(bad, precision=MIXED, method=abi.JP_METHOD_CANO, alsd=abi.JP_ALSD_LMD, tempco=2)
     assert ex.value.code == abi.JP_E_INVALID
+
+
+def test_peptide_torsions_stay_unscaled_vs_oracle(eng_mod, clustered):
+    """SCALET's peptide-bond exemption: every other torsion marked in tors_unscaled stays in
+    class BB with the torsion bit set; energies, class energies and gradients as the oracle."""
+    top = dict(clustered, tors_unscaled=(np.arange(len(clustered["tors"])) % 2).astype(np.int32))
+    kw = dict(method=abi.JP_METHOD_CANO, alsd=abi.JP_ALSD_LMD, lambda0=0.8, scale_terms=ALL_TERMS)
+    o = oracle.Oracle(top, **kw)
+    eo, go = o.energy_grad()
+    _, eco = o.get_lambda()
+    for prec, gtol, etol in ((FP64, 1e-12, 1e-8), (MIXED, 1e-5, 1e-5)):
+        with eng_mod.Engine(top, precision=prec, **kw) as e:
+            ene, g = e.energy_grad()
+            _, ec = e.get_lambda()
+        assert rms_rel(g, go) < gtol
+        np.testing.assert_allclose(ene, eo, rtol=etol, atol=1e-7 if prec == FP64 else 1e-2)
+        np.testing.assert_allclose(ec, eco, rtol=etol, atol=1e-7 if prec == FP64 else 1e-2)

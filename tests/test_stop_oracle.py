@@ -118,3 +118,44 @@ def test_scalet_factor(poly, tscale):
     if tscale == 1e-3:
         assert lam == 2.0
     np.testing.assert_allclose(xc - x0, lam * (xm - x0), rtol=1e-12, atol=1e-13)   # ulp of x
+
+
+def _clustered(top, n=40):
+    top = dict(top)
+    cl = np.zeros(top["natom"], np.int32)
+    cl[:n] = 1
+    for g, na in zip(top["shake_atoms"], top["shake_n"]):
+        if cl[g[:na]].any():
+            cl[g[:na]] = 1
+    top["cluster"] = cl
+    return top
+
+
+def test_scalet_peptide_exemption(poly):
+    """SCALET's peptide-bond exemption (scale_tor 2/3, incel.f90:846-866): a marked torsion
+    stays in class BB.  All marked = the torsion bit off; none marked = the bit on; a subset
+    moves only those torsions' energy into BB and leaves the total alone."""
+    top = _clustered(poly)
+    kw = dict(method=abi.JP_METHOD_CANO, alsd=abi.JP_ALSD_LMD, lambda0=0.7)
+    nt = len(top["tors"])
+
+    def run(scale, mark):
+        t = dict(top, tors_unscaled=mark) if mark is not None else top
+        o = oracle.Oracle(t, scale_terms=scale, **kw)
+        e, g = o.energy_grad()
+        return e, g, o.get_lambda()[1]
+
+    on = abi.JP_SCALE_TORS
+    e_off, g_off, c_off = run(0, None)
+    e_all, g_all, c_all = run(on, np.ones(nt, np.int32))
+    np.testing.assert_allclose(g_all, g_off, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(c_all, c_off, rtol=1e-12, atol=1e-10)
+    e_on, g_on, c_on = run(on, None)
+    e_none, g_none, c_none = run(on, np.zeros(nt, np.int32))
+    np.testing.assert_allclose(g_none, g_on, rtol=1e-12, atol=1e-12)
+    assert np.abs(c_on - c_off).max() > 1.0          # the bit matters for this cluster
+    sub = (np.arange(nt) % 2).astype(np.int32)
+    e_sub, g_sub, c_sub = run(on, sub)
+    np.testing.assert_allclose(e_sub, e_on, rtol=1e-12, atol=1e-10)
+    np.testing.assert_allclose(c_sub.sum(), c_on.sum(), rtol=1e-12)
+    assert c_sub[2] > c_on[2] or np.allclose(c_sub, c_on)
