@@ -212,6 +212,10 @@ typedef struct jp_system {
                                     with JP_SCALE_TORS: SCALET's peptide-bond exemption
                                     (scale_tor 2/3, incel.f90:846-866), which the caller
                                     decides from atom and residue names; NULL = none */
+  /* CELRES (CAL15M= CMM only, celpar.f90:131-153): every atom of these residues goes to the
+   * level-1 cell of the residue's geometric centre instead of its own */
+  int32_t ncelres;
+  const int32_t *celres;       /* [ncelres][2] first and last atom of each residue */
 } jp_system;
 
 /* Run parameters shared by all replicas of a context (md.inp EXE> MD keywords). */

@@ -115,7 +115,7 @@ class JpSystem(C.Structure):
         ("nshake", C.c_int32), ("shake_n", _ip), ("shake_atoms", _ip), ("shake_dist", _dp),
         ("ge", C.POINTER(JpGe)), ("cluster", _ip), ("ext_cmm", C.POINTER(JpExtCmm)),
         ("hbond", _ip), ("c10", _dp), ("c12h", _dp), ("restraints", C.POINTER(JpRestraints)),
-        ("tors_unscaled", _ip),
+        ("tors_unscaled", _ip), ("ncelres", C.c_int32), ("celres", _ip),
     ]
 
 
@@ -224,6 +224,10 @@ def make_system(top, keep, cord=None, vel=None):
         s.hbond = _ptr(np.asarray(top["hbond"], np.int32), C.c_int32, keep)
         s.c10 = _ptr(top["c10"], C.c_double, keep)
         s.c12h = _ptr(top["c12h"], C.c_double, keep)
+    if top.get("celres") is not None:   # [n][2] first / last atom of each CELRES residue
+        cr = np.asarray(top["celres"], np.int32).reshape(-1, 2)
+        s.ncelres = len(cr)
+        s.celres = _ptr(cr.reshape(-1), C.c_int32, keep)
     if top.get("tors_unscaled") is not None:
         s.tors_unscaled = _ptr(top["tors_unscaled"], C.c_int32, keep)
     if top.get("restraints") is not None:

@@ -324,6 +324,20 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
         }
       if (any && prm->cal15m == JP_CAL15M_CMM) return JP_E_INVALID;
     }
+    // CELRES residues: CMM only, atom ranges inside the system, no atom in two of them
+    if (s.ncelres < 0 || (s.ncelres > 0 && (!s.celres || prm->cal15m != JP_CAL15M_CMM)))
+      return JP_E_INVALID;
+    if (s.ncelres > 0) {
+      std::vector<char> seen(s.natom, 0);
+      for (int i = 0; i < s.ncelres; ++i) {
+        const int f = s.celres[2 * i] - s.index_base, l = s.celres[2 * i + 1] - s.index_base;
+        if (f < 0 || l >= s.natom || f > l) return JP_E_INVALID;
+        for (int a = f; a <= l; ++a) {
+          if (seen[a]) return JP_E_INVALID;
+          seen[a] = 1;
+        }
+      }
+    }
     for (int i = 0; i < s.ntors; ++i) {
       int n = (int)std::lround(s.tors_nrot[i]);
       if (n < 1 || n > 6 || s.tors_div[i] == 0) return JP_E_INVALID;
@@ -526,6 +540,10 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   c->hbond = std::find(hbp.begin(), hbp.end(), 1) != hbp.end();
   int atom0 = 0, blk0 = 0, key0 = 0, sub0 = 0, col0 = 0;
   std::vector<Restr> hres;          // restraints and CAP terms of all replicas
+  std::vector<int2> hres_cmm;       // CELRES: each atom's residue range (empty: no CELRES)
+  double celres_rmax = 0.0;         // largest distance of a CELRES atom from its residue centre
+  int N_all = 0;
+  for (int r = 0; r < nrep; ++r) N_all += sys[r].natom;
   std::vector<int> hres_idx;        // atoms of the distance-restraint groups
   std::vector<int> hcol_rep;
   for (int r = 0; r < nrep; ++r) {
@@ -885,6 +903,22 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       R.ge_upper = s.ge->upper;
       pack_ge(*s.ge, hge.data() + R.ge_off);
     }
+    if (s.ncelres > 0) {   // CELRES residues (global atom ids); their largest radius
+      if (hres_cmm.empty()) hres_cmm.assign(N_all, make_int2(-1, -1));
+      for (int i = 0; i < s.ncelres; ++i) {
+        const int f = s.celres[2 * i] - b, l = s.celres[2 * i + 1] - b;
+        double cen[3] = {0.0, 0.0, 0.0};
+        for (int a = f; a <= l; ++a)
+          for (int k = 0; k < 3; ++k) cen[k] += s.cord[3 * a + k];
+        for (int k = 0; k < 3; ++k) cen[k] /= (double)(l - f + 1);
+        for (int a = f; a <= l; ++a) {
+          hres_cmm[atom0 + a] = make_int2(atom0 + f, atom0 + l);
+          double d2 = 0.0;
+          for (int k = 0; k < 3; ++k) d2 += (s.cord[3 * a + k] - cen[k]) * (s.cord[3 * a + k] - cen[k]);
+          celres_rmax = std::max(celres_rmax, std::sqrt(d2));
+        }
+      }
+    }
     if (s.restraints) {   // dneres: POSITI, DISTAN, DIHEDR, SETBOU sphere CAP
       const jp_restraints &q = *s.restraints;
       auto item = [&](int kind) {
@@ -1035,6 +1069,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     e |= dalloc(c, &P.masks_el, (size_t)c->tile_cap_total * 32);
     e |= dalloc(c, &P.tmp_masks_el, (size_t)c->tile_cap_total * 32);
     e |= dalloc(c, &P.cmm_cell, (size_t)N);
+    if (!hres_cmm.empty()) e |= dput(c, &P.cmm_res, hres_cmm);
     e |= dalloc(c, &P.gwk, 3 * (size_t)N);
     e |= dalloc(c, &P.cmm_pop, (size_t)ntot);
     e |= dalloc(c, &P.cmm_pot, 13 * (size_t)ntot);
@@ -1133,7 +1168,10 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     double s1 = 0.0;
     for (int r = 0; r < nrep; ++r) s1 = std::max(s1, c->reps[r].siz[1]);
     c->zc.rc2 = 1.0e30;
-    c->zc.rlim = std::max(2.0 * std::sqrt(3.0) * s1, rc) * 1.0001 + 0.01;
+    // CELRES: atoms sit up to a residue radius away from the centre that picks their cell
+    // (1 A more for the deformation of a residue between rebuilds)
+    const double rres = hres_cmm.empty() ? 0.0 : 2.0 * (celres_rmax + 1.0);
+    c->zc.rlim = std::max(2.0 * std::sqrt(3.0) * s1 + rres, rc) * 1.0001 + 0.01;
   }
   c->zc.nt1 = nt1;
   IntConst &ic = c->ic;

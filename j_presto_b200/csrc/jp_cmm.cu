@@ -71,10 +71,23 @@ __global__ void k_cmm_assign(DevPtrs P, int natom) {
   int m[3];
   double x[3];
   bool bad = false;
+  // CELRES: the cell of the residue's geometric centre (celpar.f90:131-153)
+  const int2 res = P.cmm_res ? P.cmm_res[a] : make_int2(-1, -1);
+  double p[3];
   for (int k = 0; k < 3; ++k) {
     x[k] = P.x[3 * a + k];
+    p[k] = x[k];
+  }
+  if (res.x >= 0) {
+    for (int k = 0; k < 3; ++k) p[k] = 0.0;
+    for (int b = res.x; b <= res.y; ++b)
+      for (int k = 0; k < 3; ++k) p[k] += P.x[3 * b + k];
+    const double inv = 1.0 / (double)(res.y - res.x + 1);
+    for (int k = 0; k < 3; ++k) p[k] *= inv;
+  }
+  for (int k = 0; k < 3; ++k) {
     const double org = cmm_cen(R, c0, 1, 1, k) - half;
-    const double u = (x[k] - org) * rr;
+    const double u = (p[k] - org) * rr;
     m[k] = (u > -1.0 && u < (double)nv1) ? (int)u + 1 : 0;   // int(): toward zero
     bad |= m[k] < 1 || m[k] > nv1;
   }

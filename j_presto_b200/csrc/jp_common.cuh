@@ -179,6 +179,7 @@ struct DevPtrs {
   // per cell (all levels, all replicas) population and 13 multipole coefficients; level-1
   // raw sums; per replica the centroid sums and the far-field energy (last and being built)
   int *cmm_cell;
+  int2 *cmm_res;                  // CELRES: first / last atom of the atom's residue, (-1, -1) none
   double *gwk;
   int *cmm_pop;
   double *cmm_pot, *cmm_raw, *cmm_c0;

@@ -61,6 +61,9 @@ struct Ctx {
   std::vector<std::pair<int, int>> cap_groups;   // first, last atom (fechn)
   std::vector<int> cap_atoms;                    // iamcap
   double cap_c[3] = {0, 0, 0}, cap_r = 0, cap_k = 0, cap_ra = 0, cap_ka = 0;
+  // CELRES: each atom's residue (first, last atom), -1 = the atom's own position picks its
+  // cell; empty = none
+  std::vector<int> res_first, res_last;
   // H-bond type pairs (iyppid = 2) and their 10-12 parameters fynbpp(3:4,:,:); empty = none
   std::vector<int> hbp;
   std::vector<double> c10, c12h;
@@ -248,8 +251,18 @@ int cmm_rebuild(Ctx& c) {
   std::vector<std::vector<int>> members((size_t)nv1 * nv1 * nv1);
   for (int i = 0; i < n; ++i) {
     int m[3];
+    double p[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+    if (!c.res_first.empty() && c.res_first[i] >= 0) {   // CELRES (celpar.f90:131-153)
+      const int k1 = c.res_first[i], k2 = c.res_last[i];
+      const double rt = 1.0 / (double)(k2 - k1 + 1);
+      for (int k = 0; k < 3; ++k) {
+        double sum = 0.0;
+        for (int a = k1; a <= k2; ++a) sum += x[3 * a + k];
+        p[k] = sum * rt;
+      }
+    }
     for (int k = 0; k < 3; ++k) {
-      m[k] = (int)((x[3 * i + k] - org[k]) * rr) + 1;   // Fortran int(): toward zero
+      m[k] = (int)((p[k] - org[k]) * rr) + 1;   // Fortran int(): toward zero
       if (m[k] < 1 || m[k] > nv1) return JP_E_CELL_OVERFLOW;
       c.cell1[3 * i + k] = m[k];
     }
@@ -1484,6 +1497,15 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
     c->hbp.assign(s->hbond, s->hbond + nt2);
     c->c10.assign(s->c10, s->c10 + nt2);
     c->c12h.assign(s->c12h, s->c12h + nt2);
+  }
+  if (s->ncelres > 0 && s->celres) {
+    c->res_first.assign(n, -1);
+    c->res_last.assign(n, -1);
+    for (int i = 0; i < s->ncelres; ++i)
+      for (int a = s->celres[2 * i] - b; a <= s->celres[2 * i + 1] - b; ++a) {
+        c->res_first[a] = s->celres[2 * i] - b;
+        c->res_last[a] = s->celres[2 * i + 1] - b;
+      }
   }
   if (s->restraints) {
     const jp_restraints& q = *s->restraints;

@@ -126,3 +126,30 @@ def test_far_field_cadence(drop):
     o2.run(4)
     assert o2.cmm_far()[0] == ef0     # steps 2-5 reuse it
     assert ef1 != ef0
+
+
+def test_celres_cells_follow_the_residue_centre():
+    """CELRES (celpar.f90:131-153): the level-1 populations are those of the residues'
+    geometric centres, every atom of a residue counted in its residue's cell."""
+    top = dict(systems.droplet(6, 400, seed=9))
+    t = np.asarray(top["atype"])
+    ow = np.flatnonzero(t == systems.T_OW)
+    res = np.array([(o, o + 2) for o in ow], np.int32)
+    kw = dict(method=abi.JP_METHOD_CANO, cal15m=abi.JP_CAL15M_CMM, bounda=abi.JP_BOUND_NONE)
+    o = oracle.Oracle(dict(top, celres=res), **kw)
+    o.energy_grad()
+    _, pop, cen = o.cmm_levels()[0]
+    x = np.asarray(top["cord"], float)
+    pos = x.copy()
+    for f, l in res:
+        pos[f:l + 1] = x[f:l + 1].mean(0)
+    siz = cen[1, 0] - cen[0, 0]
+    org = cen[0] - 0.5 * siz
+    m = np.floor((pos - org) / siz).astype(int)   # all inside: floor = int() here
+    nv = len(cen)
+    want = np.zeros(nv ** 3, int)
+    np.add.at(want, (m[:, 2] * nv + m[:, 1]) * nv + m[:, 0], 1)
+    np.testing.assert_array_equal(pop, want)
+    plain = oracle.Oracle(top, **kw)
+    plain.energy_grad()
+    assert not np.array_equal(plain.cmm_levels()[0][1], pop)

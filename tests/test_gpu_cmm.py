@@ -76,3 +76,42 @@ def test_invalid_cmm_parameters(eng_mod, drop, kw):
     with pytest.raises(eng_mod.JpError) as ex:
         eng_mod.Engine(drop, precision=MIXED, **dict(CMM, **kw))
     assert ex.value.code == abi.JP_E_INVALID
+
+
+def _celres(top):
+    """Every water (O, H, H) and every 10-atom stretch of the chain as a CELRES residue."""
+    t = np.asarray(top["atype"])
+    ow = np.flatnonzero(t == systems.T_OW)
+    res = [(o, o + 2) for o in ow]
+    nsol = int(ow.min()) if len(ow) else int(top["natom"])
+    res += [(a, min(a + 9, nsol - 1)) for a in range(0, nsol, 10)]
+    return dict(top, celres=np.array(res, np.int32))
+
+
+def test_celres_vs_oracle(eng_mod, drop):
+    """CELRES: atoms take the cell of their residue's centre (celpar.f90:131-153), which
+    moves near/far boundaries; energies, gradients and a 12-step trajectory as the oracle."""
+    top = _celres(drop)
+    kw = dict(CMM, cmm_update=5, update=10)
+    o = oracle.Oracle(top, **kw)
+    eo, go = o.energy_grad()
+    e_plain = oracle.Oracle(drop, **kw).energy_grad()[0]
+    assert abs(eo[abi.JP_E_ELE15] - e_plain[abi.JP_E_ELE15]) > 1e-3   # the cells changed
+    for prec, gtol, etol in ((FP64, 1e-11, 1e-8), (MIXED, 1e-5, 1e-5)):
+        with eng_mod.Engine(top, precision=prec, **kw) as e:
+            ene, g = e.energy_grad()
+        assert rms_rel(g, go) < gtol
+        np.testing.assert_allclose(ene, eo, rtol=etol, atol=1e-6 if prec == FP64 else 1e-2)
+    ier, Eo, _ = o.run(12)
+    assert ier == 0
+    xo, _ = o.get_state()
+    with eng_mod.Engine(top, precision=FP64, **kw) as e:
+        e.step(12)
+        x, _ = e.get_state()
+    assert np.abs(x - xo).max() < 1e-8
+
+
+def test_celres_needs_cmm(eng_mod, drop):
+    with pytest.raises(eng_mod.JpError) as ex:
+        eng_mod.Engine(_celres(drop), precision=MIXED, method=abi.JP_METHOD_CANO)
+    assert ex.value.code == abi.JP_E_INVALID
