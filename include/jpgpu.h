@@ -426,21 +426,30 @@ void jp_destroy(jp_ctx *ctx);
  * before each move), after max_loop iterations, when the step length falls below 1e-10 A
  * per degree of freedom (JP_E_MIN_STEP) or when SHAKE fails.  The pair list is rebuilt
  * every `update` iterations and once at the end.  METHOD= CONJ is not built. */
-enum { JP_MIN_STEEP = 1 };
+enum { JP_MIN_STEEP = 1, JP_MIN_CONJ = 2 };
 typedef struct jp_min_params {
-  int32_t method;        /* JP_MIN_STEEP (METHOD= STEE) */
+  int32_t method;        /* JP_MIN_STEEP (METHOD= STEE) or JP_MIN_CONJ (METHOD= CONJ) */
   int32_t max_loop;      /* LOOPLI: iterations (force evaluations after the first), >= 1 */
   int32_t update;        /* UPDATE: list rebuild interval in iterations (default 10) */
   double convgr;         /* CONVGR: RMS gradient threshold, kcal/mol/A (default 0.1) */
   double step0;          /* ISTEPL: initial step length per atom, A (default 0.01); the
                             step length starts at step0 * sqrt(natom) */
-  double up, down;       /* step-length factors (md_run defaults 1.2 and 0.6) */
+  double up, down;       /* STEE step-length factors (md_run defaults 1.2 and 0.6) */
+  double line_conv;      /* CONJ: a line search ends at |g.d| <= line_conv |g.d|_start (0.1) */
+  int32_t line_max;      /* CONJ: at most line_max evaluations per line search (10) */
 } jp_min_params;
 
 void jp_default_min_params(jp_min_params *p);
 
-/* Minimise every replica of the context at once, each with its own step length and stop
- * condition (md_run minimises one system; replicas here are independent).  Per replica
+/* METHOD= CONJ (conj.f90): conjugate gradients with Powell's restarts (mksrdc, a steepest-
+ * descent direction whenever a direction is not downhill) and a line search that doubles
+ * the step until the directional derivative changes sign, then takes secant steps (linsrc);
+ * the search ends on line_conv or line_max, the minimisation on convgr or max_loop.  The
+ * reference refuses SHAKE here, and so does this call (JP_E_INVALID).  The iteration runs
+ * on the host over device force evaluations, one replica after the other.
+ *
+ * STEE minimises every replica of the context at once, each with its own step length and
+ * stop condition (md_run minimises one system; replicas here are independent).  Per replica
  * (arrays of nrep, each may be NULL): iters = iterations done, eneval[JP_MAXENE] = the
  * energies of the last evaluation, rmsf = its RMS gradient, state = 0 still running at
  * max_loop, 1 converged, 2 step length too small.  Returns JP_OK, JP_E_MIN_STEP if any

@@ -79,19 +79,20 @@ class JpRestraints(C.Structure):
     ]
 
 
-JP_MIN_STEEP = 1
+JP_MIN_STEEP, JP_MIN_CONJ = 1, 2
 JP_E_MIN_STEP = -140
 
 
 class JpMinParams(C.Structure):
     _fields_ = [("method", C.c_int32), ("max_loop", C.c_int32), ("update", C.c_int32),
-                ("convgr", C.c_double), ("step0", C.c_double), ("up", C.c_double), ("down", C.c_double)]
+                ("convgr", C.c_double), ("step0", C.c_double), ("up", C.c_double), ("down", C.c_double),
+                ("line_conv", C.c_double), ("line_max", C.c_int32)]
 
 
 def min_params(**kw):
     """jp_min_params with md_run's EXE> MIN defaults (inpmin.f90), overridden by kw."""
     p = JpMinParams(method=JP_MIN_STEEP, max_loop=1000, update=10, convgr=0.1, step0=0.01, up=1.2,
-                    down=0.6)
+                    down=0.6, line_conv=0.1, line_max=10)
     for k, v in kw.items():
         if not hasattr(p, k):
             raise KeyError(k)

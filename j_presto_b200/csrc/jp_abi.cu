@@ -57,6 +57,7 @@ struct jp_ctx {
   bool hbond = false;               // some type pair has the 10-12 H-bond term
   int hb_cap = 0;                   // capacity of the H-bond pair list
   int nres = 0;                     // restraint and CAP terms
+  int ngroups = 0;                  // SHAKE groups (units of 2-4 atoms)
   int cmm_ncell[6] = {0, 0, 0, 0, 0, 0};   // cells per level over all replicas
   int cmm_nlev = 0;                 // most levels of any replica
   int cano_grid = 1;
@@ -425,6 +426,128 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
 }  // namespace
 
 // =======================================================================================
+namespace {
+
+// conj (conj.f90) for one replica on the host over device force evaluations: the search
+// direction (mksrdc with mksdc1 / mksdc2 / mksrdg, chksrd) and the line search (linsrc).
+// Returns a JP code; fills iters / eneval / rmsf / state like the steepest-descent path.
+int minimize_conj(jp_ctx *c, int r, const jp_min_params *mp, int32_t *iters, double *eneval,
+                  double *rmsf_out, int32_t *state) {
+  const Rep &R = c->reps[r];
+  const int n = R.natom, m = 3 * n;
+  std::vector<double> x(m), g(m), grado(m, 0.0), difgrd(m, 0.0), d(m, 0.0), dold(m, 0.0),
+      drst(m, 0.0), trycor(m);
+  double e[JP_MAXENE];
+  int rc = jp_get_state(c, r, x.data(), nullptr);
+  if (rc != JP_OK) return rc;
+  auto dot = [m](const std::vector<double> &a, const std::vector<double> &b) {
+    double t = 0.0;
+    for (int k = 0; k < m; ++k) t += a[k] * b[k];
+    return t;
+  };
+  auto unit = [&](std::vector<double> &v) {
+    const double f = 1.0 / std::sqrt(dot(v, v));
+    for (double &w : v) w *= f;
+  };
+  rc = jp_energy_grad(c, r, x.data(), e, g.data());
+  if (rc != JP_OK) return rc;
+  double stp = mp->step0 * std::sqrt((double)n), dtdifg = 0.0;
+  double rms = std::sqrt(dot(g, g) / n);
+  int mode = 1, nsrch = 0, nrst = 0, it = 0, st = 0;
+  bool done = false;
+  while (!done) {
+    // search direction: 1 steepest descent, 3 start a restart cycle, 2 continue it
+    double gd;
+    for (;;) {
+      if (mode == 2 && std::fabs(dot(grado, g)) / dot(g, g) >= 0.2) mode = 3;
+      if (mode == 1) {
+        const double f = -1.0 / std::sqrt(dot(g, g));
+        for (int k = 0; k < m; ++k) d[k] = f * g[k];
+        dold = d;
+      } else if (mode == 2) {
+        dold = d;
+        double beta = 0.0, den = 0.0, gam = 0.0;
+        for (int k = 0; k < m; ++k) {
+          const double dg = g[k] - grado[k];
+          beta += g[k] * dg;
+          den += dold[k] * dg;
+          gam += g[k] * difgrd[k];
+        }
+        if (den != 0.0) {
+          beta /= den;
+          gam /= dtdifg;
+          for (int k = 0; k < m; ++k) d[k] = beta * dold[k] + gam * drst[k] - g[k];
+          unit(d);
+        }
+      } else {
+        dold = d;
+        drst = d;
+        double beta = 0.0, den = 0.0;
+        for (int k = 0; k < m; ++k) {
+          difgrd[k] = g[k] - grado[k];
+          beta += g[k] * difgrd[k];
+          den += dold[k] * difgrd[k];
+        }
+        dtdifg = den;
+        if (den != 0.0) {
+          beta /= den;
+          for (int k = 0; k < m; ++k) d[k] = beta * dold[k] - g[k];
+          unit(d);
+        }
+        nrst = nsrch;
+      }
+      gd = dot(g, d);
+      if (gd < 0.0) break;   // downhill: keep it
+      mode = 1;
+    }
+    ++nsrch;
+    if (mode == 1) mode = 3;
+    else if (mode == 3) mode = 2;
+    if (nsrch - nrst == 3 * n) mode = 3;
+    grado = g;
+    // line search along d from trycor
+    const double gd0 = gd;
+    bool bracket = false;
+    int j = 0;
+    double s_lo = 0.0, s_hi = 0.0, gd_lo = gd0, gd_hi = 0.0;
+    trycor = x;
+    for (;;) {
+      if (it != 0 && mp->update > 0 && it % mp->update == 0) {
+        rc = jp_rebuild_cells(c, r);
+        if (rc != JP_OK) return rc;
+      }
+      for (int k = 0; k < m; ++k) x[k] = trycor[k] + stp * d[k];
+      ++it;
+      ++j;
+      rc = jp_energy_grad(c, r, x.data(), e, g.data());
+      if (rc != JP_OK) return rc;
+      const double gdn = dot(g, d);
+      rms = std::sqrt(dot(g, g) / n);
+      if (rms <= mp->convgr) { st = 1; done = true; break; }
+      if (it >= mp->max_loop) { done = true; break; }
+      if (j == mp->line_max) break;
+      if (std::fabs(gdn / gd0) <= mp->line_conv) break;
+      if (!bracket && gdn < 0.0) {   // still downhill: double the step
+        s_lo = stp;
+        gd_lo = gdn;
+        stp = 2.0 * s_lo;
+        continue;
+      }
+      if (gdn < 0.0) { s_lo = stp; gd_lo = gdn; }
+      else { s_hi = stp; gd_hi = gdn; }
+      bracket = true;
+      stp = s_lo - (s_hi - s_lo) / (gd_hi - gd_lo) * gd_lo;   // secant on g.d
+    }
+  }
+  if (iters) iters[r] = it;
+  if (rmsf_out) rmsf_out[r] = rms;
+  if (state) state[r] = st;
+  if (eneval) std::memcpy(eneval + (size_t)r * JP_MAXENE, e, sizeof(e));
+  return JP_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 void jp_default_params(jp_params *p) {
@@ -1002,6 +1125,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   c->nblk = blk0;
   c->nslot = blk0 * kTile;
   c->nunit = (int)units.size();
+  for (const Unit &u : units) c->ngroups += u.n >= 2 ? 1 : 0;
   c->nsub = sub0;
   c->nkeys = key0;
   c->ncol = col0;
@@ -1440,16 +1564,32 @@ void jp_default_min_params(jp_min_params *p) {
   p->step0 = 0.01;
   p->up = 1.2;
   p->down = 0.6;
+  p->line_conv = 0.1;         // line-search convergence rate and limit (inpmin.f90 :90-92)
+  p->line_max = 10;
 }
+
 
 int jp_minimize(jp_ctx *c, const jp_min_params *mp, int32_t *iters, double *eneval, double *rmsf,
                 int32_t *state) {
   if (!c || !mp) return JP_E_INVALID;
-  if (mp->method != JP_MIN_STEEP || mp->max_loop < 1 || mp->update < 0 || !(mp->convgr >= 0.0) ||
-      !(mp->step0 > 0.0) || !(mp->up > 0.0) || !(mp->down > 0.0) || !std::isfinite(mp->convgr) ||
-      !std::isfinite(mp->step0) || !std::isfinite(mp->up) || !std::isfinite(mp->down))
+  if ((mp->method != JP_MIN_STEEP && mp->method != JP_MIN_CONJ) || mp->max_loop < 1 || mp->update < 0 ||
+      !(mp->convgr >= 0.0) || !(mp->step0 > 0.0) || !std::isfinite(mp->convgr) || !std::isfinite(mp->step0))
+    return JP_E_INVALID;
+  if (mp->method == JP_MIN_STEEP &&
+      (!(mp->up > 0.0) || !(mp->down > 0.0) || !std::isfinite(mp->up) || !std::isfinite(mp->down)))
     return JP_E_INVALID;
   CK(cudaSetDevice(c->device));
+  if (mp->method == JP_MIN_CONJ) {   // conj.f90:48-53: no SHAKE with conjugate gradients
+    if (mp->line_max < 1 || !(mp->line_conv >= 0.0) || !std::isfinite(mp->line_conv)) return JP_E_INVALID;
+    if (c->prm.shake_method != JP_SHAKE_NONE && c->ngroups > 0) return JP_E_INVALID;
+    for (int r = 0; r < c->nrep; ++r) {
+      const int rc = minimize_conj(c, r, mp, iters, eneval, rmsf, state);
+      if (rc != JP_OK) return rc;
+    }
+    enqueue_rebuild(c);
+    CK(cudaStreamSynchronize(c->st));
+    return check_status(c);
+  }
   if (!c->P.mins && dalloc(c, &c->P.mins, (size_t)c->nrep)) return JP_E_CUDA;
   DevPtrs &P = c->P;
   cudaStream_t st = c->st;

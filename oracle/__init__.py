@@ -52,6 +52,8 @@ def lib():
         ipp = C.POINTER(C.c_int)
         L.or_minimize.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                   ipp, dp, dp, ipp]
+        L.or_minimize_conj.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
+                                       ipp, dp, dp, ipp]
         L.or_mcmd_scale.argtypes = [vp, C.c_double]
         L.or_mcmd_scale.restype = C.c_double
         L.or_get_lambda.argtypes = [vp, dp, dp]
@@ -169,6 +171,17 @@ class Oracle:
         rm = C.c_double()
         ier = lib().or_minimize(self._h, int(max_loop), int(update), float(convgr), float(step0),
                                 float(up), float(down), C.byref(it), _dp(e), C.byref(rm), C.byref(st))
+        return ier, it.value, e, rm.value, st.value
+
+    def minimize_conj(self, max_loop=1000, update=10, convgr=0.1, step0=0.01, line_conv=0.1,
+                      line_max=10):
+        """conj (conj.f90) on this replica: (ier, iters, energies, rms gradient, state)."""
+        it, st = C.c_int(), C.c_int()
+        e = np.zeros(abi.JP_MAXENE)
+        rm = C.c_double()
+        ier = lib().or_minimize_conj(self._h, int(max_loop), int(update), float(convgr), float(step0),
+                                     float(line_conv), int(line_max), C.byref(it), _dp(e), C.byref(rm),
+                                     C.byref(st))
         return ier, it.value, e, rm.value, st.value
 
     def set_lambda(self, lam, lam_v=0.0):

@@ -1882,6 +1882,132 @@ int or_minimize(void* h, int max_loop, int update, double convgr, double step0, 
   return ier;
 }
 
+// conjugate-gradient minimisation: conj (conj.f90:2-116) -- search directions by mksrdc
+// (:122-216: steepest descent, then Powell's restart scheme, mksdc2 starting a restart
+// cycle and mksdc1 continuing it, back to steepest descent whenever a direction is not
+// downhill) and the line search linsrc (:465-658: doubling until the directional
+// derivative changes sign, then secant steps; stop at |g.d| <= fncovl |g.d at the start|
+// or after inllpl evaluations).  SHAKE is refused (conj.f90:48-53).  Returns ier (0, or
+// -1 with SHAKE groups); iters, ene, rmsf, state (0 loop limit, 1 converged).
+int or_minimize_conj(void* h, int max_loop, int update, double convgr, double step0, double line_conv,
+                     int line_max, int* iters, double* ene_out, double* rmsf_out, int* state) {
+  Ctx* c = (Ctx*)h;
+  if (c->prm.shake_method != JP_SHAKE_NONE && !(c->sk2.empty() && c->sk3.empty() && c->sk4.empty()))
+    return -1;
+  const int n = c->n, m = 3 * n;
+  double* x = c->cord.data();
+  std::vector<double> g(m), grado(m, 0.0), difgrd(m, 0.0), d(m, 0.0), dold(m, 0.0), drst(m, 0.0),
+      trycor(m);
+  double ene[JP_MAXENE];
+  auto evaluate = [&]() {
+    c->itwin = true;
+    energy_grad(*c, x, ene, g.data());
+  };
+  auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) {
+    double s2 = 0.0;
+    for (int k = 0; k < m; ++k) s2 += a[k] * b[k];
+    return s2;
+  };
+  auto normalise = [&](std::vector<double>& v) {
+    const double r = 1.0 / std::sqrt(dot(v, v));
+    for (double& w : v) w *= r;
+  };
+  evaluate();
+  double stplen = step0 * std::sqrt((double)n), dtdifg = 0.0;
+  int ifsrdr = 1, insrdr = 0, inrsdr = 0, iloop = 0, inloop = 0, st = 0;
+  double rmsf = std::sqrt(dot(g, g) / n);
+  for (;;) {
+    // mksrdc
+    double dirgrd;
+    for (;;) {
+      if (ifsrdr == 2 && std::fabs(dot(grado, g)) / dot(g, g) >= 0.2) ifsrdr = 3;
+      if (ifsrdr == 1) {   // mksrdg
+        const double conv = -1.0 / std::sqrt(dot(g, g));
+        for (int k = 0; k < m; ++k) d[k] = conv * g[k];
+        dold = d;
+      } else if (ifsrdr == 2) {   // mksdc1
+        dold = d;
+        double beta = 0.0, rss = 0.0, ganma = 0.0;
+        for (int k = 0; k < m; ++k) {
+          const double dif = g[k] - grado[k];
+          beta += g[k] * dif;
+          rss += dold[k] * dif;
+          ganma += g[k] * difgrd[k];
+        }
+        if (rss != 0.0) {
+          beta /= rss;
+          ganma /= dtdifg;
+          for (int k = 0; k < m; ++k) d[k] = beta * dold[k] + ganma * drst[k] - g[k];
+          normalise(d);
+        }
+      } else {   // mksdc2
+        dold = d;
+        drst = d;
+        double beta = 0.0, rss = 0.0;
+        for (int k = 0; k < m; ++k) {
+          difgrd[k] = g[k] - grado[k];
+          beta += g[k] * difgrd[k];
+          rss += dold[k] * difgrd[k];
+        }
+        dtdifg = rss;
+        if (rss != 0.0) {
+          beta /= rss;
+          for (int k = 0; k < m; ++k) d[k] = beta * dold[k] - g[k];
+          normalise(d);
+        }
+        inrsdr = insrdr;
+      }
+      dirgrd = dot(g, d);   // chksrd
+      if (dirgrd < 0.0) break;
+      ifsrdr = 1;
+    }
+    insrdr += 1;
+    if (ifsrdr == 1) ifsrdr = 3;
+    else if (ifsrdr == 3) ifsrdr = 2;
+    if (insrdr - inrsdr == 3 * n) ifsrdr = 3;
+    grado = g;
+    // linsrc
+    const double dirgrs = dirgrd;
+    bool onfind = false, stop = false;
+    int jloop = 0;
+    double dirgrn = dirgrs, stplnn = 0.0, stplnp = 0.0, dirgrp = 0.0;
+    trycor.assign(x, x + m);
+    for (;;) {
+      if (iloop != 0 && update > 0 && inloop % update == 0) build_list(*c);
+      for (int k = 0; k < m; ++k) x[k] = trycor[k] + stplen * d[k];
+      ++inloop; ++iloop; ++jloop;
+      evaluate();
+      const double dg = dot(g, d);
+      rmsf = std::sqrt(dot(g, g) / n);
+      if (rmsf <= convgr) { st = 1; stop = true; break; }
+      if (iloop >= max_loop) { stop = true; break; }
+      if (jloop == line_max) break;
+      if (std::fabs(dg / dirgrs) <= line_conv) break;
+      if (!onfind) {
+        if (dg < 0.0) {
+          stplnn = stplen; dirgrn = dg;
+          stplen = stplnn * 2.0;
+        } else {
+          onfind = true;
+          stplnp = stplen; dirgrp = dg;
+          stplen = stplnn - (stplnp - stplnn) / (dirgrp - dirgrn) * dirgrn;
+        }
+      } else {
+        if (dg < 0.0) { stplnn = stplen; dirgrn = dg; }
+        else { stplnp = stplen; dirgrp = dg; }
+        stplen = stplnn - (stplnp - stplnn) / (dirgrp - dirgrn) * dirgrn;
+      }
+    }
+    if (stop) break;
+  }
+  if (iters) *iters = iloop;
+  if (ene_out) std::memcpy(ene_out, ene, sizeof(ene));
+  if (rmsf_out) *rmsf_out = rmsf;
+  if (state) *state = st;
+  build_list(*c);
+  return 0;
+}
+
 // nsteps of runmd (md.f90:519-694): verlet or verlethe, then celprp every UPDATE steps.
 int or_run(void* h, int nsteps, double* ene_out, double* temp_out) {
   Ctx* c = (Ctx*)h;

@@ -113,7 +113,33 @@ def test_vanishing_step_and_bad_parameters(eng_mod, poly):
         with pytest.raises(eng_mod.JpError) as ex:
             e.minimize(max_loop=10, step0=0.1, down=1e-12, convgr=0.0)   # E rises 2.8e3 -> 2.2e4
         assert ex.value.code == abi.JP_E_MIN_STEP
-        for bad in (dict(max_loop=0), dict(step0=0.0), dict(convgr=-1.0), dict(method=2)):
+        for bad in (dict(max_loop=0), dict(step0=0.0), dict(convgr=-1.0), dict(method=3),
+                    dict(method=abi.JP_MIN_CONJ, line_max=0)):
             with pytest.raises(eng_mod.JpError) as ex:
                 e.minimize(**bad)
             assert ex.value.code == abi.JP_E_INVALID
+
+
+def test_conj_vs_oracle(eng_mod, poly):
+    """METHOD= CONJ: 40 evaluations through list rebuilds, the direction and line-search
+    decisions the same as the oracle's."""
+    kw = dict(method=CANO, shake_method=NOSHAKE)
+    o = oracle.Oracle(poly, **kw)
+    ier, it, eo, ro, so = o.minimize_conj(max_loop=40, update=5, convgr=0.0)
+    assert ier == 0 and it == 40
+    with eng_mod.Engine(poly, precision=FP64, **kw) as e:
+        its, ene, rm, st = e.minimize(method=abi.JP_MIN_CONJ, max_loop=40, update=5, convgr=0.0)
+        x = e.get_state()[0]
+        assert its[0] == 40 and st[0] == 0
+        # and MD runs on from the minimised state
+        e.step(3)
+    assert np.abs(x - o.get_state()[0]).max() < 1e-7
+    np.testing.assert_allclose(ene[0], eo, rtol=1e-8, atol=1e-6)
+    np.testing.assert_allclose(rm[0], ro, rtol=1e-6)
+
+
+def test_conj_refuses_shake(eng_mod, poly):
+    with eng_mod.Engine(poly, precision=MIXED, method=CANO) as e:
+        with pytest.raises(eng_mod.JpError) as ex:
+            e.minimize(method=abi.JP_MIN_CONJ, max_loop=5)
+        assert ex.value.code == abi.JP_E_INVALID

@@ -69,3 +69,31 @@ def test_vanishing_step_length_stops(poly):
     o = oracle.Oracle(poly, method=CANO, shake_method=NOSHAKE)
     ier, it, _, _, st = o.minimize(max_loop=10, step0=3.0, down=1e-12, convgr=0.0)
     assert (ier, it, st) == (-2, 1, 2)
+
+
+def test_conj_first_trial_and_progress(poly):
+    """METHOD= CONJ (conj.f90): the first trial point is the steepest-descent step of length
+    ISTEPL sqrt(N); over the same number of evaluations it ends lower than STEE; SHAKE is
+    refused (ier -1)."""
+    ref = oracle.Oracle(poly, method=CANO, shake_method=NOSHAKE)
+    x0 = np.asarray(poly["cord"], float)
+    _, g0 = ref.energy_grad(x0)
+    o = oracle.Oracle(poly, method=CANO, shake_method=NOSHAKE)
+    ier, it, _, _, st = o.minimize_conj(max_loop=1, update=0, convgr=0.0)
+    assert (ier, it, st) == (0, 1, 0)
+    want = x0 - 0.01 * np.sqrt(len(x0)) * g0 / np.sqrt((g0 * g0).sum())
+    np.testing.assert_allclose(o.get_state()[0], want, rtol=0, atol=1e-12)
+    oc = oracle.Oracle(poly, method=CANO, shake_method=NOSHAKE)
+    os_ = oracle.Oracle(poly, method=CANO, shake_method=NOSHAKE)
+    ec = oc.minimize_conj(max_loop=150, convgr=0.0)[2][0]
+    es = os_.minimize(max_loop=150, convgr=0.0)[2][0]
+    assert ec < es
+    e1, g1 = oc.energy_grad()
+    np.testing.assert_allclose(e1[0], ec, rtol=1e-10)
+    assert oracle.Oracle(poly, method=CANO).minimize_conj(max_loop=5)[0] == -1
+
+
+def test_conj_converges(poly):
+    o = oracle.Oracle(poly, method=CANO, shake_method=NOSHAKE)
+    ier, it, ene, rmsf, st = o.minimize_conj(max_loop=3000, convgr=1.0)
+    assert (ier, st) == (0, 1) and rmsf <= 1.0 and it < 3000
