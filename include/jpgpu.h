@@ -153,7 +153,20 @@ typedef struct jp_restraints {
   double cap_center[3];        /* fxcbou */
   double cap_radius, cap_k;            /* furcap, fukcap */
   double cap_atom_radius, cap_atom_k;  /* furcap_pro, fukcap_pro */
+  /* SETBOU shape (capshp, dnecap.f90:82-250, half-harmonic function): JP_CAP_SPHERE (or 0)
+   * as above; JP_CAP_BOX: each coordinate of a group's centre of mass minus cap_center
+   * outside [cap_wall[2k], cap_wall[2k+1]] adds 1/2 k (distance to the wall)^2, each
+   * coordinate of a listed atom (absolute) likewise with cap_atom_wall (celwal, celwal_pro,
+   * compared as dnecap.f90:126-193 compares them); JP_CAP_ELLIPSOID: with
+   * s = sum_k c_k^2 e_k > 1 (e = 1 / semi-axis^2, c = position - cap_center) the term is
+   * 1/2 k (|c| (1 - s^-1/2))^2 and its gradient k (1 - s^-1/2) c, as dnecap.f90:206-246
+   * writes it */
+  int32_t cap_shape;
+  double cap_wall[6], cap_atom_wall[6];          /* x lo, x hi, y lo, y hi, z lo, z hi */
+  double cap_ellipse[3], cap_atom_ellipse[3];    /* fxellp, fxellp_pro */
 } jp_restraints;
+
+enum { JP_CAP_SPHERE = 1, JP_CAP_BOX = 2, JP_CAP_ELLIPSOID = 3 };
 
 /* One replica's system: topology, parameters and coordinates.
  * Mirrors md_run's COMBAS/COMERG/COMMIS module arrays. */

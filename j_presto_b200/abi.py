@@ -76,10 +76,13 @@ class JpRestraints(C.Structure):
         ("ncap_group", C.c_int32), ("cap_group", _ip), ("ncap_atom", C.c_int32), ("cap_atom", _ip),
         ("cap_center", C.c_double * 3), ("cap_radius", C.c_double), ("cap_k", C.c_double),
         ("cap_atom_radius", C.c_double), ("cap_atom_k", C.c_double),
+        ("cap_shape", C.c_int32), ("cap_wall", C.c_double * 6), ("cap_atom_wall", C.c_double * 6),
+        ("cap_ellipse", C.c_double * 3), ("cap_atom_ellipse", C.c_double * 3),
     ]
 
 
 JP_MIN_STEEP, JP_MIN_CONJ = 1, 2
+JP_CAP_SPHERE, JP_CAP_BOX, JP_CAP_ELLIPSOID = 1, 2, 3
 JP_E_MIN_STEP = -140
 
 
@@ -279,6 +282,10 @@ def make_restraints(rd, keep):
         r.cap_radius, r.cap_k = float(cap["radius"]), float(cap["k"])
         r.cap_atom_radius = float(cap.get("atom_radius", 0.0))
         r.cap_atom_k = float(cap.get("atom_k", 0.0))
+        r.cap_shape = int(cap.get("shape", JP_CAP_SPHERE))   # box: wall / atom_wall [6];
+        for key, n in (("wall", 6), ("atom_wall", 6), ("ellipse", 3), ("atom_ellipse", 3)):
+            if key in cap:                                   # ellipsoid: ellipse / atom_ellipse [3]
+                getattr(r, "cap_" + key)[:] = [float(v) for v in np.ravel(cap[key])][:n]
     keep.append(r)
     return r
 

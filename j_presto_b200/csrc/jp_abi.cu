@@ -409,6 +409,16 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
             !fin(q.cap_atom_radius) || !fin(q.cap_k) || !fin(q.cap_atom_k))
           return JP_E_INVALID;
         if ((q.ncap_group && !q.cap_group) || (q.ncap_atom && !q.cap_atom)) return JP_E_INVALID;
+        if (q.cap_shape < 0 || q.cap_shape > JP_CAP_ELLIPSOID) return JP_E_INVALID;
+        for (int k = 0; k < 6 && q.cap_shape == JP_CAP_BOX; k += 2)
+          if (!fin(q.cap_wall[k]) || !fin(q.cap_wall[k + 1]) || !(q.cap_wall[k] <= q.cap_wall[k + 1]) ||
+              !fin(q.cap_atom_wall[k]) || !fin(q.cap_atom_wall[k + 1]) ||
+              !(q.cap_atom_wall[k] <= q.cap_atom_wall[k + 1]))
+            return JP_E_INVALID;
+        for (int k = 0; k < 3 && q.cap_shape == JP_CAP_ELLIPSOID; ++k)
+          if (!(q.cap_ellipse[k] > 0.0) || !(q.cap_atom_ellipse[k] > 0.0) || !fin(q.cap_ellipse[k]) ||
+              !fin(q.cap_atom_ellipse[k]))
+            return JP_E_INVALID;
         for (int i = 0; i < q.ncap_group; ++i)
           if (!okatom(q.cap_group[2 * i]) || !okatom(q.cap_group[2 * i + 1]) ||
               q.cap_group[2 * i] > q.cap_group[2 * i + 1])
@@ -1080,24 +1090,33 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
         t.p[3] = q.dihe_kup[i];
         hres.push_back(t);
       }
+      const int shape = q.cap_shape == 0 ? JP_CAP_SPHERE : q.cap_shape;
+      auto shape_params = [&](Restr &t, const double *wall, const double *ell) {
+        if (shape == JP_CAP_BOX) for (int k = 0; k < 6; ++k) t.p[6 + k] = wall[k];
+        if (shape == JP_CAP_ELLIPSOID) for (int k = 0; k < 3; ++k) t.p[6 + k] = ell[k];
+      };
       for (int i = 0; i < q.ncap_group; ++i) {
         Restr t = item(R_CAPG);
         t.a[0] = atom0 + q.cap_group[2 * i] - b;
         t.a[1] = atom0 + q.cap_group[2 * i + 1] - b;
+        t.a[2] = shape;
         double m = 0.0;
         for (int a = q.cap_group[2 * i] - b; a <= q.cap_group[2 * i + 1] - b; ++a) m += s.mass[a];
         for (int k = 0; k < 3; ++k) t.p[k] = q.cap_center[k];
         t.p[3] = q.cap_radius;
         t.p[4] = q.cap_k;
         t.p[5] = 1.0 / m;
+        shape_params(t, q.cap_wall, q.cap_ellipse);
         hres.push_back(t);
       }
       for (int i = 0; i < q.ncap_atom; ++i) {
         Restr t = item(R_CAPA);
         t.a[0] = atom0 + q.cap_atom[i] - b;
+        t.a[1] = shape;
         for (int k = 0; k < 3; ++k) t.p[k] = q.cap_center[k];
         t.p[3] = q.cap_atom_radius;
         t.p[4] = q.cap_atom_k;
+        shape_params(t, q.cap_atom_wall, q.cap_atom_ellipse);
         hres.push_back(t);
       }
     }

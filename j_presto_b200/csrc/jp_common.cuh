@@ -113,8 +113,10 @@ struct Restr {
   int rep;
   int a[4];        // POS, CAPA: atom | DIST: group i = res_idx[a0, a1), group j = res_idx[a2, a3)
                    // | DIHE: the four atoms | CAPG: first and last atom of the group
-  double p[6];     // POS: ref xyz, k | DIST, DIHE: lo, up, k_lo, k_up
-                   // | CAPG, CAPA: centre xyz, radius, k (CAPG: p[5] = 1 / group mass)
+                   // | CAPG: a[2], CAPA: a[1] = shape (JP_CAP_*)
+  double p[12];    // POS: ref xyz, k | DIST, DIHE: lo, up, k_lo, k_up
+                   // | CAPG, CAPA: centre xyz, radius, k, 1 / group mass (CAPG), then
+                   //   walls lo/hi x, y, z (box) or 1 / semi-axis^2 x, y, z (ellipsoid)
 };
 
 // steepest-descent minimisation state of one replica (jp_minimize.cu)

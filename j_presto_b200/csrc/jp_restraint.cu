@@ -6,9 +6,9 @@
 //             dE/dx_i = 4 k (R^2 - r0^2) R^8 / n  sum_j r_ij^-8 (x_i - x_j)
 //   dihedral  (dcdihe, dneres.f90:227-378): phi in [0, 2 pi); outside [lo, up] E =
 //             k (phi - wall)^2 measured from the nearer wall (the far one across 2 pi)
-//   CAP       (dnecap iufcap 1 / capshp 1, dnecap.f90:80-122 and :428-437): half-harmonic
-//             1/2 k (d - radius)^2 on the distance d of a group's centre of mass (gradient
-//             shared by mass) or of a listed atom from the centre, outside the radius
+//   CAP       (dnecap iufcap 1, dnecap.f90:80-250 and :428-437): half-harmonic terms on a
+//             group's centre of mass (gradient shared by mass) or a listed atom: outside a
+//             sphere, outside box walls per coordinate, or outside an ellipsoid
 // Minimum image as in the _PB variants under BOUNDA= PBC; none under BOUNDA= NO (_CB).
 // One restraint per thread, FP64 arithmetic on both paths (they are few); forces go to the
 // class-BB accumulators with weight 1 (grad(:,:,nfrg)), energies to enevcc(11..14).
@@ -132,6 +132,46 @@ __device__ __forceinline__ void res_dihe(const DevPtrs& P, const Rep& R, const R
   add_grad<FP64>(P, wr, Q.a[3], w[6], w[7], w[8]);
 }
 
+// one CAP term of a group centre or an atom: c = position - centre, xa = what the box walls
+// are compared with (c for groups, the absolute position for atoms, dnecap.f90:126-193);
+// energy e and gradient g (before the mass share of a group); false when nothing acts
+__device__ __forceinline__ bool cap_term(const Restr& Q, int shape, const double* c, const double* xa,
+                                         double& e, double* g) {
+  const double k = Q.p[4];
+  if (shape == JP_CAP_BOX) {
+    bool any = false;
+    double s2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      g[d] = 0.0;
+      const double lo = Q.p[6 + 2 * d], hi = Q.p[7 + 2 * d];
+      double dd = 0.0;
+      if (xa[d] < lo) dd = xa[d] - lo;
+      else if (xa[d] > hi) dd = xa[d] - hi;
+      else continue;
+      any = true;
+      s2 += dd * dd;
+      g[d] = k * dd;
+    }
+    e = 0.5 * k * s2;
+    return any;
+  }
+  if (shape == JP_CAP_ELLIPSOID) {
+    const double s = c[0] * c[0] * Q.p[6] + c[1] * c[1] * Q.p[7] + c[2] * c[2] * Q.p[8];
+    if (!(s > 1.0)) return false;
+    const double rt = 1.0 - sqrt(1.0 / s);
+    const double dist = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]) * rt;
+    e = 0.5 * k * dist * dist;
+    for (int d = 0; d < 3; ++d) g[d] = c[d] * rt * k;
+    return true;
+  }
+  const double d2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];   // sphere
+  if (!(d2 > Q.p[3] * Q.p[3])) return false;
+  const double d = sqrt(d2), dd = d - Q.p[3];
+  e = 0.5 * k * dd * dd;
+  for (int m = 0; m < 3; ++m) g[m] = k * dd / d * c[m];
+  return true;
+}
+
 template <bool FP64>
 __global__ void __launch_bounds__(kResThreads) k_restraints(DevPtrs P, int n, int alsd) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -161,30 +201,23 @@ __global__ void __launch_bounds__(kResThreads) k_restraints(DevPtrs P, int n, in
         break;
       case R_CAPG: {   // centre of mass of atoms a[0] .. a[1]; p[5] = 1 / their mass
         slot = JP_E_CAP;
-        double c[3] = {0.0, 0.0, 0.0};
+        double c[3] = {0.0, 0.0, 0.0}, g[3];
         for (int a = Q.a[0]; a <= Q.a[1]; ++a)
           for (int k = 0; k < 3; ++k) c[k] += P.mass[a] * x[3 * a + k];
         for (int k = 0; k < 3; ++k) c[k] = c[k] * Q.p[5] - Q.p[k];
-        const double d2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
-        if (d2 > Q.p[3] * Q.p[3]) {
-          const double d = sqrt(d2), dd = d - Q.p[3];
-          e = 0.5 * Q.p[4] * dd * dd;
-          const double g = Q.p[4] * dd / d * Q.p[5];
+        if (cap_term(Q, Q.a[2], c, c, e, g))
           for (int a = Q.a[0]; a <= Q.a[1]; ++a)
-            add_grad<FP64>(P, g * P.mass[a], a, c[0], c[1], c[2]);
-        }
+            add_grad<FP64>(P, Q.p[5] * P.mass[a], a, g[0], g[1], g[2]);
         break;
       }
       case R_CAPA: {
         slot = JP_E_CAP;
-        double c[3];
-        for (int k = 0; k < 3; ++k) c[k] = x[3 * Q.a[0] + k] - Q.p[k];
-        const double d2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
-        if (d2 > Q.p[3] * Q.p[3]) {
-          const double d = sqrt(d2), dd = d - Q.p[3];
-          e = 0.5 * Q.p[4] * dd * dd;
-          add_grad<FP64>(P, Q.p[4] * dd / d, Q.a[0], c[0], c[1], c[2]);
+        double c[3], xa[3], g[3];
+        for (int k = 0; k < 3; ++k) {
+          xa[k] = x[3 * Q.a[0] + k];
+          c[k] = xa[k] - Q.p[k];
         }
+        if (cap_term(Q, Q.a[1], c, xa, e, g)) add_grad<FP64>(P, 1.0, Q.a[0], g[0], g[1], g[2]);
         break;
       }
     }

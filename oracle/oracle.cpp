@@ -61,6 +61,8 @@ struct Ctx {
   std::vector<std::pair<int, int>> cap_groups;   // first, last atom (fechn)
   std::vector<int> cap_atoms;                    // iamcap
   double cap_c[3] = {0, 0, 0}, cap_r = 0, cap_k = 0, cap_ra = 0, cap_ka = 0;
+  int cap_shape = 1;                             // capshp: 1 sphere, 2 box, 3 ellipsoid
+  double cap_wall[6] = {0}, cap_awall[6] = {0}, cap_ell[3] = {0}, cap_aell[3] = {0};
   // CELRES: each atom's residue (first, last atom), -1 = the atom's own position picks its
   // cell; empty = none
   std::vector<int> res_first, res_last;
@@ -603,30 +605,54 @@ void restraints(Ctx& c, const double* x, double* ene, double* grad) {
       grad[3 * ia[3] + k] += wr * w[6 + k];
     }
   }
+  // CAP (dnecap.f90 iufcap 1): sum of squared overshoots times k, halved at the end
+  // (:121, :202, :249); Tcord = centre of mass - fxcbou for groups, Tcod per atom
   double ecap = 0.0;
+  auto cap = [&](const double* T, const double* Tbox, double k, double r, const double* wall,
+                 const double* ell, double* tg) {
+    tg[0] = tg[1] = tg[2] = 0.0;
+    if (c.cap_shape == JP_CAP_BOX) {   // capshp 2 (:123-202): walls per coordinate
+      for (int d = 0; d < 3; ++d) {
+        double dist = 0.0;
+        if (Tbox[d] < wall[2 * d]) dist = Tbox[d] - wall[2 * d];
+        else if (Tbox[d] > wall[2 * d + 1]) dist = Tbox[d] - wall[2 * d + 1];
+        else continue;
+        ecap += k * dist * dist;
+        tg[d] = dist * k;
+      }
+      return;
+    }
+    const double d2 = T[0] * T[0] + T[1] * T[1] + T[2] * T[2];
+    if (c.cap_shape == JP_CAP_ELLIPSOID) {   // capshp 3 (:205-246)
+      const double s2 = T[0] * T[0] * ell[0] + T[1] * T[1] * ell[1] + T[2] * T[2] * ell[2];
+      if (s2 <= 1.0) return;
+      const double rt = 1.0 - std::sqrt(1.0 / s2);
+      const double dist = std::sqrt(d2) * rt;
+      ecap += k * dist * dist;
+      for (int d = 0; d < 3; ++d) tg[d] = T[d] * rt * k;
+      return;
+    }
+    if (d2 <= r * r) return;   // capshp 1 (:83-122)
+    const double d = std::sqrt(d2), over = d - r;
+    ecap += k * over * over;
+    for (int m = 0; m < 3; ++m) tg[m] = T[m] * (k * over / d);
+  };
   for (const auto& g : c.cap_groups) {   // centre of mass of each included chain
-    double m = 0.0, C[3] = {0, 0, 0};
+    double m = 0.0, C[3] = {0, 0, 0}, tg[3];
     for (int a = g.first; a <= g.second; ++a) {
       m += c.mass[a];
       for (int k = 0; k < 3; ++k) C[k] += c.mass[a] * x[3 * a + k];
     }
     for (int k = 0; k < 3; ++k) C[k] = C[k] / m - c.cap_c[k];
-    const double dist = C[0] * C[0] + C[1] * C[1] + C[2] * C[2];
-    if (dist <= c.cap_r * c.cap_r) continue;
-    const double d = std::sqrt(dist), over = d - c.cap_r;
-    ecap += c.cap_k * over * over;
-    const double rt = c.cap_k * over / d;
-    for (int a = g.first; a <= g.second; ++a)
-      for (int k = 0; k < 3; ++k) grad[3 * a + k] += C[k] * rt * (c.mass[a] / m);
+    cap(C, C, c.cap_k, c.cap_r, c.cap_wall, c.cap_ell, tg);
+    for (int a = g.first; a <= g.second; ++a)   // :428-437, shared by mass
+      for (int k = 0; k < 3; ++k) grad[3 * a + k] += tg[k] * (c.mass[a] / m);
   }
   for (int a : c.cap_atoms) {
-    double T[3];
+    double T[3], tg[3];
     for (int k = 0; k < 3; ++k) T[k] = x[3 * a + k] - c.cap_c[k];
-    const double dist = T[0] * T[0] + T[1] * T[1] + T[2] * T[2];
-    if (dist <= c.cap_ra * c.cap_ra) continue;
-    const double d = std::sqrt(dist), over = d - c.cap_ra;
-    ecap += c.cap_ka * over * over;
-    for (int k = 0; k < 3; ++k) grad[3 * a + k] += c.cap_ka * over / d * T[k];
+    cap(T, x + 3 * a, c.cap_ka, c.cap_ra, c.cap_awall, c.cap_aell, tg);   // box: absolute coordinates
+    for (int k = 0; k < 3; ++k) grad[3 * a + k] += tg[k];
   }
   ecap *= 0.5;
   ene[JP_E_POSRES] += epos;
@@ -1531,6 +1557,9 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
     for (int k = 0; k < 3; ++k) c->cap_c[k] = q.cap_center[k];
     c->cap_r = q.cap_radius; c->cap_k = q.cap_k;
     c->cap_ra = q.cap_atom_radius; c->cap_ka = q.cap_atom_k;
+    c->cap_shape = q.cap_shape == 0 ? JP_CAP_SPHERE : q.cap_shape;
+    for (int k = 0; k < 6; ++k) { c->cap_wall[k] = q.cap_wall[k]; c->cap_awall[k] = q.cap_atom_wall[k]; }
+    for (int k = 0; k < 3; ++k) { c->cap_ell[k] = q.cap_ellipse[k]; c->cap_aell[k] = q.cap_atom_ellipse[k]; }
   }
   // exclusions (inpcls.f90:229-290 itab14)
   c->excl.assign(n, {});

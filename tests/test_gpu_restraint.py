@@ -1,5 +1,5 @@
-"""Restraints (POSITI, DISTAN, DIHEDR: dneres.f90) and the sphere CAP (SETBOU, dnecap.f90)
-on the GPU against the oracle: energies in their four slots and gradients, FP64 and mixed,
+"""Restraints (POSITI, DISTAN, DIHEDR: dneres.f90) and the CAP (SETBOU sphere, box and
+ellipsoid: dnecap.f90) on the GPU against the oracle: energies in their four slots and gradients, FP64 and mixed,
 periodic (restraints) and free boundary (restraints + CAP); 15-step FP64 trajectories;
 ALSD class energies (the restraints belong to class BB, unscaled); the parameter checks.
 
@@ -111,3 +111,19 @@ def test_invalid_restraints_are_rejected(eng_mod, poly, drop):
         with pytest.raises(eng_mod.JpError) as ex:
             eng_mod.Engine(top, precision=MIXED, **kw)
         assert ex.value.code == abi.JP_E_INVALID
+
+
+@pytest.mark.parametrize("shape", [abi.JP_CAP_BOX, abi.JP_CAP_ELLIPSOID])
+def test_cap_shapes_vs_oracle(eng_mod, drop, shape):
+    """SETBOU box and ellipsoid shapes (dnecap.f90:123-250) on the droplet's groups and atoms."""
+    from tests.test_restraint_oracle import _shaped
+    top = _shaped(drop, shape)
+    kw = dict(method=abi.JP_METHOD_CANO, bounda=NONE)
+    eo, go = oracle.Oracle(top, **kw).energy_grad()
+    assert eo[abi.JP_E_CAP] > 1.0
+    for prec, gtol, etol in ((FP64, 1e-12, 1e-8), (MIXED, 1e-5, 1e-5)):
+        with eng_mod.Engine(top, precision=prec, **kw) as e:
+            ene, g = e.energy_grad()
+        assert rms_rel(g, go) < gtol
+        np.testing.assert_allclose(ene, eo, rtol=etol, atol=1e-7 if prec == FP64 else 1e-2)
+        np.testing.assert_allclose(ene[abi.JP_E_CAP], eo[abi.JP_E_CAP], rtol=1e-9)

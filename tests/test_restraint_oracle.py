@@ -1,6 +1,6 @@
-"""The oracle's restraints (dneres.f90: dposc, ddistc, dcdihe) and sphere CAP (dnecap.f90
-iufcap 1 / capshp 1) against closed forms written independently in numpy, finite
-differences of their energies, and the ALSD class rules (no GPU).
+"""The oracle's restraints (dneres.f90: dposc, ddistc, dcdihe) and CAP (dnecap.f90 iufcap 1:
+sphere, box and ellipsoid shapes) against closed forms written independently in numpy,
+finite differences of their energies, and the ALSD class rules (no GPU).
 """
 import numpy as np
 import pytest
@@ -163,3 +163,82 @@ def test_alsd_restraints_are_class_bb_and_unscaled(poly):
     p1 = oracle.Oracle(poly, method=CANO).energy_grad()[1]
     p0 = oracle.Oracle(_plain(poly), method=CANO).energy_grad()[1]
     np.testing.assert_allclose(g1 - g0, p1 - p0, rtol=0, atol=1e-10)
+
+
+def _shaped(drop, shape):
+    """The droplet's CAP as a box or an ellipsoid around the same centre."""
+    rd = dict(drop["restraints"])
+    cap = dict(rd["cap"], shape=shape)
+    x = np.asarray(drop["cord"], float)
+    h = np.abs(x - cap["center"]).max(0)
+    cap["wall"] = np.ravel([(-0.8 * v, 0.8 * v) for v in h])                 # relative to the centre
+    cap["atom_wall"] = np.ravel([(c - 0.8 * v + 3.0, c + 0.8 * v - 3.0)      # absolute
+                                 for c, v in zip(cap["center"], h)])
+    cap["ellipse"] = 1.0 / (0.8 * h) ** 2
+    cap["atom_ellipse"] = 1.0 / (0.8 * h - 3.0) ** 2
+    rd["cap"] = cap
+    return dict(drop, restraints=rd)
+
+
+def _numpy_cap(top):
+    """Energy and the gradient dnecap.f90 writes for the box (capshp 2) and ellipsoid
+    (capshp 3) shapes."""
+    x = np.asarray(top["cord"], float)
+    m = np.asarray(top["mass"], float)
+    cap = top["restraints"]["cap"]
+    e, g = 0.0, np.zeros_like(x)
+
+    def term(T, Tb, k, wall, ell):
+        if cap["shape"] == abi.JP_CAP_BOX:
+            lo, hi = np.asarray(wall)[0::2], np.asarray(wall)[1::2]
+            over = np.where(Tb < lo, Tb - lo, np.where(Tb > hi, Tb - hi, 0.0))
+            return 0.5 * k * (over ** 2).sum(), k * over
+        s = (T * T * ell).sum()
+        if s <= 1.0:
+            return 0.0, np.zeros(3)
+        rt = 1.0 - np.sqrt(1.0 / s)
+        return 0.5 * k * (np.linalg.norm(T) * rt) ** 2, T * rt * k
+
+    for f, l in cap["groups"]:
+        C = (m[f:l + 1, None] * x[f:l + 1]).sum(0) / m[f:l + 1].sum() - cap["center"]
+        de, dg = term(C, C, cap["k"], cap["wall"], cap["ellipse"])
+        e += de
+        g[f:l + 1] += dg * (m[f:l + 1, None] / m[f:l + 1].sum())
+    for a in cap["atoms"]:
+        de, dg = term(x[a] - cap["center"], x[a], cap["atom_k"], cap["atom_wall"], cap["atom_ellipse"])
+        e += de
+        g[a] += dg
+    return e, g
+
+
+@pytest.mark.parametrize("shape", [abi.JP_CAP_BOX, abi.JP_CAP_ELLIPSOID])
+def test_cap_shapes_closed_form(drop, shape):
+    top = _shaped(drop, shape)
+    rd = top["restraints"]
+    only = dict(top, restraints=dict(cap=rd["cap"]))
+    kw = dict(method=CANO, bounda=NONE)
+    e1, g1 = oracle.Oracle(only, **kw).energy_grad()
+    e0, g0 = oracle.Oracle(_plain(top), **kw).energy_grad()
+    ew, gw = _numpy_cap(only)
+    assert ew > 1.0
+    np.testing.assert_allclose(e1[abi.JP_E_CAP], ew, rtol=1e-11)
+    np.testing.assert_allclose(g1 - g0, gw, rtol=0, atol=1e-10)
+
+
+def test_box_cap_gradient_is_the_derivative(drop):
+    top = _shaped(drop, abi.JP_CAP_BOX)
+    only = dict(top, restraints=dict(cap=top["restraints"]["cap"]))
+    o = oracle.Oracle(only, method=CANO, bounda=NONE)
+    o0 = oracle.Oracle(_plain(top), method=CANO, bounda=NONE)
+    g = o.energy_grad()[1] - o0.energy_grad()[1]
+    x0 = np.asarray(top["cord"], float)
+    moved = np.flatnonzero(np.abs(g).sum(1) > 1e-6)[:30]
+    assert len(moved) > 5
+    h = 1e-6
+    for a in moved:
+        for k in range(3):
+            xp, xm = x0.copy(), x0.copy()
+            xp[a, k] += h
+            xm[a, k] -= h
+            fd = (o.energy_grad(xp)[0][abi.JP_E_CAP] - o.energy_grad(xm)[0][abi.JP_E_CAP]) / (2 * h)
+            assert abs(fd - g[a, k]) < 1e-5 * max(1.0, abs(g[a, k]))
