@@ -164,9 +164,14 @@ typedef struct jp_restraints {
   int32_t cap_shape;
   double cap_wall[6], cap_atom_wall[6];          /* x lo, x hi, y lo, y hi, z lo, z hi */
   double cap_ellipse[3], cap_atom_ellipse[3];    /* fxellp, fxellp_pro */
+  /* CAP function (iufcap): 1 (or 0) half-harmonic as above; 2 half-biquadratic, sphere
+   * only (dnecap.f90:253-281): with s = (d^2 - R^2) / R^2 > 0 the term is 1/4 k R^2 s^2
+   * and its gradient k s c.  The plane-and-cylinder functions 3 and 4 are not built. */
+  int32_t cap_function;
 } jp_restraints;
 
 enum { JP_CAP_SPHERE = 1, JP_CAP_BOX = 2, JP_CAP_ELLIPSOID = 3 };
+enum { JP_CAP_HARMONIC = 1, JP_CAP_BIQUADRATIC = 2 };
 
 /* One replica's system: topology, parameters and coordinates.
  * Mirrors md_run's COMBAS/COMERG/COMMIS module arrays. */

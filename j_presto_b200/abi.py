@@ -78,11 +78,13 @@ class JpRestraints(C.Structure):
         ("cap_atom_radius", C.c_double), ("cap_atom_k", C.c_double),
         ("cap_shape", C.c_int32), ("cap_wall", C.c_double * 6), ("cap_atom_wall", C.c_double * 6),
         ("cap_ellipse", C.c_double * 3), ("cap_atom_ellipse", C.c_double * 3),
+        ("cap_function", C.c_int32),
     ]
 
 
 JP_MIN_STEEP, JP_MIN_CONJ = 1, 2
 JP_CAP_SPHERE, JP_CAP_BOX, JP_CAP_ELLIPSOID = 1, 2, 3
+JP_CAP_HARMONIC, JP_CAP_BIQUADRATIC = 1, 2
 JP_E_MIN_STEP = -140
 
 
@@ -283,6 +285,7 @@ def make_restraints(rd, keep):
         r.cap_atom_radius = float(cap.get("atom_radius", 0.0))
         r.cap_atom_k = float(cap.get("atom_k", 0.0))
         r.cap_shape = int(cap.get("shape", JP_CAP_SPHERE))   # box: wall / atom_wall [6];
+        r.cap_function = int(cap.get("function", JP_CAP_HARMONIC))
         for key, n in (("wall", 6), ("atom_wall", 6), ("ellipse", 3), ("atom_ellipse", 3)):
             if key in cap:                                   # ellipsoid: ellipse / atom_ellipse [3]
                 getattr(r, "cap_" + key)[:] = [float(v) for v in np.ravel(cap[key])][:n]

@@ -410,6 +410,10 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
           return JP_E_INVALID;
         if ((q.ncap_group && !q.cap_group) || (q.ncap_atom && !q.cap_atom)) return JP_E_INVALID;
         if (q.cap_shape < 0 || q.cap_shape > JP_CAP_ELLIPSOID) return JP_E_INVALID;
+        if (q.cap_function < 0 || q.cap_function > JP_CAP_BIQUADRATIC) return JP_E_INVALID;
+        if (q.cap_function == JP_CAP_BIQUADRATIC && q.cap_shape > JP_CAP_SPHERE) return JP_E_INVALID;
+        if (q.cap_function == JP_CAP_BIQUADRATIC && (!(q.cap_radius > 0.0) || !(q.cap_atom_radius > 0.0)))
+          return JP_E_INVALID;
         for (int k = 0; k < 6 && q.cap_shape == JP_CAP_BOX; k += 2)
           if (!fin(q.cap_wall[k]) || !fin(q.cap_wall[k + 1]) || !(q.cap_wall[k] <= q.cap_wall[k + 1]) ||
               !fin(q.cap_atom_wall[k]) || !fin(q.cap_atom_wall[k + 1]) ||
@@ -1090,7 +1094,8 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
         t.p[3] = q.dihe_kup[i];
         hres.push_back(t);
       }
-      const int shape = q.cap_shape == 0 ? JP_CAP_SPHERE : q.cap_shape;
+      const int quartic = q.cap_function == JP_CAP_BIQUADRATIC;   // sphere only (validated)
+      const int shape = quartic ? 4 : q.cap_shape == 0 ? JP_CAP_SPHERE : q.cap_shape;
       auto shape_params = [&](Restr &t, const double *wall, const double *ell) {
         if (shape == JP_CAP_BOX) for (int k = 0; k < 6; ++k) t.p[6 + k] = wall[k];
         if (shape == JP_CAP_ELLIPSOID) for (int k = 0; k < 3; ++k) t.p[6 + k] = ell[k];

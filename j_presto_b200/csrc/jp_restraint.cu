@@ -17,6 +17,7 @@
 namespace jp {
 
 constexpr int kResThreads = 128;
+constexpr int kCapSphereQuartic = 4;   // shape code of the sphere with the half-biquadratic function
 
 __device__ __forceinline__ void res_image(const Rep& R, double* d) {
   if (R.free_bnd) return;
@@ -165,6 +166,14 @@ __device__ __forceinline__ bool cap_term(const Restr& Q, int shape, const double
     return true;
   }
   const double d2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];   // sphere
+  if (shape == kCapSphereQuartic) {   // half-biquadratic (dnecap.f90:253-281)
+    const double r2 = Q.p[3] * Q.p[3];
+    if (!(d2 > r2)) return false;
+    const double sq = (d2 - r2) / r2;
+    e = 0.25 * k * sq * sq * r2;
+    for (int m = 0; m < 3; ++m) g[m] = k * sq * c[m];
+    return true;
+  }
   if (!(d2 > Q.p[3] * Q.p[3])) return false;
   const double d = sqrt(d2), dd = d - Q.p[3];
   e = 0.5 * k * dd * dd;

@@ -62,6 +62,7 @@ struct Ctx {
   std::vector<int> cap_atoms;                    // iamcap
   double cap_c[3] = {0, 0, 0}, cap_r = 0, cap_k = 0, cap_ra = 0, cap_ka = 0;
   int cap_shape = 1;                             // capshp: 1 sphere, 2 box, 3 ellipsoid
+  int cap_func = 1;                              // iufcap: 1 half-harmonic, 2 half-biquadratic
   double cap_wall[6] = {0}, cap_awall[6] = {0}, cap_ell[3] = {0}, cap_aell[3] = {0};
   // CELRES: each atom's residue (first, last atom), -1 = the atom's own position picks its
   // cell; empty = none
@@ -637,7 +638,35 @@ void restraints(Ctx& c, const double* x, double* ene, double* grad) {
     ecap += k * over * over;
     for (int m = 0; m < 3; ++m) tg[m] = T[m] * (k * over / d);
   };
+  if (c.cap_func == JP_CAP_BIQUADRATIC) {   // iufcap 2 (dnecap.f90:253-281), sphere
+    double eg = 0.0, ea = 0.0;
+    const double r2 = c.cap_r * c.cap_r, r2a = c.cap_ra * c.cap_ra;
+    for (const auto& g : c.cap_groups) {
+      double m = 0.0, C[3] = {0, 0, 0};
+      for (int a = g.first; a <= g.second; ++a) {
+        m += c.mass[a];
+        for (int k = 0; k < 3; ++k) C[k] += c.mass[a] * x[3 * a + k];
+      }
+      for (int k = 0; k < 3; ++k) C[k] = C[k] / m - c.cap_c[k];
+      const double dist = C[0] * C[0] + C[1] * C[1] + C[2] * C[2];
+      const double d3 = std::max((dist - r2) / r2, 0.0);
+      eg += d3 * d3 * r2;
+      for (int a = g.first; a <= g.second; ++a)
+        for (int k = 0; k < 3; ++k) grad[3 * a + k] += C[k] * c.cap_k * d3 * (c.mass[a] / m);
+    }
+    for (int a : c.cap_atoms) {
+      double T[3];
+      for (int k = 0; k < 3; ++k) T[k] = x[3 * a + k] - c.cap_c[k];
+      const double dist = T[0] * T[0] + T[1] * T[1] + T[2] * T[2];
+      if (dist <= r2a) continue;
+      const double d3 = (dist - r2a) / r2a;
+      ea += d3 * d3 * r2a;
+      for (int k = 0; k < 3; ++k) grad[3 * a + k] += c.cap_ka * d3 * T[k];
+    }
+    ecap = (eg * c.cap_k + ea * c.cap_ka) * 0.25;
+  }
   for (const auto& g : c.cap_groups) {   // centre of mass of each included chain
+    if (c.cap_func == JP_CAP_BIQUADRATIC) break;
     double m = 0.0, C[3] = {0, 0, 0}, tg[3];
     for (int a = g.first; a <= g.second; ++a) {
       m += c.mass[a];
@@ -649,12 +678,13 @@ void restraints(Ctx& c, const double* x, double* ene, double* grad) {
       for (int k = 0; k < 3; ++k) grad[3 * a + k] += tg[k] * (c.mass[a] / m);
   }
   for (int a : c.cap_atoms) {
+    if (c.cap_func == JP_CAP_BIQUADRATIC) break;
     double T[3], tg[3];
     for (int k = 0; k < 3; ++k) T[k] = x[3 * a + k] - c.cap_c[k];
     cap(T, x + 3 * a, c.cap_ka, c.cap_ra, c.cap_awall, c.cap_aell, tg);   // box: absolute coordinates
     for (int k = 0; k < 3; ++k) grad[3 * a + k] += tg[k];
   }
-  ecap *= 0.5;
+  if (c.cap_func != JP_CAP_BIQUADRATIC) ecap *= 0.5;
   ene[JP_E_POSRES] += epos;
   ene[JP_E_DISTRES] += enoe;
   ene[JP_E_DIHERES] += edhc;
@@ -1558,6 +1588,7 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
     c->cap_r = q.cap_radius; c->cap_k = q.cap_k;
     c->cap_ra = q.cap_atom_radius; c->cap_ka = q.cap_atom_k;
     c->cap_shape = q.cap_shape == 0 ? JP_CAP_SPHERE : q.cap_shape;
+    c->cap_func = q.cap_function == 0 ? JP_CAP_HARMONIC : q.cap_function;
     for (int k = 0; k < 6; ++k) { c->cap_wall[k] = q.cap_wall[k]; c->cap_awall[k] = q.cap_atom_wall[k]; }
     for (int k = 0; k < 3; ++k) { c->cap_ell[k] = q.cap_ellipse[k]; c->cap_aell[k] = q.cap_atom_ellipse[k]; }
   }

@@ -127,3 +127,20 @@ def test_cap_shapes_vs_oracle(eng_mod, drop, shape):
         assert rms_rel(g, go) < gtol
         np.testing.assert_allclose(ene, eo, rtol=etol, atol=1e-7 if prec == FP64 else 1e-2)
         np.testing.assert_allclose(ene[abi.JP_E_CAP], eo[abi.JP_E_CAP], rtol=1e-9)
+
+
+def test_biquadratic_cap_vs_oracle(eng_mod, drop):
+    cap = dict(drop["restraints"]["cap"], function=abi.JP_CAP_BIQUADRATIC)
+    top = dict(drop, restraints=dict(drop["restraints"], cap=cap))
+    kw = dict(method=abi.JP_METHOD_CANO, bounda=NONE)
+    eo, go = oracle.Oracle(top, **kw).energy_grad()
+    assert eo[abi.JP_E_CAP] > 1.0
+    for prec, gtol in ((FP64, 1e-12), (MIXED, 1e-5)):
+        with eng_mod.Engine(top, precision=prec, **kw) as e:
+            ene, g = e.energy_grad()
+        assert rms_rel(g, go) < gtol
+        np.testing.assert_allclose(ene[abi.JP_E_CAP], eo[abi.JP_E_CAP], rtol=1e-9)
+    bad = dict(cap, shape=abi.JP_CAP_BOX, wall=np.zeros(6), atom_wall=np.zeros(6))
+    with pytest.raises(eng_mod.JpError) as ex:   # function 2 belongs to the sphere
+        eng_mod.Engine(dict(top, restraints=dict(cap=bad)), precision=MIXED, **kw)
+    assert ex.value.code == abi.JP_E_INVALID

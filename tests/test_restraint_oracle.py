@@ -242,3 +242,37 @@ def test_box_cap_gradient_is_the_derivative(drop):
             xm[a, k] -= h
             fd = (o.energy_grad(xp)[0][abi.JP_E_CAP] - o.energy_grad(xm)[0][abi.JP_E_CAP]) / (2 * h)
             assert abs(fd - g[a, k]) < 1e-5 * max(1.0, abs(g[a, k]))
+
+
+def test_biquadratic_cap(drop):
+    """CAP function 2 (dnecap.f90:253-281): 1/4 k R^2 ((d^2 - R^2) / R^2)^2 outside the sphere,
+    for group centres and atoms; its gradient is the derivative."""
+    cap = dict(drop["restraints"]["cap"], function=abi.JP_CAP_BIQUADRATIC)
+    top = dict(drop, restraints=dict(cap=cap))
+    kw = dict(method=CANO, bounda=NONE)
+    o = oracle.Oracle(top, **kw)
+    e1, g1 = o.energy_grad()
+    g0 = oracle.Oracle(_plain(top), **kw).energy_grad()[1]
+    x = np.asarray(top["cord"], float)
+    m = np.asarray(top["mass"], float)
+    want = 0.0
+    for f, l in cap["groups"]:
+        c = (m[f:l + 1, None] * x[f:l + 1]).sum(0) / m[f:l + 1].sum() - cap["center"]
+        s = max(((c * c).sum() - cap["radius"] ** 2) / cap["radius"] ** 2, 0.0)
+        want += 0.25 * cap["k"] * cap["radius"] ** 2 * s * s
+    for a in cap["atoms"]:
+        c = x[a] - cap["center"]
+        s = max(((c * c).sum() - cap["atom_radius"] ** 2) / cap["atom_radius"] ** 2, 0.0)
+        want += 0.25 * cap["atom_k"] * cap["atom_radius"] ** 2 * s * s
+    assert want > 1.0
+    np.testing.assert_allclose(e1[abi.JP_E_CAP], want, rtol=1e-11)
+    g = g1 - g0
+    moved = np.flatnonzero(np.abs(g).sum(1) > 1e-6)[:20]
+    h = 1e-6
+    for a in moved:
+        for k in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[a, k] += h
+            xm[a, k] -= h
+            fd = (o.energy_grad(xp)[0][abi.JP_E_CAP] - o.energy_grad(xm)[0][abi.JP_E_CAP]) / (2 * h)
+            assert abs(fd - g[a, k]) < 1e-5 * max(1.0, abs(g[a, k]))
