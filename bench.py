@@ -74,10 +74,12 @@ def barrier():
 
 
 def allmax(x):
+    """Max over ranks (NCCL on the GPU; a CPU tensor under gloo)."""
     import torch
     import torch.distributed as dist
     if dist.is_available() and dist.is_initialized():
-        t = torch.tensor([float(x)], device="cuda")
+        dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([float(x)], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
     return float(x)
