@@ -94,7 +94,11 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # raw samples go to JP_CLOCKS_DIR (default: the system temporary directory); the
+        # JSON line carries their summary
+        import tempfile
+        out = os.environ.get("JP_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out, f"clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
