@@ -1095,7 +1095,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
         hres.push_back(t);
       }
       const int quartic = q.cap_function == JP_CAP_BIQUADRATIC;   // sphere only (validated)
-      const int shape = quartic ? 4 : q.cap_shape == 0 ? JP_CAP_SPHERE : q.cap_shape;
+      const int shape = quartic ? kCapSphereQuartic : q.cap_shape == 0 ? JP_CAP_SPHERE : q.cap_shape;
       auto shape_params = [&](Restr &t, const double *wall, const double *ell) {
         if (shape == JP_CAP_BOX) for (int k = 0; k < 6; ++k) t.p[6 + k] = wall[k];
         if (shape == JP_CAP_ELLIPSOID) for (int k = 0; k < 3; ++k) t.p[6 + k] = ell[k];

@@ -108,6 +108,7 @@ struct Term {
 
 // restraint or CAP term of one replica (jp_restraint.cu); atoms are global ids
 enum : int { R_POS = 0, R_DIST = 1, R_DIHE = 2, R_CAPG = 3, R_CAPA = 4 };
+constexpr int kCapSphereQuartic = 4;   // CAP shape code: sphere with the half-biquadratic function
 struct Restr {
   int kind;
   int rep;

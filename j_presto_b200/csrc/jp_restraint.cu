@@ -1,4 +1,4 @@
-// jp_restraint.cu -- restraints and the spherical CAP boundary (dneres.f90, dnecap.f90).
+// jp_restraint.cu -- restraints and the CAP boundary (dneres.f90, dnecap.f90).
 //
 //   position  (dposc,  dneres.f90:48-101):  E = 1/2 k |x - ref|^2,       dE/dx = k (x - ref)
 //   distance  (ddistc, dneres.f90:107-221): R = <r^-6>^(-1/6) over the pairs of two atom
@@ -6,9 +6,10 @@
 //             dE/dx_i = 4 k (R^2 - r0^2) R^8 / n  sum_j r_ij^-8 (x_i - x_j)
 //   dihedral  (dcdihe, dneres.f90:227-378): phi in [0, 2 pi); outside [lo, up] E =
 //             k (phi - wall)^2 measured from the nearer wall (the far one across 2 pi)
-//   CAP       (dnecap iufcap 1, dnecap.f90:80-250 and :428-437): half-harmonic terms on a
-//             group's centre of mass (gradient shared by mass) or a listed atom: outside a
-//             sphere, outside box walls per coordinate, or outside an ellipsoid
+//   CAP       (dnecap.f90:80-281 and :428-437): terms on a group's centre of mass (gradient
+//             shared by mass) or a listed atom: half-harmonic outside a sphere, outside box
+//             walls per coordinate or outside an ellipsoid (iufcap 1), half-biquadratic
+//             outside a sphere (iufcap 2)
 // Minimum image as in the _PB variants under BOUNDA= PBC; none under BOUNDA= NO (_CB).
 // One restraint per thread, FP64 arithmetic on both paths (they are few); forces go to the
 // class-BB accumulators with weight 1 (grad(:,:,nfrg)), energies to enevcc(11..14).
@@ -17,7 +18,6 @@
 namespace jp {
 
 constexpr int kResThreads = 128;
-constexpr int kCapSphereQuartic = 4;   // shape code of the sphere with the half-biquadratic function
 
 __device__ __forceinline__ void res_image(const Rep& R, double* d) {
   if (R.free_bnd) return;
