@@ -15,6 +15,52 @@ import numpy as np
 from . import engine
 
 
+def write_nf(path, nf, alsd=False):
+    """The weight as md_run reads it (inmcmd.f90:21-38, list-directed, one READ per line):
+    nwindow ndeg / c(0..ndeg) of each window one per line, then its low high / alphalw
+    alphaup / celw ceup / tempce / with ALSD (CLSTMETHOD= LMD*) the walls lower upper."""
+    coef = np.atleast_2d(np.asarray(nf["coef"], np.float64))
+    nwin, ndeg = coef.shape[0], coef.shape[1] - 1
+    lines = [f"{nwin} {ndeg}"]
+    for w in range(nwin):
+        lines += [repr(float(v)) for v in coef[w]]
+        lines.append(f"{float(nf['low'][w])!r} {float(nf['high'][w])!r}")
+    lines.append(f"{float(nf['alphalw'])!r} {float(nf['alphaup'])!r}")
+    lines.append(f"{float(nf['celw'])!r} {float(nf['ceup'])!r}")
+    lines.append(repr(float(nf["tempce"])))
+    if alsd:
+        lines.append(f"{float(nf.get('lower', 0.0))!r} {float(nf.get('upper', 0.0))!r}")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def read_nf(path, alsd=False):
+    """A weight file as inmcmd.f90 reads it: each READ takes the first values of the next
+    line (Fortran D exponents accepted); the dict has the keys jp_ge takes."""
+    with open(path) as f:
+        recs = [ln.replace("D", "E").replace("d", "e").replace(",", " ").split()
+                for ln in f if ln.strip()]
+    it = iter(recs)
+    head = next(it)
+    nwin, ndeg = int(head[0]), int(head[1])
+    coef = np.zeros((nwin, ndeg + 1))
+    low, high = np.zeros(nwin), np.zeros(nwin)
+    for w in range(nwin):
+        for j in range(ndeg + 1):
+            coef[w, j] = float(next(it)[0])
+        r = next(it)
+        low[w], high[w] = float(r[0]), float(r[1])
+    a = next(it)
+    c = next(it)
+    t = next(it)
+    nf = dict(coef=coef, low=low, high=high, alphalw=float(a[0]), alphaup=float(a[1]),
+              celw=float(c[0]), ceup=float(c[1]), tempce=float(t[0]))
+    if alsd:
+        wl = next(it)
+        nf["lower"], nf["upper"] = float(wl[0]), float(wl[1])
+    return nf
+
+
 def predicted_flatness(x, y, w, f, e_span):
     """Flatness (percent) of the next run's histogram over the sampled points (w > 0,
     0 <= x <= 1) if it ran with weight values f at x.  e_span = ceup - celw."""
