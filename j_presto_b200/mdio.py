@@ -19,6 +19,10 @@ both.  The Fortran driver keeps its own writers; these produce the same records 
 
 Under periodic boundaries outtco first moves every chain by whole box lengths so that its
 geometric centre lies in the cell (PBcord.f90); `wrap_chains` does that.
+
+Restart files (outrst.f90 / inprst.f90:37-56), always double precision:
+    title (80 characters) / natom, nvar / step, time, E_total, E_kin, E_pot /
+    coordinates (3, natom) / velocities (3, nvar) / lambda, lambda velocity
 """
 import struct
 
@@ -123,6 +127,35 @@ class EnergyWriter(_Writer):
         _rec(self.f, self._pack([("i", step), ("r", time), ("r", cpu)]))
         _rec(self.f, self._pack([("r", etot), ("r", ekin), ("r", temp)] + [("r", v) for v in e]
                                 + [("r", rmsf), ("i", n15v), ("i", n15h), ("r", rmsd)]))
+
+
+def write_restart(path, cord, vel, step=0, time=0.0, etot=0.0, ekin=0.0, epot=0.0, lam=0.0,
+                  lam_v=0.0, title="     VERLET"):
+    """A restart file as outrst.f90 writes it (all atoms variable: nvar = natom)."""
+    x = np.ascontiguousarray(cord, np.float64).reshape(-1, 3)
+    v = np.ascontiguousarray(vel, np.float64).reshape(-1, 3)
+    with open(path, "wb") as f:
+        _rec(f, title.encode("ascii", "replace")[:80].ljust(80))
+        _rec(f, struct.pack("<ii", len(x), len(v)))
+        _rec(f, struct.pack("<i4d", int(step), float(time), float(etot), float(ekin), float(epot)))
+        _rec(f, x.tobytes())
+        _rec(f, v.tobytes())
+        _rec(f, struct.pack("<2d", float(lam), float(lam_v)))
+
+
+def read_restart(path):
+    """The records inprst.f90 reads: dict(title, step, time, etot, ekin, epot, cord, vel,
+    lam, lam_v); a file without the last record has lam = lam_v = 0."""
+    recs = read_records(path)
+    natom, nvar = struct.unpack("<ii", recs[1])
+    step, time, etot, ekin, epot = struct.unpack("<i4d", recs[2])
+    out = dict(title=recs[0].decode("ascii", "replace").rstrip(), step=step, time=time, etot=etot,
+               ekin=ekin, epot=epot,
+               cord=np.frombuffer(recs[3], np.float64).reshape(natom, 3).copy(),
+               vel=np.frombuffer(recs[4], np.float64).reshape(nvar, 3).copy(), lam=0.0, lam_v=0.0)
+    if len(recs) > 5:
+        out["lam"], out["lam_v"] = struct.unpack("<2d", recs[5])
+    return out
 
 
 def read_trajectory(path, precision=REAL4):

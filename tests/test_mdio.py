@@ -52,3 +52,19 @@ def test_wrap_chains():
     out = mdio.wrap_chains(x, [(0, 1), (2, 2)], box, wall_lo=np.zeros(3))
     np.testing.assert_allclose(out, [[1.0, 1.0, 1.0], [2.0, 1.0, 1.0], [7.0, 5.0, 5.0]])
     np.testing.assert_allclose(out[1] - out[0], x[1] - x[0])
+
+
+def test_restart_round_trip(tmp_path):
+    """outrst.f90 records: title, natom nvar, step time energies, coordinates, velocities,
+    lambda; read back as inprst.f90 reads them."""
+    rng = np.random.default_rng(5)
+    x, v = rng.normal(size=(6, 3)), rng.normal(size=(6, 3))
+    p = tmp_path / "restart.dat"
+    mdio.write_restart(p, x, v, step=500, time=1.0, etot=-3.5, ekin=2.0, epot=-5.5, lam=0.8, lam_v=0.01)
+    recs = mdio.read_records(p)
+    assert [len(r) for r in recs] == [80, 8, 4 + 32, 6 * 24, 6 * 24, 16]
+    r = mdio.read_restart(p)
+    assert (r["step"], r["time"], r["epot"], r["lam"], r["lam_v"]) == (500, 1.0, -5.5, 0.8, 0.01)
+    np.testing.assert_array_equal(r["cord"], x)
+    np.testing.assert_array_equal(r["vel"], v)
+    assert r["title"].startswith("     VERLET")
