@@ -3,23 +3,28 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload: the solvated-polymer system (159-residue chain + 7,000 waters + ions, 22,860
-atoms, 62 A cubic PBC cell, zero-dipole cut-off 12 A, SHAKE on X-H and rigid waters,
-METHOD= CANO at 300 K, 2 fs), synthetic and seeded.  One step = one md_run MD step
-(forces, Hoover-Evans thermostat with the SHAKE<->thermostat loop, SHAKE) with the pair
-list rebuilt every UPDATE=10 steps, exactly as runmd does.
+Headline workload (the metric's target configuration): 64 independent McMD replicas of
+uneven size -- 8-30-residue chains in 600-9,000 waters, 2,000-30,000 atoms each, about
+1.06 M atoms in all -- METHOD= GE with degree-8 weights spanning 280-700 K, zero-dipole
+cut-off 12 A, SHAKE on X-H and rigid waters, 2 fs, the pair list rebuilt every UPDATE=10
+steps as runmd does.  All 64 run in one mixed-precision context: one CUDA graph per step.
+Synthetic and seeded.
 
 Reported (one JSON line on rank 0):
-  value      aggregate ns/day of the mixed-precision path (FP32 pair arithmetic, 64-bit
+  value      aggregate ns/day of the batched mixed path (FP32 pair arithmetic, 64-bit
              fixed-point forces, FP64 integration), device-timed with CUDA events, state
              resident in HBM, L2 flushed between timed steps
-  e2e        the same metric through the C ABI with host buffers: per step copy x, v in
-             from pinned host memory, one jp_step, copy x, v and the energies out
-  fp64       the plain FP64 GPU path on the same workload, and the speed-up over it
-  rms_force_err  RMS relative force error of the mixed path against the FP64 path
+  e2e        the same metric through the C ABI with host buffers: every step copies all
+             replicas' coordinates and velocities in from pinned host memory, runs one step
+             and copies coordinates, velocities and energies out (jp_step_io, one
+             synchronisation), timed by the host clock
+  fp64       the 64 replicas one after another on the plain FP64 GPU path; speedup_vs_fp64
   roofline   the pair kernel (dominant) against the measured FP32 FMA peak
-  cpu_baseline  the CPU oracle (OpenMP FP64 restatement of md_run) on the host cores
-With N > 1 (torchrun) every rank runs its own replica of the workload (replicas only, no
+  accuracy   per configuration the mixed path against the FP64 path (RMS relative force
+             error, potential-energy error) and the NVE drift of both paths
+  c2, c3     the single-system configurations (solvated polymer, 99,200-atom water box)
+  cpu_baseline  the CPU oracle (OpenMP FP64 restatement of md_run) on a bounded sample
+With N > 1 (torchrun) every rank runs its own copy of the workload (replicas only, no
 data-path collective); value = all ranks' simulated time / max-over-ranks device time.
 """
 import argparse
@@ -39,10 +44,17 @@ METRIC = "aggregate ns/day & pairs/s: mixed vs FP64 GPU path at ≤1e-5 RMS forc
 DT_FS = 2.0
 FLOPS_PER_PAIR = 52          # FP32 flops per pair interaction within rc (FMA = 2)
 L2_FLUSH_BYTES = 256 << 20   # > 126 MB L2
-PAIR_PROFILE = os.path.join(ROOT, "profiles", "k_pair_mixed_c2.md")
+PAIR_PROFILE = os.path.join(ROOT, "profiles", "k_pair_mixed_c4.md")
 
 
-def workload_name(natom):
+def c4_name(natoms):
+    return (f"{len(natoms)} McMD replicas batched (METHOD= GE, degree-8 weights 280-700 K): "
+            f"8-30-residue chains in 600-9,000 waters, {min(natoms):,}-{max(natoms):,} atoms, "
+            f"{sum(natoms):,} in total; ZD cut-off 12 A (list 13.5 A, UPDATE 10), SHAKE X-H + rigid "
+            "water, dt 2 fs")
+
+
+def c2_name(natom):
     return (f"solvated polymer: 159-residue chain + 7,000 waters + Na+/Cl-, {natom:,} atoms, "
             "62 A cubic PBC, ZD cut-off 12 A (list 13.5 A, UPDATE 10), SHAKE X-H + rigid "
             "water, METHOD= CANO 300 K, dt 2 fs")
@@ -157,100 +169,84 @@ def measured_peaks():
     return json.load(open(p)) if os.path.exists(p) else {}
 
 
-def cpu_baseline(top, budget_s=15.0):
+def c4_system(dev):
+    """The 64 replicas and their McMD weights: 280-700 K over a range around each replica's
+    starting potential energy (evaluated once on the FP64 path)."""
+    from j_presto_b200 import abi, engine, systems
+    reps = systems.config_c4(workers=os.cpu_count())
+    natoms = [int(t["natom"]) for t in reps]
+    for t in reps:                       # a placeholder to create the McMD context
+        t["ge"] = systems.mcmd_weight(-1.0e7, 1.0e7)
+    with engine.Engine(reps, precision=abi.JP_PREC_FP64, method=abi.JP_METHOD_GE, device=dev) as e:
+        for r, t in enumerate(reps):
+            e0 = e.energy_grad(r)[0][0]
+            t["ge"] = systems.mcmd_weight(e0 - 0.1 * natoms[r], e0 + 0.3 * natoms[r])
+    return reps, natoms
+
+
+def cpu_baseline(reps, budget_s=15.0):
     """The CPU oracle (FP64 OpenMP restatement of md_run) on a bounded sample of the same
-    workload, all host threads."""
+    workload, all host threads: every replica advanced by the same number of steps."""
     import oracle
     from j_presto_b200 import abi
     nth = os.cpu_count() or 1
-    o = oracle.Oracle(top, method=abi.JP_METHOD_CANO, nthreads=nth)
+    ors = [oracle.Oracle(t, method=abi.JP_METHOD_GE, nthreads=nth) for t in reps]
     t0 = time.perf_counter()
-    o.run(1)
+    for o in ors:
+        o.run(1)
     t1 = time.perf_counter() - t0
-    n = int(max(2, min(200, budget_s / max(t1, 1e-3))))
+    n = int(max(1, min(20, budget_s / max(t1, 1e-3))))
     t0 = time.perf_counter()
-    ier, _, _ = o.run(n)
+    ier = 0
+    for o in ors:
+        ier = ier or o.run(n)[0]
     el = time.perf_counter() - t0
-    return {"value": ns_per_day(n, el), "unit": "ns/day", "cores": nth, "kind": "port",
-            "sample": f"{n} CANO steps of the same {top['natom']}-atom workload "
-                      f"(oracle/oracle.cpp, OpenMP FP64), {el:.1f} s", "ier": ier}
+    return {"value": ns_per_day(n * len(ors), el), "unit": "ns/day (aggregate)", "cores": nth,
+            "kind": "port",
+            "sample": f"{n} McMD steps of each of the {len(ors)} replicas (oracle/oracle.cpp, OpenMP "
+                      f"FP64, one replica after another), {el:.1f} s", "ier": int(ier)}
 
 
 def run_reference(args, rank):
     """--impl reference: the reference path's CPU implementation (md_run cannot be built
-    here: no Fortran compiler), i.e. the oracle port, on the host cores."""
+    here or on the GPU box: no Fortran compiler), i.e. the oracle port, on the host cores,
+    on the same 64-replica workload: a step advances every replica by one MD step."""
     if rank != 0:
         return
-    from j_presto_b200 import systems
-    top = systems.config_c2()
     import oracle
-    from j_presto_b200 import abi
+    from j_presto_b200 import abi, systems
+    reps = systems.config_c4(workers=os.cpu_count())
+    natoms = [int(t["natom"]) for t in reps]
     nth = os.cpu_count() or 1
-    o = oracle.Oracle(top, method=abi.JP_METHOD_CANO, nthreads=nth)
+    ors = []
+    for t in reps:
+        o0 = oracle.Oracle(t, method=abi.JP_METHOD_MICR, nthreads=nth)
+        e0 = o0.energy_grad()[0][0]
+        t["ge"] = systems.mcmd_weight(e0 - 0.1 * t["natom"], e0 + 0.3 * t["natom"])
+        ors.append(oracle.Oracle(t, method=abi.JP_METHOD_GE, nthreads=nth))
     w = max(1, min(args.warmup, 3))
-    o.run(w)
+    for o in ors:
+        o.run(w)
     t0 = time.perf_counter()
     done, budget = 0, 150.0
     while done < args.steps:
-        o.run(1)
+        for o in ors:
+            o.run(1)
         done += 1
         if time.perf_counter() - t0 > budget:
             break
     el = time.perf_counter() - t0
-    v = ns_per_day(done, el)
+    v = ns_per_day(done * len(ors), el)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ns/day", "n_gpus": args.gpus,
             "steps": done, "warmup": w, "ms_per_step": 1e3 * el / done, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_name(int(top["natom"])), "atoms": int(top["natom"])},
+            "config": {"workload": c4_name(natoms), "atoms": sum(natoms), "replicas": len(natoms)},
             "cpu_baseline": {"value": v, "unit": "ns/day", "cores": nth, "kind": "port",
-                             "sample": f"{done} CANO steps, oracle/oracle.cpp OpenMP FP64 "
+                             "sample": f"{done} steps of each of the {len(ors)} McMD replicas, "
+                                       "oracle/oracle.cpp OpenMP FP64, one replica after another "
                                        "(md_run itself needs a Fortran compiler, absent)"},
             "e2e": {"value": v, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-def c4_measure(dev, steps=20, warmup=3):
-    """C4: 64 uneven McMD replicas (8-30-residue chains in 600-9,000 waters), batched in one
-    mixed-precision context (one CUDA graph per step) against the same 64 run one after the
-    other on the FP64 path.  Both device-timed over `steps` steps after `warmup`."""
-    from j_presto_b200 import abi, engine, systems
-    reps = systems.config_c4(workers=os.cpu_count())
-    natoms = [int(t["natom"]) for t in reps]
-    for t in reps:                       # a placeholder to create the McMD contexts
-        t["ge"] = systems.mcmd_weight(-1.0e7, 1.0e7)
-    kw = dict(method=abi.JP_METHOD_GE, device=dev)
-    eng = engine.Engine(reps, precision=abi.JP_PREC_MIXED, **kw)
-    weights = []
-    for r, t in enumerate(reps):         # 280-700 K over a range around each start energy
-        e0 = eng.energy_grad(r)[0][0]
-        w = systems.mcmd_weight(e0 - 0.1 * natoms[r], e0 + 0.3 * natoms[r])
-        weights.append(w)
-        eng.ge_set(w, r)
-    eng.step(warmup, energies=False, temps=False)
-    eng.step(steps, energies=False, temps=False)
-    t_mix = eng.last_timing()[0] / 1e3
-    per_step, _ = eng.launch_counts()
-    eng.close()
-    t64 = 0.0
-    for r, t in enumerate(reps):
-        t["ge"] = weights[r]
-        e = engine.Engine(t, precision=abi.JP_PREC_FP64, **kw)
-        e.step(warmup, energies=False, temps=False)
-        e.step(steps, energies=False, temps=False)
-        t64 += e.last_timing()[0] / 1e3
-        e.close()
-    n = len(reps)
-    mix = ns_per_day(steps * n, t_mix)
-    fp64 = ns_per_day(steps * n, t64)
-    return {"workload": f"{n} McMD replicas (METHOD= GE, degree-8 weights 280-700 K): 8-30-residue "
-                        f"chains in 600-9,000 waters, {min(natoms):,}-{max(natoms):,} atoms, "
-                        f"{sum(natoms):,} in total, 2 fs, SHAKE X-H + rigid water",
-            "atoms": sum(natoms), "replicas": n, "steps": steps,
-            "mixed_batched": {"value": mix, "unit": "ns/day (aggregate)",
-                              "ms_per_step": 1e3 * t_mix / steps, "launches_per_step": per_step},
-            "fp64_back_to_back": {"value": fp64, "unit": "ns/day (aggregate)",
-                                  "ms_per_step": 1e3 * t64 / steps},
-            "speedup": mix / fp64}
 
 
 def timed_loop(eng, steps, flush_buf):
@@ -265,14 +261,105 @@ def timed_loop(eng, steps, flush_buf):
     return per
 
 
+def phase_times(eng, steps):
+    """Per-launch device times of the step's phases (timing mode: direct launches with CUDA
+    events on the context's stream around each phase)."""
+    eng.set_timing(True)
+    eng.step(steps, energies=False, temps=False)
+    _, ph, ln = eng.last_timing()
+    eng.set_timing(False)
+    return {"pair": ph[0] / max(1, ln[0]), "bonded": ph[1] / max(1, ln[1]),
+            "integrate": ph[2] / max(1, ln[2]), "rebuild_per_call": ph[3] / max(1, ln[3])}
+
+
+def e2e_loop(eng, natom_total, nrep, steps):
+    """jp_step_io per step with pinned host buffers; host wall clock."""
+    import torch
+    hx = torch.empty((natom_total, 3), dtype=torch.float64, pin_memory=True).numpy()
+    hv = torch.empty((natom_total, 3), dtype=torch.float64, pin_memory=True).numpy()
+    he = torch.empty((1, nrep, 15), dtype=torch.float64, pin_memory=True).numpy()
+    eng.step_io(None, None, hx, hv, nsteps=0)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        eng.step_io(hx, hv, hx, hv, he, nsteps=1)
+    return time.perf_counter() - t0, 2 * hx.nbytes, 2 * hx.nbytes + he.nbytes
+
+
+def single_config(top, dev, steps, warmup, flush, with_e2e=False):
+    """A single-system configuration (CANO): mixed and FP64 ns/day, phase times, errors."""
+    from j_presto_b200 import abi, engine
+    kw = dict(method=abi.JP_METHOD_CANO, device=dev)
+    out = {"atoms": int(top["natom"])}
+    grads = {}
+    for name, prec in (("mixed", abi.JP_PREC_MIXED), ("fp64", abi.JP_PREC_FP64)):
+        with engine.Engine(top, precision=prec, **kw) as e:
+            ene, g = e.energy_grad()
+            grads[name] = (ene, g)
+            pairs = e.pair_count()
+            ntiles, nlisted, _ = e.list_stats()
+            e.step(warmup, energies=False, temps=False)
+            per = timed_loop(e, steps, flush)
+            t = sum(per) / 1e3
+            out[name] = {"value": ns_per_day(steps, t), "unit": "ns/day", "ms_per_step": 1e3 * t / steps,
+                         "phase_ms": phase_times(e, max(10, steps))}
+            if name == "mixed":
+                out.update(pairs_in_cutoff=pairs, tiles=ntiles, pairs_listed=nlisted,
+                           tile_efficiency=pairs / (ntiles * 1024.0) if ntiles else None)
+                if with_e2e:
+                    te, bi, bo = e2e_loop(e, int(top["natom"]), 1, steps)
+                    out["e2e"] = {"value": ns_per_day(steps, te), "unit": "ns/day",
+                                  "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo}
+    out["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    (em, gm), (e64, g64) = grads["mixed"], grads["fp64"]
+    out["rms_force_err"] = float(np.sqrt(((gm - g64) ** 2).sum() / (g64 ** 2).sum()))
+    out["energy_err"] = float(abs(em[0] - e64[0]) / abs(e64[0]))
+    return out
+
+
+def accuracy(dev, c2_acc, c3_acc):
+    """Mixed against FP64 on every single-system configuration, and NVE drift (C1': 1,000
+    waters at liquid density, METHOD= MICR, SHAKE, 2 fs, 20 ps) of both paths in kT per ns
+    per degree of freedom, the total energy kept as md_run keeps it (potential energy at t
+    plus the kinetic energy of (v(t-dt/2) + v(t+dt/2)) / 2)."""
+    import oracle
+    from j_presto_b200 import abi, engine, systems
+    kb = 8.31451 / 4184.0
+    acc = {"c2": c2_acc, "c3": c3_acc}
+    c1 = systems.config_c1()
+    g = {}
+    for name, prec in (("mixed", abi.JP_PREC_MIXED), ("fp64", abi.JP_PREC_FP64)):
+        with engine.Engine(c1, precision=prec, method=abi.JP_METHOD_MICR, device=dev) as e:
+            g[name] = e.energy_grad()
+    (em, gm), (e64, g64) = g["mixed"], g["fp64"]
+    acc["c1"] = {"rms_force_err": float(np.sqrt(((gm - g64) ** 2).sum() / (g64 ** 2).sum())),
+                 "energy_err": float(abs(em[0] - e64[0]) / abs(e64[0]))}
+    top = systems.config_c1_prime()
+    dof = oracle.Oracle(top, method=abi.JP_METHOD_MICR).dof
+    nsteps = 10000
+    drift = {}
+    for name, prec in (("mixed", abi.JP_PREC_MIXED), ("fp64", abi.JP_PREC_FP64)):
+        with engine.Engine(top, precision=prec, method=abi.JP_METHOD_MICR, device=dev) as e:
+            E, T = e.step(nsteps)
+        tot = E[:, 0, 0] + 0.5 * dof * kb * T[:, 0]
+        skip = nsteps // 10
+        t_ns = np.arange(nsteps) * DT_FS * 1e-6
+        slope = np.polyfit(t_ns[skip:], tot[skip:], 1)[0]
+        drift[name] = float(slope / (kb * T[skip:, 0].mean() * dof))
+    acc["nve_drift_kT_per_ns_per_dof"] = {
+        "workload": f"C1': 1,000 waters (3,000 atoms) in a 31 A box, METHOD= MICR, SHAKE, 2 fs, "
+                    f"{nsteps} steps ({nsteps * DT_FS / 1000:.0f} ps), {dof} degrees of freedom",
+        **drift}
+    return acc
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
-    ap.add_argument("--no-c4", action="store_true", help="skip the 64-replica batched McMD line")
+    ap.add_argument("--no-extra", action="store_true", help="only the headline (no C2/C3/accuracy)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local = dist_setup(args.gpus)
@@ -287,63 +374,51 @@ def main():
     barrier()
     dev = local
     torch.cuda.set_device(dev)
-    top = systems.config_c2()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dev}")
-    kw = dict(method=abi.JP_METHOD_CANO, device=dev)
-    eng = engine.Engine(top, precision=abi.JP_PREC_MIXED, **kw)
-    e_mix, g_mix = eng.energy_grad()
-    pairs0 = eng.pair_count()
-    ntiles, nlisted, nslots = eng.list_stats()
+    reps, natoms = c4_system(dev)
+    nrep, ntot = len(reps), sum(natoms)
+    kw = dict(method=abi.JP_METHOD_GE, device=dev)
+    eng = engine.Engine(reps, precision=abi.JP_PREC_MIXED, **kw)
+    for r in range(nrep):
+        eng.energy_grad(r)
+    pairs = float(sum(eng.pair_count(r) for r in range(nrep)))
+    ntiles, nlisted, _ = eng.list_stats()
     per_step, per_rebuild = eng.launch_counts()
-    # warm-up + timed (mixed, resident state, per-step L2 flush)
+    # warm-up + timed (resident state, L2 flushed between steps)
     eng.step(args.warmup, energies=False, temps=False)
     barrier()
     torch.cuda.synchronize()
     with Clocks(dev) as clk:
         per = timed_loop(eng, args.steps, flush)
     torch.cuda.synchronize()
-    t_mix = sum(per) / 1e3
-    t_max = allmax(t_mix)
-    value = ns_per_day(args.steps * world, t_max)
-    # steady-state without flushes (informational)
-    eng.step(args.steps, energies=False, temps=False)
-    t_resident = eng.last_timing()[0] / 1e3
-    # pair-kernel duration from CUDA events around each launch (timing mode, same stream)
-    eng.set_timing(True)
-    eng.step(args.steps, energies=False, temps=False)
-    _, ph, ln = eng.last_timing()
-    eng.set_timing(False)
-    pair_ms = ph[0] / max(1, ln[0])
-    _, _ = eng.energy_grad()
-    pairs1 = eng.pair_count()
-    pairs = 0.5 * (pairs0 + pairs1)
-    # e2e through the C ABI with host buffers (pinned)
-    n = top["natom"]
-    hx = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
-    hv = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
-    eng.get_state(0, hx, hv)
-    torch.cuda.synchronize()
+    t_max = allmax(sum(per) / 1e3)
+    value = ns_per_day(args.steps * nrep * world, t_max)
+    phases = phase_times(eng, max(10, args.steps))
+    pair_ms = phases["pair"]
     barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        eng.set_state(0, hx, hv)
-        eng.step(1, energies=True, temps=False)
-        eng.get_state(0, hx, hv)
-    t_e2e = allmax(time.perf_counter() - t0)
-    e2e = ns_per_day(args.steps * world, t_e2e)
+    te, h2d, d2h = e2e_loop(eng, ntot, nrep, args.steps)
+    t_e2e = allmax(te)
+    e2e = ns_per_day(args.steps * nrep * world, t_e2e)
     eng.close()
-    # FP64 path on the same workload
-    eng64 = engine.Engine(top, precision=abi.JP_PREC_FP64, **kw)
-    e64, g64 = eng64.energy_grad()
-    eng64.step(args.warmup, energies=False, temps=False)
-    per64 = timed_loop(eng64, args.steps, flush)
-    t64 = allmax(sum(per64) / 1e3)
-    v64 = ns_per_day(args.steps * world, t64)
-    eng64.close()
-    rms = float(np.sqrt(((g_mix - g64) ** 2).sum() / (g64 ** 2).sum()))
+    # the same replicas one after another on the FP64 path
+    t64 = 0.0
+    for t in reps:
+        with engine.Engine(t, precision=abi.JP_PREC_FP64, **kw) as e:
+            e.step(args.warmup, energies=False, temps=False)
+            e.step(args.steps, energies=False, temps=False)
+            t64 += e.last_timing()[0] / 1e3
+    t64 = allmax(t64)
+    v64 = ns_per_day(args.steps * nrep * world, t64)
     if rank != 0:
         barrier()
         return
+    clocks = clk.summary()
+    c2 = c3 = acc = None
+    if not args.no_extra and world == 1:
+        c2 = single_config(systems.config_c2(), dev, args.steps, args.warmup, flush, with_e2e=True)
+        c3 = single_config(systems.config_c3(), dev, args.steps, args.warmup, flush)
+        acc = accuracy(dev, {k: c2[k] for k in ("rms_force_err", "energy_err")},
+                       {k: c3[k] for k in ("rms_force_err", "energy_err")})
     peak = engine.calibrate_fp32(dev)
     achieved = FLOPS_PER_PAIR * pairs / (pair_ms * 1e-3) / 1e12
     traffic, tsrc = ncu_traffic()
@@ -351,32 +426,28 @@ def main():
     hbm_src = "of measured"
     if not hbm_peak:   # the pool's earlier copy-bandwidth measurement
         hbm_peak, hbm_src = 6650.0, "of fallback (MEASURED_PEAKS.json absent)"
-    cpu = None if args.no_cpu else cpu_baseline(top)
-    c4 = None if (args.no_c4 or world > 1) else c4_measure(dev)
-    clocks = clk.summary()
+    cpu = None if args.no_cpu else cpu_baseline(reps)
     nreb = args.steps // 10
     line = {
         "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_name(int(n)), "atoms": int(n), "precision": "FP32 pair arithmetic, "
-                   "64-bit fixed-point force/energy accumulation, FP64 integrate+SHAKE",
-                   "l2": "flushed (256 MB write) between timed steps", "replicas_per_gpu": 1,
+        "config": {"workload": c4_name(natoms), "atoms": ntot, "replicas": nrep,
+                   "precision": "FP32 pair arithmetic, 64-bit fixed-point force/energy accumulation, "
+                                "FP64 integrate+SHAKE",
+                   "l2": "flushed (256 MB write) between timed steps",
                    "parallelism": f"replicas x{world}"},
         "pairs_per_s": pairs * world * args.steps / t_max,
         "pairs_in_cutoff": pairs, "tiles": ntiles, "pairs_listed": nlisted,
         "tile_efficiency": pairs / (ntiles * 1024.0) if ntiles else None,
-        "ms_per_step_resident": 1e3 * t_resident / args.steps,
-        "fp64": {"value": v64, "unit": "ns/day", "ms_per_step": 1e3 * t64 / args.steps},
+        "fp64": {"value": v64, "unit": "ns/day", "ms_per_step": 1e3 * t64 / args.steps,
+                 "note": "the same replicas one after another, each in its own FP64 context"},
         "speedup_vs_fp64": value / v64,
-        "rms_force_err": rms,
-        "phase_ms_per_step": {"pair": ph[0] / max(1, ln[0]), "bonded": ph[1] / max(1, ln[1]),
-                              "integrate": ph[2] / max(1, ln[2]),
-                              "rebuild_per_call": ph[3] / max(1, ln[3])},
+        "phase_ms": phases,
         "clocks": clocks,
-        "e2e": {"value": e2e, "unit": "ns/day", "h2d_bytes_per_step": 2 * 3 * 8 * int(n),
-                "d2h_bytes_per_step": 2 * 3 * 8 * int(n) + 8 * abi.JP_MAXENE,
-                "timing": "host wall clock around set_state + jp_step(1) + get_state"},
+        "e2e": {"value": e2e, "unit": "ns/day", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "timing": "host wall clock around jp_step_io(1): all replicas' x, v in from pinned "
+                          "memory, one step, x, v and energies out, one synchronisation"},
         "gpu_launches": args.steps * per_step + nreb * per_rebuild,
         "roofline": {"bound": "fp32", "kernel": "k_pair_mixed", "achieved": achieved,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
@@ -388,8 +459,10 @@ def main():
                      "note": f"{FLOPS_PER_PAIR} FP32 flops per pair within rc x pairs per launch / "
                              "CUDA-event launch time; peak = FP32 FMA loop measured in this run "
                              "(MEASURED_PEAKS.json lists HBM and bf16 tensor peaks only)"},
+        "accuracy": acc,
+        "c2": c2,
+        "c3": c3,
         "cpu_baseline": cpu,
-        "c4_batched_mcmd": c4,
     }
     print(json.dumps(line), flush=True)
     barrier()

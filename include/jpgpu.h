@@ -325,6 +325,17 @@ int jp_energy_grad(jp_ctx *ctx, int32_t replica, const double *cord, double *ene
  * the instantaneous temperature of v(t+dt/2). */
 int jp_step(jp_ctx *ctx, int32_t nsteps, double *ene_out, double *temp_out);
 
+/* jp_step with the state in host memory, for a driver that keeps cord/vel itself: the
+ * coordinates and velocities of all replicas (concatenated in replica order, [natom_total][3];
+ * NULL = keep the device's) are copied in, nsteps steps run, and the state after the last
+ * step (NULL = not wanted), the energies and the temperatures are copied out, all queued on
+ * the context's stream ahead of one synchronisation (a second one only when a SHAKE failure
+ * has to be redone).  Equivalent to jp_set_state + jp_step + jp_get_state for every replica
+ * (md.f90:544-553 with the state exchange of outrst.f90:56-61).  Pinned host buffers make
+ * the copies asynchronous. */
+int jp_step_io(jp_ctx *ctx, int32_t nsteps, const double *cord_in, const double *vel_in,
+               double *cord_out, double *vel_out, double *ene_out, double *temp_out);
+
 /* shake_PB(r1, r2, iprint, ier) (verlet.f90:196): constrain r1 against reference r2,
  * both [natom][3] host arrays of one replica.  Test hook. */
 int jp_shake(jp_ctx *ctx, int32_t replica, double *r1, const double *r2);
@@ -355,14 +366,22 @@ int jp_set_timing(jp_ctx *ctx, int enable);
  * A step whose integration lanes exceed the grid runs the grid-stride form, with the unit
  * state in the atom arrays between phases, as large systems do.  Test and tuning hook. */
 int jp_set_grid_limit(jp_ctx *ctx, int32_t blocks);
+
+/* Bound of every grid-barrier wait inside the cooperative integration kernel, in SM clock
+ * cycles (0 = the default, 2e9: about one second).  A wait that runs out makes the kernel
+ * record the timeout and every block return at its next barrier; the step then returns
+ * JP_E_TIMEOUT with the barrier, sums and accumulators cleared, so the context stays usable
+ * after jp_set_state.  No counterpart in the reference (md_run has no device waits). */
+int jp_set_wait_limit(jp_ctx *ctx, int64_t cycles);
 int jp_last_timing(jp_ctx *ctx, double *total_ms, double *phase_ms4, int32_t *launches4);
 
 /* Kernel launches per jp_step step (excluding list rebuilds) and per list rebuild. */
 int jp_launch_counts(jp_ctx *ctx, int32_t *per_step, int32_t *per_rebuild);
 
-/* Pair-list statistics of the current list, all replicas: tiles (32x32 atom blocks), pair
- * slots set in their masks (pairs within rc+1.5 at the last rebuild, exclusions removed),
- * and the number of atoms padded into blocks. */
+/* Pair-list statistics of the current list, all replicas: tiles (the pair kernels' work
+ * units: a block of 32 i atoms with 32 j entries), pair slots set in their masks (pairs
+ * within rc+1.5 at the last rebuild, exclusions removed), and the number of atoms padded
+ * into blocks. */
 int jp_list_stats(jp_ctx *ctx, int64_t *ntiles, int64_t *npairs_listed, int64_t *nslots);
 
 /* FP32 FMA throughput of `device` in TFLOP/s (best of 5 timed FMA-chain launches): the

@@ -34,6 +34,20 @@ struct Timing {
   int launches[4] = {0, 0, 0, 0};
 };
 
+// The dynamic state an MD step changes, copied aside on the device so that a step whose
+// SHAKE failed can be undone (verlethe.f90:552-574 restores cord, vel and lambda and redoes
+// the step with half the time step): coordinates, velocities, lambda and its velocity, the
+// CMM far-field cache, the energy histograms, the step counters, and the per-step energy
+// and temperature record of the history row being written.
+struct Snap {
+  double *x = nullptr, *v = nullptr, *lam = nullptr, *gwk = nullptr;
+  long long *cmm_e = nullptr;
+  unsigned long long *hist = nullptr;
+  int *ctr = nullptr;
+  double *ene_row = nullptr, *temp_row = nullptr;
+  int row = 0;   // history row the record copies belong to
+};
+
 }  // namespace
 
 struct jp_ctx {
@@ -73,6 +87,10 @@ struct jp_ctx {
   std::vector<cudaEvent_t> tev;
   Timing tm;
   int launches_step = 0, launches_rebuild = 0;
+  bool rebuild_pending = false;     // the list rebuild due after the last step taken
+  Snap snap[3];                     // segment start, step start, a sub-step's accepted state
+  bool snap_ready = false;
+  int nstep_retry = 0;              // steps redone with a halved time step (all calls)
 };
 
 namespace {
@@ -116,6 +134,8 @@ int dput(jp_ctx *c, T **p, const std::vector<T> &h) {
 }
 
 constexpr double kEekcal = 332.06378;
+// bound of a grid-barrier wait in the integration (SM cycles: about one second)
+constexpr long long kDefaultWaitCycles = 2000000000LL;
 constexpr int kGeCap = JP_GE_MAX_WINDOWS * (JP_GE_MAX_DEG + 3);   // doubles per replica
 
 // a .nf weight in the device layout: per window [low, high, c0..cndeg]
@@ -163,8 +183,9 @@ void enqueue_rebuild(jp_ctx *c) {
   launch_tile_scan(P, c->nchunk, rlim * rlim, (float)rlim, rc * rc, c->cmm, st);
   scan_exclusive(P.chunk_cnt, P.chunk_off, c->nchunk + 1, c->scan_scratch, P.ntiles, st);
   k_tile_emit<<<nwb, 128, 0, st>>>(P, c->nchunk, c->cmm ? 1 : 0);
+  launch_compact_tiles(P, c->nblk, c->cmm, c->scan_scratch, st);
   if (c->hbond) launch_hb_list(P, c->hb_cap, c->zc.nt1, c->nblk, st);
-  c->launches_rebuild = 19 + (c->fp64 ? 1 : 0) + ncmm + (c->hbond ? 1 : 0);
+  c->launches_rebuild = 24 + (c->fp64 ? 1 : 0) + ncmm + (c->hbond ? 1 : 0);
 }
 
 // ---- one MD step ------------------------------------------------------------------------
@@ -269,6 +290,203 @@ int check_status(jp_ctx *c) {
   if (s & ERR_SHAKE_SINGULAR) return JP_E_SHAKE_SINGULAR;
   if (s & ERR_SHAKE_NOCONV) return JP_W_SHAKE_NOT_CONVERGED;
   return JP_E_INVALID;
+}
+
+// ---- undoing a step: SHAKE failure retry (verlethe.f90:552-574, :745-752) ------------------
+__global__ void k_check_finite(const double *a, long long n, unsigned *status) {
+  bool bad = false;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    bad |= !isfinite(a[i]);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, ERR_NONFINITE);
+}
+
+int snap_alloc(jp_ctx *c) {
+  if (c->snap_ready) return 0;
+  int e = 0;
+  for (Snap &S : c->snap) {
+    e |= dalloc(c, &S.x, 3 * (size_t)c->natom);
+    e |= dalloc(c, &S.v, 3 * (size_t)c->natom);
+    e |= dalloc(c, &S.lam, 2 * (size_t)c->nrep);
+    if (c->cmm) {
+      e |= dalloc(c, &S.gwk, 3 * (size_t)c->natom);
+      e |= dalloc(c, &S.cmm_e, (size_t)c->nrep);
+    }
+    e |= dalloc(c, &S.hist, (size_t)c->nrep * JP_GE_MAX_BINS);
+    e |= dalloc(c, &S.ctr, 2);
+    e |= dalloc(c, &S.ene_row, (size_t)c->nrep * JP_MAXENE);
+    e |= dalloc(c, &S.temp_row, (size_t)c->nrep);
+  }
+  if (e) return JP_E_CUDA;
+  c->snap_ready = true;
+  return 0;
+}
+
+// copy the whole state (to = true: into S; false: back from S), history row `row`
+int snap_copy(jp_ctx *c, Snap &S, bool to, int row) {
+  DevPtrs &P = c->P;
+  const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+  auto cp = [&](void *snap, void *live, size_t bytes) {
+    return to ? cudaMemcpyAsync(snap, live, bytes, k, c->st) : cudaMemcpyAsync(live, snap, bytes, k, c->st);
+  };
+  if (to) S.row = row;
+  const size_t n3 = 3 * (size_t)c->natom * sizeof(double);
+  CK(cp(S.x, P.x, n3));
+  CK(cp(S.v, P.v, n3));
+  CK(cp(S.lam, P.lam, 2 * (size_t)c->nrep * sizeof(double)));
+  if (c->cmm) {
+    CK(cp(S.gwk, P.gwk, n3));
+    CK(cp(S.cmm_e, P.cmm_e, (size_t)c->nrep * sizeof(long long)));
+  }
+  CK(cp(S.hist, P.ge_hist, (size_t)c->nrep * JP_GE_MAX_BINS * sizeof(unsigned long long)));
+  CK(cp(S.ctr, P.step_ctr, 2 * sizeof(int)));
+  CK(cp(S.ene_row, P.ene_hist + (size_t)S.row * c->nrep * JP_MAXENE, (size_t)c->nrep * JP_MAXENE * sizeof(double)));
+  CK(cp(S.temp_row, P.temp_hist + (size_t)S.row * c->nrep, (size_t)c->nrep * sizeof(double)));
+  if (!to) launch_update_pos(P, c->nslot, c->fp64, c->qscale, c->st);
+  return 0;
+}
+
+// the part of the state that belongs to replica r (S's history row)
+int snap_copy_rep(jp_ctx *c, Snap &S, bool to, int r) {
+  DevPtrs &P = c->P;
+  const Rep &R = c->reps[r];
+  const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+  auto cp = [&](void *snap, void *live, size_t bytes) {
+    return to ? cudaMemcpyAsync(snap, live, bytes, k, c->st) : cudaMemcpyAsync(live, snap, bytes, k, c->st);
+  };
+  const size_t a3 = 3 * (size_t)R.atom0, n3 = 3 * (size_t)R.natom * sizeof(double);
+  CK(cp(S.x + a3, P.x + a3, n3));
+  CK(cp(S.v + a3, P.v + a3, n3));
+  CK(cp(S.lam + 2 * r, P.lam + 2 * r, 2 * sizeof(double)));
+  if (c->cmm) {
+    CK(cp(S.gwk + a3, P.gwk + a3, n3));
+    CK(cp(S.cmm_e + r, P.cmm_e + r, sizeof(long long)));
+  }
+  const size_t h = (size_t)r * JP_GE_MAX_BINS;
+  CK(cp(S.hist + h, P.ge_hist + h, JP_GE_MAX_BINS * sizeof(unsigned long long)));
+  const size_t e = ((size_t)S.row * c->nrep + r) * JP_MAXENE;
+  CK(cp(S.ene_row + (size_t)r * JP_MAXENE, P.ene_hist + e, JP_MAXENE * sizeof(double)));
+  CK(cp(S.temp_row + r, P.temp_hist + (size_t)S.row * c->nrep + r, sizeof(double)));
+  if (!to) launch_update_pos(P, c->nslot, c->fp64, c->qscale, c->st);
+  return 0;
+}
+
+// after an integration that failed: the status word, barrier, sums and accumulators back to
+// their between-steps state (what check_status clears), without mapping the status
+int clear_after_failure(jp_ctx *c) {
+  DevPtrs &P = c->P;
+  CK(cudaMemsetAsync(P.status, 0, sizeof(unsigned), c->st));
+  CK(cudaMemsetAsync(P.bar, 0, sizeof(unsigned) * 4, c->st));
+  if (c->fp64) CK(cudaMemsetAsync(P.grd, 0, sizeof(double) * 3 * c->natom, c->st));
+  else CK(cudaMemsetAsync(P.frc, 0, sizeof(long long) * 3 * c->natom, c->st));
+  CK(cudaMemsetAsync(P.ene_fix, 0, sizeof(long long) * (16 * c->nrep + 1), c->st));
+  CK(cudaMemsetAsync(P.kin_fix, 0, sizeof(long long) * c->nkin * c->nsub, c->st));
+  if (c->ic.stop) CK(cudaMemsetAsync(P.com, 0, sizeof(double) * c->ic.ncom * c->ic.nrep * 16, c->st));
+  if (c->alsd) CK(cudaMemsetAsync(P.ene_cls, 0, sizeof(long long) * 4 * c->nrep, c->st));
+  CK(cudaMemsetAsync(P.rep_fail, 0, sizeof(int) * c->nrep, c->st));
+  return 0;
+}
+
+int read_status(jp_ctx *c, unsigned *s) {
+  CK(cudaMemcpyAsync(s, c->P.status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+constexpr unsigned kShakeBits = ERR_SHAKE_NOCONV | ERR_SHAKE_SINGULAR;
+
+// A step whose SHAKE failed in some replicas (the device state is the failed step's result,
+// `pre` holds the state before it, history row `row`).  As verlethe.f90:552-574 does for its
+// one system, each failing replica goes back to its state before the step and redoes it in
+// sub-steps: on a failure the sub-step is undone and the time step halved (jshk, ishk
+// doubled), after each successful sub-step ishk advances and two completed halves merge
+// back (:745-752), until ishk = jshk; below 1 % of dt the step is abandoned (-9999).
+// Replicas are independent, so the others keep the step they completed.  Each sub-step
+// runs the whole force and integration sequence on every replica with the reduced time
+// step and keeps only the redone replica's result.
+int retry_step(jp_ctx *c, Snap &pre, int row) {
+  std::vector<int> fail(c->nrep, 0);
+  CK(cudaMemcpyAsync(fail.data(), c->P.rep_fail, sizeof(int) * c->nrep, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (int e = clear_after_failure(c)) return e;
+  // a step that started from non-finite coordinates or velocities is not a SHAKE failure
+  for (const double *a : {pre.x, pre.v})
+    k_check_finite<<<64, 256, 0, c->st>>>(a, 3LL * c->natom, c->P.status);
+  unsigned st0 = 0;
+  if (int e = read_status(c, &st0)) return e;
+  if (st0) return check_status(c);
+  Snap &post = c->snap[2];
+  for (int r = 0; r < c->nrep; ++r)
+    if (fail[r])
+      if (int e = snap_copy_rep(c, pre, false, r)) return e;
+  if (int e = snap_copy(c, post, true, row)) return e;
+  int ctr_pre[2];
+  CK(cudaMemcpyAsync(ctr_pre, pre.ctr, sizeof(ctr_pre), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  const double dt = c->prm.dt;
+  IntConst ic = c->ic;
+  for (int r = 0; r < c->nrep; ++r) {
+    if (!fail[r]) continue;
+    double T = 0.5 * dt;
+    int ishk = 0, jshk = 2;
+    ++c->nstep_retry;
+    for (;;) {
+      // one sub-step of every replica from the saved state; replica r's result is kept
+      CK(cudaMemcpyAsync(c->P.step_ctr, ctr_pre, sizeof(ctr_pre), cudaMemcpyHostToDevice, c->st));
+      ic.dt = T;
+      enqueue_forces(c, false);
+      enqueue_bonded(c);
+      if (ic.ge_prescaled) launch_ge_scale(c->P, ic, c->st);
+      launch_integrate(c->P, ic, c->nunit, c->fp64, c->cano_grid, c->st);
+      unsigned st = 0;
+      if (int e = read_status(c, &st)) return e;
+      if (st & ERR_TIMEOUT) return check_status(c);
+      int fr = 0;
+      CK(cudaMemcpyAsync(&fr, c->P.rep_fail + r, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      if (int e = clear_after_failure(c)) return e;
+      if (!fr)
+        if (int e = snap_copy_rep(c, post, true, r)) return e;
+      if (int e = snap_copy(c, post, false, row)) return e;
+      if (fr) {
+        if (T < 0.01 * dt) {
+          CK(cudaMemcpyAsync(c->P.step_ctr, ctr_pre, sizeof(ctr_pre), cudaMemcpyHostToDevice, c->st));
+          CK(cudaStreamSynchronize(c->st));
+          return JP_E_SHAKE_ABORT;
+        }
+        jshk *= 2;
+        ishk *= 2;
+        T *= 0.5;
+        continue;
+      }
+      ++ishk;
+      if (ishk == jshk) break;
+      if (ishk % 2 == 0) { jshk /= 2; ishk /= 2; T *= 2.0; }
+    }
+  }
+  // the step is done: counters one step on; each redone replica counts the energy of its
+  // last sub-step once in its histogram (the .ene record GEprep reads holds that energy)
+  const int ctr_post[2] = {ctr_pre[0] + 1, ctr_pre[1] + 1};
+  CK(cudaMemcpyAsync(c->P.step_ctr, ctr_post, sizeof(ctr_post), cudaMemcpyHostToDevice, c->st));
+  for (int r = 0; r < c->nrep; ++r) {
+    const Rep &R = c->reps[r];
+    if (!fail[r] || R.hist_n <= 0) continue;
+    double e0 = 0.0;
+    CK(cudaMemcpyAsync(&e0, c->P.ene_hist + ((size_t)row * c->nrep + r) * JP_MAXENE, sizeof(double),
+                       cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const double u = (e0 - R.hist_min) * R.hist_inv;   // write_ene_hist's binning
+    if (u > -1.0 && u < (double)R.hist_n) {
+      unsigned long long *b = c->P.ge_hist + R.hist_off + (int)u;
+      unsigned long long cnt = 0;
+      CK(cudaMemcpy(&cnt, b, sizeof(cnt), cudaMemcpyDeviceToHost));
+      ++cnt;
+      CK(cudaMemcpy(b, &cnt, sizeof(cnt), cudaMemcpyHostToDevice));
+    }
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return JP_OK;
 }
 
 int validate(const jp_system *sys, int nrep, const jp_params *prm) {
@@ -559,6 +777,8 @@ int minimize_conj(jp_ctx *c, int r, const jp_min_params *mp, int32_t *iters, dou
   if (eneval) std::memcpy(eneval + (size_t)r * JP_MAXENE, e, sizeof(e));
   return JP_OK;
 }
+
+int flush_rebuild(jp_ctx *c);   // below, beside the step loop
 
 }  // namespace
 
@@ -1161,14 +1381,16 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   for (int r = 0; r < nrep; ++r)
     for (int bb = 0; bb < reps[r].nblk; ++bb) hblk_rep[reps[r].blk0 + bb] = r;
   // tile-list chunks: (i-block, j0) for j0 = i, i+32, ... inside the replica
-  std::vector<int> chunk_i, chunk_j0;
+  std::vector<int> chunk_i, chunk_j0, blk_chunk0(c->nblk + 1, 0);
   for (int bb = 0; bb < c->nblk; ++bb) {
     const Rep &R = reps[hblk_rep[bb]];
+    blk_chunk0[bb] = (int)chunk_i.size();
     for (int j0 = bb; j0 < R.blk0 + R.nblk; j0 += 32) {
       chunk_i.push_back(bb);
       chunk_j0.push_back(j0);
     }
   }
+  blk_chunk0[c->nblk] = (int)chunk_i.size();
   c->nchunk = (int)chunk_i.size();
   c->tile_cap_total = c->nchunk * 32;   // every candidate could be a tile: no overflow
 
@@ -1211,6 +1433,15 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.tiles, (size_t)c->tile_cap_total);
   e |= dalloc(c, &P.tile_shift, (size_t)c->tile_cap_total);
   e |= dalloc(c, &P.masks, (size_t)c->tile_cap_total * 32);
+  // compact tiles: at most one per tile (an i-block's j entries never outnumber 32 per tile)
+  e |= dput(c, &P.blk_chunk0, blk_chunk0);
+  e |= dalloc(c, &P.ct_cnt, (size_t)c->nblk + 1);
+  e |= dalloc(c, &P.ct_off, (size_t)c->nblk + 1);
+  e |= dalloc(c, &P.ct_blk, (size_t)c->tile_cap_total);
+  e |= dalloc(c, &P.ct_j, (size_t)c->tile_cap_total * 32);
+  e |= dalloc(c, &P.ct_mask, (size_t)c->tile_cap_total * 32);
+  e |= dalloc(c, &P.nctiles, 1);
+  if (c->cmm) e |= dalloc(c, &P.ct_mask_el, (size_t)c->tile_cap_total * 32);
   if (c->cmm) {
     int ntot = 0;
     for (int l = 1; l <= 5; ++l) ntot += c->cmm_ncell[l];
@@ -1270,8 +1501,10 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dput(c, &P.nfr, hnfr);
   e |= dalloc(c, &P.scale, (size_t)nrep);
   e |= dalloc(c, &P.done, (size_t)nrep);
+  e |= dalloc(c, &P.rep_fail, (size_t)nrep);
   e |= dalloc(c, &P.status, 1);
   e |= dalloc(c, &P.bar, 4);
+  P.wait_cycles = kDefaultWaitCycles;
   e |= dalloc(c, &P.pair_cnt, (size_t)nrep);
   e |= dalloc(c, &P.ene_hist, (size_t)c->hist_cap * nrep * JP_MAXENE);
   e |= dalloc(c, &P.temp_hist, (size_t)c->hist_cap * nrep);
@@ -1389,6 +1622,7 @@ void jp_destroy(jp_ctx *c) {
 int jp_rebuild_cells(jp_ctx *c, int32_t replica) {
   if (!c || replica < -1 || replica >= c->nrep) return JP_E_INVALID;
   CK(cudaSetDevice(c->device));
+  c->rebuild_pending = false;
   enqueue_rebuild(c);   // all replicas share one pass
   CK(cudaStreamSynchronize(c->st));
   return check_status(c);
@@ -1397,6 +1631,7 @@ int jp_rebuild_cells(jp_ctx *c, int32_t replica) {
 int jp_set_state(jp_ctx *c, int32_t r, const double *cord, const double *vel) {
   if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
   CK(cudaSetDevice(c->device));
+  if (int e = flush_rebuild(c)) return e;
   const Rep &R = c->reps[r];
   if (cord) CK(cudaMemcpyAsync(c->P.x + 3 * (size_t)R.atom0, cord, sizeof(double) * 3 * R.natom,
                                cudaMemcpyHostToDevice, c->st));
@@ -1422,6 +1657,7 @@ int jp_get_state(jp_ctx *c, int32_t r, double *cord, double *vel) {
 int jp_energy_grad(jp_ctx *c, int32_t r, const double *cord, double *eneval, double *grad) {
   if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
   CK(cudaSetDevice(c->device));
+  if (int e = flush_rebuild(c)) return e;
   const Rep &R = c->reps[r];
   if (cord) {
     CK(cudaMemcpyAsync(c->P.x + 3 * (size_t)R.atom0, cord, sizeof(double) * 3 * R.natom,
@@ -1603,6 +1839,7 @@ int jp_minimize(jp_ctx *c, const jp_min_params *mp, int32_t *iters, double *enev
       (!(mp->up > 0.0) || !(mp->down > 0.0) || !std::isfinite(mp->up) || !std::isfinite(mp->down)))
     return JP_E_INVALID;
   CK(cudaSetDevice(c->device));
+  if (int e = flush_rebuild(c)) return e;
   if (mp->method == JP_MIN_CONJ) {   // conj.f90:48-53: no SHAKE with conjugate gradients
     if (mp->line_max < 1 || !(mp->line_conv >= 0.0) || !std::isfinite(mp->line_conv)) return JP_E_INVALID;
     if (c->prm.shake_method != JP_SHAKE_NONE && c->ngroups > 0) return JP_E_INVALID;
@@ -1688,6 +1925,13 @@ int jp_minimize(jp_ctx *c, const jp_min_params *mp, int32_t *iters, double *enev
   return step_err ? JP_E_MIN_STEP : JP_OK;
 }
 
+int jp_set_wait_limit(jp_ctx *c, int64_t cycles) {
+  if (!c || cycles < 0) return JP_E_INVALID;
+  c->P.wait_cycles = cycles > 0 ? (long long)cycles : kDefaultWaitCycles;
+  drop_graphs(c);   // the step graph holds the limit it was captured with
+  return JP_OK;
+}
+
 int jp_set_grid_limit(jp_ctx *c, int32_t blocks) {
   if (!c || blocks < 0) return JP_E_INVALID;
   CK(cudaSetDevice(c->device));
@@ -1710,14 +1954,15 @@ int jp_last_timing(jp_ctx *c, double *total_ms, double *phase_ms4, int32_t *laun
 int jp_list_stats(jp_ctx *c, int64_t *ntiles, int64_t *npairs_listed, int64_t *nslots) {
   if (!c) return JP_E_INVALID;
   CK(cudaSetDevice(c->device));
+  if (int e = flush_rebuild(c)) return e;
   CK(cudaStreamSynchronize(c->st));
   int nt = 0;
-  CK(cudaMemcpy(&nt, c->P.ntiles, sizeof(int), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&nt, c->P.nctiles, sizeof(int), cudaMemcpyDeviceToHost));
   if (ntiles) *ntiles = nt;
   if (nslots) *nslots = c->nslot;
   if (npairs_listed) {
     std::vector<unsigned> m((size_t)nt * 32);
-    if (nt) CK(cudaMemcpy(m.data(), c->P.masks, sizeof(unsigned) * m.size(), cudaMemcpyDeviceToHost));
+    if (nt) CK(cudaMemcpy(m.data(), c->P.ct_mask, sizeof(unsigned) * m.size(), cudaMemcpyDeviceToHost));
     int64_t s = 0;
     for (unsigned v : m) s += __builtin_popcount(v);
     *npairs_listed = s;
@@ -1732,22 +1977,64 @@ int jp_launch_counts(jp_ctx *c, int32_t *per_step, int32_t *per_rebuild) {
   return JP_OK;
 }
 
-int jp_step(jp_ctx *c, int32_t nsteps, double *ene_out, double *temp_out) {
-  if (!c || nsteps < 0) return JP_E_INVALID;
-  CK(cudaSetDevice(c->device));
-  if (nsteps == 0) return JP_OK;
+}  // extern "C"
+
+namespace {
+
+// the list rebuild due after the last step of a jp_step call, run before anything that uses
+// the list (the next step, a force evaluation, a state change)
+int flush_rebuild(jp_ctx *c) {
+  if (!c->rebuild_pending) return 0;
+  c->rebuild_pending = false;
+  if (c->g_rebuild) CK(cudaGraphLaunch(c->g_rebuild, c->st));
+  else enqueue_rebuild(c);
+  return 0;
+}
+
+// what a call returns for steps [done, done + chunk): the energy and temperature records
+// and, after its last step, the state of every replica; then the status word.  Copies on
+// the context's stream, ahead of the one synchronisation that ends the chunk.
+int enqueue_tail(jp_ctx *c, int done, int chunk, double *ene_out, double *temp_out, double *xout,
+                 double *vout, bool last) {
+  DevPtrs &P = c->P;
+  CK(cudaEventRecord(c->ev_b, c->st));
+  if (ene_out)
+    CK(cudaMemcpyAsync(ene_out + (size_t)done * c->nrep * JP_MAXENE, P.ene_hist,
+                       sizeof(double) * (size_t)chunk * c->nrep * JP_MAXENE, cudaMemcpyDeviceToHost, c->st));
+  if (temp_out)
+    CK(cudaMemcpyAsync(temp_out + (size_t)done * c->nrep, P.temp_hist, sizeof(double) * (size_t)chunk * c->nrep,
+                       cudaMemcpyDeviceToHost, c->st));
+  if (last && xout)
+    CK(cudaMemcpyAsync(xout, P.x, sizeof(double) * 3 * (size_t)c->natom, cudaMemcpyDeviceToHost, c->st));
+  if (last && vout)
+    CK(cudaMemcpyAsync(vout, P.v, sizeof(double) * 3 * (size_t)c->natom, cudaMemcpyDeviceToHost, c->st));
+  return 0;
+}
+
+// nsteps iterations of runmd's loop body; xout/vout (nullable, all replicas) receive the
+// state after the last step
+int step_impl(jp_ctx *c, int nsteps, double *ene_out, double *temp_out, double *xout, double *vout) {
   if (!c->tm.enabled && !c->g_step) {
     if (capture(c, &c->g_step, false)) return JP_E_CUDA;
     if (capture(c, &c->g_rebuild, true)) return JP_E_CUDA;
   }
   for (int k = 0; k < 4; ++k) { c->tm.phase_ms[k] = 0.0; c->tm.launches[k] = 0; }
   c->tm.total_ms = 0.0;
+  // SHAKE failures of verlethe are redone with a halved time step; verlet (MICR, CONS)
+  // returns the failure, as md_run stops there (verlet.f90:203, md.f90:557)
+  const bool retry = c->prm.method >= JP_METHOD_CANO && c->prm.shake_method != JP_SHAKE_NONE;
+  if (retry && !c->tm.enabled)
+    if (int e = snap_alloc(c)) return e;
+  auto due = [&]() { return c->prm.update > 0 && c->idloop % c->prm.update == 0; };
   int done = 0;
   while (done < nsteps) {
     const int chunk = std::min(nsteps - done, c->hist_cap);
+    const bool last = done + chunk == nsteps;
     CK(cudaMemsetAsync(c->P.step_ctr + 1, 0, sizeof(int), c->st));
     CK(cudaEventRecord(c->ev_a, c->st));
+    unsigned st = 0;
     if (c->tm.enabled) {
+      if (int e = flush_rebuild(c)) return e;
       const size_t need = (size_t)chunk * 8;
       while (c->tev.size() < need) {
         cudaEvent_t ev;
@@ -1766,15 +2053,14 @@ int jp_step(jp_ctx *c, int32_t nsteps, double *ene_out, double *temp_out) {
         enqueue_integrate(c);
         CK(cudaEventRecord(E[3], c->st));
         c->idloop += 1;
-        if (c->prm.update > 0 && c->idloop % c->prm.update == 0) {
+        if (due()) {
           enqueue_rebuild(c);
           rebuilt[s] = 1;
         }
         CK(cudaEventRecord(E[4], c->st));
       }
-      CK(cudaEventRecord(c->ev_b, c->st));
-      CK(cudaStreamSynchronize(c->st));
-      CK(cudaGetLastError());
+      if (int e = enqueue_tail(c, done, chunk, ene_out, temp_out, xout, vout, last)) return e;
+      if (int e = read_status(c, &st)) return e;
       for (int s = 0; s < chunk; ++s) {
         cudaEvent_t *E = &c->tev[(size_t)s * 8];
         float ms;
@@ -1789,30 +2075,92 @@ int jp_step(jp_ctx *c, int32_t nsteps, double *ene_out, double *temp_out) {
           c->tm.launches[3] += 1;
         }
       }
-    } else {
+    } else if (!retry) {
       for (int s = 0; s < chunk; ++s) {
+        if (int e = flush_rebuild(c)) return e;
         CK(cudaGraphLaunch(c->g_step, c->st));
         c->idloop += 1;
-        if (c->prm.update > 0 && c->idloop % c->prm.update == 0) CK(cudaGraphLaunch(c->g_rebuild, c->st));
+        c->rebuild_pending = due();
       }
-      CK(cudaEventRecord(c->ev_b, c->st));
-      CK(cudaStreamSynchronize(c->st));
-      CK(cudaGetLastError());
+      if (int e = enqueue_tail(c, done, chunk, ene_out, temp_out, xout, vout, last)) return e;
+      if (int e = read_status(c, &st)) return e;
+    } else {
+      // verlethe with SHAKE: segments that end at a list rebuild, each started from a copy of
+      // the state.  A segment in which SHAKE failed is redone from that copy one step at a
+      // time, and the failing step goes through retry_step.  A segment holds no rebuild, so
+      // the copy and the pair list stay consistent.
+      for (int s = 0; s < chunk;) {
+        if (int e = flush_rebuild(c)) return e;
+        int seg = chunk - s;
+        if (c->prm.update > 0) seg = std::min<long long>(seg, c->prm.update - c->idloop % c->prm.update);
+        const bool tail = s + seg == chunk;
+        if (int e = snap_copy(c, c->snap[0], true, s)) return e;
+        for (int k = 0; k < seg; ++k) CK(cudaGraphLaunch(c->g_step, c->st));
+        if (tail)
+          if (int e = enqueue_tail(c, done, chunk, ene_out, temp_out, xout, vout, last)) return e;
+        if (int e = read_status(c, &st)) return e;
+        if (st & ERR_TIMEOUT) return check_status(c);
+        if (st & kShakeBits) {
+          if (int e = clear_after_failure(c)) return e;
+          if (int e = snap_copy(c, c->snap[0], false, s)) return e;
+          for (int k = 0; k < seg; ++k) {
+            if (int e = snap_copy(c, c->snap[1], true, s + k)) return e;
+            CK(cudaGraphLaunch(c->g_step, c->st));
+            if (int e = read_status(c, &st)) return e;
+            if ((st & kShakeBits) && !(st & ERR_TIMEOUT)) {
+              const int rc = retry_step(c, c->snap[1], s + k);
+              if (rc != JP_OK) return rc;
+            } else if (st) {
+              return check_status(c);
+            }
+          }
+          if (tail) {
+            if (int e = enqueue_tail(c, done, chunk, ene_out, temp_out, xout, vout, last)) return e;
+            if (int e = read_status(c, &st)) return e;
+          }
+        }
+        if (st) return check_status(c);
+        c->idloop += seg;
+        s += seg;
+        c->rebuild_pending = due();
+      }
     }
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev_a, c->ev_b));
     c->tm.total_ms += ms;
-    if (ene_out)
-      CK(cudaMemcpy(ene_out + (size_t)done * c->nrep * JP_MAXENE, c->P.ene_hist,
-                    sizeof(double) * (size_t)chunk * c->nrep * JP_MAXENE, cudaMemcpyDeviceToHost));
-    if (temp_out)
-      CK(cudaMemcpy(temp_out + (size_t)done * c->nrep, c->P.temp_hist,
-                    sizeof(double) * (size_t)chunk * c->nrep, cudaMemcpyDeviceToHost));
-    int rs = check_status(c);
-    if (rs != JP_OK) return rs;
+    if (st) return check_status(c);
     done += chunk;
   }
   return JP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int jp_step(jp_ctx *c, int32_t nsteps, double *ene_out, double *temp_out) {
+  if (!c || nsteps < 0) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  if (nsteps == 0) return JP_OK;
+  return step_impl(c, nsteps, ene_out, temp_out, nullptr, nullptr);
+}
+
+int jp_step_io(jp_ctx *c, int32_t nsteps, const double *cord_in, const double *vel_in, double *cord_out,
+               double *vel_out, double *ene_out, double *temp_out) {
+  if (!c || nsteps < 0) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  if (int e = flush_rebuild(c)) return e;
+  const size_t n3 = sizeof(double) * 3 * (size_t)c->natom;
+  if (cord_in) CK(cudaMemcpyAsync(c->P.x, cord_in, n3, cudaMemcpyHostToDevice, c->st));
+  if (vel_in) CK(cudaMemcpyAsync(c->P.v, vel_in, n3, cudaMemcpyHostToDevice, c->st));
+  if (cord_in) launch_update_pos(c->P, c->nslot, c->fp64, c->qscale, c->st);
+  if (nsteps == 0) {
+    if (cord_out) CK(cudaMemcpyAsync(cord_out, c->P.x, n3, cudaMemcpyDeviceToHost, c->st));
+    if (vel_out) CK(cudaMemcpyAsync(vel_out, c->P.v, n3, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return JP_OK;
+  }
+  return step_impl(c, nsteps, ene_out, temp_out, cord_out, vel_out);
 }
 
 int jp_shake(jp_ctx *c, int32_t r, double *r1, const double *r2) {

@@ -402,6 +402,102 @@ __global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm) {
   }
 }
 
+// ---- compact tiles ------------------------------------------------------------------------
+// The pair kernels run on compact tiles: an i-block with 32 j entries, the j atoms of that
+// block's tiles that have at least one listed pair with it, taken in tile order (ascending
+// j block, ascending slot).  A 32 x 32 tile of two blocks holds ~26 % listed pairs at the
+// md_run list radius; keeping only the j atoms some i atom lists raises that to ~45 %, and
+// the pair kernels' work per pair falls in proportion.  The listed pair set is unchanged.
+// Each entry carries its tile's image shift (into the i block's frame) and its slot; the
+// mask keeps the kernels' rotated layout (bit k of lane i: entry (i + k) & 31).
+
+// tiles of i-block bi: [chunk_off[blk_chunk0[bi]], chunk_off[blk_chunk0[bi + 1]])
+__device__ __forceinline__ void blk_tiles(const DevPtrs& P, int bi, int& t0, int& t1) {
+  t0 = P.chunk_off[P.blk_chunk0[bi]];
+  t1 = P.chunk_off[P.blk_chunk0[bi + 1]];
+}
+
+// pass 1: compact tiles per i-block (one warp per i-block)
+__global__ void k_ct_count(DevPtrs P, int nblk) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= nblk) return;
+  int t0, t1;
+  blk_tiles(P, w, t0, t1);
+  int cnt = 0;
+  for (int t = t0; t < t1; ++t) {
+    const unsigned m = P.masks[(size_t)t * 32 + lane];
+    const unsigned row = __funnelshift_l(m, m, lane);   // bit c: pair (lane, j lane c)
+    cnt += __popc(__reduce_or_sync(0xffffffffu, row));
+  }
+  if (lane == 0) P.ct_cnt[w] = (cnt + 31) >> 5;
+}
+
+// pass 2 (after the scan of ct_cnt): one warp per i-block writes its compact tiles.  Lane i
+// builds row i of the current compact tile: the bits of row i of each tile at the tile's
+// occupied j lanes, packed in order; lane c of the tile writes its own entry.
+__global__ void k_ct_emit(DevPtrs P, int nblk, int cmm) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= nblk) return;
+  int t0, t1;
+  blk_tiles(P, w, t0, t1);
+  int out = P.ct_off[w], pos = 0;
+  unsigned cur = 0, cur_el = 0;
+  for (int t = t0; t < t1; ++t) {
+    const unsigned m = P.masks[(size_t)t * 32 + lane];
+    const unsigned row = __funnelshift_l(m, m, lane);
+    unsigned row_el = 0;
+    if (cmm) {
+      const unsigned me = P.masks_el[(size_t)t * 32 + lane];
+      row_el = __funnelshift_l(me, me, lane);
+    }
+    const unsigned cm = __reduce_or_sync(0xffffffffu, row);
+    if (cm == 0u) continue;
+    const int n = __popc(cm);
+    if ((cm >> lane) & 1u) {
+      const int p = pos + __popc(cm & ((1u << lane) - 1u));
+      const float4 sh = P.tile_shift[t];
+      const int slot = P.tiles[t].y * kTile + lane;
+      P.ct_j[(size_t)(out + (p >> 5)) * 32 + (p & 31)] = make_float4(sh.x, sh.y, sh.z, __int_as_float(slot));
+    }
+    unsigned comp = 0, comp_el = 0;   // row's bits at the occupied lanes, packed
+    int q = 0;
+    for (unsigned b = cm; b; b &= b - 1u, ++q) {
+      const int c = __ffs(b) - 1;
+      comp |= ((row >> c) & 1u) << q;
+      comp_el |= ((row_el >> c) & 1u) << q;
+    }
+    cur |= comp << pos;
+    cur_el |= comp_el << pos;
+    if (pos + n >= 32) {
+      P.ct_mask[(size_t)out * 32 + lane] = __funnelshift_r(cur, cur, lane);
+      if (cmm) P.ct_mask_el[(size_t)out * 32 + lane] = __funnelshift_r(cur_el, cur_el, lane);
+      if (lane == 0) P.ct_blk[out] = w;
+      ++out;
+      const int used = 32 - pos;
+      cur = used < 32 ? comp >> used : 0u;
+      cur_el = used < 32 ? comp_el >> used : 0u;
+      pos += n - 32;
+    } else {
+      pos += n;
+    }
+  }
+  if (pos > 0) {   // the last, partly filled compact tile: empty entries (slot -1) after pos
+    if (lane >= pos) P.ct_j[(size_t)out * 32 + lane] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    P.ct_mask[(size_t)out * 32 + lane] = __funnelshift_r(cur, cur, lane);
+    if (cmm) P.ct_mask_el[(size_t)out * 32 + lane] = __funnelshift_r(cur_el, cur_el, lane);
+    if (lane == 0) P.ct_blk[out] = w;
+  }
+}
+
+void launch_compact_tiles(const DevPtrs& P, int nblk, bool cmm, int* scan_scratch, cudaStream_t st) {
+  const int nb = (nblk * 32 + 127) / 128;
+  k_ct_count<<<nb, 128, 0, st>>>(P, nblk);
+  scan_exclusive(P.ct_cnt, P.ct_off, nblk + 1, scan_scratch, P.nctiles, st);
+  k_ct_emit<<<nb, 128, 0, st>>>(P, nblk, cmm ? 1 : 0);
+}
+
 // ---- deterministic exclusive scan (3 passes) --------------------------------------------
 __global__ void k_scan_block_sums(const int* in, int n, int* bsum) {
   __shared__ int sh[1024];

@@ -308,7 +308,7 @@ __device__ double cmm_ext_atom(const DevPtrs& P, const Rep& R, const double* c0,
 }
 
 // warp sum of each lane's energy into a replica's fixed-point slot (rep -1: nothing)
-__device__ __forceinline__ void warp_energy(long long* dst, int rep, double e) {
+__device__ __forceinline__ void warp_energy(const DevPtrs& P, long long* dst, int rep, double e) {
   const unsigned full = 0xffffffffu;
   const unsigned has = __ballot_sync(full, rep >= 0);
   if (has == 0u) return;
@@ -316,9 +316,9 @@ __device__ __forceinline__ void warp_energy(long long* dst, int rep, double e) {
   if (__all_sync(full, rep < 0 || rep == r0)) {
     double v = rep >= 0 ? e : 0.0;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(full, v, o);
-    if ((threadIdx.x & 31) == 0) atomic_add_ll(&dst[r0], to_fix(v, kEneScale));
+    if ((threadIdx.x & 31) == 0) atomic_add_ll(&dst[r0], to_fix(v, kEneScale, P.status));
   } else if (rep >= 0) {
-    atomic_add_ll(&dst[rep], to_fix(e, kEneScale));
+    atomic_add_ll(&dst[rep], to_fix(e, kEneScale, P.status));
   }
 }
 
@@ -354,14 +354,14 @@ __global__ void k_cmm_far(DevPtrs P, int natom, int fp64, int force, double ccoe
         for (int k = 0; k < 3; ++k) {
           const double gk = P.gwk[3 * a + k] + gx[k] * q2;
           if (fp64) atomicAdd(&P.grd[3 * a + k], gk);
-          else atomic_add_ll(&P.frc[3 * a + k], to_fix(gk, kFrcScale));
+          else atomic_add_ll(&P.frc[3 * a + k], to_fix(gk, kFrcScale, P.status));
         }
       }
     }
   }
   // warp-level energy sums (one replica per warp as a rule; mixed warps add per lane)
-  warp_energy(P.cmm_enew, rep, e);
-  warp_energy(P.ene_ext, rep_x, ex);
+  warp_energy(P, P.cmm_enew, rep, e);
+  warp_energy(P, P.ene_ext, rep_x, ex);
 }
 
 // the far-field energy of the step into ELE15: the new sum when due, else the last one

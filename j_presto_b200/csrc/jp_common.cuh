@@ -27,7 +27,11 @@ constexpr double kEneScale = 4294967296.0;
 constexpr double kEneInv = 1.0 / 4294967296.0;
 constexpr double kKinScale = 1099511627776.0;
 constexpr double kKinInv = 1.0 / 1099511627776.0;
-constexpr double kFixMax = 9.0e18;   // |value*scale| must stay below this
+// Largest magnitude of one fixed-point contribution (2^56 in scaled units: a force term of
+// 1.7e7 kcal/mol/A, an energy term of 1.7e7 kcal/mol).  Each accumulator receives at most a
+// few hundred contributions per step, so sums of terms below this bound stay inside the
+// 64-bit range; a term beyond it is reported instead of wrapping the sum.
+constexpr double kFixLim = 72057594037927936.0;
 
 constexpr double kConvcv = 4.184e-4;       // md.f90:56
 constexpr double kGas = 8.31451;           // PHYCNS gascst
@@ -132,6 +136,8 @@ struct MinState {
 };
 
 struct DevPtrs {
+  // bound of every grid-barrier wait of the cooperative integration, in SM clock cycles
+  long long wait_cycles;
   // atoms
   double *x, *v, *x0, *vback, *xback, *forcec;
   double *mass, *imass, *chg;
@@ -159,6 +165,13 @@ struct DevPtrs {
   float4 *tile_shift;             // dense min-image shift of block refs (mixed path)
   unsigned *masks;                // dense masks [T][32]
   int *ntiles;                    // device scalar
+  // compact tiles (what the pair kernels run on): an i-block and 32 j entries
+  int *blk_chunk0;                // [nblk+1] first chunk of each i-block (static)
+  int *ct_cnt, *ct_off;           // compact tiles per i-block and their scan [nblk+1]
+  int *ct_blk;                    // [CT] i-block
+  float4 *ct_j;                   // [CT][32] (image shift into the i frame, slot bits; -1 = empty)
+  unsigned *ct_mask, *ct_mask_el; // [CT][32] rotated masks (listed pairs; CMM Coulomb pairs)
+  int *nctiles;                   // device scalar
   // cell sort
   unsigned *key;                  // per atom
   int *hist, *hist_scan, *cursor; // per key
@@ -198,6 +211,7 @@ struct DevPtrs {
   double *nfr;                    // DOF per sub-system
   double *scale;                  // per replica force scale (GE / pseudo-T)
   int *done;                      // per replica SHAKE-thermostat loop finished
+  int *rep_fail;                  // per replica: a SHAKE group failed this step (1)
   unsigned *status;               // error bits
   unsigned *bar;                  // grid barrier of the cooperative integrator [4]
   long long *pair_cnt;            // [nrep]
@@ -221,8 +235,16 @@ struct DevPtrs {
   MinState *mins;                 // [nrep], allocated by the first jp_minimize
 };
 
-__device__ __forceinline__ long long to_fix(double v, double scale) {
-  return __double2ll_rn(v * scale);
+// v * scale rounded to a 64-bit integer.  A product beyond +-kFixLim sets ERR_FIX_OVERFLOW
+// in *status (ERR_NONFINITE for a NaN or an infinity) and the contribution is dropped, so
+// the call that made it returns an error instead of a silently wrapped sum.
+__device__ __forceinline__ long long to_fix(double v, double scale, unsigned *status) {
+  const double s = v * scale;
+  if (!(fabs(s) < kFixLim)) {
+    atomicOr(status, isfinite(s) ? ERR_FIX_OVERFLOW : ERR_NONFINITE);
+    return 0;
+  }
+  return __double2ll_rn(s);
 }
 
 __device__ __forceinline__ void atomic_add_ll(long long *p, long long v) {
@@ -242,9 +264,9 @@ __device__ __forceinline__ void add_grad(const DevPtrs& P, double fs, int a, dou
     atomicAdd(&P.grd[3 * a + 1], gy);
     atomicAdd(&P.grd[3 * a + 2], gz);
   } else {
-    atomic_add_ll(&P.frc[3 * a + 0], to_fix(gx, kFrcScale));
-    atomic_add_ll(&P.frc[3 * a + 1], to_fix(gy, kFrcScale));
-    atomic_add_ll(&P.frc[3 * a + 2], to_fix(gz, kFrcScale));
+    atomic_add_ll(&P.frc[3 * a + 0], to_fix(gx, kFrcScale, P.status));
+    atomic_add_ll(&P.frc[3 * a + 1], to_fix(gy, kFrcScale, P.status));
+    atomic_add_ll(&P.frc[3 * a + 2], to_fix(gz, kFrcScale, P.status));
   }
 }
 
@@ -256,9 +278,9 @@ __device__ __forceinline__ void add_energy(const DevPtrs& P, int rep, int slot, 
   const bool uni = __all_sync(full, key == k0);
   if (uni) {
     for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(full, e, o);
-    if ((threadIdx.x & 31) == 0) atomic_add_ll(&P.ene_fix[key], to_fix(e, kEneScale));
+    if ((threadIdx.x & 31) == 0) atomic_add_ll(&P.ene_fix[key], to_fix(e, kEneScale, P.status));
   } else if (e != 0.0) {
-    atomic_add_ll(&P.ene_fix[key], to_fix(e, kEneScale));
+    atomic_add_ll(&P.ene_fix[key], to_fix(e, kEneScale, P.status));
   }
 }
 
@@ -269,9 +291,9 @@ __device__ __forceinline__ void add_cls_energy(const DevPtrs& P, int rep, int cl
   const int k0 = __shfl_sync(full, key, 0);
   if (__all_sync(full, key == k0)) {
     for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(full, e, o);
-    if ((threadIdx.x & 31) == 0 && e != 0.0) atomic_add_ll(&P.ene_cls[key], to_fix(e, kEneScale));
+    if ((threadIdx.x & 31) == 0 && e != 0.0) atomic_add_ll(&P.ene_cls[key], to_fix(e, kEneScale, P.status));
   } else if (e != 0.0) {
-    atomic_add_ll(&P.ene_cls[key], to_fix(e, kEneScale));
+    atomic_add_ll(&P.ene_cls[key], to_fix(e, kEneScale, P.status));
   }
 }
 

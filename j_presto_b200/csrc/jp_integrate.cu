@@ -278,9 +278,12 @@ __device__ __forceinline__ void zero_force(const DevPtrs& P, int a) {
   }
 }
 
-__device__ __forceinline__ void shake_status(const DevPtrs& P, int ier) {
+// a SHAKE failure (shake.f90 ier 1 or -2) of a group of replica `rep`: the status bit, and
+// the replica's flag that the host reads to redo its step with a halved time step
+__device__ __forceinline__ void shake_status(const DevPtrs& P, int ier, int rep) {
   if (ier == 1) atomicOr(P.status, ERR_SHAKE_NOCONV);
   else if (ier == -2) atomicOr(P.status, ERR_SHAKE_SINGULAR);
+  P.rep_fail[rep] = 1;
 }
 
 // warp-aggregated fixed-point add of m v^2 into kin_fix[slot][sub]
@@ -290,9 +293,9 @@ __device__ __forceinline__ void add_kin(const DevPtrs& P, int nsub_total, int ks
   long long* dst = P.kin_fix + (size_t)kslot * nsub_total;
   if (__all_sync(full, sub == s0)) {
     for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(full, e, o);
-    if ((threadIdx.x & 31) == 0 && s0 >= 0) atomic_add_ll(&dst[s0], to_fix(e, kKinScale));
+    if ((threadIdx.x & 31) == 0 && s0 >= 0) atomic_add_ll(&dst[s0], to_fix(e, kKinScale, P.status));
   } else if (sub >= 0 && e != 0.0) {
-    atomic_add_ll(&dst[sub], to_fix(e, kKinScale));
+    atomic_add_ll(&dst[sub], to_fix(e, kKinScale, P.status));
   }
 }
 
@@ -413,7 +416,7 @@ __device__ __forceinline__ void lam_add_ke(const DevPtrs& P, const IntConst& c, 
                                            double lvt) {
   if (R.lam_ke_sub >= 0)
     atomic_add_ll(&P.kin_fix[(size_t)kslot * c.nsub_total + R.lam_ke_sub],
-                  to_fix(R.lam_m * lvt * lvt, kKinScale));
+                  to_fix(R.lam_m * lvt * lvt, kKinScale, P.status));
 }
 
 // phase 1: the lambda force from the class energies and lambda's half-step velocity
@@ -508,10 +511,10 @@ __device__ void write_ene_hist(const DevPtrs& P, const IntConst& c, int r) {
 
 // Grid barrier for a cooperative launch (all blocks co-resident).  bar[0] counts arrivals
 // over the whole launch (never reset inside it): barrier number e is passed once it reaches
-// e * gridDim.x.  bar[2] is the abort flag.  The wait is bounded (~1 s of SM clock): on
-// timeout the kernel records ERR_TIMEOUT, raises abort and every block returns at its next
-// barrier.  `epoch` is the block's arrival target, advanced by each call.
-constexpr long long kBarrierCycles = 2000000000LL;
+// e * gridDim.x.  bar[2] is the abort flag.  The wait is bounded by P.wait_cycles of SM
+// clock (about 1 s by default): on timeout the kernel records ERR_TIMEOUT, raises abort and
+// every block returns at its next barrier.  `epoch` is the block's arrival target, advanced
+// by each call.
 
 __device__ __forceinline__ bool grid_barrier(const DevPtrs& P, unsigned& epoch) {
   __shared__ int s_ok;
@@ -525,7 +528,7 @@ __device__ __forceinline__ bool grid_barrier(const DevPtrs& P, unsigned& epoch) 
     const long long t0 = clock64();
     while (vb[0] < epoch) {
       if (vb[2] != 0u) { ok = 0; break; }
-      if (clock64() - t0 > kBarrierCycles) {
+      if (clock64() - t0 > P.wait_cycles) {
         atomicOr(P.status, ERR_TIMEOUT);
         atomicExch(&P.bar[2], 1u);
         ok = 0;
@@ -753,7 +756,7 @@ __device__ __forceinline__ double micr_unit(const DevPtrs& P, const IntConst& c,
   }
   if (u.n >= 2 && c.shake_method != JP_SHAKE_NONE) {
     const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
-    if (ier) shake_status(P, ier);
+    if (ier) shake_status(P, ier, u.rep);
     const double ri = 1.0 / c.dt;
     JP_UNIT_LOOP(q)
       for (int k = 0; k < 3; ++k) P.v[3 * u.a[q] + k] = (x1[q][k] - x0[q][k]) * ri;
@@ -843,7 +846,7 @@ __device__ __forceinline__ double micr_pos(const DevPtrs& P, const IntConst& c, 
   }
   if (u.n >= 2 && c.shake_method != JP_SHAKE_NONE) {
     const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
-    if (ier) shake_status(P, ier);
+    if (ier) shake_status(P, ier, u.rep);
     const double ri = 1.0 / c.dt;
     JP_UNIT_LOOP(q)
       for (int k = 0; k < 3; ++k) P.v[3 * u.a[q] + k] = (x1[q][k] - x0[q][k]) * ri;
@@ -1000,7 +1003,7 @@ __device__ __noinline__ double cano3_unit(const DevPtrs& P, const IntConst& c, c
   }
   if (u.n >= 2) {
     const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
-    if (ier) shake_status(P, ier);
+    if (ier) shake_status(P, ier, u.rep);
   }
   const double ri = 1.0 / c.dt;
   bool bad = false;
@@ -1169,7 +1172,7 @@ __device__ __forceinline__ double ru_cano3(const DevPtrs& P, const IntConst& c, 
   if (U.n >= 2) {
     const int ier = shake_small(P.reps[U.rep], U.n, U.d2, U.im, x, x0, c.shake_method,
                                 c.shake_tol, c.shake_maxit);
-    if (ier) shake_status(P, ier);
+    if (ier) shake_status(P, ier, U.rep);
   }
   const double ri = 1.0 / c.dt;
   double ke = 0.0;
@@ -1296,9 +1299,9 @@ __device__ __forceinline__ void add_kin_quad(const DevPtrs& P, int nsub_total, i
   if (__all_sync(full, sub == s0)) {
     e += __shfl_xor_sync(full, e, 8);
     e += __shfl_xor_sync(full, e, 16);
-    if (lane == 0 && s0 >= 0) atomic_add_ll(&dst[s0], to_fix(e, kKinScale));
+    if (lane == 0 && s0 >= 0) atomic_add_ll(&dst[s0], to_fix(e, kKinScale, P.status));
   } else if ((lane & 7) == 0 && sub >= 0 && ke_grp != 0.0) {
-    atomic_add_ll(&dst[sub], to_fix(ke_grp, kKinScale));
+    atomic_add_ll(&dst[sub], to_fix(ke_grp, kKinScale, P.status));
   }
 }
 
@@ -1469,7 +1472,7 @@ __device__ __forceinline__ double q_cano3(const DevPtrs& P, const IntConst& c, c
     x0[k] = S.x0[k][tid];
   }
   const int ier = quad_shake(P.reps[q.rep], q, x, x0, c.shake_tol, c.shake_maxit);
-  if (ier && q.sl == 0) shake_status(P, ier);
+  if (ier && q.sl == 0) shake_status(P, ier, q.rep);
   double ke = 0.0;
   if (q.a >= 0) {
     const double ri = 1.0 / c.dt;
@@ -2084,7 +2087,7 @@ __global__ void k_shake_only(DevPtrs P, IntConst c, int unit0, int nunit) {
     }
   }
   const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
-  if (ier) shake_status(P, ier);
+  if (ier) shake_status(P, ier, u.rep);
   JP_UNIT_LOOP(q)
     for (int k = 0; k < 3; ++k) P.xback[3 * u.a[q] + k] = x1[q][k];
 }

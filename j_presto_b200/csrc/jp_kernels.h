@@ -19,6 +19,8 @@ __global__ void k_fill_pos_d(DevPtrs P, int nslot, double qscale);
 void launch_tile_scan(const DevPtrs& P, int nchunk, double rlim2, float rlimf, double rc2, bool cmm,
                       cudaStream_t st);
 __global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm);
+// compact tiles of every i-block from the tile list (count, scan, emit)
+void launch_compact_tiles(const DevPtrs& P, int nblk, bool cmm, int* scan_scratch, cudaStream_t st);
 void scan_exclusive(const int* in, int* out, int n, int* scratch, int* total, cudaStream_t st);
 
 // ZD pair constants

@@ -40,6 +40,7 @@ static __device__ __align__(256) double g_nb_scratch[kHdr + 3 * JP_NOALLOC_MAX_A
 
 std::mutex g_mu;
 std::atomic<double*> g_ptr[kMaxDevices];
+int g_nsm[kMaxDevices];   // SM count of each device, written before its g_ptr is published
 
 struct NbArgs {
   int natom, ntype, base;
@@ -53,6 +54,19 @@ struct NbArgs {
 
 __device__ __forceinline__ void set_status(double* scr, unsigned bits) {
   atomicOr(reinterpret_cast<unsigned*>(scr + 3), bits);
+}
+
+// exclusion range [p0, p1) of atom i; false (and NB_BAD_INDEX) unless the CSR row is sane:
+// excl_ptr starts at 0, never decreases and no atom has more partners than there are atoms
+__device__ __forceinline__ bool excl_range(double* scr, const NbArgs& a, int i, int& p0, int& p1) {
+  p0 = a.eptr[i];
+  p1 = a.eptr[i + 1];
+  if (p0 < 0 || p1 < p0 || p1 - p0 > a.natom || (i == 0 && p0 != 0)) {
+    set_status(scr, NB_BAD_INDEX);
+    p0 = p1 = 0;
+    return false;
+  }
+  return true;
 }
 
 __device__ __forceinline__ void warp_add(double* dst, double v) {
@@ -86,7 +100,9 @@ __global__ void __launch_bounds__(kNbThreads) k_nb_tiles(double* scr, NbArgs a) 
       const int nj = min(32, a.natom - bj * 32);
       m = nj >= 32 ? 0xffffffffu : ((1u << nj) - 1u);
       if (bj == bi) m &= lane == 31 ? 0u : (0xffffffffu << (lane + 1));
-      for (int p = a.eptr[i]; p < a.eptr[i + 1]; ++p) {
+      int p0, p1;
+      excl_range(scr, a, i, p0, p1);
+      for (int p = p0; p < p1; ++p) {
         const int e = a.eidx[p] - a.base;
         if (e < 0 || e >= a.natom) { set_status(scr, NB_BAD_INDEX); continue; }
         if ((e >> 5) == bj) m &= ~(1u << (e & 31));
@@ -165,7 +181,9 @@ __global__ void __launch_bounds__(kNbThreads) k_nb_excl(double* scr, NbArgs a) {
     double qs = qi;
     const double xi = a.x[3 * i], yi = a.x[3 * i + 1], zi = a.x[3 * i + 2];
     double gx = 0, gy = 0, gz = 0;
-    for (int p = a.eptr[i]; p < a.eptr[i + 1]; ++p) {
+    int p0, p1;
+    excl_range(scr, a, i, p0, p1);
+    for (int p = p0; p < p1; ++p) {
       const int j = a.eidx[p] - a.base;
       if (j < 0 || j >= a.natom) continue;     // flagged by k_nb_tiles
       const double qj = a.q[j];
@@ -213,8 +231,8 @@ __global__ void __launch_bounds__(kNbThreads) k_nb_out(double* scr, int natom, d
 }
 
 // Set-up, once per device, with that device current: the address of this device's
-// instance of g_nb_scratch.
-int scratch_of_current_device(double** out) {
+// instance of g_nb_scratch and the device's SM count (the tile kernel's grid cap).
+int scratch_of_current_device(double** out, int* nsm) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return JP_E_NO_DEVICE;
   if (dev < 0 || dev >= kMaxDevices) return JP_E_NO_DEVICE;
@@ -226,11 +244,16 @@ int scratch_of_current_device(double** out) {
       void* sym = nullptr;
       if (cudaGetSymbolAddress(&sym, g_nb_scratch) != cudaSuccess || !sym) return JP_E_CUDA;
       if (reinterpret_cast<uintptr_t>(sym) % 256 != 0) return JP_E_CUDA;
+      int sms = 0;
+      if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+        return JP_E_CUDA;
+      g_nsm[dev] = sms;
       p = static_cast<double*>(sym);
       g_ptr[dev].store(p, std::memory_order_release);
     }
   }
   *out = p;
+  *nsm = g_nsm[dev];
   return JP_OK;
 }
 
@@ -254,7 +277,8 @@ extern "C" int jp_nonbond_noalloc(int32_t natom, const double *cord, const doubl
   for (int k = 0; k < 3; ++k)   // one image within the cut-off
     if (!(box[k] > 2.0 * cutoff) || !std::isfinite(box[k])) return JP_E_INVALID;
   double* scr = nullptr;
-  int rc = scratch_of_current_device(&scr);
+  int nsm = 0;
+  int rc = scratch_of_current_device(&scr, &nsm);
   if (rc != JP_OK) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
@@ -274,7 +298,7 @@ extern "C" int jp_nonbond_noalloc(int32_t natom, const double *cord, const doubl
   const int nb = (natom + 31) / 32;
   const long long warps = (long long)nb * nb;
   const int wpb = kNbThreads / 32;
-  const int grid = (int)std::min<long long>((warps + wpb - 1) / wpb, 148LL * 16);
+  const int grid = (int)std::min<long long>((warps + wpb - 1) / wpb, (long long)nsm * 16);
   k_nb_tiles<<<grid, kNbThreads, 0, st>>>(scr, a);
   k_nb_excl<<<(natom + kNbThreads - 1) / kNbThreads, kNbThreads, 0, st>>>(scr, a);
   k_nb_out<<<(3 * natom + kNbThreads - 1) / kNbThreads, kNbThreads, 0, st>>>(scr, natom, grad, ene);

@@ -8,24 +8,78 @@
 // with q = charge * sqrt(332.06378/eps) (chgmod, inpcls.f90:215-227), b = 1/(2 rc^3),
 // f = 1/rc^3, z = 1.5/rc (incel.f90:655-658).
 //
-// Work unit: a tile = (i-block, j-block) of 32 x 32 cell-sorted atoms with an interaction
-// mask fixed at list-build time.  One warp per tile: lane l holds i-atom l; the j-atoms and
-// their force accumulators rotate one lane per step through warp shuffles, so after 32
-// steps every lane has seen every j and each j-force is back in the lane that loaded it.
-// Newton's third law: each unordered pair is evaluated once.
+// Work unit: a compact tile (jp_cells.cu) = an i-block of 32 cell-sorted atoms and 32 j
+// entries (j atoms with at least one listed pair in the block, each with the image shift of
+// its block) with an interaction mask fixed at list-build time.  One warp per compact tile:
+// lane l holds i-atom l and at step k meets entry (l + k) & 31; the j-force accumulators
+// rotate one lane per step through warp shuffles, so after 32 steps each is back in the lane
+// of its entry.  Newton's third law: each unordered pair is evaluated once.
 //
 // Warps take tiles one at a time from a global counter, so all finish together whatever
-// their tiles hold (tile work varies with the mask).
-// Mixed path: FP32 pair arithmetic on block-local coordinates (|x| < ~10 A), forces and
-// energies summed per tile in FP32 then added as 64-bit fixed point (2^-32 kcal/mol/A) with
-// integer atomics -- order independent, so results are bit-identical run to run.
-// FP64 path: the same tiles in FP64 with absolute coordinates and FP64 force atomics.
+// their tiles hold.
+// Mixed path: FP32 pair arithmetic on block-local coordinates (|x| < ~30 A), every step of a
+// tile branch-free (a pair outside the mask or the cut-off contributes an exact zero);
+// forces summed per tile in FP32, energies in FP32 over 8 steps then in FP64, both added as
+// 64-bit fixed point
+// (2^-32 kcal/mol/A) with integer atomics -- order independent, so results are
+// bit-identical run to run.  A warp keeps two tiles in flight ahead of the one it computes:
+// the bulk-copy engine (cp.async.bulk, completion on an mbarrier) brings the entries and
+// masks of the tile after next into shared memory, and the gathers of the next tile's
+// j atoms are issued before the current tile's arithmetic.
+// FP64 path: the same compact tiles in FP64 with absolute coordinates, per-pair minimum
+// image and FP64 force atomics.
 #include "jp_kernels.h"
 
 namespace jp {
 
 constexpr int kPairThreads = 256;
-constexpr int kPairClaim = 1;   // tiles a warp claims at a time
+constexpr int kPairWarps = kPairThreads / 32;
+
+// ---- bulk copies into shared memory (TMA engine, no tensor map) -------------------------
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// arm the barrier for `bytes` of incoming copies and start one copy of `bytes` (a multiple
+// of 16, both addresses 16-byte aligned) from global to shared memory
+__device__ __forceinline__ void mbar_expect(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// the shared-memory buffer is about to be overwritten by the async proxy after generic reads
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// wait for phase `parity` of the barrier, at most `limit` SM cycles; false on timeout
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, long long limit) {
+  const long long t0 = clock64();
+  for (;;) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > limit) return false;
+  }
+}
 
 // a warp's energies (ELE15, VDW15; ALSD class AA / AB, BB the rest) and pair count into the
 // replica's slots: 64-bit fixed point, summed per tile, so the totals do not depend on which
@@ -55,123 +109,204 @@ __device__ __forceinline__ void flush_fix(const DevPtrs& P, int rep, long long e
   }
 }
 
-// One 32x32 tile: lane = i atom; the j atoms are staged in the warp's shared-memory slice
-// and read at (lane + k) & 31 in step k; the j-force accumulators rotate one lane per step
-// (3 shuffles) so that after 32 steps each is back in the lane of its atom.
-// ALSD: ci = cluster bit of the i atom; a pair with nA cluster atoms has its force times
-// f2 (nA = 2, class AA), f1 (AB) or 1 (BB), and its energy also goes to ea (AA) / eb (AB).
-// CMM: no cut-off (rc2 is huge) and the Coulomb term only for the pairs of `me` (the
-// neighbouring-cell pairs; the rest of the tile's pairs are LJ only)
+// Per-warp shared memory of the mixed kernel: two bulk-copy buffers (entries and masks of a
+// tile) and the staged j atoms of the tile being computed, stored twice so that step k
+// reads entry lane + k at a constant offset.
+struct __align__(16) MixStage {
+  float4 ent[2][32];
+  unsigned msk[2][32];
+  unsigned msk_el[2][32];
+  float4 pos[64];
+  int typ[64];
+  unsigned long long bar[2];
+};
+
+// what a lane gathers for one tile before computing it: its j entry's atom and image
+// shift, its mask rows, and its i atom
+struct Gather {
+  float4 pj;
+  float sx, sy, sz;
+  int tj, aj;
+  unsigned m, me;
+  int bi;
+};
+
+// One compact tile, every step branch-free.  ALSD: ci = cluster bit of the i atom; a pair
+// with nA cluster atoms has its force times f2 (nA = 2, class AA), f1 (AB) or 1 (BB), and its
+// energy also goes to ea (AA) / eb (AB).  CMM: no cut-off (rc2 is huge) and the Coulomb term
+// only for the pairs of `me` (the neighbouring-cell pairs; the rest are LJ only).
+// Energies: FP32 partial sums over 8 steps, accumulated in FP64.
 template <bool MINIMG, bool COUNT, bool ALSD, bool CMM>
-__device__ __forceinline__ void tile_mixed(const float4* __restrict__ sj_pos, const int* __restrict__ sj_typ,
-                                           const float2* __restrict__ s_lj, int nt1, float4 pi, int ti,
-                                           float4 sh, unsigned m, unsigned me, int lane, float bx, float by, float bz,
-                                           float ibx, float iby, float ibz, float rc2, float zb, float zf,
-                                           float zc, float& fix, float& fiy, float& fiz, float& gjx,
-                                           float& gjy, float& gjz, float& te, float& tl, int& tn,
-                                           int ci, float f1, float f2, float& ea, float& eb) {
-  const float xi = pi.x + sh.x, yi = pi.y + sh.y, zi = pi.z + sh.z;
-  const int row = (ALSD ? (ti & kTypeMask) : ti) * nt1;
-#pragma unroll 4
-  for (int k = 0; k < 32; ++k) {
-    const int jl = (lane + k) & 31;
-    if (m & 1u) {
-      const float4 pj = sj_pos[jl];
-      float dx = xi - pj.x, dy = yi - pj.y, dz = zi - pj.z;
+__device__ __forceinline__ void tile_mixed(const MixStage& S, const float2* __restrict__ s_lj, int row,
+                                           float4 pi, unsigned m, unsigned me, int lane, float bx, float by,
+                                           float bz, float ibx, float iby, float ibz, float rc2, float zb,
+                                           float zf, float zc, float& fix, float& fiy, float& fiz,
+                                           float& gjx, float& gjy, float& gjz, double& te, double& tl,
+                                           int& tn, int ci, float f1, float f2, double& ea, double& eb) {
+  const unsigned full = 0xffffffffu;
+  const int src = (lane + 1) & 31;
+#pragma unroll 1
+  for (int k0 = 0; k0 < 32; k0 += 8) {
+    const float4* __restrict__ sp = S.pos + lane + k0;
+    const int* __restrict__ st = S.typ + lane + k0;
+    const unsigned mk = m >> k0, mek = me >> k0;
+    float te8 = 0.f, tl8 = 0.f, ea8 = 0.f, eb8 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float4 pj = sp[k];
+      const int tjr = st[k];
+      float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
       if (MINIMG) {
         dx -= bx * rintf(dx * ibx);
         dy -= by * rintf(dy * iby);
         dz -= bz * rintf(dz * ibz);
       }
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      if (r2 <= rc2) {
-        const float rinv = rsqrtf(r2);
-        const float r2inv = rinv * rinv;
-        const float r6inv = r2inv * r2inv * r2inv;
-        const int tjr = sj_typ[jl];
-        const float2 lj = s_lj[row + (ALSD ? (tjr & kTypeMask) : tjr)];
-        const float qq = CMM ? ((me & 1u) ? pi.w * pj.w : 0.f) : pi.w * pj.w;
-        const float v1 = lj.x * r6inv;
-        const float v2 = lj.y * r6inv * r6inv;
-        float fs;
-        if (ALSD) {
-          const float e = qq * (rinv + fmaf(zb, r2, -zc)) + (v2 - v1);
-          te = fmaf(qq, rinv + fmaf(zb, r2, -zc), te);
-          tl += v2 - v1;
-          const int na = ci + (tjr >> 30);
-          if (na == 2) ea += e;
-          else if (na == 1) eb += e;
-          fs = (na == 2 ? f2 : na == 1 ? f1 : 1.f) *
-               fmaf(qq, fmaf(rinv, r2inv, -zf), (12.f * v2 - 6.f * v1) * r2inv);
-        } else {
-          te = fmaf(qq, rinv + fmaf(zb, r2, -zc), te);
-          tl += v2 - v1;
-          fs = fmaf(qq, fmaf(rinv, r2inv, -zf), (12.f * v2 - 6.f * v1) * r2inv);
-        }
-        const float fx = dx * fs, fy = dy * fs, fz = dz * fs;
-        fix -= fx; fiy -= fy; fiz -= fz;
-        gjx += fx; gjy += fy; gjz += fz;
-        if (COUNT && (!CMM || (me & 1u))) ++tn;
+      const bool in = ((mk >> k) & 1u) && r2 <= rc2;
+      const float rinv = rsqrtf(in ? r2 : 1.f);
+      const float r2inv = rinv * rinv;
+      const float r6inv = r2inv * r2inv * r2inv;
+      const float2 lj = s_lj[row + (ALSD ? (tjr & kTypeMask) : tjr)];
+      const bool el = CMM ? ((mek >> k) & 1u) != 0u : true;
+      const float qq = el ? pi.w * pj.w : 0.f;
+      const float v1 = lj.x * r6inv;
+      const float v2 = lj.y * r6inv * r6inv;
+      const float eel = qq * (rinv + fmaf(zb, r2, -zc));
+      const float elj = v2 - v1;
+      float fs = fmaf(qq, fmaf(rinv, r2inv, -zf), fmaf(12.f, v2, -6.f * v1) * r2inv);
+      if (ALSD) {
+        const int na = ci + (tjr >> 30);
+        const float e = in ? eel + elj : 0.f;
+        ea8 += na == 2 ? e : 0.f;
+        eb8 += na == 1 ? e : 0.f;
+        fs *= na == 2 ? f2 : (na == 1 ? f1 : 1.f);
       }
+      fs = in ? fs : 0.f;
+      te8 += in ? eel : 0.f;
+      tl8 += in ? elj : 0.f;
+      const float fx = dx * fs, fy = dy * fs, fz = dz * fs;
+      fix -= fx; fiy -= fy; fiz -= fz;
+      gjx += fx; gjy += fy; gjz += fz;
+      if (COUNT) tn += (in && el) ? 1 : 0;
+      gjx = __shfl_sync(full, gjx, src);
+      gjy = __shfl_sync(full, gjy, src);
+      gjz = __shfl_sync(full, gjz, src);
     }
-    m >>= 1;
-    if (CMM) me >>= 1;
-    const int src = (lane + 1) & 31;
-    gjx = __shfl_sync(0xffffffffu, gjx, src);
-    gjy = __shfl_sync(0xffffffffu, gjy, src);
-    gjz = __shfl_sync(0xffffffffu, gjz, src);
+    te += (double)te8;
+    tl += (double)tl8;
+    if (ALSD) {
+      ea += (double)ea8;
+      eb += (double)eb8;
+    }
   }
 }
 
 template <bool COUNT, bool ALSD, bool CMM>
-__global__ void __launch_bounds__(kPairThreads)
+__global__ void __launch_bounds__(kPairThreads, 2)
 k_pair_mixed(DevPtrs P, ZdConst z) {
   extern __shared__ float2 s_lj[];
-  __shared__ float4 s_jpos[kPairThreads];
-  __shared__ int s_jtyp[kPairThreads];
+  __shared__ MixStage s_stage[kPairWarps];
+  const unsigned full = 0xffffffffu;
   const int nlj = z.nt1 * z.nt1;
   for (int i = threadIdx.x; i < nlj; i += blockDim.x) s_lj[i] = P.lj_f[i];
-  __syncthreads();
   const int lane = threadIdx.x & 31;
-  float4* sj_pos = s_jpos + (threadIdx.x & ~31);
-  int* sj_typ = s_jtyp + (threadIdx.x & ~31);
-  const int T = *P.ntiles;
+  MixStage& S = s_stage[threadIdx.x >> 5];
+  if (lane == 0) {
+    mbar_init(&S.bar[0]);
+    mbar_init(&S.bar[1]);
+  }
+  __syncthreads();
+  const int T = *P.nctiles;
+  const long long wlim = P.wait_cycles;
   const float rc2 = (float)z.rc2, zb = (float)z.bcoeff, zf = (float)z.fcoeff, zc = (float)z.zcore;
+  const unsigned txb = CMM ? 768u : 640u;
+  unsigned phase = 0u, pend = 0u;   // per buffer: barrier parity to wait for; copy in flight
+  bool ok = true;
+
+  auto claim = [&]() {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(P.tile_ctr, 1);
+    return __shfl_sync(full, t, 0);
+  };
+  auto issue = [&](int t, int b) {
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect(&S.bar[b], txb);
+      bulk_load(S.ent[b], P.ct_j + (size_t)t * 32, 512u, &S.bar[b]);
+      bulk_load(S.msk[b], P.ct_mask + (size_t)t * 32, 128u, &S.bar[b]);
+      if (CMM) bulk_load(S.msk_el[b], P.ct_mask_el + (size_t)t * 32, 128u, &S.bar[b]);
+    }
+    pend |= 1u << b;
+  };
+  // tile t's copy has landed in buffer b: start the gathers of its atoms
+  auto fetch = [&](int t, int b, Gather& G) {
+    if (!mbar_wait(&S.bar[b], (phase >> b) & 1u, wlim)) {
+      ok = false;
+      atomicOr(P.status, ERR_TIMEOUT);
+      return;
+    }
+    phase ^= 1u << b;
+    pend &= ~(1u << b);
+    const float4 e = S.ent[b][lane];
+    G.m = S.msk[b][lane];
+    G.me = CMM ? S.msk_el[b][lane] : 0u;
+    const int sj = __float_as_int(e.w);
+    G.sx = e.x; G.sy = e.y; G.sz = e.z;
+    if (sj >= 0) {
+      G.pj = P.pos_f[sj];
+      G.tj = P.styp[sj];
+      G.aj = P.satom[sj];
+    } else {
+      G.pj = make_float4(0.f, 0.f, 0.f, 0.f);
+      G.tj = z.nt1 - 1;   // the zero dummy type
+      G.aj = -1;
+    }
+    G.bi = P.ct_blk[t];
+  };
+
   int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
   float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
   long long gix = 0, giy = 0, giz = 0;
-  long long eel = 0, elj = 0, eaa = 0, eab = 0;   // fixed point, per tile
+  long long eel = 0, elj = 0, eaa = 0, eab = 0;
   long long npair = 0;
   bool mi = true;
   float bx = 0.f, by = 0.f, bz = 0.f, ibx = 0.f, iby = 0.f, ibz = 0.f;
   float f1 = 1.f, f2 = 1.f;
-  // tiles are claimed kPairClaim at a time from a global counter (row order: consecutive
-  // tiles mostly share their i block), so warps finish together whatever their tiles hold
-  for (;;) {
-  int t0 = 0;
-  if (lane == 0) t0 = atomicAdd(P.tile_ctr, kPairClaim);
-  t0 = __shfl_sync(0xffffffffu, t0, 0);
-  if (t0 >= T) break;
-  const int t1 = min(T, t0 + kPairClaim);
-  for (int t = t0; t < t1; ++t) {
-    const int2 ij = P.tiles[t];
-    if (ij.x != cur_bi) {
+
+  int t = claim(), tn = T;
+  Gather G;
+  if (t < T) {
+    issue(t, 0);
+    tn = claim();
+    if (tn < T) issue(tn, 1);
+    fetch(t, 0, G);
+  }
+  int b = 0;
+  while (t < T && ok) {
+    // the tile's j atoms into the warp's stage, in the i block's frame
+    __syncwarp();
+    const float4 pj = make_float4(G.pj.x - G.sx, G.pj.y - G.sy, G.pj.z - G.sz, G.pj.w);
+    S.pos[lane] = pj;
+    S.pos[lane + 32] = pj;
+    S.typ[lane] = G.tj;
+    S.typ[lane + 32] = G.tj;
+    const unsigned m = G.m, me = G.me;
+    const int aj = G.aj, bi = G.bi;
+    if (bi != cur_bi) {
       if (ai >= 0 && (gix | giy | giz)) {
         atomic_add_ll(&P.frc[3 * ai + 0], gix);
         atomic_add_ll(&P.frc[3 * ai + 1], giy);
         atomic_add_ll(&P.frc[3 * ai + 2], giz);
       }
       gix = giy = giz = 0;
-      cur_bi = ij.x;
-      const int s = cur_bi * kTile + lane;
-      pi = P.pos_f[s];
-      ti = P.styp[s];
-      ai = P.satom[s];
-      const int rep = P.blk_rep[cur_bi];
+      cur_bi = bi;
+      const int si = bi * kTile + lane;
+      pi = P.pos_f[si];
+      ti = P.styp[si];
+      ai = P.satom[si];
+      const int rep = P.blk_rep[bi];
       if (rep != cur_rep) {
-        if (cur_rep >= 0) {
-          flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
-        }
+        if (cur_rep >= 0) flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
         eel = elj = eaa = eab = 0;
         npair = 0;
         cur_rep = rep;
@@ -190,41 +325,49 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
           if (0.5 * R.box[k] < z.rlim + 4.0 * (double)P.rep_hmax[3 * rep + k] + 2.0) mi = true;
       }
     }
-    const float4 sh = P.tile_shift[t];
-    const unsigned m = P.masks[(size_t)t * 32 + lane];
-    const unsigned me = CMM ? P.masks_el[(size_t)t * 32 + lane] : 0u;
-    const int sj = ij.y * kTile + lane;
     __syncwarp();
-    sj_pos[lane] = P.pos_f[sj];
-    sj_typ[lane] = P.styp[sj];
-    __syncwarp();
+    // buffer b is free again: the tile after next goes into it; the next tile's gathers
+    // are issued before this tile's arithmetic
+    int t2 = T;
+    if (tn < T) {
+      t2 = claim();
+      if (t2 < T) issue(t2, b);
+    }
+    Gather Gn;
+    if (tn < T) fetch(tn, b ^ 1, Gn);
     float gjx = 0.f, gjy = 0.f, gjz = 0.f;
     float fix = 0.f, fiy = 0.f, fiz = 0.f;
-    float te = 0.f, tl = 0.f, ea = 0.f, eb = 0.f;
-    int tn = 0;
+    double te = 0.0, tl = 0.0, ea = 0.0, eb = 0.0;
+    int tn_pairs = 0;
     const int ci = ALSD ? (ti >> 30) : 0;
+    const int row = (ALSD ? (ti & kTypeMask) : ti) * z.nt1;
     if (mi)
-      tile_mixed<true, COUNT, ALSD, CMM>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, me, lane, bx, by, bz, ibx,
-                                    iby, ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn,
-                                    ci, f1, f2, ea, eb);
+      tile_mixed<true, COUNT, ALSD, CMM>(S, s_lj, row, pi, m, me, lane, bx, by, bz, ibx, iby, ibz, rc2, zb,
+                                         zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci, f1, f2,
+                                         ea, eb);
     else
-      tile_mixed<false, COUNT, ALSD, CMM>(sj_pos, sj_typ, s_lj, z.nt1, pi, ti, sh, m, me, lane, bx, by, bz, ibx,
-                                     iby, ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl,
-                                     tn, ci, f1, f2, ea, eb);
-    const int aj = P.satom[sj];
+      tile_mixed<false, COUNT, ALSD, CMM>(S, s_lj, row, pi, m, me, lane, bx, by, bz, ibx, iby, ibz, rc2, zb,
+                                          zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci, f1,
+                                          f2, ea, eb);
     if (aj >= 0 && (gjx != 0.f || gjy != 0.f || gjz != 0.f)) {
-      atomic_add_ll(&P.frc[3 * aj + 0], to_fix((double)gjx, kFrcScale));
-      atomic_add_ll(&P.frc[3 * aj + 1], to_fix((double)gjy, kFrcScale));
-      atomic_add_ll(&P.frc[3 * aj + 2], to_fix((double)gjz, kFrcScale));
+      atomic_add_ll(&P.frc[3 * aj + 0], to_fix((double)gjx, kFrcScale, P.status));
+      atomic_add_ll(&P.frc[3 * aj + 1], to_fix((double)gjy, kFrcScale, P.status));
+      atomic_add_ll(&P.frc[3 * aj + 2], to_fix((double)gjz, kFrcScale, P.status));
     }
-    gix += to_fix((double)fix, kFrcScale);
-    giy += to_fix((double)fiy, kFrcScale);
-    giz += to_fix((double)fiz, kFrcScale);
-    eel += to_fix((double)te, kEneScale);
-    elj += to_fix((double)tl, kEneScale);
-    if (ALSD) { eaa += to_fix((double)ea, kEneScale); eab += to_fix((double)eb, kEneScale); }
-    if (COUNT) npair += tn;
-  }
+    gix += to_fix((double)fix, kFrcScale, P.status);
+    giy += to_fix((double)fiy, kFrcScale, P.status);
+    giz += to_fix((double)fiz, kFrcScale, P.status);
+    eel += to_fix(te, kEneScale, P.status);
+    elj += to_fix(tl, kEneScale, P.status);
+    if (ALSD) {
+      eaa += to_fix(ea, kEneScale, P.status);
+      eab += to_fix(eb, kEneScale, P.status);
+    }
+    if (COUNT) npair += tn_pairs;
+    t = tn;
+    tn = t2;
+    G = Gn;
+    b ^= 1;
   }
   if (ai >= 0 && (gix | giy | giz)) {
     atomic_add_ll(&P.frc[3 * ai + 0], gix);
@@ -232,17 +375,28 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     atomic_add_ll(&P.frc[3 * ai + 2], giz);
   }
   flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
+  // a copy still in flight (only after a timed-out wait) must land before the block exits
+  for (int k = 0; k < 2; ++k)
+    if ((pend >> k) & 1u) mbar_wait(&S.bar[k], (phase >> k) & 1u, wlim);
 }
+
+// Per-warp shared memory of the FP64 kernel: the tile's j atoms, twice (see MixStage).
+struct __align__(16) F64Stage {
+  double4 pos[64];
+  int typ[64];
+};
 
 template <bool COUNT, bool ALSD, bool CMM>
 __global__ void __launch_bounds__(kPairThreads)
 k_pair_fp64(DevPtrs P, ZdConst z) {
   extern __shared__ double2 s_ljd[];
+  __shared__ F64Stage s_stage[kPairWarps];
   const int nlj = z.nt1 * z.nt1;
   for (int i = threadIdx.x; i < nlj; i += blockDim.x) s_ljd[i] = P.lj_d[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int T = *P.ntiles;
+  F64Stage& S = s_stage[threadIdx.x >> 5];
+  const int T = *P.nctiles;
   const double irlim2 = 1.0 / z.rc2;
   int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
   double4 pi = make_double4(0, 0, 0, 0);
@@ -251,31 +405,27 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
   long long npair = 0;
   double bx = 0, by = 0, bz = 0, ibx = 0, iby = 0, ibz = 0;
   double f1 = 1.0, f2 = 1.0;
-  // tiles claimed one at a time, as in the mixed kernel
   for (;;) {
-  int t = 0;
-  if (lane == 0) t = atomicAdd(P.tile_ctr, 1);
-  t = __shfl_sync(0xffffffffu, t, 0);
-  if (t >= T) break;
-  {
-    const int2 ij = P.tiles[t];
-    if (ij.x != cur_bi) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(P.tile_ctr, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= T) break;
+    const int bi = P.ct_blk[t];
+    if (bi != cur_bi) {
       if (ai >= 0) {
         atomicAdd(&P.grd[3 * ai + 0], gix);
         atomicAdd(&P.grd[3 * ai + 1], giy);
         atomicAdd(&P.grd[3 * ai + 2], giz);
       }
       gix = giy = giz = 0;
-      cur_bi = ij.x;
+      cur_bi = bi;
       const int s = cur_bi * kTile + lane;
       pi = P.pos_d[s];
       ti = P.styp[s];
       ai = P.satom[s];
       const int rep = P.blk_rep[cur_bi];
       if (rep != cur_rep) {
-        if (cur_rep >= 0) {
-          flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
-        }
+        if (cur_rep >= 0) flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
         eel = elj = eaa = eab = 0;
         npair = 0;
         cur_rep = rep;
@@ -288,20 +438,30 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
         }
       }
     }
-    unsigned m = P.masks[(size_t)t * 32 + lane];
-    unsigned me = CMM ? P.masks_el[(size_t)t * 32 + lane] : 0u;
-    const int sj = ij.y * kTile + lane;
-    double4 pj = P.pos_d[sj];
-    int tj = P.styp[sj];
+    const unsigned m = P.ct_mask[(size_t)t * 32 + lane];
+    const unsigned me = CMM ? P.ct_mask_el[(size_t)t * 32 + lane] : 0u;
+    const int sj = __float_as_int(P.ct_j[(size_t)t * 32 + lane].w);
+    const double4 pj = sj >= 0 ? P.pos_d[sj] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const int tjv = sj >= 0 ? P.styp[sj] : z.nt1 - 1;
+    const int aj = sj >= 0 ? P.satom[sj] : -1;
+    __syncwarp();
+    S.pos[lane] = pj;
+    S.pos[lane + 32] = pj;
+    S.typ[lane] = tjv;
+    S.typ[lane + 32] = tjv;
+    __syncwarp();
     const int row = (ALSD ? (ti & kTypeMask) : ti) * z.nt1;
     const int ci = ALSD ? (ti >> 30) : 0;
     double gjx = 0, gjy = 0, gjz = 0;
     int tn = 0;
     double te = 0.0, tl = 0.0, ta = 0.0, tb = 0.0;   // this tile's energies
-#pragma unroll 2
+    const int src = (lane + 1) & 31;
+#pragma unroll 4
     for (int k = 0; k < 32; ++k) {
-      if (m & 1u) {
-        double dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      if ((m >> k) & 1u) {
+        const double4 q = S.pos[lane + k];
+        const int tj = S.typ[lane + k];
+        double dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
         dx -= bx * anint(dx * ibx);
         dy -= by * anint(dy * iby);
         dz -= bz * anint(dz * ibz);
@@ -310,7 +470,8 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
         if (dd2i - irlim2 >= 0.0) {
           const double ddi = sqrt(dd2i);
           const double dd6i = dd2i * dd2i * dd2i;
-          const double ee = CMM ? ((me & 1u) ? pi.w * pj.w : 0.0) : pi.w * pj.w;
+          const bool elp = CMM ? ((me >> k) & 1u) != 0u : true;
+          const double ee = elp ? pi.w * q.w : 0.0;
           const double epair = ee * (ddi + z.bcoeff * dd2 - z.zcore);
           te += epair;
           const double2 lj = s_ljd[row + (ALSD ? (tj & kTypeMask) : tj)];
@@ -326,32 +487,22 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
           const double fx = dx * cc, fy = dy * cc, fz = dz * cc;
           gix -= fx; giy -= fy; giz -= fz;
           gjx += fx; gjy += fy; gjz += fz;
-          if (COUNT && (!CMM || (me & 1u))) ++tn;
+          if (COUNT && elp) ++tn;
         }
       }
-      m >>= 1;
-      if (CMM) me >>= 1;
-      const int src = (lane + 1) & 31;
-      pj.x = __shfl_sync(0xffffffffu, pj.x, src);
-      pj.y = __shfl_sync(0xffffffffu, pj.y, src);
-      pj.z = __shfl_sync(0xffffffffu, pj.z, src);
-      pj.w = __shfl_sync(0xffffffffu, pj.w, src);
-      tj = __shfl_sync(0xffffffffu, tj, src);
       gjx = __shfl_sync(0xffffffffu, gjx, src);
       gjy = __shfl_sync(0xffffffffu, gjy, src);
       gjz = __shfl_sync(0xffffffffu, gjz, src);
     }
-    const int aj = P.satom[sj];
     if (aj >= 0 && (gjx != 0.0 || gjy != 0.0 || gjz != 0.0)) {
       atomicAdd(&P.grd[3 * aj + 0], gjx);
       atomicAdd(&P.grd[3 * aj + 1], gjy);
       atomicAdd(&P.grd[3 * aj + 2], gjz);
     }
     if (COUNT) npair += tn;
-    eel += to_fix(te, kEneScale);
-    elj += to_fix(tl, kEneScale);
-    if (ALSD) { eaa += to_fix(ta, kEneScale); eab += to_fix(tb, kEneScale); }
-  }
+    eel += to_fix(te, kEneScale, P.status);
+    elj += to_fix(tl, kEneScale, P.status);
+    if (ALSD) { eaa += to_fix(ta, kEneScale, P.status); eab += to_fix(tb, kEneScale, P.status); }
   }
   if (ai >= 0) {
     atomicAdd(&P.grd[3 * ai + 0], gix);
@@ -374,8 +525,7 @@ int pair_blocks_per_sm(bool fp64, int nt1) {
 
 void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool, bool count, bool alsd,
                        cudaStream_t st) {
-  const int wpb = kPairThreads / 32;
-  const int nb = (nwarps + wpb - 1) / wpb;
+  const int nb = (nwarps + kPairWarps - 1) / kPairWarps;
   const size_t sh = sizeof(float2) * z.nt1 * z.nt1;
   if (z.cmm) {
     if (count) k_pair_mixed<true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
@@ -391,8 +541,7 @@ void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool, boo
 
 void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, bool alsd,
                       cudaStream_t st) {
-  const int wpb = kPairThreads / 32;
-  const int nb = (nwarps + wpb - 1) / wpb;
+  const int nb = (nwarps + kPairWarps - 1) / kPairWarps;
   const size_t sh = sizeof(double2) * z.nt1 * z.nt1;
   if (z.cmm) {
     if (count) k_pair_fp64<true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);

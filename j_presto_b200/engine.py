@@ -24,7 +24,7 @@ EXPORTS = ["jp_default_params", "jp_create", "jp_rebuild_cells", "jp_energy_grad
            "jp_ge_hist_get", "jp_ge_set", "jp_lstsq_windows", "jp_ge_fit", "jp_ge_dlnn",
            "jp_mlp_nparam", "jp_mlp_init", "jp_mlp_train", "jp_mlp_forward", "jp_ge_set_mlp",
            "jp_get_lambda", "jp_set_lambda", "jp_set_grid_limit", "jp_default_min_params",
-           "jp_minimize"]
+           "jp_minimize", "jp_set_wait_limit", "jp_step_io"]
 
 
 class JpError(RuntimeError):
@@ -48,12 +48,14 @@ def lib():
         L.jp_rebuild_cells.argtypes = [vp, ip]
         L.jp_energy_grad.argtypes = [vp, ip, dp, dp, dp]
         L.jp_step.argtypes = [vp, ip, dp, dp]
+        L.jp_step_io.argtypes = [vp, ip, dp, dp, dp, dp, dp, dp]
         L.jp_shake.argtypes = [vp, ip, dp, dp]
         L.jp_get_state.argtypes = [vp, ip, dp, dp]
         L.jp_set_state.argtypes = [vp, ip, dp, dp]
         L.jp_pair_count.argtypes = [vp, ip, C.POINTER(C.c_int64)]
         L.jp_set_timing.argtypes = [vp, C.c_int]
         L.jp_set_grid_limit.argtypes = [vp, C.c_int32]
+        L.jp_set_wait_limit.argtypes = [vp, C.c_int64]
         L.jp_last_timing.argtypes = [vp, dp, dp, C.POINTER(C.c_int32)]
         L.jp_launch_counts.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.jp_list_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
@@ -299,6 +301,15 @@ class Engine:
         self.last_code = code
         return e, t
 
+    def step_io(self, x_in, v_in, x_out, v_out, ene=None, temp=None, nsteps=1, warn_ok=False):
+        """jp_step_io: all replicas' state in from host arrays [natom_total][3] (None = keep),
+        nsteps steps, state out (None = not wanted), one synchronisation.  ene [nsteps][nrep][15]
+        and temp [nsteps][nrep] are filled when given."""
+        code = lib().jp_step_io(self._h, int(nsteps), _dp(x_in), _dp(v_in), _dp(x_out), _dp(v_out),
+                                _dp(ene), _dp(temp))
+        self.last_code = _chk(code, "jp_step_io", warn_ok)
+        return code
+
     def minimize(self, warn_ok=False, **kw):
         """Steepest descent of every replica (jp_minimize); kw override the md_run defaults
         (max_loop, update, convgr, step0, up, down).  Returns per replica (iters, energies,
@@ -327,6 +338,10 @@ class Engine:
         """Cap the integration grid (0 = co-resident maximum); a smaller grid than the
         system's lanes selects the grid-stride form of the integrator."""
         _chk(lib().jp_set_grid_limit(self._h, int(blocks)), "jp_set_grid_limit")
+
+    def set_wait_limit(self, cycles):
+        """Bound of the integration kernel's grid-barrier waits in SM cycles (0 = default)."""
+        _chk(lib().jp_set_wait_limit(self._h, int(cycles)), "jp_set_wait_limit")
 
     def last_timing(self):
         tot = C.c_double()

@@ -1,0 +1,75 @@
+"""The accuracy bar of the mixed path on the full-size configurations, and NVE drift.
+
+One-step energies and gradients of both paths against the FP64 oracle on
+* C1: 3,000 waters in 31 A as specified (3x liquid density: the largest forces of the set),
+* C2: the 159-residue chain in 7,000 waters (22,860 atoms),
+* C3: 33,000 waters and 200 ions in 100 A (99,200 atoms).
+Tolerances: FP64 path -- gradient RMS relative 1e-12, energies 1e-8 relative; mixed path --
+gradient RMS relative 1e-5 (the metric's bar) and total potential energy 1e-6 relative.
+
+NVE drift: C1' (1,000 waters, liquid density), METHOD= MICR, SHAKE, 2 fs, 20 ps.  The total
+energy is md_run's bookkeeping (md.f90:578-628): potential energy at time t plus the kinetic
+energy of (v(t-dt/2) + v(t+dt/2))/2; the drift is the least-squares slope over the last 90 %
+of the run in kT per ns per degree of freedom.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from j_presto_b200 import abi, systems
+from tests._util import rms_rel
+
+pytestmark = pytest.mark.gpu
+
+FP64, MIXED = abi.JP_PREC_FP64, abi.JP_PREC_MIXED
+KB = 8.31451 / 4184.0            # kcal/mol/K (md_run gascst / 4184)
+DRIFT_MAX = 1e-4                 # kT/ns/DOF
+
+
+@pytest.fixture(scope="module")
+def eng_mod(engine_lib):
+    from j_presto_b200 import engine
+    return engine
+
+
+CONFIGS = {"c1": systems.config_c1, "c2": systems.config_c2, "c3": systems.config_c3}
+
+
+@pytest.mark.parametrize("name", sorted(CONFIGS))
+def test_full_size_energy_grad_vs_oracle(eng_mod, name):
+    top = CONFIGS[name]()
+    o = oracle.Oracle(top, method=abi.JP_METHOD_MICR)
+    eo, go = o.energy_grad()
+    res = {}
+    for prec in (FP64, MIXED):
+        with eng_mod.Engine(top, precision=prec, method=abi.JP_METHOD_MICR) as e:
+            ene, g = e.energy_grad()
+            assert e.pair_count() == o.npairs_cut
+            assert e.list_stats()[1] == o.npairs_listed
+        res[prec] = (ene, g)
+    ene, g = res[FP64]
+    assert rms_rel(g, go) < 1e-12
+    np.testing.assert_allclose(ene, eo, rtol=1e-8, atol=1e-6)
+    ene, g = res[MIXED]
+    assert rms_rel(g, go) < 1e-5
+    assert abs(ene[0] - eo[0]) < 1e-6 * abs(eo[0])
+
+
+def _drift(E, T, dof):
+    pe = E[:, 0, 0]
+    tot = pe + 0.5 * dof * KB * T[:, 0]
+    n = len(tot)
+    t_ns = np.arange(n) * 2.0e-6
+    skip = n // 10
+    slope = np.polyfit(t_ns[skip:], tot[skip:], 1)[0]
+    return slope / (KB * T[skip:, 0].mean() * dof)
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_nve_drift(eng_mod, prec):
+    top = systems.config_c1_prime()
+    dof = oracle.Oracle(top, method=abi.JP_METHOD_MICR).dof
+    with eng_mod.Engine(top, precision=prec, method=abi.JP_METHOD_MICR) as e:
+        E, T = e.step(10000)
+    drift = _drift(E, T, dof)
+    assert abs(drift) < DRIFT_MAX, drift

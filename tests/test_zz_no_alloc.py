@@ -63,12 +63,13 @@ def test_noalloc_matches_energy_grad(engine_lib):
     box = (C.c_double * 3)(*[float(b) for b in top["box"]])
     stream = torch.cuda.current_stream(dev).cuda_stream
 
-    def call(atype, excl_idx, base):
+    def call(atype, excl_idx, base, excl_ptr=None):
         grad.fill_(np.nan)
         ene.fill_(np.nan)
+        ep = eptr if excl_ptr is None else excl_ptr
         return engine_lib.jp_nonbond_noalloc(n, cord.data_ptr(), chg.data_ptr(), atype.data_ptr(),
                                              int(top["ntype"]), c6.data_ptr(), c12.data_ptr(),
-                                             eptr.data_ptr(), excl_idx.data_ptr(), base, box,
+                                             ep.data_ptr(), excl_idx.data_ptr(), base, box,
                                              rc_cut, eps, grad.data_ptr(), ene.data_ptr(), stream)
 
     def check():
@@ -89,6 +90,12 @@ def test_noalloc_matches_energy_grad(engine_lib):
     bad = typ.clone()
     bad[5] = int(top["ntype"])
     assert call(bad, eidx, 0) == abi.JP_E_INVALID
+    # so is a decreasing exclusion offset (every offset stays inside the partner list, so the
+    # check, not an out-of-range read, decides)
+    badp = eptr.clone()
+    assert int(badp[5]) >= 1
+    badp[6] = badp[5] - 1
+    assert call(typ, eidx, 0, badp) == abi.JP_E_INVALID
     # and the next call is unaffected
     assert call(typ, eidx, 0) == abi.JP_OK
     check()
