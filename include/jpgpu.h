@@ -288,7 +288,14 @@ typedef struct jp_params {
   int32_t cmm_levels;    /* CELLVL: cell levels of the CMM (raised to fit the system, <= 5) */
   double cmm_cell;       /* CELSIZ: edge of a level-1 CMM cell (Angstrom) */
   int32_t cmm_update;    /* CMMUPD: far-field interval (steps); UPDATE must be a multiple */
+  /* Block-shape tuning at jp_create (no md.inp keyword; the counterpart of md_run's
+   * SIMD_check autotuning of its vector length): 1 (default) = build each replica's list
+   * with JP_TUNE_CANDIDATES column grids and keep the one whose list has the fewest
+   * compact tiles (see jp_tile_shape); 0 = near-cubic 32-atom blocks for every replica. */
+  int32_t tune_blocks;
 } jp_params;
+
+#define JP_TUNE_CANDIDATES 5   /* column-edge factors 0.84, 0.92, 1, 1.09, 1.19 */
 
 enum { JP_ALSD_NONE = 0, JP_ALSD_LMD = 1, JP_ALSD_LMD2 = 2 };
 enum { JP_SCALE_BOND = 1, JP_SCALE_ANGLE = 2, JP_SCALE_TORS = 4, JP_SCALE_IMPR = 8 };
@@ -373,6 +380,12 @@ int jp_set_grid_limit(jp_ctx *ctx, int32_t blocks);
  * JP_E_TIMEOUT with the barrier, sums and accumulators cleared, so the context stays usable
  * after jp_set_state.  No counterpart in the reference (md_run has no device waits). */
 int jp_set_wait_limit(jp_ctx *ctx, int64_t cycles);
+
+/* The block shape jp_create chose for `replica`: the column-edge factor kept (1 = columns of
+ * edge (32/density)^(1/3)) and, per candidate, the compact tiles its list needed
+ * (tiles[JP_TUNE_CANDIDATES], -1 when tuning was off).  md_run's counterpart is the
+ * vector length SIMD_check.f90 picks and prints. */
+int jp_tile_shape(jp_ctx *ctx, int32_t replica, double *column_scale, int64_t *tiles);
 int jp_last_timing(jp_ctx *ctx, double *total_ms, double *phase_ms4, int32_t *launches4);
 
 /* Kernel launches per jp_step step (excluding list rebuilds) and per list rebuild. */

@@ -33,6 +33,7 @@ JP_E_STOP_MASS = -121
 JP_E_STOP_SINGULAR = -122
 JP_E_FREE_WINDOW = -130
 JP_NOALLOC_MAX_ATOMS = 16384
+JP_TUNE_CANDIDATES = 5           # column-edge factors tried by the block-shape tuner
 
 # energy slot names (md_run main.f90:157-159 cyenam order)
 ENERGY_NAMES = ["TOTAL", "BOND", "ANGLE", "TORSION", "IMPROPER", "VDW14", "ELEC14",
@@ -137,7 +138,7 @@ class JpParams(C.Structure):
         ("lambda_temp_control", C.c_int32), ("scale_terms", C.c_int32),
         ("taut", C.c_double), ("stop_center", C.c_int32), ("stop_natom", C.c_int32),
         ("cal15m", C.c_int32), ("bounda", C.c_int32), ("cmm_levels", C.c_int32),
-        ("cmm_cell", C.c_double), ("cmm_update", C.c_int32),
+        ("cmm_cell", C.c_double), ("cmm_update", C.c_int32), ("tune_blocks", C.c_int32),
     ]
 
 
@@ -149,7 +150,7 @@ def default_params(**kw):
                  icslop=3, fcstol=1e-3, psetmp=0.0, device=0, alsd=JP_ALSD_NONE, lambda0=1.0,
                  lambda_mass=0.0, lambda_temp_control=0, scale_terms=0, taut=40.0,
                  stop_center=JP_STOP_NONE, stop_natom=0, cal15m=JP_CAL15M_ZD,
-                 bounda=JP_BOUND_PBC, cmm_levels=3, cmm_cell=6.0, cmm_update=5)
+                 bounda=JP_BOUND_PBC, cmm_levels=3, cmm_cell=6.0, cmm_update=5, tune_blocks=1)
     for k, v in kw.items():
         if not hasattr(p, k):
             raise KeyError(k)

@@ -88,6 +88,11 @@ struct jp_ctx {
   Timing tm;
   int launches_step = 0, launches_rebuild = 0;
   bool rebuild_pending = false;     // the list rebuild due after the last step taken
+  // block-shape tuning: per replica and candidate the xy column grid, the compact tiles
+  // the list needed with it, and the candidate kept
+  std::vector<int> tune_grid;       // [nrep][JP_TUNE_CANDIDATES][2]
+  std::vector<long long> tune_tiles;  // [nrep][JP_TUNE_CANDIDATES]
+  std::vector<int> tune_pick;       // [nrep]
   Snap snap[3];                     // segment start, step start, a sub-step's accepted state
   bool snap_ready = false;
   int nstep_retry = 0;              // steps redone with a halved time step (all calls)
@@ -134,6 +139,17 @@ int dput(jp_ctx *c, T **p, const std::vector<T> &h) {
 }
 
 constexpr double kEekcal = 332.06378;
+// column-edge factors the block-shape tuner tries (1 = columns of edge (32/density)^(1/3),
+// near-cubic 32-atom blocks); kTuneDefault is the unit factor
+constexpr double kTuneScale[JP_TUNE_CANDIDATES] = {0.84, 0.92, 1.0, 1.09, 1.19};
+constexpr int kTuneDefault = 2;
+
+void set_grid(Rep &R, const int *g) {
+  for (int k = 0; k < 2; ++k) {
+    R.grid[k] = g[k];
+    R.cell[k] = R.box[k] / g[k];
+  }
+}
 // bound of a grid-barrier wait in the integration (SM cycles: about one second)
 constexpr long long kDefaultWaitCycles = 2000000000LL;
 constexpr int kGeCap = JP_GE_MAX_WINDOWS * (JP_GE_MAX_DEG + 3);   // doubles per replica
@@ -780,6 +796,48 @@ int minimize_conj(jp_ctx *c, int r, const jp_min_params *mp, int32_t *iters, dou
 
 int flush_rebuild(jp_ctx *c);   // below, beside the step loop
 
+// Block-shape tuning (the role of md_run's SIMD_check.f90:1-42 for its vector length): the
+// pair kernels' work is proportional to the compact tiles of the list, so each replica's
+// list is built with every candidate column grid and the grid needing the fewest compact
+// tiles is kept (ties to the unit factor, then to the smaller factor).  The count is exact
+// and deterministic, so the choice does not depend on timing noise, and a replica's choice
+// depends on its own atoms only (batched with others it chooses as it would alone).
+// Without tuning every replica keeps the unit factor.  Ends with the list built for the
+// chosen shapes.
+int tune_blocks(jp_ctx *c, bool tune) {
+  const int nq = JP_TUNE_CANDIDATES;
+  c->tune_tiles.assign((size_t)c->nrep * nq, -1);
+  c->tune_pick.assign(c->nrep, kTuneDefault);
+  std::vector<int> cnt(c->nblk);
+  for (int q = 0; q < (tune ? nq : 0); ++q) {
+    for (int r = 0; r < c->nrep; ++r) set_grid(c->reps[r], c->tune_grid.data() + ((size_t)r * nq + q) * 2);
+    CK(cudaMemcpy(c->P.reps, c->reps.data(), sizeof(Rep) * c->nrep, cudaMemcpyHostToDevice));
+    enqueue_rebuild(c);
+    CK(cudaMemcpyAsync(cnt.data(), c->P.ct_cnt, sizeof(int) * c->nblk, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    int rs = check_status(c);
+    if (rs < 0) return rs;
+    for (int r = 0; r < c->nrep; ++r) {
+      long long t = 0;
+      for (int b = c->reps[r].blk0; b < c->reps[r].blk0 + c->reps[r].nblk; ++b) t += cnt[b];
+      c->tune_tiles[(size_t)r * nq + q] = t;
+    }
+  }
+  for (int r = 0; r < c->nrep && tune; ++r) {
+    const long long *t = &c->tune_tiles[(size_t)r * nq];
+    int best = kTuneDefault;
+    for (int q = 0; q < nq; ++q)
+      if (t[q] < t[best]) best = q;
+    c->tune_pick[r] = best;
+  }
+  for (int r = 0; r < c->nrep; ++r)
+    set_grid(c->reps[r], c->tune_grid.data() + ((size_t)r * nq + c->tune_pick[r]) * 2);
+  CK(cudaMemcpy(c->P.reps, c->reps.data(), sizeof(Rep) * c->nrep, cudaMemcpyHostToDevice));
+  enqueue_rebuild(c);
+  CK(cudaStreamSynchronize(c->st));
+  return check_status(c);
+}
+
 }  // namespace
 
 extern "C" {
@@ -815,7 +873,8 @@ void jp_default_params(jp_params *p) {
   p->bounda = JP_BOUND_PBC;
   p->cmm_levels = 3;               // inpinp.f90:86 intele(16)
   p->cmm_cell = 6.0;               // inpinp.f90:86 reaele(17)
-  p->cmm_update = 5;               // inpmd.f90:151 intele(66)
+  p->cmm_update = 5;
+  p->tune_blocks = 1;               // inpmd.f90:151 intele(66)
 }
 
 const char *jp_strerror(int code) {
@@ -978,14 +1037,23 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       R.box[k] = box[k];
       R.invbox[k] = 1.0 / box[k];
     }
-    for (int k = 0; k < 2; ++k) {
-      R.grid[k] = std::max(1, std::min(512, (int)std::lround(box[k] / edge)));
-      R.cell[k] = box[k] / R.grid[k];
+    // the block-shape candidates: column edges scaled by kTuneScale; the columns, sort keys
+    // and blocks are laid out for the candidate with the most columns, so any of them can
+    // be taken later without reallocating
+    int ncol_cap = 0;
+    for (int q = 0; q < JP_TUNE_CANDIDATES; ++q) {
+      int g[2];
+      for (int k = 0; k < 2; ++k)
+        g[k] = std::max(1, std::min(512, (int)std::lround(box[k] / (edge * kTuneScale[q]))));
+      c->tune_grid.push_back(g[0]);
+      c->tune_grid.push_back(g[1]);
+      ncol_cap = std::max(ncol_cap, g[0] * g[1]);
     }
+    set_grid(R, c->tune_grid.data() + ((size_t)r * JP_TUNE_CANDIDATES + kTuneDefault) * 2);
     R.grid[2] = std::max(1, (int)std::ceil(box[2] / 0.25));
     R.cell[2] = box[2] / R.grid[2];
     R.col0 = col0;
-    R.ncol = R.grid[0] * R.grid[1];
+    R.ncol = ncol_cap;
     col0 += R.ncol;
     for (int q = 0; q < R.ncol; ++q) hcol_rep.push_back(r);
     R.key0 = key0;
@@ -1594,9 +1662,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
   CK(cudaEventCreate(&c->ev_a));
   CK(cudaEventCreate(&c->ev_b));
-  enqueue_rebuild(c);
-  CK(cudaStreamSynchronize(c->st));
-  int rs = check_status(c);
+  int rs = tune_blocks(c, prm->tune_blocks != 0);
   if (rs < 0) { jp_destroy(c); return rs; }
   *out = c;
   return JP_OK;
@@ -1923,6 +1989,14 @@ int jp_minimize(jp_ctx *c, const jp_min_params *mp, int32_t *iters, double *enev
   const int rs = check_status(c);
   if (rs != JP_OK) return rs;
   return step_err ? JP_E_MIN_STEP : JP_OK;
+}
+
+int jp_tile_shape(jp_ctx *c, int32_t r, double *column_scale, int64_t *tiles) {
+  if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
+  if (column_scale) *column_scale = kTuneScale[c->tune_pick[r]];
+  if (tiles)
+    for (int q = 0; q < JP_TUNE_CANDIDATES; ++q) tiles[q] = c->tune_tiles[(size_t)r * JP_TUNE_CANDIDATES + q];
+  return JP_OK;
 }
 
 int jp_set_wait_limit(jp_ctx *c, int64_t cycles) {

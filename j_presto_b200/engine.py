@@ -24,7 +24,7 @@ EXPORTS = ["jp_default_params", "jp_create", "jp_rebuild_cells", "jp_energy_grad
            "jp_ge_hist_get", "jp_ge_set", "jp_lstsq_windows", "jp_ge_fit", "jp_ge_dlnn",
            "jp_mlp_nparam", "jp_mlp_init", "jp_mlp_train", "jp_mlp_forward", "jp_ge_set_mlp",
            "jp_get_lambda", "jp_set_lambda", "jp_set_grid_limit", "jp_default_min_params",
-           "jp_minimize", "jp_set_wait_limit", "jp_step_io"]
+           "jp_minimize", "jp_set_wait_limit", "jp_step_io", "jp_tile_shape"]
 
 
 class JpError(RuntimeError):
@@ -56,6 +56,7 @@ def lib():
         L.jp_set_timing.argtypes = [vp, C.c_int]
         L.jp_set_grid_limit.argtypes = [vp, C.c_int32]
         L.jp_set_wait_limit.argtypes = [vp, C.c_int64]
+        L.jp_tile_shape.argtypes = [vp, ip, dp, C.POINTER(C.c_int64)]
         L.jp_last_timing.argtypes = [vp, dp, dp, C.POINTER(C.c_int32)]
         L.jp_launch_counts.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.jp_list_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
@@ -338,6 +339,13 @@ class Engine:
         """Cap the integration grid (0 = co-resident maximum); a smaller grid than the
         system's lanes selects the grid-stride form of the integrator."""
         _chk(lib().jp_set_grid_limit(self._h, int(blocks)), "jp_set_grid_limit")
+
+    def tile_shape(self, rep=0):
+        """(column-edge factor chosen for the replica, compact tiles per candidate)."""
+        f = C.c_double()
+        t = (C.c_int64 * abi.JP_TUNE_CANDIDATES)()
+        _chk(lib().jp_tile_shape(self._h, rep, C.byref(f), t), "jp_tile_shape")
+        return f.value, list(t)
 
     def set_wait_limit(self, cycles):
         """Bound of the integration kernel's grid-barrier waits in SM cycles (0 = default)."""
