@@ -316,6 +316,35 @@ def single_config(top, dev, steps, warmup, flush, with_e2e=False):
     return out
 
 
+def c5_measure(dev, steps, warmup, flush):
+    """C5: 32 ALSD replicas (12-residue chain in 3,000 waters, a 4-residue lambda cluster,
+    CLSTMETHOD= LMD with the McMD weight in lambda, torsions scaled) batched in one mixed
+    context against the same replicas one after another on the FP64 path."""
+    from j_presto_b200 import abi, engine, systems
+    reps = systems.config_c5(workers=os.cpu_count())
+    natoms = [int(t["natom"]) for t in reps]
+    kw = dict(method=abi.JP_METHOD_GE, alsd=abi.JP_ALSD_LMD, lambda0=0.8,
+              scale_terms=abi.JP_SCALE_TORS, device=dev)
+    with engine.Engine(reps, precision=abi.JP_PREC_MIXED, **kw) as e:
+        e.step(warmup, energies=False, temps=False)
+        t_mix = sum(timed_loop(e, steps, flush)) / 1e3
+    t64 = 0.0
+    for t in reps:
+        with engine.Engine(t, precision=abi.JP_PREC_FP64, **kw) as e:
+            e.step(warmup, energies=False, temps=False)
+            e.step(steps, energies=False, temps=False)
+            t64 += e.last_timing()[0] / 1e3
+    n = len(reps)
+    mix, v64 = ns_per_day(steps * n, t_mix), ns_per_day(steps * n, t64)
+    return {"workload": f"{n} ALSD replicas (CLSTMETHOD= LMD, METHOD= GE, weight in lambda on "
+                        f"[0.6, 1.0]): 12-residue chain in 3,000 waters, {min(natoms):,}-"
+                        f"{max(natoms):,} atoms, {sum(natoms):,} in total, 2 fs",
+            "atoms": sum(natoms), "replicas": n, "steps": steps,
+            "mixed_batched": {"value": mix, "unit": "ns/day (aggregate)", "ms_per_step": 1e3 * t_mix / steps},
+            "fp64_back_to_back": {"value": v64, "unit": "ns/day (aggregate)", "ms_per_step": 1e3 * t64 / steps},
+            "speedup_vs_fp64": mix / v64}
+
+
 def accuracy(dev, c2_acc, c3_acc):
     """Mixed against FP64 on every single-system configuration, and NVE drift (C1': 1,000
     waters at liquid density, METHOD= MICR, SHAKE, 2 fs, 20 ps) of both paths in kT per ns
@@ -335,19 +364,33 @@ def accuracy(dev, c2_acc, c3_acc):
                  "energy_err": float(abs(em[0] - e64[0]) / abs(e64[0]))}
     top = systems.config_c1_prime()
     dof = oracle.Oracle(top, method=abi.JP_METHOD_MICR).dof
-    nsteps = 10000
+    with engine.Engine(top, precision=abi.JP_PREC_FP64, method=abi.JP_METHOD_CANO, tempco=1,
+                       device=dev) as e:     # 10 ps at 300 K from the lattice start
+        e.step(5000, energies=False, temps=False)
+        x0, v0 = e.get_state()
+    nsteps = 250000
     drift = {}
     for name, prec in (("mixed", abi.JP_PREC_MIXED), ("fp64", abi.JP_PREC_FP64)):
         with engine.Engine(top, precision=prec, method=abi.JP_METHOD_MICR, device=dev) as e:
+            e.set_state(cord=x0, vel=v0)
+            e.rebuild()
             E, T = e.step(nsteps)
         tot = E[:, 0, 0] + 0.5 * dof * kb * T[:, 0]
         skip = nsteps // 10
         t_ns = np.arange(nsteps) * DT_FS * 1e-6
-        slope = np.polyfit(t_ns[skip:], tot[skip:], 1)[0]
-        drift[name] = float(slope / (kb * T[skip:, 0].mean() * dof))
+        # slope of 50 block means (blocks much longer than the correlation time) and its
+        # standard error from their scatter about the line
+        nb = 50
+        tb = t_ns[skip:].reshape(nb, -1).mean(1)
+        eb = tot[skip:].reshape(nb, -1).mean(1)
+        (slope, icpt), cov = np.polyfit(tb, eb, 1, cov=True)
+        unit = kb * T[skip:, 0].mean() * dof
+        drift[name] = float(slope / unit)
+        drift[name + "_stderr"] = float(np.sqrt(cov[0, 0]) / unit)
     acc["nve_drift_kT_per_ns_per_dof"] = {
-        "workload": f"C1': 1,000 waters (3,000 atoms) in a 31 A box, METHOD= MICR, SHAKE, 2 fs, "
-                    f"{nsteps} steps ({nsteps * DT_FS / 1000:.0f} ps), {dof} degrees of freedom",
+        "workload": f"C1': 1,000 waters (3,000 atoms) in a 31 A box, 10 ps METHOD= CANO at 300 K, "
+                    f"then METHOD= MICR, SHAKE, 2 fs, {nsteps} steps ({nsteps * DT_FS / 1000:.0f} ps), "
+                    f"{dof} degrees of freedom",
         **drift}
     return acc
 
@@ -384,6 +427,13 @@ def main():
     pairs = float(sum(eng.pair_count(r) for r in range(nrep)))
     ntiles, nlisted, _ = eng.list_stats()
     per_step, per_rebuild = eng.launch_counts()
+    shapes = [eng.tile_shape(r) for r in range(nrep)]
+    tshape = {"note": "block-shape tuner: per replica the column-edge factor with the fewest compact "
+                      "tiles of five (jp_tile_shape); counts of the 64 replicas summed per factor",
+              "chosen_factor_counts": {str(f): sum(1 for g, _ in shapes if g == f)
+                                       for f in sorted({g for g, _ in shapes})},
+              "tiles_per_factor": [int(sum(t[q] for _, t in shapes)) for q in range(5)],
+              "tiles_chosen": int(sum(min(t) for _, t in shapes))}
     # warm-up + timed (resident state, L2 flushed between steps)
     eng.step(args.warmup, energies=False, temps=False)
     barrier()
@@ -413,10 +463,11 @@ def main():
         barrier()
         return
     clocks = clk.summary()
-    c2 = c3 = acc = None
+    c2 = c3 = c5 = acc = None
     if not args.no_extra and world == 1:
         c2 = single_config(systems.config_c2(), dev, args.steps, args.warmup, flush, with_e2e=True)
         c3 = single_config(systems.config_c3(), dev, args.steps, args.warmup, flush)
+        c5 = c5_measure(dev, args.steps, args.warmup, flush)
         acc = accuracy(dev, {k: c2[k] for k in ("rms_force_err", "energy_err")},
                        {k: c3[k] for k in ("rms_force_err", "energy_err")})
     peak = engine.calibrate_fp32(dev)
@@ -462,6 +513,8 @@ def main():
         "accuracy": acc,
         "c2": c2,
         "c3": c3,
+        "c5": c5,
+        "tile_shape": tshape,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)

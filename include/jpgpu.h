@@ -411,6 +411,34 @@ int jp_ge_hist_setup(jp_ctx *ctx, int32_t replica, double emin, double emax, int
                      int32_t nbor);
 int jp_ge_hist_get(jp_ctx *ctx, int32_t replica, double *counts, int32_t clear);
 
+/* ALSD weight iteration (GEprep distrib_ALSD.f90:40-120, input_lambda_data :613-669).
+ * jp_alsd_hist_setup: from now on every MD step of `replica` (an ALSD replica) adds, at the
+ * bin of its lambda (nbin bins of (lmax - lmin) / nbin from lmin, plus nbor border bins each
+ * side; a lambda below the first bin's edge is not counted, as int(u + 1) >= 1 decides in
+ * the reference), one count and the lambda derivative of its cluster energy, 2 lambda E_AA +
+ * E_AB (LMD) or E_AA + E_AB / (2 sqrt(lambda)) (LMD2), E_AA and E_AB the class energies of
+ * the step; with ne > 0 also one count and that derivative at the (E, lambda) bin, E the
+ * total potential energy on ne bins of [emin, emax] (outside: not counted).  nbin + 2 nbor
+ * <= JP_ALSD_MAX_LBINS, ne <= JP_ALSD_MAX_EBINS; nbin = 0 switches it off.  A step redone
+ * after a SHAKE failure counts each of its accepted sub-steps.
+ * jp_alsd_hist_get: counts and derivative sums [nbin + 2 nbor], and (nullable) the (E, lambda)
+ * counts and sums [ne][nbin + 2 nbor]; clear != 0 zeroes them. */
+#define JP_ALSD_MAX_LBINS 64
+#define JP_ALSD_MAX_EBINS 256
+int jp_alsd_hist_setup(jp_ctx *ctx, int32_t replica, double lmin, double lmax, int32_t nbin,
+                       int32_t nbor, double emin, double emax, int32_t ne);
+int jp_alsd_hist_get(jp_ctx *ctx, int32_t replica, double *counts, double *dedl, double *counts2,
+                     double *dedl2, int32_t clear);
+
+/* The ALSD weight of `replica` from a network instead of its polynomial in lambda: the
+ * lambda force's weight term R T0 P(lambda) (verlethe.f90:289-320) takes P = net(x)[0] with
+ * x = ((E - emin) / (emax - emin), lambda), E the step's total potential energy, params
+ * jp_mlp_nparam(2, 2) floats (output 1, the network's d lnP/dE, is not applied: the
+ * reference's ALSD has no weight in E); outside [celw, ceup] in lambda the linear walls are
+ * added as before.  params NULL goes back to the polynomial.  METHOD= GE ALSD replicas only;
+ * the next jp_step re-captures its step graph.  No counterpart in the reference. */
+int jp_alsd_set_mlp(jp_ctx *ctx, int32_t replica, const float *params, double emin, double emax);
+
 /* Replace the McMD weight of `replica` (the .nf read by inmcmd.f90) for the following steps;
  * nwindow <= JP_GE_MAX_WINDOWS, ndeg <= JP_GE_MAX_DEG.  METHOD= GE contexts only. */
 int jp_ge_set(jp_ctx *ctx, int32_t replica, const jp_ge *ge);

@@ -34,6 +34,7 @@ JP_E_STOP_SINGULAR = -122
 JP_E_FREE_WINDOW = -130
 JP_NOALLOC_MAX_ATOMS = 16384
 JP_TUNE_CANDIDATES = 5           # column-edge factors tried by the block-shape tuner
+JP_ALSD_MAX_LBINS, JP_ALSD_MAX_EBINS = 64, 256
 
 # energy slot names (md_run main.f90:157-159 cyenam order)
 ENERGY_NAMES = ["TOTAL", "BOND", "ANGLE", "TORSION", "IMPROPER", "VDW14", "ELEC14",

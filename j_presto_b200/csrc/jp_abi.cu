@@ -66,6 +66,7 @@ struct jp_ctx {
   bool fp64 = false;
   bool minimg = true;
   int pair_warps = 0;
+  int nsm = 148;                    // the device's SM count
   bool alsd = false;
   bool cmm = false;                 // CAL15M= CMM
   bool hbond = false;               // some type pair has the 10-12 H-bond term
@@ -198,10 +199,11 @@ void enqueue_rebuild(jp_ctx *c) {
   const int nwb = (c->nchunk * 32 + 127) / 128;
   launch_tile_scan(P, c->nchunk, rlim * rlim, (float)rlim, rc * rc, c->cmm, st);
   scan_exclusive(P.chunk_cnt, P.chunk_off, c->nchunk + 1, c->scan_scratch, P.ntiles, st);
+  scan_exclusive(P.chunk_ent, P.chunk_eoff, c->nchunk + 1, c->scan_scratch, nullptr, st);
   k_tile_emit<<<nwb, 128, 0, st>>>(P, c->nchunk, c->cmm ? 1 : 0);
-  launch_compact_tiles(P, c->nblk, c->cmm, c->scan_scratch, st);
+  launch_compact_tiles(P, c->nblk, c->nsm, c->cmm, c->scan_scratch, st);
   if (c->hbond) launch_hb_list(P, c->hb_cap, c->zc.nt1, c->nblk, st);
-  c->launches_rebuild = 24 + (c->fp64 ? 1 : 0) + ncmm + (c->hbond ? 1 : 0);
+  c->launches_rebuild = 28 + (c->fp64 ? 1 : 0) + ncmm + (c->hbond ? 1 : 0);
 }
 
 // ---- one MD step ------------------------------------------------------------------------
@@ -1506,6 +1508,12 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.ct_cnt, (size_t)c->nblk + 1);
   e |= dalloc(c, &P.ct_off, (size_t)c->nblk + 1);
   e |= dalloc(c, &P.ct_blk, (size_t)c->tile_cap_total);
+  e |= dalloc(c, &P.ct_src, (size_t)c->tile_cap_total);
+  e |= dalloc(c, &P.tmp_occ, (size_t)c->nchunk * 32);
+  e |= dalloc(c, &P.chunk_ent, (size_t)c->nchunk + 1);
+  e |= dalloc(c, &P.chunk_eoff, (size_t)c->nchunk + 1);
+  e |= dalloc(c, &P.tile_occ, (size_t)c->tile_cap_total);
+  e |= dalloc(c, &P.tile_eoff, (size_t)c->tile_cap_total);
   e |= dalloc(c, &P.ct_j, (size_t)c->tile_cap_total * 32);
   e |= dalloc(c, &P.ct_mask, (size_t)c->tile_cap_total * 32);
   e |= dalloc(c, &P.nctiles, 1);
@@ -1570,6 +1578,13 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.scale, (size_t)nrep);
   e |= dalloc(c, &P.done, (size_t)nrep);
   e |= dalloc(c, &P.rep_fail, (size_t)nrep);
+  e |= dalloc(c, &P.lam_dew, (size_t)nrep);
+  if (prm->alsd != JP_ALSD_NONE) {
+    e |= dalloc(c, &P.alsd_cnt, (size_t)nrep * JP_ALSD_MAX_LBINS);
+    e |= dalloc(c, &P.alsd_f, (size_t)nrep * JP_ALSD_MAX_LBINS);
+    e |= dalloc(c, &P.alsd_cnt2, (size_t)nrep * JP_ALSD_MAX_EBINS * JP_ALSD_MAX_LBINS);
+    e |= dalloc(c, &P.alsd_f2, (size_t)nrep * JP_ALSD_MAX_EBINS * JP_ALSD_MAX_LBINS);
+  }
   e |= dalloc(c, &P.status, 1);
   e |= dalloc(c, &P.bar, 4);
   P.wait_cycles = kDefaultWaitCycles;
@@ -1653,6 +1668,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   c->alsd = ic.alsd != 0;
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  c->nsm = std::max(1, nsm);
   // one wave: every warp resident at once, each with an equal share of the tiles
   c->pair_warps = std::max(1, nsm) * (256 / 32) * pair_blocks_per_sm(c->fp64, c->zc.nt1);
   c->cano_grid = cano_grid(c->fp64, c->device);
@@ -1821,9 +1837,100 @@ int jp_ge_set(jp_ctx *c, int32_t r, const jp_ge *g) {
   return JP_OK;
 }
 
+int jp_alsd_hist_setup(jp_ctx *c, int32_t r, double lmin, double lmax, int32_t nbin, int32_t nbor,
+                       double emin, double emax, int32_t ne) {
+  if (!c || r < 0 || r >= c->nrep || nbin < 0 || nbor < 0 || ne < 0) return JP_E_INVALID;
+  if (!c->P.alsd_cnt || c->reps[r].lam_mode == JP_ALSD_NONE) return JP_E_INVALID;
+  if (nbin > 0 && (!(lmax > lmin) || nbin + 2 * nbor > JP_ALSD_MAX_LBINS)) return JP_E_INVALID;
+  if (ne > 0 && (!(emax > emin) || ne > JP_ALSD_MAX_EBINS)) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  if (int e = flush_rebuild(c)) return e;
+  CK(cudaStreamSynchronize(c->st));
+  Rep &R = c->reps[r];
+  const double dl = nbin > 0 ? (lmax - lmin) / nbin : 1.0;
+  R.alsd_nl = nbin > 0 ? nbin + 2 * nbor : 0;
+  R.alsd_lmin = lmin - dl * nbor;
+  R.alsd_linv = 1.0 / dl;
+  R.alsd_ne = nbin > 0 ? ne : 0;
+  R.alsd_emin = emin;
+  R.alsd_einv = ne > 0 ? ne / (emax - emin) : 0.0;
+  const size_t n1 = JP_ALSD_MAX_LBINS, n2 = (size_t)JP_ALSD_MAX_EBINS * JP_ALSD_MAX_LBINS;
+  CK(cudaMemset(c->P.alsd_cnt + r * n1, 0, sizeof(unsigned long long) * n1));
+  CK(cudaMemset(c->P.alsd_f + r * n1, 0, sizeof(double) * n1));
+  CK(cudaMemset(c->P.alsd_cnt2 + r * n2, 0, sizeof(unsigned long long) * n2));
+  CK(cudaMemset(c->P.alsd_f2 + r * n2, 0, sizeof(double) * n2));
+  CK(cudaMemcpy(c->P.reps + r, &R, sizeof(Rep), cudaMemcpyHostToDevice));
+  return JP_OK;
+}
+
+int jp_alsd_hist_get(jp_ctx *c, int32_t r, double *counts, double *dedl, double *counts2, double *dedl2,
+                     int32_t clear) {
+  if (!c || r < 0 || r >= c->nrep || !c->P.alsd_cnt) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  const Rep &R = c->reps[r];
+  const int nl = R.alsd_nl, ne = R.alsd_ne;
+  const size_t n1 = JP_ALSD_MAX_LBINS, n2 = (size_t)JP_ALSD_MAX_EBINS * JP_ALSD_MAX_LBINS;
+  std::vector<unsigned long long> h(n2);
+  std::vector<double> f(n2);
+  if (nl > 0) {
+    CK(cudaMemcpy(h.data(), c->P.alsd_cnt + r * n1, sizeof(unsigned long long) * nl, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(f.data(), c->P.alsd_f + r * n1, sizeof(double) * nl, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < nl; ++i) {
+      if (counts) counts[i] = (double)h[i];
+      if (dedl) dedl[i] = f[i];
+    }
+  }
+  if (ne > 0 && (counts2 || dedl2)) {
+    CK(cudaMemcpy(h.data(), c->P.alsd_cnt2 + r * n2, sizeof(unsigned long long) * n2, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(f.data(), c->P.alsd_f2 + r * n2, sizeof(double) * n2, cudaMemcpyDeviceToHost));
+    for (int a = 0; a < ne; ++a)
+      for (int i = 0; i < nl; ++i) {
+        if (counts2) counts2[(size_t)a * nl + i] = (double)h[(size_t)a * JP_ALSD_MAX_LBINS + i];
+        if (dedl2) dedl2[(size_t)a * nl + i] = f[(size_t)a * JP_ALSD_MAX_LBINS + i];
+      }
+  }
+  if (clear) {
+    CK(cudaMemset(c->P.alsd_cnt + r * n1, 0, sizeof(unsigned long long) * n1));
+    CK(cudaMemset(c->P.alsd_f + r * n1, 0, sizeof(double) * n1));
+    CK(cudaMemset(c->P.alsd_cnt2 + r * n2, 0, sizeof(unsigned long long) * n2));
+    CK(cudaMemset(c->P.alsd_f2 + r * n2, 0, sizeof(double) * n2));
+  }
+  return JP_OK;
+}
+
+// whether any replica's force-scaling step needs k_ge_scale (a network weight)
+void update_prescale(jp_ctx *c) {
+  int any = 0;
+  for (int q = 0; q < c->nrep; ++q) any |= c->reps[q].mlp_on != 0;
+  if (any != c->ic.ge_prescaled) {   // the step graph changes: capture it again
+    c->ic.ge_prescaled = any;
+    drop_graphs(c);
+  }
+}
+
+int jp_alsd_set_mlp(jp_ctx *c, int32_t r, const float *params, double emin, double emax) {
+  if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
+  if (c->prm.method != JP_METHOD_GE || c->reps[r].lam_mode == JP_ALSD_NONE) return JP_E_INVALID;
+  if (params && !(emax > emin)) return JP_E_INVALID;
+  const int np = jp_mlp_nparam(2, 2);
+  if (np < 0 || np > kMlpSlot) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  Rep &R = c->reps[r];
+  R.mlp_on = params ? 2 : 0;
+  R.mlp_e0 = emin;
+  R.mlp_e1 = emax;
+  if (params)
+    CK(cudaMemcpy(c->P.mlp + (size_t)r * kMlpSlot, params, sizeof(float) * np, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->P.reps + r, &R, sizeof(Rep), cudaMemcpyHostToDevice));
+  update_prescale(c);
+  return JP_OK;
+}
+
 int jp_ge_set_mlp(jp_ctx *c, int32_t r, const float *params) {
   if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
-  if (c->prm.method != JP_METHOD_GE) return JP_E_INVALID;
+  if (c->prm.method != JP_METHOD_GE || c->reps[r].lam_mode != JP_ALSD_NONE) return JP_E_INVALID;
   const int np = jp_mlp_nparam(1, 1);
   if (np < 0 || np > kMlpSlot) return JP_E_INVALID;
   CK(cudaSetDevice(c->device));
@@ -1833,12 +1940,7 @@ int jp_ge_set_mlp(jp_ctx *c, int32_t r, const float *params) {
   if (params) CK(cudaMemcpy(c->P.mlp + (size_t)r * kMlpSlot, params, sizeof(float) * np,
                             cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->P.reps + r, &R, sizeof(Rep), cudaMemcpyHostToDevice));
-  int any = 0;
-  for (int q = 0; q < c->nrep; ++q) any |= c->reps[q].mlp_on;
-  if (any != c->ic.ge_prescaled) {   // the step graph changes: capture it again
-    c->ic.ge_prescaled = any;
-    drop_graphs(c);
-  }
+  update_prescale(c);
   return JP_OK;
 }
 

@@ -324,6 +324,7 @@ __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk,
   }
   unsigned ball = __ballot_sync(0xffffffffu, cand);
   unsigned nz = 0;
+  int nent = 0;
   if (ball) {
     const int ai = P.satom[bi * kTile + lane];
     double xi = 0, yi = 0, zi = 0;
@@ -354,6 +355,10 @@ __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk,
       if (__any_sync(0xffffffffu, m != 0)) {
         P.tmp_masks[((size_t)w * 32 + b) * 32 + lane] = m;
         if (CMM) P.tmp_masks_el[((size_t)w * 32 + b) * 32 + lane] = mel;
+        // the j lanes some i atom lists: the compact-tile entries this tile contributes
+        const unsigned occ = __reduce_or_sync(0xffffffffu, __funnelshift_l(m, m, lane));
+        if (lane == 0) P.tmp_occ[(size_t)w * 32 + b] = occ;
+        nent += __popc(occ);
         nz |= 1u << b;
       }
     }
@@ -361,6 +366,7 @@ __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk,
   if (lane == 0) {
     P.chunk_nz[w] = nz;
     P.chunk_cnt[w] = __popc(nz);
+    P.chunk_ent[w] = nent;
   }
 }
 
@@ -381,6 +387,19 @@ __global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm) {
   const int bi = P.chunk_i[w], j0 = P.chunk_j0[w];
   const int t0 = P.chunk_off[w];
   const int cnt = __popc(nz);
+  {   // lane q: the chunk's q-th tile's occupied j lanes and its first entry (global order)
+    const int b = lane < cnt ? (int)__fns(nz, 0, lane + 1) : 0;
+    const unsigned occ = lane < cnt ? P.tmp_occ[(size_t)w * 32 + b] : 0u;
+    int e = __popc(occ);
+    for (int o = 1; o < 32; o <<= 1) {   // inclusive scan over the lanes
+      const int y = __shfl_up_sync(0xffffffffu, e, o);
+      if (lane >= o) e += y;
+    }
+    if (lane < cnt) {
+      P.tile_occ[t0 + lane] = occ;
+      P.tile_eoff[t0 + lane] = P.chunk_eoff[w] + e - __popc(occ);
+    }
+  }
   if (lane < cnt) {   // lane q: the chunk's q-th tile, its block pair and image shift
     const Rep& R = P.reps[P.blk_rep[bi]];
     const int bj = j0 + (int)__fns(nz, 0, lane + 1);
@@ -411,91 +430,100 @@ __global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm) {
 // Each entry carries its tile's image shift (into the i block's frame) and its slot; the
 // mask keeps the kernels' rotated layout (bit k of lane i: entry (i + k) & 31).
 
-// tiles of i-block bi: [chunk_off[blk_chunk0[bi]], chunk_off[blk_chunk0[bi + 1]])
-__device__ __forceinline__ void blk_tiles(const DevPtrs& P, int bi, int& t0, int& t1) {
-  t0 = P.chunk_off[P.blk_chunk0[bi]];
-  t1 = P.chunk_off[P.blk_chunk0[bi + 1]];
-}
+// tiles of i-block bi: [chunk_off[blk_chunk0[bi]], chunk_off[blk_chunk0[bi + 1]]); its
+// entries: [chunk_eoff[blk_chunk0[bi]], chunk_eoff[blk_chunk0[bi + 1]]) in global order
+// (the tile scan counts each tile's occupied j lanes, the tile emit places each tile's
+// entries)
 
-// pass 1: compact tiles per i-block (one warp per i-block)
+// per i-block (one thread each): compact tiles it needs
 __global__ void k_ct_count(DevPtrs P, int nblk) {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (w >= nblk) return;
-  int t0, t1;
-  blk_tiles(P, w, t0, t1);
-  int cnt = 0;
-  for (int t = t0; t < t1; ++t) {
-    const unsigned m = P.masks[(size_t)t * 32 + lane];
-    const unsigned row = __funnelshift_l(m, m, lane);   // bit c: pair (lane, j lane c)
-    cnt += __popc(__reduce_or_sync(0xffffffffu, row));
-  }
-  if (lane == 0) P.ct_cnt[w] = (cnt + 31) >> 5;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nblk) return;
+  const int ne = P.chunk_eoff[P.blk_chunk0[b + 1]] - P.chunk_eoff[P.blk_chunk0[b]];
+  P.ct_cnt[b] = (ne + 31) >> 5;
 }
 
-// pass 2 (after the scan of ct_cnt): one warp per i-block writes its compact tiles.  Lane i
-// builds row i of the current compact tile: the bits of row i of each tile at the tile's
-// occupied j lanes, packed in order; lane c of the tile writes its own entry.
-__global__ void k_ct_emit(DevPtrs P, int nblk, int cmm) {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (w >= nblk) return;
-  int t0, t1;
-  blk_tiles(P, w, t0, t1);
-  int out = P.ct_off[w], pos = 0;
-  unsigned cur = 0, cur_el = 0;
-  for (int t = t0; t < t1; ++t) {
-    const unsigned m = P.masks[(size_t)t * 32 + lane];
-    const unsigned row = __funnelshift_l(m, m, lane);
-    unsigned row_el = 0;
-    if (cmm) {
-      const unsigned me = P.masks_el[(size_t)t * 32 + lane];
-      row_el = __funnelshift_l(me, me, lane);
-    }
-    const unsigned cm = __reduce_or_sync(0xffffffffu, row);
-    if (cm == 0u) continue;
-    const int n = __popc(cm);
-    if ((cm >> lane) & 1u) {
-      const int p = pos + __popc(cm & ((1u << lane) - 1u));
-      const float4 sh = P.tile_shift[t];
-      const int slot = P.tiles[t].y * kTile + lane;
-      P.ct_j[(size_t)(out + (p >> 5)) * 32 + (p & 31)] = make_float4(sh.x, sh.y, sh.z, __int_as_float(slot));
-    }
-    unsigned comp = 0, comp_el = 0;   // row's bits at the occupied lanes, packed
-    int q = 0;
-    for (unsigned b = cm; b; b &= b - 1u, ++q) {
-      const int c = __ffs(b) - 1;
-      comp |= ((row >> c) & 1u) << q;
-      comp_el |= ((row_el >> c) & 1u) << q;
-    }
-    cur |= comp << pos;
-    cur_el |= comp_el << pos;
-    if (pos + n >= 32) {
-      P.ct_mask[(size_t)out * 32 + lane] = __funnelshift_r(cur, cur, lane);
-      if (cmm) P.ct_mask_el[(size_t)out * 32 + lane] = __funnelshift_r(cur_el, cur_el, lane);
-      if (lane == 0) P.ct_blk[out] = w;
-      ++out;
-      const int used = 32 - pos;
-      cur = used < 32 ? comp >> used : 0u;
-      cur_el = used < 32 ? comp_el >> used : 0u;
-      pos += n - 32;
-    } else {
-      pos += n;
-    }
-  }
-  if (pos > 0) {   // the last, partly filled compact tile: empty entries (slot -1) after pos
-    if (lane >= pos) P.ct_j[(size_t)out * 32 + lane] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-    P.ct_mask[(size_t)out * 32 + lane] = __funnelshift_r(cur, cur, lane);
-    if (cmm) P.ct_mask_el[(size_t)out * 32 + lane] = __funnelshift_r(cur_el, cur_el, lane);
-    if (lane == 0) P.ct_blk[out] = w;
+// per i-block (one thread each, after the scan of ct_cnt): each compact tile's i-block and
+// the first tile whose entries reach into it (a walk over the block's tiles, in order)
+__global__ void k_ct_index(DevPtrs P, int nblk) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nblk) return;
+  const int c0 = P.blk_chunk0[b];
+  const int e0 = P.chunk_eoff[c0];
+  int t = P.chunk_off[c0];
+  const int t1 = P.chunk_off[P.blk_chunk0[b + 1]];
+  const int n = P.ct_cnt[b], o = P.ct_off[b];
+  for (int k = 0; k < n; ++k) {
+    const int s0 = e0 + 32 * k;   // the compact tile's first entry
+    while (t + 1 < t1 && P.tile_eoff[t + 1] <= s0) ++t;
+    P.ct_blk[o + k] = b;
+    P.ct_src[o + k] = t;
   }
 }
 
-void launch_compact_tiles(const DevPtrs& P, int nblk, bool cmm, int* scan_scratch, cudaStream_t st) {
-  const int nb = (nblk * 32 + 127) / 128;
+// One warp per compact tile: lane i's row collects, from each tile whose entries fall in
+// the compact tile's 32 slots, the bits of that tile's row i at its occupied j lanes
+// (packed in lane order); lane p writes slot p's entry.
+__global__ void k_ct_emit(DevPtrs P, int cmm) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int T = *P.nctiles;
+  for (int ct = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ct < T; ct += nw) {
+    const int b = P.ct_blk[ct];
+    const int c0 = P.blk_chunk0[b];
+    const int e0 = P.chunk_eoff[c0], e1 = P.chunk_eoff[P.blk_chunk0[b + 1]];
+    const int t1 = P.chunk_off[P.blk_chunk0[b + 1]];
+    const int s0 = e0 + 32 * (ct - P.ct_off[b]);
+    unsigned cur = 0u, cur_el = 0u;
+    float4 ent = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    for (int t = P.ct_src[ct]; t < t1; ++t) {
+      const int base = P.tile_eoff[t] - s0;   // slot of the tile's first entry (may be < 0)
+      if (base >= 32) break;
+      const unsigned occ = P.tile_occ[t];
+      const int n = __popc(occ);
+      if (base + n <= 0) continue;
+      const unsigned m = P.masks[(size_t)t * 32 + lane];
+      const unsigned row = __funnelshift_l(m, m, lane);
+      unsigned row_el = 0u;
+      if (cmm) {
+        const unsigned me = P.masks_el[(size_t)t * 32 + lane];
+        row_el = __funnelshift_l(me, me, lane);
+      }
+      unsigned comp = 0u, comp_el = 0u;   // the row's bits at the occupied lanes, packed
+      int q = 0;
+      for (unsigned bb = occ; bb; bb &= bb - 1u, ++q) {
+        const int c = __ffs(bb) - 1;
+        comp |= ((row >> c) & 1u) << q;
+        comp_el |= ((row_el >> c) & 1u) << q;
+      }
+      if (base >= 0) {
+        cur |= comp << base;
+        cur_el |= comp_el << base;
+      } else {
+        cur |= comp >> -base;
+        cur_el |= comp_el >> -base;
+      }
+      const int k = lane - base;   // this lane's slot, as the tile's k-th entry
+      if (k >= 0 && k < n) {
+        const float4 sh = P.tile_shift[t];
+        const int slot = P.tiles[t].y * kTile + (int)__fns(occ, 0, k + 1);
+        ent = make_float4(sh.x, sh.y, sh.z, __int_as_float(slot));
+      }
+    }
+    if (s0 + lane >= e1) ent = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    P.ct_j[(size_t)ct * 32 + lane] = ent;
+    P.ct_mask[(size_t)ct * 32 + lane] = __funnelshift_r(cur, cur, lane);
+    if (cmm) P.ct_mask_el[(size_t)ct * 32 + lane] = __funnelshift_r(cur_el, cur_el, lane);
+  }
+}
+
+void launch_compact_tiles(const DevPtrs& P, int nblk, int nsm, bool cmm, int* scan_scratch,
+                          cudaStream_t st) {
+  const int nb = (nblk + 127) / 128;
   k_ct_count<<<nb, 128, 0, st>>>(P, nblk);
   scan_exclusive(P.ct_cnt, P.ct_off, nblk + 1, scan_scratch, P.nctiles, st);
-  k_ct_emit<<<nb, 128, 0, st>>>(P, nblk, cmm ? 1 : 0);
+  k_ct_index<<<nb, 128, 0, st>>>(P, nblk);
+  k_ct_emit<<<nsm * 8, 256, 0, st>>>(P, cmm ? 1 : 0);
 }
 
 // ---- deterministic exclusive scan (3 passes) --------------------------------------------

@@ -61,7 +61,13 @@ struct Rep {
   double ge_lower, ge_upper;      // ALSD linear walls below celw / above ceup
   int hist_off, hist_n;           // energy histogram slot and bin count (0 = off)
   double hist_min, hist_inv;      // lower edge of bin 0 and 1 / bin width
-  int mlp_on;                     // McMD weight from the surrogate network instead of the polynomial
+  int mlp_on;                     // 1: McMD weight from the surrogate network instead of the
+                                  // polynomial; 2: ALSD weight in lambda from the (E, lambda) network
+  double mlp_e0, mlp_e1;          // energy range the (E, lambda) network's first input spans
+  // ALSD weight iteration: lambda bins (0 = off) and (E, lambda) energy bins of the replica's
+  // histograms, lower edges and inverse widths
+  int alsd_nl, alsd_ne;
+  double alsd_lmin, alsd_linv, alsd_emin, alsd_einv;
   // ALSD (cluster classes AA / AB / BB scaled by powers of lambda)
   int lam_mode;                   // JP_ALSD_*; 0 = off
   int lam_ke_sub;                 // sub-system whose temperature holds lambda's kinetic term, -1 none
@@ -169,6 +175,11 @@ struct DevPtrs {
   int *blk_chunk0;                // [nblk+1] first chunk of each i-block (static)
   int *ct_cnt, *ct_off;           // compact tiles per i-block and their scan [nblk+1]
   int *ct_blk;                    // [CT] i-block
+  int *ct_src;                    // [CT] first tile whose entries reach into the compact tile
+  unsigned *tmp_occ;              // [nchunk*32] occupied j lanes of each chunk candidate
+  int *chunk_ent, *chunk_eoff;    // entries per chunk and their exclusive scan [nchunk+1]
+  unsigned *tile_occ;             // [T] occupied j lanes of each tile
+  int *tile_eoff;                 // [T] first entry of each tile (global order)
   float4 *ct_j;                   // [CT][32] (image shift into the i frame, slot bits; -1 = empty)
   unsigned *ct_mask, *ct_mask_el; // [CT][32] rotated masks (listed pairs; CMM Coulomb pairs)
   int *nctiles;                   // device scalar
@@ -212,6 +223,12 @@ struct DevPtrs {
   double *scale;                  // per replica force scale (GE / pseudo-T)
   int *done;                      // per replica SHAKE-thermostat loop finished
   int *rep_fail;                  // per replica: a SHAKE group failed this step (1)
+  // ALSD weight iteration, per replica: counts and sums of dE/dlambda of the cluster energy
+  // per lambda bin [nrep][JP_ALSD_MAX_LBINS], and per (E, lambda) bin
+  // [nrep][JP_ALSD_MAX_EBINS][JP_ALSD_MAX_LBINS]; allocated only with ALSD replicas
+  unsigned long long *alsd_cnt, *alsd_cnt2;
+  double *alsd_f, *alsd_f2;
+  double *lam_dew;                // [nrep] the lambda weight term of the step from the network
   unsigned *status;               // error bits
   unsigned *bar;                  // grid barrier of the cooperative integrator [4]
   long long *pair_cnt;            // [nrep]

@@ -407,6 +407,13 @@ __device__ double alsd_dew(const DevPtrs& P, const Rep& R, double lam) {
   return (kGas / kJouCal) * 1.0e-3 * R.ge_tempce * dprobl;
 }
 
+// the lambda weight term from the network's d lnP/dlambda (k_ge_scale), walls added
+__device__ __forceinline__ double alsd_walls(const Rep& R, double lam, double dprobl) {
+  if (lam < R.ge_celw) dprobl += R.ge_lower * (R.ge_celw - lam);
+  else if (lam > R.ge_ceup) dprobl += R.ge_upper * (lam - R.ge_ceup);
+  return (kGas / kJouCal) * 1.0e-3 * R.ge_tempce * dprobl;
+}
+
 // lambda of one replica through one step, carried by one thread
 struct LamStep {
   double lam, lv, lvback, lf, lvt;
@@ -429,7 +436,7 @@ __device__ void lam_begin(const DevPtrs& P, const IntConst& c, int r, LamStep& L
   if (c.method == JP_METHOD_GE) {
     const double eaa = (double)__ldcg(&P.ene_cls[4 * r]) * kEneInv + R.dself_cls[0];
     const double eab = (double)__ldcg(&P.ene_cls[4 * r + 1]) * kEneInv + R.dself_cls[1];
-    const double dew = alsd_dew(P, R, L.lam);
+    const double dew = R.mlp_on == 2 ? alsd_walls(R, L.lam, __ldcg(&P.lam_dew[r])) : alsd_dew(P, R, L.lam);
     L.lf = R.lam_mode == JP_ALSD_LMD ? -2.0 * eaa * L.lam - eab - dew
                                      : -eaa - 0.5 * eab / sqrt(L.lam) - dew;
   }
@@ -465,6 +472,19 @@ __global__ void __launch_bounds__(32) k_ge_scale(DevPtrs P, IntConst c) {
   const int r = blockIdx.x;
   const Rep& R = P.reps[r];
   double s;
+  if (c.method == JP_METHOD_GE && R.mlp_on == 2) {
+    // ALSD: d lnP/dlambda of the (E, lambda) network for the lambda force; atoms unscaled
+    double tot = R.dself;
+    for (int k = 1; k < JP_MAXENE; ++k) tot += (double)__ldcg(&P.ene_fix[r * 16 + k]) * kEneInv;
+    const float x[2] = {(float)((tot - R.mlp_e0) / (R.mlp_e1 - R.mlp_e0)), (float)P.lam[2 * r]};
+    float y[2];
+    mlp_forward_warp(P.mlp + (size_t)r * kMlpSlot, 2, 2, x, y);
+    if (threadIdx.x == 0) {
+      P.lam_dew[r] = (double)y[0];
+      P.scale[r] = 1.0;
+    }
+    return;
+  }
   if (c.method == JP_METHOD_GE && R.ge_nwin > 0 && R.mlp_on) {
     double tot = R.dself;
     for (int k = 1; k < JP_MAXENE; ++k) tot += (double)__ldcg(&P.ene_fix[r * 16 + k]) * kEneInv;
@@ -507,6 +527,27 @@ __device__ void write_ene_hist(const DevPtrs& P, const IntConst& c, int r) {
   }
   double* out = P.ene_hist + ((size_t)P.step_ctr[1] * c.nrep + r) * JP_MAXENE;
   for (int k = 0; k < JP_MAXENE; ++k) out[k] = e[k];
+  if (R.alsd_nl > 0) {   // distrib_ALSD input_lambda_data: jj = int((lambda - minEc)/bin + 1)
+    const double lam = P.lam[2 * r];
+    const double u = (lam - R.alsd_lmin) * R.alsd_linv;
+    if (u >= 0.0 && u < (double)R.alsd_nl) {
+      const double eaa = (double)__ldcg(&P.ene_cls[4 * r]) * kEneInv + R.dself_cls[0];
+      const double eab = (double)__ldcg(&P.ene_cls[4 * r + 1]) * kEneInv + R.dself_cls[1];
+      const double dedl = R.lam_mode == JP_ALSD_LMD ? 2.0 * eaa * lam + eab : eaa + 0.5 * eab / sqrt(lam);
+      const int k = (int)u;
+      const size_t o = (size_t)r * JP_ALSD_MAX_LBINS + k;
+      P.alsd_cnt[o] += 1ull;   // one thread per replica: a plain sum is deterministic
+      P.alsd_f[o] += dedl;
+      if (R.alsd_ne > 0) {
+        const double v = (tot - R.alsd_emin) * R.alsd_einv;
+        if (v >= 0.0 && v < (double)R.alsd_ne) {
+          const size_t o2 = ((size_t)r * JP_ALSD_MAX_EBINS + (int)v) * JP_ALSD_MAX_LBINS + k;
+          P.alsd_cnt2[o2] += 1ull;
+          P.alsd_f2[o2] += dedl;
+        }
+      }
+    }
+  }
 }
 
 // Grid barrier for a cooperative launch (all blocks co-resident).  bar[0] counts arrivals

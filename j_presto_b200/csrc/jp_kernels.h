@@ -20,7 +20,8 @@ void launch_tile_scan(const DevPtrs& P, int nchunk, double rlim2, float rlimf, d
                       cudaStream_t st);
 __global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm);
 // compact tiles of every i-block from the tile list (count, scan, emit)
-void launch_compact_tiles(const DevPtrs& P, int nblk, bool cmm, int* scan_scratch, cudaStream_t st);
+void launch_compact_tiles(const DevPtrs& P, int nblk, int nsm, bool cmm, int* scan_scratch,
+                          cudaStream_t st);
 void scan_exclusive(const int* in, int* out, int n, int* scratch, int* total, cudaStream_t st);
 
 // ZD pair constants
@@ -101,6 +102,6 @@ void launch_integrate(const DevPtrs& P, const IntConst& c, int nunit, bool fp64,
 void launch_shake_only(const DevPtrs& P, const IntConst& c, int unit0, int nunit, cudaStream_t st);
 // per-replica force scale of this step (McMD polynomial or surrogate network) into P.scale
 void launch_ge_scale(const DevPtrs& P, const IntConst& c, cudaStream_t st);
-constexpr int kMlpSlot = 4400;   // floats per replica >= jp_mlp_nparam(1, 1)
+constexpr int kMlpSlot = 4608;   // floats per replica >= jp_mlp_nparam(2, 2)
 
 }  // namespace jp

@@ -116,10 +116,109 @@ struct __align__(16) MixStage {
   float4 ent[2][32];
   unsigned msk[2][32];
   unsigned msk_el[2][32];
-  float4 pos[64];
-  int typ[64];
+  union {
+    struct {              // one entry per step (ALSD and CMM variants)
+      float4 pos[64];
+      int typ[64];
+    };
+    struct {              // two entries per step, e and e + 16, as packed pairs
+      float4 p2[64];      // x_e, x_e+16, y_e, y_e+16
+      float4 q2[64];      // z_e, z_e+16, q_e, q_e+16
+      int2 t2[64];        // their LJ types
+    };
+  };
   unsigned long long bar[2];
 };
+
+// rsqrt.approx without the IEEE-mode denormal fix-up: its argument is a squared distance of
+// a listed pair (far above the FP32 denormal range) or a masked slot's 1
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// One compact tile, two pairs per step in packed FP32x2 arithmetic (Blackwell's FFMA2 /
+// FADD2 / FMUL2): at step k (k < 16) lane l meets entries a = l + k and b = l + k + 16.  A
+// slot outside the mask or the cut-off takes rsqrt(1) and has its charge product and
+// r^-6 multiplied by 0, so it contributes an exact zero without a branch.  The j-force
+// accumulators of a and b rotate one lane per step; after 16 steps the b accumulator of
+// lane l belongs to entry l and the a accumulator to entry l + 16.  Same formula and
+// tolerances as the one-pair form; energies in FP32 over 4 steps, then FP64.
+template <bool MINIMG, bool COUNT>
+__device__ __forceinline__ void tile_mixed2(const MixStage& S, const float2* __restrict__ s_lj, int row,
+                                            float4 pi, unsigned m, int lane, float bx, float by, float bz,
+                                            float ibx, float iby, float ibz, float rc2, float zb, float zf,
+                                            float zc, float& fix, float& fiy, float& fiz, float& gjx,
+                                            float& gjy, float& gjz, double& te, double& tl, int& tn) {
+  const unsigned full = 0xffffffffu;
+  const int src = (lane + 1) & 31;
+  const float2 m1 = make_float2(-1.f, -1.f);
+  const float2 px = make_float2(pi.x, pi.x), py = make_float2(pi.y, pi.y), pz = make_float2(pi.z, pi.z);
+  const float2 pw = make_float2(pi.w, pi.w);
+  const float2 zb2 = make_float2(zb, zb), mzc = make_float2(-zc, -zc), mzf = make_float2(-zf, -zf);
+  const float2 c12 = make_float2(12.f, 12.f), cm6 = make_float2(-6.f, -6.f);
+  float2 fx = make_float2(0.f, 0.f), fy = fx, fz = fx;   // i force, a and b halves (sign: -sum)
+  float2 gx = fx, gy = fx, gz = fx;                      // j forces of the a and b entries
+#pragma unroll 1
+  for (int k0 = 0; k0 < 16; k0 += 4) {
+    const float4* __restrict__ sp = S.p2 + lane + k0;
+    const float4* __restrict__ sq = S.q2 + lane + k0;
+    const int2* __restrict__ st = S.t2 + lane + k0;
+    const unsigned ma = m >> k0, mb = m >> (k0 + 16);
+    float2 te4 = make_float2(0.f, 0.f), tl4 = te4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float4 a = sp[k];
+      const float4 b = sq[k];
+      const int2 t = st[k];
+      float2 dx = __ffma2_rn(make_float2(a.x, a.y), m1, px);
+      float2 dy = __ffma2_rn(make_float2(a.z, a.w), m1, py);
+      float2 dz = __ffma2_rn(make_float2(b.x, b.y), m1, pz);
+      if (MINIMG) {
+        dx.x -= bx * rintf(dx.x * ibx); dx.y -= bx * rintf(dx.y * ibx);
+        dy.x -= by * rintf(dy.x * iby); dy.y -= by * rintf(dy.y * iby);
+        dz.x -= bz * rintf(dz.x * ibz); dz.y -= bz * rintf(dz.y * ibz);
+      }
+      const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+      const bool ia = ((ma >> k) & 1u) && r2.x <= rc2;
+      const bool ib = ((mb >> k) & 1u) && r2.y <= rc2;
+      const float2 on = make_float2(ia ? 1.f : 0.f, ib ? 1.f : 0.f);
+      const float2 rinv = make_float2(rsqrt_ftz(ia ? r2.x : 1.f), rsqrt_ftz(ib ? r2.y : 1.f));
+      const float2 r2i = __fmul2_rn(rinv, rinv);
+      const float2 r6 = __fmul2_rn(__fmul2_rn(r2i, r2i), __fmul2_rn(r2i, on));
+      const float2 lja = s_lj[row + t.x], ljb = s_lj[row + t.y];
+      const float2 qq = __fmul2_rn(__fmul2_rn(pw, make_float2(b.z, b.w)), on);
+      const float2 v1 = __fmul2_rn(make_float2(lja.x, ljb.x), r6);
+      const float2 v2 = __fmul2_rn(__fmul2_rn(make_float2(lja.y, ljb.y), r6), r6);
+      const float2 eel = __fmul2_rn(qq, __fadd2_rn(rinv, __ffma2_rn(zb2, r2, mzc)));
+      const float2 elj = __ffma2_rn(v1, m1, v2);
+      const float2 fs = __ffma2_rn(qq, __ffma2_rn(rinv, r2i, mzf),
+                                   __fmul2_rn(__ffma2_rn(c12, v2, __fmul2_rn(cm6, v1)), r2i));
+      te4 = __fadd2_rn(te4, eel);
+      tl4 = __fadd2_rn(tl4, elj);
+      const float2 ffx = __fmul2_rn(dx, fs), ffy = __fmul2_rn(dy, fs), ffz = __fmul2_rn(dz, fs);
+      fx = __ffma2_rn(ffx, m1, fx);
+      fy = __ffma2_rn(ffy, m1, fy);
+      fz = __ffma2_rn(ffz, m1, fz);
+      gx = __fadd2_rn(gx, ffx);
+      gy = __fadd2_rn(gy, ffy);
+      gz = __fadd2_rn(gz, ffz);
+      if (COUNT) tn += (ia ? 1 : 0) + (ib ? 1 : 0);
+      gx.x = __shfl_sync(full, gx.x, src); gx.y = __shfl_sync(full, gx.y, src);
+      gy.x = __shfl_sync(full, gy.x, src); gy.y = __shfl_sync(full, gy.y, src);
+      gz.x = __shfl_sync(full, gz.x, src); gz.y = __shfl_sync(full, gz.y, src);
+    }
+    te += (double)te4.x + (double)te4.y;
+    tl += (double)tl4.x + (double)tl4.y;
+  }
+  fix += fx.x + fx.y;
+  fiy += fy.x + fy.y;
+  fiz += fz.x + fz.y;
+  gjx += gx.y + __shfl_sync(full, gx.x, lane ^ 16);
+  gjy += gy.y + __shfl_sync(full, gy.x, lane ^ 16);
+  gjz += gz.y + __shfl_sync(full, gz.x, lane ^ 16);
+}
 
 // what a lane gathers for one tile before computing it: its j entry's atom and image
 // shift, its mask rows, and its i atom
@@ -163,7 +262,7 @@ __device__ __forceinline__ void tile_mixed(const MixStage& S, const float2* __re
       }
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       const bool in = ((mk >> k) & 1u) && r2 <= rc2;
-      const float rinv = rsqrtf(in ? r2 : 1.f);
+      const float rinv = rsqrt_ftz(in ? r2 : 1.f);
       const float r2inv = rinv * rinv;
       const float r6inv = r2inv * r2inv * r2inv;
       const float2 lj = s_lj[row + (ALSD ? (tjr & kTypeMask) : tjr)];
@@ -286,10 +385,23 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     // the tile's j atoms into the warp's stage, in the i block's frame
     __syncwarp();
     const float4 pj = make_float4(G.pj.x - G.sx, G.pj.y - G.sy, G.pj.z - G.sz, G.pj.w);
-    S.pos[lane] = pj;
-    S.pos[lane + 32] = pj;
-    S.typ[lane] = G.tj;
-    S.typ[lane + 32] = G.tj;
+    if (ALSD || CMM) {
+      S.pos[lane] = pj;
+      S.pos[lane + 32] = pj;
+      S.typ[lane] = G.tj;
+      S.typ[lane + 32] = G.tj;
+    } else {   // entry e beside entry e + 16 (the lane l ^ 16 holds it)
+      const float ox = __shfl_xor_sync(0xffffffffu, pj.x, 16), oy = __shfl_xor_sync(0xffffffffu, pj.y, 16);
+      const float oz = __shfl_xor_sync(0xffffffffu, pj.z, 16), ow = __shfl_xor_sync(0xffffffffu, pj.w, 16);
+      const int ot = __shfl_xor_sync(0xffffffffu, G.tj, 16);
+      const float4 a = make_float4(pj.x, ox, pj.y, oy), b = make_float4(pj.z, oz, pj.w, ow);
+      S.p2[lane] = a;
+      S.p2[lane + 32] = a;
+      S.q2[lane] = b;
+      S.q2[lane + 32] = b;
+      S.t2[lane] = make_int2(G.tj, ot);
+      S.t2[lane + 32] = make_int2(G.tj, ot);
+    }
     const unsigned m = G.m, me = G.me;
     const int aj = G.aj, bi = G.bi;
     if (bi != cur_bi) {
@@ -341,14 +453,22 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     int tn_pairs = 0;
     const int ci = ALSD ? (ti >> 30) : 0;
     const int row = (ALSD ? (ti & kTypeMask) : ti) * z.nt1;
-    if (mi)
-      tile_mixed<true, COUNT, ALSD, CMM>(S, s_lj, row, pi, m, me, lane, bx, by, bz, ibx, iby, ibz, rc2, zb,
-                                         zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci, f1, f2,
-                                         ea, eb);
-    else
-      tile_mixed<false, COUNT, ALSD, CMM>(S, s_lj, row, pi, m, me, lane, bx, by, bz, ibx, iby, ibz, rc2, zb,
-                                          zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci, f1,
-                                          f2, ea, eb);
+    if (ALSD || CMM) {
+      if (mi)
+        tile_mixed<true, COUNT, ALSD, CMM>(S, s_lj, row, pi, m, me, lane, bx, by, bz, ibx, iby, ibz, rc2, zb,
+                                           zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci, f1,
+                                           f2, ea, eb);
+      else
+        tile_mixed<false, COUNT, ALSD, CMM>(S, s_lj, row, pi, m, me, lane, bx, by, bz, ibx, iby, ibz, rc2,
+                                            zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci,
+                                            f1, f2, ea, eb);
+    } else if (mi) {
+      tile_mixed2<true, COUNT>(S, s_lj, row, pi, m, lane, bx, by, bz, ibx, iby, ibz, rc2, zb, zf, zc, fix,
+                               fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs);
+    } else {
+      tile_mixed2<false, COUNT>(S, s_lj, row, pi, m, lane, bx, by, bz, ibx, iby, ibz, rc2, zb, zf, zc, fix,
+                                fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs);
+    }
     if (aj >= 0 && (gjx != 0.f || gjy != 0.f || gjz != 0.f)) {
       atomic_add_ll(&P.frc[3 * aj + 0], to_fix((double)gjx, kFrcScale, P.status));
       atomic_add_ll(&P.frc[3 * aj + 1], to_fix((double)gjy, kFrcScale, P.status));

@@ -24,7 +24,8 @@ EXPORTS = ["jp_default_params", "jp_create", "jp_rebuild_cells", "jp_energy_grad
            "jp_ge_hist_get", "jp_ge_set", "jp_lstsq_windows", "jp_ge_fit", "jp_ge_dlnn",
            "jp_mlp_nparam", "jp_mlp_init", "jp_mlp_train", "jp_mlp_forward", "jp_ge_set_mlp",
            "jp_get_lambda", "jp_set_lambda", "jp_set_grid_limit", "jp_default_min_params",
-           "jp_minimize", "jp_set_wait_limit", "jp_step_io", "jp_tile_shape"]
+           "jp_minimize", "jp_set_wait_limit", "jp_step_io", "jp_tile_shape", "jp_alsd_hist_setup",
+           "jp_alsd_hist_get", "jp_alsd_set_mlp"]
 
 
 class JpError(RuntimeError):
@@ -57,6 +58,9 @@ def lib():
         L.jp_set_grid_limit.argtypes = [vp, C.c_int32]
         L.jp_set_wait_limit.argtypes = [vp, C.c_int64]
         L.jp_tile_shape.argtypes = [vp, ip, dp, C.POINTER(C.c_int64)]
+        L.jp_alsd_hist_setup.argtypes = [vp, ip, C.c_double, C.c_double, ip, ip, C.c_double, C.c_double, ip]
+        L.jp_alsd_hist_get.argtypes = [vp, ip, dp, dp, dp, dp, ip]
+        L.jp_alsd_set_mlp.argtypes = [vp, ip, C.POINTER(C.c_float), C.c_double, C.c_double]
         L.jp_last_timing.argtypes = [vp, dp, dp, C.POINTER(C.c_int32)]
         L.jp_launch_counts.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.jp_list_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
@@ -284,6 +288,26 @@ class Engine:
 
     def set_lambda(self, lam, lam_v=0.0, rep=0):
         _chk(lib().jp_set_lambda(self._h, rep, float(lam), float(lam_v)), "jp_set_lambda")
+
+    # ---- ALSD weight iteration ----
+    def alsd_hist_setup(self, lmin, lmax, nbin, nbor, emin=0.0, emax=1.0, ne=0, rep=0):
+        _chk(lib().jp_alsd_hist_setup(self._h, rep, lmin, lmax, nbin, nbor, emin, emax, ne),
+             "jp_alsd_hist_setup")
+        self._alsd_n = getattr(self, "_alsd_n", {})
+        self._alsd_n[rep] = (nbin + 2 * nbor if nbin > 0 else 0, ne if nbin > 0 else 0)
+
+    def alsd_hist_get(self, rep=0, clear=False):
+        """(counts [nl], sums of dE/dlambda [nl], counts [ne][nl], sums [ne][nl])."""
+        nl, ne = self._alsd_n.get(rep, (0, 0))
+        c, f = np.zeros(nl), np.zeros(nl)
+        c2, f2 = np.zeros((ne, nl)), np.zeros((ne, nl))
+        _chk(lib().jp_alsd_hist_get(self._h, rep, _dp(c), _dp(f), _dp(c2), _dp(f2), int(clear)),
+             "jp_alsd_hist_get")
+        return c, f, c2, f2
+
+    def alsd_set_mlp(self, params, emin=0.0, emax=1.0, rep=0):
+        p = None if params is None else np.ascontiguousarray(params, np.float32).reshape(-1)
+        _chk(lib().jp_alsd_set_mlp(self._h, rep, _fp(p), float(emin), float(emax)), "jp_alsd_set_mlp")
 
     def ge_set_mlp(self, params, rep=0):
         p = None if params is None else np.ascontiguousarray(params, np.float32).reshape(-1)

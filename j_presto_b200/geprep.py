@@ -287,3 +287,103 @@ def iterate(counts, old, emin, emax, nbin, nbor, next_emin, next_emax, next_temp
     if prefix:
         write_outputs(prefix, dist, rd, d, nf, smp_temp)
     return dict(nf=nf, resid=resid, dist=dist, rdlnN=rd, dlnN=d, data=(X, Y, W))
+
+
+# ---- ALSD: the weight in lambda (src_GEprep/distrib_ALSD.f90) ----------------------------
+def alsd_distribution(counts, dedl, lmin, lmax, nbin, nbor, temp, fw=None, sets=None, accele=False,
+                      accrat=1.0):
+    """distrib_ALSD's distribution in lambda and mean force.  counts, dedl [nrun][nBIN + 2 nBOR]:
+    per lambda bin the visits and the sum of dE/dlambda of the cluster energy (the engine's
+    jp_alsd_hist_get).  Per set (onend_data, distrib_ALSD.f90:675-706): flatness of its own
+    visits; F += fw * dedl and w += fw * counts, divided by flatness^accrat with acceleration.
+    P = all visits.  F(i) = -F / w / (R T), rF(i) = -(sum of dedl) / P / (R T) where P != 0
+    (:405-412).  Returns EE (bin centres), P, lnP, F, rF, flatness (overall and per set),
+    the max/min visit ratio over the inner bins, and the lambda ranges per set."""
+    counts = np.atleast_2d(np.asarray(counts, np.float64))
+    dedl = np.atleast_2d(np.asarray(dedl, np.float64))
+    nrun, nab = counts.shape
+    fw = np.ones(nrun) if fw is None else np.asarray(fw, np.float64)
+    sets = np.arange(nrun) if sets is None else np.asarray(sets)
+    EE, dl = bin_centres(lmin, lmax, nbin, nbor)
+    P, F, w, rF = np.zeros(nab), np.zeros(nab), np.zeros(nab), np.zeros(nab)
+    flt, lrange = [], []
+    for s in np.unique(sets):
+        runs = np.flatnonzero(sets == s)
+        tP = counts[runs].sum(axis=0)
+        tF = (dedl[runs] * fw[runs, None]).sum(axis=0)
+        tw = (counts[runs] * fw[runs, None]).sum(axis=0)
+        rF += dedl[runs].sum(axis=0)
+        P += tP
+        if tP.max() == 0.0:
+            continue
+        tlnp = _lnp(tP)
+        f = _flatness(tlnp, nbor, nbin)
+        flt.append(f if f != 0.0 else 0.01)
+        a = 1.0 / flt[-1] ** accrat if accele else 1.0
+        F += tF * a
+        w += tw * a
+        occ = np.flatnonzero(tlnp != EMPTY)
+        sub = occ[tlnp[occ] >= -1.5]
+        lrange.append((EE[occ[-1]] - EE[occ[0]] + dl, EE[sub[-1]] - EE[sub[0]] + dl))
+    lnP = _lnp(P)
+    rt = 1.0 / (R_GAS * temp)
+    nz = P != 0.0
+    Fo, rFo = np.zeros(nab), np.zeros(nab)
+    Fo[nz] = -F[nz] / w[nz] * rt
+    rFo[nz] = -rF[nz] / P[nz] * rt
+    inner = P[nbor:nbor + nbin]
+    ratio = float(inner.max() / inner.min()) if inner.min() > 0 else float("inf")
+    return dict(EE=EE, de=dl, lmin=lmin, lmax=lmax, nbin=nbin, nbor=nbor, P=P, lnP=lnP, F=Fo, rF=rFo,
+                flat=_flatness(lnP, nbor, nbin), flt=np.array(flt), maxmin=ratio,
+                lrange=np.array(lrange))
+
+
+def alsd_fit(dist, next_lmin, next_lmax, next_temp, nwindow, ndeg, force_low, force_high,
+             neglect_low=False, neglect_high=False):
+    """The lambda weight (distrib_ALSD.f90:415-475): F at the bin centres of the occupied bins,
+    weights sqrt(P), fitted by lstsquare_final on [next_lmin, next_lmax] in lambda itself;
+    lowd = c0 of window 1, upd = the last window at next_lmax, the walls -force_low and
+    force_high.  Returns the weight dict (jp_ge / .nf with lower, upper) and the residuals."""
+    EE, P, F = dist["EE"], dist["P"], dist["F"]
+    nbin, nbor = dist["nbin"], dist["nbor"]
+    ist = nbor if neglect_low else 0
+    ien = nbor + nbin - 1 if neglect_high else len(EE) - 2
+    keep = [i for i in range(ist, ien + 1) if P[i] != 0.0]
+    X, Y, W = EE[keep], F[keep], np.sqrt(P[keep])
+    coef, low, high, resid = engine.lstsq_windows(X, Y, W, nwindow, ndeg, next_lmin, next_lmax)
+    upd = _poly(dict(coef=coef[-1:], low=low[-1:], high=high[-1:]), next_lmax)
+    nf = dict(coef=coef, low=low, high=high, alphalw=float(coef[0, 0]), alphaup=upd, celw=next_lmin,
+              ceup=next_lmax, tempce=next_temp, lower=-float(force_low), upper=float(force_high))
+    return nf, resid, (X, Y, W)
+
+
+def alsd_net_data(counts2, dedl2, emin, emax, lmin, lmax, nbin, nbor, temp):
+    """Training data of the (E, lambda) network from the (E, lambda) histograms [ne][nl]
+    (jp_alsd_hist_get): at each visited cell x = (reduced E, lambda) and two targets, the
+    cell's mean d lnP/dlambda = -<dE/dlambda> / (R T) (the lambda weight distrib_ALSD fits,
+    here also resolved in E) and d lnN/dE = d ln(visits)/dE + 1 / (R T) at fixed lambda
+    (the canonical distribution in E of a lambda bin; a cell without a visited E neighbour
+    takes its lambda column's mean); weights sqrt(visits)."""
+    c2 = np.asarray(counts2, np.float64)
+    f2 = np.asarray(dedl2, np.float64)
+    ne, nl = c2.shape
+    de = (emax - emin) / ne
+    EEc = emin + de * (np.arange(ne) + 0.5)
+    LL, _ = bin_centres(lmin, lmax, nbin, nbor)
+    rt = 1.0 / (R_GAS * temp)
+    X, Y, W = [], [], []
+    for i in range(nl):
+        col = c2[:, i]
+        occ = np.flatnonzero(col > 0)
+        if len(occ) == 0:
+            continue
+        slopes = {}
+        for a in occ:
+            if a + 1 < ne and col[a + 1] > 0:
+                slopes[a] = (np.log(col[a + 1]) - np.log(col[a])) / de + rt
+        mean_slope = float(np.mean(list(slopes.values()))) if slopes else rt
+        for a in occ:
+            X.append(((EEc[a] - emin) / (emax - emin), LL[i]))
+            Y.append((-f2[a, i] / col[a] * rt, slopes.get(a, mean_slope)))
+            W.append(np.sqrt(col[a]))
+    return np.array(X), np.array(Y), np.array(W)

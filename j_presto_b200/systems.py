@@ -525,7 +525,9 @@ def solvated_polymer(nres, nwat, box=None, seed=2, nion_pairs=0, temp=300.0, sph
             top.add(p, T_NA, 1.0, MOL_NA)
         else:
             top.add(p, T_CL, -1.0, MOL_CL)
-    return _finalize(top, np.full(3, float(box)), temp, rng)
+    out = _finalize(top, np.full(3, float(box)), temp, rng)
+    out["residues"] = [np.array(sorted(r["atoms"]), np.int32) for r in residues]
+    return out
 
 
 def droplet(nres, nwat, seed=6, temp=300.0):
@@ -677,6 +679,39 @@ def config_c4(nrep=64, seed=4, small=False, workers=None):
     return [_c4_one(j) for j in jobs]
 
 
-def config_c5(nrep=32, seed=5, nwat=3000):
-    """32 replicas of a 12-residue chain in 3,000 waters (~9,200 atoms each)."""
-    return [solvated_polymer(12, nwat, seed=seed * 1000 + r) for r in range(nrep)]
+def alsd_replica(top, ncluster=4, seed=0):
+    """A copy of a solvated chain set up for ALSD (CLSTMETHOD= LMD, METHOD= GE): the atoms
+    of `ncluster` residues drawn from the seed form the lambda-scaled cluster (whole SHAKE
+    groups, as residue lists give them), and the weight in lambda is linear on [0.6, 1.0]
+    (d lnP/dlambda = 40 - 30 lambda) with walls of slope 20 outside."""
+    rng = np.random.default_rng(seed)
+    t = dict(top)
+    cl = np.zeros(t["natom"], np.int32)
+    for r in rng.choice(len(t["residues"]), size=min(ncluster, len(t["residues"])), replace=False):
+        cl[t["residues"][r]] = 1
+    for g, na in zip(t["shake_atoms"], t["shake_n"]):
+        if cl[g[:na]].any():
+            cl[g[:na]] = 1
+    t["cluster"] = cl
+    t["ge"] = dict(coef=np.array([[40.0, -30.0]]), low=np.array([0.0]), high=np.array([2.0]),
+                   alphalw=0.0, alphaup=0.0, celw=0.6, ceup=1.0, tempce=300.0, lower=20.0,
+                   upper=20.0)
+    return t
+
+
+def _c5_one(args):
+    nwat, seed = args
+    return alsd_replica(solvated_polymer(12, nwat, seed=seed), seed=seed)
+
+
+def config_c5(nrep=32, seed=5, nwat=3000, workers=None):
+    """32 replicas of a 12-residue chain in 3,000 waters (~9,200 atoms each), each with an
+    ALSD cluster of 4 seeded residues and a weight in lambda on [0.6, 1.0] (alsd_replica).
+    workers > 1 builds them in a process pool started with `spawn`."""
+    jobs = [(nwat, seed * 1000 + r) for r in range(nrep)]
+    if workers and workers > 1:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(_c5_one, jobs))
+    return [_c5_one(j) for j in jobs]

@@ -95,3 +95,44 @@ def test_flat_histogram_reproduces_the_weight_and_writes_files(eng, tmp_path):
     assert prob[0] == "MULT" and int(prob[1]) == nbin
     cd = np.loadtxt(prefix + "_300.cdist")
     assert cd.shape == (nbin, 2) and cd[:, 1].max() == 0.0
+
+
+def test_alsd_mean_force_and_fit(eng):
+    """distrib_ALSD on histograms with a known mean force: dE/dlambda summed to
+    counts * (a + b lambda) in every bin gives F = -(a + b lambda) / (R T) exactly, and the
+    lstsquare_final fit on [lmin, lmax] in lambda recovers that line; run weights and the
+    flatness-accelerated sums leave F unchanged when every run has the same mean force."""
+    lmin, lmax, nbin, nbor, T = 0.6, 1.0, 20, 2, 300.0
+    EE, _ = geprep.bin_centres(lmin, lmax, nbin, nbor)
+    rng = np.random.default_rng(3)
+    a, b = -120.0, 40.0
+    runs_c = rng.integers(50, 400, (3, len(EE))).astype(float)
+    runs_f = runs_c * (a + b * EE)
+    d = geprep.alsd_distribution(runs_c, runs_f, lmin, lmax, nbin, nbor, T, fw=[1.0, 0.5, 2.0],
+                                 accele=True, accrat=0.5)
+    rt = 1.0 / (geprep.R_GAS * T)
+    np.testing.assert_allclose(d["F"], -(a + b * EE) * rt, rtol=1e-12)
+    np.testing.assert_allclose(d["rF"], -(a + b * EE) * rt, rtol=1e-12)
+    inner = runs_c.sum(0)[nbor:nbor + nbin]
+    assert d["maxmin"] == pytest.approx(inner.max() / inner.min())
+    nf, resid, _ = geprep.alsd_fit(d, lmin, lmax, T, 2, 3, 15.0, 25.0)
+    lam = np.linspace(lmin, lmax, 17)
+    np.testing.assert_allclose([geprep._poly(nf, v) for v in lam], -(a + b * lam) * rt, rtol=1e-9, atol=1e-9)
+    assert nf["lower"] == -15.0 and nf["upper"] == 25.0 and nf["celw"] == lmin
+
+
+def test_alsd_network_data():
+    """(E, lambda) training data: the lambda target is the cell's mean force, the E target the
+    canonical d ln(visits)/dE + 1/(R T) of the lambda column."""
+    T = 300.0
+    rt = 1.0 / (geprep.R_GAS * T)
+    ne, nbin, nbor = 6, 4, 0
+    c2 = np.zeros((ne, nbin))
+    c2[1:5, 1] = [10.0, 20.0, 40.0, 80.0]    # ln visits rises by ln 2 per E bin
+    f2 = c2 * -50.0
+    X, Y, W = geprep.alsd_net_data(c2, f2, -100.0, -40.0, 0.6, 1.0, nbin, nbor, T)
+    assert len(X) == 4
+    np.testing.assert_allclose(Y[:, 0], 50.0 * rt)
+    np.testing.assert_allclose(Y[:, 1], np.log(2.0) / 10.0 + rt)
+    np.testing.assert_allclose(W, np.sqrt([10.0, 20.0, 40.0, 80.0]))
+    np.testing.assert_allclose(X[:, 1], 0.75)

@@ -7,10 +7,11 @@ One-step energies and gradients of both paths against the FP64 oracle on
 Tolerances: FP64 path -- gradient RMS relative 1e-12, energies 1e-8 relative; mixed path --
 gradient RMS relative 1e-5 (the metric's bar) and total potential energy 1e-6 relative.
 
-NVE drift: C1' (1,000 waters, liquid density), METHOD= MICR, SHAKE, 2 fs, 20 ps.  The total
-energy is md_run's bookkeeping (md.f90:578-628): potential energy at time t plus the kinetic
-energy of (v(t-dt/2) + v(t+dt/2))/2; the drift is the least-squares slope over the last 90 %
-of the run in kT per ns per degree of freedom.
+NVE drift: C1' (1,000 waters, liquid density) brought to 300 K by 10 ps of METHOD= CANO
+(the lattice start releases ~10 kcal/mol per water), then METHOD= MICR, SHAKE, 2 fs, 100 ps
+from that state.  The total energy is md_run's bookkeeping (md.f90:578-628): potential
+energy at time t plus the kinetic energy of (v(t-dt/2) + v(t+dt/2))/2; the drift is the
+least-squares slope over the last 90 % of the run in kT per ns per degree of freedom.
 """
 import numpy as np
 import pytest
@@ -23,7 +24,7 @@ pytestmark = pytest.mark.gpu
 
 FP64, MIXED = abi.JP_PREC_FP64, abi.JP_PREC_MIXED
 KB = 8.31451 / 4184.0            # kcal/mol/K (md_run gascst / 4184)
-DRIFT_MAX = 1e-4                 # kT/ns/DOF
+DRIFT_MAX = 3e-4                 # kT/ns/DOF over 100 ps (see test_nve_drift)
 
 
 @pytest.fixture(scope="module")
@@ -44,8 +45,12 @@ def test_full_size_energy_grad_vs_oracle(eng_mod, name):
     for prec in (FP64, MIXED):
         with eng_mod.Engine(top, precision=prec, method=abi.JP_METHOD_MICR) as e:
             ene, g = e.energy_grad()
-            assert e.pair_count() == o.npairs_cut
+            npair = e.pair_count()
             assert e.list_stats()[1] == o.npairs_listed
+        if prec == FP64:
+            assert npair == o.npairs_cut
+        else:   # r^2 <= rc^2 in FP32: a few pairs within rounding of the cut-off may flip
+            assert abs(npair - o.npairs_cut) <= 1e-6 * o.npairs_cut + 4, (npair, o.npairs_cut)
         res[prec] = (ene, g)
     ene, g = res[FP64]
     assert rms_rel(g, go) < 1e-12
@@ -65,11 +70,24 @@ def _drift(E, T, dof):
     return slope / (KB * T[skip:, 0].mean() * dof)
 
 
-@pytest.mark.parametrize("prec", [FP64, MIXED])
-def test_nve_drift(eng_mod, prec):
+@pytest.fixture(scope="module")
+def equilibrated(eng_mod):
     top = systems.config_c1_prime()
+    with eng_mod.Engine(top, precision=FP64, method=abi.JP_METHOD_CANO, tempco=1) as e:
+        e.step(5000, energies=False, temps=False)
+        x, v = e.get_state()
+    return top, x, v
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_nve_drift(eng_mod, equilibrated, prec):
+    top, x, v = equilibrated
     dof = oracle.Oracle(top, method=abi.JP_METHOD_MICR).dof
     with eng_mod.Engine(top, precision=prec, method=abi.JP_METHOD_MICR) as e:
-        E, T = e.step(10000)
+        e.set_state(cord=x, vel=v)
+        e.rebuild()
+        E, T = e.step(50000)
+    # 100 ps resolve a slope to ~7e-5 kT/ns/DOF (the total energy fluctuates by ~0.25
+    # kcal/mol with ~0.1 ps correlation); bench.py measures 0.5 ns against the 1e-4 bar
     drift = _drift(E, T, dof)
     assert abs(drift) < DRIFT_MAX, drift
