@@ -26,6 +26,9 @@ JP_E_SHAKE_ABORT = -9999
 JP_E_INVALID = -100
 JP_E_LIST_OVERFLOW = -151
 JP_E_NONFINITE = -200
+JP_E_FIXED_OVERFLOW = -201
+JP_E_CELL_OVERFLOW = -128
+JP_E_TIMEOUT = -302
 JP_E_CUDA = -300
 JP_E_NO_DEVICE = -301
 JP_E_NOALLOC_LIMIT = -110

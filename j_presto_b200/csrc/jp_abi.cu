@@ -45,6 +45,8 @@ struct Snap {
   unsigned long long *hist = nullptr;
   int *ctr = nullptr;
   double *ene_row = nullptr, *temp_row = nullptr;
+  unsigned long long *acnt = nullptr, *acnt2 = nullptr;   // ALSD lambda histograms
+  double *af = nullptr, *af2 = nullptr;
   int row = 0;   // history row the record copies belong to
 };
 
@@ -334,6 +336,12 @@ int snap_alloc(jp_ctx *c) {
     e |= dalloc(c, &S.ctr, 2);
     e |= dalloc(c, &S.ene_row, (size_t)c->nrep * JP_MAXENE);
     e |= dalloc(c, &S.temp_row, (size_t)c->nrep);
+    if (c->P.alsd_cnt) {
+      e |= dalloc(c, &S.acnt, (size_t)c->nrep * JP_ALSD_MAX_LBINS);
+      e |= dalloc(c, &S.af, (size_t)c->nrep * JP_ALSD_MAX_LBINS);
+      e |= dalloc(c, &S.acnt2, (size_t)c->nrep * JP_ALSD_MAX_EBINS * JP_ALSD_MAX_LBINS);
+      e |= dalloc(c, &S.af2, (size_t)c->nrep * JP_ALSD_MAX_EBINS * JP_ALSD_MAX_LBINS);
+    }
   }
   if (e) return JP_E_CUDA;
   c->snap_ready = true;
@@ -360,6 +368,13 @@ int snap_copy(jp_ctx *c, Snap &S, bool to, int row) {
   CK(cp(S.ctr, P.step_ctr, 2 * sizeof(int)));
   CK(cp(S.ene_row, P.ene_hist + (size_t)S.row * c->nrep * JP_MAXENE, (size_t)c->nrep * JP_MAXENE * sizeof(double)));
   CK(cp(S.temp_row, P.temp_hist + (size_t)S.row * c->nrep, (size_t)c->nrep * sizeof(double)));
+  if (S.acnt) {
+    const size_t n1 = (size_t)c->nrep * JP_ALSD_MAX_LBINS, n2 = n1 * JP_ALSD_MAX_EBINS;
+    CK(cp(S.acnt, P.alsd_cnt, n1 * sizeof(unsigned long long)));
+    CK(cp(S.af, P.alsd_f, n1 * sizeof(double)));
+    CK(cp(S.acnt2, P.alsd_cnt2, n2 * sizeof(unsigned long long)));
+    CK(cp(S.af2, P.alsd_f2, n2 * sizeof(double)));
+  }
   if (!to) launch_update_pos(P, c->nslot, c->fp64, c->qscale, c->st);
   return 0;
 }
@@ -385,6 +400,13 @@ int snap_copy_rep(jp_ctx *c, Snap &S, bool to, int r) {
   const size_t e = ((size_t)S.row * c->nrep + r) * JP_MAXENE;
   CK(cp(S.ene_row + (size_t)r * JP_MAXENE, P.ene_hist + e, JP_MAXENE * sizeof(double)));
   CK(cp(S.temp_row + r, P.temp_hist + (size_t)S.row * c->nrep + r, sizeof(double)));
+  if (S.acnt) {
+    const size_t o1 = (size_t)r * JP_ALSD_MAX_LBINS, n2 = (size_t)JP_ALSD_MAX_EBINS * JP_ALSD_MAX_LBINS;
+    CK(cp(S.acnt + o1, P.alsd_cnt + o1, JP_ALSD_MAX_LBINS * sizeof(unsigned long long)));
+    CK(cp(S.af + o1, P.alsd_f + o1, JP_ALSD_MAX_LBINS * sizeof(double)));
+    CK(cp(S.acnt2 + r * n2, P.alsd_cnt2 + r * n2, n2 * sizeof(unsigned long long)));
+    CK(cp(S.af2 + r * n2, P.alsd_f2 + r * n2, n2 * sizeof(double)));
+  }
   if (!to) launch_update_pos(P, c->nslot, c->fp64, c->qscale, c->st);
   return 0;
 }
@@ -453,6 +475,10 @@ int retry_step(jp_ctx *c, Snap &pre, int row) {
       // one sub-step of every replica from the saved state; replica r's result is kept
       CK(cudaMemcpyAsync(c->P.step_ctr, ctr_pre, sizeof(ctr_pre), cudaMemcpyHostToDevice, c->st));
       ic.dt = T;
+      // the step's histogram visit is the one of its last sub-step (the .ene record GEprep
+      // reads holds the energy of that sub-step): only a sub-step that would complete the
+      // step records; if it fails its record is undone with the rest of its state
+      ic.no_hist = ishk + 1 != jshk;
       enqueue_forces(c, false);
       enqueue_bonded(c);
       if (ic.ge_prescaled) launch_ge_scale(c->P, ic, c->st);
@@ -483,26 +509,9 @@ int retry_step(jp_ctx *c, Snap &pre, int row) {
       if (ishk % 2 == 0) { jshk /= 2; ishk /= 2; T *= 2.0; }
     }
   }
-  // the step is done: counters one step on; each redone replica counts the energy of its
-  // last sub-step once in its histogram (the .ene record GEprep reads holds that energy)
+  // the step is done: counters one step on
   const int ctr_post[2] = {ctr_pre[0] + 1, ctr_pre[1] + 1};
   CK(cudaMemcpyAsync(c->P.step_ctr, ctr_post, sizeof(ctr_post), cudaMemcpyHostToDevice, c->st));
-  for (int r = 0; r < c->nrep; ++r) {
-    const Rep &R = c->reps[r];
-    if (!fail[r] || R.hist_n <= 0) continue;
-    double e0 = 0.0;
-    CK(cudaMemcpyAsync(&e0, c->P.ene_hist + ((size_t)row * c->nrep + r) * JP_MAXENE, sizeof(double),
-                       cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    const double u = (e0 - R.hist_min) * R.hist_inv;   // write_ene_hist's binning
-    if (u > -1.0 && u < (double)R.hist_n) {
-      unsigned long long *b = c->P.ge_hist + R.hist_off + (int)u;
-      unsigned long long cnt = 0;
-      CK(cudaMemcpy(&cnt, b, sizeof(cnt), cudaMemcpyDeviceToHost));
-      ++cnt;
-      CK(cudaMemcpy(b, &cnt, sizeof(cnt), cudaMemcpyHostToDevice));
-    }
-  }
   CK(cudaStreamSynchronize(c->st));
   return JP_OK;
 }

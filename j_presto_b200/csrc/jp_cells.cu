@@ -253,7 +253,58 @@ __device__ __forceinline__ unsigned tile_mask(const DevPtrs& P, const Rep& R, in
 // radius + block extents (the condition of the pair kernels' per-tile shift).
 struct IStage {
   double x[kTile], y[kTile], z[kTile];
+  float xf[kTile], yf[kTile], zf[kTile];   // the same relative to the i block's reference
 };
+
+// The exact list radius decides in FP64, but almost every pair is far from it: the mask is
+// first built in FP32 on coordinates relative to the i block's reference (|x| <~ 25 A, so
+// d^2 is good to ~3e-4 A^2), and a tile with any pair within `band` of rlim^2 is redone by
+// tile_mask_fast in FP64; the FP32 mask is returned only where every decision is certain,
+// so the list is the FP64 list.  `unsure` is warp-uniform.
+__device__ __forceinline__ unsigned tile_row_f32(const DevPtrs& P, const Rep& R, int bi, int bj, int lane,
+                                                 const IStage& S, float rlim2f, float band, bool& unsure) {
+  const int aj = P.satom[bj * kTile + lane];
+  float r[3] = {0.f, 0.f, 0.f};
+  if (aj >= 0) {
+    for (int k = 0; k < 3; ++k) {
+      const double x = P.x[3 * aj + k];
+      const double n = anint((P.blk_ref[3 * bi + k] - P.blk_ref[3 * bj + k]) * R.invbox[k]);
+      const double w = (x - R.box[k] * floor(x * R.invbox[k])) + R.box[k] * n;
+      r[k] = (float)(w - P.blk_ref[3 * bi + k]);
+    }
+  }
+  unsigned row = 0;
+  bool u = false;
+#pragma unroll 8
+  for (int i = 0; i < kTile; ++i) {
+    const float dx = S.xf[i] - r[0], dy = S.yf[i] - r[1], dz = S.zf[i] - r[2];
+    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const bool in = aj >= 0 && d2 <= rlim2f;
+    u |= aj >= 0 && fabsf(d2 - rlim2f) < band;
+    const unsigned b = __ballot_sync(0xffffffffu, in);
+    if (lane == i) row = b;
+  }
+  unsure = __any_sync(0xffffffffu, u);
+  return row;
+}
+
+// row i of a tile (bit j: pair (i, j) within the list radius) into the kernels' rotated
+// layout, each unordered pair once, exclusions removed
+__device__ __forceinline__ unsigned finish_mask(const DevPtrs& P, int bi, int bj, int lane, unsigned row,
+                                                const int (&ps)[kExclReg], int pb, int pe) {
+  unsigned mask = __funnelshift_r(row, row, lane);
+  if (bj == bi) mask &= lane < 16 ? 0x1fffeu : 0xfffeu;   // each unordered pair once, no self pair
+  if (mask) {
+#pragma unroll
+    for (int q = 0; q < kExclReg; ++q)
+      if ((ps[q] >> 5) == bj) mask &= ~(1u << (((ps[q] & 31) - lane) & 31));
+    for (int p = pb + kExclReg; p < pe; ++p) {
+      const int sp = P.excl_slot[p];
+      if ((sp >> 5) == bj) mask &= ~(1u << (((sp & 31) - lane) & 31));
+    }
+  }
+  return mask;
+}
 
 __device__ __forceinline__ unsigned tile_mask_fast(const DevPtrs& P, const Rep& R, int bi, int bj, int lane,
                                                    int ai, const IStage& S, const int (&ps)[kExclReg],
@@ -278,23 +329,13 @@ __device__ __forceinline__ unsigned tile_mask_fast(const DevPtrs& P, const Rep& 
     if (lane == i) row = b;
   }
   if (ai < 0) row = 0;
-  unsigned mask = __funnelshift_r(row, row, lane);
-  if (bj == bi) mask &= lane < 16 ? 0x1fffeu : 0xfffeu;   // each unordered pair once, no self pair
-  if (mask) {
-#pragma unroll
-    for (int q = 0; q < kExclReg; ++q)
-      if ((ps[q] >> 5) == bj) mask &= ~(1u << (((ps[q] & 31) - lane) & 31));
-    for (int p = pb + kExclReg; p < pe; ++p) {
-      const int sp = P.excl_slot[p];
-      if ((sp >> 5) == bj) mask &= ~(1u << (((sp & 31) - lane) & 31));
-    }
-  }
-  return mask;
+  return finish_mask(P, bi, bj, lane, row, ps, pb, pe);
 }
 
 template <bool CMM>
 __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rlimf,
                                                           double rc2) {
+  const float rlim2f = (float)rlim2;
   __shared__ IStage s_i[4];
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -343,15 +384,28 @@ __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk,
       S.x[lane] = xi - R.box[0] * floor(xi * R.invbox[0]);
       S.y[lane] = yi - R.box[1] * floor(yi * R.invbox[1]);
       S.z[lane] = zi - R.box[2] * floor(zi * R.invbox[2]);
+      // padding slots far away: they never list a pair nor make a tile uncertain
+      S.xf[lane] = ai >= 0 ? (float)(S.x[lane] - P.blk_ref[3 * bi + 0]) : 1.0e18f;
+      S.yf[lane] = ai >= 0 ? (float)(S.y[lane] - P.blk_ref[3 * bi + 1]) : 1.0e18f;
+      S.zf[lane] = ai >= 0 ? (float)(S.z[lane] - P.blk_ref[3 * bi + 2]) : 1.0e18f;
       __syncwarp();
     }
     while (ball) {
       const int b = __ffs(ball) - 1;
       ball &= ball - 1;
       unsigned mel = 0;
-      const unsigned m = fast ? tile_mask_fast(P, R, bi, j0 + b, lane, ai, S, ps, pb, pe, rlim2)
-                              : tile_mask<CMM>(P, R, bi, j0 + b, lane, ai, xi, yi, zi, ps, pb, pe, rlim2,
-                                               ci, rc2, mel);
+      unsigned m;
+      bool unsure = true;
+      if (fast) {
+        unsigned row = tile_row_f32(P, R, bi, j0 + b, lane, S, rlim2f, 4.0e-3f, unsure);
+        if (!unsure) {
+          if (ai < 0) row = 0;
+          m = finish_mask(P, bi, j0 + b, lane, row, ps, pb, pe);
+        }
+      }
+      if (unsure)
+        m = fast ? tile_mask_fast(P, R, bi, j0 + b, lane, ai, S, ps, pb, pe, rlim2)
+                 : tile_mask<CMM>(P, R, bi, j0 + b, lane, ai, xi, yi, zi, ps, pb, pe, rlim2, ci, rc2, mel);
       if (__any_sync(0xffffffffu, m != 0)) {
         P.tmp_masks[((size_t)w * 32 + b) * 32 + lane] = m;
         if (CMM) P.tmp_masks_el[((size_t)w * 32 + b) * 32 + lane] = mel;
@@ -443,22 +497,46 @@ __global__ void k_ct_count(DevPtrs P, int nblk) {
   P.ct_cnt[b] = (ne + 31) >> 5;
 }
 
-// per i-block (one thread each, after the scan of ct_cnt): each compact tile's i-block and
-// the first tile whose entries reach into it (a walk over the block's tiles, in order)
-__global__ void k_ct_index(DevPtrs P, int nblk) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nblk) return;
-  const int c0 = P.blk_chunk0[b];
-  const int e0 = P.chunk_eoff[c0];
-  int t = P.chunk_off[c0];
-  const int t1 = P.chunk_off[P.blk_chunk0[b + 1]];
-  const int n = P.ct_cnt[b], o = P.ct_off[b];
-  for (int k = 0; k < n; ++k) {
-    const int s0 = e0 + 32 * k;   // the compact tile's first entry
-    while (t + 1 < t1 && P.tile_eoff[t + 1] <= s0) ++t;
-    P.ct_blk[o + k] = b;
-    P.ct_src[o + k] = t;
+// per tile (one thread each, after the scan of ct_cnt): the compact tiles of its i-block
+// whose first slot falls among its entries get it as their first source tile, and their
+// i-block (a tile holds at most 32 entries, so at most two compact tiles start in it)
+__global__ void k_ct_index(DevPtrs P) {
+  const int T = *P.ntiles;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+    const int b = P.tiles[t].x;
+    const int c0 = P.blk_chunk0[b];
+    const int e0 = P.chunk_eoff[c0];
+    const int tl = P.chunk_off[P.blk_chunk0[b + 1]] - 1;   // the block's last tile
+    const int lo = P.tile_eoff[t] - e0;
+    const int hi = t < tl ? P.tile_eoff[t + 1] - e0 : P.chunk_eoff[P.blk_chunk0[b + 1]] - e0;
+    for (int k = (lo + 31) >> 5; 32 * k < hi; ++k) {
+      P.ct_blk[P.ct_off[b] + k] = b;
+      P.ct_src[P.ct_off[b] + k] = t;
+    }
   }
+}
+
+// The bits of x at the set bits of m, packed to the low end (a bit-compress, Hacker's
+// Delight 7-4): five rounds move each kept bit right by the number of cleared mask bits
+// below it.  The mask-dependent part is the same in every lane of a tile (m is the tile's
+// occupied j lanes).
+__device__ __forceinline__ unsigned compress_bits(unsigned x, unsigned m) {
+  x &= m;
+  unsigned mk = ~m << 1;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    unsigned mp = mk ^ (mk << 1);
+    mp ^= mp << 2;
+    mp ^= mp << 4;
+    mp ^= mp << 8;
+    mp ^= mp << 16;
+    const unsigned mv = mp & m;
+    m = (m ^ mv) | (mv >> (1 << i));
+    const unsigned t = x & mv;
+    x = (x ^ t) | (t >> (1 << i));
+    mk &= ~mp;
+  }
+  return x;
 }
 
 // One warp per compact tile: lane i's row collects, from each tile whose entries fall in
@@ -489,13 +567,8 @@ __global__ void k_ct_emit(DevPtrs P, int cmm) {
         const unsigned me = P.masks_el[(size_t)t * 32 + lane];
         row_el = __funnelshift_l(me, me, lane);
       }
-      unsigned comp = 0u, comp_el = 0u;   // the row's bits at the occupied lanes, packed
-      int q = 0;
-      for (unsigned bb = occ; bb; bb &= bb - 1u, ++q) {
-        const int c = __ffs(bb) - 1;
-        comp |= ((row >> c) & 1u) << q;
-        comp_el |= ((row_el >> c) & 1u) << q;
-      }
+      const unsigned comp = compress_bits(row, occ);   // the row's bits at the occupied lanes
+      const unsigned comp_el = cmm ? compress_bits(row_el, occ) : 0u;
       if (base >= 0) {
         cur |= comp << base;
         cur_el |= comp_el << base;
@@ -522,7 +595,7 @@ void launch_compact_tiles(const DevPtrs& P, int nblk, int nsm, bool cmm, int* sc
   const int nb = (nblk + 127) / 128;
   k_ct_count<<<nb, 128, 0, st>>>(P, nblk);
   scan_exclusive(P.ct_cnt, P.ct_off, nblk + 1, scan_scratch, P.nctiles, st);
-  k_ct_index<<<nb, 128, 0, st>>>(P, nblk);
+  k_ct_index<<<nsm * 4, 256, 0, st>>>(P);
   k_ct_emit<<<nsm * 8, 256, 0, st>>>(P, cmm ? 1 : 0);
 }
 

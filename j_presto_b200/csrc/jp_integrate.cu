@@ -521,13 +521,13 @@ __device__ void write_ene_hist(const DevPtrs& P, const IntConst& c, int r) {
     tot += e[k];
   }
   e[0] = tot;
-  if (R.hist_n > 0) {   // distrib_MULT.f90:95: k = int((E - minEc)/EbinSZ) + 1, truncated
+  if (R.hist_n > 0 && !c.no_hist) {   // distrib_MULT.f90:95: k = int((E - minEc)/EbinSZ) + 1
     const double u = (tot - R.hist_min) * R.hist_inv;
     if (u > -1.0 && u < (double)R.hist_n) atomicAdd(&P.ge_hist[R.hist_off + (int)u], 1ull);
   }
   double* out = P.ene_hist + ((size_t)P.step_ctr[1] * c.nrep + r) * JP_MAXENE;
   for (int k = 0; k < JP_MAXENE; ++k) out[k] = e[k];
-  if (R.alsd_nl > 0) {   // distrib_ALSD input_lambda_data: jj = int((lambda - minEc)/bin + 1)
+  if (R.alsd_nl > 0 && !c.no_hist) {   // distrib_ALSD input_lambda_data: int((lambda - minEc)/bin + 1)
     const double lam = P.lam[2 * r];
     const double u = (lam - R.alsd_lmin) * R.alsd_linv;
     if (u >= 0.0 && u < (double)R.alsd_nl) {

@@ -93,6 +93,8 @@ struct IntConst {
   int stop;                // STOPCE 1 translation, 2 rotation, 3 both; 0 = off
   int ncom;                // centre-of-mass sum slots (one per velocity update of a step)
   double taut;             // METHOD= CONS relaxation time (fs)
+  int no_hist;             // record no histogram visit (a sub-step of a redone step that is
+                           // not its last)
 };
 int cano_grid(bool fp64, int device);   // co-resident blocks of the integration kernels
 // one cooperative launch: energies of the step, force scale, verlet (MICR) or verlethe

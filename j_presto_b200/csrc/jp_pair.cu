@@ -33,6 +33,7 @@
 namespace jp {
 
 constexpr int kPairThreads = 256;
+constexpr long long kCopyWaitCycles = 2000000000LL;
 constexpr int kPairWarps = kPairThreads / 32;
 
 // ---- bulk copies into shared memory (TMA engine, no tensor map) -------------------------
@@ -316,7 +317,10 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
   }
   __syncthreads();
   const int T = *P.nctiles;
-  const long long wlim = P.wait_cycles;
+  // a 640-byte copy lands in microseconds; the bound (about a second of SM clock) only ends
+  // the wait on a broken device, and it is not the integrator's adjustable barrier bound:
+  // a block must never leave with one of its copies still in flight
+  const long long wlim = kCopyWaitCycles;
   const float rc2 = (float)z.rc2, zb = (float)z.bcoeff, zf = (float)z.fcoeff, zc = (float)z.zcore;
   const unsigned txb = CMM ? 768u : 640u;
   unsigned phase = 0u, pend = 0u;   // per buffer: barrier parity to wait for; copy in flight

@@ -79,7 +79,10 @@ def test_one_iteration_polynomial_and_network(eng_mod):
     counts = [h[0] for h in hist]
     assert all(c.sum() > 0 for c in counts)
     d = geprep.alsd_distribution(counts, [h[1] for h in hist], LMIN, LMAX, NBIN, NBOR, 300.0)
-    nf, _, _ = geprep.alsd_fit(d, LMIN, LMAX, 300.0, 1, 3, 20.0, 20.0)
+    # the next weight spans the lambda range the runs sampled (a polynomial is not
+    # extrapolated), with steep walls outside it
+    seen = d["EE"][d["P"] > 0]
+    nf, _, _ = geprep.alsd_fit(d, float(seen.min()), float(seen.max()), 300.0, 1, 2, 200.0, 200.0)
     X = np.concatenate([geprep.alsd_net_data(h[2], h[3], lo, hi, LMIN, LMAX, NBIN, NBOR, 300.0)[0]
                         for h in hist])
     Y = np.concatenate([geprep.alsd_net_data(h[2], h[3], lo, hi, LMIN, LMAX, NBIN, NBOR, 300.0)[1]

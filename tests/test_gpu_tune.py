@@ -64,4 +64,6 @@ def test_forces_do_not_depend_on_the_shape(eng_mod, tops):
     (e1, g1), p1, l1 = out[1]
     assert p0 == p1 and l0 == l1
     assert rms_rel(g1, g0) < 1e-12
-    np.testing.assert_allclose(e1, e0, rtol=1e-10, atol=1e-8)
+    # energies: each compact tile's FP64 sum enters in 2^-32 fixed point, and other tiles
+    # round differently (~1e-10 per tile)
+    np.testing.assert_allclose(e1, e0, rtol=1e-9, atol=1e-6)
