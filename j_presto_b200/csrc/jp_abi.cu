@@ -253,7 +253,7 @@ void drop_graphs(jp_ctx *c) {
 int launches_per_step(const jp_ctx *c) {
   int n = 1;                       // pair
   n += c->nterm > 0 ? 1 : 0;      // bonded
-  n += 1;                          // the fused cooperative MICR or CANO/GE kernel
+  n += integrate_launches(c->ic, c->cano_grid);   // the integration (one or per-phase kernels)
   n += c->ic.ge_prescaled ? 1 : 0; // k_ge_scale
   n += c->cmm ? 2 : 0;             // k_cmm_far, k_cmm_energy
   n += c->hbond ? 1 : 0;           // k_hbond
@@ -1588,6 +1588,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.done, (size_t)nrep);
   e |= dalloc(c, &P.rep_fail, (size_t)nrep);
   e |= dalloc(c, &P.lam_dew, (size_t)nrep);
+  e |= dalloc(c, &P.lam_step, (size_t)5 * nrep);
   if (prm->alsd != JP_ALSD_NONE) {
     e |= dalloc(c, &P.alsd_cnt, (size_t)nrep * JP_ALSD_MAX_LBINS);
     e |= dalloc(c, &P.alsd_f, (size_t)nrep * JP_ALSD_MAX_LBINS);

@@ -229,6 +229,7 @@ struct DevPtrs {
   unsigned long long *alsd_cnt, *alsd_cnt2;
   double *alsd_f, *alsd_f2;
   double *lam_dew;                // [nrep] the lambda weight term of the step from the network
+  double *lam_step;               // [5 nrep] lambda's state through a step of per-phase launches
   unsigned *status;               // error bits
   unsigned *bar;                  // grid barrier of the cooperative integrator [4]
   long long *pair_cnt;            // [nrep]

@@ -978,12 +978,12 @@ __global__ void __launch_bounds__(64) k_micr_fused(DevPtrs P, IntConst c, int nu
 }
 
 // ---- METHOD= CANO / GE: verlethe.f90 ----------------------------------------------------
-// Streaming form: one unit's state lives in global memory between phases (any number of
-// units per thread; also used for 4-atom groups by the register-resident form).
+// Streaming form of a 1-3 atom unit: its state lives in the atom arrays between phases (the
+// per-phase launches below; 4-atom groups take the eight-lane form further down).
 
 // phase 1 (verlethe.f90:380-398): back up x, v; velt = v - dt/2 c g/m; KE(velt) -> slot 0
 template <bool FP64>
-__device__ __noinline__ double cano1_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s) {
+__device__ __forceinline__ double cano1_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s) {
   const double rt = 0.5 * c.dt * kConvcv;
   double ke = 0.0;
   JP_UNIT_LOOP(q) {
@@ -1006,7 +1006,7 @@ __device__ __noinline__ double cano1_unit(const DevPtrs& P, const IntConst& c, c
 
 // phase 2 (verlethe.f90:400-516): chi from slot 0; v = (2chi-1)v - chi dt c g/m; x += dt v
 template <bool FP64>
-__device__ __noinline__ void cano2_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
+__device__ __forceinline__ void cano2_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
                                         double tt) {
   double tempc = c.temp;
   if (c.shake_method != JP_SHAKE_NONE) tempc = sub_temp(P, c, 0, u.sub);
@@ -1030,7 +1030,7 @@ __device__ __noinline__ void cano2_unit(const DevPtrs& P, const IntConst& c, con
 // phase 3 of an iteration (verlethe.f90:524-612): SHAKE, v = (x-x0)/dt,
 // velt = (vback+v)/2, KE(velt)
 template <bool FP64>
-__device__ __noinline__ double cano3_unit(const DevPtrs& P, const IntConst& c, const Unit& u) {
+__device__ __forceinline__ double cano3_unit(const DevPtrs& P, const IntConst& c, const Unit& u) {
   const Rep& R = P.reps[u.rep];
   double x1[4][3], x0[4][3], im[4];
   JP_UNIT_LOOP(q) {
@@ -1042,8 +1042,8 @@ __device__ __noinline__ double cano3_unit(const DevPtrs& P, const IntConst& c, c
       P.xback[3 * a + k] = x1[q][k];
     }
   }
-  if (u.n >= 2) {
-    const int ier = shake_group(R, u, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
+  if (u.n >= 2) {   // 2-3 atoms: the register-array form
+    const int ier = shake_small(R, u.n, u.d2, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
     if (ier) shake_status(P, ier, u.rep);
   }
   const double ri = 1.0 / c.dt;
@@ -1069,7 +1069,7 @@ __device__ __noinline__ double cano3_unit(const DevPtrs& P, const IntConst& c, c
 
 // phase 4 (verlethe.f90:625-640): forcec += (x - xback)/dt^2; velt; KE
 template <bool FP64>
-__device__ __noinline__ double cano4_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s) {
+__device__ __forceinline__ double cano4_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s) {
   const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
   double ke = 0.0;
   JP_UNIT_LOOP(q) {
@@ -1093,7 +1093,7 @@ __device__ __noinline__ double cano4_unit(const DevPtrs& P, const IntConst& c, c
 // phase 5 (verlethe.f90:641-718): chi from slot 2*it; v = chi dt (-c g/m + forcec) +
 // (2chi-1) vback; x = x0 + dt v
 template <bool FP64>
-__device__ __noinline__ void cano5_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
+__device__ __forceinline__ void cano5_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
                                         int it, double tt) {
   const double chi = sqrt(tt / sub_temp(P, c, 2 * it, u.sub));
   const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
@@ -1470,9 +1470,9 @@ __device__ int quad_shake(const Rep& R, const QLane& q, double x[3], const doubl
 }
 
 // the per-atom phases of a quad lane, on its shared-memory slot (component 0-2)
-template <bool FP64>
+template <bool FP64, class SM>
 __device__ __forceinline__ double q_cano1(const DevPtrs& P, const IntConst& c, const QLane& q,
-                                          UnitSmem& S, int tid, double s) {
+                                          SM& S, int tid, double s) {
   double ke = 0.0;
   if (q.a >= 0) {
     const double rt = 0.5 * c.dt * kConvcv;
@@ -1489,9 +1489,9 @@ __device__ __forceinline__ double q_cano1(const DevPtrs& P, const IntConst& c, c
   return sum8(ke);
 }
 
-template <bool FP64>
+template <bool FP64, class SM>
 __device__ __forceinline__ void q_cano2(const DevPtrs& P, const IntConst& c, const QLane& q,
-                                        UnitSmem& S, int tid, double s, double chi) {
+                                        SM& S, int tid, double s, double chi) {
   if (q.a < 0) return;
   const double a1 = chi * c.dt * kConvcv, b1 = 2.0 * chi - 1.0;
   double g[3];
@@ -1504,8 +1504,9 @@ __device__ __forceinline__ void q_cano2(const DevPtrs& P, const IntConst& c, con
   }
 }
 
+template <class SM>
 __device__ __forceinline__ double q_cano3(const DevPtrs& P, const IntConst& c, const QLane& q,
-                                          UnitSmem& S, int tid) {
+                                          SM& S, int tid) {
   double x[3], x0[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -1529,9 +1530,9 @@ __device__ __forceinline__ double q_cano3(const DevPtrs& P, const IntConst& c, c
   return sum8(ke);
 }
 
-template <bool FP64>
+template <bool FP64, class SM>
 __device__ __forceinline__ double q_cano4(const DevPtrs& P, const IntConst& c, const QLane& q,
-                                          UnitSmem& S, int tid, double s) {
+                                          SM& S, int tid, double s) {
   double ke = 0.0;
   if (q.a >= 0) {
     const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
@@ -1549,9 +1550,9 @@ __device__ __forceinline__ double q_cano4(const DevPtrs& P, const IntConst& c, c
   return sum8(ke);
 }
 
-template <bool FP64>
+template <bool FP64, class SM>
 __device__ __forceinline__ void q_cano5(const DevPtrs& P, const IntConst& c, const QLane& q,
-                                        UnitSmem& S, int tid, double s, double chi) {
+                                        SM& S, int tid, double s, double chi) {
   if (q.a < 0) return;
   const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
   double g[3];
@@ -1565,8 +1566,8 @@ __device__ __forceinline__ void q_cano5(const DevPtrs& P, const IntConst& c, con
 
 // streaming form of a quad lane: its slot is filled from and returned to the atom arrays
 // around each phase (x, x0, v(t-dt/2) = vback, forcec, and x - xback for the SHAKE shift)
-__device__ __forceinline__ void q_fetch(const DevPtrs& P, const QLane& q, UnitSmem& S, int tid,
-                                        bool first) {
+template <class SM>
+__device__ __forceinline__ void q_fetch(const DevPtrs& P, const QLane& q, SM& S, int tid, bool first) {
   if (q.a < 0) return;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -1585,8 +1586,9 @@ __device__ __forceinline__ void q_fetch(const DevPtrs& P, const QLane& q, UnitSm
   }
 }
 
-__device__ __forceinline__ void q_spill(const DevPtrs& P, const IntConst& c, const QLane& q,
-                                        UnitSmem& S, int tid, bool fp64) {
+template <class SM>
+__device__ __forceinline__ void q_spill(const DevPtrs& P, const IntConst& c, const QLane& q, SM& S,
+                                        int tid, bool fp64) {
   if (q.a < 0) return;
   const double ri = 1.0 / c.dt;
   double xq[3];
@@ -1654,8 +1656,9 @@ __device__ __forceinline__ void fix_small(const DevPtrs& P, const IntConst& c, i
   }
 }
 
-__device__ __forceinline__ int com_quad(const DevPtrs& P, const IntConst& c, const QLane& q,
-                                        const UnitSmem& S, int tid, double* w) {
+template <class SM>
+__device__ __forceinline__ int com_quad(const DevPtrs& P, const IntConst& c, const QLane& q, const SM& S,
+                                        int tid, double* w) {
 #pragma unroll
   for (int k = 0; k < kCom; ++k) w[k] = 0.0;
   if (q.a < 0 || !stopped(P.reps[q.rep], q.a)) return -1;
@@ -1670,8 +1673,9 @@ __device__ __forceinline__ int com_quad(const DevPtrs& P, const IntConst& c, con
   return q.rep;
 }
 
+template <class SM>
 __device__ __forceinline__ void fix_quad(const DevPtrs& P, const IntConst& c, int slot, const QLane& q,
-                                         UnitSmem& S, int tid) {
+                                         SM& S, int tid) {
   ComFix F;
   if (q.a < 0 || !stopped(P.reps[q.rep], q.a) || !com_fix(P, c, slot, q.rep, F)) return;
   double x0[3], d[3];
@@ -1724,15 +1728,13 @@ __device__ __forceinline__ void fix_unit(const DevPtrs& P, const IntConst& c, in
   }
 }
 
-// Whole step for all replicas, one launch.  Virtual lanes: [0, nsmall) one 1-3 atom unit
-// each; [qbase, nvirt) eight lanes per 4-atom group.  RESIDENT: one virtual lane per thread
-// and all unit state on chip for the whole step; else grid-stride over the virtual lanes
-// with the state in the atom arrays between phases.
-template <bool FP64, bool RESIDENT, bool STOP>
-__global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst c, int nunit) {
+// Whole step for all replicas, one cooperative launch, when every virtual lane has a thread of
+// its own: [0, nsmall) one 1-3 atom unit each, [qbase, nvirt) eight lanes per 4-atom group, all
+// unit state on chip for the whole step, a grid barrier between phases.
+template <bool FP64, bool STOP>
+__global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst c) {
   __shared__ UnitSmem S;
   __shared__ unsigned char s_act[kActCache];   // replicas still in the SHAKE<->thermostat loop
-  const int nthr = gridDim.x * blockDim.x;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int tid = threadIdx.x;
   const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
@@ -1743,53 +1745,28 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
   LamStep L{};
   const bool lam_thread = c.alsd && gt < c.nrep && P.reps[gt].lam_mode != 0;
   if (lam_thread) lam_begin(P, c, gt, L, shk);
-  const int nv = RESIDENT ? nthr : c.nvirt;
-  // RESIDENT state of this thread's lane
+  // the lane's state (warp-uniform kinds: qbase and nvirt are multiples of 32)
   UnitScal U;
   QLane Q;
-  bool small = false, quad = false;
+  const bool small = gt < c.nsmall;
+  const bool quad = gt >= c.qbase && gt < c.nvirt;
   double s = 1.0;
-  if (RESIDENT) {
-    const int v = gt;
-    small = v < c.nsmall;
-    quad = v >= c.qbase && v < c.nvirt;
-    if (small) {
-      const Unit u = P.units[P.small_idx[v]];
-      ru_load(P, u, U, S, tid);
-      s = rep_scale(P, c, u.rep);
-    } else if (quad) {
-      Q = ql_make(P, c, v);
-      q_fetch(P, Q, S, tid, true);
-      s = rep_scale(P, c, Q.rep);
-    }
+  if (small) {
+    const Unit u = P.units[P.small_idx[gt]];
+    ru_load(P, u, U, S, tid);
+    s = rep_scale(P, c, u.rep);
+  } else if (quad) {
+    Q = ql_make(P, c, gt);
+    q_fetch(P, Q, S, tid, true);
+    s = rep_scale(P, c, Q.rep);
   }
   // phase 1 (verlethe.f90:380-398); with the centre-of-mass stop also without SHAKE (x0)
   if (shk || STOP) {
-    for (int base = 0; base < nv; base += nthr) {
-      const int v = base + gt;
-      if (RESIDENT) {
-        if (quad) {   // warp-uniform: one kinetic-sum call site per warp kind
-          add_kin_quad(P, c.nsub_total, 0, Q.sub, q_cano1<FP64>(P, c, Q, S, tid, s));
-        } else {
-          const double ke = small ? ru_cano1<FP64>(P, c, U, S, tid, s) : 0.0;
-          add_kin(P, c.nsub_total, 0, small ? U.sub : -1, ke);
-        }
-      } else if (v >= c.qbase) {
-        const QLane q = ql_make(P, c, v);
-        q_fetch(P, q, S, tid, true);
-        const double ke = q_cano1<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep));
-        q_spill(P, c, q, S, tid, FP64);
-        add_kin_quad(P, c.nsub_total, 0, q.sub, ke);
-      } else {
-        double ke = 0.0;
-        int sub = -1;
-        if (v < c.nsmall) {
-          const Unit u = P.units[P.small_idx[v]];
-          sub = u.sub;
-          ke = cano1_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
-        }
-        add_kin(P, c.nsub_total, 0, sub, ke);
-      }
+    if (quad) {   // warp-uniform: one kinetic-sum call site per warp kind
+      add_kin_quad(P, c.nsub_total, 0, Q.sub, q_cano1<FP64>(P, c, Q, S, tid, s));
+    } else {
+      const double ke = small ? ru_cano1<FP64>(P, c, U, S, tid, s) : 0.0;
+      add_kin(P, c.nsub_total, 0, small ? U.sub : -1, ke);
     }
     if (!grid_barrier(P, epoch)) return;
   }
@@ -1797,26 +1774,239 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
   // phase 2 (verlethe.f90:400-516) + phase 3 of the first SHAKE pass; the centre-of-mass
   // stop puts its sums and a grid barrier between the two (com slot 0)
   constexpr bool split = STOP;   // c.stop != 0
-  for (int base = 0; base < nv; base += nthr) {
-    const int v = base + gt;
+  {
     double w[kCom];
-    if (RESIDENT) {
-      if (quad) {
-        const double chi = Q.grp ? sqrt(tt / sub_temp(P, c, 0, Q.sub)) : 1.0;
-        q_cano2<FP64>(P, c, Q, S, tid, s, chi);
-        if (split) com_add(P, c, 0, com_quad(P, c, Q, S, tid, w), w);
-        else add_kin_quad(P, c.nsub_total, 1, Q.sub, q_cano3(P, c, Q, S, tid));
-      } else {
-        double ke = 0.0;
-        if (small) {
-          const double chi = sqrt(tt / (shk ? sub_temp(P, c, 0, U.sub) : c.temp));
-          ru_cano2<FP64>(P, c, U, S, tid, s, chi, shk);
-          if (shk && !split) ke = ru_cano3(P, c, U, S, tid);
-        }
-        if (split) com_add(P, c, 0, small ? com_small(P, c, U, S, tid, w) : -1, w);
-        else if (shk) add_kin(P, c.nsub_total, 1, small ? U.sub : -1, ke);
+    if (quad) {
+      const double chi = Q.grp ? sqrt(tt / sub_temp(P, c, 0, Q.sub)) : 1.0;
+      q_cano2<FP64>(P, c, Q, S, tid, s, chi);
+      if (split) com_add(P, c, 0, com_quad(P, c, Q, S, tid, w), w);
+      else add_kin_quad(P, c.nsub_total, 1, Q.sub, q_cano3(P, c, Q, S, tid));
+    } else {
+      double ke = 0.0;
+      if (small) {
+        const double chi = sqrt(tt / (shk ? sub_temp(P, c, 0, U.sub) : c.temp));
+        ru_cano2<FP64>(P, c, U, S, tid, s, chi, shk);
+        if (shk && !split) ke = ru_cano3(P, c, U, S, tid);
       }
-    } else if (v >= c.qbase) {
+      if (split) com_add(P, c, 0, small ? com_small(P, c, U, S, tid, w) : -1, w);
+      else if (shk) add_kin(P, c.nsub_total, 1, small ? U.sub : -1, ke);
+    }
+  }
+  if (split) {
+    if (!grid_barrier(P, epoch)) return;
+    // the correction, then phase 3
+    if (quad) {
+      fix_quad(P, c, 0, Q, S, tid);
+      add_kin_quad(P, c.nsub_total, 1, Q.sub, q_cano3(P, c, Q, S, tid));
+    } else {
+      double ke = 0.0;
+      if (small) {
+        fix_small(P, c, 0, U, S, tid, shk);
+        if (shk) ke = ru_cano3(P, c, U, S, tid);
+      }
+      if (shk) add_kin(P, c.nsub_total, 1, small ? U.sub : -1, ke);
+    }
+  }
+  if (shk) {
+    for (int it = 1; it < c.icslop; ++it) {
+      if (!grid_barrier(P, epoch)) return;
+      if (!any_active(P, c, it, tt, s_act)) break;
+      // lambda's velocity stays (v_back + v)/2 through the loop (verlethe.f90:529)
+      const bool lam_act = lam_thread && rep_active(P, c, s_act, gt, it, tt);
+      if (lam_act) {
+        lam_add_ke(P, c, P.reps[gt], 2 * it, L.lvt);
+        lam_add_ke(P, c, P.reps[gt], 2 * it + 1, L.lvt);
+      }
+      // phase 4 (verlethe.f90:625-640)
+      if (quad) {
+        const bool act = Q.grp && rep_active(P, c, s_act, Q.rep, it, tt);
+        const double ke = q_cano4<FP64>(P, c, Q, S, tid, s);
+        add_kin_quad(P, c.nsub_total, 2 * it, act ? Q.sub : -1, act ? ke : 0.0);
+      } else {
+        const bool act = small && rep_active(P, c, s_act, U.rep, it, tt);
+        const double ke = act ? ru_cano4<FP64>(P, c, U, S, tid, s) : 0.0;
+        add_kin(P, c.nsub_total, 2 * it, act ? U.sub : -1, ke);
+      }
+      if (!grid_barrier(P, epoch)) return;
+      // phase 5 (verlethe.f90:641-718) + phase 3 of the next SHAKE pass; with the
+      // centre-of-mass stop: phase 5 and the sums (com slot it), barrier, correction + phase 3
+      if (split) {
+        double w[kCom];
+        int rep = -1;
+        if (!quad) {
+          if (small && rep_active(P, c, s_act, U.rep, it, tt)) {
+            ru_cano5<FP64>(P, c, U, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, U.sub)));
+            rep = com_small(P, c, U, S, tid, w);
+          }
+        } else if (Q.grp && rep_active(P, c, s_act, Q.rep, it, tt)) {
+          q_cano5<FP64>(P, c, Q, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, Q.sub)));
+          rep = com_quad(P, c, Q, S, tid, w);
+        }
+        com_add(P, c, it, rep, w);
+        if (!grid_barrier(P, epoch)) return;
+        // the correction, then phase 3
+        if (!quad) {
+          const bool act = small && rep_active(P, c, s_act, U.rep, it, tt);
+          double ke = 0.0;
+          if (act) {
+            fix_small(P, c, it, U, S, tid, shk);
+            ke = ru_cano3(P, c, U, S, tid);
+          }
+          add_kin(P, c.nsub_total, 2 * it + 1, act ? U.sub : -1, ke);
+        } else {
+          const bool act = Q.grp && rep_active(P, c, s_act, Q.rep, it, tt);
+          double sx[3], sdx[3];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) { sx[k] = S.x[k][tid]; sdx[k] = S.dxs[k][tid]; }
+          if (act) fix_quad(P, c, it, Q, S, tid);
+          const double ke = q_cano3(P, c, Q, S, tid);
+          if (!act && Q.a >= 0) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { S.x[k][tid] = sx[k]; S.dxs[k][tid] = sdx[k]; }
+          }
+          add_kin_quad(P, c.nsub_total, 2 * it + 1, act ? Q.sub : -1, act ? ke : 0.0);
+        }
+        continue;
+      }
+      if (!quad) {
+        const bool act = small && rep_active(P, c, s_act, U.rep, it, tt);
+        double ke = 0.0;
+        if (act) {
+          ru_cano5<FP64>(P, c, U, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, U.sub)));
+          ke = ru_cano3(P, c, U, S, tid);
+        }
+        add_kin(P, c.nsub_total, 2 * it + 1, act ? U.sub : -1, ke);
+      } else {
+        // the whole warp runs the SHAKE (its shuffles); inactive groups keep their state
+        const bool act = Q.grp && rep_active(P, c, s_act, Q.rep, it, tt);
+        double sx[3], sdx[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { sx[k] = S.x[k][tid]; sdx[k] = S.dxs[k][tid]; }
+        if (act) q_cano5<FP64>(P, c, Q, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, Q.sub)));
+        const double ke = q_cano3(P, c, Q, S, tid);
+        if (!act && Q.a >= 0) {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) { S.x[k][tid] = sx[k]; S.dxs[k][tid] = sdx[k]; }
+        }
+        add_kin_quad(P, c.nsub_total, 2 * it + 1, act ? Q.sub : -1, act ? ke : 0.0);
+      }
+    }
+  }
+  // the lane's new state back to memory
+  if (small) {
+    bool bad = false;
+    const double ri = 1.0 / c.dt;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      if (q < U.n) {
+        const int a = U.a[q];
+        double xq[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const int i = 3 * q + k;
+          xq[k] = S.x[i][tid];
+          P.x[3 * a + k] = xq[k];
+          P.v[3 * a + k] = shk ? (xq[k] - S.x0[i][tid]) * ri : S.dxs[i][tid];
+          bad |= !isfinite(xq[k]);
+        }
+        write_slot(P, a, xq, FP64);
+      }
+    }
+    if (bad) atomicOr(P.status, ERR_NONFINITE);
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      if (q < U.n) zero_force<FP64>(P, U.a[q]);
+  } else if (quad) {
+    q_spill(P, c, Q, S, tid, FP64);
+    if (Q.a >= 0) zero_force<FP64>(P, Q.a);
+  }
+  if (lam_thread) {
+    P.lam[2 * gt] = L.lam;
+    P.lam[2 * gt + 1] = L.lv;
+  }
+  finish_last(P, c, tt);
+}
+
+// ---- METHOD= CANO / GE, streaming form: one launch per phase -------------------------------
+// A system with more virtual lanes than the cooperative launch holds at once runs its step as
+// a chain of ordinary launches with one virtual lane per thread, so that every lane's loads
+// are in flight together: each launch is one phase of the form above, the launch boundary
+// stands where that form has a grid barrier, and a lane's state is in the atom arrays between
+// launches (x, x0, v, vback, xback, forcec).  A launch for a SHAKE <-> thermostat pass that no
+// replica still runs returns at once.  Lambda's state through the step is kept in lam_step.
+enum : int {
+  PH_BEGIN = 0,     // energy record, lambda force; phase 1
+  PH_UPDATE = 1,    // lambda advance; phase 2, then phase 3 (with the stop: its sums, slot 0)
+  PH_FIX = 2,       // with the stop: correction by the sums of slot `it`, then phase 3
+  PH_CORR = 3,      // pass `it`: phase 4
+  PH_RESCALE = 4,   // pass `it`: phase 5, then phase 3 (with the stop: its sums, slot it)
+  PH_END = 5        // forces cleared, lambda stored, temperatures and step counters
+};
+
+// shared-memory state of the 4-atom group lanes of a launch (component 0-2)
+struct QuadSmem {
+  double x[3][kIntThreads], x0[3][kIntThreads], vb[3][kIntThreads];
+  double dxs[3][kIntThreads], fc[3][kIntThreads];
+};
+
+__device__ __forceinline__ void lam_save(const DevPtrs& P, int r, const LamStep& L) {
+  double* d = P.lam_step + 5 * r;
+  d[0] = L.lam; d[1] = L.lv; d[2] = L.lvback; d[3] = L.lf; d[4] = L.lvt;
+}
+
+__device__ __forceinline__ void lam_load(const DevPtrs& P, int r, LamStep& L) {
+  const double* d = P.lam_step + 5 * r;
+  L.lam = d[0]; L.lv = d[1]; L.lvback = d[2]; L.lf = d[3]; L.lvt = d[4];
+}
+
+// KIND 0: the 1-3 atom units [0, nsmall) and the per-replica threads (energy record,
+// lambda); KIND 1: the 4-atom group lanes [qbase, nvirt) (a launch of its own, as their
+// SHAKE needs several times the registers); KIND 2 (PH_END only): every lane.
+template <bool FP64, bool STOP, int PH, int KIND>
+__global__ void __launch_bounds__(kIntThreads) k_cano_phase(DevPtrs P, IntConst c, int it) {
+  __shared__ QuadSmem S;
+  __shared__ unsigned char s_act[kActCache];
+  const int v = (KIND == 1 ? c.qbase : 0) + blockIdx.x * blockDim.x + threadIdx.x;
+  const int tid = threadIdx.x;
+  const double tt = target_temp(c, (long long)P.step_ctr[0] + 1);
+  const bool shk = c.shake_method != JP_SHAKE_NONE;
+  const bool lam_thread = KIND != 1 && c.alsd && v < c.nrep && P.reps[v].lam_mode != 0;
+  const bool small = KIND != 1 && v < c.nsmall;
+  const bool quad = KIND != 0 && v >= c.qbase && v < c.nvirt;   // warp-uniform (multiples of 32)
+  constexpr bool split = STOP;
+  if (PH == PH_BEGIN) {
+    if (KIND == 0 && v < c.nrep) write_ene_hist(P, c, v);
+    if (lam_thread) {
+      LamStep L{};
+      lam_begin(P, c, v, L, shk);
+      lam_save(P, v, L);
+    }
+    if (!(shk || STOP)) return;
+    if (quad) {
+      const QLane q = ql_make(P, c, v);
+      q_fetch(P, q, S, tid, true);
+      const double ke = q_cano1<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep));
+      q_spill(P, c, q, S, tid, FP64);
+      add_kin_quad(P, c.nsub_total, 0, q.sub, ke);
+    } else {
+      double ke = 0.0;
+      int sub = -1;
+      if (small) {
+        const Unit u = P.units[P.small_idx[v]];
+        sub = u.sub;
+        ke = cano1_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
+      }
+      add_kin(P, c.nsub_total, 0, sub, ke);
+    }
+  } else if (PH == PH_UPDATE) {
+    if (lam_thread) {
+      LamStep L;
+      lam_load(P, v, L);
+      lam_advance(P, c, v, L, tt, shk);
+      lam_save(P, v, L);
+    }
+    double w[kCom];
+    if (quad) {
       const QLane q = ql_make(P, c, v);
       q_fetch(P, q, S, tid, false);
       const double chi = q.grp ? sqrt(tt / sub_temp(P, c, 0, q.sub)) : 1.0;
@@ -1833,7 +2023,7 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
     } else {
       double ke = 0.0;
       int sub = -1, rep = -1;
-      if (v < c.nsmall) {
+      if (small) {
         const Unit u = P.units[P.small_idx[v]];
         cano2_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), tt);
         if (split) {
@@ -1846,268 +2036,120 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_fused(DevPtrs P, IntConst 
       if (split) com_add(P, c, 0, rep, w);
       else if (shk) add_kin(P, c.nsub_total, 1, sub, ke);
     }
-  }
-  if (split) {
-    if (!grid_barrier(P, epoch)) return;
-    for (int base = 0; base < nv; base += nthr) {   // the correction, then phase 3
-      const int v = base + gt;
-      if (RESIDENT) {
-        if (quad) {
-          fix_quad(P, c, 0, Q, S, tid);
-          add_kin_quad(P, c.nsub_total, 1, Q.sub, q_cano3(P, c, Q, S, tid));
-        } else {
-          double ke = 0.0;
-          if (small) {
-            fix_small(P, c, 0, U, S, tid, shk);
-            if (shk) ke = ru_cano3(P, c, U, S, tid);
-          }
-          if (shk) add_kin(P, c.nsub_total, 1, small ? U.sub : -1, ke);
-        }
-      } else if (v >= c.qbase) {
-        const QLane q = ql_make(P, c, v);
-        q_fetch(P, q, S, tid, false);
-        fix_quad(P, c, 0, q, S, tid);
-        const double ke = q_cano3(P, c, q, S, tid);
-        q_spill(P, c, q, S, tid, FP64);
-        add_kin_quad(P, c.nsub_total, 1, q.sub, ke);
-      } else {
-        double ke = 0.0;
-        int sub = -1;
-        if (v < c.nsmall) {
-          const Unit u = P.units[P.small_idx[v]];
-          fix_unit(P, c, 0, u, shk, FP64);
+  } else if (PH == PH_FIX) {
+    // after phase 2 (it = 0, every replica) or after phase 5 of pass it
+    if (it > 0 && !any_active(P, c, it, tt, s_act)) return;
+    const int ks = it == 0 ? 1 : 2 * it + 1;
+    if (quad) {
+      const QLane q = ql_make(P, c, v);
+      const bool act = it == 0 || (q.grp && rep_active(P, c, s_act, q.rep, it, tt));
+      q_fetch(P, q, S, tid, false);
+      if (act) fix_quad(P, c, it, q, S, tid);
+      const double ke = q_cano3(P, c, q, S, tid);
+      if (act) q_spill(P, c, q, S, tid, FP64);
+      add_kin_quad(P, c.nsub_total, ks, act ? q.sub : -1, act ? ke : 0.0);
+    } else {
+      double ke = 0.0;
+      int sub = -1;
+      if (small) {
+        const Unit u = P.units[P.small_idx[v]];
+        if (it == 0 || rep_active(P, c, s_act, u.rep, it, tt)) {
+          fix_unit(P, c, it, u, shk, FP64);
           if (shk) {
             sub = u.sub;
             ke = cano3_unit<FP64>(P, c, u);
           }
         }
-        if (shk) add_kin(P, c.nsub_total, 1, sub, ke);
       }
+      if (shk) add_kin(P, c.nsub_total, ks, sub, ke);
     }
-  }
-  if (shk) {
-    for (int it = 1; it < c.icslop; ++it) {
-      if (!grid_barrier(P, epoch)) return;
-      if (!any_active(P, c, it, tt, s_act)) break;
-      // lambda's velocity stays (v_back + v)/2 through the loop (verlethe.f90:529)
-      const bool lam_act = lam_thread && rep_active(P, c, s_act, gt, it, tt);
-      if (lam_act) {
-        lam_add_ke(P, c, P.reps[gt], 2 * it, L.lvt);
-        lam_add_ke(P, c, P.reps[gt], 2 * it + 1, L.lvt);
-      }
-      // phase 4 (verlethe.f90:625-640)
-      for (int base = 0; base < nv; base += nthr) {
-        const int v = base + gt;
-        if (RESIDENT) {
-          if (quad) {
-            const bool act = Q.grp && rep_active(P, c, s_act, Q.rep, it, tt);
-            const double ke = q_cano4<FP64>(P, c, Q, S, tid, s);
-            add_kin_quad(P, c.nsub_total, 2 * it, act ? Q.sub : -1, act ? ke : 0.0);
-          } else {
-            const bool act = small && rep_active(P, c, s_act, U.rep, it, tt);
-            const double ke = act ? ru_cano4<FP64>(P, c, U, S, tid, s) : 0.0;
-            add_kin(P, c.nsub_total, 2 * it, act ? U.sub : -1, ke);
-          }
-        } else if (v >= c.qbase) {
-          const QLane q = ql_make(P, c, v);
-          const bool act = q.grp && rep_active(P, c, s_act, q.rep, it, tt);
-          q_fetch(P, q, S, tid, false);
-          const double ke = q_cano4<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep));
-          if (act) q_spill(P, c, q, S, tid, FP64);
-          add_kin_quad(P, c.nsub_total, 2 * it, act ? q.sub : -1, act ? ke : 0.0);
-        } else {
-          double ke = 0.0;
-          int sub = -1;
-          if (v < c.nsmall) {
-            const Unit u = P.units[P.small_idx[v]];
-            if (rep_active(P, c, s_act, u.rep, it, tt)) {
-              sub = u.sub;
-              ke = cano4_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
-            }
-          }
-          add_kin(P, c.nsub_total, 2 * it, sub, ke);
-        }
-      }
-      if (!grid_barrier(P, epoch)) return;
-      // phase 5 (verlethe.f90:641-718) + phase 3 of the next SHAKE pass; with the
-      // centre-of-mass stop: phase 5 and the sums (com slot it), barrier, correction + phase 3
-      if (split) {
-        for (int base = 0; base < nv; base += nthr) {
-          const int v = base + gt;
-          double w[kCom];
-          int rep = -1;
-          if (RESIDENT) {
-            if (!quad) {
-              if (small && rep_active(P, c, s_act, U.rep, it, tt)) {
-                ru_cano5<FP64>(P, c, U, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, U.sub)));
-                rep = com_small(P, c, U, S, tid, w);
-              }
-            } else if (Q.grp && rep_active(P, c, s_act, Q.rep, it, tt)) {
-              q_cano5<FP64>(P, c, Q, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, Q.sub)));
-              rep = com_quad(P, c, Q, S, tid, w);
-            }
-          } else if (v >= c.qbase) {
-            const QLane q = ql_make(P, c, v);
-            if (q.grp && rep_active(P, c, s_act, q.rep, it, tt)) {
-              q_fetch(P, q, S, tid, false);
-              q_cano5<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep), sqrt(tt / sub_temp(P, c, 2 * it, q.sub)));
-              rep = com_quad(P, c, q, S, tid, w);
-              q_spill(P, c, q, S, tid, FP64);
-            }
-          } else if (v < c.nsmall) {
-            const Unit u = P.units[P.small_idx[v]];
-            if (rep_active(P, c, s_act, u.rep, it, tt)) {
-              cano5_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
-              rep = com_unit(P, c, u, w);
-            }
-          }
-          com_add(P, c, it, rep, w);
-        }
-        if (!grid_barrier(P, epoch)) return;
-      }
-      for (int base = 0; base < nv; base += nthr) {
-        const int v = base + gt;
-        if (split) {   // the correction, then phase 3 (phase 5 ran above)
-          if (RESIDENT) {
-            if (!quad) {
-              const bool act = small && rep_active(P, c, s_act, U.rep, it, tt);
-              double ke = 0.0;
-              if (act) {
-                fix_small(P, c, it, U, S, tid, shk);
-                ke = ru_cano3(P, c, U, S, tid);
-              }
-              add_kin(P, c.nsub_total, 2 * it + 1, act ? U.sub : -1, ke);
-            } else {
-              const bool act = Q.grp && rep_active(P, c, s_act, Q.rep, it, tt);
-              double sx[3], sdx[3];
-#pragma unroll
-              for (int k = 0; k < 3; ++k) { sx[k] = S.x[k][tid]; sdx[k] = S.dxs[k][tid]; }
-              if (act) fix_quad(P, c, it, Q, S, tid);
-              const double ke = q_cano3(P, c, Q, S, tid);
-              if (!act && Q.a >= 0) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k) { S.x[k][tid] = sx[k]; S.dxs[k][tid] = sdx[k]; }
-              }
-              add_kin_quad(P, c.nsub_total, 2 * it + 1, act ? Q.sub : -1, act ? ke : 0.0);
-            }
-          } else if (v >= c.qbase) {
-            const QLane q = ql_make(P, c, v);
-            const bool act = q.grp && rep_active(P, c, s_act, q.rep, it, tt);
-            q_fetch(P, q, S, tid, false);
-            if (act) fix_quad(P, c, it, q, S, tid);
-            const double ke = q_cano3(P, c, q, S, tid);
-            if (act) q_spill(P, c, q, S, tid, FP64);
-            add_kin_quad(P, c.nsub_total, 2 * it + 1, act ? q.sub : -1, act ? ke : 0.0);
-          } else {
-            double ke = 0.0;
-            int sub = -1;
-            if (v < c.nsmall) {
-              const Unit u = P.units[P.small_idx[v]];
-              if (rep_active(P, c, s_act, u.rep, it, tt)) {
-                fix_unit(P, c, it, u, shk, FP64);
-                sub = u.sub;
-                ke = cano3_unit<FP64>(P, c, u);
-              }
-            }
-            add_kin(P, c.nsub_total, 2 * it + 1, sub, ke);
-          }
-          continue;
-        }
-        if (RESIDENT) {
-          if (!quad) {
-            const bool act = small && rep_active(P, c, s_act, U.rep, it, tt);
-            double ke = 0.0;
-            if (act) {
-              ru_cano5<FP64>(P, c, U, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, U.sub)));
-              ke = ru_cano3(P, c, U, S, tid);
-            }
-            add_kin(P, c.nsub_total, 2 * it + 1, act ? U.sub : -1, ke);
-          } else {
-            // the whole warp runs the SHAKE (its shuffles); inactive groups keep their state
-            const bool act = Q.grp && rep_active(P, c, s_act, Q.rep, it, tt);
-            double sx[3], sdx[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) { sx[k] = S.x[k][tid]; sdx[k] = S.dxs[k][tid]; }
-            if (act) q_cano5<FP64>(P, c, Q, S, tid, s, sqrt(tt / sub_temp(P, c, 2 * it, Q.sub)));
-            const double ke = q_cano3(P, c, Q, S, tid);
-            if (!act && Q.a >= 0) {
-#pragma unroll
-              for (int k = 0; k < 3; ++k) { S.x[k][tid] = sx[k]; S.dxs[k][tid] = sdx[k]; }
-            }
-            add_kin_quad(P, c.nsub_total, 2 * it + 1, act ? Q.sub : -1, act ? ke : 0.0);
-          }
-        } else if (v >= c.qbase) {
-          const QLane q = ql_make(P, c, v);
-          const bool act = q.grp && rep_active(P, c, s_act, q.rep, it, tt);
-          q_fetch(P, q, S, tid, false);
-          if (act) q_cano5<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep),
-                                 sqrt(tt / sub_temp(P, c, 2 * it, q.sub)));
-          const double ke = q_cano3(P, c, q, S, tid);
-          if (act) q_spill(P, c, q, S, tid, FP64);
-          add_kin_quad(P, c.nsub_total, 2 * it + 1, act ? q.sub : -1, act ? ke : 0.0);
-        } else {
-          double ke = 0.0;
-          int sub = -1;
-          if (v < c.nsmall) {
-            const Unit u = P.units[P.small_idx[v]];
-            if (rep_active(P, c, s_act, u.rep, it, tt)) {
-              cano5_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
-              sub = u.sub;
-              ke = cano3_unit<FP64>(P, c, u);
-            }
-          }
-          add_kin(P, c.nsub_total, 2 * it + 1, sub, ke);
-        }
-      }
+  } else if (PH == PH_CORR) {
+    if (!any_active(P, c, it, tt, s_act)) return;
+    // lambda's velocity stays (v_back + v)/2 through the loop (verlethe.f90:529)
+    if (lam_thread && rep_active(P, c, s_act, v, it, tt)) {
+      LamStep L;
+      lam_load(P, v, L);
+      lam_add_ke(P, c, P.reps[v], 2 * it, L.lvt);
+      lam_add_ke(P, c, P.reps[v], 2 * it + 1, L.lvt);
     }
-  }
-  if (RESIDENT) {   // the lane's new state back to memory
-    if (small) {
-      bool bad = false;
-      const double ri = 1.0 / c.dt;
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        if (q < U.n) {
-          const int a = U.a[q];
-          double xq[3];
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            const int i = 3 * q + k;
-            xq[k] = S.x[i][tid];
-            P.x[3 * a + k] = xq[k];
-            P.v[3 * a + k] = shk ? (xq[k] - S.x0[i][tid]) * ri : S.dxs[i][tid];
-            bad |= !isfinite(xq[k]);
-          }
-          write_slot(P, a, xq, FP64);
-        }
-      }
-      if (bad) atomicOr(P.status, ERR_NONFINITE);
-#pragma unroll
-      for (int q = 0; q < 3; ++q)
-        if (q < U.n) zero_force<FP64>(P, U.a[q]);
-    } else if (quad) {
-      q_spill(P, c, Q, S, tid, FP64);
-      if (Q.a >= 0) zero_force<FP64>(P, Q.a);
-    }
-  } else {   // grid-stride form: each thread clears the atoms of the lanes it ran
-    for (int base = 0; base < nv; base += nthr) {
-      const int v = base + gt;
-      if (v >= c.qbase) {
-        if (v < c.nvirt) {
-          const QLane q = ql_make(P, c, v);
-          if (q.a >= 0) zero_force<FP64>(P, q.a);
-        }
-      } else if (v < c.nsmall) {
+    if (quad) {
+      const QLane q = ql_make(P, c, v);
+      const bool act = q.grp && rep_active(P, c, s_act, q.rep, it, tt);
+      q_fetch(P, q, S, tid, false);
+      const double ke = q_cano4<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep));
+      if (act) q_spill(P, c, q, S, tid, FP64);
+      add_kin_quad(P, c.nsub_total, 2 * it, act ? q.sub : -1, act ? ke : 0.0);
+    } else {
+      double ke = 0.0;
+      int sub = -1;
+      if (small) {
         const Unit u = P.units[P.small_idx[v]];
-        JP_UNIT_LOOP(q) zero_force<FP64>(P, u.a[q]);
+        if (rep_active(P, c, s_act, u.rep, it, tt)) {
+          sub = u.sub;
+          ke = cano4_unit<FP64>(P, c, u, rep_scale(P, c, u.rep));
+        }
       }
+      add_kin(P, c.nsub_total, 2 * it, sub, ke);
     }
+  } else if (PH == PH_RESCALE) {
+    if (!any_active(P, c, it, tt, s_act)) return;
+    if (split) {
+      double w[kCom];
+      int rep = -1;
+      if (quad) {
+        const QLane q = ql_make(P, c, v);
+        if (q.grp && rep_active(P, c, s_act, q.rep, it, tt)) {
+          q_fetch(P, q, S, tid, false);
+          q_cano5<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep), sqrt(tt / sub_temp(P, c, 2 * it, q.sub)));
+          rep = com_quad(P, c, q, S, tid, w);
+          q_spill(P, c, q, S, tid, FP64);
+        }
+      } else if (small) {
+        const Unit u = P.units[P.small_idx[v]];
+        if (rep_active(P, c, s_act, u.rep, it, tt)) {
+          cano5_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
+          rep = com_unit(P, c, u, w);
+        }
+      }
+      com_add(P, c, it, rep, w);
+    } else if (quad) {
+      const QLane q = ql_make(P, c, v);
+      const bool act = q.grp && rep_active(P, c, s_act, q.rep, it, tt);
+      q_fetch(P, q, S, tid, false);
+      if (act)
+        q_cano5<FP64>(P, c, q, S, tid, rep_scale(P, c, q.rep), sqrt(tt / sub_temp(P, c, 2 * it, q.sub)));
+      const double ke = q_cano3(P, c, q, S, tid);   // the whole warp runs the SHAKE shuffles
+      if (act) q_spill(P, c, q, S, tid, FP64);
+      add_kin_quad(P, c.nsub_total, 2 * it + 1, act ? q.sub : -1, act ? ke : 0.0);
+    } else {
+      double ke = 0.0;
+      int sub = -1;
+      if (small) {
+        const Unit u = P.units[P.small_idx[v]];
+        if (rep_active(P, c, s_act, u.rep, it, tt)) {
+          cano5_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
+          sub = u.sub;
+          ke = cano3_unit<FP64>(P, c, u);
+        }
+      }
+      add_kin(P, c.nsub_total, 2 * it + 1, sub, ke);
+    }
+  } else {   // PH_END
+    if (quad) {
+      const QLane q = ql_make(P, c, v);
+      if (q.a >= 0) zero_force<FP64>(P, q.a);
+    } else if (small) {
+      const Unit u = P.units[P.small_idx[v]];
+      JP_UNIT_LOOP(q) zero_force<FP64>(P, u.a[q]);
+    }
+    if (lam_thread) {
+      LamStep L;
+      lam_load(P, v, L);
+      P.lam[2 * v] = L.lam;
+      P.lam[2 * v + 1] = L.lv;
+    }
+    finish_last(P, c, tt);
   }
-  if (lam_thread) {
-    P.lam[2 * gt] = L.lam;
-    P.lam[2 * gt + 1] = L.lv;
-  }
-  finish_last(P, c, tt);
 }
 
 // ---- standalone SHAKE (test hook): r1 constrained against r2, positions in xback / x0 -----
@@ -2143,20 +2185,16 @@ static int coop_grid(K kernel, int device) {
 }
 
 int cano_grid(bool fp64, int device) {
-  // the smallest co-resident grid among the integration kernels of this precision
+  // the smallest co-resident grid among the cooperative integration kernels of this precision
   int g;
   if (fp64) {
-    g = coop_grid(k_cano_fused<true, true, false>, device);
-    g = std::min(g, coop_grid(k_cano_fused<true, false, false>, device));
-    g = std::min(g, coop_grid(k_cano_fused<true, true, true>, device));
-    g = std::min(g, coop_grid(k_cano_fused<true, false, true>, device));
+    g = coop_grid(k_cano_fused<true, false>, device);
+    g = std::min(g, coop_grid(k_cano_fused<true, true>, device));
     g = std::min(g, coop_grid(k_micr_fused<true, false>, device));
     g = std::min(g, coop_grid(k_micr_fused<true, true>, device));
   } else {
-    g = coop_grid(k_cano_fused<false, true, false>, device);
-    g = std::min(g, coop_grid(k_cano_fused<false, false, false>, device));
-    g = std::min(g, coop_grid(k_cano_fused<false, true, true>, device));
-    g = std::min(g, coop_grid(k_cano_fused<false, false, true>, device));
+    g = coop_grid(k_cano_fused<false, false>, device);
+    g = std::min(g, coop_grid(k_cano_fused<false, true>, device));
     g = std::min(g, coop_grid(k_micr_fused<false, false>, device));
     g = std::min(g, coop_grid(k_micr_fused<false, true>, device));
   }
@@ -2178,26 +2216,81 @@ static void coop_launch(void (*kernel)(Args...), int grid, cudaStream_t st, Args
   cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
+// does a CANO/GE step of this system take the per-phase launches (more virtual lanes than
+// the cooperative grid holds)?
+static bool cano_streaming(const IntConst& c, int grid_max) {
+  if (c.method <= JP_METHOD_MICR) return false;
+  const int want = std::max(1, (c.nvirt + kIntThreads - 1) / kIntThreads);
+  return want > grid_max;
+}
+
+// one phase: the unit lanes (and per-replica threads), then the 4-atom group lanes
+template <bool FP64, bool STOP, int PH>
+static void launch_phase(const DevPtrs& P, const IntConst& c, int it, cudaStream_t st) {
+  const int g0 = (std::max(c.nsmall, c.nrep) + kIntThreads - 1) / kIntThreads;
+  const int g1 = (c.nvirt - c.qbase + kIntThreads - 1) / kIntThreads;
+  k_cano_phase<FP64, STOP, PH, 0><<<g0, kIntThreads, 0, st>>>(P, c, it);
+  if (g1 > 0) k_cano_phase<FP64, STOP, PH, 1><<<g1, kIntThreads, 0, st>>>(P, c, it);
+}
+
+template <bool FP64, bool STOP>
+static void launch_cano_phases(const DevPtrs& P, const IntConst& c, cudaStream_t st) {
+  const bool shk = c.shake_method != JP_SHAKE_NONE;
+  launch_phase<FP64, STOP, PH_BEGIN>(P, c, 0, st);
+  launch_phase<FP64, STOP, PH_UPDATE>(P, c, 0, st);
+  if (STOP) launch_phase<FP64, STOP, PH_FIX>(P, c, 0, st);
+  if (shk) {
+    for (int it = 1; it < c.icslop; ++it) {
+      launch_phase<FP64, STOP, PH_CORR>(P, c, it, st);
+      launch_phase<FP64, STOP, PH_RESCALE>(P, c, it, st);
+      if (STOP) launch_phase<FP64, STOP, PH_FIX>(P, c, it, st);
+    }
+  }
+  const int grid = (std::max(c.nvirt, c.nrep) + kIntThreads - 1) / kIntThreads;
+  k_cano_phase<FP64, STOP, PH_END, 2><<<grid, kIntThreads, 0, st>>>(P, c, 0);
+}
+
+int integrate_launches(const IntConst& c, int grid_max) {
+  if (!cano_streaming(c, grid_max)) return 1;
+  const bool stop = c.stop != 0, shk = c.shake_method != JP_SHAKE_NONE;
+  int phases = 2 + (stop ? 1 : 0);
+  if (shk) phases += std::max(0, c.icslop - 1) * (stop ? 3 : 2);
+  int n = phases * (c.nvirt > c.qbase ? 2 : 1) + 1;            // + PH_END
+  if (c.method == JP_METHOD_GE && !c.ge_prescaled) n += 1;   // k_ge_scale
+  return n;
+}
+
 void launch_integrate(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
                       cudaStream_t st) {
   // bar, the kinetic sums and the centre-of-mass sums are zero here: created so, and reset
   // by the last block of the previous integration (or by the host after an error)
   const bool verlet = c.method <= JP_METHOD_MICR;   // MICR or CONS
-  const int lanes = verlet ? nunit : c.nvirt;
-  const int want = std::max(1, (lanes + kIntThreads - 1) / kIntThreads);
-  const int grid = std::min(want, grid_max);
-  const bool resident = want <= grid_max;
   const bool stop = c.stop != 0;
   if (verlet) {
+    const int want = std::max(1, (nunit + kIntThreads - 1) / kIntThreads);
+    const int grid = std::min(want, grid_max);
     const bool split = stop || c.method == JP_METHOD_CONS;
     if (fp64) coop_launch(split ? k_micr_fused<true, true> : k_micr_fused<true, false>, grid, st, P, c, nunit);
     else coop_launch(split ? k_micr_fused<false, true> : k_micr_fused<false, false>, grid, st, P, c, nunit);
-  } else if (resident) {
-    if (fp64) coop_launch(stop ? k_cano_fused<true, true, true> : k_cano_fused<true, true, false>, grid, st, P, c, nunit);
-    else coop_launch(stop ? k_cano_fused<false, true, true> : k_cano_fused<false, true, false>, grid, st, P, c, nunit);
+  } else if (!cano_streaming(c, grid_max)) {
+    const int grid = std::max(1, (c.nvirt + kIntThreads - 1) / kIntThreads);
+    if (fp64) coop_launch(stop ? k_cano_fused<true, true> : k_cano_fused<true, false>, grid, st, P, c);
+    else coop_launch(stop ? k_cano_fused<false, true> : k_cano_fused<false, false>, grid, st, P, c);
   } else {
-    if (fp64) coop_launch(stop ? k_cano_fused<true, false, true> : k_cano_fused<true, false, false>, grid, st, P, c, nunit);
-    else coop_launch(stop ? k_cano_fused<false, false, true> : k_cano_fused<false, false, false>, grid, st, P, c, nunit);
+    // every lane of every phase reads the replica's force scale: McMD polynomials are
+    // evaluated once per replica beforehand
+    IntConst cs = c;
+    if (c.method == JP_METHOD_GE && !c.ge_prescaled) {
+      launch_ge_scale(P, c, st);
+      cs.ge_prescaled = 1;
+    }
+    if (fp64) {
+      if (stop) launch_cano_phases<true, true>(P, cs, st);
+      else launch_cano_phases<true, false>(P, cs, st);
+    } else {
+      if (stop) launch_cano_phases<false, true>(P, cs, st);
+      else launch_cano_phases<false, false>(P, cs, st);
+    }
   }
 }
 

@@ -97,10 +97,12 @@ struct IntConst {
                            // not its last)
 };
 int cano_grid(bool fp64, int device);   // co-resident blocks of the integration kernels
-// one cooperative launch: energies of the step, force scale, verlet (MICR) or verlethe
-// (CANO/GE) with SHAKE, temperatures and step counters
+// energies of the step, force scale, verlet (MICR) or verlethe (CANO/GE) with SHAKE,
+// temperatures and step counters: one cooperative launch, or for a CANO/GE system with more
+// virtual lanes than the cooperative grid (grid_max blocks) holds, one launch per phase
 void launch_integrate(const DevPtrs& P, const IntConst& c, int nunit, bool fp64, int grid_max,
                       cudaStream_t st);
+int integrate_launches(const IntConst& c, int grid_max);   // kernels launch_integrate launches
 void launch_shake_only(const DevPtrs& P, const IntConst& c, int unit0, int nunit, cudaStream_t st);
 // per-replica force scale of this step (McMD polynomial or surrogate network) into P.scale
 void launch_ge_scale(const DevPtrs& P, const IntConst& c, cudaStream_t st);

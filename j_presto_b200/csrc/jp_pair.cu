@@ -15,8 +15,8 @@
 // rotate one lane per step through warp shuffles, so after 32 steps each is back in the lane
 // of its entry.  Newton's third law: each unordered pair is evaluated once.
 //
-// Warps take tiles one at a time from a global counter, so all finish together whatever
-// their tiles hold.
+// Warps take short runs of consecutive tiles from a global counter, so all finish together
+// whatever their tiles hold.
 // Mixed path: FP32 pair arithmetic on block-local coordinates (|x| < ~30 A), every step of a
 // tile branch-free (a pair outside the mask or the cut-off contributes an exact zero);
 // forces summed per tile in FP32, energies in FP32 over 8 steps then in FP64, both added as
@@ -326,10 +326,21 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
   unsigned phase = 0u, pend = 0u;   // per buffer: barrier parity to wait for; copy in flight
   bool ok = true;
 
+  // tiles are claimed in runs of `run` consecutive ones: the tiles of an i block are
+  // consecutive, so a run mostly keeps its i atoms (no reload, no i-force flush between
+  // tiles); the run is short enough that every warp still gets several (8 per warp at most
+  // of the total, 1 to 16 tiles)
+  const int run = max(1, min(16, T / (int)(gridDim.x * kPairWarps * 8)));
+  int run_next = 0, run_end = 0;
   auto claim = [&]() {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(P.tile_ctr, 1);
-    return __shfl_sync(full, t, 0);
+    if (run_next >= run_end) {
+      int t = 0;
+      if (lane == 0) t = atomicAdd(P.tile_ctr, run);
+      t = __shfl_sync(full, t, 0);
+      run_next = t;
+      run_end = min(t + run, T);
+    }
+    return run_next < run_end ? run_next++ : T;
   };
   auto issue = [&](int t, int b) {
     if (lane == 0) {

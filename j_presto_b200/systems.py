@@ -679,11 +679,13 @@ def config_c4(nrep=64, seed=4, small=False, workers=None):
     return [_c4_one(j) for j in jobs]
 
 
-def alsd_replica(top, ncluster=4, seed=0):
+def alsd_replica(top, ncluster=4, seed=0, walls=20.0):
     """A copy of a solvated chain set up for ALSD (CLSTMETHOD= LMD, METHOD= GE): the atoms
     of `ncluster` residues drawn from the seed form the lambda-scaled cluster (whole SHAKE
     groups, as residue lists give them), and the weight in lambda is linear on [0.6, 1.0]
-    (d lnP/dlambda = 40 - 30 lambda) with walls of slope 20 outside."""
+    (d lnP/dlambda = 40 - 30 lambda) with restoring walls of slope `walls` outside (lower
+    -walls, upper +walls: below celw d lnP/dlambda falls, above ceup it rises, and the force
+    on lambda, -dE/dlambda - R T d lnP/dlambda, points back into the range)."""
     rng = np.random.default_rng(seed)
     t = dict(top)
     cl = np.zeros(t["natom"], np.int32)
@@ -694,8 +696,8 @@ def alsd_replica(top, ncluster=4, seed=0):
             cl[g[:na]] = 1
     t["cluster"] = cl
     t["ge"] = dict(coef=np.array([[40.0, -30.0]]), low=np.array([0.0]), high=np.array([2.0]),
-                   alphalw=0.0, alphaup=0.0, celw=0.6, ceup=1.0, tempce=300.0, lower=20.0,
-                   upper=20.0)
+                   alphalw=0.0, alphaup=0.0, celw=0.6, ceup=1.0, tempce=300.0, lower=-float(walls),
+                   upper=float(walls))
     return t
 
 

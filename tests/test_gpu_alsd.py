@@ -60,13 +60,17 @@ def test_alsd_energy_grad_vs_oracle(eng_mod, clustered, mode):
     np.testing.assert_allclose(eco.sum(), eo[0], rtol=1e-10)
 
 
-@pytest.mark.parametrize("method,tempco,tc,mode", [
-    (abi.JP_METHOD_GE, 1, 1, abi.JP_ALSD_LMD),
-    (abi.JP_METHOD_GE, 2, 1, abi.JP_ALSD_LMD),
-    (abi.JP_METHOD_GE, 2, 0, abi.JP_ALSD_LMD2),
-    (abi.JP_METHOD_CANO, 1, 0, abi.JP_ALSD_LMD),
+@pytest.mark.parametrize("method,tempco,tc,mode,grid", [
+    (abi.JP_METHOD_GE, 1, 1, abi.JP_ALSD_LMD, 0),
+    (abi.JP_METHOD_GE, 2, 1, abi.JP_ALSD_LMD, 0),
+    (abi.JP_METHOD_GE, 2, 0, abi.JP_ALSD_LMD2, 0),
+    (abi.JP_METHOD_CANO, 1, 0, abi.JP_ALSD_LMD, 0),
+    # per-phase launches (forced by a two-block cooperative grid): lambda's state of the
+    # step is carried between the launches
+    (abi.JP_METHOD_GE, 2, 1, abi.JP_ALSD_LMD, 2),
+    (abi.JP_METHOD_GE, 1, 0, abi.JP_ALSD_LMD2, 2),
 ])
-def test_alsd_trajectory_vs_oracle(eng_mod, clustered, method, tempco, tc, mode):
+def test_alsd_trajectory_vs_oracle(eng_mod, clustered, method, tempco, tc, mode, grid):
     kw = dict(method=method, alsd=mode, lambda0=0.8, scale_terms=abi.JP_SCALE_TORS, tempco=tempco,
               lambda_temp_control=tc)
     o = oracle.Oracle(clustered, **kw)
@@ -75,6 +79,8 @@ def test_alsd_trajectory_vs_oracle(eng_mod, clustered, method, tempco, tc, mode)
     xo, _ = o.get_state()
     lo, _ = o.get_lambda()
     with eng_mod.Engine(clustered, precision=FP64, **kw) as e:
+        if grid:
+            e.set_grid_limit(grid)
         E, T = e.step(15)
         x, _ = e.get_state()
         l2, _ = e.get_lambda()

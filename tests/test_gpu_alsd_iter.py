@@ -19,6 +19,7 @@ pytestmark = pytest.mark.gpu
 
 KW = dict(method=abi.JP_METHOD_GE, alsd=abi.JP_ALSD_LMD, lambda0=0.81, scale_terms=abi.JP_SCALE_TORS)
 LMIN, LMAX, NBIN, NBOR = 0.6, 1.0, 20, 2
+WALL = 20000.0
 
 
 @pytest.fixture(scope="module")
@@ -27,7 +28,12 @@ def eng_mod(engine_lib):
 
 
 def _reps(n):
-    return [systems.alsd_replica(systems.solvated_polymer(4, 500, seed=31 + r), seed=r) for r in range(n)]
+    # walls that hold lambda near [0.6, 1.0]: the cluster's solvation force
+    # (-2 lambda E_AA - E_AB, some 300 kcal/mol) drives lambda past a weak wall until the
+    # trajectory fails (the oracle shows the same); with slope 20000 the oracle keeps lambda
+    # in [0.90, 1.09] over 1500 steps for these four seeds
+    return [systems.alsd_replica(systems.solvated_polymer(4, 500, seed=31 + r), seed=r, walls=WALL)
+            for r in range(n)]
 
 
 def test_histogram_records_the_step(eng_mod):
@@ -82,7 +88,7 @@ def test_one_iteration_polynomial_and_network(eng_mod):
     # the next weight spans the lambda range the runs sampled (a polynomial is not
     # extrapolated), with steep walls outside it
     seen = d["EE"][d["P"] > 0]
-    nf, _, _ = geprep.alsd_fit(d, float(seen.min()), float(seen.max()), 300.0, 1, 2, 200.0, 200.0)
+    nf, _, _ = geprep.alsd_fit(d, float(seen.min()), float(seen.max()), 300.0, 1, 2, WALL, WALL)
     X = np.concatenate([geprep.alsd_net_data(h[2], h[3], lo, hi, LMIN, LMAX, NBIN, NBOR, 300.0)[0]
                         for h in hist])
     Y = np.concatenate([geprep.alsd_net_data(h[2], h[3], lo, hi, LMIN, LMAX, NBIN, NBOR, 300.0)[1]

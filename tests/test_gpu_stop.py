@@ -1,6 +1,7 @@
 """Centre-of-mass stop (STOPCE, remotv) and METHOD= CONS (Berendsen, scalet) on the GPU
-against the oracle, in both forms of the CANO/GE integrator: register/shared-memory resident
-(the default at these sizes) and grid-stride (forced by a small integration grid).
+against the oracle, in both forms of the CANO/GE integrator: one cooperative launch with the
+unit state on chip (the default at these sizes) and one launch per phase (the form of
+systems with more lanes than the cooperative grid holds, forced by a small grid limit).
 
 Tolerances as the other parity tests: 15-step FP64 trajectories within 1e-8 A of the
 oracle; the mixed path's stopped momentum and angular momentum within 1e-9 of the
@@ -63,11 +64,16 @@ def test_stop_natom_vs_oracle(eng_mod, poly):
     _parity(eng_mod, poly, method=CANO, stop_center=BOTH, stop_natom=40)
 
 
-@pytest.mark.parametrize("stop", [NONE, BOTH])
-def test_grid_stride_form_vs_oracle(eng_mod, poly, stop):
-    """Two blocks for a few thousand lanes: every phase loops over the lanes with the unit
-    state in the atom arrays, 4-atom groups included."""
-    _parity(eng_mod, poly, grid=2, method=CANO, stop_center=stop, tempco=2)
+@pytest.mark.parametrize("method,stop,tempco", [(CANO, NONE, 2), (CANO, BOTH, 2), (GE, TR, 1), (GE, NONE, 2)])
+def test_per_phase_form_vs_oracle(eng_mod, poly, method, stop, tempco):
+    """A two-block cooperative grid for a few thousand lanes: the step runs as one launch per
+    phase with the unit state in the atom arrays between them, 4-atom groups included (GE:
+    the McMD force scale evaluated per replica before the phases)."""
+    _parity(eng_mod, poly, grid=2, method=method, stop_center=stop, tempco=tempco)
+
+
+def test_per_phase_form_without_shake_vs_oracle(eng_mod, poly):
+    _parity(eng_mod, poly, grid=2, method=CANO, stop_center=BOTH, shake_method=abi.JP_SHAKE_NONE)
 
 
 def test_mixed_path_stops_the_molecule(eng_mod, poly):
