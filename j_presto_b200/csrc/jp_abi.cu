@@ -186,11 +186,12 @@ void enqueue_rebuild(jp_ctx *c) {
     ncmm = 3 + std::max(0, c->cmm_nlev - 1);
   }
   k_cell_key<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
-  scan_exclusive(P.hist, P.hist_scan, c->nkeys + 1, c->scan_scratch, nullptr, st);
+  int nl = 10;   // the single kernels below
+  nl += scan_exclusive(P.hist, P.hist_scan, c->nkeys + 1, c->scan_scratch, nullptr, st);
   k_scatter<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
   k_sort_bins<<<(c->nkeys + nt - 1) / nt, nt, 0, st>>>(P, c->nkeys);
   k_col_count<<<(c->ncol + nt - 1) / nt, nt, 0, st>>>(P, c->ncol);
-  scan_exclusive(P.col_nb, P.col_blk, c->ncol + 1, c->scan_scratch, nullptr, st);
+  nl += scan_exclusive(P.col_nb, P.col_blk, c->ncol + 1, c->scan_scratch, nullptr, st);
   k_clear_slots<<<(c->nslot + nt - 1) / nt, nt, 0, st>>>(P, c->nslot, c->zc.nt1 - 1);
   k_fill_slots<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
   k_excl_slots<<<(c->natom + nt - 1) / nt, nt, 0, st>>>(P, c->natom);
@@ -200,12 +201,12 @@ void enqueue_rebuild(jp_ctx *c) {
   const double rc = c->prm.cutoff;
   const int nwb = (c->nchunk * 32 + 127) / 128;
   launch_tile_scan(P, c->nchunk, rlim * rlim, (float)rlim, rc * rc, c->cmm, st);
-  scan_exclusive(P.chunk_cnt, P.chunk_off, c->nchunk + 1, c->scan_scratch, P.ntiles, st);
-  scan_exclusive(P.chunk_ent, P.chunk_eoff, c->nchunk + 1, c->scan_scratch, nullptr, st);
+  nl += scan_exclusive(P.chunk_cnt, P.chunk_off, c->nchunk + 1, c->scan_scratch, P.ntiles, st);
+  nl += scan_exclusive(P.chunk_ent, P.chunk_eoff, c->nchunk + 1, c->scan_scratch, nullptr, st);
   k_tile_emit<<<nwb, 128, 0, st>>>(P, c->nchunk, c->cmm ? 1 : 0);
-  launch_compact_tiles(P, c->nblk, c->nsm, c->cmm, c->scan_scratch, st);
+  nl += launch_compact_tiles(P, c->nblk, c->nsm, c->cmm, c->scan_scratch, st);
   if (c->hbond) launch_hb_list(P, c->hb_cap, c->zc.nt1, c->nblk, st);
-  c->launches_rebuild = 28 + (c->fp64 ? 1 : 0) + ncmm + (c->hbond ? 1 : 0);
+  c->launches_rebuild = nl + (c->fp64 ? 1 : 0) + ncmm + (c->hbond ? 1 : 0);
 }
 
 // ---- one MD step ------------------------------------------------------------------------

@@ -261,22 +261,31 @@ struct IStage {
 // d^2 is good to ~3e-4 A^2), and a tile with any pair within `band` of rlim^2 is redone by
 // tile_mask_fast in FP64; the FP32 mask is returned only where every decision is certain,
 // so the list is the FP64 list.  `unsure` is warp-uniform.
+// A j atom in the i frame is its block-local position (pos_f, relative to its block's
+// reference in the wrapped frame) plus block bj's reference shifted by the tiles' image into
+// the i block's frame.  Only the i atoms within the list radius of block bj's bounding box
+// (with a margin of 1e-4 rlim^2 + 1e-3 A^2, far wider than `band` and the FP32 rounding) can
+// list a pair; the rows of the others are certainly empty, and the loop skips them.
 __device__ __forceinline__ unsigned tile_row_f32(const DevPtrs& P, const Rep& R, int bi, int bj, int lane,
                                                  const IStage& S, float rlim2f, float band, bool& unsure) {
   const int aj = P.satom[bj * kTile + lane];
-  float r[3] = {0.f, 0.f, 0.f};
-  if (aj >= 0) {
-    for (int k = 0; k < 3; ++k) {
-      const double x = P.x[3 * aj + k];
-      const double n = anint((P.blk_ref[3 * bi + k] - P.blk_ref[3 * bj + k]) * R.invbox[k]);
-      const double w = (x - R.box[k] * floor(x * R.invbox[k])) + R.box[k] * n;
-      r[k] = (float)(w - P.blk_ref[3 * bi + k]);
-    }
+  float cj[3];   // block bj's reference (its bounding-box centre) in the i block's frame
+  for (int k = 0; k < 3; ++k) {
+    const double d = P.blk_ref[3 * bi + k] - P.blk_ref[3 * bj + k];
+    cj[k] = (float)(R.box[k] * anint(d * R.invbox[k]) - d);
   }
+  const float4 pj = P.pos_f[bj * kTile + lane];
+  const float r[3] = {pj.x + cj[0], pj.y + cj[1], pj.z + cj[2]};
+  const float4 hj = P.blk_half[bj];
+  const float gx = fmaxf(fabsf(S.xf[lane] - cj[0]) - hj.x, 0.f);
+  const float gy = fmaxf(fabsf(S.yf[lane] - cj[1]) - hj.y, 0.f);
+  const float gz = fmaxf(fabsf(S.zf[lane] - cj[2]) - hj.z, 0.f);
+  unsigned live = __ballot_sync(0xffffffffu, fmaf(gx, gx, fmaf(gy, gy, gz * gz)) <= rlim2f * 1.0001f + 1e-3f);
   unsigned row = 0;
   bool u = false;
-#pragma unroll 8
-  for (int i = 0; i < kTile; ++i) {
+  while (live) {   // warp-uniform
+    const int i = __ffs(live) - 1;
+    live &= live - 1;
     const float dx = S.xf[i] - r[0], dy = S.yf[i] - r[1], dz = S.zf[i] - r[2];
     const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     const bool in = aj >= 0 && d2 <= rlim2f;
@@ -590,13 +599,14 @@ __global__ void k_ct_emit(DevPtrs P, int cmm) {
   }
 }
 
-void launch_compact_tiles(const DevPtrs& P, int nblk, int nsm, bool cmm, int* scan_scratch,
-                          cudaStream_t st) {
+int launch_compact_tiles(const DevPtrs& P, int nblk, int nsm, bool cmm, int* scan_scratch,
+                         cudaStream_t st) {
   const int nb = (nblk + 127) / 128;
   k_ct_count<<<nb, 128, 0, st>>>(P, nblk);
-  scan_exclusive(P.ct_cnt, P.ct_off, nblk + 1, scan_scratch, P.nctiles, st);
+  const int ns = scan_exclusive(P.ct_cnt, P.ct_off, nblk + 1, scan_scratch, P.nctiles, st);
   k_ct_index<<<nsm * 4, 256, 0, st>>>(P);
   k_ct_emit<<<nsm * 8, 256, 0, st>>>(P, cmm ? 1 : 0);
+  return 3 + ns;
 }
 
 // ---- deterministic exclusive scan (3 passes) --------------------------------------------
@@ -653,11 +663,53 @@ __global__ void k_scan_final(const int* in, int n, const int* bsum, int* out, in
   if (i == n - 1 && total) *total = bsum[blockIdx.x] + sh[threadIdx.x];
 }
 
-void scan_exclusive(const int* in, int* out, int n, int* scratch, int* total, cudaStream_t st) {
+// one block for up to kScanOneMax values: thread t sums its run of consecutive values, the
+// 1024 run sums are scanned with warp shuffles, and each thread writes its run's prefixes
+constexpr int kScanOneMax = 1 << 16;
+
+__global__ void __launch_bounds__(1024) k_scan_one(const int* in, int n, int* out, int* total) {
+  __shared__ int wsum[32];
+  const unsigned full = 0xffffffffu;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const int per = (n + 1023) / 1024;
+  const int b = min(t * per, n), e = min(b + per, n);
+  int s = 0;
+  for (int i = b; i < e; ++i) s += in[i];
+  int x = s;   // inclusive scan of the run sums: within the warp, then over the warps
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(full, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int w = wsum[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(full, w, o);
+      if (lane >= o) w += y;
+    }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  int run = x - s + (wid > 0 ? wsum[wid - 1] : 0);
+  for (int i = b; i < e; ++i) {
+    const int v = in[i];
+    out[i] = run;
+    run += v;
+  }
+  if (t == 0 && total) *total = wsum[31];
+}
+
+int scan_exclusive(const int* in, int* out, int n, int* scratch, int* total, cudaStream_t st) {
+  if (n <= kScanOneMax) {
+    k_scan_one<<<1, 1024, 0, st>>>(in, n, out, total);
+    return 1;
+  }
   int nb = (n + 1023) / 1024;
   k_scan_block_sums<<<nb, 1024, 0, st>>>(in, n, scratch);
   k_scan_small<<<1, 1024, 0, st>>>(scratch, nb);
   k_scan_final<<<nb, 1024, 0, st>>>(in, n, scratch, out, total);
+  return 3;
 }
 
 }  // namespace jp
