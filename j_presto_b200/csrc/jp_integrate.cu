@@ -21,6 +21,8 @@ constexpr int kCom = 16;   // centre-of-mass stop sums per replica and slot
 // unrolled with a guard: the per-unit arrays then live in registers.  (A runtime trip count
 // over these small local arrays produced wrong values on sm_100a with nvcc 12.9.)
 #define JP_UNIT_LOOP(q) _Pragma("unroll") for (int q = 0; q < 4; ++q) if (q < u.n)
+// the same over a 1-3 atom unit (the units of the small lanes: 4-atom groups take eight lanes)
+#define JP_SMALL_LOOP(q) _Pragma("unroll") for (int q = 0; q < 3; ++q) if (q < u.n)
 
 __host__ __device__ __forceinline__ void mimg(const Rep& R, double* d) {
   for (int k = 0; k < 3; ++k) d[k] -= R.box[k] * anint(d[k] * R.invbox[k]);
@@ -1111,6 +1113,90 @@ __device__ __forceinline__ void cano5_unit(const DevPtrs& P, const IntConst& c, 
   }
 }
 
+// The SHAKE pass after a velocity update of a 1-3 atom unit, on positions still in registers: x1 (the updated
+// positions) is written to xback, constrained against x0, and becomes x with v = (x1 - x0)/dt;
+// returns the kinetic term of (vb + v)/2, vb = v(t - dt/2).  As phase 3 (cano3_unit) reading
+// x, x0 and vback back from the atom arrays.
+template <bool FP64>
+__device__ __forceinline__ double shake_finish_unit(const DevPtrs& P, const IntConst& c, const Unit& u,
+                                                    const double* im, double (*x1)[3],
+                                                    const double (*x0)[3], const double (*vb)[3]) {
+  JP_SMALL_LOOP(q)
+    for (int k = 0; k < 3; ++k) P.xback[3 * u.a[q] + k] = x1[q][k];
+  if (u.n >= 2) {
+    const int ier = shake_small(P.reps[u.rep], u.n, u.d2, im, x1, x0, c.shake_method, c.shake_tol,
+                                c.shake_maxit);
+    if (ier) shake_status(P, ier, u.rep);
+  }
+  const double ri = 1.0 / c.dt;
+  bool bad = false;
+  double ke = 0.0;
+  JP_SMALL_LOOP(q) {
+    const int a = u.a[q];
+    double vv = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const double v = (x1[q][k] - x0[q][k]) * ri;
+      P.v[3 * a + k] = v;
+      P.x[3 * a + k] = x1[q][k];
+      const double vt = 0.5 * (vb[q][k] + v);
+      vv += vt * vt;
+      bad |= !isfinite(x1[q][k]);
+    }
+    ke += P.mass[a] * vv;
+    write_slot(P, a, x1[q], FP64);
+  }
+  if (bad) atomicOr(P.status, ERR_NONFINITE);
+  return ke;
+}
+
+// phase 2 then phase 3 with SHAKE and no centre-of-mass stop (the form of cano2_unit followed
+// by cano3_unit): phase 1 left x0 = x and vback = v, so both come from one read of x and v
+template <bool FP64>
+__device__ __forceinline__ double cano23_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
+                                              double tt) {
+  const double chi = sqrt(tt / sub_temp(P, c, 0, u.sub));
+  const double a1 = chi * c.dt * kConvcv, b1 = 2.0 * chi - 1.0;
+  double x1[3][3], x0[3][3], vb[3][3], im[3];
+  JP_SMALL_LOOP(q) {
+    const int a = u.a[q];
+    double g[3];
+    load_grad<FP64>(P, a, s, g);
+    im[q] = P.imass[a];
+    for (int k = 0; k < 3; ++k) {
+      const int i = 3 * a + k;
+      vb[q][k] = P.v[i];
+      x0[q][k] = P.x[i];
+      const double v = b1 * vb[q][k] - a1 * g[k] * im[q];
+      x1[q][k] = x0[q][k] + c.dt * v;
+      P.forcec[i] = 0.0;
+    }
+  }
+  return shake_finish_unit<FP64>(P, c, u, im, x1, x0, vb);
+}
+
+// phase 5 then phase 3 (cano5_unit followed by cano3_unit), no centre-of-mass stop
+template <bool FP64>
+__device__ __forceinline__ double cano53_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
+                                              int it, double tt) {
+  const double chi = sqrt(tt / sub_temp(P, c, 2 * it, u.sub));
+  const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
+  double x1[3][3], x0[3][3], vb[3][3], im[3];
+  JP_SMALL_LOOP(q) {
+    const int a = u.a[q];
+    double g[3];
+    load_grad<FP64>(P, a, s, g);
+    im[q] = P.imass[a];
+    for (int k = 0; k < 3; ++k) {
+      const int i = 3 * a + k;
+      vb[q][k] = P.vback[i];
+      x0[q][k] = P.x0[i];
+      const double v = (-kConvcv * g[k] * im[q] + P.forcec[i]) * a1 + vb[q][k] * b1;
+      x1[q][k] = x0[q][k] + c.dt * v;
+    }
+  }
+  return shake_finish_unit<FP64>(P, c, u, im, x1, x0, vb);
+}
+
 // Resident form: a 1-3 atom unit keeps its state through every phase of the step on chip:
 // positions x, x0, v(t-dt/2), forcec and the shift of the last SHAKE pass in shared memory
 // (component-major, 9 values per state per thread), scalars in registers.  v(t+dt/2) is
@@ -1943,6 +2029,9 @@ enum : int {
   PH_END = 5        // forces cleared, lambda stored, temperatures and step counters
 };
 
+// blocks per SM the unit-lane launches are compiled for (their registers: 65,536 / (64 x this))
+constexpr int kPhaseBlocks = 8;
+
 // shared-memory state of the 4-atom group lanes of a launch (component 0-2)
 struct QuadSmem {
   double x[3][kIntThreads], x0[3][kIntThreads], vb[3][kIntThreads];
@@ -1963,7 +2052,7 @@ __device__ __forceinline__ void lam_load(const DevPtrs& P, int r, LamStep& L) {
 // lambda); KIND 1: the 4-atom group lanes [qbase, nvirt) (a launch of its own, as their
 // SHAKE needs several times the registers); KIND 2 (PH_END only): every lane.
 template <bool FP64, bool STOP, int PH, int KIND>
-__global__ void __launch_bounds__(kIntThreads) k_cano_phase(DevPtrs P, IntConst c, int it) {
+__global__ void __launch_bounds__(kIntThreads, KIND == 1 ? 4 : kPhaseBlocks) k_cano_phase(DevPtrs P, IntConst c, int it) {
   __shared__ QuadSmem S;
   __shared__ unsigned char s_act[kActCache];
   const int v = (KIND == 1 ? c.qbase : 0) + blockIdx.x * blockDim.x + threadIdx.x;
@@ -2025,12 +2114,12 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_phase(DevPtrs P, IntConst 
       int sub = -1, rep = -1;
       if (small) {
         const Unit u = P.units[P.small_idx[v]];
-        cano2_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), tt);
-        if (split) {
-          rep = com_unit(P, c, u, w);
-        } else if (shk) {
+        if (split || !shk) {
+          cano2_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), tt);
+          if (split) rep = com_unit(P, c, u, w);
+        } else {
           sub = u.sub;
-          ke = cano3_unit<FP64>(P, c, u);
+          ke = cano23_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), tt);
         }
       }
       if (split) com_add(P, c, 0, rep, w);
@@ -2127,9 +2216,8 @@ __global__ void __launch_bounds__(kIntThreads) k_cano_phase(DevPtrs P, IntConst 
       if (small) {
         const Unit u = P.units[P.small_idx[v]];
         if (rep_active(P, c, s_act, u.rep, it, tt)) {
-          cano5_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
           sub = u.sub;
-          ke = cano3_unit<FP64>(P, c, u);
+          ke = cano53_unit<FP64>(P, c, u, rep_scale(P, c, u.rep), it, tt);
         }
       }
       add_kin(P, c.nsub_total, 2 * it + 1, sub, ke);
