@@ -399,6 +399,13 @@ __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk,
       S.zf[lane] = ai >= 0 ? (float)(S.z[lane] - P.blk_ref[3 * bi + 2]) : 1.0e18f;
       __syncwarp();
     }
+    // the FP32 mask's uncertainty band: every coordinate tile_row_f32 works with is below
+    // M = rlim + 3 h_max in magnitude (h_max: the replica's largest block half extent) and
+    // carries at most 2.5 roundings of 2^-24 M, a difference one more, so |error of d^2| <=
+    // 2 sqrt(3) rlim 5 2^-24 M + 3 2^-24 rlim^2; pairs within 4 times that of rlim^2 are
+    // decided in FP64 (about 1.5e-3 A^2 for water blocks at rc = 12 A)
+    const float hm = fmaxf(P.rep_hmax[3 * rep], fmaxf(P.rep_hmax[3 * rep + 1], P.rep_hmax[3 * rep + 2]));
+    const float band = 4.f * 5.9604645e-8f * (17.33f * rlimf * (rlimf + 3.f * hm) + 3.f * rlimf * rlimf);
     while (ball) {
       const int b = __ffs(ball) - 1;
       ball &= ball - 1;
@@ -406,7 +413,7 @@ __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk,
       unsigned m;
       bool unsure = true;
       if (fast) {
-        unsigned row = tile_row_f32(P, R, bi, j0 + b, lane, S, rlim2f, 4.0e-3f, unsure);
+        unsigned row = tile_row_f32(P, R, bi, j0 + b, lane, S, rlim2f, band, unsure);
         if (!unsure) {
           if (ai < 0) row = 0;
           m = finish_mask(P, bi, j0 + b, lane, row, ps, pb, pe);
@@ -550,49 +557,76 @@ __device__ __forceinline__ unsigned compress_bits(unsigned x, unsigned m) {
 
 // One warp per compact tile: lane i's row collects, from each tile whose entries fall in
 // the compact tile's 32 slots, the bits of that tile's row i at its occupied j lanes
-// (packed in lane order); lane p writes slot p's entry.
+// (packed in lane order); lane p writes slot p's entry.  Those source tiles are consecutive
+// from ct_src and at most 32 (each holds at least one entry and the first covers slot 0), so
+// lane q reads source tile q's offset, occupancy, j block and image shift in one coalesced
+// pass, the mask rows are read four tiles at a time, and each slot's entry comes from its
+// tile's lane by shuffles: no load waits on another.
 __global__ void k_ct_emit(DevPtrs P, int cmm) {
+  const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const int T = *P.nctiles;
   for (int ct = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ct < T; ct += nw) {
     const int b = P.ct_blk[ct];
-    const int c0 = P.blk_chunk0[b];
-    const int e0 = P.chunk_eoff[c0], e1 = P.chunk_eoff[P.blk_chunk0[b + 1]];
-    const int t1 = P.chunk_off[P.blk_chunk0[b + 1]];
-    const int s0 = e0 + 32 * (ct - P.ct_off[b]);
-    unsigned cur = 0u, cur_el = 0u;
-    float4 ent = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-    for (int t = P.ct_src[ct]; t < t1; ++t) {
-      const int base = P.tile_eoff[t] - s0;   // slot of the tile's first entry (may be < 0)
-      if (base >= 32) break;
-      const unsigned occ = P.tile_occ[t];
-      const int n = __popc(occ);
-      if (base + n <= 0) continue;
-      const unsigned m = P.masks[(size_t)t * 32 + lane];
-      const unsigned row = __funnelshift_l(m, m, lane);
-      unsigned row_el = 0u;
-      if (cmm) {
-        const unsigned me = P.masks_el[(size_t)t * 32 + lane];
-        row_el = __funnelshift_l(me, me, lane);
-      }
-      const unsigned comp = compress_bits(row, occ);   // the row's bits at the occupied lanes
-      const unsigned comp_el = cmm ? compress_bits(row_el, occ) : 0u;
-      if (base >= 0) {
-        cur |= comp << base;
-        cur_el |= comp_el << base;
-      } else {
-        cur |= comp >> -base;
-        cur_el |= comp_el >> -base;
-      }
-      const int k = lane - base;   // this lane's slot, as the tile's k-th entry
-      if (k >= 0 && k < n) {
-        const float4 sh = P.tile_shift[t];
-        const int slot = P.tiles[t].y * kTile + (int)__fns(occ, 0, k + 1);
-        ent = make_float4(sh.x, sh.y, sh.z, __int_as_float(slot));
+    const int c1 = P.blk_chunk0[b + 1];
+    const int e1 = P.chunk_eoff[c1];
+    const int t1 = P.chunk_off[c1];
+    const int s0 = P.chunk_eoff[P.blk_chunk0[b]] + 32 * (ct - P.ct_off[b]);
+    const int ts = P.ct_src[ct];
+    const int tq = ts + lane;   // lane q: source tile q
+    int qb = 32, qy = 0;
+    unsigned qocc = 0u;
+    float4 qsh = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (tq < t1) {
+      qb = P.tile_eoff[tq] - s0;   // slot of the tile's first entry (may be < 0)
+      if (qb < 32) {
+        qocc = P.tile_occ[tq];
+        qy = P.tiles[tq].y;
+        qsh = P.tile_shift[tq];
       }
     }
-    if (s0 + lane >= e1) ent = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    const int nt = __popc(__ballot_sync(full, tq < t1 && qb < 32));   // lanes 0 .. nt-1
+    unsigned cur = 0u, cur_el = 0u;
+    int src = -1, kk = 0;   // this slot's source tile and its rank among the tile's entries
+    for (int j0 = 0; j0 < nt; j0 += 4) {   // warp-uniform
+      unsigned m[4], me[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        m[u] = j0 + u < nt ? P.masks[(size_t)(ts + j0 + u) * 32 + lane] : 0u;
+        me[u] = cmm && j0 + u < nt ? P.masks_el[(size_t)(ts + j0 + u) * 32 + lane] : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int j = j0 + u;
+        const int base = __shfl_sync(full, qb, j & 31);
+        const unsigned occ = __shfl_sync(full, qocc, j & 31);
+        if (j >= nt) break;
+        const int n = __popc(occ);
+        const unsigned comp = compress_bits(__funnelshift_l(m[u], m[u], lane), occ);
+        const unsigned comp_el = cmm ? compress_bits(__funnelshift_l(me[u], me[u], lane), occ) : 0u;
+        if (base >= 0) {
+          cur |= comp << base;
+          cur_el |= comp_el << base;
+        } else {
+          cur |= comp >> -base;
+          cur_el |= comp_el >> -base;
+        }
+        const int k = lane - base;
+        if (k >= 0 && k < n) {
+          src = j;
+          kk = k;
+        }
+      }
+    }
+    const int sy = __shfl_sync(full, qy, src & 31);
+    const unsigned socc = __shfl_sync(full, qocc, src & 31);
+    const float shx = __shfl_sync(full, qsh.x, src & 31);
+    const float shy = __shfl_sync(full, qsh.y, src & 31);
+    const float shz = __shfl_sync(full, qsh.z, src & 31);
+    float4 ent = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+    if (src >= 0 && s0 + lane < e1)
+      ent = make_float4(shx, shy, shz, __int_as_float(sy * kTile + (int)__fns(socc, 0, kk + 1)));
     P.ct_j[(size_t)ct * 32 + lane] = ent;
     P.ct_mask[(size_t)ct * 32 + lane] = __funnelshift_r(cur, cur, lane);
     if (cmm) P.ct_mask_el[(size_t)ct * 32 + lane] = __funnelshift_r(cur_el, cur_el, lane);
@@ -665,7 +699,7 @@ __global__ void k_scan_final(const int* in, int n, const int* bsum, int* out, in
 
 // one block for up to kScanOneMax values: thread t sums its run of consecutive values, the
 // 1024 run sums are scanned with warp shuffles, and each thread writes its run's prefixes
-constexpr int kScanOneMax = 1 << 16;
+constexpr int kScanOneMax = 1 << 13;   // above it the three-pass scan is faster
 
 __global__ void __launch_bounds__(1024) k_scan_one(const int* in, int n, int* out, int* total) {
   __shared__ int wsum[32];

@@ -36,11 +36,13 @@ def test_measured_flatness_decides(eng_mod):
         # the lattice start releases some 5000 kcal/mol over its first thousand steps:
         # minimise (200 iterations: with SHAKE the step length of a longer descent vanishes,
         # JP_E_MIN_STEP) and run 800 steps first (on the oracle the energy then stays within
-        # +-100 kcal/mol), and centre the weight's range on the energy reached
+        # +-100 kcal/mol); the weight's range starts just below the energy reached, where its
+        # temperature ramp (280 K at the bottom, 700 K at the top) is near the 300 K the
+        # system has, so the McMD walk starts inside the range and explores upwards
         e.minimize(warn_ok=True, max_loop=200)
         e.step(800, energies=False, temps=False)
         e1 = [e.energy_grad(r)[0][0] for r in range(4)]
-        w0 = [systems.mcmd_weight(x - 300.0, x + 300.0) for x in e1]
+        w0 = [systems.mcmd_weight(x - 200.0, x + 1500.0) for x in e1]
         for r in range(4):
             e.ge_set(w0[r], r)
             e.ge_hist_setup(w0[r]["celw"], w0[r]["ceup"], NBIN, NBOR, rep=r)
