@@ -981,27 +981,63 @@ __global__ void __launch_bounds__(64) k_micr_fused(DevPtrs P, IntConst c, int nu
 
 // ---- METHOD= CANO / GE: verlethe.f90 ----------------------------------------------------
 // Streaming form of a 1-3 atom unit: its state lives in the atom arrays between phases (the
-// per-phase launches below; 4-atom groups take the eight-lane form further down).
+// per-phase launches below; 4-atom groups take the eight-lane form further down).  Each
+// function reads everything it needs of the unit's atoms before it writes anything: the atom
+// arrays are separate pointers that the compiler must assume may overlap, so a store placed
+// between two loads holds the later load back until the store's own inputs have arrived, and
+// a unit would wait for memory once per atom component instead of once.
+
+// an atom's slot record, read ahead of the position update that rewrites it (write_slot)
+struct SlotRef {
+  int s;
+  float w;          // the mixed path's scaled charge (pos_f.w)
+  double o[3];      // the mixed path's block frame origin of the slot
+  double w64;       // the FP64 path's scaled charge (pos_d.w)
+};
+
+template <bool FP64>
+__device__ __forceinline__ void slot_load(const DevPtrs& P, int a, SlotRef& r) {
+  r.s = P.slot_of[a];
+  if (FP64) {
+    r.w64 = P.pos_d[r.s].w;
+  } else {
+    r.w = P.pos_f[r.s].w;
+    for (int k = 0; k < 3; ++k) r.o[k] = P.off[3 * r.s + k];
+  }
+}
+
+template <bool FP64>
+__device__ __forceinline__ void slot_store(const DevPtrs& P, const SlotRef& r, const double* x) {
+  if (FP64) P.pos_d[r.s] = make_double4(x[0], x[1], x[2], r.w64);
+  else P.pos_f[r.s] = make_float4((float)(x[0] - r.o[0]), (float)(x[1] - r.o[1]), (float)(x[2] - r.o[2]), r.w);
+}
 
 // phase 1 (verlethe.f90:380-398): back up x, v; velt = v - dt/2 c g/m; KE(velt) -> slot 0
 template <bool FP64>
 __device__ __forceinline__ double cano1_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s) {
   const double rt = 0.5 * c.dt * kConvcv;
-  double ke = 0.0;
-  JP_UNIT_LOOP(q) {
+  double g[3][3], v[3][3], x[3][3], im[3], m[3];
+  JP_SMALL_LOOP(q) {
     const int a = u.a[q];
-    double g[3];
-    load_grad<FP64>(P, a, s, g);
-    const double im = P.imass[a];
+    load_grad<FP64>(P, a, s, g[q]);
+    im[q] = P.imass[a];
+    m[q] = P.mass[a];
+    for (int k = 0; k < 3; ++k) {
+      v[q][k] = P.v[3 * a + k];
+      x[q][k] = P.x[3 * a + k];
+    }
+  }
+  double ke = 0.0;
+  JP_SMALL_LOOP(q) {
+    const int a = u.a[q];
     double vv = 0.0;
     for (int k = 0; k < 3; ++k) {
-      const double v = P.v[3 * a + k];
-      P.x0[3 * a + k] = P.x[3 * a + k];
-      P.vback[3 * a + k] = v;
-      const double vt = v - rt * g[k] * im;
+      P.x0[3 * a + k] = x[q][k];
+      P.vback[3 * a + k] = v[q][k];
+      const double vt = v[q][k] - rt * g[q][k] * im[q];
       vv += vt * vt;
     }
-    ke += P.mass[a] * vv;
+    ke += m[q] * vv;
   }
   return ke;
 }
@@ -1009,118 +1045,44 @@ __device__ __forceinline__ double cano1_unit(const DevPtrs& P, const IntConst& c
 // phase 2 (verlethe.f90:400-516): chi from slot 0; v = (2chi-1)v - chi dt c g/m; x += dt v
 template <bool FP64>
 __device__ __forceinline__ void cano2_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
-                                        double tt) {
-  double tempc = c.temp;
-  if (c.shake_method != JP_SHAKE_NONE) tempc = sub_temp(P, c, 0, u.sub);
+                                           double tt) {
+  const bool shk = c.shake_method != JP_SHAKE_NONE;
+  const double tempc = shk ? sub_temp(P, c, 0, u.sub) : c.temp;
   const double chi = sqrt(tt / tempc);
   const double a1 = chi * c.dt * kConvcv, b1 = 2.0 * chi - 1.0;
-  JP_UNIT_LOOP(q) {
+  double g[3][3], v[3][3], x[3][3], im[3];
+  SlotRef sl[3];
+  JP_SMALL_LOOP(q) {
     const int a = u.a[q];
-    double g[3];
-    load_grad<FP64>(P, a, s, g);
-    const double im = P.imass[a];
-    for (int k = 0; k < 3; ++k) {
-      const double v = b1 * P.v[3 * a + k] - a1 * g[k] * im;
-      P.v[3 * a + k] = v;
-      P.x[3 * a + k] += c.dt * v;
-      P.forcec[3 * a + k] = 0.0;
-    }
-    if (c.shake_method == JP_SHAKE_NONE) write_slot(P, a, P.x + 3 * a, FP64);
-  }
-}
-
-// phase 3 of an iteration (verlethe.f90:524-612): SHAKE, v = (x-x0)/dt,
-// velt = (vback+v)/2, KE(velt)
-template <bool FP64>
-__device__ __forceinline__ double cano3_unit(const DevPtrs& P, const IntConst& c, const Unit& u) {
-  const Rep& R = P.reps[u.rep];
-  double x1[4][3], x0[4][3], im[4];
-  JP_UNIT_LOOP(q) {
-    const int a = u.a[q];
+    load_grad<FP64>(P, a, s, g[q]);
     im[q] = P.imass[a];
     for (int k = 0; k < 3; ++k) {
-      x1[q][k] = P.x[3 * a + k];
-      x0[q][k] = P.x0[3 * a + k];
-      P.xback[3 * a + k] = x1[q][k];
+      v[q][k] = P.v[3 * a + k];
+      x[q][k] = P.x[3 * a + k];
     }
+    if (!shk) slot_load<FP64>(P, a, sl[q]);
   }
-  if (u.n >= 2) {   // 2-3 atoms: the register-array form
-    const int ier = shake_small(R, u.n, u.d2, im, x1, x0, c.shake_method, c.shake_tol, c.shake_maxit);
-    if (ier) shake_status(P, ier, u.rep);
-  }
-  const double ri = 1.0 / c.dt;
-  bool bad = false;
-  double ke = 0.0;
-  JP_UNIT_LOOP(q) {
+  JP_SMALL_LOOP(q) {
     const int a = u.a[q];
-    double vv = 0.0;
     for (int k = 0; k < 3; ++k) {
-      const double v = (x1[q][k] - x0[q][k]) * ri;
-      P.v[3 * a + k] = v;
-      P.x[3 * a + k] = x1[q][k];
-      const double vt = 0.5 * (P.vback[3 * a + k] + v);
-      vv += vt * vt;
-      bad |= !isfinite(x1[q][k]);
+      const double vn = b1 * v[q][k] - a1 * g[q][k] * im[q];
+      x[q][k] += c.dt * vn;
+      P.v[3 * a + k] = vn;
+      P.x[3 * a + k] = x[q][k];
+      P.forcec[3 * a + k] = 0.0;
     }
-    ke += P.mass[a] * vv;
-    write_slot(P, a, x1[q], FP64);
-  }
-  if (bad) atomicOr(P.status, ERR_NONFINITE);
-  return ke;
-}
-
-// phase 4 (verlethe.f90:625-640): forcec += (x - xback)/dt^2; velt; KE
-template <bool FP64>
-__device__ __forceinline__ double cano4_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s) {
-  const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
-  double ke = 0.0;
-  JP_UNIT_LOOP(q) {
-    const int a = u.a[q];
-    double g[3];
-    load_grad<FP64>(P, a, s, g);
-    const double im = P.imass[a];
-    double vv = 0.0;
-    for (int k = 0; k < 3; ++k) {
-      const int i = 3 * a + k;
-      const double fc = P.forcec[i] + r2 * (P.x[i] - P.xback[i]);
-      P.forcec[i] = fc;
-      const double vt = h * (-kConvcv * g[k] * im + fc) + P.vback[i];
-      vv += vt * vt;
-    }
-    ke += P.mass[a] * vv;
-  }
-  return ke;
-}
-
-// phase 5 (verlethe.f90:641-718): chi from slot 2*it; v = chi dt (-c g/m + forcec) +
-// (2chi-1) vback; x = x0 + dt v
-template <bool FP64>
-__device__ __forceinline__ void cano5_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
-                                        int it, double tt) {
-  const double chi = sqrt(tt / sub_temp(P, c, 2 * it, u.sub));
-  const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
-  JP_UNIT_LOOP(q) {
-    const int a = u.a[q];
-    double g[3];
-    load_grad<FP64>(P, a, s, g);
-    const double im = P.imass[a];
-    for (int k = 0; k < 3; ++k) {
-      const int i = 3 * a + k;
-      const double v = (-kConvcv * g[k] * im + P.forcec[i]) * a1 + P.vback[i] * b1;
-      P.v[i] = v;
-      P.x[i] = P.x0[i] + c.dt * v;
-    }
+    if (!shk) slot_store<FP64>(P, sl[q], x[q]);
   }
 }
 
-// The SHAKE pass after a velocity update of a 1-3 atom unit, on positions still in registers: x1 (the updated
-// positions) is written to xback, constrained against x0, and becomes x with v = (x1 - x0)/dt;
-// returns the kinetic term of (vb + v)/2, vb = v(t - dt/2).  As phase 3 (cano3_unit) reading
-// x, x0 and vback back from the atom arrays.
+// The SHAKE pass after a velocity update of a 1-3 atom unit, on positions in registers: x1
+// (the updated positions) is written to xback, constrained against x0, and becomes x with
+// v = (x1 - x0)/dt; returns the kinetic term of (vb + v)/2, vb = v(t - dt/2).
 template <bool FP64>
 __device__ __forceinline__ double shake_finish_unit(const DevPtrs& P, const IntConst& c, const Unit& u,
-                                                    const double* im, double (*x1)[3],
-                                                    const double (*x0)[3], const double (*vb)[3]) {
+                                                    const double* im, const double* m, const SlotRef* sl,
+                                                    double (*x1)[3], const double (*x0)[3],
+                                                    const double (*vb)[3]) {
   JP_SMALL_LOOP(q)
     for (int k = 0; k < 3; ++k) P.xback[3 * u.a[q] + k] = x1[q][k];
   if (u.n >= 2) {
@@ -1142,11 +1104,93 @@ __device__ __forceinline__ double shake_finish_unit(const DevPtrs& P, const IntC
       vv += vt * vt;
       bad |= !isfinite(x1[q][k]);
     }
-    ke += P.mass[a] * vv;
-    write_slot(P, a, x1[q], FP64);
+    ke += m[q] * vv;
+    slot_store<FP64>(P, sl[q], x1[q]);
   }
   if (bad) atomicOr(P.status, ERR_NONFINITE);
   return ke;
+}
+
+// phase 3 of an iteration (verlethe.f90:524-612): SHAKE, v = (x-x0)/dt,
+// velt = (vback+v)/2, KE(velt)
+template <bool FP64>
+__device__ __forceinline__ double cano3_unit(const DevPtrs& P, const IntConst& c, const Unit& u) {
+  double x1[3][3], x0[3][3], vb[3][3], im[3], m[3];
+  SlotRef sl[3];
+  JP_SMALL_LOOP(q) {
+    const int a = u.a[q];
+    im[q] = P.imass[a];
+    m[q] = P.mass[a];
+    for (int k = 0; k < 3; ++k) {
+      x1[q][k] = P.x[3 * a + k];
+      x0[q][k] = P.x0[3 * a + k];
+      vb[q][k] = P.vback[3 * a + k];
+    }
+    slot_load<FP64>(P, a, sl[q]);
+  }
+  return shake_finish_unit<FP64>(P, c, u, im, m, sl, x1, x0, vb);
+}
+
+// phase 4 (verlethe.f90:625-640): forcec += (x - xback)/dt^2; velt; KE
+template <bool FP64>
+__device__ __forceinline__ double cano4_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s) {
+  const double r2 = 1.0 / (c.dt * c.dt), h = 0.5 * c.dt;
+  double g[3][3], fc[3][3], x[3][3], xb[3][3], vb[3][3], im[3], m[3];
+  JP_SMALL_LOOP(q) {
+    const int a = u.a[q];
+    load_grad<FP64>(P, a, s, g[q]);
+    im[q] = P.imass[a];
+    m[q] = P.mass[a];
+    for (int k = 0; k < 3; ++k) {
+      const int i = 3 * a + k;
+      fc[q][k] = P.forcec[i];
+      x[q][k] = P.x[i];
+      xb[q][k] = P.xback[i];
+      vb[q][k] = P.vback[i];
+    }
+  }
+  double ke = 0.0;
+  JP_SMALL_LOOP(q) {
+    const int a = u.a[q];
+    double vv = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      const double f = fc[q][k] + r2 * (x[q][k] - xb[q][k]);
+      P.forcec[3 * a + k] = f;
+      const double vt = h * (-kConvcv * g[q][k] * im[q] + f) + vb[q][k];
+      vv += vt * vt;
+    }
+    ke += m[q] * vv;
+  }
+  return ke;
+}
+
+// phase 5 (verlethe.f90:641-718): chi from slot 2*it; v = chi dt (-c g/m + forcec) +
+// (2chi-1) vback; x = x0 + dt v
+template <bool FP64>
+__device__ __forceinline__ void cano5_unit(const DevPtrs& P, const IntConst& c, const Unit& u, double s,
+                                           int it, double tt) {
+  const double chi = sqrt(tt / sub_temp(P, c, 2 * it, u.sub));
+  const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
+  double g[3][3], fc[3][3], vb[3][3], x0[3][3], im[3];
+  JP_SMALL_LOOP(q) {
+    const int a = u.a[q];
+    load_grad<FP64>(P, a, s, g[q]);
+    im[q] = P.imass[a];
+    for (int k = 0; k < 3; ++k) {
+      const int i = 3 * a + k;
+      fc[q][k] = P.forcec[i];
+      vb[q][k] = P.vback[i];
+      x0[q][k] = P.x0[i];
+    }
+  }
+  JP_SMALL_LOOP(q) {
+    const int a = u.a[q];
+    for (int k = 0; k < 3; ++k) {
+      const double v = (-kConvcv * g[q][k] * im[q] + fc[q][k]) * a1 + vb[q][k] * b1;
+      P.v[3 * a + k] = v;
+      P.x[3 * a + k] = x0[q][k] + c.dt * v;
+    }
+  }
 }
 
 // phase 2 then phase 3 with SHAKE and no centre-of-mass stop (the form of cano2_unit followed
@@ -1156,22 +1200,26 @@ __device__ __forceinline__ double cano23_unit(const DevPtrs& P, const IntConst& 
                                               double tt) {
   const double chi = sqrt(tt / sub_temp(P, c, 0, u.sub));
   const double a1 = chi * c.dt * kConvcv, b1 = 2.0 * chi - 1.0;
-  double x1[3][3], x0[3][3], vb[3][3], im[3];
+  double x1[3][3], x0[3][3], vb[3][3], g[3][3], im[3], m[3];
+  SlotRef sl[3];
   JP_SMALL_LOOP(q) {
     const int a = u.a[q];
-    double g[3];
-    load_grad<FP64>(P, a, s, g);
+    load_grad<FP64>(P, a, s, g[q]);
     im[q] = P.imass[a];
+    m[q] = P.mass[a];
     for (int k = 0; k < 3; ++k) {
-      const int i = 3 * a + k;
-      vb[q][k] = P.v[i];
-      x0[q][k] = P.x[i];
-      const double v = b1 * vb[q][k] - a1 * g[k] * im[q];
-      x1[q][k] = x0[q][k] + c.dt * v;
-      P.forcec[i] = 0.0;
+      vb[q][k] = P.v[3 * a + k];
+      x0[q][k] = P.x[3 * a + k];
     }
+    slot_load<FP64>(P, a, sl[q]);
   }
-  return shake_finish_unit<FP64>(P, c, u, im, x1, x0, vb);
+  JP_SMALL_LOOP(q)
+    for (int k = 0; k < 3; ++k) {
+      const double v = b1 * vb[q][k] - a1 * g[q][k] * im[q];
+      x1[q][k] = x0[q][k] + c.dt * v;
+      P.forcec[3 * u.a[q] + k] = 0.0;
+    }
+  return shake_finish_unit<FP64>(P, c, u, im, m, sl, x1, x0, vb);
 }
 
 // phase 5 then phase 3 (cano5_unit followed by cano3_unit), no centre-of-mass stop
@@ -1180,21 +1228,27 @@ __device__ __forceinline__ double cano53_unit(const DevPtrs& P, const IntConst& 
                                               int it, double tt) {
   const double chi = sqrt(tt / sub_temp(P, c, 2 * it, u.sub));
   const double a1 = chi * c.dt, b1 = 2.0 * chi - 1.0;
-  double x1[3][3], x0[3][3], vb[3][3], im[3];
+  double x1[3][3], x0[3][3], vb[3][3], g[3][3], fc[3][3], im[3], m[3];
+  SlotRef sl[3];
   JP_SMALL_LOOP(q) {
     const int a = u.a[q];
-    double g[3];
-    load_grad<FP64>(P, a, s, g);
+    load_grad<FP64>(P, a, s, g[q]);
     im[q] = P.imass[a];
+    m[q] = P.mass[a];
     for (int k = 0; k < 3; ++k) {
       const int i = 3 * a + k;
       vb[q][k] = P.vback[i];
       x0[q][k] = P.x0[i];
-      const double v = (-kConvcv * g[k] * im[q] + P.forcec[i]) * a1 + vb[q][k] * b1;
+      fc[q][k] = P.forcec[i];
+    }
+    slot_load<FP64>(P, a, sl[q]);
+  }
+  JP_SMALL_LOOP(q)
+    for (int k = 0; k < 3; ++k) {
+      const double v = (-kConvcv * g[q][k] * im[q] + fc[q][k]) * a1 + vb[q][k] * b1;
       x1[q][k] = x0[q][k] + c.dt * v;
     }
-  }
-  return shake_finish_unit<FP64>(P, c, u, im, x1, x0, vb);
+  return shake_finish_unit<FP64>(P, c, u, im, m, sl, x1, x0, vb);
 }
 
 // Resident form: a 1-3 atom unit keeps its state through every phase of the step on chip:

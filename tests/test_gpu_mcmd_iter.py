@@ -50,8 +50,16 @@ def test_measured_flatness_decides(eng_mod):
         hist = [e.ge_hist_get(r) for r in range(4)]
         state = [e.get_state(r) for r in range(4)]
     assert all(h.sum() > 0 for h in hist)
-    its = [ge.iterate(hist[r], w0[r], w0[r]["celw"], w0[r]["ceup"], NBIN, NBOR, w0[r]["celw"],
-                      w0[r]["ceup"], 300.0, epochs=1500, seed=r) for r in range(4)]
+    # the next weight spans the energies the runs sampled (GEprep's next range: a polynomial
+    # is not extrapolated over a range without data), and its flatness is measured there
+    nxt = []
+    for r in range(4):
+        de = (w0[r]["ceup"] - w0[r]["celw"]) / NBIN
+        centres = w0[r]["celw"] + (np.arange(NBIN + 2 * NBOR) - NBOR + 0.5) * de
+        seen = centres[hist[r] > 0]
+        nxt.append((float(seen.min()), float(seen.max()) + de))
+    its = [ge.iterate(hist[r], w0[r], w0[r]["celw"], w0[r]["ceup"], NBIN, NBOR, nxt[r][0], nxt[r][1],
+                      300.0, epochs=1500, seed=r) for r in range(4)]
 
     def run(use_net):
         with eng_mod.Engine(tops, precision=abi.JP_PREC_MIXED, **kw) as e:
@@ -60,10 +68,10 @@ def test_measured_flatness_decides(eng_mod):
                 e.ge_set(its[r]["poly"], r)
                 if use_net:
                     e.ge_set_mlp(its[r]["mlp"], r)
-                e.ge_hist_setup(w0[r]["celw"], w0[r]["ceup"], NBIN, NBOR, rep=r)
+                e.ge_hist_setup(nxt[r][0], nxt[r][1], NBIN, NBOR, rep=r)
             e.rebuild()
             e.step(nsteps, energies=False, temps=False)
-            out = [_flat([e.ge_hist_get(r)], w0[r]["celw"], w0[r]["ceup"]) for r in range(4)]
+            out = [_flat([e.ge_hist_get(r)], nxt[r][0], nxt[r][1]) for r in range(4)]
         return out
 
     poly, net = run(False), run(True)
