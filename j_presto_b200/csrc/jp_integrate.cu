@@ -2083,8 +2083,9 @@ enum : int {
   PH_END = 5        // forces cleared, lambda stored, temperatures and step counters
 };
 
-// blocks per SM the unit-lane launches are compiled for (their registers: 65,536 / (64 x this))
-constexpr int kPhaseBlocks = 8;
+// blocks per SM the unit-lane launches are compiled for (their registers: 65,536 / (64 x this));
+// on C4 a bound of 8 (128 registers, with spills) measured 3 % slower than 4 (no spills)
+constexpr int kPhaseBlocks = 4;
 
 // shared-memory state of the 4-atom group lanes of a launch (component 0-2)
 struct QuadSmem {

@@ -139,6 +139,19 @@ __device__ __forceinline__ float rsqrt_ftz(float x) {
   return y;
 }
 
+// Nearest integer of v (ties to even, as rintf) for |v| < 2^22, on the FMA pipe: adding and
+// subtracting 1.5 * 2^23 rounds v at the unit place in round-to-nearest-even (the explicit
+// _rn adds are never contracted or reassociated).  The minimum-image multiples are a few
+// units at most.
+__device__ __forceinline__ float2 rint2(float2 v) {
+  const float2 m = make_float2(12582912.f, 12582912.f), nm = make_float2(-12582912.f, -12582912.f);
+  return __fadd2_rn(__fadd2_rn(v, m), nm);
+}
+
+__device__ __forceinline__ float rint1(float v) {
+  return __fadd_rn(__fadd_rn(v, 12582912.f), -12582912.f);
+}
+
 // One compact tile, two pairs per step in packed FP32x2 arithmetic (Blackwell's FFMA2 /
 // FADD2 / FMUL2): at step k (k < 16) lane l meets entries a = l + k and b = l + k + 16.  A
 // slot outside the mask or the cut-off takes rsqrt(1) and has its charge product and
@@ -177,9 +190,9 @@ __device__ __forceinline__ void tile_mixed2(const MixStage& S, const float2* __r
       float2 dy = __ffma2_rn(make_float2(a.z, a.w), m1, py);
       float2 dz = __ffma2_rn(make_float2(b.x, b.y), m1, pz);
       if (MINIMG) {
-        dx.x -= bx * rintf(dx.x * ibx); dx.y -= bx * rintf(dx.y * ibx);
-        dy.x -= by * rintf(dy.x * iby); dy.y -= by * rintf(dy.y * iby);
-        dz.x -= bz * rintf(dz.x * ibz); dz.y -= bz * rintf(dz.y * ibz);
+        dx = __ffma2_rn(make_float2(-bx, -bx), rint2(__fmul2_rn(dx, make_float2(ibx, ibx))), dx);
+        dy = __ffma2_rn(make_float2(-by, -by), rint2(__fmul2_rn(dy, make_float2(iby, iby))), dy);
+        dz = __ffma2_rn(make_float2(-bz, -bz), rint2(__fmul2_rn(dz, make_float2(ibz, ibz))), dz);
       }
       const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
       const bool ia = ((ma >> k) & 1u) && r2.x <= rc2;
@@ -257,9 +270,9 @@ __device__ __forceinline__ void tile_mixed(const MixStage& S, const float2* __re
       const int tjr = st[k];
       float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
       if (MINIMG) {
-        dx -= bx * rintf(dx * ibx);
-        dy -= by * rintf(dy * iby);
-        dz -= bz * rintf(dz * ibz);
+        dx = fmaf(-bx, rint1(dx * ibx), dx);
+        dy = fmaf(-by, rint1(dy * iby), dy);
+        dz = fmaf(-bz, rint1(dz * ibz), dz);
       }
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       const bool in = ((mk >> k) & 1u) && r2 <= rc2;
