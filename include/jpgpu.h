@@ -213,8 +213,9 @@ typedef struct jp_system {
   const double *shake_dist;    /* [nshake][6] target distances d0 in md_run pair order
                                   (1,2),(2,3),(3,1),(4,1),(3,4),(2,4) -- setshk.f90 redshk */
   const jp_ge *ge;             /* McMD weight for METHOD= GE; NULL otherwise */
-  const int32_t *cluster;      /* [natom] 1 = atom of the lambda-scaled cluster (CLUSTA
-                                  residues, inpcls.f90 icls = 1), else 0; NULL = none */
+  const int32_t *cluster;      /* [natom] 1 = atom of region A (CLUSTA, inpcls.f90 icls = 1:
+                                  the lambda-scaled cluster of ALSD), 2 = atom of region B
+                                  (CLUSTB; GEPSME= AND / OR / XOR only), else 0; NULL = none */
   const jp_ext_cmm *ext_cmm;   /* EXTCMM= environment (CAL15M= CMM only); NULL = none */
   /* Hydrogen-bond 10-12 term (md_run iyeflg(10), on when a type pair has iyppid = 2,
    * incel.f90:170-171; CAL15M= ZD and ATOM): a listed 1-5 pair whose types are marked
@@ -260,7 +261,7 @@ typedef struct jp_params {
    * (both / one / no atom in the cluster) enters the forces times lambda^2 / lambda / 1
    * (LMD) or lambda / sqrt(lambda) / 1 (LMD2); lambda moves under
    * f = -2 E_AA lambda - E_AB - dew (LMD), dew the McMD weight in lambda (METHOD= GE). */
-  int32_t alsd;          /* JP_ALSD_* */
+  int32_t alsd;          /* GEPSME= (cluster_method): JP_ALSD_* or JP_GEPS_* */
   double lambda0;        /* initial lambda (LAMBDA) */
   double lambda_mass;    /* its mass; 0 = total mass of the cluster (inpcls.f90:350-360) */
   int32_t lambda_temp_control;  /* lambda velocity coupled to the thermostat (l_temp_control) */
@@ -298,6 +299,18 @@ typedef struct jp_params {
 #define JP_TUNE_CANDIDATES 5   /* column-edge factors 0.84, 0.92, 1, 1.09, 1.19 */
 
 enum { JP_ALSD_NONE = 0, JP_ALSD_LMD = 1, JP_ALSD_LMD2 = 2 };
+/* GEPSME= AND / OR / XOR (inpinp.f90:44-54, n_matrix inpcls.f90:298-325): partial McMD.
+ * With jp_system.cluster set, every term belongs to class 1 or 2 by the regions of its atoms
+ * (n_matrix of the region pair: AND -- both atoms in A, or both in B; OR -- both in A, or one
+ * in A and one in B, or (without B) at least one in A; XOR -- one in A and one in B, or
+ * (without B) exactly one in A); bonded terms that SCALET leaves unscaled are class 2.  The
+ * class-1 forces are scaled and the class-2 forces are not (verlet.f90:118-142,
+ * verlethe.f90:170-238 with nfrg = 2): by the McMD weight of the class-1 potential energy
+ * (METHOD= GE) or by SETTEM/PSETMP (PSETMP > 0, any other METHOD).  Without GE or PSETMP
+ * md_run integrates the class-2 forces alone, so that combination is refused.  Replicas
+ * without cluster atoms run plain McMD / pseudo temperature on their whole energy.  Not with
+ * CAL15M= CMM or jp_minimize. */
+enum { JP_GEPS_AND = 3, JP_GEPS_OR = 4, JP_GEPS_XOR = 5 };
 enum { JP_SCALE_BOND = 1, JP_SCALE_ANGLE = 2, JP_SCALE_TORS = 4, JP_SCALE_IMPR = 8 };
 enum { JP_STOP_TRANS = 1, JP_STOP_ROT = 2, JP_STOP_BOTH = 3, JP_STOP_NONE = 4 };   /* STOPCE */
 enum { JP_CAL15M_CMM = 1, JP_CAL15M_ATOM = 2, JP_CAL15M_ZD = 4 };                  /* CAL15M */
@@ -324,6 +337,16 @@ int jp_rebuild_cells(jp_ctx *ctx, int32_t replica);
  * eneval[JP_MAXENE], grad[natom][3] (dE/dx, kcal/mol/Angstrom). */
 int jp_energy_grad(jp_ctx *ctx, int32_t replica, const double *cord, double *eneval,
                    double *grad);
+
+/* dnergy's outputs by class (dnergy.f90:2-84: the class totals enevcc(1, 1:nfrg) and the
+ * gradient grad(3, N, 1:nfrg) before verlethe combines the classes).  nfrg = 1 for a replica
+ * without cluster atoms, 3 for ALSD (classes AA, AB, BB), 2 for GEPSME= AND / OR / XOR
+ * (classes 1, 2); *nfrg_out receives it.  ecls[nfrg] (nullable) the class totals, the ZD self
+ * term included; grad[nfrg][natom][3] (nullable) each class's unscaled gradient (dE/dx);
+ * eneval[JP_MAXENE] (nullable) as jp_energy_grad.  cord as jp_energy_grad.  An ALSD replica
+ * is evaluated once per class (the class weights set to one class at a time). */
+int jp_energy_grad_cls(jp_ctx *ctx, int32_t replica, const double *cord, double *eneval,
+                       double *ecls, double *grad, int32_t *nfrg_out);
 
 /* nsteps iterations of runmd's loop body (md.f90:519-694): one verlet (MICR) or verlethe
  * (CANO/GE) step including SHAKE, then the pair-list rebuild every UPDATE steps.

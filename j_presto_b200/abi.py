@@ -14,6 +14,7 @@ JP_PREC_FP64, JP_PREC_MIXED = 0, 1
 JP_METHOD_CONS, JP_METHOD_MICR, JP_METHOD_CANO, JP_METHOD_GE = 1, 2, 3, 4
 JP_SHAKE_NONE, JP_SHAKE_HBON, JP_SHAKE_ALLB = 0, 1, 2
 JP_ALSD_NONE, JP_ALSD_LMD, JP_ALSD_LMD2 = 0, 1, 2
+JP_GEPS_AND, JP_GEPS_OR, JP_GEPS_XOR = 3, 4, 5
 JP_SCALE_BOND, JP_SCALE_ANGLE, JP_SCALE_TORS, JP_SCALE_IMPR = 1, 2, 4, 8
 JP_STOP_TRANS, JP_STOP_ROT, JP_STOP_BOTH, JP_STOP_NONE = 1, 2, 3, 4
 JP_CAL15M_CMM, JP_CAL15M_ATOM, JP_CAL15M_ZD = 1, 2, 4

@@ -69,7 +69,9 @@ struct jp_ctx {
   bool minimg = true;
   int pair_warps = 0;
   int nsm = 148;                    // the device's SM count
-  bool alsd = false;
+  bool alsd = false;                // some replica has ALSD classes (lambda)
+  bool split = false;               // some replica keeps partial-McMD class-1 forces apart
+  bool classes = false;             // alsd or split: class energies are kept
   bool cmm = false;                 // CAL15M= CMM
   bool hbond = false;               // some type pair has the 10-12 H-bond term
   int hb_cap = 0;                   // capacity of the H-bond pair list
@@ -215,17 +217,19 @@ void enqueue_zero(jp_ctx *c, bool count) {
   cudaStream_t st = c->st;
   if (c->fp64) cudaMemsetAsync(P.grd, 0, sizeof(double) * 3 * c->natom, st);
   else cudaMemsetAsync(P.frc, 0, sizeof(long long) * 3 * c->natom, st);
+  if (c->split && c->fp64) cudaMemsetAsync(P.grd1, 0, sizeof(double) * 3 * c->natom, st);
+  if (c->split && !c->fp64) cudaMemsetAsync(P.frc1, 0, sizeof(long long) * 3 * c->natom, st);
   cudaMemsetAsync(P.ene_fix, 0, sizeof(long long) * (16 * c->nrep + 1), st);   // + tile counter
-  if (c->alsd) cudaMemsetAsync(P.ene_cls, 0, sizeof(long long) * 4 * c->nrep, st);
+  if (c->classes) cudaMemsetAsync(P.ene_cls, 0, sizeof(long long) * 4 * c->nrep, st);
   if (count) cudaMemsetAsync(P.pair_cnt, 0, sizeof(long long) * c->nrep, st);
 }
 
 // the non-bonded forces: pair tiles, and with CMM the far field (recomputed every CMMUPD
 // steps by the step counter, or always with force_far: a single-point evaluation)
 void enqueue_pair(jp_ctx *c, bool count, bool force_far = false) {
-  if (c->fp64) launch_pair_fp64(c->P, c->zc, c->pair_warps, count, c->alsd, c->st);
-  else launch_pair_mixed(c->P, c->zc, c->pair_warps, c->minimg, count, c->alsd, c->st);
-  if (c->hbond) launch_hbond(c->P, c->hb_cap, c->zc.rc2, c->zc.nt1, c->fp64, c->alsd, c->st);
+  if (c->fp64) launch_pair_fp64(c->P, c->zc, c->pair_warps, count, c->alsd, c->split, c->st);
+  else launch_pair_mixed(c->P, c->zc, c->pair_warps, count, c->alsd, c->split, c->st);
+  if (c->hbond) launch_hbond(c->P, c->hb_cap, c->zc.rc2, c->zc.nt1, c->fp64, c->classes, c->st);
   if (c->cmm) launch_cmm_far(c->P, c->natom, c->nrep, c->fp64, force_far, c->qscale * c->qscale, c->st);
 }
 
@@ -235,8 +239,8 @@ void enqueue_forces(jp_ctx *c, bool count, bool force_far = false) {
 }
 
 void enqueue_bonded(jp_ctx *c) {
-  launch_bonded(c->P, c->nterm, c->fp64, c->zc.bcoeff, c->zc.fcoeff, c->alsd, c->st);
-  launch_restraints(c->P, c->nres, c->fp64, c->alsd, c->st);
+  launch_bonded(c->P, c->nterm, c->fp64, c->zc.bcoeff, c->zc.fcoeff, c->classes, c->st);
+  launch_restraints(c->P, c->nres, c->fp64, c->classes, c->st);
 }
 
 void enqueue_integrate(jp_ctx *c) {
@@ -272,11 +276,11 @@ int capture(jp_ctx *c, cudaGraphExec_t *out, bool rebuild) {
     // call that last used them, left them so); the bonded terms run beside the pair tiles
     // (both only add into the accumulators, as order-independent integer sums on the mixed
     // path), joined before the integration
-    if (c->alsd) cudaMemsetAsync(c->P.ene_cls, 0, sizeof(long long) * 4 * c->nrep, c->st);
+    if (c->classes) cudaMemsetAsync(c->P.ene_cls, 0, sizeof(long long) * 4 * c->nrep, c->st);
     CK(cudaEventRecord(c->ev_fork, c->st));
     CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
-    launch_bonded(c->P, c->nterm, c->fp64, c->zc.bcoeff, c->zc.fcoeff, c->alsd, c->st2);
-    launch_restraints(c->P, c->nres, c->fp64, c->alsd, c->st2);
+    launch_bonded(c->P, c->nterm, c->fp64, c->zc.bcoeff, c->zc.fcoeff, c->classes, c->st2);
+    launch_restraints(c->P, c->nres, c->fp64, c->classes, c->st2);
     CK(cudaEventRecord(c->ev_join, c->st2));
     enqueue_pair(c, false);
     CK(cudaStreamWaitEvent(c->st, c->ev_join, 0));
@@ -297,6 +301,8 @@ int check_status(jp_ctx *c) {
   CK(cudaMemset(c->P.bar, 0, sizeof(unsigned) * 4));
   if (c->fp64) CK(cudaMemset(c->P.grd, 0, sizeof(double) * 3 * c->natom));
   else CK(cudaMemset(c->P.frc, 0, sizeof(long long) * 3 * c->natom));
+  if (c->split && c->fp64) CK(cudaMemset(c->P.grd1, 0, sizeof(double) * 3 * c->natom));
+  if (c->split && !c->fp64) CK(cudaMemset(c->P.frc1, 0, sizeof(long long) * 3 * c->natom));
   CK(cudaMemset(c->P.ene_fix, 0, sizeof(long long) * (16 * c->nrep + 1)));
   CK(cudaMemset(c->P.kin_fix, 0, sizeof(long long) * c->nkin * c->nsub));
   if (c->ic.stop) CK(cudaMemset(c->P.com, 0, sizeof(double) * c->ic.ncom * c->ic.nrep * 16));
@@ -420,10 +426,12 @@ int clear_after_failure(jp_ctx *c) {
   CK(cudaMemsetAsync(P.bar, 0, sizeof(unsigned) * 4, c->st));
   if (c->fp64) CK(cudaMemsetAsync(P.grd, 0, sizeof(double) * 3 * c->natom, c->st));
   else CK(cudaMemsetAsync(P.frc, 0, sizeof(long long) * 3 * c->natom, c->st));
+  if (c->split && c->fp64) CK(cudaMemsetAsync(P.grd1, 0, sizeof(double) * 3 * c->natom, c->st));
+  if (c->split && !c->fp64) CK(cudaMemsetAsync(P.frc1, 0, sizeof(long long) * 3 * c->natom, c->st));
   CK(cudaMemsetAsync(P.ene_fix, 0, sizeof(long long) * (16 * c->nrep + 1), c->st));
   CK(cudaMemsetAsync(P.kin_fix, 0, sizeof(long long) * c->nkin * c->nsub, c->st));
   if (c->ic.stop) CK(cudaMemsetAsync(P.com, 0, sizeof(double) * c->ic.ncom * c->ic.nrep * 16, c->st));
-  if (c->alsd) CK(cudaMemsetAsync(P.ene_cls, 0, sizeof(long long) * 4 * c->nrep, c->st));
+  if (c->classes) CK(cudaMemsetAsync(P.ene_cls, 0, sizeof(long long) * 4 * c->nrep, c->st));
   CK(cudaMemsetAsync(P.rep_fail, 0, sizeof(int) * c->nrep, c->st));
   return 0;
 }
@@ -533,10 +541,24 @@ int validate(const jp_system *sys, int nrep, const jp_params *prm) {
   }
   if (prm->bounda != JP_BOUND_PBC && prm->bounda != JP_BOUND_NONE) return JP_E_INVALID;
   if (prm->precision != JP_PREC_FP64 && prm->precision != JP_PREC_MIXED) return JP_E_INVALID;
-  if (prm->alsd < JP_ALSD_NONE || prm->alsd > JP_ALSD_LMD2) return JP_E_INVALID;
-  if (prm->alsd != JP_ALSD_NONE) {   // verlethe only; lambda^(1/2) needs lambda > 0
+  if (prm->alsd < JP_ALSD_NONE || prm->alsd > JP_GEPS_XOR) return JP_E_INVALID;
+  const bool lmd = prm->alsd == JP_ALSD_LMD || prm->alsd == JP_ALSD_LMD2;
+  const bool geps = prm->alsd >= JP_GEPS_AND;
+  if (lmd) {   // verlethe only; lambda^(1/2) needs lambda > 0
     if (prm->method <= JP_METHOD_MICR || !std::isfinite(prm->lambda0)) return JP_E_INVALID;
     if (prm->alsd == JP_ALSD_LMD2 && !(prm->lambda0 > 0.0)) return JP_E_INVALID;
+  }
+  for (int r = 0; r < nrep && prm->alsd != JP_ALSD_NONE; ++r) {
+    if (!sys[r].cluster) continue;
+    bool any = false;
+    for (int i = 0; i < sys[r].natom; ++i) {   // region codes: A 1, B 2 (partial McMD only)
+      const int v = sys[r].cluster[i];
+      if (v < 0 || v > (geps ? 2 : 1)) return JP_E_INVALID;
+      any |= v != 0;
+    }
+    // partial McMD combines the classes only under the McMD weight or a pseudo temperature
+    // (verlet.f90:118-142, verlethe.f90:170-238); md_run would integrate class 2 alone
+    if (geps && any && prm->method != JP_METHOD_GE && !(prm->psetmp > 1.0e-10)) return JP_E_INVALID;
   }
   const double rlim = prm->cutoff + 1.5;
   for (int r = 0; r < nrep; ++r) {
@@ -1073,11 +1095,38 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     // block capacity: every column wastes less than one block
     R.nblk = (n + kTile - 1) / kTile + R.ncol;
     // ALSD cluster (inpcls.f90 icls): the atom's class bit rides in bit 30 of its LJ type
-    const bool ralsd = prm->alsd != JP_ALSD_NONE && s.cluster;
+    const bool ralsd = (prm->alsd == JP_ALSD_LMD || prm->alsd == JP_ALSD_LMD2) && s.cluster;
     std::vector<int> inA(n, 0);
     if (ralsd)
       for (int i = 0; i < n; ++i) inA[i] = s.cluster[i] ? 1 : 0;
-    auto pcls = [&](int a1, int a2) { return ralsd ? 2 - inA[a1] - inA[a2] : 2; };
+    // partial McMD (GEPSME= AND / OR / XOR): region codes A 0, B 1, neither 2 in bits 28-29
+    // of the LJ type, and the replica's class-1 table (n_matrix = 1, inpcls.f90:298-325); a
+    // replica without cluster atoms (nfrag = 1) keeps one class and plain McMD
+    std::vector<int> icl(n, 2);
+    bool rsplit = false;
+    unsigned tab1 = 0;
+    if (prm->alsd >= JP_GEPS_AND && s.cluster) {
+      bool hasA = false, hasB = false;
+      for (int i = 0; i < n; ++i) {
+        if (s.cluster[i] == 1) { icl[i] = 0; hasA = true; }
+        else if (s.cluster[i] == 2) { icl[i] = 1; hasB = true; }
+      }
+      rsplit = hasA || hasB;
+      auto bit = [](int a, int c2) { return (1u << (3 * a + c2)) | (1u << (3 * c2 + a)); };
+      if (!hasB) {   // nfrag = 2: region A and the rest
+        tab1 = prm->alsd == JP_GEPS_AND ? bit(0, 0) : prm->alsd == JP_GEPS_OR ? bit(0, 0) | bit(0, 2) : bit(0, 2);
+      } else {       // nfrag = 3: A, B and the rest
+        tab1 = prm->alsd == JP_GEPS_AND ? bit(0, 0) | bit(1, 1) : prm->alsd == JP_GEPS_OR ? bit(0, 0) | bit(0, 1)
+                                                                                     : bit(0, 1);
+      }
+    }
+    R.split = rsplit ? 1 : 0;
+    R.cls_tab = tab1;
+    R.cls_over = 0;
+    auto pcls = [&](int a1, int a2) {
+      if (rsplit) return ((tab1 >> (3 * icl[a1] + icl[a2])) & 1u) ? 0 : 2;
+      return ralsd ? 2 - inA[a1] - inA[a2] : 2;
+    };
     for (int i = 0; i < n; ++i) {
       for (int k = 0; k < 3; ++k) {
         hx.push_back(s.cord[3 * i + k]);
@@ -1086,7 +1135,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
       hmass.push_back(s.mass[i]);
       himass.push_back(1.0 / s.mass[i]);
       hchg.push_back(s.charge[i]);
-      htyp.push_back((s.atype[i] - b) | (inA[i] << 30));
+      htyp.push_back((s.atype[i] - b) | (inA[i] << 30) | (rsplit ? icl[i] << kRegionShift : 0));
       hrep.push_back(r);
     }
     // exclusions
@@ -1104,7 +1153,10 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
     if (s.molecule && prm->tempco == 2) {
       // with clusters each molecule splits into its cluster and non-cluster part (md.f90
       // ixamol2 = (ixamol - 1) * nfrag + icls, renumbered densely)
-      auto key = [&](int i) { return ralsd ? 2 * (s.molecule[i] - b) + (inA[i] ? 0 : 1) : s.molecule[i] - b; };
+      auto key = [&](int i) {
+        return ralsd ? 2 * (s.molecule[i] - b) + (inA[i] ? 0 : 1) : rsplit ? 3 * (s.molecule[i] - b) + icl[i]
+                                                                          : s.molecule[i] - b;
+      };
       std::vector<int> u;
       for (int i = 0; i < n; ++i) u.push_back(key(i));
       std::sort(u.begin(), u.end());
@@ -1313,6 +1365,13 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
         int na = 0;
         for (int k = 0; k < 4; ++k) na += inA[s.impr[4 * i + k] - b];
         t.cls = na == 4 ? 0 : (na > 0 ? 1 : 2);
+      } else if ((sct & JP_SCALE_IMPR) && rsplit) {
+        int lo = 2, hi = 0;
+        for (int k = 0; k < 4; ++k) {
+          lo = std::min(lo, icl[s.impr[4 * i + k] - b]);
+          hi = std::max(hi, icl[s.impr[4 * i + k] - b]);
+        }
+        t.cls = ((tab1 >> (3 * lo + hi)) & 1u) ? 0 : 2;
       }
       terms_by_kind[T_IMPR].push_back(t);
     }
@@ -1492,6 +1551,10 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.slot_of, (size_t)N);
   e |= dalloc(c, &P.frc, 3 * (size_t)N);
   e |= dalloc(c, &P.grd, 3 * (size_t)N);
+  bool anysplit = false;   // partial McMD: the class-1 gradient set
+  for (int r = 0; r < nrep; ++r) anysplit |= reps[r].split != 0;
+  if (anysplit && c->fp64) e |= dalloc(c, &P.grd1, 3 * (size_t)N);
+  if (anysplit && !c->fp64) e |= dalloc(c, &P.frc1, 3 * (size_t)N);
   e |= dput(c, &P.excl_ptr, hexp);
   e |= dput(c, &P.excl_idx, hexi);
   e |= dalloc(c, &P.excl_slot, hexi.size());
@@ -1677,6 +1740,9 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   ic.alsd = 0;
   for (int r = 0; r < nrep; ++r) ic.alsd |= reps[r].lam_mode != 0;
   c->alsd = ic.alsd != 0;
+  ic.split = anysplit ? 1 : 0;
+  c->split = anysplit;
+  c->classes = c->alsd || c->split;
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   c->nsm = std::max(1, nsm);
@@ -1747,9 +1813,9 @@ int jp_get_state(jp_ctx *c, int32_t r, double *cord, double *vel) {
   return JP_OK;
 }
 
-int jp_energy_grad(jp_ctx *c, int32_t r, const double *cord, double *eneval, double *grad) {
-  if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
-  CK(cudaSetDevice(c->device));
+// One dnergy of every replica, synchronised: the accumulators then hold its gradients and
+// energies (cord: the replica's new coordinates first, nullable)
+int eval_forces(jp_ctx *c, int32_t r, const double *cord) {
   if (int e = flush_rebuild(c)) return e;
   const Rep &R = c->reps[r];
   if (cord) {
@@ -1761,34 +1827,132 @@ int jp_energy_grad(jp_ctx *c, int32_t r, const double *cord, double *eneval, dou
   enqueue_bonded(c);
   CK(cudaStreamSynchronize(c->st));
   CK(cudaGetLastError());
-  if (eneval) {
-    long long ef[16];
-    CK(cudaMemcpy(ef, c->P.ene_fix + 16 * (size_t)r, sizeof(ef), cudaMemcpyDeviceToHost));
-    double tot = 0.0;
-    for (int k = 1; k < JP_MAXENE; ++k) {
-      eneval[k] = (double)ef[k] * kEneInv;
-      if (k == JP_E_ELE15) eneval[k] += R.dself;
-      tot += eneval[k];
-    }
-    eneval[0] = tot;
+  return JP_OK;
+}
+
+// the replica's eneval from the energy slots (the ZD self term into ELE15)
+int read_eneval(jp_ctx *c, int32_t r, double *eneval) {
+  long long ef[16];
+  CK(cudaMemcpy(ef, c->P.ene_fix + 16 * (size_t)r, sizeof(ef), cudaMemcpyDeviceToHost));
+  double tot = 0.0;
+  for (int k = 1; k < JP_MAXENE; ++k) {
+    eneval[k] = (double)ef[k] * kEneInv;
+    if (k == JP_E_ELE15) eneval[k] += c->reps[r].dself;
+    tot += eneval[k];
   }
-  if (grad) {
-    if (c->fp64) {
-      CK(cudaMemcpy(grad, c->P.grd + 3 * (size_t)R.atom0, sizeof(double) * 3 * R.natom,
-                    cudaMemcpyDeviceToHost));
-    } else {
-      std::vector<long long> g(3 * (size_t)R.natom);
-      CK(cudaMemcpy(g.data(), c->P.frc + 3 * (size_t)R.atom0, sizeof(long long) * g.size(),
-                    cudaMemcpyDeviceToHost));
-      for (size_t i = 0; i < g.size(); ++i) grad[i] = (double)g[i] * kFrcInv;
-    }
+  eneval[0] = tot;
+  return JP_OK;
+}
+
+// the replica's gradient in accumulator set `set` (0: frc / grd, 1: the class-1 set frc1 /
+// grd1), written to out or, with add, added to it
+int read_grad(jp_ctx *c, int32_t r, int set, double *out, bool add) {
+  const Rep &R = c->reps[r];
+  const size_t n3 = 3 * (size_t)R.natom;
+  std::vector<double> g(n3);
+  if (c->fp64) {
+    CK(cudaMemcpy(g.data(), (set ? c->P.grd1 : c->P.grd) + 3 * (size_t)R.atom0, sizeof(double) * n3,
+                  cudaMemcpyDeviceToHost));
+  } else {
+    std::vector<long long> f(n3);
+    CK(cudaMemcpy(f.data(), (set ? c->P.frc1 : c->P.frc) + 3 * (size_t)R.atom0, sizeof(long long) * n3,
+                  cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n3; ++i) g[i] = (double)f[i] * kFrcInv;
   }
-  // steps start from zero force and energy accumulators; the class energies stay readable
-  // (jp_get_lambda) until the next step clears them
+  for (size_t i = 0; i < n3; ++i) out[i] = add ? out[i] + g[i] : g[i];
+  return JP_OK;
+}
+
+// steps start from zero force and energy accumulators; the class energies stay readable
+// (jp_get_lambda) until the next step clears them
+int clear_eval(jp_ctx *c) {
   if (c->fp64) CK(cudaMemsetAsync(c->P.grd, 0, sizeof(double) * 3 * c->natom, c->st));
   else CK(cudaMemsetAsync(c->P.frc, 0, sizeof(long long) * 3 * c->natom, c->st));
+  if (c->split && c->fp64) CK(cudaMemsetAsync(c->P.grd1, 0, sizeof(double) * 3 * c->natom, c->st));
+  if (c->split && !c->fp64) CK(cudaMemsetAsync(c->P.frc1, 0, sizeof(long long) * 3 * c->natom, c->st));
   CK(cudaMemsetAsync(c->P.ene_fix, 0, sizeof(long long) * (16 * c->nrep + 1), c->st));
   CK(cudaStreamSynchronize(c->st));
+  return JP_OK;
+}
+
+int jp_energy_grad(jp_ctx *c, int32_t r, const double *cord, double *eneval, double *grad) {
+  if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  if (int e = eval_forces(c, r, cord)) return e;
+  if (eneval)
+    if (int e = read_eneval(c, r, eneval)) return e;
+  if (grad) {   // classes 1 and 2 together for a partial-McMD replica
+    if (int e = read_grad(c, r, 0, grad, false)) return e;
+    if (c->reps[r].split)
+      if (int e = read_grad(c, r, 1, grad, true)) return e;
+  }
+  if (int e = clear_eval(c)) return e;
+  return check_status(c);
+}
+
+// the class-weight override of replica r (jp_energy_grad_cls on an ALSD replica): weights of
+// one class (cls 0..2) or back to lambda's (cls < 0)
+int set_cls_override(jp_ctx *c, int32_t r, int cls) {
+  Rep &R = c->reps[r];
+  R.cls_over = cls >= 0 ? 1 : 0;
+  for (int k = 0; k < 3; ++k) R.cls_w[k] = k == cls ? 1.0 : 0.0;
+  CK(cudaMemcpyAsync(c->P.reps + r, &R, sizeof(Rep), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return JP_OK;
+}
+
+int jp_energy_grad_cls(jp_ctx *c, int32_t r, const double *cord, double *eneval, double *ecls, double *grad,
+                       int32_t *nfrg_out) {
+  if (!c || r < 0 || r >= c->nrep) return JP_E_INVALID;
+  CK(cudaSetDevice(c->device));
+  const Rep &R = c->reps[r];
+  const int nfrg = R.lam_mode ? 3 : R.split ? 2 : 1;
+  if (nfrg_out) *nfrg_out = nfrg;
+  const size_t n3 = 3 * (size_t)R.natom;
+  if (nfrg == 3) {   // one evaluation per class, the weights set to that class alone
+    for (int q = 0; q < 3; ++q) {
+      if (int e = set_cls_override(c, r, q)) return e;
+      int e = eval_forces(c, r, q == 0 ? cord : nullptr);
+      if (!e && eneval && q == 0) e = read_eneval(c, r, eneval);
+      if (!e && grad) e = read_grad(c, r, 0, grad + q * n3, false);
+      if (!e && ecls) {
+        long long ef[4];
+        CK(cudaMemcpy(ef, c->P.ene_cls + 4 * (size_t)r, sizeof(ef), cudaMemcpyDeviceToHost));
+        ecls[q] = (double)ef[q] * kEneInv + R.dself_cls[q];
+      }
+      if (!e) e = clear_eval(c);
+      if (!e) e = check_status(c);
+      if (e) {
+        set_cls_override(c, r, -1);
+        return e;
+      }
+    }
+    return set_cls_override(c, r, -1);
+  }
+  if (int e = eval_forces(c, r, cord)) return e;
+  if (eneval)
+    if (int e = read_eneval(c, r, eneval)) return e;
+  if (nfrg == 2) {   // partial McMD: class 1 in the frc1 / grd1 set, class 2 in frc / grd
+    if (grad) {
+      if (int e = read_grad(c, r, 1, grad, false)) return e;
+      if (int e = read_grad(c, r, 0, grad + n3, false)) return e;
+    }
+    if (ecls) {
+      long long ef[4];
+      CK(cudaMemcpy(ef, c->P.ene_cls + 4 * (size_t)r, sizeof(ef), cudaMemcpyDeviceToHost));
+      ecls[0] = (double)ef[0] * kEneInv + R.dself_cls[0];
+      ecls[1] = (double)ef[2] * kEneInv + R.dself_cls[2];
+    }
+  } else {
+    if (grad)
+      if (int e = read_grad(c, r, 0, grad, false)) return e;
+    if (ecls) {
+      double ev[JP_MAXENE];
+      if (int e = read_eneval(c, r, ev)) return e;
+      ecls[0] = ev[0];
+    }
+  }
+  if (int e = clear_eval(c)) return e;
   return check_status(c);
 }
 
@@ -1962,7 +2126,7 @@ int jp_get_lambda(jp_ctx *c, int32_t r, double *lam2, double *ecls) {
   if (lam2) CK(cudaMemcpy(lam2, c->P.lam + 2 * r, sizeof(double) * 2, cudaMemcpyDeviceToHost));
   if (ecls) {
     long long ef[4] = {0, 0, 0, 0};
-    if (c->alsd) CK(cudaMemcpy(ef, c->P.ene_cls + 4 * (size_t)r, sizeof(ef), cudaMemcpyDeviceToHost));
+    if (c->classes) CK(cudaMemcpy(ef, c->P.ene_cls + 4 * (size_t)r, sizeof(ef), cudaMemcpyDeviceToHost));
     for (int k = 0; k < 3; ++k) ecls[k] = (double)ef[k] * kEneInv + c->reps[r].dself_cls[k];
   }
   return JP_OK;
@@ -2017,6 +2181,7 @@ int jp_minimize(jp_ctx *c, const jp_min_params *mp, int32_t *iters, double *enev
   if (mp->method == JP_MIN_STEEP &&
       (!(mp->up > 0.0) || !(mp->down > 0.0) || !std::isfinite(mp->up) || !std::isfinite(mp->down)))
     return JP_E_INVALID;
+  if (c->split) return JP_E_INVALID;   // the class-1 gradient set has no role in the minimiser
   CK(cudaSetDevice(c->device));
   if (int e = flush_rebuild(c)) return e;
   if (mp->method == JP_MIN_CONJ) {   // conj.f90:48-53: no SHAKE with conjugate gradients

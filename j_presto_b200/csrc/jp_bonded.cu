@@ -29,9 +29,13 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
     rep = T.rep;
     const Rep& R = P.reps[rep];
     double fs = 1.0;
+    bool c1 = false;   // a class-1 term of a partial-McMD replica
     if (alsd && R.lam_mode) {
       cls = T.cls;
-      fs = lam_factor(R.lam_mode, P.lam[2 * rep], cls);
+      fs = cls_weight(R, P.lam[2 * rep], cls);
+    } else if (alsd && R.split) {
+      cls = T.cls;
+      c1 = cls == 0;
     }
     Img im;
     for (int k = 0; k < 3; ++k) { im.b[k] = R.box[k]; im.ib[k] = R.invbox[k]; }
@@ -46,8 +50,8 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
         double coef = T.p0 * dif;
         e1 = coef * dif;
         coef = 2.0 * coef / r12;
-        add_grad<FP64>(P, fs, T.a[0], coef * d[0], coef * d[1], coef * d[2]);
-        add_grad<FP64>(P, fs, T.a[1], -coef * d[0], -coef * d[1], -coef * d[2]);
+        add_grad<FP64>(P, fs, T.a[0], coef * d[0], coef * d[1], coef * d[2], c1);
+        add_grad<FP64>(P, fs, T.a[1], -coef * d[0], -coef * d[1], -coef * d[2], c1);
         slot1 = JP_E_BOND;
         break;
       }
@@ -78,9 +82,9 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
         for (int k = 0; k < 3; ++k) w[k] = coef * (d32[k] * r12r32 - d12[k] * rt);
         rt = cost * r32;
         for (int k = 0; k < 3; ++k) w[3 + k] = coef * (d12[k] * r12r32 - d32[k] * rt);
-        add_grad<FP64>(P, fs, T.a[0], w[0], w[1], w[2]);
-        add_grad<FP64>(P, fs, T.a[1], -(w[0] + w[3]), -(w[1] + w[4]), -(w[2] + w[5]));
-        add_grad<FP64>(P, fs, T.a[2], w[3], w[4], w[5]);
+        add_grad<FP64>(P, fs, T.a[0], w[0], w[1], w[2], c1);
+        add_grad<FP64>(P, fs, T.a[1], -(w[0] + w[3]), -(w[1] + w[4]), -(w[2] + w[5]), c1);
+        add_grad<FP64>(P, fs, T.a[2], w[3], w[4], w[5], c1);
         slot1 = JP_E_ANGLE;
         break;
       }
@@ -143,10 +147,10 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
         w[7] = d32[0] * p12[2] - d32[2] * p12[0] - q23 * (d32[0] * p23[2] - d32[2] * p23[0]);
         w[8] = d32[1] * p12[0] - d32[0] * p12[1] - q23 * (d32[1] * p23[0] - d32[0] * p23[1]);
         for (int k = 0; k < 9; ++k) w[k] *= w0;
-        add_grad<FP64>(P, fs, T.a[0], w[0], w[1], w[2]);
-        add_grad<FP64>(P, fs, T.a[1], w[3], w[4], w[5]);
-        add_grad<FP64>(P, fs, T.a[2], -(w[0] + w[3] + w[6]), -(w[1] + w[4] + w[7]), -(w[2] + w[5] + w[8]));
-        add_grad<FP64>(P, fs, T.a[3], w[6], w[7], w[8]);
+        add_grad<FP64>(P, fs, T.a[0], w[0], w[1], w[2], c1);
+        add_grad<FP64>(P, fs, T.a[1], w[3], w[4], w[5], c1);
+        add_grad<FP64>(P, fs, T.a[2], -(w[0] + w[3] + w[6]), -(w[1] + w[4] + w[7]), -(w[2] + w[5] + w[8]), c1);
+        add_grad<FP64>(P, fs, T.a[3], w[6], w[7], w[8], c1);
         break;
       }
       case T_P14: {
@@ -169,8 +173,8 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
         e2 = coef;
         coef *= -r14;
         for (int k = 0; k < 3; ++k) w[k] += coef * d[k];
-        add_grad<FP64>(P, fs, T.a[0], w[0], w[1], w[2]);
-        add_grad<FP64>(P, fs, T.a[1], -w[0], -w[1], -w[2]);
+        add_grad<FP64>(P, fs, T.a[0], w[0], w[1], w[2], c1);
+        add_grad<FP64>(P, fs, T.a[1], -w[0], -w[1], -w[2], c1);
         break;
       }
       case T_EXCESS: {
@@ -182,8 +186,8 @@ __global__ void __launch_bounds__(256) k_bonded(DevPtrs P, int nterm, double zb,
         double cc = T.p0;   // chgmod(a)*chgmod(b)
         e1 = cc * zb * dd2;
         cc *= zf;
-        add_grad<FP64>(P, fs, T.a[0], d[0] * cc, d[1] * cc, d[2] * cc);
-        add_grad<FP64>(P, fs, T.a[1], -d[0] * cc, -d[1] * cc, -d[2] * cc);
+        add_grad<FP64>(P, fs, T.a[0], d[0] * cc, d[1] * cc, d[2] * cc, c1);
+        add_grad<FP64>(P, fs, T.a[1], -d[0] * cc, -d[1] * cc, -d[2] * cc, c1);
         break;
       }
     }

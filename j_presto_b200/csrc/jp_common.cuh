@@ -75,6 +75,15 @@ struct Rep {
   int stop_n;                     // centre-of-mass stop: atoms [atom0, atom0 + stop_n); 0 = off
   double lam_m, lam_im;           // lambda mass and its inverse
   double dself_cls[3];            // ZD self term by class
+  // GEPSME= AND / OR / XOR with cluster atoms (partial McMD, nfrg = 2): class-1 terms
+  // (bit 3 ca + cb of cls_tab set for atom regions ca, cb: 0 A, 1 B, 2 neither) accumulate
+  // into frc1 / grd1, class-2 terms into frc / grd; class energies in slots 0 and 2
+  int split;
+  unsigned cls_tab;
+  // class weights set to one class at a time (cls_over = 1) while dnergy's per-class
+  // outputs of an ALSD replica are evaluated; cls_w[AA, AB, BB]
+  int cls_over;
+  double cls_w[3];
   // BOUNDA= NO: the periodic box is a container large enough that minimum image is the
   // identity while every atom stays in [win_lo, win_hi]
   int free_bnd;
@@ -94,7 +103,14 @@ __host__ __device__ __forceinline__ double lam_factor(int mode, double lam, int 
   if (cls == 0) return mode == JP_ALSD_LMD ? lam * lam : lam;
   return mode == JP_ALSD_LMD ? lam : sqrt(lam);
 }
-constexpr int kTypeMask = 0xffff;   // LJ type in the low bits of typ/styp; bit 30 = cluster atom
+// the same, or the replica's one-class weights while its per-class outputs are evaluated
+__host__ __device__ __forceinline__ double cls_weight(const Rep& R, double lam, int cls) {
+  return R.cls_over ? R.cls_w[cls] : lam_factor(R.lam_mode, lam, cls);
+}
+// LJ type in the low bits of typ/styp; bit 30 = ALSD cluster atom; bits 28-29 = the atom's
+// region code (0 A, 1 B, 2 neither) in a partial-McMD replica
+constexpr int kTypeMask = 0xffff;
+constexpr int kRegionShift = 28;
 
 // integration unit: a SHAKE group (2-4 atoms) or a lone atom (n = 1)
 struct Unit {
@@ -150,6 +166,8 @@ struct DevPtrs {
   int *typ, *rep_of, *slot_of;
   long long *frc;
   double *grd;
+  long long *frc1;                // partial McMD: class-1 gradient (fixed point / FP64 path)
+  double *grd1;
   // exclusions (global atom ids)
   int *excl_ptr, *excl_idx;
   int *excl_slot;                 // slot of each partner after the last sort
@@ -272,19 +290,22 @@ __device__ __forceinline__ void atomic_add_ll(long long *p, long long v) {
 __host__ __device__ __forceinline__ double anint(double x) { return round(x); }
 
 // gradient of one atom from a term evaluated in FP64, times its ALSD class weight fs:
-// FP64 atomics on the FP64 path, 64-bit fixed point on the mixed path
+// FP64 atomics on the FP64 path, 64-bit fixed point on the mixed path; c1: a class-1 term of
+// a partial-McMD replica (into frc1 / grd1)
 template <bool FP64>
 __device__ __forceinline__ void add_grad(const DevPtrs& P, double fs, int a, double gx, double gy,
-                                         double gz) {
+                                         double gz, bool c1 = false) {
   gx *= fs; gy *= fs; gz *= fs;   // ALSD class weight (1 otherwise)
   if (FP64) {
-    atomicAdd(&P.grd[3 * a + 0], gx);
-    atomicAdd(&P.grd[3 * a + 1], gy);
-    atomicAdd(&P.grd[3 * a + 2], gz);
+    double* g = c1 ? P.grd1 : P.grd;
+    atomicAdd(&g[3 * a + 0], gx);
+    atomicAdd(&g[3 * a + 1], gy);
+    atomicAdd(&g[3 * a + 2], gz);
   } else {
-    atomic_add_ll(&P.frc[3 * a + 0], to_fix(gx, kFrcScale, P.status));
-    atomic_add_ll(&P.frc[3 * a + 1], to_fix(gy, kFrcScale, P.status));
-    atomic_add_ll(&P.frc[3 * a + 2], to_fix(gz, kFrcScale, P.status));
+    long long* f = c1 ? P.frc1 : P.frc;
+    atomic_add_ll(&f[3 * a + 0], to_fix(gx, kFrcScale, P.status));
+    atomic_add_ll(&f[3 * a + 1], to_fix(gy, kFrcScale, P.status));
+    atomic_add_ll(&f[3 * a + 2], to_fix(gz, kFrcScale, P.status));
   }
 }
 

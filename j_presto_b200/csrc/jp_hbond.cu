@@ -90,13 +90,18 @@ __global__ void __launch_bounds__(kHbThreads) k_hbond(DevPtrs P, int cap, double
         const double v2 = h.y * (dd4i * dd4i * dd4i);   // C12h / r^12
         e = v2 - v1;
         double fs = 1.0;
-        if (ALSD) {
+        bool c1 = false;   // class 1 of a partial-McMD replica
+        if (ALSD && R.split) {
+          const int ci = (ti >> kRegionShift) & 3, cj = (tj >> kRegionShift) & 3;
+          cls = ((R.cls_tab >> (3 * ci + cj)) & 1u) ? 0 : 2;
+          c1 = cls == 0;
+        } else if (ALSD) {
           cls = 2 - (((ti >> 30) & 1) + ((tj >> 30) & 1));
-          fs = lam_factor(R.lam_mode, P.lam[2 * rep], cls);
+          fs = cls_weight(R, P.lam[2 * rep], cls);
         }
         const double cc = (12.0 * v2 - 10.0 * v1) * dd2i;
-        add_grad<FP64>(P, fs, pr.x, -d[0] * cc, -d[1] * cc, -d[2] * cc);
-        add_grad<FP64>(P, fs, pr.y, d[0] * cc, d[1] * cc, d[2] * cc);
+        add_grad<FP64>(P, fs, pr.x, -d[0] * cc, -d[1] * cc, -d[2] * cc, c1);
+        add_grad<FP64>(P, fs, pr.y, d[0] * cc, d[1] * cc, d[2] * cc, c1);
       }
     }
     add_energy(P, rep, JP_E_HBOND, e);

@@ -28,6 +28,20 @@ __host__ __device__ __forceinline__ void mimg(const Rep& R, double* d) {
   for (int k = 0; k < 3; ++k) d[k] -= R.box[k] * anint(d[k] * R.invbox[k]);
 }
 
+// A partial-McMD replica scales its class-1 gradient alone (verlet.f90:130-141,
+// verlethe.f90:176-187, :223-234: grad(:,:,2) = grad(:,:,1) dew + grad(:,:,2)); the class-1
+// set exists only in contexts with such replicas (a uniform test of a kernel parameter)
+template <bool FP64>
+__device__ __forceinline__ void split_grad(const DevPtrs& P, int a, double s, double* g) {
+  if (FP64 ? P.grd1 == nullptr : P.frc1 == nullptr) return;
+  if (!P.reps[P.rep_of[a]].split) return;
+  for (int k = 0; k < 3; ++k) {
+    const double g1 = FP64 ? P.grd1[3 * a + k] : (double)P.frc1[3 * a + k] * kFrcInv;
+    const double g2 = FP64 ? P.grd[3 * a + k] : (double)P.frc[3 * a + k] * kFrcInv;
+    g[k] = g1 * s + g2;
+  }
+}
+
 template <bool FP64>
 __device__ __forceinline__ void load_grad(const DevPtrs& P, int a, double s, double* g) {
   if (FP64) {
@@ -35,6 +49,7 @@ __device__ __forceinline__ void load_grad(const DevPtrs& P, int a, double s, dou
   } else {
     for (int k = 0; k < 3; ++k) g[k] = (double)P.frc[3 * a + k] * kFrcInv * s;
   }
+  split_grad<FP64>(P, a, s, g);
 }
 
 __host__ __device__ __noinline__ int shake_group4(const Rep& R, const Unit& u, const double* im,
@@ -275,8 +290,10 @@ template <bool FP64>
 __device__ __forceinline__ void zero_force(const DevPtrs& P, int a) {
   if (FP64) {
     P.grd[3 * a] = 0.0; P.grd[3 * a + 1] = 0.0; P.grd[3 * a + 2] = 0.0;
+    if (P.grd1) { P.grd1[3 * a] = 0.0; P.grd1[3 * a + 1] = 0.0; P.grd1[3 * a + 2] = 0.0; }
   } else {
     P.frc[3 * a] = 0; P.frc[3 * a + 1] = 0; P.frc[3 * a + 2] = 0;
+    if (P.frc1) { P.frc1[3 * a] = 0; P.frc1[3 * a + 1] = 0; P.frc1[3 * a + 2] = 0; }
   }
 }
 
@@ -363,12 +380,20 @@ __device__ __forceinline__ double rep_scale(const DevPtrs& P, const IntConst& c,
   return rep_scale_poly(P, c, r);
 }
 
+// the energy of the McMD weight: the potential energy, or a partial-McMD replica's class-1
+// energy epotcc(1,1) (verlethe.f90:199-210)
+__device__ __forceinline__ double mcmd_energy(const DevPtrs& P, const Rep& R, int r) {
+  if (R.split) return (double)__ldcg(&P.ene_cls[4 * r]) * kEneInv + R.dself_cls[0];
+  double tot = R.dself;
+  for (int k = 1; k < JP_MAXENE; ++k) tot += (double)__ldcg(&P.ene_fix[r * 16 + k]) * kEneInv;
+  return tot;
+}
+
 __device__ double rep_scale_poly(const DevPtrs& P, const IntConst& c, int r) {
   const Rep& R = P.reps[r];
   if (R.lam_mode) return 1.0;   // ALSD: the weight acts on lambda, forces go by class
   if (c.method == JP_METHOD_GE && R.ge_nwin > 0) {
-    double tot = R.dself;
-    for (int k = 1; k < JP_MAXENE; ++k) tot += (double)__ldcg(&P.ene_fix[r * 16 + k]) * kEneInv;
+    const double tot = mcmd_energy(P, R, r);
     double dprobl;
     if (tot <= R.ge_celw) dprobl = R.ge_alphalw;
     else if (tot >= R.ge_ceup) dprobl = R.ge_alphaup;
@@ -488,8 +513,7 @@ __global__ void __launch_bounds__(32) k_ge_scale(DevPtrs P, IntConst c) {
     return;
   }
   if (c.method == JP_METHOD_GE && R.ge_nwin > 0 && R.mlp_on) {
-    double tot = R.dself;
-    for (int k = 1; k < JP_MAXENE; ++k) tot += (double)__ldcg(&P.ene_fix[r * 16 + k]) * kEneInv;
+    const double tot = mcmd_energy(P, R, r);
     double dprobl;
     if (tot <= R.ge_celw) {
       dprobl = R.ge_alphalw;
@@ -524,7 +548,7 @@ __device__ void write_ene_hist(const DevPtrs& P, const IntConst& c, int r) {
   }
   e[0] = tot;
   if (R.hist_n > 0 && !c.no_hist) {   // distrib_MULT.f90:95: k = int((E - minEc)/EbinSZ) + 1
-    const double u = (tot - R.hist_min) * R.hist_inv;
+    const double u = ((R.split ? mcmd_energy(P, R, r) : tot) - R.hist_min) * R.hist_inv;
     if (u > -1.0 && u < (double)R.hist_n) atomicAdd(&P.ge_hist[R.hist_off + (int)u], 1ull);
   }
   double* out = P.ene_hist + ((size_t)P.step_ctr[1] * c.nrep + r) * JP_MAXENE;
@@ -1276,6 +1300,7 @@ __device__ __forceinline__ void ru_grad(const DevPtrs& P, int a, double s, doubl
   } else {
     for (int k = 0; k < 3; ++k) g[k] = (double)__ldg(&P.frc[3 * a + k]) * kFrcInv * s;
   }
+  split_grad<FP64>(P, a, s, g);
 }
 
 __device__ __forceinline__ void ru_load(const DevPtrs& P, const Unit& u, UnitScal& U, UnitSmem& S,

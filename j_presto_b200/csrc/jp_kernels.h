@@ -41,9 +41,11 @@ void launch_cmm_far(const DevPtrs& P, int natom, int nrep, bool fp64, bool force
                     cudaStream_t st);
 
 // pair kernels (jp_pair.cu)
-void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool minimg, bool count,
-                       bool alsd, cudaStream_t st);
-void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, bool alsd,
+// alsd: some replica has ALSD classes; split: some replica keeps partial-McMD class-1 forces
+// apart (frc1 / grd1)
+void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, bool alsd, bool split,
+                       cudaStream_t st);
+void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, bool alsd, bool split,
                       cudaStream_t st);
 // co-resident blocks per SM of the (non-counting) pair kernel: the grid is one full wave
 int pair_blocks_per_sm(bool fp64, int nt1);
@@ -91,6 +93,7 @@ struct IntConst {
   int nsmall, nquad, qbase, nvirt;
   int ge_prescaled;        // force scales computed by k_ge_scale before the integration kernel
   int alsd;                // some replica runs ALSD (lambda carried by the integration kernel)
+  int split;               // some replica keeps partial-McMD class-1 forces apart (frc1 / grd1)
   int stop;                // STOPCE 1 translation, 2 rotation, 3 both; 0 = off
   int ncom;                // centre-of-mass sum slots (one per velocity update of a step)
   double taut;             // METHOD= CONS relaxation time (fs)

@@ -245,7 +245,8 @@ struct Gather {
 };
 
 // One compact tile, every step branch-free.  ALSD: ci = cluster bit of the i atom; a pair
-// with nA cluster atoms has its force times f2 (nA = 2, class AA), f1 (AB) or 1 (BB), and its
+// with nA cluster atoms has its force times f2 (nA = 2, class AA), f1 (AB) or f0 (BB: 1 but
+// while per-class outputs are evaluated), and its
 // energy also goes to ea (AA) / eb (AB).  CMM: no cut-off (rc2 is huge) and the Coulomb term
 // only for the pairs of `me` (the neighbouring-cell pairs; the rest are LJ only).
 // Energies: FP32 partial sums over 8 steps, accumulated in FP64.
@@ -255,7 +256,8 @@ __device__ __forceinline__ void tile_mixed(const MixStage& S, const float2* __re
                                            float bz, float ibx, float iby, float ibz, float rc2, float zb,
                                            float zf, float zc, float& fix, float& fiy, float& fiz,
                                            float& gjx, float& gjy, float& gjz, double& te, double& tl,
-                                           int& tn, int ci, float f1, float f2, double& ea, double& eb) {
+                                           int& tn, int ci, float f0, float f1, float f2, double& ea,
+                                           double& eb) {
   const unsigned full = 0xffffffffu;
   const int src = (lane + 1) & 31;
 #pragma unroll 1
@@ -292,7 +294,7 @@ __device__ __forceinline__ void tile_mixed(const MixStage& S, const float2* __re
         const float e = in ? eel + elj : 0.f;
         ea8 += na == 2 ? e : 0.f;
         eb8 += na == 1 ? e : 0.f;
-        fs *= na == 2 ? f2 : (na == 1 ? f1 : 1.f);
+        fs *= na == 2 ? f2 : (na == 1 ? f1 : f0);
       }
       fs = in ? fs : 0.f;
       te8 += in ? eel : 0.f;
@@ -314,7 +316,69 @@ __device__ __forceinline__ void tile_mixed(const MixStage& S, const float2* __re
   }
 }
 
-template <bool COUNT, bool ALSD, bool CMM>
+// One compact tile of a partial-McMD replica (GEPSME= AND / OR / XOR): the one-entry-per-step
+// form with each pair's class from the regions of its atoms (bit cj of trow = bits 3 ci..3 ci+2
+// of the replica's class table: class 1), the class-1 forces in accumulators of their own
+// (fi[3..5], gj[3..5], rotated like the class-2 ones) and the class-1 energy in ea.
+template <bool MINIMG, bool COUNT>
+__device__ __forceinline__ void tile_split(const MixStage& S, const float2* __restrict__ s_lj, int row,
+                                           float4 pi, unsigned m, int lane, float bx, float by, float bz,
+                                           float ibx, float iby, float ibz, float rc2, float zb, float zf,
+                                           float zc, float (&fi)[6], float (&gj)[6], double& te, double& tl,
+                                           int& tn, unsigned trow, double& ea) {
+  const unsigned full = 0xffffffffu;
+  const int src = (lane + 1) & 31;
+#pragma unroll 1
+  for (int k0 = 0; k0 < 32; k0 += 8) {
+    const float4* __restrict__ sp = S.pos + lane + k0;
+    const int* __restrict__ st = S.typ + lane + k0;
+    const unsigned mk = m >> k0;
+    float te8 = 0.f, tl8 = 0.f, ea8 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float4 pj = sp[k];
+      const int tjr = st[k];
+      float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      if (MINIMG) {
+        dx = fmaf(-bx, rint1(dx * ibx), dx);
+        dy = fmaf(-by, rint1(dy * iby), dy);
+        dz = fmaf(-bz, rint1(dz * ibz), dz);
+      }
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      const bool in = ((mk >> k) & 1u) && r2 <= rc2;
+      const float rinv = rsqrt_ftz(in ? r2 : 1.f);
+      const float r2inv = rinv * rinv;
+      const float r6inv = r2inv * r2inv * r2inv;
+      const float2 lj = s_lj[row + (tjr & kTypeMask)];
+      const float qq = pi.w * pj.w;
+      const float v1 = lj.x * r6inv;
+      const float v2 = lj.y * r6inv * r6inv;
+      const float eel = qq * (rinv + fmaf(zb, r2, -zc));
+      const float elj = v2 - v1;
+      float fs = fmaf(qq, fmaf(rinv, r2inv, -zf), fmaf(12.f, v2, -6.f * v1) * r2inv);
+      const bool c1 = ((trow >> ((tjr >> kRegionShift) & 3)) & 1u) != 0u;
+      fs = in ? fs : 0.f;
+      te8 += in ? eel : 0.f;
+      tl8 += in ? elj : 0.f;
+      ea8 += (in && c1) ? eel + elj : 0.f;
+      const float fs1 = c1 ? fs : 0.f, fs2 = fs - fs1;
+      const float ax = dx * fs2, ay = dy * fs2, az = dz * fs2;
+      const float bxf = dx * fs1, byf = dy * fs1, bzf = dz * fs1;
+      fi[0] -= ax; fi[1] -= ay; fi[2] -= az;
+      fi[3] -= bxf; fi[4] -= byf; fi[5] -= bzf;
+      gj[0] += ax; gj[1] += ay; gj[2] += az;
+      gj[3] += bxf; gj[4] += byf; gj[5] += bzf;
+      if (COUNT) tn += in ? 1 : 0;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) gj[q] = __shfl_sync(full, gj[q], src);
+    }
+    te += (double)te8;
+    tl += (double)tl8;
+    ea += (double)ea8;
+  }
+}
+
+template <bool COUNT, bool ALSD, bool CMM, bool SPLIT = false>
 __global__ void __launch_bounds__(kPairThreads, 2)
 k_pair_mixed(DevPtrs P, ZdConst z) {
   extern __shared__ float2 s_lj[];
@@ -394,11 +458,13 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
   int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
   float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
   long long gix = 0, giy = 0, giz = 0;
+  long long gix1 = 0, giy1 = 0, giz1 = 0;   // partial McMD: class-1 i forces
   long long eel = 0, elj = 0, eaa = 0, eab = 0;
   long long npair = 0;
   bool mi = true;
   float bx = 0.f, by = 0.f, bz = 0.f, ibx = 0.f, iby = 0.f, ibz = 0.f;
-  float f1 = 1.f, f2 = 1.f;
+  float f0 = 1.f, f1 = 1.f, f2 = 1.f;
+  unsigned tab = 0u;
 
   int t = claim(), tn = T;
   Gather G;
@@ -438,7 +504,13 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
         atomic_add_ll(&P.frc[3 * ai + 1], giy);
         atomic_add_ll(&P.frc[3 * ai + 2], giz);
       }
+      if (SPLIT && ai >= 0 && (gix1 | giy1 | giz1)) {
+        atomic_add_ll(&P.frc1[3 * ai + 0], gix1);
+        atomic_add_ll(&P.frc1[3 * ai + 1], giy1);
+        atomic_add_ll(&P.frc1[3 * ai + 2], giz1);
+      }
       gix = giy = giz = 0;
+      gix1 = giy1 = giz1 = 0;
       cur_bi = bi;
       const int si = bi * kTile + lane;
       pi = P.pos_f[si];
@@ -455,14 +527,24 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
         ibx = (float)R.invbox[0]; iby = (float)R.invbox[1]; ibz = (float)R.invbox[2];
         if (ALSD) {
           const double lam = P.lam[2 * rep];
-          f1 = (float)lam_factor(R.lam_mode, lam, 1);
-          f2 = (float)lam_factor(R.lam_mode, lam, 0);
+          f0 = (float)cls_weight(R, lam, 2);
+          f1 = (float)cls_weight(R, lam, 1);
+          f2 = (float)cls_weight(R, lam, 0);
         }
-        // Per-pair minimum image is needed only if a listed pair could reach half a box
-        // length: |d| <= rlim + 2*(h_i + h_j) + motion since the build (2 A margin).
+        if (SPLIT) tab = R.split ? R.cls_tab : 0u;
+        // Per-pair minimum image is needed only where a pair within the cut-off can have
+        // another image than its tile's.  Per axis the tile's image puts the two block
+        // references at most box/2 apart, and a pair's separation differs from theirs by at
+        // most h_i + h_j <= 2 h_max plus the atoms' motion since the build (2 A margin), so
+        // in the tile's image |d| <= box/2 + 2 h_max + 2; in any other image |d| >= box - rc.
+        // Both hold at once only if box/2 <= rc + 2 h_max + 2.  CMM (no cut-off): the
+        // farthest near-field pair rlim in place of rc, with twice the block margin.
         mi = false;
-        for (int k = 0; k < 3; ++k)
-          if (0.5 * R.box[k] < z.rlim + 4.0 * (double)P.rep_hmax[3 * rep + k] + 2.0) mi = true;
+        for (int k = 0; k < 3; ++k) {
+          const double h = (double)P.rep_hmax[3 * rep + k];
+          const double reach = CMM ? z.rlim + 4.0 * h : sqrt(z.rc2) + 2.0 * h;
+          if (0.5 * R.box[k] < reach + 2.0) mi = true;
+        }
       }
     }
     __syncwarp();
@@ -477,19 +559,30 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     if (tn < T) fetch(tn, b ^ 1, Gn);
     float gjx = 0.f, gjy = 0.f, gjz = 0.f;
     float fix = 0.f, fiy = 0.f, fiz = 0.f;
+    float fi6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, gj6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     double te = 0.0, tl = 0.0, ea = 0.0, eb = 0.0;
     int tn_pairs = 0;
     const int ci = ALSD ? (ti >> 30) : 0;
     const int row = (ALSD ? (ti & kTypeMask) : ti) * z.nt1;
-    if (ALSD || CMM) {
+    if (SPLIT) {
+      const unsigned trow = tab >> (3 * ((ti >> kRegionShift) & 3));
+      if (mi)
+        tile_split<true, COUNT>(S, s_lj, row, pi, m, lane, bx, by, bz, ibx, iby, ibz, rc2, zb, zf, zc, fi6,
+                                gj6, te, tl, tn_pairs, trow, ea);
+      else
+        tile_split<false, COUNT>(S, s_lj, row, pi, m, lane, bx, by, bz, ibx, iby, ibz, rc2, zb, zf, zc, fi6,
+                                 gj6, te, tl, tn_pairs, trow, ea);
+      fix = fi6[0]; fiy = fi6[1]; fiz = fi6[2];
+      gjx = gj6[0]; gjy = gj6[1]; gjz = gj6[2];
+    } else if (ALSD || CMM) {
       if (mi)
         tile_mixed<true, COUNT, ALSD, CMM>(S, s_lj, row, pi, m, me, lane, bx, by, bz, ibx, iby, ibz, rc2, zb,
-                                           zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci, f1,
-                                           f2, ea, eb);
+                                           zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci, f0,
+                                           f1, f2, ea, eb);
       else
         tile_mixed<false, COUNT, ALSD, CMM>(S, s_lj, row, pi, m, me, lane, bx, by, bz, ibx, iby, ibz, rc2,
                                             zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci,
-                                            f1, f2, ea, eb);
+                                            f0, f1, f2, ea, eb);
     } else if (mi) {
       tile_mixed2<true, COUNT>(S, s_lj, row, pi, m, lane, bx, by, bz, ibx, iby, ibz, rc2, zb, zf, zc, fix,
                                fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs);
@@ -505,6 +598,16 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     gix += to_fix((double)fix, kFrcScale, P.status);
     giy += to_fix((double)fiy, kFrcScale, P.status);
     giz += to_fix((double)fiz, kFrcScale, P.status);
+    if (SPLIT) {
+      if (aj >= 0 && (gj6[3] != 0.f || gj6[4] != 0.f || gj6[5] != 0.f)) {
+        atomic_add_ll(&P.frc1[3 * aj + 0], to_fix((double)gj6[3], kFrcScale, P.status));
+        atomic_add_ll(&P.frc1[3 * aj + 1], to_fix((double)gj6[4], kFrcScale, P.status));
+        atomic_add_ll(&P.frc1[3 * aj + 2], to_fix((double)gj6[5], kFrcScale, P.status));
+      }
+      gix1 += to_fix((double)fi6[3], kFrcScale, P.status);
+      giy1 += to_fix((double)fi6[4], kFrcScale, P.status);
+      giz1 += to_fix((double)fi6[5], kFrcScale, P.status);
+    }
     eel += to_fix(te, kEneScale, P.status);
     elj += to_fix(tl, kEneScale, P.status);
     if (ALSD) {
@@ -522,6 +625,11 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     atomic_add_ll(&P.frc[3 * ai + 1], giy);
     atomic_add_ll(&P.frc[3 * ai + 2], giz);
   }
+  if (SPLIT && ai >= 0 && (gix1 | giy1 | giz1)) {
+    atomic_add_ll(&P.frc1[3 * ai + 0], gix1);
+    atomic_add_ll(&P.frc1[3 * ai + 1], giy1);
+    atomic_add_ll(&P.frc1[3 * ai + 2], giz1);
+  }
   flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
   // a copy still in flight (only after a timed-out wait) must land before the block exits
   for (int k = 0; k < 2; ++k)
@@ -534,7 +642,7 @@ struct __align__(16) F64Stage {
   int typ[64];
 };
 
-template <bool COUNT, bool ALSD, bool CMM>
+template <bool COUNT, bool ALSD, bool CMM, bool SPLIT = false>
 __global__ void __launch_bounds__(kPairThreads)
 k_pair_fp64(DevPtrs P, ZdConst z) {
   extern __shared__ double2 s_ljd[];
@@ -549,10 +657,12 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
   int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
   double4 pi = make_double4(0, 0, 0, 0);
   double gix = 0, giy = 0, giz = 0;
+  double gix1 = 0, giy1 = 0, giz1 = 0;            // partial McMD: class-1 i forces
   long long eel = 0, elj = 0, eaa = 0, eab = 0;   // fixed point, per tile
   long long npair = 0;
   double bx = 0, by = 0, bz = 0, ibx = 0, iby = 0, ibz = 0;
-  double f1 = 1.0, f2 = 1.0;
+  double f0 = 1.0, f1 = 1.0, f2 = 1.0;
+  unsigned tab = 0u;
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(P.tile_ctr, 1);
@@ -564,8 +674,14 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
         atomicAdd(&P.grd[3 * ai + 0], gix);
         atomicAdd(&P.grd[3 * ai + 1], giy);
         atomicAdd(&P.grd[3 * ai + 2], giz);
+        if (SPLIT) {
+          atomicAdd(&P.grd1[3 * ai + 0], gix1);
+          atomicAdd(&P.grd1[3 * ai + 1], giy1);
+          atomicAdd(&P.grd1[3 * ai + 2], giz1);
+        }
       }
       gix = giy = giz = 0;
+      gix1 = giy1 = giz1 = 0;
       cur_bi = bi;
       const int s = cur_bi * kTile + lane;
       pi = P.pos_d[s];
@@ -581,9 +697,11 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
         bx = R.box[0]; by = R.box[1]; bz = R.box[2];
         ibx = R.invbox[0]; iby = R.invbox[1]; ibz = R.invbox[2];
         if (ALSD) {
-          f1 = lam_factor(R.lam_mode, P.lam[2 * rep], 1);
-          f2 = lam_factor(R.lam_mode, P.lam[2 * rep], 0);
+          f0 = cls_weight(R, P.lam[2 * rep], 2);
+          f1 = cls_weight(R, P.lam[2 * rep], 1);
+          f2 = cls_weight(R, P.lam[2 * rep], 0);
         }
+        if (SPLIT) tab = R.split ? R.cls_tab : 0u;
       }
     }
     const unsigned m = P.ct_mask[(size_t)t * 32 + lane];
@@ -600,7 +718,9 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
     __syncwarp();
     const int row = (ALSD ? (ti & kTypeMask) : ti) * z.nt1;
     const int ci = ALSD ? (ti >> 30) : 0;
+    const unsigned trow = SPLIT ? tab >> (3 * ((ti >> kRegionShift) & 3)) : 0u;
     double gjx = 0, gjy = 0, gjz = 0;
+    double gjx1 = 0, gjy1 = 0, gjz1 = 0;
     int tn = 0;
     double te = 0.0, tl = 0.0, ta = 0.0, tb = 0.0;   // this tile's energies
     const int src = (lane + 1) & 31;
@@ -627,25 +747,45 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
           const double v2 = lj.y * dd6i * dd6i;
           tl += -v1 + v2;
           double cc = ee * (dd2i * ddi - z.fcoeff) + (-6.0 * v1 + 12.0 * v2) * dd2i;
-          if (ALSD) {
+          bool c1 = false;
+          if (SPLIT) {   // partial McMD: class 1 by the regions of the two atoms
+            c1 = ((trow >> ((tj >> kRegionShift) & 3)) & 1u) != 0u;
+            if (c1) ta += epair + (-v1 + v2);
+          } else if (ALSD) {
             const int na = ci + (tj >> 30);
             if (na == 2) { ta += epair + (-v1 + v2); cc *= f2; }
             else if (na == 1) { tb += epair + (-v1 + v2); cc *= f1; }
+            else cc *= f0;
           }
           const double fx = dx * cc, fy = dy * cc, fz = dz * cc;
-          gix -= fx; giy -= fy; giz -= fz;
-          gjx += fx; gjy += fy; gjz += fz;
+          if (SPLIT && c1) {
+            gix1 -= fx; giy1 -= fy; giz1 -= fz;
+            gjx1 += fx; gjy1 += fy; gjz1 += fz;
+          } else {
+            gix -= fx; giy -= fy; giz -= fz;
+            gjx += fx; gjy += fy; gjz += fz;
+          }
           if (COUNT && elp) ++tn;
         }
       }
       gjx = __shfl_sync(0xffffffffu, gjx, src);
       gjy = __shfl_sync(0xffffffffu, gjy, src);
       gjz = __shfl_sync(0xffffffffu, gjz, src);
+      if (SPLIT) {
+        gjx1 = __shfl_sync(0xffffffffu, gjx1, src);
+        gjy1 = __shfl_sync(0xffffffffu, gjy1, src);
+        gjz1 = __shfl_sync(0xffffffffu, gjz1, src);
+      }
     }
     if (aj >= 0 && (gjx != 0.0 || gjy != 0.0 || gjz != 0.0)) {
       atomicAdd(&P.grd[3 * aj + 0], gjx);
       atomicAdd(&P.grd[3 * aj + 1], gjy);
       atomicAdd(&P.grd[3 * aj + 2], gjz);
+    }
+    if (SPLIT && aj >= 0 && (gjx1 != 0.0 || gjy1 != 0.0 || gjz1 != 0.0)) {
+      atomicAdd(&P.grd1[3 * aj + 0], gjx1);
+      atomicAdd(&P.grd1[3 * aj + 1], gjy1);
+      atomicAdd(&P.grd1[3 * aj + 2], gjz1);
     }
     if (COUNT) npair += tn;
     eel += to_fix(te, kEneScale, P.status);
@@ -656,6 +796,11 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
     atomicAdd(&P.grd[3 * ai + 0], gix);
     atomicAdd(&P.grd[3 * ai + 1], giy);
     atomicAdd(&P.grd[3 * ai + 2], giz);
+    if (SPLIT) {
+      atomicAdd(&P.grd1[3 * ai + 0], gix1);
+      atomicAdd(&P.grd1[3 * ai + 1], giy1);
+      atomicAdd(&P.grd1[3 * ai + 2], giz1);
+    }
   }
   flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
 }
@@ -671,11 +816,14 @@ int pair_blocks_per_sm(bool fp64, int nt1) {
   return per > 0 ? per : 1;
 }
 
-void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool, bool count, bool alsd,
+void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, bool alsd, bool split,
                        cudaStream_t st) {
   const int nb = (nwarps + kPairWarps - 1) / kPairWarps;
   const size_t sh = sizeof(float2) * z.nt1 * z.nt1;
-  if (z.cmm) {
+  if (split) {
+    if (count) k_pair_mixed<true, true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_mixed<false, true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+  } else if (z.cmm) {
     if (count) k_pair_mixed<true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
     else k_pair_mixed<false, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
   } else if (alsd) {
@@ -687,11 +835,14 @@ void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool, boo
   }
 }
 
-void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, bool alsd,
+void launch_pair_fp64(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, bool alsd, bool split,
                       cudaStream_t st) {
   const int nb = (nwarps + kPairWarps - 1) / kPairWarps;
   const size_t sh = sizeof(double2) * z.nt1 * z.nt1;
-  if (z.cmm) {
+  if (split) {
+    if (count) k_pair_fp64<true, true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+    else k_pair_fp64<false, true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
+  } else if (z.cmm) {
     if (count) k_pair_fp64<true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
     else k_pair_fp64<false, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
   } else if (alsd) {

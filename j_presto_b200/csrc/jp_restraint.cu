@@ -25,7 +25,8 @@ __device__ __forceinline__ void res_image(const Rep& R, double* d) {
 }
 
 template <bool FP64>
-__device__ __forceinline__ void res_dist(const DevPtrs& P, const Rep& R, const Restr& Q, double& e) {
+__device__ __forceinline__ void res_dist(const DevPtrs& P, const Rep& R, const Restr& Q, double& e,
+                                         double wg) {
   const double* x = P.x;
   const int* idx = P.res_idx;
   const int n = (Q.a[1] - Q.a[0]) * (Q.a[3] - Q.a[2]);
@@ -65,13 +66,14 @@ __device__ __forceinline__ void res_dist(const DevPtrs& P, const Rep& R, const R
         const double r8i = 1.0 / (r2 * r2);
         for (int kk = 0; kk < 3; ++kk) td[kk] += d[kk] * r8i;
       }
-      add_grad<FP64>(P, coef, idx[p], td[0], td[1], td[2]);
+      add_grad<FP64>(P, coef * wg, idx[p], td[0], td[1], td[2]);
     }
   }
 }
 
 template <bool FP64>
-__device__ __forceinline__ void res_dihe(const DevPtrs& P, const Rep& R, const Restr& Q, double& e) {
+__device__ __forceinline__ void res_dihe(const DevPtrs& P, const Rep& R, const Restr& Q, double& e,
+                                         double wg) {
   constexpr double kTwoPi = 2.0 * 3.141592653589793;
   const double* x = P.x;
   double d21[3], d32[3], d43[3];
@@ -127,10 +129,10 @@ __device__ __forceinline__ void res_dihe(const DevPtrs& P, const Rep& R, const R
   w[6] = d32[2] * p12[1] - d32[1] * p12[2] - q23 * (d32[2] * p23[1] - d32[1] * p23[2]);
   w[7] = d32[0] * p12[2] - d32[2] * p12[0] - q23 * (d32[0] * p23[2] - d32[2] * p23[0]);
   w[8] = d32[1] * p12[0] - d32[0] * p12[1] - q23 * (d32[1] * p23[0] - d32[0] * p23[1]);
-  add_grad<FP64>(P, wr, Q.a[0], w[0], w[1], w[2]);
-  add_grad<FP64>(P, wr, Q.a[1], w[3], w[4], w[5]);
-  add_grad<FP64>(P, wr, Q.a[2], -(w[0] + w[3] + w[6]), -(w[1] + w[4] + w[7]), -(w[2] + w[5] + w[8]));
-  add_grad<FP64>(P, wr, Q.a[3], w[6], w[7], w[8]);
+  add_grad<FP64>(P, wr * wg, Q.a[0], w[0], w[1], w[2]);
+  add_grad<FP64>(P, wr * wg, Q.a[1], w[3], w[4], w[5]);
+  add_grad<FP64>(P, wr * wg, Q.a[2], -(w[0] + w[3] + w[6]), -(w[1] + w[4] + w[7]), -(w[2] + w[5] + w[8]));
+  add_grad<FP64>(P, wr * wg, Q.a[3], w[6], w[7], w[8]);
 }
 
 // one CAP term of a group centre or an atom: c = position - centre, xa = what the box walls
@@ -191,22 +193,25 @@ __global__ void __launch_bounds__(kResThreads) k_restraints(DevPtrs P, int n, in
     rep = Q.rep;
     const Rep& R = P.reps[rep];
     const double* x = P.x;
+    // restraint gradients are class BB / class 2 (grad(:,:,nfrg)): weight 1, or the BB weight
+    // while an ALSD replica's per-class outputs are evaluated
+    const double wg = R.cls_over ? R.cls_w[2] : 1.0;
     switch (Q.kind) {
       case R_POS: {
         double d[3];
         for (int k = 0; k < 3; ++k) d[k] = x[3 * Q.a[0] + k] - Q.p[k];
         res_image(R, d);
         e = 0.5 * Q.p[3] * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-        add_grad<FP64>(P, Q.p[3], Q.a[0], d[0], d[1], d[2]);
+        add_grad<FP64>(P, Q.p[3] * wg, Q.a[0], d[0], d[1], d[2]);
         break;
       }
       case R_DIST:
         slot = JP_E_DISTRES;
-        res_dist<FP64>(P, R, Q, e);
+        res_dist<FP64>(P, R, Q, e, wg);
         break;
       case R_DIHE:
         slot = JP_E_DIHERES;
-        res_dihe<FP64>(P, R, Q, e);
+        res_dihe<FP64>(P, R, Q, e, wg);
         break;
       case R_CAPG: {   // centre of mass of atoms a[0] .. a[1]; p[5] = 1 / their mass
         slot = JP_E_CAP;
@@ -216,7 +221,7 @@ __global__ void __launch_bounds__(kResThreads) k_restraints(DevPtrs P, int n, in
         for (int k = 0; k < 3; ++k) c[k] = c[k] * Q.p[5] - Q.p[k];
         if (cap_term(Q, Q.a[2], c, c, e, g))
           for (int a = Q.a[0]; a <= Q.a[1]; ++a)
-            add_grad<FP64>(P, Q.p[5] * P.mass[a], a, g[0], g[1], g[2]);
+            add_grad<FP64>(P, Q.p[5] * P.mass[a] * wg, a, g[0], g[1], g[2]);
         break;
       }
       case R_CAPA: {
@@ -226,7 +231,7 @@ __global__ void __launch_bounds__(kResThreads) k_restraints(DevPtrs P, int n, in
           xa[k] = x[3 * Q.a[0] + k];
           c[k] = xa[k] - Q.p[k];
         }
-        if (cap_term(Q, Q.a[1], c, xa, e, g)) add_grad<FP64>(P, 1.0, Q.a[0], g[0], g[1], g[2]);
+        if (cap_term(Q, Q.a[1], c, xa, e, g)) add_grad<FP64>(P, wg, Q.a[0], g[0], g[1], g[2]);
         break;
       }
     }

@@ -25,7 +25,7 @@ EXPORTS = ["jp_default_params", "jp_create", "jp_rebuild_cells", "jp_energy_grad
            "jp_mlp_nparam", "jp_mlp_init", "jp_mlp_train", "jp_mlp_forward", "jp_ge_set_mlp",
            "jp_get_lambda", "jp_set_lambda", "jp_set_grid_limit", "jp_default_min_params",
            "jp_minimize", "jp_set_wait_limit", "jp_step_io", "jp_tile_shape", "jp_alsd_hist_setup",
-           "jp_alsd_hist_get", "jp_alsd_set_mlp"]
+           "jp_alsd_hist_get", "jp_alsd_set_mlp", "jp_energy_grad_cls"]
 
 
 class JpError(RuntimeError):
@@ -48,6 +48,7 @@ def lib():
         L.jp_create.argtypes = [C.POINTER(abi.JpSystem), ip, C.POINTER(abi.JpParams), C.POINTER(vp)]
         L.jp_rebuild_cells.argtypes = [vp, ip]
         L.jp_energy_grad.argtypes = [vp, ip, dp, dp, dp]
+        L.jp_energy_grad_cls.argtypes = [vp, ip, dp, dp, dp, dp, C.POINTER(C.c_int32)]
         L.jp_step.argtypes = [vp, ip, dp, dp]
         L.jp_step_io.argtypes = [vp, ip, dp, dp, dp, dp, dp, dp]
         L.jp_shake.argtypes = [vp, ip, dp, dp]
@@ -261,6 +262,20 @@ class Engine:
         g = np.zeros((n, 3))
         _chk(lib().jp_energy_grad(self._h, rep, _dp(c), _dp(e), _dp(g)), "jp_energy_grad")
         return e, g
+
+    def energy_grad_cls(self, rep=0, cord=None):
+        """dnergy's outputs by class: (eneval, class totals [nfrg], unscaled class gradients
+        [nfrg, natom, 3]); nfrg = 1 without cluster atoms, 3 for ALSD (AA, AB, BB), 2 for
+        GEPSME= AND / OR / XOR (classes 1, 2)."""
+        n = self.natoms[rep]
+        c = None if cord is None else np.ascontiguousarray(cord, np.float64)
+        e = np.zeros(abi.JP_MAXENE)
+        ec = np.zeros(3)
+        g = np.zeros((3, n, 3))
+        nf = C.c_int32(0)
+        _chk(lib().jp_energy_grad_cls(self._h, rep, _dp(c), _dp(e), _dp(ec), _dp(g), C.byref(nf)),
+             "jp_energy_grad_cls")
+        return e, ec[:nf.value].copy(), g[:nf.value].copy()
 
     # ---- McMD iteration ----
     def ge_hist_setup(self, emin, emax, nbin, nbor, rep=-1):

@@ -43,6 +43,7 @@ def lib():
         L.or_dof.argtypes = [vp]
         L.or_dof.restype = C.c_int
         L.or_energy_grad.argtypes = [vp, dp, dp, dp]
+        L.or_energy_grad_cls.argtypes = [vp, dp, dp, dp, dp]
         L.or_shake.argtypes = [vp, dp, dp]
         L.or_temperature.argtypes = [vp, dp]
         L.or_temperature.restype = C.c_double
@@ -113,6 +114,16 @@ class Oracle:
         g = np.zeros((self.n, 3))
         lib().or_energy_grad(self._h, _dp(c), _dp(e), _dp(g))
         return e, g
+
+    def energy_grad_cls(self, cord=None):
+        """dnergy's per-class outputs: (eneval, class totals [nfrg], unscaled gradients
+        [nfrg, natom, 3]); nfrg = 1 without clusters, 3 for ALSD, 2 for GEPSME= AND/OR/XOR."""
+        c = None if cord is None else np.ascontiguousarray(cord, np.float64)
+        e = np.zeros(abi.JP_MAXENE)
+        ec = np.zeros(3)
+        g = np.zeros((3, self.n, 3))
+        nfrg = lib().or_energy_grad_cls(self._h, _dp(c), _dp(e), _dp(ec), _dp(g))
+        return e, ec[:nfrg].copy(), g[:nfrg].copy()
 
     def shake(self, r1, r2):
         r1 = np.ascontiguousarray(r1, np.float64).copy()

@@ -94,8 +94,21 @@ struct Ctx {
   int ifg_lambda = -1;                // sub-system carrying lambda's degree of freedom
   double ecls[3] = {0.0, 0.0, 0.0};   // class energies (unscaled) of the last force call
   double dself_cls[3] = {0.0, 0.0, 0.0};
-  int pcls(int a, int b) const { return alsd ? 2 - inA[a] - inA[b] : 2; }
+  // ---- partial McMD (GEPSME= AND / OR / XOR, nfrg = 2: inpcls.f90:160-183, :298-325;
+  // verlet.f90:118-142, verlethe.f90:170-238) ----
+  int geps = 0;                       // JP_GEPS_*; 0 = none
+  bool split = false;                 // geps with cluster atoms: classes 1 and 2 kept apart
+  std::vector<int> icl;               // region code: 0 = A (CLUSTA), 1 = B (CLUSTB), 2 = neither
+  unsigned tab1 = 0;                  // bit 3 ca + cb set: n_matrix of the regions = 1
+  int pcls(int a, int b) const {      // slot of a term's class: 0 AA / class 1, 1 AB, 2 BB / class 2
+    if (split) return ((tab1 >> (3 * icl[a] + icl[b])) & 1u) ? 0 : 2;
+    return alsd ? 2 - inA[a] - inA[b] : 2;
+  }
+  // the class weights can be set to one class at a time (per-class gradients)
+  bool fover = false;
+  double fo[3] = {1.0, 1.0, 1.0};
   void factors(double* f) const {     // class weights of the gradient
+    if (fover) { f[0] = fo[0]; f[1] = fo[1]; f[2] = fo[2]; return; }
     if (alsd == JP_ALSD_LMD) { f[0] = lam * lam; f[1] = lam; f[2] = 1.0; }
     else if (alsd == JP_ALSD_LMD2) { f[0] = lam; f[1] = std::sqrt(lam); f[2] = 1.0; }
     else { f[0] = f[1] = f[2] = 1.0; }
@@ -858,7 +871,13 @@ void energy_grad(Ctx& c, const double* x, double* ene, double* grad) {
     }
   }
 
-  restraints(c, x, ene, grad);
+  if (f[2] == 1.0) {
+    restraints(c, x, ene, grad);
+  } else {   // restraint gradients belong to the last class (grad(:,:,nfrg))
+    std::vector<double> rg((size_t)3 * n, 0.0);
+    restraints(c, x, ene, rg.data());
+    for (int k = 0; k < 3 * n; ++k) grad[k] += f[2] * rg[k];
+  }
 
   // ZD + LJ pair loop: enear_ZD_redu_PB (enear.f90:107-257, #ZD #REDU #PB lines),
   // per-thread gradient copies stand in for the OpenMP reduction(+:Tgrad).
@@ -1298,14 +1317,20 @@ inline int remotv_code(int ier) { return ier == -1 ? JP_E_STOP_MASS : JP_E_STOP_
 
 // One verlet step (verlet.f90:2-226), METHOD= MICR or CONS: pseudo-temperature force scale,
 // velocity update, centre-of-mass stop, Berendsen scaling (scalet.f90), positions, SHAKE.
+void split_force(Ctx& c, double* ene);
+
 int step_verlet(Ctx& c, double* ene) {
   const int n = c.n;
   std::vector<double> x0(c.cord);
   const bool cons = c.prm.method == JP_METHOD_CONS;
   const double tempc = cons ? caltmp(c, c.vel.data()) : 0.0;   // T of v(t-dt/2), verlet.f90:31-34
-  energy_grad(c, c.cord.data(), ene, c.grad.data());
-  if (c.prm.psetmp > kEps)   // verlet.f90:118-142
-    for (auto& g : c.grad) g *= c.prm.temp / c.prm.psetmp;
+  if (c.split) {
+    split_force(c, ene);
+  } else {
+    energy_grad(c, c.cord.data(), ene, c.grad.data());
+    if (c.prm.psetmp > kEps)   // verlet.f90:118-142
+      for (auto& g : c.grad) g *= c.prm.temp / c.prm.psetmp;
+  }
   const double dt = c.prm.dt;
   double rt = -dt * kConvcv;
   for (int i = 0; i < n; ++i)
@@ -1335,8 +1360,34 @@ int step_verlet(Ctx& c, double* ene) {
 // temperature (CANO), the McMD weight (GE) or the ALSD class combination (done inside
 // energy_grad) with the lambda force; c.grad gets the gradient the integration uses, the
 // return value is lambda_f.  This is the state that FDEBUG dumps (verlethe.f90:325-387).
+// partial McMD: the class-1 gradient into g1 and the class-2 gradient into g2, from two
+// evaluations with the class weights set to one class each (the energies do not depend on
+// them; c.ecls holds the class totals afterwards)
+void split_eval(Ctx& c, double* ene, double* g1, double* g2) {
+  c.fover = true;
+  c.fo[0] = 1.0; c.fo[1] = 0.0; c.fo[2] = 0.0;
+  energy_grad(c, c.cord.data(), ene, g1);
+  c.fo[0] = 0.0; c.fo[2] = 1.0;
+  energy_grad(c, c.cord.data(), ene, g2);
+  c.fover = false;
+}
+
+// grad(:,:,2) = grad(:,:,1) * dew + grad(:,:,2) (verlet.f90:130-141, verlethe.f90:176-187,
+// :223-234): dew the McMD weight of the class-1 energy epotcc(1,1) (METHOD= GE) or
+// SETTEM / PSETMP
+void split_force(Ctx& c, double* ene) {
+  std::vector<double> g2(c.grad.size());
+  split_eval(c, ene, c.grad.data(), g2.data());
+  const double dew = c.prm.method == JP_METHOD_GE ? mcmd_scale(c, c.ecls[0]) : c.prm.temp / c.prm.psetmp;
+  for (size_t k = 0; k < g2.size(); ++k) c.grad[k] = c.grad[k] * dew + g2[k];
+}
+
 double verlethe_force(Ctx& c, double* ene) {
   double lambda_f = 0.0;
+  if (c.split) {
+    split_force(c, ene);
+    return lambda_f;
+  }
   energy_grad(c, c.cord.data(), ene, c.grad.data());
   if (c.alsd) {
     // forces already combined by class (energy_grad); lambda force (verlethe.f90:289-320)
@@ -1530,16 +1581,42 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
   c->typ.resize(n);
   for (int i = 0; i < n; ++i) c->typ[i] = s->atype[i] - b;
   c->mol.assign(n, 0);
-  c->alsd = (prm->alsd != JP_ALSD_NONE && s->cluster) ? prm->alsd : 0;
+  c->alsd = ((prm->alsd == JP_ALSD_LMD || prm->alsd == JP_ALSD_LMD2) && s->cluster) ? prm->alsd : 0;
   c->inA.assign(n, 0);
   if (c->alsd)
     for (int i = 0; i < n; ++i) c->inA[i] = s->cluster[i] ? 1 : 0;
+  c->geps = (prm->alsd >= JP_GEPS_AND && prm->alsd <= JP_GEPS_XOR) ? prm->alsd : 0;
+  c->icl.assign(n, 2);
+  if (c->geps && s->cluster) {
+    bool hasA = false, hasB = false;
+    for (int i = 0; i < n; ++i) {
+      if (s->cluster[i] == 1) { c->icl[i] = 0; hasA = true; }
+      else if (s->cluster[i] == 2) { c->icl[i] = 1; hasB = true; }
+    }
+    c->split = hasA || hasB;   // nfrag > 1, nfrg = 2
+    // n_matrix(icls_a, icls_b) = 1 (inpcls.f90:298-325) on the region codes A 0, B 1,
+    // neither 2; without region B the nfrag = 2 matrix (A, the rest)
+    auto bit = [](int a, int b) { return (1u << (3 * a + b)) | (1u << (3 * b + a)); };
+    unsigned t = 0;
+    if (!hasB) {
+      if (c->geps == JP_GEPS_AND) t = bit(0, 0);
+      else if (c->geps == JP_GEPS_OR) t = bit(0, 0) | bit(0, 2);
+      else t = bit(0, 2);
+    } else {
+      if (c->geps == JP_GEPS_AND) t = bit(0, 0) | bit(1, 1);
+      else if (c->geps == JP_GEPS_OR) t = bit(0, 0) | bit(0, 1);
+      else t = bit(0, 1);
+    }
+    c->tab1 = t;
+  }
   if (s->molecule && prm->tempco == 2) {
     // sub-system ids renumbered densely in order, empty ids removed (md.f90:133-151);
     // with clusters each molecule splits into its cluster and non-cluster part (ixamol2)
     std::vector<int> ids;
     for (int i = 0; i < n; ++i)
-      ids.push_back(c->alsd ? 2 * (s->molecule[i] - b) + (c->inA[i] ? 0 : 1) : s->molecule[i] - b);
+      ids.push_back(c->alsd    ? 2 * (s->molecule[i] - b) + (c->inA[i] ? 0 : 1)
+                    : c->split ? 3 * (s->molecule[i] - b) + c->icl[i]
+                               : s->molecule[i] - b);
     std::vector<int> u(ids);
     std::sort(u.begin(), u.end());
     u.erase(std::unique(u.begin(), u.end()), u.end());
@@ -1662,6 +1739,10 @@ void* or_create(const jp_system* s, const jp_params* prm, int nthreads) {
       int na = 0;
       for (int k = 0; k < 4; ++k) na += c->inA[t.a[k]];
       t.cls = na == 4 ? 0 : (na > 0 ? 1 : 2);
+    } else if ((prm->scale_terms & JP_SCALE_IMPR) && c->split) {
+      int lo = 2, hi = 0;
+      for (int k = 0; k < 4; ++k) { lo = std::min(lo, c->icl[t.a[k]]); hi = std::max(hi, c->icl[t.a[k]]); }
+      t.cls = ((c->tab1 >> (3 * lo + hi)) & 1u) ? 0 : 2;
     }
     c->imprs.push_back(t);
   }
@@ -1844,6 +1925,27 @@ int or_energy_grad(void* h, const double* cord, double* ene, double* grad) {
 
 // CMM state of level l (1-based): returns nv (0 without CMM); pot [nv^3][13], pop [nv^3],
 // cen [nv][3] (each nullable).  Test hook.
+// dnergy's per-class outputs: enevcc(1, 1:nfrg) and grad(3, N, 1:nfrg) (unscaled), one
+// evaluation per class with the class weights set to that class; returns nfrg
+int or_energy_grad_cls(void* h, const double* cord, double* ene, double* ecls, double* grad) {
+  Ctx& c = *(Ctx*)h;
+  if (cord) std::copy(cord, cord + 3 * c.n, c.cord.begin());
+  const int nfrg = c.alsd ? 3 : c.split ? 2 : 1;
+  const int slot[3][3] = {{2, 2, 2}, {0, 2, 2}, {0, 1, 2}};
+  std::vector<double> g((size_t)3 * c.n);
+  for (int q = 0; q < nfrg; ++q) {
+    const int k = slot[nfrg - 1][q];
+    c.fover = true;
+    for (int z = 0; z < 3; ++z) c.fo[z] = z == k ? 1.0 : 0.0;
+    if (nfrg == 1) c.fo[0] = c.fo[1] = c.fo[2] = 1.0;
+    energy_grad(c, c.cord.data(), ene, g.data());
+    c.fover = false;
+    if (ecls) ecls[q] = nfrg == 1 ? ene[JP_E_TOTAL] : c.ecls[k];
+    if (grad) std::copy(g.begin(), g.end(), grad + (size_t)q * 3 * c.n);
+  }
+  return nfrg;
+}
+
 int or_cmm_level(void* h, int l, double* pot, int* pop, double* cen) {
   Ctx* c = (Ctx*)h;
   if (!c->cmm || l < 1 || l > c->nlev) return 0;

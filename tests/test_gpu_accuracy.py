@@ -3,7 +3,10 @@
 One-step energies and gradients of both paths against the FP64 oracle on
 * C1: 3,000 waters in 31 A as specified (3x liquid density: the largest forces of the set),
 * C2: the 159-residue chain in 7,000 waters (22,860 atoms),
-* C3: 33,000 waters and 200 ions in 100 A (99,200 atoms).
+* C3: 33,000 waters and 200 ions in 100 A (99,200 atoms),
+* one C5 replica: a 12-residue chain in 3,000 waters (~45 A box), just above the box at
+  which the mixed kernel stops imaging pair by pair and keeps each tile's periodic image
+  for all its pairs (box/2 > cut-off + 2 block half-extents + 2 A).
 Tolerances: FP64 path -- gradient RMS relative 1e-12, energies 1e-8 relative; mixed path --
 gradient RMS relative 1e-5 (the metric's bar) and total potential energy 1e-6 relative.
 
@@ -33,7 +36,8 @@ def eng_mod(engine_lib):
     return engine
 
 
-CONFIGS = {"c1": systems.config_c1, "c2": systems.config_c2, "c3": systems.config_c3}
+CONFIGS = {"c1": systems.config_c1, "c2": systems.config_c2, "c3": systems.config_c3,
+           "c5_replica": lambda: systems.solvated_polymer(12, 3000, seed=5000)}
 
 
 @pytest.mark.parametrize("name", sorted(CONFIGS))
