@@ -370,8 +370,11 @@ def accuracy(dev, c2_acc, c3_acc):
         x0, v0 = e.get_state()
     nsteps = 500000
     drift = {}
-    for name, prec in (("mixed", abi.JP_PREC_MIXED), ("fp64", abi.JP_PREC_FP64)):
-        with engine.Engine(top, precision=prec, method=abi.JP_METHOD_MICR, device=dev) as e:
+    # md_run's SHAKE tolerance (COVSHK 1e-6), and 1e-10 to show how much of the drift it makes
+    runs = (("mixed", abi.JP_PREC_MIXED, 1e-6), ("fp64", abi.JP_PREC_FP64, 1e-6),
+            ("mixed_covshk1e-10", abi.JP_PREC_MIXED, 1e-10), ("fp64_covshk1e-10", abi.JP_PREC_FP64, 1e-10))
+    for name, prec, tol in runs:
+        with engine.Engine(top, precision=prec, method=abi.JP_METHOD_MICR, shake_tol=tol, device=dev) as e:
             e.set_state(cord=x0, vel=v0)
             e.rebuild()
             E, T = e.step(nsteps)
@@ -391,8 +394,8 @@ def accuracy(dev, c2_acc, c3_acc):
         drift[name + "_wander_kcal"] = float(tot[skip:].std())
     acc["nve_drift_kT_per_ns_per_dof"] = {
         "workload": f"C1': 1,000 waters (3,000 atoms) in a 31 A box, 10 ps METHOD= CANO at 300 K, "
-                    f"then METHOD= MICR, SHAKE, 2 fs, {nsteps} steps ({nsteps * DT_FS / 1000:.0f} ps), "
-                    f"{dof} degrees of freedom",
+                    f"then METHOD= MICR, SHAKE (COVSHK 1e-6, md_run's default, and 1e-10), 2 fs, "
+                    f"{nsteps} steps ({nsteps * DT_FS / 1000:.0f} ps), {dof} degrees of freedom",
         **drift}
     return acc
 

@@ -266,6 +266,9 @@ struct IStage {
 // the i block's frame.  Only the i atoms within the list radius of block bj's bounding box
 // (with a margin of 1e-4 rlim^2 + 1e-3 A^2, far wider than `band` and the FP32 rounding) can
 // list a pair; the rows of the others are certainly empty, and the loop skips them.
+// PIMG (a box at most twice the list radius plus two block extents): the tiles' image is not
+// every pair's, so each pair takes its own minimum image in FP32 and no i atom is culled.
+template <bool PIMG>
 __device__ __forceinline__ unsigned tile_row_f32(const DevPtrs& P, const Rep& R, int bi, int bj, int lane,
                                                  const IStage& S, float rlim2f, float band, bool& unsure) {
   const int aj = P.satom[bj * kTile + lane];
@@ -276,17 +279,29 @@ __device__ __forceinline__ unsigned tile_row_f32(const DevPtrs& P, const Rep& R,
   }
   const float4 pj = P.pos_f[bj * kTile + lane];
   const float r[3] = {pj.x + cj[0], pj.y + cj[1], pj.z + cj[2]};
-  const float4 hj = P.blk_half[bj];
-  const float gx = fmaxf(fabsf(S.xf[lane] - cj[0]) - hj.x, 0.f);
-  const float gy = fmaxf(fabsf(S.yf[lane] - cj[1]) - hj.y, 0.f);
-  const float gz = fmaxf(fabsf(S.zf[lane] - cj[2]) - hj.z, 0.f);
-  unsigned live = __ballot_sync(0xffffffffu, fmaf(gx, gx, fmaf(gy, gy, gz * gz)) <= rlim2f * 1.0001f + 1e-3f);
+  unsigned live;
+  if (PIMG) {   // every real i atom (padding slots sit at 1e18)
+    live = __ballot_sync(0xffffffffu, S.xf[lane] < 1.0e17f);
+  } else {
+    const float4 hj = P.blk_half[bj];
+    const float gx = fmaxf(fabsf(S.xf[lane] - cj[0]) - hj.x, 0.f);
+    const float gy = fmaxf(fabsf(S.yf[lane] - cj[1]) - hj.y, 0.f);
+    const float gz = fmaxf(fabsf(S.zf[lane] - cj[2]) - hj.z, 0.f);
+    live = __ballot_sync(0xffffffffu, fmaf(gx, gx, fmaf(gy, gy, gz * gz)) <= rlim2f * 1.0001f + 1e-3f);
+  }
+  const float bx = (float)R.box[0], by = (float)R.box[1], bz = (float)R.box[2];
+  const float ibx = (float)R.invbox[0], iby = (float)R.invbox[1], ibz = (float)R.invbox[2];
   unsigned row = 0;
   bool u = false;
   while (live) {   // warp-uniform
     const int i = __ffs(live) - 1;
     live &= live - 1;
-    const float dx = S.xf[i] - r[0], dy = S.yf[i] - r[1], dz = S.zf[i] - r[2];
+    float dx = S.xf[i] - r[0], dy = S.yf[i] - r[1], dz = S.zf[i] - r[2];
+    if (PIMG) {
+      dx = fmaf(-bx, rintf(dx * ibx), dx);
+      dy = fmaf(-by, rintf(dy * iby), dy);
+      dz = fmaf(-bz, rintf(dz * ibz), dz);
+    }
     const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     const bool in = aj >= 0 && d2 <= rlim2f;
     u |= aj >= 0 && fabsf(d2 - rlim2f) < band;
@@ -389,7 +404,7 @@ __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk,
 #pragma unroll
     for (int q = 0; q < kExclReg; ++q) ps[q] = pb + q < pe ? P.excl_slot[pb + q] : -64;
     IStage& S = s_i[threadIdx.x >> 5];
-    if (fast) {   // the i block, wrapped, for the broadcast reads
+    if (!CMM) {   // the i block, wrapped, for the broadcast reads
       S.x[lane] = xi - R.box[0] * floor(xi * R.invbox[0]);
       S.y[lane] = yi - R.box[1] * floor(yi * R.invbox[1]);
       S.z[lane] = zi - R.box[2] * floor(zi * R.invbox[2]);
@@ -405,15 +420,19 @@ __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk,
     // 2 sqrt(3) rlim 5 2^-24 M + 3 2^-24 rlim^2; pairs within 4 times that of rlim^2 are
     // decided in FP64 (about 1.5e-3 A^2 for water blocks at rc = 12 A)
     const float hm = fmaxf(P.rep_hmax[3 * rep], fmaxf(P.rep_hmax[3 * rep + 1], P.rep_hmax[3 * rep + 2]));
-    const float band = 4.f * 5.9604645e-8f * (17.33f * rlimf * (rlimf + 3.f * hm) + 3.f * rlimf * rlimf);
+    // with per-pair images (a small box) the coordinates before imaging reach the box edge
+    const float mb = fast ? rlimf + 3.f * hm
+                          : fmaxf(rlimf + 3.f * hm, (float)fmax(R.box[0], fmax(R.box[1], R.box[2])) + 3.f * hm);
+    const float band = 4.f * 5.9604645e-8f * (17.33f * rlimf * mb + 3.f * rlimf * rlimf);
     while (ball) {
       const int b = __ffs(ball) - 1;
       ball &= ball - 1;
       unsigned mel = 0;
       unsigned m;
       bool unsure = true;
-      if (fast) {
-        unsigned row = tile_row_f32(P, R, bi, j0 + b, lane, S, rlim2f, band, unsure);
+      if (!CMM) {
+        unsigned row = fast ? tile_row_f32<false>(P, R, bi, j0 + b, lane, S, rlim2f, band, unsure)
+                            : tile_row_f32<true>(P, R, bi, j0 + b, lane, S, rlim2f, band, unsure);
         if (!unsure) {
           if (ai < 0) row = 0;
           m = finish_mask(P, bi, j0 + b, lane, row, ps, pb, pe);
