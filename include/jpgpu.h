@@ -292,7 +292,7 @@ typedef struct jp_params {
   /* Block-shape tuning at jp_create (no md.inp keyword; the counterpart of md_run's
    * SIMD_check autotuning of its vector length): 1 (default) = build each replica's list
    * with JP_TUNE_CANDIDATES column grids and keep the one whose list has the fewest
-   * compact tiles (see jp_tile_shape); 0 = near-cubic 32-atom blocks for every replica. */
+   * pair records (see jp_tile_shape); 0 = near-cubic 32-atom blocks for every replica. */
   int32_t tune_blocks;
 } jp_params;
 
@@ -405,7 +405,7 @@ int jp_set_grid_limit(jp_ctx *ctx, int32_t blocks);
 int jp_set_wait_limit(jp_ctx *ctx, int64_t cycles);
 
 /* The block shape jp_create chose for `replica`: the column-edge factor kept (1 = columns of
- * edge (32/density)^(1/3)) and, per candidate, the compact tiles its list needed
+ * edge (32/density)^(1/3)) and, per candidate, the pair records its list needed
  * (tiles[JP_TUNE_CANDIDATES], -1 when tuning was off).  md_run's counterpart is the
  * vector length SIMD_check.f90 picks and prints. */
 int jp_tile_shape(jp_ctx *ctx, int32_t replica, double *column_scale, int64_t *tiles);
@@ -414,8 +414,9 @@ int jp_last_timing(jp_ctx *ctx, double *total_ms, double *phase_ms4, int32_t *la
 /* Kernel launches per jp_step step (excluding list rebuilds) and per list rebuild. */
 int jp_launch_counts(jp_ctx *ctx, int32_t *per_step, int32_t *per_rebuild);
 
-/* Pair-list statistics of the current list, all replicas: tiles (the pair kernels' work
- * units: a block of 32 i atoms with 32 j entries), pair slots set in their masks (pairs
+/* Pair-list statistics of the current list, all replicas: pair records (the pair kernels'
+ * work units: half a block, 16 i atoms, with 32 j entries: 512 pair slots), pair slots set
+ * in their masks (pairs
  * within rc+1.5 at the last rebuild, exclusions removed), and the number of atoms padded
  * into blocks. */
 int jp_list_stats(jp_ctx *ctx, int64_t *ntiles, int64_t *npairs_listed, int64_t *nslots);

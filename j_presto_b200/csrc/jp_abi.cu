@@ -204,9 +204,11 @@ void enqueue_rebuild(jp_ctx *c) {
   const int nwb = (c->nchunk * 32 + 127) / 128;
   launch_tile_scan(P, c->nchunk, rlim * rlim, (float)rlim, rc * rc, c->cmm, st);
   nl += scan_exclusive(P.chunk_cnt, P.chunk_off, c->nchunk + 1, c->scan_scratch, P.ntiles, st);
-  nl += scan_exclusive(P.chunk_ent, P.chunk_eoff, c->nchunk + 1, c->scan_scratch, nullptr, st);
+  for (int h = 0; h < 2; ++h)   // the entries of each half block
+    nl += scan_exclusive(P.chunk_ent + h * (c->nchunk + 1), P.chunk_eoff + h * (c->nchunk + 1), c->nchunk + 1,
+                         c->scan_scratch, nullptr, st);
   k_tile_emit<<<nwb, 128, 0, st>>>(P, c->nchunk, c->cmm ? 1 : 0);
-  nl += launch_compact_tiles(P, c->nblk, c->nsm, c->cmm, c->scan_scratch, st);
+  nl += launch_compact_tiles(P, c->nblk, c->nchunk, c->nsm, c->cmm, c->scan_scratch, st);
   if (c->hbond) launch_hb_list(P, c->hb_cap, c->zc.nt1, c->nblk, st);
   c->launches_rebuild = nl + (c->fp64 ? 1 : 0) + ncmm + (c->hbond ? 1 : 0);
 }
@@ -842,18 +844,18 @@ int tune_blocks(jp_ctx *c, bool tune) {
   const int nq = JP_TUNE_CANDIDATES;
   c->tune_tiles.assign((size_t)c->nrep * nq, -1);
   c->tune_pick.assign(c->nrep, kTuneDefault);
-  std::vector<int> cnt(c->nblk);
+  std::vector<int> cnt(2 * (size_t)c->nblk);   // pair records per unit (two per block)
   for (int q = 0; q < (tune ? nq : 0); ++q) {
     for (int r = 0; r < c->nrep; ++r) set_grid(c->reps[r], c->tune_grid.data() + ((size_t)r * nq + q) * 2);
     CK(cudaMemcpy(c->P.reps, c->reps.data(), sizeof(Rep) * c->nrep, cudaMemcpyHostToDevice));
     enqueue_rebuild(c);
-    CK(cudaMemcpyAsync(cnt.data(), c->P.ct_cnt, sizeof(int) * c->nblk, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(cnt.data(), c->P.ct_cnt, sizeof(int) * 2 * c->nblk, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     int rs = check_status(c);
     if (rs < 0) return rs;
     for (int r = 0; r < c->nrep; ++r) {
       long long t = 0;
-      for (int b = c->reps[r].blk0; b < c->reps[r].blk0 + c->reps[r].nblk; ++b) t += cnt[b];
+      for (int b = c->reps[r].blk0; b < c->reps[r].blk0 + c->reps[r].nblk; ++b) t += cnt[2 * b] + cnt[2 * b + 1];
       c->tune_tiles[(size_t)r * nq + q] = t;
     }
   }
@@ -1578,19 +1580,22 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.masks, (size_t)c->tile_cap_total * 32);
   // compact tiles: at most one per tile (an i-block's j entries never outnumber 32 per tile)
   e |= dput(c, &P.blk_chunk0, blk_chunk0);
-  e |= dalloc(c, &P.ct_cnt, (size_t)c->nblk + 1);
-  e |= dalloc(c, &P.ct_off, (size_t)c->nblk + 1);
-  e |= dalloc(c, &P.ct_blk, (size_t)c->tile_cap_total);
-  e |= dalloc(c, &P.ct_src, (size_t)c->tile_cap_total);
-  e |= dalloc(c, &P.tmp_occ, (size_t)c->nchunk * 32);
-  e |= dalloc(c, &P.chunk_ent, (size_t)c->nchunk + 1);
-  e |= dalloc(c, &P.chunk_eoff, (size_t)c->nchunk + 1);
-  e |= dalloc(c, &P.tile_occ, (size_t)c->tile_cap_total);
-  e |= dalloc(c, &P.tile_eoff, (size_t)c->tile_cap_total);
-  e |= dalloc(c, &P.ct_j, (size_t)c->tile_cap_total * 32);
-  e |= dalloc(c, &P.ct_mask, (size_t)c->tile_cap_total * 32);
+  // pair records: at most one per tile and half (a unit's records never outnumber the tiles
+  // of its block), plus one so that the kernels' record pairs stay inside the arrays
+  const size_t rec_cap = 2 * (size_t)c->tile_cap_total + 2;
+  e |= dalloc(c, &P.ct_cnt, 2 * (size_t)c->nblk + 1);
+  e |= dalloc(c, &P.ct_off, 2 * (size_t)c->nblk + 1);
+  e |= dalloc(c, &P.ct_blk, rec_cap);
+  e |= dalloc(c, &P.ct_info, rec_cap);
+  e |= dalloc(c, &P.tmp_occ, (size_t)c->nchunk * 32 * 2);
+  e |= dalloc(c, &P.chunk_ent, 2 * ((size_t)c->nchunk + 1));
+  e |= dalloc(c, &P.chunk_eoff, 2 * ((size_t)c->nchunk + 1));
+  e |= dalloc(c, &P.tile_occ, 2 * (size_t)c->tile_cap_total);
+  e |= dalloc(c, &P.tile_eoff, 2 * (size_t)c->tile_cap_total);
+  e |= dalloc(c, &P.ct_j, rec_cap * 32);
+  e |= dalloc(c, &P.ct_mask, rec_cap * kHalf);
   e |= dalloc(c, &P.nctiles, 1);
-  if (c->cmm) e |= dalloc(c, &P.ct_mask_el, (size_t)c->tile_cap_total * 32);
+  if (c->cmm) e |= dalloc(c, &P.ct_mask_el, rec_cap * kHalf);
   if (c->cmm) {
     int ntot = 0;
     for (int l = 1; l <= 5; ++l) ntot += c->cmm_ncell[l];
@@ -2313,7 +2318,7 @@ int jp_list_stats(jp_ctx *c, int64_t *ntiles, int64_t *npairs_listed, int64_t *n
   if (ntiles) *ntiles = nt;
   if (nslots) *nslots = c->nslot;
   if (npairs_listed) {
-    std::vector<unsigned> m((size_t)nt * 32);
+    std::vector<unsigned> m((size_t)nt * kHalf);
     if (nt) CK(cudaMemcpy(m.data(), c->P.ct_mask, sizeof(unsigned) * m.size(), cudaMemcpyDeviceToHost));
     int64_t s = 0;
     for (unsigned v : m) s += __builtin_popcount(v);

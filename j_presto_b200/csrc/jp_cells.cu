@@ -293,20 +293,30 @@ __device__ __forceinline__ unsigned tile_row_f32(const DevPtrs& P, const Rep& R,
   const float ibx = (float)R.invbox[0], iby = (float)R.invbox[1], ibz = (float)R.invbox[2];
   unsigned row = 0;
   bool u = false;
-  while (live) {   // warp-uniform
-    const int i = __ffs(live) - 1;
-    live &= live - 1;
+  // two i atoms per pass: two independent distance chains and ballots
+  auto d2of = [&](int i) {
     float dx = S.xf[i] - r[0], dy = S.yf[i] - r[1], dz = S.zf[i] - r[2];
     if (PIMG) {
       dx = fmaf(-bx, rintf(dx * ibx), dx);
       dy = fmaf(-by, rintf(dy * iby), dy);
       dz = fmaf(-bz, rintf(dz * ibz), dz);
     }
-    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  };
+  while (live) {   // warp-uniform
+    const int i = __ffs(live) - 1;
+    live &= live - 1;
+    const int i2 = live ? __ffs(live) - 1 : -1;
+    live &= live - 1;
+    const float d2 = d2of(i), e2 = d2of(i2 < 0 ? i : i2);
     const bool in = aj >= 0 && d2 <= rlim2f;
+    const bool in2 = aj >= 0 && i2 >= 0 && e2 <= rlim2f;
     u |= aj >= 0 && fabsf(d2 - rlim2f) < band;
+    u |= aj >= 0 && i2 >= 0 && fabsf(e2 - rlim2f) < band;
     const unsigned b = __ballot_sync(0xffffffffu, in);
+    const unsigned b2 = __ballot_sync(0xffffffffu, in2);
     if (lane == i) row = b;
+    if (lane == i2) row = b2;
   }
   unsure = __any_sync(0xffffffffu, u);
   return row;
@@ -389,7 +399,7 @@ __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk,
   }
   unsigned ball = __ballot_sync(0xffffffffu, cand);
   unsigned nz = 0;
-  int nent = 0;
+  int nent0 = 0, nent1 = 0;   // entries of the two half blocks (rows 0-15, 16-31)
   if (ball) {
     const int ai = P.satom[bi * kTile + lane];
     double xi = 0, yi = 0, zi = 0;
@@ -444,10 +454,17 @@ __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk,
       if (__any_sync(0xffffffffu, m != 0)) {
         P.tmp_masks[((size_t)w * 32 + b) * 32 + lane] = m;
         if (CMM) P.tmp_masks_el[((size_t)w * 32 + b) * 32 + lane] = mel;
-        // the j lanes some i atom lists: the compact-tile entries this tile contributes
-        const unsigned occ = __reduce_or_sync(0xffffffffu, __funnelshift_l(m, m, lane));
-        if (lane == 0) P.tmp_occ[(size_t)w * 32 + b] = occ;
-        nent += __popc(occ);
+        // the j lanes some i atom of each half block lists: the entries this tile
+        // contributes to the two halves' pair records
+        const unsigned rowj = __funnelshift_l(m, m, lane);
+        const unsigned occ0 = __reduce_or_sync(0xffffffffu, lane < kHalf ? rowj : 0u);
+        const unsigned occ1 = __reduce_or_sync(0xffffffffu, lane < kHalf ? 0u : rowj);
+        if (lane == 0) {
+          P.tmp_occ[((size_t)w * 32 + b) * 2 + 0] = occ0;
+          P.tmp_occ[((size_t)w * 32 + b) * 2 + 1] = occ1;
+        }
+        nent0 += __popc(occ0);
+        nent1 += __popc(occ1);
         nz |= 1u << b;
       }
     }
@@ -455,7 +472,8 @@ __global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk,
   if (lane == 0) {
     P.chunk_nz[w] = nz;
     P.chunk_cnt[w] = __popc(nz);
-    P.chunk_ent[w] = nent;
+    P.chunk_ent[w] = nent0;
+    P.chunk_ent[nchunk + 1 + w] = nent1;
   }
 }
 
@@ -476,17 +494,19 @@ __global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm) {
   const int bi = P.chunk_i[w], j0 = P.chunk_j0[w];
   const int t0 = P.chunk_off[w];
   const int cnt = __popc(nz);
-  {   // lane q: the chunk's q-th tile's occupied j lanes and its first entry (global order)
+  // lane q: the chunk's q-th tile's occupied j lanes of each half block and its first entry
+  // in that half's entry order (global)
+  for (int h = 0; h < 2; ++h) {
     const int b = lane < cnt ? (int)__fns(nz, 0, lane + 1) : 0;
-    const unsigned occ = lane < cnt ? P.tmp_occ[(size_t)w * 32 + b] : 0u;
+    const unsigned occ = lane < cnt ? P.tmp_occ[((size_t)w * 32 + b) * 2 + h] : 0u;
     int e = __popc(occ);
     for (int o = 1; o < 32; o <<= 1) {   // inclusive scan over the lanes
       const int y = __shfl_up_sync(0xffffffffu, e, o);
       if (lane >= o) e += y;
     }
     if (lane < cnt) {
-      P.tile_occ[t0 + lane] = occ;
-      P.tile_eoff[t0 + lane] = P.chunk_eoff[w] + e - __popc(occ);
+      P.tile_occ[2 * (size_t)(t0 + lane) + h] = occ;
+      P.tile_eoff[2 * (size_t)(t0 + lane) + h] = P.chunk_eoff[h * (nchunk + 1) + w] + e - __popc(occ);
     }
   }
   if (lane < cnt) {   // lane q: the chunk's q-th tile, its block pair and image shift
@@ -510,43 +530,54 @@ __global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm) {
   }
 }
 
-// ---- compact tiles ------------------------------------------------------------------------
-// The pair kernels run on compact tiles: an i-block with 32 j entries, the j atoms of that
-// block's tiles that have at least one listed pair with it, taken in tile order (ascending
-// j block, ascending slot).  A 32 x 32 tile of two blocks holds ~26 % listed pairs at the
-// md_run list radius; keeping only the j atoms some i atom lists raises that to ~45 %, and
-// the pair kernels' work per pair falls in proportion.  The listed pair set is unchanged.
-// Each entry carries its tile's image shift (into the i block's frame) and its slot; the
-// mask keeps the kernels' rotated layout (bit k of lane i: entry (i + k) & 31).
+// ---- pair records ------------------------------------------------------------------------
+// The pair kernels run on pair records: a half block (16 i atoms: rows 0-15 or 16-31 of an
+// i-block, unit u = 2 i-block + half) with 32 j entries, the j atoms of that block's tiles
+// that at least one of the 16 i atoms lists, taken in tile order (ascending j block,
+// ascending slot).  A 32 x 32 tile of two blocks holds ~26 % listed pairs at the md_run list
+// radius; keeping only the j atoms a half block lists raises that to ~55 %, because 16 atoms
+// span a smaller volume than 32 (within the cut-off: 32 % of the slots with whole blocks,
+// 39 % with half blocks), and the pair kernels' work per pair falls in proportion.  The
+// listed pair set is unchanged.  Each entry carries its tile's image shift (into the i
+// block's frame) and its slot; the mask of i atom l (0..15) has bit k = entry (l + k) & 15
+// and bit 16 + k = entry 16 + ((l + k) & 15), the order in which the kernels meet them.
 
-// tiles of i-block bi: [chunk_off[blk_chunk0[bi]], chunk_off[blk_chunk0[bi + 1]]); its
-// entries: [chunk_eoff[blk_chunk0[bi]], chunk_eoff[blk_chunk0[bi + 1]]) in global order
-// (the tile scan counts each tile's occupied j lanes, the tile emit places each tile's
-// entries)
+// tiles of i-block bi: [chunk_off[blk_chunk0[bi]], chunk_off[blk_chunk0[bi + 1]]); the
+// entries of its half h: [eoff_h[blk_chunk0[bi]], eoff_h[blk_chunk0[bi + 1]]) in global
+// order, eoff_h = chunk_eoff + h (nchunk + 1) (the tile scan counts each tile's occupied j
+// lanes per half, the tile emit places each tile's entries)
 
-// per i-block (one thread each): compact tiles it needs
-__global__ void k_ct_count(DevPtrs P, int nblk) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nblk) return;
-  const int ne = P.chunk_eoff[P.blk_chunk0[b + 1]] - P.chunk_eoff[P.blk_chunk0[b]];
-  P.ct_cnt[b] = (ne + 31) >> 5;
+// per unit (one thread each): the pair records it needs
+__global__ void k_ct_count(DevPtrs P, int nblk, int nchunk) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= 2 * nblk) return;
+  const int b = u >> 1, h = u & 1;
+  const int* eoff = P.chunk_eoff + h * (nchunk + 1);
+  const int ne = eoff[P.blk_chunk0[b + 1]] - eoff[P.blk_chunk0[b]];
+  P.ct_cnt[u] = (ne + 31) >> 5;
 }
 
-// per tile (one thread each, after the scan of ct_cnt): the compact tiles of its i-block
-// whose first slot falls among its entries get it as their first source tile, and their
-// i-block (a tile holds at most 32 entries, so at most two compact tiles start in it)
-__global__ void k_ct_index(DevPtrs P) {
+// per tile (one thread each, after the scan of ct_cnt) and half: the records of the unit
+// whose first slot falls among the tile's entries of that half get their unit and, for the
+// emit, the tile as their first source tile, their first slot's global entry, the end of the
+// unit's entries and of the block's tiles (a tile holds at most 32 entries, so at most two
+// records start in it)
+__global__ void k_ct_index(DevPtrs P, int nchunk) {
   const int T = *P.ntiles;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
     const int b = P.tiles[t].x;
-    const int c0 = P.blk_chunk0[b];
-    const int e0 = P.chunk_eoff[c0];
-    const int tl = P.chunk_off[P.blk_chunk0[b + 1]] - 1;   // the block's last tile
-    const int lo = P.tile_eoff[t] - e0;
-    const int hi = t < tl ? P.tile_eoff[t + 1] - e0 : P.chunk_eoff[P.blk_chunk0[b + 1]] - e0;
-    for (int k = (lo + 31) >> 5; 32 * k < hi; ++k) {
-      P.ct_blk[P.ct_off[b] + k] = b;
-      P.ct_src[P.ct_off[b] + k] = t;
+    const int c0 = P.blk_chunk0[b], c1 = P.blk_chunk0[b + 1];
+    const int tl = P.chunk_off[c1] - 1;   // the block's last tile
+    for (int h = 0; h < 2; ++h) {
+      const int* eoff = P.chunk_eoff + h * (nchunk + 1);
+      const int e0 = eoff[c0];
+      const int lo = P.tile_eoff[2 * (size_t)t + h] - e0;
+      const int hi = t < tl ? P.tile_eoff[2 * (size_t)(t + 1) + h] - e0 : eoff[c1] - e0;
+      const int u = 2 * b + h;
+      for (int k = (lo + 31) >> 5; 32 * k < hi; ++k) {
+        P.ct_blk[P.ct_off[u] + k] = u;
+        P.ct_info[P.ct_off[u] + k] = make_int4(t, e0 + 32 * k, eoff[c1], ((tl + 1) << 1) | h);
+      }
     }
   }
 }
@@ -574,33 +605,40 @@ __device__ __forceinline__ unsigned compress_bits(unsigned x, unsigned m) {
   return x;
 }
 
-// One warp per compact tile: lane i's row collects, from each tile whose entries fall in
-// the compact tile's 32 slots, the bits of that tile's row i at its occupied j lanes
-// (packed in lane order); lane p writes slot p's entry.  Those source tiles are consecutive
-// from ct_src and at most 32 (each holds at least one entry and the first covers slot 0), so
-// lane q reads source tile q's offset, occupancy, j block and image shift in one coalesced
-// pass, the mask rows are read four tiles at a time, and each slot's entry comes from its
-// tile's lane by shuffles: no load waits on another.
-__global__ void k_ct_emit(DevPtrs P, int cmm) {
+// a record row (bit e: entry e) into the kernels' order for i atom l: each 16-bit half
+// rotated right by l
+__device__ __forceinline__ unsigned record_row(unsigned row, int l) {
+  const unsigned lo = row & 0xffffu, hi = row >> 16;
+  const unsigned rl = ((lo >> l) | (lo << (16 - l))) & 0xffffu;
+  const unsigned rh = ((hi >> l) | (hi << (16 - l))) & 0xffffu;
+  return rl | (rh << 16);
+}
+
+// One warp per record: lane l's row (row 16 h + l of the i-block, l < 16; lanes 16-31 repeat
+// lanes 0-15) collects, from each tile whose entries fall in the record's 32 slots, the bits
+// of that tile's row at its occupied j lanes of half h (packed in lane order); lane p writes
+// slot p's entry.  Those source tiles are consecutive from ct_src and at most 32 (each holds
+// at least one entry and the first covers slot 0), so lane q reads source tile q's offset,
+// occupancy, j block and image shift in one coalesced pass, the mask rows are read four tiles
+// at a time, and each slot's entry comes from its tile's lane by shuffles: no load waits on
+// another.
+__global__ void k_ct_emit(DevPtrs P, int nchunk, int cmm) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const int T = *P.nctiles;
   for (int ct = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ct < T; ct += nw) {
-    const int b = P.ct_blk[ct];
-    const int c1 = P.blk_chunk0[b + 1];
-    const int e1 = P.chunk_eoff[c1];
-    const int t1 = P.chunk_off[c1];
-    const int s0 = P.chunk_eoff[P.blk_chunk0[b]] + 32 * (ct - P.ct_off[b]);
-    const int ts = P.ct_src[ct];
+    const int4 info = P.ct_info[ct];
+    const int ts = info.x, s0 = info.y, e1 = info.z, t1 = info.w >> 1, h = info.w & 1;
     const int tq = ts + lane;   // lane q: source tile q
+    const int ri = kHalf * h + (lane & (kHalf - 1));   // this lane's row of the i-block
     int qb = 32, qy = 0;
     unsigned qocc = 0u;
     float4 qsh = make_float4(0.f, 0.f, 0.f, 0.f);
     if (tq < t1) {
-      qb = P.tile_eoff[tq] - s0;   // slot of the tile's first entry (may be < 0)
+      qb = P.tile_eoff[2 * (size_t)tq + h] - s0;   // slot of the tile's first entry (may be < 0)
       if (qb < 32) {
-        qocc = P.tile_occ[tq];
+        qocc = P.tile_occ[2 * (size_t)tq + h];
         qy = P.tiles[tq].y;
         qsh = P.tile_shift[tq];
       }
@@ -611,19 +649,19 @@ __global__ void k_ct_emit(DevPtrs P, int cmm) {
     for (int j0 = 0; j0 < nt; j0 += 4) {   // warp-uniform
       unsigned m[4], me[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        m[u] = j0 + u < nt ? P.masks[(size_t)(ts + j0 + u) * 32 + lane] : 0u;
-        me[u] = cmm && j0 + u < nt ? P.masks_el[(size_t)(ts + j0 + u) * 32 + lane] : 0u;
+      for (int v = 0; v < 4; ++v) {
+        m[v] = j0 + v < nt ? P.masks[(size_t)(ts + j0 + v) * 32 + ri] : 0u;
+        me[v] = cmm && j0 + v < nt ? P.masks_el[(size_t)(ts + j0 + v) * 32 + ri] : 0u;
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int j = j0 + u;
+      for (int v = 0; v < 4; ++v) {
+        const int j = j0 + v;
         const int base = __shfl_sync(full, qb, j & 31);
         const unsigned occ = __shfl_sync(full, qocc, j & 31);
         if (j >= nt) break;
         const int n = __popc(occ);
-        const unsigned comp = compress_bits(__funnelshift_l(m[u], m[u], lane), occ);
-        const unsigned comp_el = cmm ? compress_bits(__funnelshift_l(me[u], me[u], lane), occ) : 0u;
+        const unsigned comp = compress_bits(__funnelshift_l(m[v], m[v], ri), occ);
+        const unsigned comp_el = cmm ? compress_bits(__funnelshift_l(me[v], me[v], ri), occ) : 0u;
         if (base >= 0) {
           cur |= comp << base;
           cur_el |= comp_el << base;
@@ -647,18 +685,20 @@ __global__ void k_ct_emit(DevPtrs P, int cmm) {
     if (src >= 0 && s0 + lane < e1)
       ent = make_float4(shx, shy, shz, __int_as_float(sy * kTile + (int)__fns(socc, 0, kk + 1)));
     P.ct_j[(size_t)ct * 32 + lane] = ent;
-    P.ct_mask[(size_t)ct * 32 + lane] = __funnelshift_r(cur, cur, lane);
-    if (cmm) P.ct_mask_el[(size_t)ct * 32 + lane] = __funnelshift_r(cur_el, cur_el, lane);
+    if (lane < kHalf) {
+      P.ct_mask[(size_t)ct * kHalf + lane] = record_row(cur, lane);
+      if (cmm) P.ct_mask_el[(size_t)ct * kHalf + lane] = record_row(cur_el, lane);
+    }
   }
 }
 
-int launch_compact_tiles(const DevPtrs& P, int nblk, int nsm, bool cmm, int* scan_scratch,
+int launch_compact_tiles(const DevPtrs& P, int nblk, int nchunk, int nsm, bool cmm, int* scan_scratch,
                          cudaStream_t st) {
-  const int nb = (nblk + 127) / 128;
-  k_ct_count<<<nb, 128, 0, st>>>(P, nblk);
-  const int ns = scan_exclusive(P.ct_cnt, P.ct_off, nblk + 1, scan_scratch, P.nctiles, st);
-  k_ct_index<<<nsm * 4, 256, 0, st>>>(P);
-  k_ct_emit<<<nsm * 8, 256, 0, st>>>(P, cmm ? 1 : 0);
+  const int nb = (2 * nblk + 127) / 128;
+  k_ct_count<<<nb, 128, 0, st>>>(P, nblk, nchunk);
+  const int ns = scan_exclusive(P.ct_cnt, P.ct_off, 2 * nblk + 1, scan_scratch, P.nctiles, st);
+  k_ct_index<<<nsm * 4, 256, 0, st>>>(P, nchunk);
+  k_ct_emit<<<nsm * 8, 256, 0, st>>>(P, nchunk, cmm ? 1 : 0);
   return 3 + ns;
 }
 

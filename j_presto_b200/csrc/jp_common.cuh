@@ -19,6 +19,7 @@
 namespace jp {
 
 constexpr int kTile = 32;
+constexpr int kHalf = 16;   // i atoms of a pair record: half a block
 // fixed-point scales: forces 2^32 per kcal/mol/A, energies 2^32 per kcal/mol,
 // kinetic sums (m v^2, amu A^2/fs^2) 2^40.
 constexpr double kFrcScale = 4294967296.0;
@@ -191,13 +192,15 @@ struct DevPtrs {
   int *ntiles;                    // device scalar
   // compact tiles (what the pair kernels run on): an i-block and 32 j entries
   int *blk_chunk0;                // [nblk+1] first chunk of each i-block (static)
-  int *ct_cnt, *ct_off;           // compact tiles per i-block and their scan [nblk+1]
-  int *ct_blk;                    // [CT] i-block
-  int *ct_src;                    // [CT] first tile whose entries reach into the compact tile
-  unsigned *tmp_occ;              // [nchunk*32] occupied j lanes of each chunk candidate
-  int *chunk_ent, *chunk_eoff;    // entries per chunk and their exclusive scan [nchunk+1]
-  unsigned *tile_occ;             // [T] occupied j lanes of each tile
-  int *tile_eoff;                 // [T] first entry of each tile (global order)
+  int *ct_cnt, *ct_off;           // pair records per unit (2 i-block + half) and their scan [2 nblk+1]
+  int *ct_blk;                    // [CT] unit of each pair record
+  int4 *ct_info;                  // [CT] what the emit needs of each record: its first source tile,
+                                  // the global entry of its slot 0, the end of its unit's entries,
+                                  // and (end of its block's tiles) << 1 | half
+  unsigned *tmp_occ;              // [nchunk*32][2] occupied j lanes of each chunk candidate, per half
+  int *chunk_ent, *chunk_eoff;    // per half [2][nchunk+1]: entries per chunk, their exclusive scan
+  unsigned *tile_occ;             // [T][2] occupied j lanes of each tile, per half
+  int *tile_eoff;                 // [T][2] first entry of each tile in its half's order (global)
   float4 *ct_j;                   // [CT][32] (image shift into the i frame, slot bits; -1 = empty)
   unsigned *ct_mask, *ct_mask_el; // [CT][32] rotated masks (listed pairs; CMM Coulomb pairs)
   int *nctiles;                   // device scalar
@@ -281,6 +284,18 @@ __device__ __forceinline__ long long to_fix(double v, double scale, unsigned *st
     return 0;
   }
   return __double2ll_rn(s);
+}
+
+// The same for an FP32 force at the force scale 2^32: v * 2^32 is exact in FP32, and its
+// conversion rounds as the FP64 one does (a float above 2^24 is already an integer), so the
+// result equals to_fix((double)v, kFrcScale, status) without the FP64 arithmetic.
+__device__ __forceinline__ long long to_fix_f(float v, unsigned *status) {
+  const float s = v * 4294967296.0f;
+  if (!(fabsf(s) < 72057594037927936.0f)) {
+    atomicOr(status, isfinite(v) ? ERR_FIX_OVERFLOW : ERR_NONFINITE);
+    return 0;
+  }
+  return __float2ll_rn(s);
 }
 
 __device__ __forceinline__ void atomic_add_ll(long long *p, long long v) {

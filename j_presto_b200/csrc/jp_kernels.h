@@ -20,7 +20,7 @@ void launch_tile_scan(const DevPtrs& P, int nchunk, double rlim2, float rlimf, d
                       cudaStream_t st);
 __global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm);
 // compact tiles of every i-block from the tile list (count, scan, emit); returns the launches
-int launch_compact_tiles(const DevPtrs& P, int nblk, int nsm, bool cmm, int* scan_scratch,
+int launch_compact_tiles(const DevPtrs& P, int nblk, int nchunk, int nsm, bool cmm, int* scan_scratch,
                          cudaStream_t st);
 // deterministic exclusive scan of n ints (total: the sum, or null); returns the launches
 int scan_exclusive(const int* in, int* out, int n, int* scratch, int* total, cudaStream_t st);

@@ -8,26 +8,27 @@
 // with q = charge * sqrt(332.06378/eps) (chgmod, inpcls.f90:215-227), b = 1/(2 rc^3),
 // f = 1/rc^3, z = 1.5/rc (incel.f90:655-658).
 //
-// Work unit: a compact tile (jp_cells.cu) = an i-block of 32 cell-sorted atoms and 32 j
-// entries (j atoms with at least one listed pair in the block, each with the image shift of
-// its block) with an interaction mask fixed at list-build time.  One warp per compact tile:
-// lane l holds i-atom l and at step k meets entry (l + k) & 31; the j-force accumulators
-// rotate one lane per step through warp shuffles, so after 32 steps each is back in the lane
-// of its entry.  Newton's third law: each unordered pair is evaluated once.
+// Work unit: a pair record (jp_cells.cu) = half an i-block (16 cell-sorted atoms) and 32 j
+// entries (j atoms with at least one listed pair in the half block, each with the image
+// shift of its block) with an interaction mask fixed at list-build time.  One warp takes two
+// consecutive records, a half-warp each: lane l (l < 16 of its half) holds i atom l and at
+// step k (k < 16) meets entries a = (l + k) & 15 and b = 16 + a; the j-force accumulators of
+// a and b rotate one lane per step inside the half-warp (warp shuffles), so after 16 steps
+// lane l holds those of entries l and 16 + l, the ones it gathered.  Newton's third law:
+// each unordered pair is evaluated once.
 //
-// Warps take short runs of consecutive tiles from a global counter, so all finish together
-// whatever their tiles hold.
+// Warps take short runs of consecutive record pairs from a global counter, so all finish
+// together whatever their records hold.
 // Mixed path: FP32 pair arithmetic on block-local coordinates (|x| < ~30 A), every step of a
-// tile branch-free (a pair outside the mask or the cut-off contributes an exact zero);
-// forces summed per tile in FP32, energies in FP32 over 8 steps then in FP64, both added as
-// 64-bit fixed point
-// (2^-32 kcal/mol/A) with integer atomics -- order independent, so results are
-// bit-identical run to run.  A warp keeps two tiles in flight ahead of the one it computes:
-// the bulk-copy engine (cp.async.bulk, completion on an mbarrier) brings the entries and
-// masks of the tile after next into shared memory, and the gathers of the next tile's
-// j atoms are issued before the current tile's arithmetic.
-// FP64 path: the same compact tiles in FP64 with absolute coordinates, per-pair minimum
-// image and FP64 force atomics.
+// record branch-free (a pair outside the mask or the cut-off contributes an exact zero);
+// forces summed per record in FP32, energies in FP32 over 4 steps then in FP64, both added
+// as 64-bit fixed point (2^-32 kcal/mol/A) with integer atomics -- order independent, so
+// results are bit-identical run to run.  A warp keeps two record pairs in flight ahead of
+// the one it computes: the bulk-copy engine (cp.async.bulk, completion on an mbarrier)
+// brings the entries and masks of the pair after next into shared memory, and the gathers
+// of the next pair's j atoms are issued before the current pair's arithmetic.
+// FP64 path: the same records in FP64 with absolute coordinates, per-pair minimum image and
+// FP64 force atomics.
 #include "jp_kernels.h"
 
 namespace jp {
@@ -82,13 +83,14 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
   }
 }
 
-// a warp's energies (ELE15, VDW15; ALSD class AA / AB, BB the rest) and pair count into the
-// replica's slots: 64-bit fixed point, summed per tile, so the totals do not depend on which
-// warp took which tile (the kernels claim their tiles dynamically)
+// each half-warp's energies (ELE15, VDW15; ALSD class AA / AB, BB the rest) and pair count
+// into the slots of its replica: 64-bit fixed point, summed per record, so the totals do not
+// depend on which warp took which record (the kernels claim their records dynamically).  The
+// two halves of a warp may work for different replicas: the sums stay inside each half.
 __device__ __forceinline__ void flush_fix(const DevPtrs& P, int rep, long long eel, long long elj,
                                           long long eaa, long long eab, long long npair, bool count,
                                           bool alsd) {
-  for (int o = 16; o > 0; o >>= 1) {
+  for (int o = 8; o > 0; o >>= 1) {
     eel += __shfl_xor_sync(0xffffffffu, eel, o);
     elj += __shfl_xor_sync(0xffffffffu, elj, o);
     if (alsd) {
@@ -97,7 +99,7 @@ __device__ __forceinline__ void flush_fix(const DevPtrs& P, int rep, long long e
     }
     if (count) npair += __shfl_xor_sync(0xffffffffu, npair, o);
   }
-  if ((threadIdx.x & 31) == 0 && rep >= 0) {
+  if ((threadIdx.x & 15) == 0 && rep >= 0) {
     atomic_add_ll(&P.ene_fix[rep * 16 + JP_E_ELE15], eel);
     atomic_add_ll(&P.ene_fix[rep * 16 + JP_E_VDW15], elj);
     if (alsd) {
@@ -111,23 +113,17 @@ __device__ __forceinline__ void flush_fix(const DevPtrs& P, int rep, long long e
 }
 
 // Per-warp shared memory of the mixed kernel: two bulk-copy buffers (entries and masks of a
-// tile) and the staged j atoms of the tile being computed, stored twice so that step k
-// reads entry lane + k at a constant offset.
+// record pair: record 0 in entries 0-31 and masks 0-15, record 1 in 32-63 and 16-31) and the
+// staged j atoms of the pair being computed.  Half-warp h stages its record at [32 h, 32 h +
+// 32): lane l's entries a = l and b = 16 + l side by side, stored twice (at 32 h + l and
+// 32 h + l + 16) so that step k reads slot 32 h + l + k at a constant offset.
 struct __align__(16) MixStage {
-  float4 ent[2][32];
+  float4 ent[2][64];
   unsigned msk[2][32];
   unsigned msk_el[2][32];
-  union {
-    struct {              // one entry per step (ALSD and CMM variants)
-      float4 pos[64];
-      int typ[64];
-    };
-    struct {              // two entries per step, e and e + 16, as packed pairs
-      float4 p2[64];      // x_e, x_e+16, y_e, y_e+16
-      float4 q2[64];      // z_e, z_e+16, q_e, q_e+16
-      int2 t2[64];        // their LJ types
-    };
-  };
+  float4 p2[64];      // x_a, x_b, y_a, y_b
+  float4 q2[64];      // z_a, z_b, q_a, q_b
+  int2 t2[64];        // their LJ type words (with TRI: x = the type-triple index a * nt1 + b)
   unsigned long long bar[2];
 };
 
@@ -152,25 +148,24 @@ __device__ __forceinline__ float rint1(float v) {
   return __fadd_rn(__fadd_rn(v, 12582912.f), -12582912.f);
 }
 
-// One compact tile, two pairs per step in packed FP32x2 arithmetic (Blackwell's FFMA2 /
-// FADD2 / FMUL2): at step k (k < 16) lane l meets entries a = l + k and b = l + k + 16.  A
-// slot outside the mask or the cut-off takes r^2 = 1e30 (its r^-6 = 1e-90 is zero in FP32)
-// and a zero charge product, so it contributes an exact zero without a branch.  The j-force
-// accumulators of a and b rotate one lane per step; after 16 steps the b accumulator of
-// lane l belongs to entry l and the a accumulator to entry l + 16.  Same formula and
-// tolerances as the one-pair form; energies in FP32 over 4 steps, then FP64.
+// One record, two pairs per step in packed FP32x2 arithmetic (Blackwell's FFMA2 / FADD2 /
+// FMUL2): at step k (k < 16) lane l of the half-warp meets entries a = (l + k) & 15 and
+// b = 16 + a, staged at sidx + k (sidx = 32 h + l).  A slot outside the mask or the cut-off
+// takes r^2 = 1e30 (its r^-6 = 1e-90 is zero in FP32) and a zero charge product, so it
+// contributes an exact zero without a branch.  The j-force accumulators of a and b move one
+// lane per step (from lane src = l + 1 of the same half); after 16 steps lane l holds those
+// of entries l and 16 + l, returned in (gja, gjb).  Energies in FP32 over 4 steps, then FP64.
 // TRI: the LJ parameters of both pairs come from one 16-byte record of the type-triple
 // table (i type, a type, b type) -> (C6_a, C6_b, C12_a, C12_b), indexed by row3 (the i type)
 // plus the staged a * nt1 + b; else from two type-pair records.
 template <bool MINIMG, bool COUNT, bool TRI>
 __device__ __forceinline__ void tile_mixed2(const MixStage& S, const float2* __restrict__ s_lj,
                                             const float4* __restrict__ s_lj3, int row,
-                                            float4 pi, unsigned m, int lane, float bx, float by, float bz,
-                                            float ibx, float iby, float ibz, float rc2, float zb, float zf,
-                                            float zc, float& fix, float& fiy, float& fiz, float& gjx,
-                                            float& gjy, float& gjz, double& te, double& tl, int& tn) {
+                                            float4 pi, unsigned m, int sidx, int src, float bx, float by,
+                                            float bz, float ibx, float iby, float ibz, float rc2, float zb,
+                                            float zf, float zc, float& fix, float& fiy, float& fiz,
+                                            float3& gja, float3& gjb, double& te, double& tl, int& tn) {
   const unsigned full = 0xffffffffu;
-  const int src = (lane + 1) & 31;
   const float2 m1 = make_float2(-1.f, -1.f);
   const float2 px = make_float2(pi.x, pi.x), py = make_float2(pi.y, pi.y), pz = make_float2(pi.z, pi.z);
   const float2 pw = make_float2(pi.w, pi.w);
@@ -180,10 +175,9 @@ __device__ __forceinline__ void tile_mixed2(const MixStage& S, const float2* __r
   float2 gx = fx, gy = fx, gz = fx;                      // j forces of the a and b entries
 #pragma unroll 1
   for (int k0 = 0; k0 < 16; k0 += 4) {
-    const float4* __restrict__ sp = S.p2 + lane + k0;
-    const float4* __restrict__ sq = S.q2 + lane + k0;
-    const int2* __restrict__ st = S.t2 + lane + k0;
-    const int* __restrict__ st3 = reinterpret_cast<const int*>(S.t2) + lane + k0;
+    const float4* __restrict__ sp = S.p2 + sidx + k0;
+    const float4* __restrict__ sq = S.q2 + sidx + k0;
+    const int2* __restrict__ st = S.t2 + sidx + k0;
     const unsigned ma = m >> k0, mb = m >> (k0 + 16);
     float2 te4 = make_float2(0.f, 0.f), tl4 = te4;
 #pragma unroll
@@ -206,7 +200,7 @@ __device__ __forceinline__ void tile_mixed2(const MixStage& S, const float2* __r
       const float2 r6 = __fmul2_rn(__fmul2_rn(r2i, r2i), r2i);
       float2 c6, c12v;
       if (TRI) {
-        const float4 lj = s_lj3[row + st3[k]];
+        const float4 lj = s_lj3[row + st[k].x];
         c6 = make_float2(lj.x, lj.y);
         c12v = make_float2(lj.z, lj.w);
       } else {
@@ -243,152 +237,121 @@ __device__ __forceinline__ void tile_mixed2(const MixStage& S, const float2* __r
   fix += fx.x + fx.y;
   fiy += fy.x + fy.y;
   fiz += fz.x + fz.y;
-  gjx += gx.y + __shfl_sync(full, gx.x, lane ^ 16);
-  gjy += gy.y + __shfl_sync(full, gy.x, lane ^ 16);
-  gjz += gz.y + __shfl_sync(full, gz.x, lane ^ 16);
+  gja = make_float3(gx.x, gy.x, gz.x);
+  gjb = make_float3(gx.y, gy.y, gz.y);
 }
 
-// what a lane gathers for one tile before computing it: its j entry's atom and image
-// shift, its mask rows, and its i atom
+// what a lane gathers for a record pair before computing it: its two j entries a = l and
+// b = 16 + l of its record (position in the i block's frame with the charge, type word,
+// atom), its mask rows and its record's unit (-1: no record)
 struct Gather {
-  float4 pj;
-  float sx, sy, sz;
-  int tj, aj;
+  float4 pa, pb;
+  int ta, tb, aa, ab;
   unsigned m, me;
-  int bi;
+  int unit;
 };
 
-// One compact tile, every step branch-free.  ALSD: ci = cluster bit of the i atom; a pair
-// with nA cluster atoms has its force times f2 (nA = 2, class AA), f1 (AB) or f0 (BB: 1 but
-// while per-class outputs are evaluated), and its
-// energy also goes to ea (AA) / eb (AB).  CMM: no cut-off (rc2 is huge) and the Coulomb term
-// only for the pairs of `me` (the neighbouring-cell pairs; the rest are LJ only).
-// Energies: FP32 partial sums over 8 steps, accumulated in FP64.
-template <bool MINIMG, bool COUNT, bool ALSD, bool CMM>
-__device__ __forceinline__ void tile_mixed(const MixStage& S, const float2* __restrict__ s_lj, int row,
-                                           float4 pi, unsigned m, unsigned me, int lane, float bx, float by,
-                                           float bz, float ibx, float iby, float ibz, float rc2, float zb,
-                                           float zf, float zc, float& fix, float& fiy, float& fiz,
-                                           float& gjx, float& gjy, float& gjz, double& te, double& tl,
-                                           int& tn, int ci, float f0, float f1, float f2, double& ea,
-                                           double& eb) {
-  const unsigned full = 0xffffffffu;
-  const int src = (lane + 1) & 31;
-#pragma unroll 1
-  for (int k0 = 0; k0 < 32; k0 += 8) {
-    const float4* __restrict__ sp = S.pos + lane + k0;
-    const int* __restrict__ st = S.typ + lane + k0;
-    const unsigned mk = m >> k0, mek = me >> k0;
-    float te8 = 0.f, tl8 = 0.f, ea8 = 0.f, eb8 = 0.f;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const float4 pj = sp[k];
-      const int tjr = st[k];
-      float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-      if (MINIMG) {
-        dx = fmaf(-bx, rint1(dx * ibx), dx);
-        dy = fmaf(-by, rint1(dy * iby), dy);
-        dz = fmaf(-bz, rint1(dz * ibz), dz);
-      }
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      const bool in = ((mk >> k) & 1u) && r2 <= rc2;
-      const float rinv = rsqrt_ftz(in ? r2 : 1.f);
-      const float r2inv = rinv * rinv;
-      const float r6inv = r2inv * r2inv * r2inv;
-      const float2 lj = s_lj[row + (ALSD ? (tjr & kTypeMask) : tjr)];
-      const bool el = CMM ? ((mek >> k) & 1u) != 0u : true;
-      const float qq = el ? pi.w * pj.w : 0.f;
-      const float v1 = lj.x * r6inv;
-      const float v2 = lj.y * r6inv * r6inv;
-      const float eel = qq * (rinv + fmaf(zb, r2, -zc));
-      const float elj = v2 - v1;
-      float fs = fmaf(qq, fmaf(rinv, r2inv, -zf), fmaf(12.f, v2, -6.f * v1) * r2inv);
-      if (ALSD) {
-        const int na = ci + (tjr >> 30);
-        const float e = in ? eel + elj : 0.f;
-        ea8 += na == 2 ? e : 0.f;
-        eb8 += na == 1 ? e : 0.f;
-        fs *= na == 2 ? f2 : (na == 1 ? f1 : f0);
-      }
-      fs = in ? fs : 0.f;
-      te8 += in ? eel : 0.f;
-      tl8 += in ? elj : 0.f;
-      const float fx = dx * fs, fy = dy * fs, fz = dz * fs;
-      fix -= fx; fiy -= fy; fiz -= fz;
-      gjx += fx; gjy += fy; gjz += fz;
-      if (COUNT) tn += (in && el) ? 1 : 0;
-      gjx = __shfl_sync(full, gjx, src);
-      gjy = __shfl_sync(full, gjy, src);
-      gjz = __shfl_sync(full, gjz, src);
-    }
-    te += (double)te8;
-    tl += (double)tl8;
-    if (ALSD) {
-      ea += (double)ea8;
-      eb += (double)eb8;
-    }
+// One pair in the scalar form, branch-free like the packed step: d = x_i - x_j, and the
+// force scalar fs (F = -fs d on the i atom) and energies, all zero outside the mask (`bit`)
+// or the cut-off.  CMM: the Coulomb term only where `elbit` is set.
+template <bool MINIMG, bool CMM>
+__device__ __forceinline__ void pair_scalar(float4 pi, float xj, float yj, float zj, float qj, float2 lj,
+                                            bool bit, bool elbit, float bx, float by, float bz, float ibx,
+                                            float iby, float ibz, float rc2, float zb, float zf, float zc,
+                                            float& dx, float& dy, float& dz, float& fs, float& eel,
+                                            float& elj, bool& in) {
+  dx = pi.x - xj;
+  dy = pi.y - yj;
+  dz = pi.z - zj;
+  if (MINIMG) {
+    dx = fmaf(-bx, rint1(dx * ibx), dx);
+    dy = fmaf(-by, rint1(dy * iby), dy);
+    dz = fmaf(-bz, rint1(dz * ibz), dz);
   }
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  in = bit && r2 <= rc2;
+  const float rinv = rsqrt_ftz(in ? r2 : 1.f);
+  const float r2inv = rinv * rinv;
+  const float r6inv = r2inv * r2inv * r2inv;
+  const float qq = (CMM ? elbit : true) ? pi.w * qj : 0.f;
+  const float v1 = lj.x * r6inv;
+  const float v2 = lj.y * r6inv * r6inv;
+  const float e1 = qq * (rinv + fmaf(zb, r2, -zc));
+  const float e2 = v2 - v1;
+  const float f = fmaf(qq, fmaf(rinv, r2inv, -zf), fmaf(12.f, v2, -6.f * v1) * r2inv);
+  fs = in ? f : 0.f;
+  eel = in ? e1 : 0.f;
+  elj = in ? e2 : 0.f;
 }
 
-// One compact tile of a partial-McMD replica (GEPSME= AND / OR / XOR): the one-entry-per-step
-// form with each pair's class from the regions of its atoms (bit cj of trow = bits 3 ci..3 ci+2
-// of the replica's class table: class 1), the class-1 forces in accumulators of their own
-// (fi[3..5], gj[3..5], rotated like the class-2 ones) and the class-1 energy in ea.
-template <bool MINIMG, bool COUNT>
-__device__ __forceinline__ void tile_split(const MixStage& S, const float2* __restrict__ s_lj, int row,
-                                           float4 pi, unsigned m, int lane, float bx, float by, float bz,
-                                           float ibx, float iby, float ibz, float rc2, float zb, float zf,
-                                           float zc, float (&fi)[6], float (&gj)[6], double& te, double& tl,
-                                           int& tn, unsigned trow, double& ea) {
+// One record in the scalar form (ALSD, CMM and partial-McMD variants), the two entries of a
+// step one after the other, same staging and rotation as tile_mixed2.  ALSD: ci = cluster bit
+// of the i atom; a pair with nA cluster atoms has its force times f2 (nA = 2, class AA), f1
+// (AB) or f0 (BB: 1 but while per-class outputs are evaluated), and its energy also goes to
+// ea (AA) / eb (AB).  SPLIT (partial McMD): the pair's class from the regions of its atoms
+// (bit cj of trow: class 1), the class-1 forces in accumulators of their own (fi[3..5],
+// gj[6..11], rotated like the others) and the class-1 energy in ea.  CMM: no cut-off (rc2 is
+// huge) and the Coulomb term only for the pairs of `me`.  gj[0..5]: entries a and b.
+template <bool MINIMG, bool COUNT, bool ALSD, bool CMM, bool SPLIT>
+__device__ __forceinline__ void tile_scalar(const MixStage& S, const float2* __restrict__ s_lj, int row,
+                                            float4 pi, unsigned m, unsigned me, int sidx, int src, float bx,
+                                            float by, float bz, float ibx, float iby, float ibz, float rc2,
+                                            float zb, float zf, float zc, float (&fi)[6], float (&gj)[12],
+                                            double& te, double& tl, int& tn, int ci, float f0, float f1,
+                                            float f2, unsigned trow, double& ea, double& eb) {
   const unsigned full = 0xffffffffu;
-  const int src = (lane + 1) & 31;
+  constexpr int NG = SPLIT ? 12 : 6;
 #pragma unroll 1
-  for (int k0 = 0; k0 < 32; k0 += 8) {
-    const float4* __restrict__ sp = S.pos + lane + k0;
-    const int* __restrict__ st = S.typ + lane + k0;
-    const unsigned mk = m >> k0;
-    float te8 = 0.f, tl8 = 0.f, ea8 = 0.f;
+  for (int k0 = 0; k0 < 16; k0 += 4) {
+    float te4 = 0.f, tl4 = 0.f, ea4 = 0.f, eb4 = 0.f;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const float4 pj = sp[k];
-      const int tjr = st[k];
-      float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-      if (MINIMG) {
-        dx = fmaf(-bx, rint1(dx * ibx), dx);
-        dy = fmaf(-by, rint1(dy * iby), dy);
-        dz = fmaf(-bz, rint1(dz * ibz), dz);
+    for (int k = 0; k < 4; ++k) {
+      const float4 a = S.p2[sidx + k0 + k];
+      const float4 b = S.q2[sidx + k0 + k];
+      const int2 t = S.t2[sidx + k0 + k];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int tj = e ? t.y : t.x;
+        const int sh = k0 + k + 16 * e;
+        const float2 lj = s_lj[row + ((ALSD || SPLIT) ? (tj & kTypeMask) : tj)];
+        float dx, dy, dz, fs, eel, elj;
+        bool in;
+        pair_scalar<MINIMG, CMM>(pi, e ? a.y : a.x, e ? a.w : a.z, e ? b.y : b.x, e ? b.w : b.z, lj,
+                                 ((m >> sh) & 1u) != 0u, ((me >> sh) & 1u) != 0u, bx, by, bz, ibx, iby, ibz,
+                                 rc2, zb, zf, zc, dx, dy, dz, fs, eel, elj, in);
+        te4 += eel;
+        tl4 += elj;
+        float fs1 = 0.f;
+        if (SPLIT) {
+          const bool c1 = ((trow >> ((tj >> kRegionShift) & 3)) & 1u) != 0u;
+          ea4 += c1 ? eel + elj : 0.f;
+          fs1 = c1 ? fs : 0.f;
+          fs -= fs1;
+        } else if (ALSD) {
+          const int na = ci + ((tj >> 30) & 1);
+          ea4 += na == 2 ? eel + elj : 0.f;
+          eb4 += na == 1 ? eel + elj : 0.f;
+          fs *= na == 2 ? f2 : (na == 1 ? f1 : f0);
+        }
+        const float fx = dx * fs, fy = dy * fs, fz = dz * fs;
+        fi[0] -= fx; fi[1] -= fy; fi[2] -= fz;
+        gj[3 * e + 0] += fx; gj[3 * e + 1] += fy; gj[3 * e + 2] += fz;
+        if (SPLIT) {
+          const float hx = dx * fs1, hy = dy * fs1, hz = dz * fs1;
+          fi[3] -= hx; fi[4] -= hy; fi[5] -= hz;
+          gj[6 + 3 * e + 0] += hx; gj[6 + 3 * e + 1] += hy; gj[6 + 3 * e + 2] += hz;
+        }
+        if (COUNT) tn += (in && (CMM ? ((me >> sh) & 1u) != 0u : true)) ? 1 : 0;
       }
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      const bool in = ((mk >> k) & 1u) && r2 <= rc2;
-      const float rinv = rsqrt_ftz(in ? r2 : 1.f);
-      const float r2inv = rinv * rinv;
-      const float r6inv = r2inv * r2inv * r2inv;
-      const float2 lj = s_lj[row + (tjr & kTypeMask)];
-      const float qq = pi.w * pj.w;
-      const float v1 = lj.x * r6inv;
-      const float v2 = lj.y * r6inv * r6inv;
-      const float eel = qq * (rinv + fmaf(zb, r2, -zc));
-      const float elj = v2 - v1;
-      float fs = fmaf(qq, fmaf(rinv, r2inv, -zf), fmaf(12.f, v2, -6.f * v1) * r2inv);
-      const bool c1 = ((trow >> ((tjr >> kRegionShift) & 3)) & 1u) != 0u;
-      fs = in ? fs : 0.f;
-      te8 += in ? eel : 0.f;
-      tl8 += in ? elj : 0.f;
-      ea8 += (in && c1) ? eel + elj : 0.f;
-      const float fs1 = c1 ? fs : 0.f, fs2 = fs - fs1;
-      const float ax = dx * fs2, ay = dy * fs2, az = dz * fs2;
-      const float bxf = dx * fs1, byf = dy * fs1, bzf = dz * fs1;
-      fi[0] -= ax; fi[1] -= ay; fi[2] -= az;
-      fi[3] -= bxf; fi[4] -= byf; fi[5] -= bzf;
-      gj[0] += ax; gj[1] += ay; gj[2] += az;
-      gj[3] += bxf; gj[4] += byf; gj[5] += bzf;
-      if (COUNT) tn += in ? 1 : 0;
 #pragma unroll
-      for (int q = 0; q < 6; ++q) gj[q] = __shfl_sync(full, gj[q], src);
+      for (int q = 0; q < NG; ++q) gj[q] = __shfl_sync(full, gj[q], src);
     }
-    te += (double)te8;
-    tl += (double)tl8;
-    ea += (double)ea8;
+    te += (double)te4;
+    tl += (double)tl4;
+    if (ALSD || SPLIT) {
+      ea += (double)ea4;
+      eb += (double)eb4;
+    }
   }
 }
 
@@ -414,27 +377,31 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
       s_lj3[i] = make_float4(a.x, b.x, a.y, b.y);
     }
   const int lane = threadIdx.x & 31;
+  const int hw = lane >> 4, lp = lane & (kHalf - 1);   // half-warp, lane inside it
+  const int sidx = 32 * hw + lp;                        // this lane's staging slot
+  const int src = ((lp + 1) & (kHalf - 1)) | (hw << 4); // rotation: from the next lane of the half
   MixStage& S = s_stage[threadIdx.x >> 5];
   if (lane == 0) {
     mbar_init(&S.bar[0]);
     mbar_init(&S.bar[1]);
   }
   __syncthreads();
-  const int T = *P.nctiles;
-  // a 640-byte copy lands in microseconds; the bound (about a second of SM clock) only ends
+  const int T = *P.nctiles;         // records
+  const int TU = (T + 1) >> 1;      // record pairs: a warp's work units
+  // a 1.2-KiB copy lands in microseconds; the bound (about a second of SM clock) only ends
   // the wait on a broken device, and it is not the integrator's adjustable barrier bound:
   // a block must never leave with one of its copies still in flight
   const long long wlim = kCopyWaitCycles;
   const float rc2 = (float)z.rc2, zb = (float)z.bcoeff, zf = (float)z.fcoeff, zc = (float)z.zcore;
-  const unsigned txb = CMM ? 768u : 640u;
+  const unsigned txb = CMM ? 1280u : 1152u;
   unsigned phase = 0u, pend = 0u;   // per buffer: barrier parity to wait for; copy in flight
   bool ok = true;
 
-  // tiles are claimed in runs of `run` consecutive ones: the tiles of an i block are
+  // record pairs are claimed in runs of `run` consecutive ones: the records of a unit are
   // consecutive, so a run mostly keeps its i atoms (no reload, no i-force flush between
-  // tiles); the run is short enough that every warp still gets several (8 per warp at most
-  // of the total, 1 to 16 tiles)
-  const int run = max(1, min(16, T / (int)(gridDim.x * kPairWarps * 8)));
+  // records); the run is short enough that every warp still gets several (8 per warp at most
+  // of the total, 1 to 16 pairs)
+  const int run = max(1, min(16, TU / (int)(gridDim.x * kPairWarps * 8)));
   int run_next = 0, run_end = 0;
   auto claim = [&]() {
     if (run_next >= run_end) {
@@ -442,21 +409,36 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
       if (lane == 0) t = atomicAdd(P.tile_ctr, run);
       t = __shfl_sync(full, t, 0);
       run_next = t;
-      run_end = min(t + run, T);
+      run_end = min(t + run, TU);
     }
-    return run_next < run_end ? run_next++ : T;
+    return run_next < run_end ? run_next++ : TU;
   };
+  // the entries and masks of records 2t and 2t + 1 into buffer b (one past the last record
+  // is padding inside the arrays: read, never used)
   auto issue = [&](int t, int b) {
     if (lane == 0) {
       fence_proxy_async();
       mbar_expect(&S.bar[b], txb);
-      bulk_load(S.ent[b], P.ct_j + (size_t)t * 32, 512u, &S.bar[b]);
+      bulk_load(S.ent[b], P.ct_j + (size_t)t * 64, 1024u, &S.bar[b]);
       bulk_load(S.msk[b], P.ct_mask + (size_t)t * 32, 128u, &S.bar[b]);
       if (CMM) bulk_load(S.msk_el[b], P.ct_mask_el + (size_t)t * 32, 128u, &S.bar[b]);
     }
     pend |= 1u << b;
   };
-  // tile t's copy has landed in buffer b: start the gathers of its atoms
+  auto gather1 = [&](float4 e, bool valid, float4& p, int& ty, int& at) {
+    const int sj = valid ? __float_as_int(e.w) : -1;
+    if (sj >= 0) {
+      const float4 q = P.pos_f[sj];
+      p = make_float4(q.x - e.x, q.y - e.y, q.z - e.z, q.w);   // into the i block's frame
+      ty = P.styp[sj];
+      at = P.satom[sj];
+    } else {
+      p = make_float4(0.f, 0.f, 0.f, 0.f);
+      ty = z.nt1 - 1;   // the zero dummy type
+      at = -1;
+    }
+  };
+  // pair t's copy has landed in buffer b: start the gathers of this lane's two entries
   auto fetch = [&](int t, int b, Gather& G) {
     if (!mbar_wait(&S.bar[b], (phase >> b) & 1u, wlim)) {
       ok = false;
@@ -465,73 +447,53 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     }
     phase ^= 1u << b;
     pend &= ~(1u << b);
-    const float4 e = S.ent[b][lane];
-    G.m = S.msk[b][lane];
-    G.me = CMM ? S.msk_el[b][lane] : 0u;
-    const int sj = __float_as_int(e.w);
-    G.sx = e.x; G.sy = e.y; G.sz = e.z;
-    if (sj >= 0) {
-      G.pj = P.pos_f[sj];
-      G.tj = P.styp[sj];
-      G.aj = P.satom[sj];
-    } else {
-      G.pj = make_float4(0.f, 0.f, 0.f, 0.f);
-      G.tj = z.nt1 - 1;   // the zero dummy type
-      G.aj = -1;
-    }
-    G.bi = P.ct_blk[t];
+    const int rec = 2 * t + hw;
+    const bool valid = rec < T;
+    G.m = valid ? S.msk[b][lane] : 0u;
+    G.me = CMM && valid ? S.msk_el[b][lane] : 0u;
+    G.unit = valid ? P.ct_blk[rec] : -1;
+    gather1(S.ent[b][32 * hw + lp], valid, G.pa, G.ta, G.aa);
+    gather1(S.ent[b][32 * hw + kHalf + lp], valid, G.pb, G.tb, G.ab);
   };
 
-  int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
+  int cur_unit = -2, cur_rep = -1, rep = -1, ai = -1, ti = 0;
   float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
   long long gix = 0, giy = 0, giz = 0;
   long long gix1 = 0, giy1 = 0, giz1 = 0;   // partial McMD: class-1 i forces
   long long eel = 0, elj = 0, eaa = 0, eab = 0;
   long long npair = 0;
-  bool mi = true;
+  bool mi = false;
   float bx = 0.f, by = 0.f, bz = 0.f, ibx = 0.f, iby = 0.f, ibz = 0.f;
   float f0 = 1.f, f1 = 1.f, f2 = 1.f;
   unsigned tab = 0u;
 
-  int t = claim(), tn = T;
+  int t = claim(), tn = TU;
   Gather G;
-  if (t < T) {
+  if (t < TU) {
     issue(t, 0);
     tn = claim();
-    if (tn < T) issue(tn, 1);
+    if (tn < TU) issue(tn, 1);
     fetch(t, 0, G);
   }
   int b = 0;
-  while (t < T && ok) {
-    // the tile's j atoms into the warp's stage, in the i block's frame
+  while (t < TU && ok) {
+    // this lane's two entries into the stage, twice
     __syncwarp();
-    const float4 pj = make_float4(G.pj.x - G.sx, G.pj.y - G.sy, G.pj.z - G.sz, G.pj.w);
-    if (ALSD || CMM) {
-      S.pos[lane] = pj;
-      S.pos[lane + 32] = pj;
-      S.typ[lane] = G.tj;
-      S.typ[lane + 32] = G.tj;
-    } else {   // entry e beside entry e + 16 (the lane l ^ 16 holds it)
-      const float ox = __shfl_xor_sync(0xffffffffu, pj.x, 16), oy = __shfl_xor_sync(0xffffffffu, pj.y, 16);
-      const float oz = __shfl_xor_sync(0xffffffffu, pj.z, 16), ow = __shfl_xor_sync(0xffffffffu, pj.w, 16);
-      const int ot = __shfl_xor_sync(0xffffffffu, G.tj, 16);
-      const float4 a = make_float4(pj.x, ox, pj.y, oy), b = make_float4(pj.z, oz, pj.w, ow);
-      S.p2[lane] = a;
-      S.p2[lane + 32] = a;
-      S.q2[lane] = b;
-      S.q2[lane + 32] = b;
-      if (TRI) {   // the a * nt1 + b index of the type-triple table
-        int* t3 = reinterpret_cast<int*>(S.t2);
-        t3[lane] = G.tj * z.nt1 + ot;
-        t3[lane + 32] = G.tj * z.nt1 + ot;
-      } else {
-        S.t2[lane] = make_int2(G.tj, ot);
-        S.t2[lane + 32] = make_int2(G.tj, ot);
-      }
+    {
+      const float4 p2 = make_float4(G.pa.x, G.pb.x, G.pa.y, G.pb.y);
+      const float4 q2 = make_float4(G.pa.z, G.pb.z, G.pa.w, G.pb.w);
+      const int2 t2 = TRI ? make_int2(G.ta * z.nt1 + G.tb, 0) : make_int2(G.ta, G.tb);
+      S.p2[sidx] = p2;
+      S.p2[sidx + kHalf] = p2;
+      S.q2[sidx] = q2;
+      S.q2[sidx + kHalf] = q2;
+      S.t2[sidx] = t2;
+      S.t2[sidx + kHalf] = t2;
     }
     const unsigned m = G.m, me = G.me;
-    const int aj = G.aj, bi = G.bi;
-    if (bi != cur_bi) {
+    const int aa = G.aa, ab = G.ab, unit = G.unit;
+    // the lane's i atom: a new unit flushes the last one's force and loads the new atom
+    if (unit != cur_unit) {
       if (ai >= 0 && (gix | giy | giz)) {
         atomic_add_ll(&P.frc[3 * ai + 0], gix);
         atomic_add_ll(&P.frc[3 * ai + 1], giy);
@@ -544,16 +506,25 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
       }
       gix = giy = giz = 0;
       gix1 = giy1 = giz1 = 0;
-      cur_bi = bi;
-      const int si = bi * kTile + lane;
-      pi = P.pos_f[si];
-      ti = P.styp[si];
-      ai = P.satom[si];
-      const int rep = P.blk_rep[bi];
+      cur_unit = unit;
+      if (unit >= 0) {
+        const int si = (unit >> 1) * kTile + (unit & 1) * kHalf + lp;
+        pi = P.pos_f[si];
+        ti = P.styp[si];
+        ai = P.satom[si];
+        rep = P.blk_rep[unit >> 1];
+      } else {
+        pi = make_float4(0.f, 0.f, 0.f, 0.f);
+        ti = z.nt1 - 1;
+        ai = -1;
+      }
+    }
+    // a new replica in either half: both halves' energies go to their replicas so far
+    if (__any_sync(full, rep != cur_rep)) {
+      flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD || SPLIT);
+      eel = elj = eaa = eab = 0;
+      npair = 0;
       if (rep != cur_rep) {
-        if (cur_rep >= 0) flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
-        eel = elj = eaa = eab = 0;
-        npair = 0;
         cur_rep = rep;
         const Rep& R = P.reps[rep];
         bx = (float)R.box[0]; by = (float)R.box[1]; bz = (float)R.box[2];
@@ -580,70 +551,72 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
         }
       }
     }
+    const bool wmi = __any_sync(full, mi);   // one image form for the whole warp
     __syncwarp();
-    // buffer b is free again: the tile after next goes into it; the next tile's gathers
-    // are issued before this tile's arithmetic
-    int t2 = T;
-    if (tn < T) {
+    // buffer b is free again: the pair after next goes into it; the next pair's gathers
+    // are issued before this pair's arithmetic
+    int t2 = TU;
+    if (tn < TU) {
       t2 = claim();
-      if (t2 < T) issue(t2, b);
+      if (t2 < TU) issue(t2, b);
     }
     Gather Gn;
-    if (tn < T) fetch(tn, b ^ 1, Gn);
-    float gjx = 0.f, gjy = 0.f, gjz = 0.f;
+    if (tn < TU) fetch(tn, b ^ 1, Gn);
     float fix = 0.f, fiy = 0.f, fiz = 0.f;
-    float fi6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, gj6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float3 gja = make_float3(0.f, 0.f, 0.f), gjb = gja, gja1 = gja, gjb1 = gja;
     double te = 0.0, tl = 0.0, ea = 0.0, eb = 0.0;
     int tn_pairs = 0;
-    const int ci = ALSD ? (ti >> 30) : 0;
-    const int row = (ALSD ? (ti & kTypeMask) : ti) * z.nt1;
-    if (SPLIT) {
-      const unsigned trow = tab >> (3 * ((ti >> kRegionShift) & 3));
-      if (mi)
-        tile_split<true, COUNT>(S, s_lj, row, pi, m, lane, bx, by, bz, ibx, iby, ibz, rc2, zb, zf, zc, fi6,
-                                gj6, te, tl, tn_pairs, trow, ea);
+    const int ci = ALSD ? ((ti >> 30) & 1) : 0;
+    const int row = ((ALSD || SPLIT) ? (ti & kTypeMask) : ti) * z.nt1;
+    if (ALSD || CMM || SPLIT) {
+      float fi6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      float gj[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      const unsigned trow = SPLIT ? tab >> (3 * ((ti >> kRegionShift) & 3)) : 0u;
+      if (wmi)
+        tile_scalar<true, COUNT, ALSD, CMM, SPLIT>(S, s_lj, row, pi, m, me, sidx, src, bx, by, bz, ibx, iby,
+                                                   ibz, rc2, zb, zf, zc, fi6, gj, te, tl, tn_pairs, ci, f0,
+                                                   f1, f2, trow, ea, eb);
       else
-        tile_split<false, COUNT>(S, s_lj, row, pi, m, lane, bx, by, bz, ibx, iby, ibz, rc2, zb, zf, zc, fi6,
-                                 gj6, te, tl, tn_pairs, trow, ea);
+        tile_scalar<false, COUNT, ALSD, CMM, SPLIT>(S, s_lj, row, pi, m, me, sidx, src, bx, by, bz, ibx, iby,
+                                                    ibz, rc2, zb, zf, zc, fi6, gj, te, tl, tn_pairs, ci, f0,
+                                                    f1, f2, trow, ea, eb);
       fix = fi6[0]; fiy = fi6[1]; fiz = fi6[2];
-      gjx = gj6[0]; gjy = gj6[1]; gjz = gj6[2];
-    } else if (ALSD || CMM) {
-      if (mi)
-        tile_mixed<true, COUNT, ALSD, CMM>(S, s_lj, row, pi, m, me, lane, bx, by, bz, ibx, iby, ibz, rc2, zb,
-                                           zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci, f0,
-                                           f1, f2, ea, eb);
-      else
-        tile_mixed<false, COUNT, ALSD, CMM>(S, s_lj, row, pi, m, me, lane, bx, by, bz, ibx, iby, ibz, rc2,
-                                            zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs, ci,
-                                            f0, f1, f2, ea, eb);
-    } else if (mi) {
-      tile_mixed2<true, COUNT, TRI>(S, s_lj, s_lj3, TRI ? ti * nlj : row, pi, m, lane, bx, by, bz, ibx, iby,
-                                    ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs);
-    } else {
-      tile_mixed2<false, COUNT, TRI>(S, s_lj, s_lj3, TRI ? ti * nlj : row, pi, m, lane, bx, by, bz, ibx, iby,
-                                     ibz, rc2, zb, zf, zc, fix, fiy, fiz, gjx, gjy, gjz, te, tl, tn_pairs);
-    }
-    if (aj >= 0 && (gjx != 0.f || gjy != 0.f || gjz != 0.f)) {
-      atomic_add_ll(&P.frc[3 * aj + 0], to_fix((double)gjx, kFrcScale, P.status));
-      atomic_add_ll(&P.frc[3 * aj + 1], to_fix((double)gjy, kFrcScale, P.status));
-      atomic_add_ll(&P.frc[3 * aj + 2], to_fix((double)gjz, kFrcScale, P.status));
-    }
-    gix += to_fix((double)fix, kFrcScale, P.status);
-    giy += to_fix((double)fiy, kFrcScale, P.status);
-    giz += to_fix((double)fiz, kFrcScale, P.status);
-    if (SPLIT) {
-      if (aj >= 0 && (gj6[3] != 0.f || gj6[4] != 0.f || gj6[5] != 0.f)) {
-        atomic_add_ll(&P.frc1[3 * aj + 0], to_fix((double)gj6[3], kFrcScale, P.status));
-        atomic_add_ll(&P.frc1[3 * aj + 1], to_fix((double)gj6[4], kFrcScale, P.status));
-        atomic_add_ll(&P.frc1[3 * aj + 2], to_fix((double)gj6[5], kFrcScale, P.status));
+      gja = make_float3(gj[0], gj[1], gj[2]);
+      gjb = make_float3(gj[3], gj[4], gj[5]);
+      if (SPLIT) {
+        gja1 = make_float3(gj[6], gj[7], gj[8]);
+        gjb1 = make_float3(gj[9], gj[10], gj[11]);
+        gix1 += to_fix_f(fi6[3], P.status);
+        giy1 += to_fix_f(fi6[4], P.status);
+        giz1 += to_fix_f(fi6[5], P.status);
       }
-      gix1 += to_fix((double)fi6[3], kFrcScale, P.status);
-      giy1 += to_fix((double)fi6[4], kFrcScale, P.status);
-      giz1 += to_fix((double)fi6[5], kFrcScale, P.status);
+    } else if (wmi) {
+      tile_mixed2<true, COUNT, TRI>(S, s_lj, s_lj3, TRI ? ti * nlj : row, pi, m, sidx, src, bx, by, bz, ibx,
+                                    iby, ibz, rc2, zb, zf, zc, fix, fiy, fiz, gja, gjb, te, tl, tn_pairs);
+    } else {
+      tile_mixed2<false, COUNT, TRI>(S, s_lj, s_lj3, TRI ? ti * nlj : row, pi, m, sidx, src, bx, by, bz,
+                                     ibx, iby, ibz, rc2, zb, zf, zc, fix, fiy, fiz, gja, gjb, te, tl,
+                                     tn_pairs);
     }
+    auto add_j = [&](long long* f, int aj, float3 g) {
+      if (aj >= 0 && (g.x != 0.f || g.y != 0.f || g.z != 0.f)) {
+        atomic_add_ll(&f[3 * aj + 0], to_fix_f(g.x, P.status));
+        atomic_add_ll(&f[3 * aj + 1], to_fix_f(g.y, P.status));
+        atomic_add_ll(&f[3 * aj + 2], to_fix_f(g.z, P.status));
+      }
+    };
+    add_j(P.frc, aa, gja);
+    add_j(P.frc, ab, gjb);
+    if (SPLIT) {
+      add_j(P.frc1, aa, gja1);
+      add_j(P.frc1, ab, gjb1);
+    }
+    gix += to_fix_f(fix, P.status);
+    giy += to_fix_f(fiy, P.status);
+    giz += to_fix_f(fiz, P.status);
     eel += to_fix(te, kEneScale, P.status);
     elj += to_fix(tl, kEneScale, P.status);
-    if (ALSD) {
+    if (ALSD || SPLIT) {
       eaa += to_fix(ea, kEneScale, P.status);
       eab += to_fix(eb, kEneScale, P.status);
     }
@@ -663,16 +636,17 @@ k_pair_mixed(DevPtrs P, ZdConst z) {
     atomic_add_ll(&P.frc1[3 * ai + 1], giy1);
     atomic_add_ll(&P.frc1[3 * ai + 2], giz1);
   }
-  flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
+  flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD || SPLIT);
   // a copy still in flight (only after a timed-out wait) must land before the block exits
   for (int k = 0; k < 2; ++k)
     if ((pend >> k) & 1u) mbar_wait(&S.bar[k], (phase >> k) & 1u, wlim);
 }
 
-// Per-warp shared memory of the FP64 kernel: the tile's j atoms, twice (see MixStage).
+// Per-warp shared memory of the FP64 kernel: each half-warp's record, entries a and b of
+// every lane, twice (see MixStage).
 struct __align__(16) F64Stage {
-  double4 pos[64];
-  int typ[64];
+  double4 pa[64], pb[64];
+  int2 t[64];
 };
 
 template <bool COUNT, bool ALSD, bool CMM, bool SPLIT = false>
@@ -680,51 +654,69 @@ __global__ void __launch_bounds__(kPairThreads)
 k_pair_fp64(DevPtrs P, ZdConst z) {
   extern __shared__ double2 s_ljd[];
   __shared__ F64Stage s_stage[kPairWarps];
+  const unsigned full = 0xffffffffu;
   const int nlj = z.nt1 * z.nt1;
   for (int i = threadIdx.x; i < nlj; i += blockDim.x) s_ljd[i] = P.lj_d[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
+  const int hw = lane >> 4, lp = lane & (kHalf - 1);
+  const int sidx = 32 * hw + lp;
+  const int src = ((lp + 1) & (kHalf - 1)) | (hw << 4);
   F64Stage& S = s_stage[threadIdx.x >> 5];
   const int T = *P.nctiles;
+  const int TU = (T + 1) >> 1;
   const double irlim2 = 1.0 / z.rc2;
-  int cur_bi = -1, cur_rep = -1, ai = -1, ti = 0;
+  int cur_unit = -2, cur_rep = -1, rep = -1, ai = -1, ti = 0;
   double4 pi = make_double4(0, 0, 0, 0);
   double gix = 0, giy = 0, giz = 0;
   double gix1 = 0, giy1 = 0, giz1 = 0;            // partial McMD: class-1 i forces
-  long long eel = 0, elj = 0, eaa = 0, eab = 0;   // fixed point, per tile
+  long long eel = 0, elj = 0, eaa = 0, eab = 0;   // fixed point, per record
   long long npair = 0;
   double bx = 0, by = 0, bz = 0, ibx = 0, iby = 0, ibz = 0;
   double f0 = 1.0, f1 = 1.0, f2 = 1.0;
   unsigned tab = 0u;
+  auto flush_i = [&]() {
+    if (ai >= 0) {
+      atomicAdd(&P.grd[3 * ai + 0], gix);
+      atomicAdd(&P.grd[3 * ai + 1], giy);
+      atomicAdd(&P.grd[3 * ai + 2], giz);
+      if (SPLIT) {
+        atomicAdd(&P.grd1[3 * ai + 0], gix1);
+        atomicAdd(&P.grd1[3 * ai + 1], giy1);
+        atomicAdd(&P.grd1[3 * ai + 2], giz1);
+      }
+    }
+    gix = giy = giz = 0;
+    gix1 = giy1 = giz1 = 0;
+  };
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(P.tile_ctr, 1);
-    t = __shfl_sync(0xffffffffu, t, 0);
-    if (t >= T) break;
-    const int bi = P.ct_blk[t];
-    if (bi != cur_bi) {
-      if (ai >= 0) {
-        atomicAdd(&P.grd[3 * ai + 0], gix);
-        atomicAdd(&P.grd[3 * ai + 1], giy);
-        atomicAdd(&P.grd[3 * ai + 2], giz);
-        if (SPLIT) {
-          atomicAdd(&P.grd1[3 * ai + 0], gix1);
-          atomicAdd(&P.grd1[3 * ai + 1], giy1);
-          atomicAdd(&P.grd1[3 * ai + 2], giz1);
-        }
+    t = __shfl_sync(full, t, 0);
+    if (t >= TU) break;
+    const int rec = 2 * t + hw;
+    const bool valid = rec < T;
+    const int unit = valid ? P.ct_blk[rec] : -1;
+    if (unit != cur_unit) {
+      flush_i();
+      cur_unit = unit;
+      if (unit >= 0) {
+        const int si = (unit >> 1) * kTile + (unit & 1) * kHalf + lp;
+        pi = P.pos_d[si];
+        ti = P.styp[si];
+        ai = P.satom[si];
+        rep = P.blk_rep[unit >> 1];
+      } else {
+        pi = make_double4(0, 0, 0, 0);
+        ti = z.nt1 - 1;
+        ai = -1;
       }
-      gix = giy = giz = 0;
-      gix1 = giy1 = giz1 = 0;
-      cur_bi = bi;
-      const int s = cur_bi * kTile + lane;
-      pi = P.pos_d[s];
-      ti = P.styp[s];
-      ai = P.satom[s];
-      const int rep = P.blk_rep[cur_bi];
+    }
+    if (__any_sync(full, rep != cur_rep)) {
+      flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD || SPLIT);
+      eel = elj = eaa = eab = 0;
+      npair = 0;
       if (rep != cur_rep) {
-        if (cur_rep >= 0) flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
-        eel = elj = eaa = eab = 0;
-        npair = 0;
         cur_rep = rep;
         const Rep& R = P.reps[rep];
         bx = R.box[0]; by = R.box[1]; bz = R.box[2];
@@ -737,105 +729,101 @@ k_pair_fp64(DevPtrs P, ZdConst z) {
         if (SPLIT) tab = R.split ? R.cls_tab : 0u;
       }
     }
-    const unsigned m = P.ct_mask[(size_t)t * 32 + lane];
-    const unsigned me = CMM ? P.ct_mask_el[(size_t)t * 32 + lane] : 0u;
-    const int sj = __float_as_int(P.ct_j[(size_t)t * 32 + lane].w);
-    const double4 pj = sj >= 0 ? P.pos_d[sj] : make_double4(0.0, 0.0, 0.0, 0.0);
-    const int tjv = sj >= 0 ? P.styp[sj] : z.nt1 - 1;
-    const int aj = sj >= 0 ? P.satom[sj] : -1;
+    const unsigned m = valid ? P.ct_mask[(size_t)rec * kHalf + lp] : 0u;
+    const unsigned me = CMM && valid ? P.ct_mask_el[(size_t)rec * kHalf + lp] : 0u;
+    int aj[2], tjv[2];
+    double4 pj[2];
+    for (int e = 0; e < 2; ++e) {
+      const int sj = valid ? __float_as_int(P.ct_j[(size_t)rec * 32 + kHalf * e + lp].w) : -1;
+      pj[e] = sj >= 0 ? P.pos_d[sj] : make_double4(0.0, 0.0, 0.0, 0.0);
+      tjv[e] = sj >= 0 ? P.styp[sj] : z.nt1 - 1;
+      aj[e] = sj >= 0 ? P.satom[sj] : -1;
+    }
     __syncwarp();
-    S.pos[lane] = pj;
-    S.pos[lane + 32] = pj;
-    S.typ[lane] = tjv;
-    S.typ[lane + 32] = tjv;
+    S.pa[sidx] = pj[0];
+    S.pa[sidx + kHalf] = pj[0];
+    S.pb[sidx] = pj[1];
+    S.pb[sidx + kHalf] = pj[1];
+    S.t[sidx] = make_int2(tjv[0], tjv[1]);
+    S.t[sidx + kHalf] = make_int2(tjv[0], tjv[1]);
     __syncwarp();
-    const int row = (ALSD ? (ti & kTypeMask) : ti) * z.nt1;
-    const int ci = ALSD ? (ti >> 30) : 0;
+    const int row = ((ALSD || SPLIT) ? (ti & kTypeMask) : ti) * z.nt1;
+    const int ci = ALSD ? ((ti >> 30) & 1) : 0;
     const unsigned trow = SPLIT ? tab >> (3 * ((ti >> kRegionShift) & 3)) : 0u;
-    double gjx = 0, gjy = 0, gjz = 0;
-    double gjx1 = 0, gjy1 = 0, gjz1 = 0;
+    constexpr int NG = SPLIT ? 12 : 6;
+    double gj[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};   // entries a, b; class 1 a, b
     int tn = 0;
-    double te = 0.0, tl = 0.0, ta = 0.0, tb = 0.0;   // this tile's energies
-    const int src = (lane + 1) & 31;
-#pragma unroll 4
-    for (int k = 0; k < 32; ++k) {
-      if ((m >> k) & 1u) {
-        const double4 q = S.pos[lane + k];
-        const int tj = S.typ[lane + k];
-        double dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
-        dx -= bx * anint(dx * ibx);
-        dy -= by * anint(dy * iby);
-        dz -= bz * anint(dz * ibz);
-        const double dd2 = dx * dx + dy * dy + dz * dz;
-        const double dd2i = 1.0 / dd2;
-        if (dd2i - irlim2 >= 0.0) {
-          const double ddi = sqrt(dd2i);
-          const double dd6i = dd2i * dd2i * dd2i;
-          const bool elp = CMM ? ((me >> k) & 1u) != 0u : true;
-          const double ee = elp ? pi.w * q.w : 0.0;
-          const double epair = ee * (ddi + z.bcoeff * dd2 - z.zcore);
-          te += epair;
-          const double2 lj = s_ljd[row + (ALSD ? (tj & kTypeMask) : tj)];
-          const double v1 = lj.x * dd6i;
-          const double v2 = lj.y * dd6i * dd6i;
-          tl += -v1 + v2;
-          double cc = ee * (dd2i * ddi - z.fcoeff) + (-6.0 * v1 + 12.0 * v2) * dd2i;
-          bool c1 = false;
-          if (SPLIT) {   // partial McMD: class 1 by the regions of the two atoms
-            c1 = ((trow >> ((tj >> kRegionShift) & 3)) & 1u) != 0u;
-            if (c1) ta += epair + (-v1 + v2);
-          } else if (ALSD) {
-            const int na = ci + (tj >> 30);
-            if (na == 2) { ta += epair + (-v1 + v2); cc *= f2; }
-            else if (na == 1) { tb += epair + (-v1 + v2); cc *= f1; }
-            else cc *= f0;
+    double te = 0.0, tl = 0.0, ta = 0.0, tb = 0.0;   // this record's energies
+#pragma unroll 2
+    for (int k = 0; k < kHalf; ++k) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int sh = k + kHalf * e;
+        if ((m >> sh) & 1u) {
+          const double4 q = e ? S.pb[sidx + k] : S.pa[sidx + k];
+          const int tj = e ? S.t[sidx + k].y : S.t[sidx + k].x;
+          double dx = pi.x - q.x, dy = pi.y - q.y, dz = pi.z - q.z;
+          dx -= bx * anint(dx * ibx);
+          dy -= by * anint(dy * iby);
+          dz -= bz * anint(dz * ibz);
+          const double dd2 = dx * dx + dy * dy + dz * dz;
+          const double dd2i = 1.0 / dd2;
+          if (dd2i - irlim2 >= 0.0) {
+            const double ddi = sqrt(dd2i);
+            const double dd6i = dd2i * dd2i * dd2i;
+            const bool elp = CMM ? ((me >> sh) & 1u) != 0u : true;
+            const double ee = elp ? pi.w * q.w : 0.0;
+            const double epair = ee * (ddi + z.bcoeff * dd2 - z.zcore);
+            te += epair;
+            const double2 lj = s_ljd[row + ((ALSD || SPLIT) ? (tj & kTypeMask) : tj)];
+            const double v1 = lj.x * dd6i;
+            const double v2 = lj.y * dd6i * dd6i;
+            tl += -v1 + v2;
+            double cc = ee * (dd2i * ddi - z.fcoeff) + (-6.0 * v1 + 12.0 * v2) * dd2i;
+            bool c1 = false;
+            if (SPLIT) {   // partial McMD: class 1 by the regions of the two atoms
+              c1 = ((trow >> ((tj >> kRegionShift) & 3)) & 1u) != 0u;
+              if (c1) ta += epair + (-v1 + v2);
+            } else if (ALSD) {
+              const int na = ci + ((tj >> 30) & 1);
+              if (na == 2) { ta += epair + (-v1 + v2); cc *= f2; }
+              else if (na == 1) { tb += epair + (-v1 + v2); cc *= f1; }
+              else cc *= f0;
+            }
+            const double fx = dx * cc, fy = dy * cc, fz = dz * cc;
+            if (SPLIT && c1) {
+              gix1 -= fx; giy1 -= fy; giz1 -= fz;
+              gj[6 + 3 * e] += fx; gj[7 + 3 * e] += fy; gj[8 + 3 * e] += fz;
+            } else {
+              gix -= fx; giy -= fy; giz -= fz;
+              gj[3 * e] += fx; gj[1 + 3 * e] += fy; gj[2 + 3 * e] += fz;
+            }
+            if (COUNT && elp) ++tn;
           }
-          const double fx = dx * cc, fy = dy * cc, fz = dz * cc;
-          if (SPLIT && c1) {
-            gix1 -= fx; giy1 -= fy; giz1 -= fz;
-            gjx1 += fx; gjy1 += fy; gjz1 += fz;
-          } else {
-            gix -= fx; giy -= fy; giz -= fz;
-            gjx += fx; gjy += fy; gjz += fz;
-          }
-          if (COUNT && elp) ++tn;
         }
       }
-      gjx = __shfl_sync(0xffffffffu, gjx, src);
-      gjy = __shfl_sync(0xffffffffu, gjy, src);
-      gjz = __shfl_sync(0xffffffffu, gjz, src);
-      if (SPLIT) {
-        gjx1 = __shfl_sync(0xffffffffu, gjx1, src);
-        gjy1 = __shfl_sync(0xffffffffu, gjy1, src);
-        gjz1 = __shfl_sync(0xffffffffu, gjz1, src);
+#pragma unroll
+      for (int q = 0; q < NG; ++q) gj[q] = __shfl_sync(full, gj[q], src);
+    }
+    for (int e = 0; e < 2; ++e) {
+      if (aj[e] >= 0 && (gj[3 * e] != 0.0 || gj[1 + 3 * e] != 0.0 || gj[2 + 3 * e] != 0.0)) {
+        atomicAdd(&P.grd[3 * aj[e] + 0], gj[3 * e]);
+        atomicAdd(&P.grd[3 * aj[e] + 1], gj[1 + 3 * e]);
+        atomicAdd(&P.grd[3 * aj[e] + 2], gj[2 + 3 * e]);
       }
-    }
-    if (aj >= 0 && (gjx != 0.0 || gjy != 0.0 || gjz != 0.0)) {
-      atomicAdd(&P.grd[3 * aj + 0], gjx);
-      atomicAdd(&P.grd[3 * aj + 1], gjy);
-      atomicAdd(&P.grd[3 * aj + 2], gjz);
-    }
-    if (SPLIT && aj >= 0 && (gjx1 != 0.0 || gjy1 != 0.0 || gjz1 != 0.0)) {
-      atomicAdd(&P.grd1[3 * aj + 0], gjx1);
-      atomicAdd(&P.grd1[3 * aj + 1], gjy1);
-      atomicAdd(&P.grd1[3 * aj + 2], gjz1);
+      if (SPLIT && aj[e] >= 0 && (gj[6 + 3 * e] != 0.0 || gj[7 + 3 * e] != 0.0 || gj[8 + 3 * e] != 0.0)) {
+        atomicAdd(&P.grd1[3 * aj[e] + 0], gj[6 + 3 * e]);
+        atomicAdd(&P.grd1[3 * aj[e] + 1], gj[7 + 3 * e]);
+        atomicAdd(&P.grd1[3 * aj[e] + 2], gj[8 + 3 * e]);
+      }
     }
     if (COUNT) npair += tn;
     eel += to_fix(te, kEneScale, P.status);
     elj += to_fix(tl, kEneScale, P.status);
-    if (ALSD) { eaa += to_fix(ta, kEneScale, P.status); eab += to_fix(tb, kEneScale, P.status); }
+    if (ALSD || SPLIT) { eaa += to_fix(ta, kEneScale, P.status); eab += to_fix(tb, kEneScale, P.status); }
   }
-  if (ai >= 0) {
-    atomicAdd(&P.grd[3 * ai + 0], gix);
-    atomicAdd(&P.grd[3 * ai + 1], giy);
-    atomicAdd(&P.grd[3 * ai + 2], giz);
-    if (SPLIT) {
-      atomicAdd(&P.grd1[3 * ai + 0], gix1);
-      atomicAdd(&P.grd1[3 * ai + 1], giy1);
-      atomicAdd(&P.grd1[3 * ai + 2], giz1);
-    }
-  }
-  flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD);
+  flush_i();
+  flush_fix(P, cur_rep, eel, elj, eaa, eab, npair, COUNT, ALSD || SPLIT);
 }
 
 // the mixed kernels that read the type-triple table need more than the default 48 KiB of
