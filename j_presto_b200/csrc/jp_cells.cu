@@ -646,36 +646,45 @@ __global__ void k_ct_emit(DevPtrs P, int nchunk, int cmm) {
     const int nt = __popc(__ballot_sync(full, tq < t1 && qb < 32));   // lanes 0 .. nt-1
     unsigned cur = 0u, cur_el = 0u;
     int src = -1, kk = 0;   // this slot's source tile and its rank among the tile's entries
+    for (int j = 0; j < nt; ++j) {   // warp-uniform: every lane looks for its slot
+      const int base = __shfl_sync(full, qb, j);
+      const int n = __popc(__shfl_sync(full, qocc, j));   // both shuffles by every lane
+      const int k = lane - base;
+      if (k >= 0 && k < n) {
+        src = j;
+        kk = k;
+      }
+    }
+    // the row bits: the two half-warps compute the same 16 rows, so each takes every other
+    // source tile and the halves' bits are merged at the end
     for (int j0 = 0; j0 < nt; j0 += 4) {   // warp-uniform
-      unsigned m[4], me[4];
+      unsigned m[2], me[2];
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        m[v] = j0 + v < nt ? P.masks[(size_t)(ts + j0 + v) * 32 + ri] : 0u;
-        me[v] = cmm && j0 + v < nt ? P.masks_el[(size_t)(ts + j0 + v) * 32 + ri] : 0u;
+      for (int v = 0; v < 2; ++v) {
+        const int j = j0 + 2 * v + (lane >> 4);
+        m[v] = j < nt ? P.masks[(size_t)(ts + j) * 32 + ri] : 0u;
+        me[v] = cmm && j < nt ? P.masks_el[(size_t)(ts + j) * 32 + ri] : 0u;
       }
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int j = j0 + v;
+      for (int v = 0; v < 2; ++v) {
+        const int j = j0 + 2 * v + (lane >> 4);
         const int base = __shfl_sync(full, qb, j & 31);
         const unsigned occ = __shfl_sync(full, qocc, j & 31);
-        if (j >= nt) break;
-        const int n = __popc(occ);
-        const unsigned comp = compress_bits(__funnelshift_l(m[v], m[v], ri), occ);
-        const unsigned comp_el = cmm ? compress_bits(__funnelshift_l(me[v], me[v], ri), occ) : 0u;
-        if (base >= 0) {
-          cur |= comp << base;
-          cur_el |= comp_el << base;
-        } else {
-          cur |= comp >> -base;
-          cur_el |= comp_el >> -base;
-        }
-        const int k = lane - base;
-        if (k >= 0 && k < n) {
-          src = j;
-          kk = k;
+        if (j < nt) {
+          const unsigned comp = compress_bits(__funnelshift_l(m[v], m[v], ri), occ);
+          const unsigned comp_el = cmm ? compress_bits(__funnelshift_l(me[v], me[v], ri), occ) : 0u;
+          if (base >= 0) {
+            cur |= comp << base;
+            cur_el |= comp_el << base;
+          } else {
+            cur |= comp >> -base;
+            cur_el |= comp_el >> -base;
+          }
         }
       }
     }
+    cur |= __shfl_xor_sync(full, cur, 16);
+    if (cmm) cur_el |= __shfl_xor_sync(full, cur_el, 16);
     const int sy = __shfl_sync(full, qy, src & 31);
     const unsigned socc = __shfl_sync(full, qocc, src & 31);
     const float shx = __shfl_sync(full, qsh.x, src & 31);

@@ -380,7 +380,7 @@ class Engine:
         _chk(lib().jp_set_grid_limit(self._h, int(blocks)), "jp_set_grid_limit")
 
     def tile_shape(self, rep=0):
-        """(column-edge factor chosen for the replica, compact tiles per candidate)."""
+        """(column-edge factor chosen for the replica, pair records per candidate)."""
         f = C.c_double()
         t = (C.c_int64 * abi.JP_TUNE_CANDIDATES)()
         _chk(lib().jp_tile_shape(self._h, rep, C.byref(f), t), "jp_tile_shape")
