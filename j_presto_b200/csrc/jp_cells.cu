@@ -254,6 +254,7 @@ __device__ __forceinline__ unsigned tile_mask(const DevPtrs& P, const Rep& R, in
 struct IStage {
   double x[kTile], y[kTile], z[kTile];
   float xf[kTile], yf[kTile], zf[kTile];   // the same relative to the i block's reference
+  float4 live[kTile];                      // a candidate's live i atoms, compacted (x, y, z, lane)
 };
 
 // The exact list radius decides in FP64, but almost every pair is far from it: the mask is
@@ -270,7 +271,7 @@ struct IStage {
 // every pair's, so each pair takes its own minimum image in FP32 and no i atom is culled.
 template <bool PIMG>
 __device__ __forceinline__ unsigned tile_row_f32(const DevPtrs& P, const Rep& R, int bi, int bj, int lane,
-                                                 const IStage& S, float rlim2f, float band, bool& unsure) {
+                                                 IStage& S, float rlim2f, float band, bool& unsure) {
   const int aj = P.satom[bj * kTile + lane];
   float cj[3];   // block bj's reference (its bounding-box centre) in the i block's frame
   for (int k = 0; k < 3; ++k) {
@@ -293,9 +294,16 @@ __device__ __forceinline__ unsigned tile_row_f32(const DevPtrs& P, const Rep& R,
   const float ibx = (float)R.invbox[0], iby = (float)R.invbox[1], ibz = (float)R.invbox[2];
   unsigned row = 0;
   bool u = false;
-  // two i atoms per pass: two independent distance chains and ballots
-  auto d2of = [&](int i) {
-    float dx = S.xf[i] - r[0], dy = S.yf[i] - r[1], dz = S.zf[i] - r[2];
+  // the live i atoms compacted in shared memory, so each pass reads two of them by
+  // position instead of scanning the bit mask (bit scans run on the XU pipe); two i atoms
+  // per pass: two independent distance chains and ballots
+  const int nlive = __popc(live);
+  __syncwarp();   // the previous candidate's passes are done with S.live
+  if ((live >> lane) & 1u)
+    S.live[__popc(live & ((1u << lane) - 1u))] = make_float4(S.xf[lane], S.yf[lane], S.zf[lane], __int_as_float(lane));
+  __syncwarp();
+  auto d2of = [&](float4 a) {
+    float dx = a.x - r[0], dy = a.y - r[1], dz = a.z - r[2];
     if (PIMG) {
       dx = fmaf(-bx, rintf(dx * ibx), dx);
       dy = fmaf(-by, rintf(dy * iby), dy);
@@ -303,20 +311,19 @@ __device__ __forceinline__ unsigned tile_row_f32(const DevPtrs& P, const Rep& R,
     }
     return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
   };
-  while (live) {   // warp-uniform
-    const int i = __ffs(live) - 1;
-    live &= live - 1;
-    const int i2 = live ? __ffs(live) - 1 : -1;
-    live &= live - 1;
-    const float d2 = d2of(i), e2 = d2of(i2 < 0 ? i : i2);
+  for (int q = 0; q < nlive; q += 2) {   // warp-uniform
+    const bool has2 = q + 1 < nlive;
+    const float4 a = S.live[q];
+    const float4 c = S.live[has2 ? q + 1 : q];
+    const float d2 = d2of(a), e2 = d2of(c);
     const bool in = aj >= 0 && d2 <= rlim2f;
-    const bool in2 = aj >= 0 && i2 >= 0 && e2 <= rlim2f;
+    const bool in2 = aj >= 0 && has2 && e2 <= rlim2f;
     u |= aj >= 0 && fabsf(d2 - rlim2f) < band;
-    u |= aj >= 0 && i2 >= 0 && fabsf(e2 - rlim2f) < band;
+    u |= aj >= 0 && has2 && fabsf(e2 - rlim2f) < band;
     const unsigned b = __ballot_sync(0xffffffffu, in);
     const unsigned b2 = __ballot_sync(0xffffffffu, in2);
-    if (lane == i) row = b;
-    if (lane == i2) row = b2;
+    if (lane == __float_as_int(a.w)) row = b;
+    if (has2 && lane == __float_as_int(c.w)) row = b2;
   }
   unsure = __any_sync(0xffffffffu, u);
   return row;
@@ -367,7 +374,7 @@ __device__ __forceinline__ unsigned tile_mask_fast(const DevPtrs& P, const Rep& 
 }
 
 template <bool CMM>
-__global__ void __launch_bounds__(128) k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rlimf,
+__global__ void __launch_bounds__(128, 6) k_tile_scan_chunks(DevPtrs P, int nchunk, double rlim2, float rlimf,
                                                           double rc2) {
   const float rlim2f = (float)rlim2;
   __shared__ IStage s_i[4];
