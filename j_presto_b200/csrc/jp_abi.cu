@@ -1577,7 +1577,7 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   e |= dalloc(c, &P.tmp_masks, (size_t)c->tile_cap_total * 32);
   e |= dalloc(c, &P.tiles, (size_t)c->tile_cap_total);
   e |= dalloc(c, &P.tile_shift, (size_t)c->tile_cap_total);
-  e |= dalloc(c, &P.masks, (size_t)c->tile_cap_total * 32);
+  e |= dalloc(c, &P.tile_src, (size_t)c->tile_cap_total);
   // compact tiles: at most one per tile (an i-block's j entries never outnumber 32 per tile)
   e |= dput(c, &P.blk_chunk0, blk_chunk0);
   // pair records: at most one per tile and half (a unit's records never outnumber the tiles
@@ -1599,7 +1599,6 @@ int jp_create(const jp_system *sys, int32_t nrep, const jp_params *prm, jp_ctx *
   if (c->cmm) {
     int ntot = 0;
     for (int l = 1; l <= 5; ++l) ntot += c->cmm_ncell[l];
-    e |= dalloc(c, &P.masks_el, (size_t)c->tile_cap_total * 32);
     e |= dalloc(c, &P.tmp_masks_el, (size_t)c->tile_cap_total * 32);
     e |= dalloc(c, &P.cmm_cell, (size_t)N);
     if (!hres_cmm.empty()) e |= dput(c, &P.cmm_res, hres_cmm);

@@ -520,20 +520,13 @@ __global__ void k_tile_emit(DevPtrs P, int nchunk, int cmm) {
     const Rep& R = P.reps[P.blk_rep[bi]];
     const int bj = j0 + (int)__fns(nz, 0, lane + 1);
     P.tiles[t0 + lane] = make_int2(bi, bj);
+    P.tile_src[t0 + lane] = w * 32 + (bj - j0);   // its mask rows stay where the scan wrote them
     float sh[3];
     for (int k = 0; k < 3; ++k) {
       const double d = P.blk_ref[3 * bi + k] - P.blk_ref[3 * bj + k];
       sh[k] = (float)(d - R.box[k] * anint(d * R.invbox[k]));
     }
     P.tile_shift[t0 + lane] = make_float4(sh[0], sh[1], sh[2], 0.f);
-  }
-  unsigned m = nz;   // masks: one coalesced row of 32 per tile
-#pragma unroll 4
-  for (int q = 0; q < cnt; ++q) {
-    const int b = __ffs(m) - 1;
-    m &= m - 1;
-    P.masks[(size_t)(t0 + q) * 32 + lane] = P.tmp_masks[((size_t)w * 32 + b) * 32 + lane];
-    if (cmm) P.masks_el[(size_t)(t0 + q) * 32 + lane] = P.tmp_masks_el[((size_t)w * 32 + b) * 32 + lane];
   }
 }
 
@@ -639,7 +632,7 @@ __global__ void k_ct_emit(DevPtrs P, int nchunk, int cmm) {
     const int ts = info.x, s0 = info.y, e1 = info.z, t1 = info.w >> 1, h = info.w & 1;
     const int tq = ts + lane;   // lane q: source tile q
     const int ri = kHalf * h + (lane & (kHalf - 1));   // this lane's row of the i-block
-    int qb = 32, qy = 0;
+    int qb = 32, qy = 0, qs = 0;
     unsigned qocc = 0u;
     float4 qsh = make_float4(0.f, 0.f, 0.f, 0.f);
     if (tq < t1) {
@@ -648,6 +641,7 @@ __global__ void k_ct_emit(DevPtrs P, int nchunk, int cmm) {
         qocc = P.tile_occ[2 * (size_t)tq + h];
         qy = P.tiles[tq].y;
         qsh = P.tile_shift[tq];
+        qs = P.tile_src[tq];
       }
     }
     const int nt = __popc(__ballot_sync(full, tq < t1 && qb < 32));   // lanes 0 .. nt-1
@@ -669,8 +663,9 @@ __global__ void k_ct_emit(DevPtrs P, int nchunk, int cmm) {
 #pragma unroll
       for (int v = 0; v < 2; ++v) {
         const int j = j0 + 2 * v + (lane >> 4);
-        m[v] = j < nt ? P.masks[(size_t)(ts + j) * 32 + ri] : 0u;
-        me[v] = cmm && j < nt ? P.masks_el[(size_t)(ts + j) * 32 + ri] : 0u;
+        const int sm = __shfl_sync(full, qs, j & 31);   // the tile's rows in tmp_masks
+        m[v] = j < nt ? P.tmp_masks[(size_t)sm * 32 + ri] : 0u;
+        me[v] = cmm && j < nt ? P.tmp_masks_el[(size_t)sm * 32 + ri] : 0u;
       }
 #pragma unroll
       for (int v = 0; v < 2; ++v) {

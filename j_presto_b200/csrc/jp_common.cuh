@@ -188,7 +188,7 @@ struct DevPtrs {
   // tiles
   int2 *tiles;                    // dense (i-block, j-block)
   float4 *tile_shift;             // dense min-image shift of block refs (mixed path)
-  unsigned *masks;                // dense masks [T][32]
+  int *tile_src;                  // [T] where each tile's mask rows are in tmp_masks: chunk * 32 + candidate
   int *ntiles;                    // device scalar
   // compact tiles (what the pair kernels run on): an i-block and 32 j entries
   int *blk_chunk0;                // [nblk+1] first chunk of each i-block (static)
@@ -233,7 +233,7 @@ struct DevPtrs {
   double *cmm_pot, *cmm_raw, *cmm_c0;
   long long *cmm_e, *cmm_enew;
   long long *ene_ext;             // EXTCMM energy of the step, per replica (fixed point)
-  unsigned *masks_el, *tmp_masks_el;   // CMM tiles: pairs with the Coulomb term
+  unsigned *tmp_masks_el;         // CMM tiles: pairs with the Coulomb term (as tmp_masks)
   unsigned char *ext_flag;        // EXTCMM: occupied external level-1 cells (CMM cell index)
   double *ext_pot;                // their 13 coefficients
   // accumulators

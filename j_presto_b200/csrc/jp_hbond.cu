@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(kHbThreads) k_hb_list(DevPtrs P, int cap, int 
     const int ti = P.styp[si] & kTypeMask, tj = P.styp[sj] & kTypeMask;
     const bool hi = P.hb_type[ti] != 0;
     if (!__any_sync(full, hi) || !__any_sync(full, P.hb_type[tj] != 0)) continue;
-    const unsigned m = P.masks[(size_t)t * 32 + lane];
+    const unsigned m = P.tmp_masks[(size_t)P.tile_src[t] * 32 + lane];
     unsigned hm = 0;
     for (int k = 0; k < 32; ++k) {
       const int tk = __shfl_sync(full, tj, (lane + k) & 31);
