@@ -433,8 +433,8 @@ def main():
     ntiles, nlisted, _ = eng.list_stats()
     per_step, per_rebuild = eng.launch_counts()
     shapes = [eng.tile_shape(r) for r in range(nrep)]
-    tshape = {"note": "block-shape tuner: per replica the column-edge factor with the fewest compact "
-                      "tiles of five (jp_tile_shape); counts of the 64 replicas summed per factor",
+    tshape = {"note": "block-shape tuner: per replica the column-edge factor with the fewest pair "
+                      "records of five (jp_tile_shape); counts of the 64 replicas summed per factor",
               "chosen_factor_counts": {str(f): sum(1 for g, _ in shapes if g == f)
                                        for f in sorted({g for g, _ in shapes})},
               "tiles_per_factor": [int(sum(t[q] for _, t in shapes)) for q in range(5)],

@@ -1,7 +1,7 @@
 """The block-shape tuner of jp_create (the role of md_run's SIMD_check.f90 autotuning).
 
 Every replica's list is built with each candidate column grid and the grid needing the
-fewest compact tiles is kept.  Checked: the kept candidate is the minimum of the reported
+fewest pair records is kept.  Checked: the kept candidate is the minimum of the reported
 counts; two contexts on the same input choose the same and report the same counts (the
 choice is deterministic); a replica chooses alone as it does in a batch; with tuning off
 the unit factor is kept; the forces do not depend on the block shape (FP64 path, RMS
@@ -64,6 +64,6 @@ def test_forces_do_not_depend_on_the_shape(eng_mod, tops):
     (e1, g1), p1, l1 = out[1]
     assert p0 == p1 and l0 == l1
     assert rms_rel(g1, g0) < 1e-12
-    # energies: each compact tile's FP64 sum enters in 2^-32 fixed point, and other tiles
+    # energies: each pair record's FP64 sum enters in 2^-32 fixed point, and other records
     # round differently (~1e-10 per tile)
     np.testing.assert_allclose(e1, e0, rtol=1e-9, atol=1e-6)
