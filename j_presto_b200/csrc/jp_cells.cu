@@ -582,29 +582,6 @@ __global__ void k_ct_index(DevPtrs P, int nchunk) {
   }
 }
 
-// The bits of x at the set bits of m, packed to the low end (a bit-compress, Hacker's
-// Delight 7-4): five rounds move each kept bit right by the number of cleared mask bits
-// below it.  The mask-dependent part is the same in every lane of a tile (m is the tile's
-// occupied j lanes).
-__device__ __forceinline__ unsigned compress_bits(unsigned x, unsigned m) {
-  x &= m;
-  unsigned mk = ~m << 1;
-#pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    unsigned mp = mk ^ (mk << 1);
-    mp ^= mp << 2;
-    mp ^= mp << 4;
-    mp ^= mp << 8;
-    mp ^= mp << 16;
-    const unsigned mv = mp & m;
-    m = (m ^ mv) | (mv >> (1 << i));
-    const unsigned t = x & mv;
-    x = (x ^ t) | (t >> (1 << i));
-    mk &= ~mp;
-  }
-  return x;
-}
-
 // a record row (bit e: entry e) into the kernels' order for i atom l: each 16-bit half
 // rotated right by l
 __device__ __forceinline__ unsigned record_row(unsigned row, int l) {
@@ -614,14 +591,13 @@ __device__ __forceinline__ unsigned record_row(unsigned row, int l) {
   return rl | (rh << 16);
 }
 
-// One warp per record: lane l's row (row 16 h + l of the i-block, l < 16; lanes 16-31 repeat
-// lanes 0-15) collects, from each tile whose entries fall in the record's 32 slots, the bits
-// of that tile's row at its occupied j lanes of half h (packed in lane order); lane p writes
-// slot p's entry.  Those source tiles are consecutive from ct_src and at most 32 (each holds
-// at least one entry and the first covers slot 0), so lane q reads source tile q's offset,
-// occupancy, j block and image shift in one coalesced pass, the mask rows are read four tiles
-// at a time, and each slot's entry comes from its tile's lane by shuffles: no load waits on
-// another.
+// One warp per record, lane p for slot p.  The record's source tiles are consecutive from
+// ct_info's first tile and at most 32 (each holds at least one entry and the first covers
+// slot 0), so lane q reads source tile q's entry offset, occupancy, j block, image shift and
+// mask rows' place in one coalesced pass; each slot finds its tile and its rank among the
+// tile's entries by shuffles, and writes its entry.  Record row r (i atom 16 h + r) is then
+// one ballot: every slot contributes the bit of its j lane in row 16 h + r of its tile, so no
+// lane packs bits and lane r keeps row r.
 __global__ void k_ct_emit(DevPtrs P, int nchunk, int cmm) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -631,7 +607,6 @@ __global__ void k_ct_emit(DevPtrs P, int nchunk, int cmm) {
     const int4 info = P.ct_info[ct];
     const int ts = info.x, s0 = info.y, e1 = info.z, t1 = info.w >> 1, h = info.w & 1;
     const int tq = ts + lane;   // lane q: source tile q
-    const int ri = kHalf * h + (lane & (kHalf - 1));   // this lane's row of the i-block
     int qb = 32, qy = 0, qs = 0;
     unsigned qocc = 0u;
     float4 qsh = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -656,46 +631,40 @@ __global__ void k_ct_emit(DevPtrs P, int nchunk, int cmm) {
         kk = k;
       }
     }
-    // the row bits: the two half-warps compute the same 16 rows, so each takes every other
-    // source tile and the halves' bits are merged at the end
-    for (int j0 = 0; j0 < nt; j0 += 4) {   // warp-uniform
-      unsigned m[2], me[2];
-#pragma unroll
-      for (int v = 0; v < 2; ++v) {
-        const int j = j0 + 2 * v + (lane >> 4);
-        const int sm = __shfl_sync(full, qs, j & 31);   // the tile's rows in tmp_masks
-        m[v] = j < nt ? P.tmp_masks[(size_t)sm * 32 + ri] : 0u;
-        me[v] = cmm && j < nt ? P.tmp_masks_el[(size_t)sm * 32 + ri] : 0u;
-      }
-#pragma unroll
-      for (int v = 0; v < 2; ++v) {
-        const int j = j0 + 2 * v + (lane >> 4);
-        const int base = __shfl_sync(full, qb, j & 31);
-        const unsigned occ = __shfl_sync(full, qocc, j & 31);
-        if (j < nt) {
-          const unsigned comp = compress_bits(__funnelshift_l(m[v], m[v], ri), occ);
-          const unsigned comp_el = cmm ? compress_bits(__funnelshift_l(me[v], me[v], ri), occ) : 0u;
-          if (base >= 0) {
-            cur |= comp << base;
-            cur_el |= comp_el << base;
-          } else {
-            cur |= comp >> -base;
-            cur_el |= comp_el >> -base;
-          }
-        }
-      }
-    }
-    cur |= __shfl_xor_sync(full, cur, 16);
-    if (cmm) cur_el |= __shfl_xor_sync(full, cur_el, 16);
     const int sy = __shfl_sync(full, qy, src & 31);
     const unsigned socc = __shfl_sync(full, qocc, src & 31);
+    const int sm = __shfl_sync(full, qs, src & 31);   // the source tile's rows in tmp_masks
     const float shx = __shfl_sync(full, qsh.x, src & 31);
     const float shy = __shfl_sync(full, qsh.y, src & 31);
     const float shz = __shfl_sync(full, qsh.z, src & 31);
+    const bool live = src >= 0 && s0 + lane < e1;
+    const int jl = live ? (int)__fns(socc, 0, kk + 1) : 0;   // the slot's j lane in its tile
     float4 ent = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-    if (src >= 0 && s0 + lane < e1)
-      ent = make_float4(shx, shy, shz, __int_as_float(sy * kTile + (int)__fns(socc, 0, kk + 1)));
+    if (live) ent = make_float4(shx, shy, shz, __int_as_float(sy * kTile + jl));
     P.ct_j[(size_t)ct * 32 + lane] = ent;
+    // record row r (bit p: slot p) is one ballot: slot p's bit is bit jl of row 16 h + r of its
+    // source tile (stored rotated: bit k is j lane (row + k) & 31); lane r keeps row r
+    {
+      const unsigned* rows = P.tmp_masks + (size_t)(live ? sm : 0) * 32 + kHalf * h;
+      unsigned m[kHalf];
+#pragma unroll
+      for (int r = 0; r < kHalf; ++r) m[r] = live ? rows[r] : 0u;
+#pragma unroll
+      for (int r = 0; r < kHalf; ++r) {
+        const unsigned row = __ballot_sync(full, (m[r] >> ((jl - kHalf * h - r) & 31)) & 1u);
+        if (lane == r) cur = row;
+      }
+      if (cmm) {
+        const unsigned* rows_el = P.tmp_masks_el + (size_t)(live ? sm : 0) * 32 + kHalf * h;
+#pragma unroll
+        for (int r = 0; r < kHalf; ++r) m[r] = live ? rows_el[r] : 0u;
+#pragma unroll
+        for (int r = 0; r < kHalf; ++r) {
+          const unsigned row = __ballot_sync(full, (m[r] >> ((jl - kHalf * h - r) & 31)) & 1u);
+          if (lane == r) cur_el = row;
+        }
+      }
+    }
     if (lane < kHalf) {
       P.ct_mask[(size_t)ct * kHalf + lane] = record_row(cur, lane);
       if (cmm) P.ct_mask_el[(size_t)ct * kHalf + lane] = record_row(cur_el, lane);

@@ -12,6 +12,7 @@ MICR, CANO in both integrator forms, McMD with the network weight, ALSD, CMM, H-
 restraints with the CAP, steepest descent, network training).
 """
 import argparse
+import time
 
 import numpy as np
 
@@ -91,6 +92,8 @@ def main():
     ap.add_argument("--method", default="cano", choices=["micr", "cano"])
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--direct", action="store_true")
+    ap.add_argument("--rebuilds", type=int, default=0,
+                    help="then time this many list builds (host clock around each synchronous call)")
     ap.add_argument("--tempco", type=int, default=2, choices=[1, 2])
     a = ap.parse_args()
     build.build()
@@ -110,9 +113,15 @@ def main():
         e.step(a.steps, energies=False, temps=False)
         tot, ph, ln = e.last_timing()
         nt, nl, ns = e.list_stats()
+        reb = []
+        for _ in range(a.rebuilds):
+            t0 = time.perf_counter()
+            e.rebuild()
+            reb.append(1e3 * (time.perf_counter() - t0))
     natom = sum(t["natom"] for t in top) if isinstance(top, list) else top["natom"]
     print(f"{a.workload} natom={natom} steps={a.steps} ms/step={tot / a.steps:.4f} "
-          f"tiles={nt} listed={nl} phases_ms={[round(p, 4) for p in ph]} launches={ln}")
+          f"tiles={nt} listed={nl} phases_ms={[round(p, 4) for p in ph]} launches={ln}"
+          + (f" rebuild_ms_median={sorted(reb)[len(reb) // 2]:.4f}" if reb else ""))
 
 
 if __name__ == "__main__":
