@@ -2,7 +2,7 @@
 
 GEprep fits d lnN/dE by windowed polynomials (jp_ge_fit).  Here the same data also trains a
 64-64 tanh network on the GPU (jp_mlp_train); the polynomial remains the fallback and the
-judge: the network is taken only if the flatness it predicts for the next run is no worse
+yardstick: the network is taken only if the flatness it predicts for the next run is no worse
 than the polynomial's.
 
 Predicted flatness.  With the data's d lnN/dE estimate y(x) and a candidate weight f(x), a

@@ -8,7 +8,7 @@ GEprep distrib_ALSD fit of the weight in lambda, and the (E, lambda) network wei
 * one iteration on four small replicas: the polynomial weight from distrib_ALSD and the
   network trained on the (E, lambda) histograms each drive a run from the same state; both
   runs count every step, and the network is kept only if the flatness measured on its run
-  (GEprep's percentage) is no worse than the polynomial's, the polynomial being the judge.
+  (GEprep's percentage) is no worse than the polynomial's, the polynomial being the yardstick.
 """
 import numpy as np
 import pytest

@@ -1,6 +1,6 @@
 """One McMD weight iteration measured, not predicted: four small McMD replicas run with a
 starting weight and record their energy histograms on the device; GEprep's fit (the
-polynomial, fallback and judge) and the surrogate network are made from those histograms;
+polynomial, fallback and yardstick) and the surrogate network are made from those histograms;
 each then drives the next run of all four replicas from the same state, and the flatness
 of the energy histograms those runs actually record (distrib_MULT's percentage and the
 max/min visit ratio) decides: the network is kept only if it is no worse.

@@ -1,5 +1,5 @@
 """The CPU oracle against the closed-form known-answer vectors (tests/golden/kat.json)
-and analytic identities.  Pins the oracle before it is used to judge the CUDA engine."""
+and analytic identities.  Pins the oracle before it is used to check the CUDA engine."""
 import numpy as np
 import pytest
 
